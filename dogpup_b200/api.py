@@ -1,0 +1,198 @@
+"""Thin, typed wrappers over the C ABI on torch device tensors.
+
+PyTorch only provides device memory and the current stream here; every
+operation runs in libdogpup_b200's CUDA kernels.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import torch
+
+from . import _lib
+from ._lib import lib, check
+
+
+def stream_ptr() -> int:
+    return torch.cuda.current_stream().cuda_stream
+
+
+def ptr(t: torch.Tensor) -> int:
+    if not t.is_cuda:
+        raise ValueError("dogpup_b200 operates on CUDA tensors")
+    if not t.is_contiguous():
+        raise ValueError("tensor must be contiguous")
+    return t.data_ptr()
+
+
+def as_real(t: torch.Tensor) -> torch.Tensor:
+    """complex tensor -> interleaved real view (no copy)."""
+    return torch.view_as_real(t) if t.is_complex() else t
+
+
+class Fem:
+    """Device FEM topology + assembly plan (``prepare_mesh``/``gen_fwdmat``, dMesh.m:945-1235)."""
+
+    def __init__(self, node: torch.Tensor, elem: torch.Tensor, nr: float):
+        node = node.to(device="cuda", dtype=torch.float64).contiguous()
+        elem = elem.to(device="cuda", dtype=torch.int32).contiguous()
+        self.nn, self.ne = int(node.shape[0]), int(elem.shape[0])
+        h = C.c_void_p()
+        check(lib.dgp_fem_create(C.byref(h), ptr(node), ptr(elem), self.nn, self.ne, float(nr), stream_ptr()))
+        self._h = h
+        nnz, nf, nb, c = C.c_int64(), C.c_int64(), C.c_int64(), C.c_double()
+        check(lib.dgp_fem_info(h, C.byref(nnz), C.byref(nf), C.byref(nb), C.byref(c)))
+        self.nnz, self.n_robin_faces, self.n_boundary, self.c = nnz.value, nf.value, nb.value, c.value
+        rp, cp = C.c_void_p(), C.c_void_p()
+        check(lib.dgp_fem_pattern(h, C.byref(rp), C.byref(cp)))
+        # own copies of the pattern as torch tensors
+        self.rowptr = torch.empty(self.nn + 1, dtype=torch.int32, device="cuda")
+        self.col = torch.empty(self.nnz, dtype=torch.int32, device="cuda")
+        _d2d(self.rowptr, rp.value)
+        _d2d(self.col, cp.value)
+        self.bnd = torch.empty(self.nn, dtype=torch.int32, device="cuda")
+        check(lib.dgp_fem_boundary(h, ptr(self.bnd), stream_ptr()))
+
+    def assemble(self, mua: torch.Tensor, musp: torch.Tensor):
+        mua = mua.to(device="cuda", dtype=torch.float64).contiguous()
+        musp = musp.to(device="cuda", dtype=torch.float64).contiguous()
+        K = torch.empty(self.nnz, dtype=torch.float64, device="cuda")
+        M = torch.empty(self.nnz, dtype=torch.float64, device="cuda")
+        check(lib.dgp_fem_assemble(self._h, ptr(mua), ptr(musp), ptr(K), ptr(M), stream_ptr()))
+        return K, M
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib.dgp_fem_destroy(h)
+            self._h = None
+
+
+def _d2d(dst: torch.Tensor, src_ptr: int):
+    """Copy library-owned device memory into a torch tensor of the same size."""
+    dst.copy_(_borrow(src_ptr, dst.numel(), dst.dtype))
+
+
+def _borrow(p: int, n: int, dtype) -> torch.Tensor:
+    """Non-owning tensor view of device memory owned by the library."""
+    class _Holder:
+        def __init__(self, p, n, dtype):
+            typestr = {torch.int32: "<i4", torch.float64: "<f8"}[dtype]
+            self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (p, False), "version": 3,
+                                             "strides": None}
+    return torch.as_tensor(_Holder(p, n, dtype), device="cuda")
+
+
+class Solver:
+    """Batched FSAI-BiCGSTAB plan for A_k = K + i*k*dfc*M (gpuBicstab_FSAIP, dMesh.m:1247-1385)."""
+
+    def __init__(self, rowptr, col, K, M, dfc: float, nf: int, ns_max: int, opts: _lib.SolveOpts | None = None):
+        self.n = int(rowptr.numel() - 1)
+        self.nnz = int(col.numel())
+        self.nf, self.ns_max, self.dfc = int(nf), int(ns_max), float(dfc)
+        o = opts or _lib.default_opts()
+        h = C.c_void_p()
+        check(lib.dgp_solver_create(C.byref(h), ptr(rowptr), ptr(col), self.n, self.nnz, ptr(K), ptr(M),
+                                    self.dfc, self.nf, self.ns_max, C.byref(o), stream_ptr()))
+        self._h = h
+
+    def update(self, K, M):
+        check(lib.dgp_solver_update(self._h, ptr(K), ptr(M), stream_ptr()))
+
+    def memory(self) -> int:
+        b = C.c_int64()
+        check(lib.dgp_solver_memory(self._h, C.byref(b)))
+        return b.value
+
+    def profile_kernel(self, which: int, reps: int = 10):
+        """(ms per launch, algorithmic bytes per launch) of one sweep kernel, CUDA-event timed."""
+        ms, b = C.c_float(), C.c_double()
+        check(lib.dgp_solver_profile_kernel(self._h, which, reps, C.byref(ms), C.byref(b), stream_ptr()))
+        return ms.value, b.value
+
+    def solve(self, B: torch.Tensor, opts=None, status=None):
+        """X[k] = A_k^-1 B[k], B complex128 [NF][NN][NS]."""
+        nf, n, ns = B.shape
+        X = torch.empty_like(B)
+        rep = _lib.SolveReport()
+        if status is not None:
+            rep.d_status = ptr(status)
+        o = opts or _lib.default_opts()
+        rc = lib.dgp_solve(self._h, ptr(as_real(B)), ptr(as_real(X)), ns, C.byref(o), C.byref(rep), stream_ptr())
+        check(rc, allow=(_lib.ERR_NOT_CONVERGED,))
+        return X, rep
+
+    def solve_sources(self, nodes, w, fpsf, opts=None, status=None, out=None):
+        """Point-source right-hand sides b[k][nodes[s,l]][s] = w[s,l]*fpsf[k] (dMesh.m:124-129)."""
+        ns = int(nodes.shape[0])
+        X = out if out is not None else torch.empty((self.nf, self.n, ns), dtype=torch.complex128, device="cuda")
+        rep = _lib.SolveReport()
+        if status is not None:
+            rep.d_status = ptr(status)
+        o = opts or _lib.default_opts()
+        rc = lib.dgp_solve_sources(self._h, ptr(nodes), ptr(w), ptr(as_real(fpsf)), ns, ptr(as_real(X)),
+                                   C.byref(o), C.byref(rep), stream_ptr())
+        check(rc, allow=(_lib.ERR_NOT_CONVERGED,))
+        return X, rep
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib.dgp_solver_destroy(h)
+            self._h = None
+
+
+def make_opts(**kw) -> _lib.SolveOpts:
+    o = _lib.default_opts()
+    for k, v in kw.items():
+        if v is None:
+            continue
+        if k == "precision" and isinstance(v, str):
+            v = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}[v]
+        if k == "stop_rule" and isinstance(v, str):
+            v = {"max_all": _lib.STOP_MAX_ALL, "per_column": _lib.STOP_PER_COLUMN}[v]
+        setattr(o, k, v)
+    return o
+
+
+# ------------------------------------------------------------- transforms
+def td2fc(x: torch.Tensor, f: torch.Tensor, t: torch.Tensor) -> torch.Tensor:
+    """Fourier-series coefficients along the last axis (td2fc.m:26-32)."""
+    x2 = x.to(torch.float64).reshape(-1, x.shape[-1]).contiguous()
+    f = f.to(device="cuda", dtype=torch.float64).contiguous()
+    t = t.to(device="cuda", dtype=torch.float64).contiguous()
+    out = torch.empty((x2.shape[0], f.numel()), dtype=torch.complex128, device="cuda")
+    check(lib.dgp_td2fc(ptr(x2), x2.shape[0], x2.shape[1], ptr(t), ptr(f), f.numel(), ptr(as_real(out)),
+                        stream_ptr()))
+    return out.reshape(*x.shape[:-1], f.numel())
+
+
+def fc2td(c: torch.Tensor, f: torch.Tensor, t: torch.Tensor) -> torch.Tensor:
+    """Time-domain signal from coefficients along the last axis (fc2td.m:60-71)."""
+    c2 = c.to(torch.complex128).reshape(-1, c.shape[-1]).contiguous()
+    f = f.to(device="cuda", dtype=torch.float64).contiguous()
+    t = t.to(device="cuda", dtype=torch.float64).contiguous()
+    out = torch.empty((c2.shape[0], t.numel()), dtype=torch.float64, device="cuda")
+    check(lib.dgp_fc2td(ptr(as_real(c2)), c2.shape[0], c2.shape[1], ptr(f), ptr(t), t.numel(), ptr(out),
+                        stream_ptr()))
+    return out.reshape(*c.shape[:-1], t.numel())
+
+
+def fc2tg(c: torch.Tensor, gate_fc: torch.Tensor, nt: int) -> torch.Tensor:
+    """Time-gated data from coefficients along the last axis (fc2tg.m:100-111)."""
+    c2 = c.to(torch.complex128).reshape(-1, c.shape[-1]).contiguous()
+    g = gate_fc.to(device="cuda", dtype=torch.complex128).contiguous()
+    out = torch.empty((c2.shape[0], g.shape[0]), dtype=torch.float64, device="cuda")
+    check(lib.dgp_fc2tg(ptr(as_real(c2)), c2.shape[0], c2.shape[1], ptr(as_real(g)), g.shape[0], int(nt),
+                        ptr(out), stream_ptr()))
+    return out.reshape(*c.shape[:-1], g.shape[0])
+
+
+def meas(det_nodes, det_w, link, phi) -> torch.Tensor:
+    """Detector data [NM][NF] from phi [NF][NN][NS] (meas_flu, dMesh.m:144-171)."""
+    nf, n, ns = phi.shape
+    nm = int(link.shape[0])
+    out = torch.empty((nm, nf), dtype=torch.complex128, device="cuda")
+    check(lib.dgp_meas(ptr(det_nodes), ptr(det_w), int(det_nodes.shape[0]), ptr(link), nm, ptr(as_real(phi)), n,
+                       nf, ns, ptr(as_real(out)), stream_ptr()))
+    return out

@@ -1,0 +1,95 @@
+// Internal plan structures shared by the dogpup_b200 translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dgp_common.cuh"
+
+namespace dgp {
+
+// ------------------------------------------------------------------ FEM
+struct FemPlan {
+  int64_t nn = 0, ne = 0, nfaces = 0, nnz = 0, nk = 0, nbnd = 0;
+  double nr = 0, c = 0, rfac = 0;
+  DevBuf node, elem;      // copies of the mesh
+  DevBuf bnd;             // int32 [nn]
+  DevBuf faces;           // int32 [nfaces][3] Robin face set
+  DevBuf rowptr, col;     // int32 CSR pattern (full symmetric)
+  DevBuf cstart, payload; // per-slot contribution lists
+  DevBuf Ke, Me, Be;      // element / face blocks (scratch of every assembly)
+};
+
+int fem_create(FemPlan *F, const double *d_node, const int32_t *d_elem, int64_t nn, int64_t ne, double nr,
+               cudaStream_t st);
+int fem_assemble(FemPlan *F, const double *d_mua, const double *d_musp, double *d_K, double *d_M,
+                 cudaStream_t st);
+
+// ----------------------------------------------------------------- FSAI
+struct FsaiPattern {
+  int64_t n = 0, nnzG = 0;
+  int32_t mmax = 0;          // longest pattern row
+  DevBuf rowptr, col;        // lower-triangular pattern of G
+  DevBuf rowptrT, colT;      // pattern of G^T
+  DevBuf permT;              // G^T slot t holds G slot permT[t]
+};
+
+int fsai_pattern_build(FsaiPattern *P, const int32_t *d_rowptr, const int32_t *d_col, const double *d_K,
+                       const double *d_M, double dfc, int64_t n, int32_t cap, cudaStream_t st);
+// pattern counts / fill as exposed by the C ABI
+int fsai_pattern_rows(const int32_t *d_rowptr, const int32_t *d_col, const double *d_K, const double *d_M,
+                      double dfc, int64_t n, int32_t cap, int32_t *d_rowptrG, int32_t *d_colG,
+                      int32_t *h_nnzG, int32_t *h_mmax, cudaStream_t st);
+// G values for harmonics k = k0 .. k0+nf-1 of A_k = Re + i*k*Im, written to
+// out[slot * s_slot + (k-k0) * s_k] (complex128 interleaved).
+int fsai_factor_run(const int32_t *d_rowptr, const int32_t *d_col, const double *d_re, const double *d_im,
+                    int64_t n, const int32_t *d_rowptrG, const int32_t *d_colG, int32_t mmax, int32_t nf,
+                    double2 *d_out, int64_t s_slot, int64_t s_k, cudaStream_t st);
+int fsai_transpose_pattern(FsaiPattern *P, cudaStream_t st);
+int fsai_factor_full(const int32_t *d_rowptr, const int32_t *d_col, const double *d_K, const double *d_M, double dfc,
+                     int64_t n, const int32_t *d_rowptrG, const int32_t *d_colG, int32_t nf, double2 *d_G,
+                     cudaStream_t st);
+
+// ---------------------------------------------------------------- solver
+struct SolverPlan {
+  int64_t n = 0, nnz = 0, nnzG = 0;
+  int32_t nf = 0, ns_max = 0, nsp = 0;  // nsp: padded sources per harmonic
+  double dfc = 0;
+  dgp_solve_opts opts{};
+  DevBuf rowptr, col;            // A pattern
+  DevBuf KM64, KM32;             // interleaved (K, M) per slot
+  DevBuf omega;                  // [nf] k * dfc
+  FsaiPattern P;
+  DevBuf G64, GT64, G32, GT32;   // [nf][nnzG] complex
+  // workspace (allocated lazily per precision)
+  int ws_prec = -1;
+  int64_t ws_cols = 0;
+  DevBuf vec[12];                // solver vectors
+  DevBuf x64, r64;               // mixed: FP64 solution and residual work
+  DevBuf scal;                   // per-column scalars
+  DevBuf ctl;                    // control block
+  DevBuf status;                 // per-column status
+  void *h_ctl = nullptr;         // pinned mirror of the control block
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  int graph_iters[2] = {0, 0};
+  int64_t bytes = 0;
+  ~SolverPlan();
+};
+
+int solver_build(SolverPlan *S, const int32_t *d_rowptr, const int32_t *d_col, int64_t n, int64_t nnz,
+                 const double *d_K, const double *d_M, double dfc, int32_t nf, int32_t ns_max,
+                 const dgp_solve_opts *opts, cudaStream_t st);
+int solver_update(SolverPlan *S, const double *d_K, const double *d_M, cudaStream_t st);
+int solver_solve(SolverPlan *S, const double *d_B, const int32_t *d_nodes, const double *d_w,
+                 const double *d_fpsf, double *d_X, int32_t ns, const dgp_solve_opts *opts,
+                 dgp_solve_report *rep, cudaStream_t st);
+
+int solver_profile(SolverPlan *S, int which, int reps, float *ms, double *bytes, cudaStream_t st);
+
+// batched operators (layout [nf][n][ns] complex)
+int spmm_A_f64(const int32_t *rowptr, const int32_t *col, const double2 *KM, const double *omega, int64_t n,
+               int32_t nf, int32_t ns, const double2 *X, double2 *Y, cudaStream_t st);
+int fsai_apply_f64(const int32_t *rowptr, const int32_t *col, const double2 *G, int64_t n, int64_t nnzG,
+                   int32_t nf, int32_t ns, const double2 *X, double2 *Y, cudaStream_t st);
+
+}  // namespace dgp

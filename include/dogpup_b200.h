@@ -1,0 +1,246 @@
+/*
+ * dogpup_b200.h -- C ABI of the B200 (sm_100a) forward/sensitivity path of
+ * DOGPUP (diffuse optical tomography: frequency-domain diffusion FEM,
+ * FSAI-preconditioned BiCGSTAB over all source x harmonic right-hand sides,
+ * adjoint absorption Jacobian, Fourier-series time-domain / time-gate
+ * transforms, weighted Levenberg-Marquardt normal-equation step).
+ *
+ * Conventions
+ *   - Every pointer named d_* is device memory owned by the caller unless a
+ *     function says otherwise; h_* is host memory.
+ *   - Complex numbers are interleaved (re, im) pairs of double or float.
+ *   - Batched fields use the layout [NF][NN][NS]: harmonic k slowest, node i,
+ *     source s fastest (element (k,i,s) at ((k*NN)+i)*NS+s).  The
+ *     MATLAB-facing drop-ins below keep the reference's own layouts.
+ *   - Indices are 0-based int32; element counts and offsets are int64.
+ *   - Functions return 0 (DGP_OK) or a dgp_status code; dgp_last_error()
+ *     returns a message for the calling thread's last failure.
+ *   - Work is enqueued on the given stream and is asynchronous unless a
+ *     function says it synchronises.
+ */
+#ifndef DOGPUP_B200_H
+#define DOGPUP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *dgp_stream_t; /* same type as cudaStream_t */
+
+typedef enum dgp_status {
+  DGP_OK = 0,
+  DGP_ERR_ARG = 1,        /* invalid argument or size                       */
+  DGP_ERR_CUDA = 2,       /* a CUDA runtime call failed                     */
+  DGP_ERR_NOMEM = 3,      /* device allocation failed                       */
+  DGP_ERR_MESH = 4,       /* degenerate mesh / pattern (e.g. zero volume)   */
+  DGP_ERR_NOT_CONVERGED = 5, /* solver hit maxit before tol (x still valid) */
+  DGP_ERR_BREAKDOWN = 6,  /* BiCGSTAB breakdown (rho or omega = 0 / non-finite) */
+  DGP_ERR_UNSUPPORTED = 7
+} dgp_status;
+
+/* Per-column solver status words written to dgp_solve_report.d_status. */
+enum {
+  DGP_COL_CONVERGED = 0,
+  DGP_COL_MAXIT = 1,
+  DGP_COL_BREAKDOWN_RHO = 2,
+  DGP_COL_BREAKDOWN_OMEGA = 3,
+  DGP_COL_NONFINITE = 4,
+  DGP_COL_ZERO_RHS = 5
+};
+
+const char *dgp_last_error(void);
+const char *dgp_status_string(int status);
+int dgp_version(void);
+
+/* ====================================================================== *
+ *  Drop-in host functions of the reference mex sources.  Same names,
+ *  argument order and layouts (split real/imag planes, column-major
+ *  [N x NS x NF]); C++ linkage like the reference headers, declared in
+ *  dogpup_b200_mex.hpp.  The extern "C" forms below add a stream and a
+ *  status return.
+ * ====================================================================== */
+
+/* Replaces smv_call, cuda_lib/mex_sources/smvMex.hpp:4-15 (smv_CUDA.cu:59-82):
+ * y[:,s,f] = (Re A + i*fAxis[f]*Im A) x[:,s,f], A full symmetric CSR. */
+int dgp_smv_mex(double *d_out_real, double *d_out_imag, const double *d_x_real,
+                const double *d_x_imag, const double *d_fAxis,
+                const double *d_valA_real, const double *d_valA_imag,
+                const int *d_rPtr, const int *d_cPtr, int nrows, int ncols,
+                int nfreqs, dgp_stream_t stream);
+
+/* Replaces FSAImv_call, cuda_lib/mex_sources/FSAImvMex.hpp:4-15
+ * (FSAImv_CUDA.cu:58-81): y[:,s,f] = G_f x[:,s,f], G values [nnz x NF]. */
+int dgp_fsaimv_mex(double *d_out_real, double *d_out_imag,
+                   const double *d_x_real, const double *d_x_imag,
+                   const double *d_valG_real, const double *d_valG_imag,
+                   const int *d_rPtr, const int *d_cPtr, int nnz, int nrows,
+                   int ncols, int nfreqs, dgp_stream_t stream);
+
+/* Replaces FSAIP_call, cuda_lib/mex_sources/FSAIP.hpp:4-13
+ * (FSAIP_CUDA.cu:162-180): FSAI factor of tril(A) for harmonics
+ * 0..nfreqs-1, output [NF x nnzG] (harmonic fastest) like the reference. */
+int dgp_fsaip_mex(double *d_out_real, double *d_out_imag,
+                  const double *d_valA_real, const double *d_valA_imag,
+                  const int *d_rPtrA, const int *d_cPtrA, const int *d_rPtrG,
+                  const int *d_cPtrG, int nfreqs, int nrows,
+                  dgp_stream_t stream);
+
+/* ====================================================================== *
+ *  FEM topology and assembly on the device.
+ *  Replaces prepare_mesh + gen_fwdmat + update_properties,
+ *  DOGPUP/dMesh.m:80-88, :945-1030, :1033-1235.
+ * ====================================================================== */
+typedef struct dgp_fem_s *dgp_fem_t;
+
+/* Builds, on the device: element volumes and inverse-Jacobians, the
+ * boundary-node flags (faces owned by one tet), the Robin face set of
+ * dMesh.m:1129-1140, the full symmetric CSR pattern of the FEM matrix and
+ * the element-to-slot gather map.  d_node [nn][3] f64, d_elem [ne][4].
+ * Synchronises the stream (it reads sizes back). */
+int dgp_fem_create(dgp_fem_t *fem, const double *d_node, const int32_t *d_elem,
+                   int64_t nn, int64_t ne, double nr, dgp_stream_t stream);
+int dgp_fem_destroy(dgp_fem_t fem);
+/* nnz of the pattern, number of Robin faces, number of boundary nodes,
+ * and the speed of light in the medium c = cVac/nr (mm/s). */
+int dgp_fem_info(dgp_fem_t fem, int64_t *nnz, int64_t *n_robin_faces,
+                 int64_t *n_boundary, double *c_medium);
+/* Borrowed device pointers to the CSR pattern (valid until destroy). */
+int dgp_fem_pattern(dgp_fem_t fem, const int32_t **d_rowptr,
+                    const int32_t **d_col);
+/* Boundary flags (int32 0/1) of every node. */
+int dgp_fem_boundary(dgp_fem_t fem, int32_t *d_bnd, dgp_stream_t stream);
+/* K (stiffness with kappa = 1/(3(mua+musp)) + absorption + Robin) and M
+ * (mass) values on the pattern, float64, from nodal mua and musp. */
+int dgp_fem_assemble(dgp_fem_t fem, const double *d_mua, const double *d_musp,
+                     double *d_K, double *d_M, dgp_stream_t stream);
+
+/* ====================================================================== *
+ *  Batched solver: FSAI setup + BiCGSTAB over every source x harmonic.
+ *  Replaces fluGPU + gpuBicstab_FSAIP + FSAIP_gen, dMesh.m:1238-1385,
+ *  as one call instead of a MATLAB loop over mex mat-vecs.
+ * ====================================================================== */
+enum { DGP_PREC_FP64 = 0, DGP_PREC_MIXED = 1 };
+enum { DGP_STOP_MAX_ALL = 0, DGP_STOP_PER_COLUMN = 1 };
+
+typedef struct dgp_solve_opts {
+  double tol;          /* relative residual target (reference: 1e-12)      */
+  int32_t maxit;       /* BiCGSTAB iterations (reference: 1000)            */
+  int32_t precision;   /* DGP_PREC_FP64 | DGP_PREC_MIXED                   */
+  double inner_tol;    /* mixed: complex-FP32 inner target per refinement  */
+  int32_t max_refine;  /* mixed: maximum FP64 refinement steps             */
+  int32_t fsai_cap;    /* FSAI pattern cap per row (reference: 30)         */
+  int32_t stop_rule;   /* DGP_STOP_MAX_ALL (reference) | PER_COLUMN        */
+  int32_t check_every; /* iterations per host convergence poll (>= 1)      */
+} dgp_solve_opts;
+
+void dgp_solve_opts_default(dgp_solve_opts *opts);
+
+typedef struct dgp_solve_report {
+  int32_t iterations;       /* BiCGSTAB iterations (summed over refinement) */
+  int32_t refinements;      /* FP64 refinement steps (mixed)                */
+  double max_rel_residual;  /* max over columns of ||b-Ax||/||b|| (FP64)    */
+  int32_t n_not_converged;  /* columns whose status is not CONVERGED        */
+  int32_t *d_status;        /* optional [NF*NS] per-column status (in/out)  */
+} dgp_solve_report;
+
+typedef struct dgp_solver_s *dgp_solver_t;
+
+/* Creates a solver for A_k = K + i*k*dfc*M, k = 0..nf-1, on the CSR pattern
+ * (d_rowptr, d_col) with values d_K, d_M (float64, copied), for up to
+ * ns_max sources per harmonic.  dfc = df/c (rad/s over mm/s).  Builds the
+ * FSAI pattern and factors for all harmonics and allocates the workspace. */
+int dgp_solver_create(dgp_solver_t *solver, const int32_t *d_rowptr,
+                      const int32_t *d_col, int64_t n, int64_t nnz,
+                      const double *d_K, const double *d_M, double dfc,
+                      int32_t nf, int32_t ns_max, const dgp_solve_opts *opts,
+                      dgp_stream_t stream);
+/* New K, M values on the same pattern (e.g. after a property update):
+ * re-copies them and refactors FSAI. */
+int dgp_solver_update(dgp_solver_t solver, const double *d_K, const double *d_M,
+                      dgp_stream_t stream);
+int dgp_solver_destroy(dgp_solver_t solver);
+/* Bytes of device memory the solver holds. */
+int dgp_solver_memory(dgp_solver_t solver, int64_t *bytes);
+
+/* Solves A_k X[k] = B[k] for every harmonic, B and X complex128
+ * [NF][NN][NS] with ns <= ns_max.  Synchronises the stream; returns
+ * DGP_ERR_NOT_CONVERGED if any column missed tol (X is still written). */
+int dgp_solve(dgp_solver_t solver, const double *d_B, double *d_X, int32_t ns,
+              const dgp_solve_opts *opts, dgp_solve_report *report,
+              dgp_stream_t stream);
+
+/* Same solve with the point-source right-hand sides of flu_solve /
+ * adj_flu_solve (dMesh.m:124-129, :191-196) generated on the device:
+ * B[k][node_s[l]][s] = w_s[l] * fpsf[k] for the 4 nodes of each optode's
+ * tet.  d_nodes [ns][4] int32, d_w [ns][4] f64, d_fpsf [nf] complex128. */
+int dgp_solve_sources(dgp_solver_t solver, const int32_t *d_nodes,
+                      const double *d_w, const double *d_fpsf, int32_t ns,
+                      double *d_X, const dgp_solve_opts *opts,
+                      dgp_solve_report *report, dgp_stream_t stream);
+
+/* Times one sweep kernel of the complex-FP32 iteration on the solver's
+ * workspace with CUDA events on `stream` (which: 0 = t = A z SpMM,
+ * 1 = G p SpMM, 2 = x/r/p update, 3 = h/s update) and returns the average
+ * milliseconds per launch and the kernel's algorithmic bytes per launch.
+ * Needs a prior DGP_PREC_MIXED solve; overwrites workspace vectors. */
+int dgp_solver_profile_kernel(dgp_solver_t solver, int32_t which, int32_t reps,
+                              float *ms, double *bytes, dgp_stream_t stream);
+
+/* ====================================================================== *
+ *  Batched sparse operators (the solver's building blocks), layout
+ *  [NF][NN][NS] complex128.
+ * ====================================================================== */
+/* Y[k] = (K + i*omega[k]*M) X[k]; d_KM interleaved (K_ij, M_ij) per slot. */
+int dgp_spmm_A(const int32_t *d_rowptr, const int32_t *d_col,
+               const double *d_KM, const double *d_omega, int64_t n,
+               int32_t nf, int32_t ns, const double *d_X, double *d_Y,
+               dgp_stream_t stream);
+/* FSAI pattern (rule of dMesh.m:1361-1380) of tril(K + i*dfc*M): counts
+ * rows first (d_rowptrG [n+1]), then fills columns with a second call that
+ * passes d_colG (size from d_rowptrG[n]). */
+int dgp_fsai_pattern(const int32_t *d_rowptr, const int32_t *d_col,
+                     const double *d_K, const double *d_M, double dfc,
+                     int64_t n, int32_t cap, int32_t *d_rowptrG,
+                     int32_t *d_colG, dgp_stream_t stream);
+/* FSAI factor values G[k][slot] (complex128) for k = 0..nf-1 of
+ * A_k = K + i*k*dfc*M on the pattern (arithmetic of FSAIP_CUDA.cu:92-160). */
+int dgp_fsai_factor(const int32_t *d_rowptr, const int32_t *d_col,
+                    const double *d_K, const double *d_M, double dfc,
+                    int64_t n, const int32_t *d_rowptrG, const int32_t *d_colG,
+                    int32_t nf, double *d_G, dgp_stream_t stream);
+/* Y[k] = G_k X[k] (transpose = 0) or G_k^T X[k] (transpose = 1). */
+int dgp_fsai_apply(const int32_t *d_rowptrG, const int32_t *d_colG,
+                   const double *d_G, int64_t n, int64_t nnzG, int32_t nf,
+                   int32_t ns, int32_t transpose, const double *d_X,
+                   double *d_Y, dgp_stream_t stream);
+
+/* ====================================================================== *
+ *  Detector data, Jacobian, transforms (dMesh.m:144-171, :206-247;
+ *  td2fc.m, fc2td.m, fc2tg.m).
+ * ====================================================================== */
+/* data[m][k] = sum_l w_d[l] * phi[k][node_d[l]][s] for link m = (s, d).
+ * d_nodes/d_w are the detectors' tet nodes and barycentric weights [nd][4]. */
+int dgp_meas(const int32_t *d_det_nodes, const double *d_det_w, int32_t nd,
+             const int32_t *d_link, int32_t nm, const double *d_phi,
+             int64_t n, int32_t nf, int32_t ns, double *d_data,
+             dgp_stream_t stream);
+
+/* Fourier coefficients of sampled signals: c[r][k] = dt/t_end *
+ * sum_t exp(-i f_k t) x[r][t]  (td2fc.m:26-32).  x [nr][nt] f64. */
+int dgp_td2fc(const double *d_x, int64_t nr, int32_t nt, const double *d_t,
+              const double *d_f, int32_t nf, double *d_c, dgp_stream_t stream);
+/* x[r][t] = 2 Re sum_k exp(i f_k t) c~[r][k], c~_0 = c_0/2 (fc2td.m:60-71). */
+int dgp_fc2td(const double *d_c, int64_t nr, int32_t nf, const double *d_f,
+              const double *d_t, int32_t nt, double *d_x, dgp_stream_t stream);
+/* y[r][g] = nt * 2 Re sum_k conj(gate[g][k]) c~[r][k] (fc2tg.m:100-111). */
+int dgp_fc2tg(const double *d_c, int64_t nr, int32_t nf, const double *d_gate_fc,
+              int32_t ng, int32_t nt, double *d_y, dgp_stream_t stream);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* DOGPUP_B200_H */

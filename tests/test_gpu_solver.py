@@ -1,0 +1,201 @@
+"""GPU parity of assembly, FSAI, SpMM and the batched solver against the oracle.
+
+Tolerances: integer/index data (CSR pattern, boundary flags, FSAI pattern)
+must match exactly; FP64 values to 1e-12 relative (different summation
+order); the FP64 solver to 1e-9 of the oracle's own BiCGSTAB; the
+mixed-precision solver to 1e-6 relative fluence error against a sparse-direct
+complex128 solve (the north-star accuracy bar).
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+pytestmark = pytest.mark.gpu
+
+C_VAC = 2.99792458e11
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+    return torch
+
+
+@pytest.fixture(scope="module")
+def gpu_case(small_case, torch):
+    from dogpup_b200 import api
+    m = small_case["mesh"]
+    fem = api.Fem(torch.as_tensor(m.node), torch.as_tensor(m.elem), 1.4)
+    K, M = fem.assemble(torch.as_tensor(small_case["mua"]), torch.as_tensor(small_case["musp"]))
+    return dict(fem=fem, K=K, M=M)
+
+
+def rel(a, b):
+    return np.linalg.norm(np.ravel(a - b)) / max(np.linalg.norm(np.ravel(b)), 1e-300)
+
+
+def test_fem_pattern_and_values(small_case, gpu_case):
+    from oracle.fem import robin_faces
+    K0, M0 = small_case["K"], small_case["M"]
+    fem = gpu_case["fem"]
+    assert np.array_equal(fem.rowptr.cpu().numpy(), K0.indptr)
+    assert np.array_equal(fem.col.cpu().numpy(), K0.indices)
+    assert np.array_equal(fem.bnd.cpu().numpy().astype(bool), small_case["mesh"].bnd)
+    assert fem.n_robin_faces == robin_faces(small_case["mesh"].elem, small_case["geo"]["bnd"]).shape[0]
+    K, M = gpu_case["K"].cpu().numpy(), gpu_case["M"].cpu().numpy()
+    assert np.abs(K - K0.data).max() <= 1e-13 * np.abs(K0.data).max()
+    assert np.abs(M - M0.data).max() <= 1e-13 * np.abs(M0.data).max()
+    # bitwise-symmetric assembly
+    Kg = sp.csr_matrix((K, K0.indices, K0.indptr), shape=K0.shape)
+    assert abs(Kg - Kg.T).max() == 0.0
+
+
+def test_fem_rejects_degenerate_tet(torch):
+    from dogpup_b200 import api, DgpError
+    node = torch.tensor([[0., 0, 0], [1, 0, 0], [0, 1, 0], [1, 1, 0]], dtype=torch.float64)
+    elem = torch.tensor([[0, 1, 2, 3]], dtype=torch.int32)
+    with pytest.raises(DgpError):
+        api.Fem(node, elem, 1.4)
+
+
+def test_fsai_pattern_and_factor(small_case, gpu_case, torch):
+    from dogpup_b200 import api
+    from dogpup_b200._lib import lib, check
+    from oracle import solver as osv
+    K0, M0 = small_case["K"], small_case["M"]
+    dfc = 2 * np.pi / 10e-9 / (C_VAC / 1.4)
+    nf = 5
+    fem = gpu_case["fem"]
+    n = fem.nn
+    rpg = torch.empty(n + 1, dtype=torch.int32, device="cuda")
+    check(lib.dgp_fsai_pattern(api.ptr(fem.rowptr), api.ptr(fem.col), api.ptr(gpu_case["K"]), api.ptr(gpu_case["M"]),
+                               dfc, n, 30, api.ptr(rpg), None, api.stream_ptr()))
+    nnzG = int(rpg[-1].item())
+    colg = torch.empty(nnzG, dtype=torch.int32, device="cuda")
+    check(lib.dgp_fsai_pattern(api.ptr(fem.rowptr), api.ptr(fem.col), api.ptr(gpu_case["K"]), api.ptr(gpu_case["M"]),
+                               dfc, n, 30, api.ptr(rpg), api.ptr(colg), api.stream_ptr()))
+    A = sp.tril(K0 + 1j * dfc * M0).tocsr()
+    r0, c0 = osv.fsai_pattern(A)
+    assert np.array_equal(rpg.cpu().numpy(), r0) and np.array_equal(colg.cpu().numpy(), c0)
+    G = torch.empty((nf, nnzG), dtype=torch.complex128, device="cuda")
+    check(lib.dgp_fsai_factor(api.ptr(fem.rowptr), api.ptr(fem.col), api.ptr(gpu_case["K"]), api.ptr(gpu_case["M"]),
+                              dfc, n, api.ptr(rpg), api.ptr(colg), nf, api.ptr(torch.view_as_real(G)),
+                              api.stream_ptr()))
+    G0 = osv.fsai_factor(sp.tril(K0).tocsr(), sp.tril(dfc * M0).tocsr(), r0, c0, nf)
+    assert rel(G.cpu().numpy().T, G0) < 1e-12
+
+
+def test_spmm_A_matches_smv(small_case, gpu_case, torch):
+    from dogpup_b200 import api
+    from dogpup_b200._lib import lib, check
+    from oracle import solver as osv
+    K0, M0 = small_case["K"], small_case["M"]
+    dfc = 1e-3
+    nf, ns = 4, 8
+    n = K0.shape[0]
+    rng = np.random.default_rng(5)
+    X = rng.standard_normal((nf, n, ns)) + 1j * rng.standard_normal((nf, n, ns))
+    KM = torch.stack([gpu_case["K"], gpu_case["M"]], dim=1).contiguous()
+    om = torch.arange(nf, dtype=torch.float64, device="cuda") * dfc
+    Xd = torch.as_tensor(X, device="cuda")
+    Y = torch.empty_like(Xd)
+    check(lib.dgp_spmm_A(api.ptr(gpu_case["fem"].rowptr), api.ptr(gpu_case["fem"].col), api.ptr(KM), api.ptr(om), n,
+                         nf, ns, api.ptr(torch.view_as_real(Xd)), api.ptr(torch.view_as_real(Y)), api.stream_ptr()))
+    Y0 = osv.smv(np.transpose(X, (1, 2, 0)), np.arange(nf, dtype=float), K0, dfc * M0)
+    assert rel(np.transpose(Y.cpu().numpy(), (1, 2, 0)), Y0) < 1e-13
+
+
+def _point_sources(small_case, ns, seed):
+    m = small_case["mesh"]
+    rng = np.random.default_rng(seed)
+    eid = rng.choice(m.ne, ns, replace=False)
+    w = rng.random((ns, 4))
+    w /= w.sum(axis=1, keepdims=True)
+    return m.elem[eid].astype(np.int32), w
+
+
+@pytest.mark.parametrize("ns", [3, 16])
+def test_solver_fp64_matches_oracle_bicgstab(small_case, gpu_case, torch, ns):
+    from dogpup_b200 import api
+    from oracle import solver as osv
+    K0, M0 = small_case["K"], small_case["M"]
+    nf = 6
+    dfc = 2 * np.pi / 10e-9 / (C_VAC / 1.4)
+    nodes, w = _point_sources(small_case, ns, 7)
+    fpsf = np.exp(-0.2j * np.arange(nf)) * (1.0 + 0.1 * np.arange(nf))
+    fem = gpu_case["fem"]
+    S = api.Solver(fem.rowptr, fem.col, gpu_case["K"], gpu_case["M"], dfc, nf, ns)
+    opts = api.make_opts(tol=1e-12, maxit=1000, precision="fp64", check_every=1)
+    X, rep = S.solve_sources(torch.as_tensor(nodes, device="cuda"), torch.as_tensor(w, device="cuda"),
+                             torch.as_tensor(fpsf, device="cuda"), opts)
+    Q = np.zeros((K0.shape[0], ns, nf), complex)
+    for s in range(ns):
+        Q[nodes[s], s, :] = w[s][:, None] * fpsf[None, :]
+    pc = osv.FsaiPrecond(K0, M0, dfc, nf)
+    x0, it0 = osv.bicgstab_fsai(pc, Q, 1e-12, 1000)
+    Xh = np.transpose(X.cpu().numpy(), (1, 2, 0))
+    assert abs(rep.iterations - it0) <= 1
+    assert rel(Xh, x0) < 1e-9
+    xd = osv.direct_solve(K0, M0, dfc, Q)
+    assert rel(Xh, xd) < 1e-9
+    assert rep.max_rel_residual < 1e-10
+
+
+def test_solver_dense_rhs_and_status(small_case, gpu_case, torch):
+    from dogpup_b200 import api
+    from oracle import solver as osv
+    K0, M0 = small_case["K"], small_case["M"]
+    nf, ns = 3, 4
+    dfc = 2 * np.pi / 10e-9 / (C_VAC / 1.4)
+    n = K0.shape[0]
+    rng = np.random.default_rng(9)
+    B = rng.standard_normal((nf, n, ns)) + 1j * rng.standard_normal((nf, n, ns))
+    B[:, :, 2] = 0  # a zero right-hand side column is solved exactly by x = 0
+    fem = gpu_case["fem"]
+    S = api.Solver(fem.rowptr, fem.col, gpu_case["K"], gpu_case["M"], dfc, nf, ns)
+    status = torch.full((nf * ns,), -1, dtype=torch.int32, device="cuda")
+    X, rep = S.solve(torch.as_tensor(B, device="cuda"), api.make_opts(tol=1e-11, precision="fp64"), status=status)
+    xd = osv.direct_solve(K0, M0, dfc, np.transpose(B, (1, 2, 0)))
+    assert rel(np.transpose(X.cpu().numpy(), (1, 2, 0)), xd) < 1e-8
+    assert (status.cpu().numpy() == 0).all()
+    assert np.abs(X[:, :, 2].cpu().numpy()).max() == 0.0
+
+
+def test_solver_mixed_precision_accuracy(small_case, gpu_case, torch):
+    from dogpup_b200 import api
+    from oracle import solver as osv
+    K0, M0 = small_case["K"], small_case["M"]
+    nf, ns = 8, 16
+    dfc = 2 * np.pi / 10e-9 / (C_VAC / 1.4)
+    nodes, w = _point_sources(small_case, ns, 13)
+    fpsf = np.exp(-0.3j * np.arange(nf))
+    fem = gpu_case["fem"]
+    S = api.Solver(fem.rowptr, fem.col, gpu_case["K"], gpu_case["M"], dfc, nf, ns)
+    opts = api.make_opts(tol=1e-10, precision="mixed", inner_tol=1e-4)
+    X, rep = S.solve_sources(torch.as_tensor(nodes, device="cuda"), torch.as_tensor(w, device="cuda"),
+                             torch.as_tensor(fpsf, device="cuda"), opts)
+    Q = np.zeros((K0.shape[0], ns, nf), complex)
+    for s in range(ns):
+        Q[nodes[s], s, :] = w[s][:, None] * fpsf[None, :]
+    xd = osv.direct_solve(K0, M0, dfc, Q)
+    Xh = np.transpose(X.cpu().numpy(), (1, 2, 0))
+    # per right-hand side relative error
+    err = np.linalg.norm(Xh - xd, axis=0) / np.linalg.norm(xd, axis=0)
+    assert err.max() < 1e-6, err.max()
+    assert rep.max_rel_residual < 1e-10
+    assert rep.refinements >= 2
+
+
+def test_solver_reports_maxit(small_case, gpu_case, torch):
+    from dogpup_b200 import api
+    nf, ns = 2, 2
+    fem = gpu_case["fem"]
+    S = api.Solver(fem.rowptr, fem.col, gpu_case["K"], gpu_case["M"], 1e-4, nf, ns)
+    nodes, w = _point_sources(small_case, ns, 1)
+    status = torch.full((nf * ns,), -1, dtype=torch.int32, device="cuda")
+    X, rep = S.solve_sources(torch.as_tensor(nodes, device="cuda"), torch.as_tensor(w, device="cuda"),
+                             torch.ones(nf, dtype=torch.complex128, device="cuda"),
+                             api.make_opts(tol=1e-14, maxit=2, precision="fp64", check_every=1), status=status)
+    assert rep.iterations == 2
+    assert (status.cpu().numpy() == 1).all()
+    assert np.isfinite(X.cpu().numpy()).all()

@@ -1,0 +1,122 @@
+"""CPU tests of the oracle itself: identities the reference formulation must satisfy."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from dogpup_b200.meshgen import box_mesh, cylinder_mesh, ellipsoid_mesh
+from oracle import fem, solver, transforms, jacobian
+
+
+def test_mesh_generators_are_conforming():
+    for m in (cylinder_mesh(6, 8, 1.5, 0.2, 1), ellipsoid_mesh((12, 10, 8), 1.0, 0.1, 2), box_mesh((4, 3, 5), 1.0)):
+        geo = fem.prepare_mesh(m.node, m.elem, 1.4)
+        assert (geo["vol"] > 0).all()
+        assert np.array_equal(geo["bnd"].astype(bool), m.bnd)
+        # every interior face is shared by exactly two tets: surface = faces seen once
+        assert geo["face"].shape[0] > 0
+
+
+def test_mass_matrix_identities(small_case):
+    K, M, geo = small_case["K"], small_case["M"], small_case["geo"]
+    assert abs(M.sum() - geo["vol"].sum()) < 1e-9 * geo["vol"].sum()
+    assert abs(M - M.T).max() < 1e-15 * abs(M).max()
+    assert abs(K - K.T).max() < 1e-15 * abs(K).max()
+    # P1 consistent mass of one tet: vol/20 (1 + delta_ij)
+    m = small_case["mesh"]
+    Ke, Me = fem.element_matrices(m.node, m.elem[:1], {"vol": geo["vol"][:1], "gradScale": geo["gradScale"][:1]},
+                                  np.zeros(m.nn), np.zeros(m.nn))
+    assert np.allclose(Me[0], geo["vol"][0] / 20 * (np.ones((4, 4)) + np.eye(4)), rtol=1e-14)
+
+
+def test_stiffness_rows_vanish_without_absorption_or_boundary():
+    m = box_mesh((3, 3, 3), 1.0, 0.2, 4)
+    geo = fem.prepare_mesh(m.node, m.elem, 1.4)
+    geo = dict(geo, bnd=np.zeros_like(geo["bnd"]), R=np.zeros(m.nn))
+    K, M = fem.gen_fwdmat(m.node, m.elem, geo, 0.0, 1.0)
+    assert np.abs(np.asarray(K.sum(axis=1))).max() < 1e-13
+
+
+def test_absorption_term_equals_mua_times_mass():
+    m = box_mesh((3, 3, 3), 1.0, 0.2, 5)
+    geo = fem.prepare_mesh(m.node, m.elem, 1.4)
+    geo0 = dict(geo, bnd=np.zeros_like(geo["bnd"]), R=np.zeros(m.nn))
+    K1, M = fem.gen_fwdmat(m.node, m.elem, geo0, 0.02, 1.0)
+    # kappa depends on mua: compare with the stiffness at the same kappa but mua = 0
+    kap = 1.0 / (3.0 * (0.02 + 1.0))
+    K0, _ = fem.gen_fwdmat(m.node, m.elem, geo0, 0.0, 1.0 / (3 * kap))
+    assert abs((K1 - K0) - 0.02 * M).max() < 1e-14
+
+
+def test_robin_face_rule_counts():
+    m = cylinder_mesh(4, 4, 1.0, 0.0, 0)
+    geo = fem.prepare_mesh(m.node, m.elem, 1.4)
+    f = fem.robin_faces(m.elem, geo["bnd"])
+    # includes every true surface face (as node sets)
+    surf = {tuple(sorted(x)) for x in geo["face"]}
+    rob = {tuple(x) for x in f}
+    assert surf <= rob
+
+
+def test_fsai_pattern_rule_rowwise_equals_global_sort(small_case):
+    K, M = small_case["K"], small_case["M"]
+    A = sp.tril(K + 1j * 3e-3 * M).tocsr()
+    for cap in (30, 5, 3):
+        r1, c1 = solver.fsai_pattern(A, cap)
+        r2, c2 = solver.fsai_pattern_rowwise(A, cap)
+        assert np.array_equal(r1, r2) and np.array_equal(c1, c2)
+
+
+def test_fsai_identity(small_case):
+    K, M = small_case["K"], small_case["M"]
+    dfc = 2 * np.pi / 10e-9 / (2.99792458e11 / 1.4)
+    pc = solver.FsaiPrecond(K, M, dfc, 6)
+    n = K.shape[0]
+    for k in range(6):
+        Gk = sp.csr_matrix((pc.G[:, k], pc.colsG, pc.rptrG), shape=(n, n))
+        d = (Gk @ (K + 1j * k * dfc * M) @ Gk.T).diagonal()
+        assert np.abs(d - 1).max() < 1e-12
+
+
+def test_bicgstab_matches_direct(small_case):
+    K, M = small_case["K"], small_case["M"]
+    dfc = 2 * np.pi / 10e-9 / (2.99792458e11 / 1.4)
+    pc = solver.FsaiPrecond(K, M, dfc, 4)
+    rng = np.random.default_rng(0)
+    Q = np.zeros((K.shape[0], 3, 4), complex)
+    for s in range(3):
+        idx = rng.choice(K.shape[0], 4, replace=False)
+        Q[idx, s, :] = rng.random(4)[:, None] * np.exp(0.3j * np.arange(4))[None]
+    x, it = solver.bicgstab_fsai(pc, Q, 1e-12, 1000)
+    xd = solver.direct_solve(K, M, dfc, Q)
+    assert np.linalg.norm(x - xd) / np.linalg.norm(xd) < 1e-9
+    assert 5 < it < 200
+
+
+def test_transform_round_trip_and_gates():
+    t = np.arange(0, 141) * 50e-12
+    T = t[-1]
+    nf = 40
+    f = np.arange(nf) * 2 * np.pi / T
+    x = transforms.gaussian_tpsf(t, 250e-12)
+    c = transforms.td2fc(x, f, t)
+    xr = transforms.fc2td(c, f, t)
+    assert np.abs(xr - x).max() < 2e-3 * x.max()
+    # fc2tg with gate coefficients = Nt * sum over the gate of x * gate / Nt (discrete Parseval)
+    gates = np.stack([transforms.gaussian_tpsf(t - 1e-9 * g, 400e-12) for g in range(3)])
+    gfc = transforms.td2fc(gates, f, t)
+    y = transforms.fc2tg(c, gfc, f, t.size)
+    direct = np.array([(gates[g] * x).sum() * (t[1] - t[0]) / T * 1.0 for g in range(3)])
+    assert np.allclose(y * (t[1] - t[0]) / T / t.size * T / (t[1] - t[0]), direct, rtol=5e-3, atol=1e-6 * direct.max())
+
+
+def test_tik_inv_matches_normal_equations():
+    rng = np.random.default_rng(1)
+    J = rng.standard_normal((40, 12))
+    y = rng.standard_normal(40)
+    u = jacobian.tik_inv(J, 0.1, y)
+    H = J.T @ J + 0.1 * np.max((J ** 2).sum(0)) * np.eye(12)
+    assert np.allclose(u, np.linalg.solve(H, J.T @ y), rtol=1e-12)
+    w = rng.random(40) + 0.5
+    uw = jacobian.tik_inv(J, 0.1, y, weights=w)
+    Hw = J.T @ (w[:, None] * J) + 0.1 * np.max((w[:, None] * J ** 2).sum(0)) * np.eye(12)
+    assert np.allclose(uw, np.linalg.solve(Hw, J.T @ (w * y)), rtol=1e-12)
