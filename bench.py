@@ -50,6 +50,10 @@ def parse():
     return ap.parse_args()
 
 
+def log(msg):
+    print(msg, file=sys.stderr, flush=True)
+
+
 def workload(name, seed=1):
     from dogpup_b200 import workloads
     return {"ellipsoid": workloads.ellipsoid_fwd, "cylinder": workloads.cylinder_fwd,
@@ -158,8 +162,12 @@ def run_ours(a, rank, world, local_rank):
         phi, data, rep = mesh.flu_solve(precision="mixed", tol=a.tol, inner_tol=a.inner_tol, return_report=True)
         return rep
 
-    for _ in range(a.warmup):
+    log(f"[rank {rank}] setup done: {mesh.nn} nodes, nnz {mesh.fem.nnz}, solver {solver.memory() / 1e9:.1f} GB")
+    for q in range(a.warmup):
+        t0 = time.perf_counter()
         rep = step()
+        log(f"[rank {rank}] warmup {q}: {time.perf_counter() - t0:.2f}s, {rep.iterations} it, "
+            f"{rep.refinements} ref, res {rep.max_rel_residual:.2e}, mem {solver.memory() / 1e9:.1f} GB")
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -225,7 +233,7 @@ def run_ours(a, rank, world, local_rank):
             "frac": round(ach / peak, 4), "traffic": None, "peak_source": "measured" if pk else "fallback",
             "per_kernel_ms": {names[q]: round(prof[q][0], 3) for q in prof},
             "per_kernel_gbs": {names[q]: round(prof[q][1] / (prof[q][0] * 1e-3) / 1e9, 1) for q in prof}}
-    res.update(ms_step=ms_step, value=value, e2e=e2e, rep=rep, clocks=clocks, roof=roof, mesh=mesh, w=w)
+    res.update(ms_per_step=ms_step, value=value, e2e=e2e, rep=rep, clocks=clocks, roof=roof, mesh=mesh, w=w)
     return res
 
 

@@ -303,8 +303,13 @@ __global__ void k_face_blocks(const double *__restrict__ node, const int32_t *__
 
 // one thread per CSR slot: K = (sum of element entries) + (sum of Robin
 // entries), M = sum of element entries, each in ascending element order.
+// A slot (r, c) below the diagonal takes the transposed local entry of each
+// contribution, i.e. exactly the value of slot (c, r): the reference keeps
+// triu(K), triu(M) and mirrors them (dMesh.m:1189-1190, :1242), so A is
+// bitwise symmetric there as well.
 __global__ void k_gather_slots(const int32_t *__restrict__ cstart, const int32_t *__restrict__ payload,
-                               int32_t nnz, int64_t nk, int64_t ne16, const double *__restrict__ Ke,
+                               int32_t nnz, int64_t nk, int64_t ne16, const int32_t *__restrict__ elem,
+                               const int32_t *__restrict__ faces, const double *__restrict__ Ke,
                                const double *__restrict__ Me, const double *__restrict__ Be, double *K,
                                double *M) {
   int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -315,10 +320,17 @@ __global__ void k_gather_slots(const int32_t *__restrict__ cstart, const int32_t
   for (int64_t p = b; p < e; ++p) {
     int64_t t = payload[p];
     if (t < ne16) {
+      int64_t el = t >> 4;
+      int a = (t >> 2) & 3, c = t & 3;
+      if (elem[4 * el + a] > elem[4 * el + c]) t = (el << 4) | (c << 2) | a;
       kv += Ke[t];
       mv += Me[t];
     } else {
-      kb += Be[t - ne16];
+      int64_t q = t - ne16;
+      int64_t f = q / 9;
+      int a = (int)(q % 9) / 3, c = (int)(q % 9) % 3;
+      if (faces[3 * f + a] > faces[3 * f + c]) q = 9 * f + 3 * c + a;
+      kb += Be[q];
     }
   }
   K[u] = kv + kb;
@@ -517,7 +529,8 @@ int fem_assemble(FemPlan *F, const double *d_mua, const double *d_musp, double *
     DGP_CHECK_LAUNCH();
   }
   k_gather_slots<<<grid1(F->nnz, 256), 256, 0, st>>>(F->cstart.as<int32_t>(), F->payload.as<int32_t>(), F->nnz,
-                                                    F->nk, 16 * F->ne, F->Ke.as<double>(), F->Me.as<double>(),
+                                                    F->nk, 16 * F->ne, F->elem.as<int32_t>(),
+                                                    F->faces.as<int32_t>(), F->Ke.as<double>(), F->Me.as<double>(),
                                                     F->Be.as<double>(), d_K, d_M);
   DGP_CHECK_LAUNCH();
   return DGP_OK;
