@@ -40,6 +40,7 @@ _SIGS = {
     "dgp_smv_mex": (C.c_int, [P, P, P, P, P, P, P, P, P, C.c_int, C.c_int, C.c_int, P]),
     "dgp_fsaimv_mex": (C.c_int, [P, P, P, P, P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, P]),
     "dgp_fsaip_mex": (C.c_int, [P, P, P, P, P, P, P, P, C.c_int, C.c_int, P]),
+    "dgp_fsaip_mex_noalloc": (C.c_int, [P, P, P, P, P, P, P, P, C.c_int, C.c_int, P]),
     "dgp_fem_create": (C.c_int, [C.POINTER(P), P, P, I64, I64, D, P]),
     "dgp_fem_destroy": (C.c_int, [P]),
     "dgp_fem_info": (C.c_int, [P, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64), C.POINTER(D)]),

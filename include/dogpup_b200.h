@@ -88,6 +88,22 @@ int dgp_fsaip_mex(double *d_out_real, double *d_out_imag,
                   const int *d_cPtrG, int nfreqs, int nrows,
                   dgp_stream_t stream);
 
+/* No counterpart in the reference.  dgp_fsaip_mex for callers that must not
+ * allocate device memory -- a MATLAB mex gateway whose device memory has to
+ * come from MATLAB's gpuArray pool, or an application whose own pooling
+ * allocator owns the GPU.  Same arguments and output; it allocates nothing
+ * and stages its work in one fixed 16 MiB device array that every GPU loading
+ * the library keeps until exit.  Limit: nfreqs * (longest pattern row)
+ * <= 1048576, else DGP_ERR_ARG.  All calls share that array: calls that
+ * overlap on the GPU race, so serialise them.  The first call on a device
+ * looks the array up; make it before any stream capture.  Synchronises the
+ * stream. */
+int dgp_fsaip_mex_noalloc(double *d_out_real, double *d_out_imag,
+                          const double *d_valA_real, const double *d_valA_imag,
+                          const int *d_rPtrA, const int *d_cPtrA,
+                          const int *d_rPtrG, const int *d_cPtrG, int nfreqs,
+                          int nrows, dgp_stream_t stream);
+
 /* ====================================================================== *
  *  FEM topology and assembly on the device.
  *  Replaces prepare_mesh + gen_fwdmat + update_properties,
