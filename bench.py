@@ -42,7 +42,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="ellipsoid", choices=["ellipsoid", "cylinder", "small"])
+    ap.add_argument("--workload", default="ellipsoid", choices=["ellipsoid", "medium", "cylinder", "small"])
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--inner-tol", type=float, default=1e-4)
     ap.add_argument("--no-e2e", action="store_true")
@@ -56,6 +56,8 @@ def log(msg):
 
 def workload(name, seed=1):
     from dogpup_b200 import workloads
+    if name == "medium":  # same shape family at a coarser lattice: 19k nodes, 64 x 32 RHS (profiling case)
+        return workloads.ellipsoid_fwd(seed=seed, h=2.4, nf=32)
     return {"ellipsoid": workloads.ellipsoid_fwd, "cylinder": workloads.cylinder_fwd,
             "small": workloads.small_fwd}[name](seed=seed)
 
