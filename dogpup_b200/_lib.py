@@ -63,6 +63,12 @@ _SIGS = {
     "dgp_td2fc": (C.c_int, [P, I64, I32, P, P, I32, P, P]),
     "dgp_fc2td": (C.c_int, [P, I64, I32, P, P, I32, P, P]),
     "dgp_fc2tg": (C.c_int, [P, I64, I32, P, I32, I32, P, P]),
+    "dgp_normal_eq": (C.c_int, [P, I64, I64, P, P, D, I32, P, I64, P, P]),
+    "dgp_cholesky_solve": (C.c_int, [P, I64, I64, P, P]),
+    "dgp_jacobian_complex":(C.c_int, [P, P, P, I64, P, P, I32, P, I32, I64, I32, P, P, I32, P, P]),
+    "dgp_jacobian_tg": (C.c_int, [P, P, P, I64, P, P, I32, P, I32, I64, I32, P, P, I32, P, I32, I32, P, P, P]),
+    "dgp_jacobian_tg_vjp": (C.c_int, [P, P, P, I64, P, P, I32, P, I32, I64, I32, P, P, I32, P, I32, I32, P, P, P,
+                                      P]),
 }
 
 # every extern "C" symbol include/dogpup_b200.h declares

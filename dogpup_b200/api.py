@@ -188,6 +188,67 @@ def fc2tg(c: torch.Tensor, gate_fc: torch.Tensor, nt: int) -> torch.Tensor:
     return out.reshape(*c.shape[:-1], g.shape[0])
 
 
+class Basis:
+    """Jacobian basis: P = m2g as device CSR (voxel grid) or None (nodal), plus weights w [nv]."""
+
+    def __init__(self, P=None, w=None, nn=None):
+        if P is not None:
+            P = P.tocsr()
+            P.sort_indices()
+            self.rowptr = torch.as_tensor(P.indptr.astype("int32"), device="cuda")
+            self.col = torch.as_tensor(P.indices.astype("int32"), device="cuda")
+            self.val = torch.as_tensor(P.data.astype("float64"), device="cuda")
+            self.nv = P.shape[0]
+        else:
+            self.rowptr = self.col = self.val = None
+            self.nv = int(nn)
+        self.w = None if w is None else torch.as_tensor(w, dtype=torch.float64, device="cuda").contiguous()
+
+    def args(self):
+        p = lambda t: None if t is None else ptr(t)
+        return [p(self.rowptr), p(self.col), p(self.val), self.nv, p(self.w)]
+
+
+def _jac_common(basis, phi, phiA, fpsf, link):
+    nf, nn, ns = phi.shape
+    nd = phiA.shape[2]
+    link = link.to(device="cuda", dtype=torch.int32).contiguous()
+    fpsf = fpsf.to(device="cuda", dtype=torch.complex128).contiguous()
+    return [*basis.args(), ptr(as_real(phi)), ns, ptr(as_real(phiA)), nd, nn, nf, ptr(as_real(fpsf)), ptr(link),
+            int(link.shape[0])], (link, fpsf)
+
+
+def jacobian_complex(basis, phi, phiA, fpsf, link) -> torch.Tensor:
+    """J[v][k][m] (J_complex, dMesh.m:206-247), complex128."""
+    args, keep = _jac_common(basis, phi, phiA, fpsf, link)
+    out = torch.empty((basis.nv, phi.shape[0], int(link.shape[0])), dtype=torch.complex128, device="cuda")
+    check(lib.dgp_jacobian_complex(*args, ptr(as_real(out)), stream_ptr()))
+    return out
+
+
+def jacobian_tg(basis, phi, phiA, fpsf, link, gate_fc, nt, data_tg=None) -> torch.Tensor:
+    """Time-gated Jacobian J_tg[v][g][m] float32 (optionally Rytov-normalised by data_tg [nm][ng])."""
+    args, keep = _jac_common(basis, phi, phiA, fpsf, link)
+    g = gate_fc.to(device="cuda", dtype=torch.complex128).contiguous()
+    rt = None if data_tg is None else data_tg.to(device="cuda", dtype=torch.float64).contiguous()
+    out = torch.empty((basis.nv, g.shape[0], int(link.shape[0])), dtype=torch.float32, device="cuda")
+    check(lib.dgp_jacobian_tg(*args, ptr(as_real(g)), g.shape[0], int(nt), None if rt is None else ptr(rt), ptr(out),
+                              stream_ptr()))
+    return out
+
+
+def jacobian_tg_vjp(basis, phi, phiA, fpsf, link, gate_fc, nt, gin, data_tg=None) -> torch.Tensor:
+    """J_tg^T g [nv] for an upstream gradient g [nm][ng], without forming J."""
+    args, keep = _jac_common(basis, phi, phiA, fpsf, link)
+    g = gate_fc.to(device="cuda", dtype=torch.complex128).contiguous()
+    rt = None if data_tg is None else data_tg.to(device="cuda", dtype=torch.float64).contiguous()
+    gin = gin.to(device="cuda", dtype=torch.float64).contiguous()
+    out = torch.empty(basis.nv, dtype=torch.float64, device="cuda")
+    check(lib.dgp_jacobian_tg_vjp(*args, ptr(as_real(g)), g.shape[0], int(nt), None if rt is None else ptr(rt),
+                                  ptr(gin), ptr(out), stream_ptr()))
+    return out
+
+
 def meas(det_nodes, det_w, link, phi) -> torch.Tensor:
     """Detector data [NM][NF] from phi [NF][NN][NS] (meas_flu, dMesh.m:144-171)."""
     nf, n, ns = phi.shape

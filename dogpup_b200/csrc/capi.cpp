@@ -74,6 +74,13 @@ int meas_run(const int32_t *dn, const double *dw, int nd, const int32_t *link, i
              int nf, int ns, double *data, cudaStream_t st);
 int mex_fsaip(double *out_re, double *out_im, const double *A_re, const double *A_im, const int *rPtrA,
               const int *cPtrA, const int *rPtrG, const int *cPtrG, int nfreqs, int nrows, cudaStream_t st);
+int jacobian_run(int mode, const int32_t *prow, const int32_t *pcol, const double *pval, int64_t nv, const double *w,
+                 const double *phi, int ns, const double *phiA, int nd, int64_t nn, int nf, const double *fpsf,
+                 const int32_t *link, int nm, const double *gate, int ng, int nt, const double *rytov, void *out,
+                 const double *gin, cudaStream_t st);
+int normal_eq_run(const float *Jt, int64_t nv, int64_t nm, const double *W, const double *y, double lam, int mode,
+                  double *H, int64_t ldh, double *rhs, cudaStream_t st);
+int cholesky_solve_run(double *H, int64_t n, int64_t ldh, double *x, cudaStream_t st);
 
 }  // namespace dgp
 
@@ -318,6 +325,42 @@ int dgp_fc2td(const double *d_c, int64_t nr, int32_t nf, const double *d_f, cons
 int dgp_fc2tg(const double *d_c, int64_t nr, int32_t nf, const double *d_gate_fc, int32_t ng, int32_t nt,
               double *d_y, dgp_stream_t stream) {
   DGP_GUARD(fc2tg_run(d_c, nr, nf, d_gate_fc, ng, nt, d_y, (cudaStream_t)stream));
+}
+
+// --------------------------------------------------------------- Jacobian
+int dgp_jacobian_complex(const int32_t *d_P_rowptr, const int32_t *d_P_col, const double *d_P_val, int64_t nv,
+                         const double *d_w, const double *d_phi, int32_t ns, const double *d_phiA, int32_t nd,
+                         int64_t nn, int32_t nf, const double *d_fpsf, const int32_t *d_link, int32_t nm, double *d_J,
+                         dgp_stream_t stream) {
+  DGP_GUARD(jacobian_run(1, d_P_rowptr, d_P_col, d_P_val, nv, d_w, d_phi, ns, d_phiA, nd, nn, nf, d_fpsf, d_link, nm,
+                         nullptr, 0, 0, nullptr, d_J, nullptr, (cudaStream_t)stream));
+}
+
+int dgp_jacobian_tg(const int32_t *d_P_rowptr, const int32_t *d_P_col, const double *d_P_val, int64_t nv,
+                    const double *d_w, const double *d_phi, int32_t ns, const double *d_phiA, int32_t nd, int64_t nn,
+                    int32_t nf, const double *d_fpsf, const int32_t *d_link, int32_t nm, const double *d_gate_fc,
+                    int32_t ng, int32_t nt, const double *d_data_tg, float *d_J, dgp_stream_t stream) {
+  DGP_GUARD(jacobian_run(0, d_P_rowptr, d_P_col, d_P_val, nv, d_w, d_phi, ns, d_phiA, nd, nn, nf, d_fpsf, d_link, nm,
+                         d_gate_fc, ng, nt, d_data_tg, d_J, nullptr, (cudaStream_t)stream));
+}
+
+int dgp_jacobian_tg_vjp(const int32_t *d_P_rowptr, const int32_t *d_P_col, const double *d_P_val, int64_t nv,
+                        const double *d_w, const double *d_phi, int32_t ns, const double *d_phiA, int32_t nd,
+                        int64_t nn, int32_t nf, const double *d_fpsf, const int32_t *d_link, int32_t nm,
+                        const double *d_gate_fc, int32_t ng, int32_t nt, const double *d_data_tg, const double *d_g,
+                        double *d_out, dgp_stream_t stream) {
+  DGP_GUARD(jacobian_run(2, d_P_rowptr, d_P_col, d_P_val, nv, d_w, d_phi, ns, d_phiA, nd, nn, nf, d_fpsf, d_link, nm,
+                         d_gate_fc, ng, nt, d_data_tg, d_out, d_g, (cudaStream_t)stream));
+}
+
+// -------------------------------------------------------- normal equations
+int dgp_normal_eq(const float *d_Jt, int64_t nv, int64_t nmeas, const double *d_w, const double *d_y, double lambda,
+                  int32_t damping, double *d_H, int64_t ldh, double *d_rhs, dgp_stream_t stream) {
+  DGP_GUARD(normal_eq_run(d_Jt, nv, nmeas, d_w, d_y, lambda, damping, d_H, ldh, d_rhs, (cudaStream_t)stream));
+}
+
+int dgp_cholesky_solve(double *d_H, int64_t n, int64_t ldh, double *d_x, dgp_stream_t stream) {
+  DGP_GUARD(cholesky_solve_run(d_H, n, ldh, d_x, (cudaStream_t)stream));
 }
 
 }  // extern "C"

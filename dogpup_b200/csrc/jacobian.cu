@@ -1,0 +1,239 @@
+// Adjoint absorption Jacobian, its time-gated form and vector-Jacobian product.
+//
+//   J_complex  DOGPUP/dMesh.m:206-247
+//     J[m,k,v] = -(P phi_s)[v,k] (P phiA_d)[v,k] w_v / s_fpsf[k],  m <-> (s,d) by link
+//   fc2tg on J (tutorials/tut_2_fluence_and_sensitivity.m:147, wghtd_LM_recon.m:61)
+//     J_tg[m,g,v] = Nt 2 Re sum_k conj(gate_fc[g,k]) c~_k,  c~_0 = J_0 / 2
+//   optional Rytov normalisation J_tg[m,g,v] / data_tg[m,g] (wghtd_LM_recon.m:61)
+//
+// Everything per voxel is folded into one complex table
+//   C[g,k] = -2 Nt h_k conj(gate_fc[g,k]) / s_fpsf[k]     (h_0 = 1/2, else 1)
+// so that J_tg[m,g,v] = w_v * sum_k Re(C[g,k] a_k),  a_k = (P phi_s)_k (P phiA_d)_k.
+//
+// P is the mesh-to-voxel interpolation (mesh.m2g, <= 8 entries per row) or the
+// identity (nodal basis, P = NULL).  Output layouts follow the reference's
+// memory order (MATLAB column-major [NM x NF x NV] / [NM x NG x NV]): voxel
+// slowest, measurement fastest, i.e. [nv][nf][nm] and [nv][ng][nm].  The TG
+// layout is J^T row-major with the measurement index g*NM + m, the K-major
+// operand of the J^T W J contraction.
+//
+// One block per voxel (grid-stride): the block gathers P phi and P phiA for
+// all harmonics and optodes into shared memory once (FP64 sums, stored as
+// complex FP32), then each thread owns measurements m and accumulates all NG
+// gates in registers; consecutive threads write consecutive m (coalesced).
+#include <algorithm>
+
+#include "dgp_common.cuh"
+#include "dgp_internal.h"
+
+namespace dgp {
+
+namespace {
+
+constexpr int JBS = 256;
+constexpr int NGMAX = 32;
+constexpr int PMAX = 8;
+
+struct JArgs {
+  const int32_t *prow, *pcol;
+  const double *pval;
+  int64_t nv, nn;
+  const double *w;           // [nv] voxel weights
+  const double2 *phi, *phiA; // [nf][nn][ns], [nf][nn][nd]
+  int ns, nd, nf, nm, ng;
+  const int32_t *link;       // [nm][2]
+};
+
+// stage (P phi)[v] -> sh[k*cnt + o] for o < cnt optodes of field f [nf][nn][cnt]
+__device__ void stage_field(const JArgs &a, int64_t v, const double2 *__restrict__ f, int cnt, float2 *sh) {
+  int32_t nodes[PMAX];
+  double wts[PMAX];
+  int np;
+  if (a.prow) {
+    int b = a.prow[v], e = a.prow[v + 1];
+    np = min(e - b, PMAX);
+    for (int q = 0; q < np; ++q) {
+      nodes[q] = a.pcol[b + q];
+      wts[q] = a.pval[b + q];
+    }
+  } else {
+    np = 1;
+    nodes[0] = (int32_t)v;
+    wts[0] = 1.0;
+  }
+  for (int t = threadIdx.x; t < a.nf * cnt; t += blockDim.x) {
+    int k = t / cnt, o = t % cnt;
+    double2 acc = make_double2(0, 0);
+    for (int q = 0; q < np; ++q) {
+      double2 x = f[((int64_t)k * a.nn + nodes[q]) * cnt + o];
+      acc.x += wts[q] * x.x;
+      acc.y += wts[q] * x.y;
+    }
+    sh[t] = make_float2((float)acc.x, (float)acc.y);
+  }
+}
+
+// MODE 0: time-gated Jacobian (float [nv][ng][nm]); MODE 1: complex FD Jacobian
+// (double2 [nv][nf][nm]); MODE 2: vector-Jacobian product out[v] (FP64).
+template <int MODE>
+__global__ void __launch_bounds__(JBS) k_jacobian(JArgs a, const float2 *__restrict__ Ctab,
+                                                  const double2 *__restrict__ fpsf_inv,
+                                                  const double *__restrict__ rytov, float *__restrict__ Jtg,
+                                                  double2 *__restrict__ Jfd, const float2 *__restrict__ Chat,
+                                                  double *__restrict__ vjp) {
+  extern __shared__ float2 sh[];
+  float2 *Ps = sh;                         // [nf][ns]
+  float2 *Pd = Ps + a.nf * a.ns;           // [nf][nd]
+  float2 *Cs = Pd + a.nf * a.nd;           // [ng][nf] (MODE 0)
+  if (MODE == 0)
+    for (int t = threadIdx.x; t < a.ng * a.nf; t += blockDim.x) Cs[t] = Ctab[t];
+  __shared__ double red[JBS / 32];
+  for (int64_t v = blockIdx.x; v < a.nv; v += gridDim.x) {
+    __syncthreads();
+    stage_field(a, v, a.phi, a.ns, Ps);
+    stage_field(a, v, a.phiA, a.nd, Pd);
+    __syncthreads();
+    const double wv = a.w ? a.w[v] : 1.0;
+    double part = 0.0;
+    for (int m = threadIdx.x; m < a.nm; m += blockDim.x) {
+      const int s = a.link[2 * m], d = a.link[2 * m + 1];
+      if (MODE == 0) {
+        float acc[NGMAX];
+#pragma unroll
+        for (int g = 0; g < NGMAX; ++g) acc[g] = 0.f;
+        for (int k = 0; k < a.nf; ++k) {
+          float2 x = Ps[k * a.ns + s], y = Pd[k * a.nd + d];
+          float ar = x.x * y.x - x.y * y.y, ai = x.x * y.y + x.y * y.x;
+#pragma unroll
+          for (int g = 0; g < NGMAX; ++g) {
+            if (g < a.ng) {
+              float2 c = Cs[g * a.nf + k];
+              acc[g] = fmaf(c.x, ar, fmaf(-c.y, ai, acc[g]));
+            }
+          }
+        }
+#pragma unroll
+        for (int g = 0; g < NGMAX; ++g) {
+          if (g < a.ng) {
+            double val = wv * (double)acc[g];
+            if (rytov) val /= rytov[(int64_t)m * a.ng + g];
+            Jtg[((int64_t)v * a.ng + g) * a.nm + m] = (float)val;
+          }
+        }
+      } else if (MODE == 1) {
+        for (int k = 0; k < a.nf; ++k) {
+          float2 x = Ps[k * a.ns + s], y = Pd[k * a.nd + d];
+          double2 p = make_double2((double)x.x * y.x - (double)x.y * y.y, (double)x.x * y.y + (double)x.y * y.x);
+          double2 r = cmul(p, fpsf_inv[k]);  // -1 / s_fpsf[k]
+          Jfd[((int64_t)v * a.nf + k) * a.nm + m] = make_double2(wv * r.x, wv * r.y);
+        }
+      } else {
+        double acc = 0.0;
+        for (int k = 0; k < a.nf; ++k) {
+          float2 x = Ps[k * a.ns + s], y = Pd[k * a.nd + d];
+          float ar = x.x * y.x - x.y * y.y, ai = x.x * y.y + x.y * y.x;
+          float2 c = Chat[(int64_t)m * a.nf + k];
+          acc += (double)(c.x * ar - c.y * ai);
+        }
+        part += acc;
+      }
+    }
+    if (MODE == 2) {
+      for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(0xffffffffu, part, off);
+      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int q = 0; q < JBS / 32; ++q) tot += red[q];
+        vjp[v] = wv * tot;
+      }
+    }
+  }
+}
+
+// C[g,k] = -2 Nt h_k conj(gate[g,k]) / fpsf[k]; also -1/fpsf[k] for the FD form
+__global__ void k_ctab(const double2 *__restrict__ gate, const double2 *__restrict__ fpsf, int ng, int nf, int nt,
+                       float2 *C, double2 *finv) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < nf) finv[t] = cdiv(make_double2(-1.0, 0.0), fpsf[t]);
+  if (t >= ng * nf || !gate) return;
+  int g = t / nf, k = t % nf;
+  double h = k == 0 ? 0.5 : 1.0;
+  double2 gc = make_double2(gate[t].x, -gate[t].y);
+  double2 r = cdiv(gc, fpsf[k]);
+  double s = -2.0 * (double)nt * h;
+  C[t] = make_float2((float)(s * r.x), (float)(s * r.y));
+}
+
+// Chat[m,k] = sum_g gin[m,g] C[g,k]   (the upstream gradient folded into the DFT)
+__global__ void k_chat(const double *__restrict__ gin, const float2 *__restrict__ C, const double *__restrict__ rytov,
+                       int nm, int ng, int nf, float2 *Chat) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= (int64_t)nm * nf) return;
+  int m = (int)(t / nf), k = (int)(t % nf);
+  double re = 0, im = 0;
+  for (int g = 0; g < ng; ++g) {
+    double q = gin[(int64_t)m * ng + g];
+    if (rytov) q /= rytov[(int64_t)m * ng + g];
+    float2 c = C[g * nf + k];
+    re += q * c.x;
+    im += q * c.y;
+  }
+  Chat[t] = make_float2((float)re, (float)im);
+}
+
+int launch_common(JArgs &a, size_t &smem, int &grid) {
+  DGP_REQUIRE(a.nv > 0 && a.nn > 0 && a.ns > 0 && a.nd > 0 && a.nf > 0 && a.nm > 0, "jacobian: sizes must be positive");
+  smem = sizeof(float2) * ((size_t)a.nf * (a.ns + a.nd) + (size_t)a.ng * a.nf);
+  DGP_REQUIRE(smem <= 200 * 1024, "jacobian: NF*(NS+ND+NG) too large for one block's shared memory");
+  grid = (int)std::min<int64_t>(a.nv, (int64_t)sm_count() * 8);
+  return DGP_OK;
+}
+
+}  // namespace
+
+int jacobian_run(int mode, const int32_t *prow, const int32_t *pcol, const double *pval, int64_t nv, const double *w,
+                 const double *phi, int ns, const double *phiA, int nd, int64_t nn, int nf, const double *fpsf,
+                 const int32_t *link, int nm, const double *gate, int ng, int nt, const double *rytov, void *out,
+                 const double *gin, cudaStream_t st) {
+  DGP_REQUIRE(phi && phiA && fpsf && link && out, "jacobian: null pointer");
+  DGP_REQUIRE(mode == 1 || (gate && ng >= 1 && ng <= NGMAX), "jacobian: need gate coefficients, 1 <= NG <= 32");
+  DGP_REQUIRE(prow || nv == nn, "jacobian: the nodal basis (P = NULL) needs nv == nn");
+  JArgs a{prow, pcol, pval, nv, nn, w, (const double2 *)phi, (const double2 *)phiA, ns, nd, nf, nm, mode == 1 ? 0 : ng,
+          link};
+  size_t smem;
+  int grid;
+  DGP_TRY(launch_common(a, smem, grid));
+  DevBuf ctab, finv, chat;
+  DGP_TRY(ctab.alloc(sizeof(float2) * (size_t)std::max(1, ng) * nf));
+  DGP_TRY(finv.alloc(sizeof(double2) * nf));
+  int nt_ = std::max(ng * nf, nf);
+  k_ctab<<<(unsigned)ceil_div(nt_, 256), 256, 0, st>>>((const double2 *)gate, (const double2 *)fpsf, mode == 1 ? 0 : ng,
+                                                        nf, nt, ctab.as<float2>(), finv.as<double2>());
+  DGP_CHECK_LAUNCH();
+  if (smem > 48 * 1024) {
+    DGP_CUDA(cudaFuncSetAttribute(k_jacobian<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    DGP_CUDA(cudaFuncSetAttribute(k_jacobian<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    DGP_CUDA(cudaFuncSetAttribute(k_jacobian<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  }
+  if (mode == 0) {
+    k_jacobian<0><<<grid, JBS, smem, st>>>(a, ctab.as<float2>(), finv.as<double2>(), rytov, (float *)out, nullptr,
+                                           nullptr, nullptr);
+  } else if (mode == 1) {
+    k_jacobian<1><<<grid, JBS, smem, st>>>(a, ctab.as<float2>(), finv.as<double2>(), nullptr, nullptr,
+                                           (double2 *)out, nullptr, nullptr);
+  } else {
+    DGP_REQUIRE(gin, "jacobian vjp: null upstream gradient");
+    DGP_TRY(chat.alloc(sizeof(float2) * (size_t)nm * nf));
+    k_chat<<<(unsigned)ceil_div((int64_t)nm * nf, 256), 256, 0, st>>>(gin, ctab.as<float2>(), rytov, nm, ng, nf,
+                                                                      chat.as<float2>());
+    DGP_CHECK_LAUNCH();
+    k_jacobian<2><<<grid, JBS, smem, st>>>(a, ctab.as<float2>(), finv.as<double2>(), nullptr, nullptr, nullptr,
+                                           chat.as<float2>(), (double *)out);
+  }
+  DGP_CHECK_LAUNCH();
+  DGP_CUDA(cudaStreamSynchronize(st));  // scratch tables are released on return
+  return DGP_OK;
+}
+
+}  // namespace dgp

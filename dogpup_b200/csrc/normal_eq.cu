@@ -1,0 +1,533 @@
+// Weighted Levenberg-Marquardt normal-equation step on the device.
+//
+// Replaces tik_inv (DOGPUP/reconstruction/tik_inv.m:1-20), which forms
+// H = J'J on the CPU, adds lam * max_j sum_i J_ij^2 to the diagonal and
+// solves H \ (J'y) with MATLAB's backslash (Cholesky for SPD H); here with
+// a diagonal data weight W = 1/sigma^2:
+//
+//   H = J' W J                         split-BF16 tcgen05 SYRK, FP32 accumulate
+//   H_ii += lam * max_j (J'WJ)_jj      (or lam * (J'WJ)_ii), FP64 exact diagonal
+//   r = J' W y                         FP64
+//   H = L L', solve L L' x = r         FP64 blocked Cholesky + triangular solves
+//
+// Input J is given transposed, Jt [nv][nmeas] float32 row-major -- the layout
+// the TG Jacobian kernel writes -- so both GEMM operands are K-major.
+//
+// Split BF16: Js = sqrt(W) * Jt = hi + lo with hi = bf16(Js), lo =
+// bf16(Js - hi); H = hi hi' + hi lo' + lo hi' (the lo lo' term, ~2^-16
+// relative, is dropped), three BF16 tensor-core products per K step into one
+// FP32 accumulator in tensor memory.
+//
+// SYRK kernel: one CTA per 128 x 128 tile of the lower triangle of H.
+//   warp 0 lane 0: TMA producer (4 tiles per stage: A hi/lo, B hi/lo, each
+//                  128 rows x 64 K of bf16 with the 128-byte swizzle),
+//   warp 1 lane 0: MMA issuer (tcgen05.mma kind::f16, M=128 N=128 K=16),
+//   warps 0..3:    epilogue (tcgen05.ld 32x32b, FP32 -> FP64 stores).
+// Three pipeline stages (192 KB of shared memory).  Every mbarrier wait is
+// bounded; a timeout sets an error flag, skips the remaining work, waits
+// (bounded) for copies in flight and always frees the tensor memory.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+
+#include "dgp_common.cuh"
+#include "dgp_internal.h"
+
+namespace dgp {
+
+namespace {
+
+constexpr int TM = 128, TN = 128, TK = 64, STAGES = 3;
+constexpr int TILE_BYTES = TM * TK * 2;       // 16 KB: 128 rows x 64 bf16
+constexpr int STAGE_BYTES = 4 * TILE_BYTES;   // A hi, A lo, B hi, B lo
+constexpr int SYRK_SMEM = STAGES * STAGE_BYTES + 1024;  // + alignment slack
+constexpr uint32_t kSpinLimit = 1u << 22;     // bounded mbarrier waits (~0.5 s)
+
+__device__ inline uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ inline void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ inline void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// bounded wait for the phase with the given parity; false on timeout
+__device__ inline bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  const uint32_t addr = smem_u32(bar);
+  for (uint32_t it = 0; it < kSpinLimit; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (it > 256) __nanosleep(100);
+  }
+  return false;
+}
+
+__device__ inline void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// UMMA shared-memory descriptor: K-major operand, 128-byte swizzle, rows of
+// 128 B grouped by 8 (stride 1024 B), sm100 descriptor version 1.
+__device__ inline uint64_t sdesc_k_sw128(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1 << 16;             // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;   // stride byte offset
+  d |= (uint64_t)1 << 46;             // descriptor version
+  d |= (uint64_t)2 << 61;             // SWIZZLE_128B
+  return d;
+}
+
+// instruction descriptor, kind::f16: BF16 x BF16 -> F32, both K-major, M=128, N=128
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) |
+                            ((uint32_t)(TM >> 4) << 24);
+
+__device__ inline void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accum)
+      : "memory");
+}
+
+__device__ inline void umma_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ inline void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__global__ void __launch_bounds__(128, 1) k_syrk_tc(const __grid_constant__ CUtensorMap map_hi,
+                                                    const __grid_constant__ CUtensorMap map_lo, int nk, int64_t nv,
+                                                    double *__restrict__ H, int64_t ldh, int *err) {
+  extern __shared__ __align__(1024) unsigned char sm_raw[];
+  __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], done;
+  __shared__ uint32_t tmem_slot;
+  __shared__ int abort_flag;
+  // 1024-byte aligned stage buffers (the 128-byte swizzle atom is 8 rows x 128 B)
+  unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~uintptr_t(1023));
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // lower-triangular tile (ti >= tj) of this block
+  const int64_t b = blockIdx.x;
+  int64_t ti = (int64_t)((sqrt(8.0 * (double)b + 1.0) - 1.0) * 0.5);
+  while (ti * (ti + 1) / 2 > b) --ti;
+  while ((ti + 1) * (ti + 2) / 2 <= b) ++ti;
+  const int64_t tj = b - ti * (ti + 1) / 2;
+
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(&done, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                 "r"(TN)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---------------- TMA producer
+    int issued = 0;
+    for (int kb = 0; kb < nk; ++kb) {
+      const int s = kb % STAGES;
+      const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
+      if (!mbar_wait(&empty[s], ph ^ 1u)) { atomicOr(err, 1); abort_flag = 1; break; }
+      if (*(volatile int *)&abort_flag) break;
+      unsigned char *st = sm + (size_t)s * STAGE_BYTES;
+      mbar_expect_tx(&full[s], STAGE_BYTES);
+      const int x = kb * TK;
+      tma_load_2d(st + 0 * TILE_BYTES, &map_hi, &full[s], x, (int)(ti * TM));
+      tma_load_2d(st + 1 * TILE_BYTES, &map_lo, &full[s], x, (int)(ti * TM));
+      tma_load_2d(st + 2 * TILE_BYTES, &map_hi, &full[s], x, (int)(tj * TN));
+      tma_load_2d(st + 3 * TILE_BYTES, &map_lo, &full[s], x, (int)(tj * TN));
+      issued = kb + 1;
+    }
+    // on an abort, wait (bounded) for the copies still in flight before teardown
+    if (*(volatile int *)&abort_flag) {
+      for (int kb = std::max(0, issued - STAGES); kb < issued; ++kb)
+        mbar_wait(&full[kb % STAGES], (uint32_t)(kb / STAGES) & 1u);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---------------- MMA issuer
+    bool ok = true;
+    for (int kb = 0; kb < nk; ++kb) {
+      const int s = kb % STAGES;
+      const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
+      if (!mbar_wait(&full[s], ph)) { atomicOr(err, 2); abort_flag = 1; ok = false; break; }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t base = smem_u32(sm + (size_t)s * STAGE_BYTES);
+#pragma unroll
+      for (int k = 0; k < TK / 16; ++k) {
+        const uint32_t off = (uint32_t)k * 32u;  // 16 bf16 along K inside the swizzle atom
+        const uint64_t ahi = sdesc_k_sw128(base + 0 * TILE_BYTES + off);
+        const uint64_t alo = sdesc_k_sw128(base + 1 * TILE_BYTES + off);
+        const uint64_t bhi = sdesc_k_sw128(base + 2 * TILE_BYTES + off);
+        const uint64_t blo = sdesc_k_sw128(base + 3 * TILE_BYTES + off);
+        umma_bf16(tmem, ahi, bhi, (kb | k) ? 1u : 0u);
+        umma_bf16(tmem, ahi, blo, 1u);
+        umma_bf16(tmem, alo, bhi, 1u);
+      }
+      umma_commit(&empty[s]);  // frees the stage once these MMAs have read it
+    }
+    if (ok) umma_commit(&done);
+  }
+  __syncwarp();
+  // ---------------- epilogue: TMEM -> registers -> H (FP64)
+  bool have = !*(volatile int *)&abort_flag;
+  if (have) have = mbar_wait(&done, 0);
+  have = __all_sync(0xffffffffu, have);  // tcgen05.ld below is warp-collective
+  if (!have && lane == 0) atomicOr(err, 4);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (have) {
+    const int64_t row = ti * TM + warp * 32 + lane;
+#pragma unroll 1
+    for (int c = 0; c < TN; c += 32) {
+      uint32_t r[32];
+      tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, r);
+      if (row < nv) {
+        double *dst = H + row * ldh + tj * TN + c;
+#pragma unroll
+        for (int q = 0; q < 32; ++q)
+          if (tj * TN + c + q < nv) dst[q] = (double)__uint_as_float(r[q]);
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TN) : "memory");
+}
+
+// Js = sqrt(W) Jt split into bf16 hi + lo, zero-padded to [nvp][nmp]; exact
+// FP64 diagonal d[v] = sum_m W_m Jt[v][m]^2
+__global__ void k_split(const float *__restrict__ Jt, const double *__restrict__ W, int64_t nv, int64_t nm,
+                        int64_t nvp, int64_t nmp, __nv_bfloat16 *hi, __nv_bfloat16 *lo) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= nvp * nmp) return;
+  int64_t v = t / nmp, m = t % nmp;
+  float x = 0.f;
+  if (v < nv && m < nm) x = Jt[v * nm + m] * (W ? (float)sqrt(W[m]) : 1.f);
+  __nv_bfloat16 h = __float2bfloat16_rn(x);
+  hi[t] = h;
+  lo[t] = __float2bfloat16_rn(x - __bfloat162float(h));
+}
+
+__global__ void k_row_dots(const float *__restrict__ Jt, const double *__restrict__ W, const double *__restrict__ y,
+                           int64_t nv, int64_t nm, double *diag, double *rhs) {
+  __shared__ double sd[256], sr[256];
+  for (int64_t v = blockIdx.x; v < nv; v += gridDim.x) {
+    double d = 0, r = 0;
+    for (int64_t m = threadIdx.x; m < nm; m += blockDim.x) {
+      double j = Jt[v * nm + m], w = W ? W[m] : 1.0;
+      d += w * j * j;
+      if (y) r += j * w * y[m];
+    }
+    sd[threadIdx.x] = d;
+    sr[threadIdx.x] = r;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+      if (threadIdx.x < o) {
+        sd[threadIdx.x] += sd[threadIdx.x + o];
+        sr[threadIdx.x] += sr[threadIdx.x + o];
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      diag[v] = sd[0];
+      if (rhs) rhs[v] = sr[0];
+    }
+    __syncthreads();
+  }
+}
+
+// H_ii = d_i + lam * (mode 0: max_j d_j, the tik_inv rule; mode 1: d_i)
+__global__ void k_damp(double *H, int64_t ldh, const double *__restrict__ diag, int64_t nv, double lam, int mode) {
+  __shared__ double smax;
+  if (threadIdx.x == 0) {
+    double m = 0;
+    for (int64_t i = 0; i < nv; ++i) m = fmax(m, diag[i]);
+    smax = m;
+  }
+  __syncthreads();
+  for (int64_t i = threadIdx.x; i < nv; i += blockDim.x)
+    H[i * ldh + i] = diag[i] + lam * (mode == 0 ? smax : diag[i]);
+}
+
+// ------------------------------------------------------- FP64 Cholesky
+constexpr int NB = 64;
+
+// factor the diagonal block in place (unblocked right-looking, shared memory)
+__global__ void __launch_bounds__(256) k_potrf_diag(double *H, int64_t ldh, int64_t k0, int nb, int *err) {
+  __shared__ double A[NB][NB + 1];
+  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
+    int i = t / nb, j = t % nb;
+    A[i][j] = j <= i ? H[(k0 + i) * ldh + k0 + j] : 0.0;
+  }
+  __syncthreads();
+  for (int j = 0; j < nb; ++j) {
+    if (threadIdx.x == 0) {
+      double d = A[j][j];
+      if (!(d > 0.0) || !isfinite(d)) { atomicOr(err, 8); d = 1.0; }
+      A[j][j] = sqrt(d);
+    }
+    __syncthreads();
+    for (int i = j + 1 + threadIdx.x; i < nb; i += blockDim.x) A[i][j] /= A[j][j];
+    __syncthreads();
+    for (int t = threadIdx.x; t < (nb - j - 1) * (nb - j - 1); t += blockDim.x) {
+      int i = j + 1 + t / (nb - j - 1), l = j + 1 + t % (nb - j - 1);
+      if (l <= i) A[i][l] -= A[i][j] * A[l][j];
+    }
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
+    int i = t / nb, j = t % nb;
+    if (j <= i) H[(k0 + i) * ldh + k0 + j] = A[i][j];
+  }
+}
+
+// panel rows i >= k0 + nb: x L_kk^T = a  (forward substitution per row)
+__global__ void __launch_bounds__(128) k_trsm_panel(double *H, int64_t ldh, int64_t k0, int nb, int64_t n) {
+  __shared__ double L[NB][NB + 1];
+  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
+    int i = t / nb, j = t % nb;
+    L[i][j] = j <= i ? H[(k0 + i) * ldh + k0 + j] : 0.0;
+  }
+  __syncthreads();
+  int64_t i = k0 + nb + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double x[NB];
+  double *row = H + i * ldh + k0;
+  for (int j = 0; j < nb; ++j) {
+    double a = row[j];
+    for (int l = 0; l < j; ++l) a -= x[l] * L[j][l];
+    x[j] = a / L[j][j];
+  }
+  for (int j = 0; j < nb; ++j) row[j] = x[j];
+}
+
+// trailing update of the lower triangle: H[i][l] -= sum_j L[i][j] L[l][j], one 64x64 tile per block
+__global__ void __launch_bounds__(256) k_chol_update(double *H, int64_t ldh, int64_t k0, int nb, int64_t n) {
+  constexpr int KC = 32;  // K chunk staged in shared memory
+  __shared__ double As[NB][KC + 1], Bs[NB][KC + 1];
+  const int64_t b = blockIdx.x;
+  int64_t ti = (int64_t)((sqrt(8.0 * (double)b + 1.0) - 1.0) * 0.5);
+  while (ti * (ti + 1) / 2 > b) --ti;
+  while ((ti + 1) * (ti + 2) / 2 <= b) ++ti;
+  const int64_t tl = b - ti * (ti + 1) / 2;
+  const int64_t r0 = k0 + nb + ti * NB, c0 = k0 + nb + tl * NB;
+  const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;  // 4x4 outputs per thread
+  double acc[4][4] = {};
+  for (int j0 = 0; j0 < nb; j0 += KC) {
+    const int kc = min(KC, nb - j0);
+    __syncthreads();
+    for (int t = threadIdx.x; t < NB * KC; t += blockDim.x) {
+      int i = t / KC, j = t % KC;
+      bool in = j < kc;
+      As[i][j] = (in && r0 + i < n) ? H[(r0 + i) * ldh + k0 + j0 + j] : 0.0;
+      Bs[i][j] = (in && c0 + i < n) ? H[(c0 + i) * ldh + k0 + j0 + j] : 0.0;
+    }
+    __syncthreads();
+    for (int j = 0; j < kc; ++j) {
+      double a[4], c[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        a[q] = As[ty + 16 * q][j];
+        c[q] = Bs[tx + 16 * q][j];
+      }
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[p][q] = fma(a[p], c[q], acc[p][q]);
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      int64_t i = r0 + ty + 16 * p, l = c0 + tx + 16 * q;
+      if (i < n && l <= i) H[i * ldh + l] -= acc[p][q];
+    }
+}
+
+// forward / backward substitution on one diagonal block (one block of threads)
+__global__ void k_trsv_diag(const double *H, int64_t ldh, int64_t k0, int nb, double *x, int lower) {
+  __shared__ double xs[NB];
+  if (threadIdx.x == 0) {
+    if (lower) {
+      for (int j = 0; j < nb; ++j) {
+        double a = x[k0 + j];
+        for (int l = 0; l < j; ++l) a -= H[(k0 + j) * ldh + k0 + l] * xs[l];
+        xs[j] = a / H[(k0 + j) * ldh + k0 + j];
+      }
+    } else {
+      for (int j = nb - 1; j >= 0; --j) {
+        double a = x[k0 + j];
+        for (int l = j + 1; l < nb; ++l) a -= H[(k0 + l) * ldh + k0 + j] * xs[l];
+        xs[j] = a / H[(k0 + j) * ldh + k0 + j];
+      }
+    }
+    for (int j = 0; j < nb; ++j) x[k0 + j] = xs[j];
+  }
+}
+
+// forward: x[i] -= sum_{j in block} L[i][j] x[j] for i below the block
+__global__ void k_trsv_fwd_update(const double *H, int64_t ldh, int64_t k0, int nb, int64_t n, double *x) {
+  int64_t i = k0 + nb + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double a = 0;
+  for (int j = 0; j < nb; ++j) a += H[i * ldh + k0 + j] * x[k0 + j];
+  x[i] -= a;
+}
+
+// backward: x[k0+j] -= sum_{i >= k0+nb} L[i][k0+j] x[i]   (column reduction)
+__global__ void k_trsv_bwd_update(const double *H, int64_t ldh, int64_t k0, int nb, int64_t n, double *x) {
+  __shared__ double part[256];
+  const int j = blockIdx.x;
+  double a = 0;
+  for (int64_t i = k0 + nb + threadIdx.x; i < n; i += blockDim.x) a += H[i * ldh + k0 + j] * x[i];
+  part[threadIdx.x] = a;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) x[k0 + j] -= part[0];
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+int make_map(CUtensorMap *map, void *base, int64_t rows, int64_t cols) {
+  auto enc = get_encode();
+  if (!enc) return fail(DGP_ERR_CUDA, "normal_eq: cuTensorMapEncodeTiled is unavailable");
+  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
+  cuuint32_t box[2] = {(cuuint32_t)TK, (cuuint32_t)TM};
+  cuuint32_t es[2] = {1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, es,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(DGP_ERR_CUDA, "normal_eq: tensor map encoding failed");
+  return DGP_OK;
+}
+
+}  // namespace
+
+int normal_eq_run(const float *Jt, int64_t nv, int64_t nm, const double *W, const double *y, double lam, int mode,
+                  double *H, int64_t ldh, double *rhs, cudaStream_t st) {
+  DGP_REQUIRE(Jt && H, "normal_eq: null pointer");
+  DGP_REQUIRE(nv > 0 && nm > 0 && ldh >= nv, "normal_eq: bad sizes");
+  DGP_REQUIRE(mode == 0 || mode == 1, "normal_eq: damping mode is 0 (lam*max diag) or 1 (lam*diag)");
+  const int64_t nvp = ceil_div(nv, TM) * TM, nmp = ceil_div(nm, TK) * TK;
+  DGP_REQUIRE(nmp < (int64_t)INT32_MAX && nvp < (int64_t)INT32_MAX, "normal_eq: sizes exceed TMA coordinates");
+  DevBuf hi, lo, diag, errb;
+  DGP_TRY(hi.alloc(sizeof(__nv_bfloat16) * (size_t)nvp * nmp));
+  DGP_TRY(lo.alloc(sizeof(__nv_bfloat16) * (size_t)nvp * nmp));
+  DGP_TRY(diag.alloc(sizeof(double) * nv));
+  DGP_TRY(errb.alloc(sizeof(int)));
+  DGP_CUDA(cudaMemsetAsync(errb.p, 0, sizeof(int), st));
+  k_split<<<(unsigned)ceil_div(nvp * nmp, 256), 256, 0, st>>>(Jt, W, nv, nm, nvp, nmp, hi.as<__nv_bfloat16>(),
+                                                               lo.as<__nv_bfloat16>());
+  DGP_CHECK_LAUNCH();
+  k_row_dots<<<(unsigned)std::min<int64_t>(nv, 4096), 256, 0, st>>>(Jt, W, y, nv, nm, diag.as<double>(), rhs);
+  DGP_CHECK_LAUNCH();
+  CUtensorMap mhi, mlo;
+  DGP_TRY(make_map(&mhi, hi.p, nvp, nmp));
+  DGP_TRY(make_map(&mlo, lo.p, nvp, nmp));
+  DGP_CUDA(cudaFuncSetAttribute(k_syrk_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, SYRK_SMEM));
+  const int64_t T = nvp / TM;
+  const int64_t tiles = T * (T + 1) / 2;
+  k_syrk_tc<<<(unsigned)tiles, 128, SYRK_SMEM, st>>>(mhi, mlo, (int)(nmp / TK), nv, H, ldh, errb.as<int>());
+  DGP_CHECK_LAUNCH();
+  k_damp<<<1, 256, 0, st>>>(H, ldh, diag.as<double>(), nv, lam, mode);
+  DGP_CHECK_LAUNCH();
+  int herr = 0;
+  DGP_CUDA(cudaMemcpyAsync(&herr, errb.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  DGP_CUDA(cudaStreamSynchronize(st));
+  if (herr) return fail(DGP_ERR_CUDA, "normal_eq: tensor-core pipeline wait timed out (error flags " +
+                                          std::to_string(herr) + ")");
+  return DGP_OK;
+}
+
+int cholesky_solve_run(double *H, int64_t n, int64_t ldh, double *x, cudaStream_t st) {
+  DGP_REQUIRE(H && x && n > 0 && ldh >= n, "cholesky: bad arguments");
+  DevBuf errb;
+  DGP_TRY(errb.alloc(sizeof(int)));
+  DGP_CUDA(cudaMemsetAsync(errb.p, 0, sizeof(int), st));
+  for (int64_t k0 = 0; k0 < n; k0 += NB) {
+    const int nb = (int)std::min<int64_t>(NB, n - k0);
+    k_potrf_diag<<<1, 256, 0, st>>>(H, ldh, k0, nb, errb.as<int>());
+    const int64_t rest = n - k0 - nb;
+    if (rest > 0) {
+      k_trsm_panel<<<(unsigned)ceil_div(rest, 128), 128, 0, st>>>(H, ldh, k0, nb, n);
+      const int64_t T = ceil_div(rest, NB);
+      k_chol_update<<<(unsigned)(T * (T + 1) / 2), 256, 0, st>>>(H, ldh, k0, nb, n);
+    }
+  }
+  DGP_CHECK_LAUNCH();
+  for (int64_t k0 = 0; k0 < n; k0 += NB) {  // L y = b
+    const int nb = (int)std::min<int64_t>(NB, n - k0);
+    k_trsv_diag<<<1, 32, 0, st>>>(H, ldh, k0, nb, x, 1);
+    if (n - k0 - nb > 0) k_trsv_fwd_update<<<(unsigned)ceil_div(n - k0 - nb, 256), 256, 0, st>>>(H, ldh, k0, nb, n, x);
+  }
+  for (int64_t k0 = ((n - 1) / NB) * NB; k0 >= 0; k0 -= NB) {  // L' x = y
+    const int nb = (int)std::min<int64_t>(NB, n - k0);
+    if (n - k0 - nb > 0) k_trsv_bwd_update<<<nb, 256, 0, st>>>(H, ldh, k0, nb, n, x);
+    k_trsv_diag<<<1, 32, 0, st>>>(H, ldh, k0, nb, x, 0);
+  }
+  DGP_CHECK_LAUNCH();
+  int herr = 0;
+  DGP_CUDA(cudaMemcpyAsync(&herr, errb.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  DGP_CUDA(cudaStreamSynchronize(st));
+  if (herr) return fail(DGP_ERR_ARG, "cholesky: matrix is not positive definite");
+  return DGP_OK;
+}
+
+}  // namespace dgp

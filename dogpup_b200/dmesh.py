@@ -129,6 +129,44 @@ class DMesh:
         link = torch.as_tensor(self.optode.link.astype(np.int32), device="cuda").contiguous()
         return api.meas(nodes, w, link, phi)
 
+    # ------------------------------------------------------------ Jacobian
+    def mesh2grid(self, x, y, z):
+        """Voxel basis of the Jacobian (dMesh.m:286-380): m2g, g2m, gridinmesh, dxyz."""
+        from .grid import mesh2grid
+        g = mesh2grid(self.node_host, self.elem_host, np.asarray(x), np.asarray(y), np.asarray(z), self.locator())
+        self.grid, self.m2g, self.g2m = g["grid"], g["m2g"], g["g2m"]
+        self.gridinmesh, self.dxyz, self.gridSize = g["gridinmesh"], g["dxyz"], g["size"]
+        self.grid_basis = api.Basis(self.m2g, np.full(self.m2g.shape[0], self.dxyz ** 3))
+        return self
+
+    def nodal_basis(self):
+        """Nodal basis: J per node weighted by the lumped mass sum_j M_ij."""
+        rows = torch.repeat_interleave(torch.arange(self.nn, device="cuda"),
+                                       (self.fem.rowptr[1:] - self.fem.rowptr[:-1]).long())
+        lump = torch.zeros(self.nn, dtype=torch.float64, device="cuda").index_add_(0, rows, self.M)
+        return api.Basis(None, lump, nn=self.nn)
+
+    def _link(self):
+        return torch.as_tensor(self.optode.link.astype(np.int32), device="cuda").contiguous()
+
+    def J_complex(self, phi=None, phiA=None, basis=None, **solve_kw):
+        """Complex absorption Jacobian J[v][k][m] (dMesh.m:206-247) plus data, phi, phiA."""
+        if phiA is None:
+            phiA = self.adj_flu_solve(**solve_kw)
+        if phi is None:
+            phi, _ = self.flu_solve(**solve_kw)
+        data = self.meas_flu(phi)
+        basis = basis or self.grid_basis
+        J = api.jacobian_complex(basis, phi, phiA, self.optode.s_fpsf, self._link())
+        return J, data, phi, phiA
+
+    def J_tg(self, gate_fc, phi, phiA, basis=None, rytov=False):
+        """Time-gated Jacobian J_tg[v][g][m] (fc2tg of J_complex), optionally / data_tg (Rytov)."""
+        basis = basis or self.grid_basis
+        nt = len(self.optode.tAxis)
+        data_tg = api.fc2tg(self.meas_flu(phi), gate_fc, nt) if rytov else None
+        return api.jacobian_tg(basis, phi, phiA, self.optode.s_fpsf, self._link(), gate_fc, nt, data_tg), data_tg
+
 
 def to_reference_layout(phi: torch.Tensor) -> torch.Tensor:
     """[NF][NN][NS] -> the reference's [NN][NF][NS]."""

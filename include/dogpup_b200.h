@@ -255,6 +255,69 @@ int dgp_fc2td(const double *d_c, int64_t nr, int32_t nf, const double *d_f,
 int dgp_fc2tg(const double *d_c, int64_t nr, int32_t nf, const double *d_gate_fc,
               int32_t ng, int32_t nt, double *d_y, dgp_stream_t stream);
 
+/* ====================================================================== *
+ *  Absorption Jacobian (J_complex, dMesh.m:206-247) and its time-gated
+ *  form (fc2tg along the harmonic axis, tut_2...m:147, wghtd_LM_recon.m:61).
+ *
+ *  Basis: d_P_* is the CSR of the mesh-to-voxel interpolation m2g
+ *  ([nv x nn], <= 8 entries per row, dMesh.m:286-327) or NULL for the nodal
+ *  basis (nv == nn).  d_w [nv]: voxel weight (dxyz^3 for the voxel grid, the
+ *  lumped nodal mass for the nodal basis), NULL = 1.
+ *  Fields: d_phi [nf][nn][ns], d_phiA [nf][nn][nd] complex128 (forward and
+ *  adjoint fluence as dgp_solve writes them); d_fpsf [nf] complex128;
+ *  d_link [nm][2] (source, detector).  Outputs use the reference's memory
+ *  order: voxel slowest, measurement fastest.
+ * ====================================================================== */
+/* J[v][k][m] complex128 = -(P phi_s)(P phiA_d) w_v / s_fpsf[k]. */
+int dgp_jacobian_complex(const int32_t *d_P_rowptr, const int32_t *d_P_col,
+                         const double *d_P_val, int64_t nv, const double *d_w,
+                         const double *d_phi, int32_t ns, const double *d_phiA,
+                         int32_t nd, int64_t nn, int32_t nf,
+                         const double *d_fpsf, const int32_t *d_link,
+                         int32_t nm, double *d_J, dgp_stream_t stream);
+/* J_tg[v][g][m] float32 = Nt 2 Re sum_k conj(gate_fc[g][k]) J~[m][k][v]
+ * (J~_0 = J_0/2), divided by d_data_tg[m][g] when that is not NULL (Rytov
+ * normalisation).  1 <= ng <= 32.  Row v of the output is row v of J^T
+ * with measurement index g*nm + m. */
+int dgp_jacobian_tg(const int32_t *d_P_rowptr, const int32_t *d_P_col,
+                    const double *d_P_val, int64_t nv, const double *d_w,
+                    const double *d_phi, int32_t ns, const double *d_phiA,
+                    int32_t nd, int64_t nn, int32_t nf, const double *d_fpsf,
+                    const int32_t *d_link, int32_t nm, const double *d_gate_fc,
+                    int32_t ng, int32_t nt, const double *d_data_tg,
+                    float *d_J, dgp_stream_t stream);
+/* out[v] = sum_{m,g} J_tg[v][g][m] * d_g[m][g]: the TG Jacobian's transpose
+ * applied to an upstream gradient without forming J (same arguments). */
+int dgp_jacobian_tg_vjp(const int32_t *d_P_rowptr, const int32_t *d_P_col,
+                        const double *d_P_val, int64_t nv, const double *d_w,
+                        const double *d_phi, int32_t ns, const double *d_phiA,
+                        int32_t nd, int64_t nn, int32_t nf,
+                        const double *d_fpsf, const int32_t *d_link,
+                        int32_t nm, const double *d_gate_fc, int32_t ng,
+                        int32_t nt, const double *d_data_tg, const double *d_g,
+                        double *d_out, dgp_stream_t stream);
+
+/* ====================================================================== *
+ *  Levenberg-Marquardt normal equations (tik_inv, reconstruction/
+ *  tik_inv.m:1-20, with a diagonal data weight W = 1/sigma^2).
+ * ====================================================================== */
+enum { DGP_DAMP_MAX_DIAG = 0, DGP_DAMP_DIAG = 1 };
+/* H = J^T W J (lower triangle of d_H [nv][ldh] in FP64, from split-BF16
+ * tensor-core products with FP32 accumulation), H_ii = (J^T W J)_ii (exact
+ * FP64) + lambda * (max_j (J^T W J)_jj for DGP_DAMP_MAX_DIAG, the tik_inv
+ * rule; (J^T W J)_ii for DGP_DAMP_DIAG), and d_rhs = J^T W y (FP64) when
+ * d_y and d_rhs are not NULL.  d_Jt is J transposed, [nv][nmeas] float32
+ * (the dgp_jacobian_tg output); d_w [nmeas] or NULL (W = I).  The strict
+ * upper triangle of d_H is not written. */
+int dgp_normal_eq(const float *d_Jt, int64_t nv, int64_t nmeas, const double *d_w,
+                  const double *d_y, double lambda, int32_t damping, double *d_H,
+                  int64_t ldh, double *d_rhs, dgp_stream_t stream);
+/* Solves H x = b in place (d_x: b in, x out) by an FP64 Cholesky
+ * factorisation of the lower triangle of d_H (overwritten by L).
+ * Returns DGP_ERR_ARG if H is not positive definite. */
+int dgp_cholesky_solve(double *d_H, int64_t n, int64_t ldh, double *d_x,
+                       dgp_stream_t stream);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -1,0 +1,85 @@
+"""GPU Jacobian, TG Jacobian and vjp against the oracle's J_complex restatement.
+
+Tolerances (norm-wise relative): complex Jacobian 1e-6 and TG Jacobian 1e-5
+(fields are staged in complex FP32, sums accumulate in FP32 / FP64); the vjp
+against the explicit J^T g from the same Jacobian, 1e-5.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def jac_case():
+    import torch
+    from dogpup_b200 import workloads, api
+    from oracle.transforms import td2fc
+    w = workloads.small_fwd(ns=4, nd=5, nf=16)
+    mesh = workloads.build_dmesh(w)
+    phi, data = mesh.flu_solve(precision="fp64", tol=1e-12)
+    phiA = mesh.adj_flu_solve(precision="fp64", tol=1e-12)
+    t = w["t"]
+    sd = 250e-12 / (2 * np.sqrt(2 * np.log(2)))
+    gates = np.stack([np.exp(-(t - (0.3e-9 + q * 250e-12)) ** 2 / (2 * sd ** 2)) for q in range(20)])
+    gfc = td2fc(gates, mesh.optode.fAxis, t)
+    lo, hi = w["mesh"].node.min(0), w["mesh"].node.max(0)
+    xs = [np.arange(lo[d] - 2, hi[d] + 2.001, 2.0) for d in range(3)]
+    mesh.mesh2grid(*xs)
+    return dict(w=w, mesh=mesh, phi=phi, phiA=phiA, gfc=gfc, gates=gates,
+                gfc_d=torch.as_tensor(gfc, device="cuda"))
+
+
+def rel(a, b):
+    return np.linalg.norm(np.ravel(a - b)) / np.linalg.norm(np.ravel(b))
+
+
+def _oracle_J(case, P, wts):
+    from oracle.jacobian import j_complex
+    mesh = case["mesh"]
+    phi = np.transpose(case["phi"].cpu().numpy(), (1, 2, 0))     # [NN, NS, NF]
+    phiA = np.transpose(case["phiA"].cpu().numpy(), (1, 2, 0))
+    return j_complex(P, wts, phi, phiA, mesh.optode.link, mesh.optode.s_fpsf.cpu().numpy())
+
+
+def test_complex_jacobian_voxel_basis(jac_case):
+    mesh = jac_case["mesh"]
+    J, data, _, _ = mesh.J_complex(jac_case["phi"], jac_case["phiA"])
+    J0 = _oracle_J(jac_case, mesh.m2g, mesh.dxyz ** 3)             # [NM, NF, NV]
+    assert rel(np.transpose(J.cpu().numpy(), (2, 1, 0)), J0) < 1e-6
+
+
+def test_tg_jacobian_and_rytov(jac_case):
+    from oracle.jacobian import j_tg
+    from oracle.transforms import fc2tg
+    mesh = jac_case["mesh"]
+    nt = len(mesh.optode.tAxis)
+    J0 = j_tg(_oracle_J(jac_case, mesh.m2g, mesh.dxyz ** 3), jac_case["gfc"], nt)   # [NM, NG, NV]
+    Jt, _ = mesh.J_tg(jac_case["gfc_d"], jac_case["phi"], jac_case["phiA"])
+    assert rel(np.transpose(Jt.cpu().numpy(), (2, 1, 0)), J0) < 1e-5
+    Jr, dtg = mesh.J_tg(jac_case["gfc_d"], jac_case["phi"], jac_case["phiA"], rytov=True)
+    d0 = fc2tg(mesh.meas_flu(jac_case["phi"]).cpu().numpy(), jac_case["gfc"], None, nt)
+    assert rel(dtg.cpu().numpy(), d0) < 1e-12
+    assert rel(np.transpose(Jr.cpu().numpy(), (2, 1, 0)), J0 / d0[:, :, None]) < 1e-5
+
+
+def test_vjp_matches_explicit_jacobian_nodal(jac_case):
+    import torch
+    from dogpup_b200 import api
+    mesh = jac_case["mesh"]
+    nb = mesh.nodal_basis()
+    nt = len(mesh.optode.tAxis)
+    link = mesh._link()
+    Jt = api.jacobian_tg(nb, jac_case["phi"], jac_case["phiA"], mesh.optode.s_fpsf, link, jac_case["gfc_d"], nt)
+    rng = np.random.default_rng(0)
+    g = rng.standard_normal((link.shape[0], 20))
+    v = api.jacobian_tg_vjp(nb, jac_case["phi"], jac_case["phiA"], mesh.optode.s_fpsf, link, jac_case["gfc_d"], nt,
+                            torch.as_tensor(g))
+    explicit = np.einsum("vgm,mg->v", Jt.cpu().numpy().astype(np.float64), g)
+    assert rel(v.cpu().numpy(), explicit) < 1e-5
+    # nodal basis = the identity interpolation with lumped-mass weights
+    lump = nb.w.cpu().numpy()
+    import scipy.sparse as sp
+    from oracle.jacobian import j_tg
+    J0 = j_tg(_oracle_J(jac_case, sp.identity(mesh.nn, format="csr"), lump), jac_case["gfc"], nt)
+    assert rel(np.transpose(Jt.cpu().numpy(), (2, 1, 0)), J0) < 1e-5

@@ -1,0 +1,91 @@
+"""GPU J^T W J (split-BF16 tcgen05), damping, J^T W y and the FP64 Cholesky solve.
+
+Tolerances: H from the three-term BF16 split with FP32 accumulation, 3e-5
+norm-wise relative; J^T W y (FP64) 1e-12; the Cholesky solve on an exact
+FP64 matrix 1e-10; the whole LM step against the all-FP64 oracle
+(tik_inv with W), 1e-3.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _v(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def _case(nv, nm, seed):
+    rng = np.random.default_rng(seed)
+    J = rng.standard_normal((nm, nv)) * np.exp(rng.uniform(-2, 2, nv))[None, :]
+    W = rng.uniform(0.5, 2.0, nm)
+    y = rng.standard_normal(nm)
+    return J, W, y
+
+
+@pytest.mark.parametrize("nv,nm", [(300, 1000), (128, 64), (257, 777)])
+def test_normal_equations_match_fp64(nv, nm):
+    import torch
+    from dogpup_b200._lib import lib, check
+    J, W, y = _case(nv, nm, nv + nm)
+    Jt = torch.as_tensor(np.ascontiguousarray(J.T), dtype=torch.float32, device="cuda")
+    Jf = Jt.cpu().numpy().T.astype(np.float64)          # the FP32 values actually used
+    Wd = torch.as_tensor(W, device="cuda")
+    yd = torch.as_tensor(y, device="cuda")
+    H = torch.zeros((nv, nv), dtype=torch.float64, device="cuda")
+    rhs = torch.zeros(nv, dtype=torch.float64, device="cuda")
+    lam = 0.1
+    check(lib.dgp_normal_eq(_v(Jt), nv, nm, _v(Wd), _v(yd), lam, 0, _v(H), nv, _v(rhs), None))
+    H0 = Jf.T @ (W[:, None] * Jf)
+    d = np.diag(H0).copy()
+    H0[np.diag_indices(nv)] = d + lam * d.max()
+    Hl = np.tril(H.cpu().numpy())
+    err = np.linalg.norm(Hl - np.tril(H0)) / np.linalg.norm(np.tril(H0))
+    assert err < 3e-5, err
+    r0 = Jf.T @ (W * y)
+    assert np.linalg.norm(rhs.cpu().numpy() - r0) / np.linalg.norm(r0) < 1e-12
+
+
+def test_cholesky_solve_exact_matrix():
+    import torch
+    from dogpup_b200._lib import lib, check
+    rng = np.random.default_rng(3)
+    n = 333
+    A = rng.standard_normal((n, n))
+    H0 = A @ A.T + n * np.eye(n)
+    b = rng.standard_normal(n)
+    H = torch.as_tensor(np.tril(H0), device="cuda").contiguous()
+    x = torch.as_tensor(b, device="cuda").clone()
+    check(lib.dgp_cholesky_solve(_v(H), n, n, _v(x), None))
+    x0 = np.linalg.solve(H0, b)
+    assert np.linalg.norm(x.cpu().numpy() - x0) / np.linalg.norm(x0) < 1e-10
+    L = np.tril(H.cpu().numpy())
+    assert np.linalg.norm(L @ L.T - H0) / np.linalg.norm(H0) < 1e-13
+
+
+def test_cholesky_rejects_indefinite_matrix():
+    import torch
+    from dogpup_b200._lib import lib
+    n = 70
+    H = torch.as_tensor(-np.eye(n), device="cuda").contiguous()
+    x = torch.ones(n, dtype=torch.float64, device="cuda")
+    assert lib.dgp_cholesky_solve(_v(H), n, n, _v(x), None) == 1
+
+
+def test_lm_step_against_fp64_tik_inv():
+    import torch
+    from dogpup_b200._lib import lib, check
+    from oracle.jacobian import tik_inv
+    nv, nm = 400, 2048
+    J, W, y = _case(nv, nm, 7)
+    Jt = torch.as_tensor(np.ascontiguousarray(J.T), dtype=torch.float32, device="cuda")
+    H = torch.zeros((nv, nv), dtype=torch.float64, device="cuda")
+    x = torch.zeros(nv, dtype=torch.float64, device="cuda")
+    lam = 1e-2
+    check(lib.dgp_normal_eq(_v(Jt), nv, nm, _v(torch.as_tensor(W, device="cuda")),
+                            _v(torch.as_tensor(y, device="cuda")), lam, 0, _v(H), nv, _v(x), None))
+    check(lib.dgp_cholesky_solve(_v(H), nv, nv, _v(x), None))
+    u0 = tik_inv(Jt.cpu().numpy().T.astype(np.float64), lam, y, weights=W)
+    assert np.linalg.norm(x.cpu().numpy() - u0) / np.linalg.norm(u0) < 1e-3
