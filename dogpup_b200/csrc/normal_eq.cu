@@ -249,6 +249,11 @@ __global__ void k_split(const float *__restrict__ Jt, const double *__restrict__
   lo[t] = __float2bfloat16_rn(x - __bfloat162float(h));
 }
 
+__global__ void k_check_weights(const double *__restrict__ W, int64_t nm, int *err) {
+  int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (m < nm && !(W[m] >= 0.0 && isfinite(W[m]))) atomicOr(err, 16);
+}
+
 __global__ void k_row_dots(const float *__restrict__ Jt, const double *__restrict__ W, const double *__restrict__ y,
                            int64_t nv, int64_t nm, double *diag, double *rhs) {
   __shared__ double sd[256], sr[256];
@@ -473,6 +478,14 @@ int normal_eq_run(const float *Jt, int64_t nv, int64_t nm, const double *W, cons
   DGP_TRY(diag.alloc(sizeof(double) * nv));
   DGP_TRY(errb.alloc(sizeof(int)));
   DGP_CUDA(cudaMemsetAsync(errb.p, 0, sizeof(int), st));
+  if (W) {
+    k_check_weights<<<(unsigned)ceil_div(nm, 256), 256, 0, st>>>(W, nm, errb.as<int>());
+    DGP_CHECK_LAUNCH();
+    int werr = 0;
+    DGP_CUDA(cudaMemcpyAsync(&werr, errb.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    DGP_CUDA(cudaStreamSynchronize(st));
+    if (werr) return fail(DGP_ERR_ARG, "normal_eq: data weights must be finite and non-negative");
+  }
   k_split<<<(unsigned)ceil_div(nvp * nmp, 256), 256, 0, st>>>(Jt, W, nv, nm, nvp, nmp, hi.as<__nv_bfloat16>(),
                                                                lo.as<__nv_bfloat16>());
   DGP_CHECK_LAUNCH();

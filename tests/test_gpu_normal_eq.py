@@ -83,9 +83,10 @@ def test_lm_step_against_fp64_tik_inv():
     Jt = torch.as_tensor(np.ascontiguousarray(J.T), dtype=torch.float32, device="cuda")
     H = torch.zeros((nv, nv), dtype=torch.float64, device="cuda")
     x = torch.zeros(nv, dtype=torch.float64, device="cuda")
+    Wd = torch.as_tensor(W, device="cuda")   # kept alive: the library reads these pointers
+    yd = torch.as_tensor(y, device="cuda")
     lam = 1e-2
-    check(lib.dgp_normal_eq(_v(Jt), nv, nm, _v(torch.as_tensor(W, device="cuda")),
-                            _v(torch.as_tensor(y, device="cuda")), lam, 0, _v(H), nv, _v(x), None))
+    check(lib.dgp_normal_eq(_v(Jt), nv, nm, _v(Wd), _v(yd), lam, 0, _v(H), nv, _v(x), None))
     check(lib.dgp_cholesky_solve(_v(H), nv, nv, _v(x), None))
     u0 = tik_inv(Jt.cpu().numpy().T.astype(np.float64), lam, y, weights=W)
     assert np.linalg.norm(x.cpu().numpy() - u0) / np.linalg.norm(u0) < 1e-3
