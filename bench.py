@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--inner-tol", type=float, default=1e-4)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true", help="skip the TG Jacobian / LM / plain-FP64 timings")
     return ap.parse_args()
 
 
@@ -146,6 +147,126 @@ def cpu_sample(w, harmonics=(1, 64), ns=8, tol=1e-8):
                       f"{len(w['src']) * w['nf']} RHS", "seconds": t_asm + t_solve}
 
 
+# ------------------------------------------------------- secondary metrics
+def _gates(t, n, width, start, spacing):
+    sd = width / (2 * np.sqrt(2 * np.log(2)))
+    return np.stack([np.exp(-(t - (start + q * spacing)) ** 2 / (2 * sd ** 2)) for q in range(n)])
+
+
+def _event_ms(fn, reps):
+    import torch
+    st = torch.cuda.current_stream()
+    fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(reps):
+        fn()
+    e1.record(st)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def tg_jacobian_bench(reps=3):
+    """Time-gated Jacobian of the 100k-node configuration: ellipsoid, 32 sources x 32 detectors,
+    64 harmonics, 20 gates of 250 ps, nodal basis (J^T is [nodes][20 x 1024] FP32), and its vjp."""
+    import torch
+    from dogpup_b200 import api, workloads
+    w = workloads.ellipsoid_fwd(seed=3, h=1.38, ns=32, nd=32, nf=64)
+    mesh = workloads.build_dmesh(w)
+    t0 = time.perf_counter()
+    phi, _ = mesh.flu_solve(precision="mixed", tol=1e-8)
+    phiA = mesh.adj_flu_solve(precision="mixed", tol=1e-8)
+    torch.cuda.synchronize()
+    t_solve = time.perf_counter() - t0
+    gfc = api.td2fc(torch.as_tensor(_gates(w["t"], 20, 250e-12, 0.5e-9, 250e-12), device="cuda"),
+                    torch.as_tensor(mesh.optode.fAxis), torch.as_tensor(w["t"]))
+    nb = mesh.nodal_basis()
+    link = mesh._link()
+    nt = len(w["t"])
+    fpsf = mesh.optode.s_fpsf
+    out = {}
+    ms = _event_ms(lambda: out.__setitem__("J", api.jacobian_tg(nb, phi, phiA, fpsf, link, gfc, nt)), reps)
+    g = torch.as_tensor(np.random.default_rng(5).standard_normal((link.shape[0], 20)), device="cuda")
+    ms_vjp = _event_ms(lambda: api.jacobian_tg_vjp(nb, phi, phiA, fpsf, link, gfc, nt, g), reps)
+    nv, nm, nf = mesh.nn, int(link.shape[0]), w["nf"]
+    field_bytes = 16.0 * nf * nv * (len(w["src"]) + len(w["det"]))
+    j_bytes = 4.0 * nv * 20 * nm
+    flops = 2.0 * nv * nm * nf * (2 + 2 * 20)
+    del out
+    return {"workload": f"ellipsoid 90x75x70 @1.38mm, {nv} nodes, 32x32 optodes, 64 harmonics, 20 gates",
+            "J_shape": [20 * nm, nv], "ms": round(ms, 3), "vjp_ms": round(ms_vjp, 3),
+            "forward_and_adjoint_solve_s": round(t_solve, 2),
+            "achieved_gbs": round((field_bytes + j_bytes) / (ms * 1e-3) / 1e9, 1),
+            "achieved_tflops_fp32": round(flops / (ms * 1e-3) / 1e12, 2)}
+
+
+def lm_step_bench(reps=2):
+    """Weighted LM normal-equation step of the 50k-node configuration: cylinder r30 h60 @1.5 mm,
+    32 x 32 optodes, 10 gates (10240 measurements), J on the in-mesh voxels of a 2 mm grid."""
+    import ctypes as C
+    import torch
+    from dogpup_b200 import api, workloads
+    from dogpup_b200._lib import lib, check
+    w = workloads.cylinder_fwd(seed=4, ns=32, nd=32, nf=32)
+    mesh = workloads.build_dmesh(w)
+    lo, hi = w["mesh"].node.min(0), w["mesh"].node.max(0)
+    mesh.mesh2grid(*[np.arange(lo[d], hi[d] + 1e-9, 2.0) for d in range(3)])
+    P = mesh.m2g[mesh.gridinmesh]
+    basis = api.Basis(P, np.full(P.shape[0], mesh.dxyz ** 3))
+    phi, data = mesh.flu_solve(precision="mixed", tol=1e-8)
+    phiA = mesh.adj_flu_solve(precision="mixed", tol=1e-8)
+    nt = len(w["t"])
+    gfc = api.td2fc(torch.as_tensor(_gates(w["t"], 10, 500e-12, 0.5e-9, 500e-12), device="cuda"),
+                    torch.as_tensor(mesh.optode.fAxis), torch.as_tensor(w["t"]))
+    data_tg = api.fc2tg(data, gfc, nt)
+    J = api.jacobian_tg(basis, phi, phiA, mesh.optode.s_fpsf, mesh._link(), gfc, nt, data_tg)  # Rytov
+    nv, nmeas = J.shape[0], J.shape[1] * J.shape[2]
+    Jt = J.reshape(nv, nmeas).contiguous()
+    rng = np.random.default_rng(9)
+    W = torch.as_tensor(1.0 / (0.01 * (1 + rng.random(nmeas))) ** 2, device="cuda")
+    y = torch.as_tensor(rng.standard_normal(nmeas) * 0.01, device="cuda")
+    H = torch.empty((nv, nv), dtype=torch.float64, device="cuda")
+    x = torch.empty(nv, dtype=torch.float64, device="cuda")
+    v = lambda t: C.c_void_p(t.data_ptr())
+    ms_ne = _event_ms(lambda: check(lib.dgp_normal_eq(v(Jt), nv, nmeas, v(W), v(y), 1e-2, 0, v(H), nv, v(x),
+                                                      api.stream_ptr())), reps)
+    Hc = H.clone()
+    xc = x.clone()
+
+    def chol():
+        Hc.copy_(H)
+        xc.copy_(x)
+        check(lib.dgp_cholesky_solve(v(Hc), nv, nv, v(xc), api.stream_ptr()))
+    ms_chol = _event_ms(chol, reps)
+    syrk_flops = 3 * 2.0 * nmeas * nv * (nv + 128) / 2
+    return {"workload": f"cylinder r30 h60 @1.5mm, {mesh.nn} nodes, 32x32 optodes, 10 gates, {nv} voxels (2 mm)",
+            "nmeas": nmeas, "nv": nv, "normal_eq_ms": round(ms_ne, 3), "cholesky_solve_ms": round(ms_chol, 3),
+            "syrk_tflops_bf16_lower_bound": round(syrk_flops / (ms_ne * 1e-3) / 1e12, 1),
+            "cholesky_tflops_fp64": round(nv ** 3 / 3 / (ms_chol * 1e-3) / 1e12, 2)}
+
+
+def plain_fp64_per_rhs(w, mesh, nh=8):
+    """The plain baseline of the path: FP64 BiCGSTAB (reference arithmetic) on one right-hand side per
+    harmonic, through the same library, on the bench mesh; solves/s over a sample of harmonics."""
+    import torch
+    from dogpup_b200 import api
+    nodes, wts = mesh._sources(mesh.optode.s_bary[:1])
+    o = mesh.optode
+    S = api.Solver(mesh.fem.rowptr, mesh.fem.col, mesh.K, mesh.M, o.df / mesh.c, nh, 1)
+    fpsf = o.s_fpsf[:nh].contiguous()
+    opts = api.make_opts(tol=1e-8, maxit=1000, precision="fp64")
+    S.solve_sources(nodes, wts, fpsf, opts)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _, rep = S.solve_sources(nodes, wts, fpsf, opts)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    del S
+    return {"value": nh / dt, "unit": "src.freq solves/s", "iterations": rep.iterations,
+            "sample": f"1 source x harmonics 0..{nh - 1}, FP64 to 1e-8, one RHS per harmonic"}
+
+
 # --------------------------------------------------------------- our arm
 def run_ours(a, rank, world, local_rank):
     import torch
@@ -174,6 +295,8 @@ def run_ours(a, rank, world, local_rank):
         dist.barrier()
     torch.cuda.synchronize()
     clk = Clocks(torch.cuda.current_device()) if rank == 0 else None
+    from dogpup_b200._lib import lib as _dlib
+    n_launch0 = _dlib.dgp_kernel_launches()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(st)
     for _ in range(a.steps):
@@ -181,6 +304,7 @@ def run_ours(a, rank, world, local_rank):
     e1.record(st)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
+    launches = _dlib.dgp_kernel_launches() - n_launch0
     clocks = clk.stop() if clk else None
     if world > 1:
         t = torch.tensor([ms], device="cuda")
@@ -225,7 +349,7 @@ def run_ours(a, rank, world, local_rank):
     # ---- roofline: the dominant sweep kernel, CUDA-event timed on the solver's stream
     launches = {0: 2, 1: 5, 2: 1, 3: 1}  # per BiCGSTAB iteration: A SpMM x2, G SpMM x5, x/r/p, h/s
     names = {0: "k_spmm_A<float> (K + i w M SpMM)", 1: "k_spmm_G<float> (FSAI apply)",
-             2: "k_update_xrp<float>", 3: "k_update_hs<float>"}
+             2: "k_update_xrp<float>", 3: "k_update_s<float>"}
     prof = {q: solver.profile_kernel(q, 5) for q in launches}
     dom = max(prof, key=lambda q: prof[q][0] * launches[q])
     pk = json.load(open(ROOT / "MEASURED_PEAKS.json")) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
@@ -235,7 +359,15 @@ def run_ours(a, rank, world, local_rank):
             "frac": round(ach / peak, 4), "traffic": None, "peak_source": "measured" if pk else "fallback",
             "per_kernel_ms": {names[q]: round(prof[q][0], 3) for q in prof},
             "per_kernel_gbs": {names[q]: round(prof[q][1] / (prof[q][0] * 1e-3) / 1e9, 1) for q in prof}}
-    res.update(ms_per_step=ms_step, value=value, e2e=e2e, rep=rep, clocks=clocks, roof=roof, mesh=mesh, w=w)
+    res.update(ms_per_step=ms_step, value=value, e2e=e2e, rep=rep, clocks=clocks, roof=roof, mesh=mesh, w=w,
+               launches=launches)
+    if rank == 0 and not a.no_secondary:
+        res["plain"] = plain_fp64_per_rhs(w, mesh)
+        log(f"[rank 0] plain FP64 per-RHS: {res['plain']}")
+        res["tg"] = tg_jacobian_bench()
+        log(f"[rank 0] TG Jacobian: {res['tg']}")
+        res["lm"] = lm_step_bench()
+        log(f"[rank 0] LM step: {res['lm']}")
     return res
 
 
@@ -291,7 +423,8 @@ def main():
                        "max_rel_residual": rep.max_rel_residual, "l2": "inputs larger than L2 (vectors ~GB)",
                        "parallelism": f"replicas x{world}"},
             "e2e": r["e2e"], "roofline": r["roof"], "cpu_baseline": cpu, "clocks": r["clocks"],
-            "gpu_launches": None,
+            "gpu_launches": r["launches"],
+            "plain_fp64_per_rhs": r.get("plain"), "tg_jacobian": r.get("tg"), "lm_step": r.get("lm"),
         }
         print(json.dumps(line))
     if world > 1:

@@ -37,6 +37,7 @@ _SIGS = {
     "dgp_last_error": (C.c_char_p, []),
     "dgp_status_string": (C.c_char_p, [C.c_int]),
     "dgp_version": (C.c_int, []),
+    "dgp_kernel_launches": (I64, []),
     "dgp_smv_mex": (C.c_int, [P, P, P, P, P, P, P, P, P, C.c_int, C.c_int, C.c_int, P]),
     "dgp_fsaimv_mex": (C.c_int, [P, P, P, P, P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, P]),
     "dgp_fsaip_mex": (C.c_int, [P, P, P, P, P, P, P, P, C.c_int, C.c_int, P]),

@@ -4,23 +4,26 @@
 // reference runs the iteration from MATLAB: 7 mex mat-vec calls per
 // iteration, each re-copying A, x and the index arrays to fresh device
 // arrays, about 20 gpuArray BLAS-1 launches and 4 device-wide waits.  Here
-// one iteration is 10 sweep kernels + 4 single-block scalar kernels,
+// one iteration is 10 sweep kernels + 5 single-block scalar kernels,
 // captured once in a CUDA graph and replayed; convergence is decided on the
 // device (FP64 dot products and norms) and polled by the host every
 // `check_every` iterations.
 //
-// Arithmetic follows the reference exactly: bilinear (unconjugated) dots
-// r^0.v, r^0.r and (G t).(G s), (G t).(G t); alph = (v.r^0)/rho0 (here its
-// reciprocal alpha = rho0/(v.r^0) is stored and multiplied); omega in the
-// G-weighted bilinear form; stop when the maximum over all columns of
-// ||s||/||r0|| or ||r||/||r0|| is below tol; x = h on the early exit.
+// Arithmetic follows the reference: bilinear (unconjugated) dots r^0.v,
+// r^0.r and (G t).(G s), (G t).(G t); alph = (v.r^0)/rho0 (its reciprocal
+// alpha = rho0/(v.r^0) is stored and multiplied); omega in the G-weighted
+// bilinear form; stop when the maximum over all columns of ||s||/||r0|| or
+// ||r||/||r0|| is below tol; x = x + alpha h on the early exit.  The update
+// h = x + alpha h of dMesh.m:1305 is folded into the x update
+// (x = x + alpha h + omega z), which saves three vector passes.
 //
 // Layout of every vector: [NF][NN][NSP] complex (harmonic, node, source),
 // NSP = sources padded to a power of two.  A tile of the SpMM is one
-// harmonic x a block of rows; each lane carries 2 consecutive sources, so one
-// row of one harmonic is a contiguous 16-byte (FP32) / 32-byte (FP64)
-// segment per lane and a whole row is one coalesced load per warp.  K and M
-// are read once per row block and combined on the fly into K + i*omega_k*M.
+// harmonic x a block of rows; each lane carries VEC consecutive sources, so a
+// row of one harmonic is one coalesced load per warp.  In the FP32 path each
+// nonzero is one 16-byte record (column, K, M) for A -- combined on the fly
+// into K + i w_k M -- or (column, Re G_k, Im G_k) for the FSAI factors, so a
+// nonzero costs one broadcast load besides its x gather.
 //
 // Mixed precision (DGP_PREC_MIXED): the BiCGSTAB runs in complex FP32 on the
 // current FP64 residual; the FP64 solution is updated and the FP64 residual
@@ -42,6 +45,7 @@ namespace {
 
 constexpr int BS = 256;
 constexpr int WARPS = BS / 32;
+constexpr int KERNELS_PER_ITER = 15;
 
 enum { ST_RUNNING = 0, ST_FINAL = 1, ST_DONE = 2 };
 enum { ACC_D1 = 0, ACC_NS = 1, ACC_D2 = 2, ACC_D3 = 3, ACC_NR = 4, ACC_RHO = 5, NACC = 6 };
@@ -63,51 +67,63 @@ struct Cols {
   double *err;      // last relative residual
   double2 *rho0, *alpha, *omega, *beta;
   double2 *acc;     // [NACC][C]
-  int *active;      // column still iterating
+  int *active;      // 1 iterating, 2 converged at s this iteration, 0 frozen
   int *status;      // DGP_COL_*
 };
 
 struct Layout {
   int64_t n;
   int nf, nsp;
-  int lpr;  // lanes per row chunk (power of two <= 32)
-  int nch;  // chunks per row
+  int lpr;  // lanes per row (power of two <= 32)
   int rpw;  // rows per warp step
   int ipb;  // warp steps per block
   __host__ __device__ int64_t rows_per_block() const { return (int64_t)WARPS * rpw * ipb; }
 };
 
-Layout make_layout(int64_t n, int nf, int nsp, int ipb) {
-  Layout L;
-  L.n = n; L.nf = nf; L.nsp = nsp;
-  int lanes = nsp / 2;
-  if (lanes <= 32) { L.lpr = lanes; L.nch = 1; } else { L.lpr = 32; L.nch = lanes / 32; }
-  L.rpw = 32 / L.lpr;
-  L.ipb = ipb;
-  return L;
-}
+// 16-byte record per nonzero of the FP32 path: A -> (col, K, M), G -> (col, Re, Im)
+struct __align__(16) Rec32 {
+  int col;
+  float a, b, pad;
+};
 
 // ------------------------------------------------------------ vector I/O
 template <class R> struct CT;
-template <> struct CT<float> { using C = float2; using KM = float2; };
-template <> struct CT<double> { using C = double2; using KM = double2; };
+template <> struct CT<float> { using C = float2; };
+template <> struct CT<double> { using C = double2; };
 
-__device__ inline void ld2(const float2 *p, float2 c[2]) {
-  float4 v = *reinterpret_cast<const float4 *>(p);
-  c[0] = make_float2(v.x, v.y);
-  c[1] = make_float2(v.z, v.w);
+template <int VEC> __device__ inline void ldv(const float2 *p, float2 (&c)[VEC]) {
+#pragma unroll
+  for (int q = 0; q < VEC; q += 2) {
+    float4 v = *reinterpret_cast<const float4 *>(p + q);
+    c[q] = make_float2(v.x, v.y);
+    c[q + 1] = make_float2(v.z, v.w);
+  }
 }
-__device__ inline void ld2(const double2 *p, double2 c[2]) { c[0] = p[0]; c[1] = p[1]; }
-__device__ inline void ldg2(const float2 *p, float2 c[2]) {
-  float4 v = __ldg(reinterpret_cast<const float4 *>(p));
-  c[0] = make_float2(v.x, v.y);
-  c[1] = make_float2(v.z, v.w);
+template <int VEC> __device__ inline void ldv(const double2 *p, double2 (&c)[VEC]) {
+#pragma unroll
+  for (int q = 0; q < VEC; ++q) c[q] = p[q];
 }
-__device__ inline void ldg2(const double2 *p, double2 c[2]) { c[0] = __ldg(p); c[1] = __ldg(p + 1); }
-__device__ inline void st2(float2 *p, const float2 c[2]) {
-  *reinterpret_cast<float4 *>(p) = make_float4(c[0].x, c[0].y, c[1].x, c[1].y);
+template <int VEC> __device__ inline void ldgv(const float2 *p, float2 (&c)[VEC]) {
+#pragma unroll
+  for (int q = 0; q < VEC; q += 2) {
+    float4 v = __ldg(reinterpret_cast<const float4 *>(p + q));
+    c[q] = make_float2(v.x, v.y);
+    c[q + 1] = make_float2(v.z, v.w);
+  }
 }
-__device__ inline void st2(double2 *p, const double2 c[2]) { p[0] = c[0]; p[1] = c[1]; }
+template <int VEC> __device__ inline void ldgv(const double2 *p, double2 (&c)[VEC]) {
+#pragma unroll
+  for (int q = 0; q < VEC; ++q) c[q] = __ldg(p + q);
+}
+template <int VEC> __device__ inline void stv(float2 *p, const float2 (&c)[VEC]) {
+#pragma unroll
+  for (int q = 0; q < VEC; q += 2)
+    *reinterpret_cast<float4 *>(p + q) = make_float4(c[q].x, c[q].y, c[q + 1].x, c[q + 1].y);
+}
+template <int VEC> __device__ inline void stv(double2 *p, const double2 (&c)[VEC]) {
+#pragma unroll
+  for (int q = 0; q < VEC; ++q) p[q] = c[q];
+}
 
 template <class C> __device__ inline C czero();
 template <> __device__ inline float2 czero<float2>() { return make_float2(0.f, 0.f); }
@@ -115,6 +131,8 @@ template <> __device__ inline double2 czero<double2>() { return make_double2(0.0
 
 __device__ inline float2 cfmaT(float2 b, float2 c, float2 a) { return cfmaf(b, c, a); }
 __device__ inline double2 cfmaT(double2 b, double2 c, double2 a) { return cfma(b, c, a); }
+__device__ inline float2 cneg(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ inline double2 cneg(double2 a) { return make_double2(-a.x, -a.y); }
 
 template <class R> __device__ inline typename CT<R>::C cvt(double2 a);
 template <> __device__ inline float2 cvt<float>(double2 a) { return make_float2((float)a.x, (float)a.y); }
@@ -135,52 +153,49 @@ template <class C> __device__ inline void acc_abs2(double &s, C a) {
 
 // ------------------------------------------------------------ lane mapping
 struct Lane {
-  int warp, lane, sub, rsub;
-  int64_t row0;  // first row of this block
-  int k;
+  int warp, sub, rsub, k;
+  int64_t row0;
   __device__ Lane(const Layout &L) {
     warp = threadIdx.x >> 5;
-    lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31;
     sub = lane % L.lpr;
     rsub = lane / L.lpr;
     row0 = (int64_t)blockIdx.x * L.rows_per_block();
     k = blockIdx.y;
   }
-  __device__ int64_t row(const Layout &L, int it) const {
-    return row0 + ((int64_t)it * WARPS + warp) * L.rpw + rsub;
-  }
-  __device__ int s0(const Layout &L, int ch) const { return (ch * L.lpr + sub) * 2; }
+  __device__ int64_t row(const Layout &L, int it) const { return row0 + ((int64_t)it * WARPS + warp) * L.rpw + rsub; }
 };
 
 __device__ inline int64_t vidx(const Layout &L, int k, int64_t i, int s) {
   return ((int64_t)k * L.n + i) * L.nsp + s;
 }
 
-// Block reduction of per-lane column partials into acc[q][k*nsp + s] (FP64 atomics).
-// part[ch][v] holds NQ values (complex accumulators as double2; real ones use .x).
-template <int NQ>
-__device__ inline void block_reduce(const Layout &L, const Lane &ln, double2 (&part)[2][2][NQ], double2 *acc,
+// Block reduction of per-lane column partials into acc[slot[q]][k*nsp + s] (FP64 atomics).
+template <int VEC, int NQ>
+__device__ inline void block_reduce(const Layout &L, const Lane &ln, double2 (&part)[VEC][NQ], double2 *acc,
                                     int64_t C, const int (&slot)[NQ], double2 *sm /*[WARPS][nsp][NQ]*/) {
-  for (int ch = 0; ch < L.nch; ++ch)
-    for (int v = 0; v < 2; ++v)
-      for (int q = 0; q < NQ; ++q) {
-        double2 x = part[ch][v][q];
-        for (int off = L.lpr; off < 32; off <<= 1) {
-          x.x += __shfl_xor_sync(0xffffffffu, x.x, off);
-          x.y += __shfl_xor_sync(0xffffffffu, x.y, off);
-        }
-        part[ch][v][q] = x;
+#pragma unroll
+  for (int v = 0; v < VEC; ++v)
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      double2 x = part[v][q];
+      for (int off = L.lpr; off < 32; off <<= 1) {
+        x.x += __shfl_xor_sync(0xffffffffu, x.x, off);
+        x.y += __shfl_xor_sync(0xffffffffu, x.y, off);
       }
+      part[v][q] = x;
+    }
   if (ln.rsub == 0) {
-    for (int ch = 0; ch < L.nch; ++ch)
-      for (int v = 0; v < 2; ++v) {
-        int s = ln.s0(L, ch) + v;
-        for (int q = 0; q < NQ; ++q) sm[((int64_t)ln.warp * L.nsp + s) * NQ + q] = part[ch][v][q];
-      }
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) {
+      const int s = ln.sub * VEC + v;
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) sm[((int64_t)ln.warp * L.nsp + s) * NQ + q] = part[v][q];
+    }
   }
   __syncthreads();
   for (int t = threadIdx.x; t < L.nsp * NQ; t += blockDim.x) {
-    int s = t / NQ, q = t % NQ;
+    const int s = t / NQ, q = t % NQ;
     double2 x = make_double2(0.0, 0.0);
     for (int w = 0; w < WARPS; ++w) {
       double2 y = sm[((int64_t)w * L.nsp + s) * NQ + q];
@@ -193,41 +208,91 @@ __device__ inline void block_reduce(const Layout &L, const Lane &ln, double2 (&p
   }
 }
 
-// ------------------------------------------------------------- SpMM row
-template <class R> struct CoefA {
-  const typename CT<R>::KM *KM;
-  R om;
-  __device__ typename CT<R>::C get(int p) const {
-    auto km = __ldg(KM + p);
-    return mk((R)km.x, (R)(om * km.y));
+// -------------------------------------------------- coefficient policies
+struct CoefA32 {  // K + i w_k M from one record
+  const Rec32 *rec;
+  float om;
+  __device__ inline void get(int p, int &j, float2 &c) const {
+    int4 r = __ldg(reinterpret_cast<const int4 *>(rec + p));
+    j = r.x;
+    c = make_float2(__int_as_float(r.y), om * __int_as_float(r.z));
   }
 };
-template <class R> struct CoefG {
-  const typename CT<R>::C *G;
-  __device__ typename CT<R>::C get(int p) const { return __ldg(G + p); }
+struct CoefG32 {  // G_k (or G_k^T) from one record
+  const Rec32 *rec;
+  __device__ inline void get(int p, int &j, float2 &c) const {
+    int4 r = __ldg(reinterpret_cast<const int4 *>(rec + p));
+    j = r.x;
+    c = make_float2(__int_as_float(r.y), __int_as_float(r.z));
+  }
+};
+struct CoefA64 {
+  const int32_t *col;
+  const double2 *KM;
+  double om;
+  __device__ inline void get(int p, int &j, double2 &c) const {
+    j = __ldg(col + p);
+    double2 km = __ldg(KM + p);
+    c = make_double2(km.x, om * km.y);
+  }
+};
+struct CoefG64 {
+  const int32_t *col;
+  const double2 *G;
+  __device__ inline void get(int p, int &j, double2 &c) const {
+    j = __ldg(col + p);
+    c = __ldg(G + p);
+  }
 };
 
-// y[0..1] = sum_p coef(p) * X[k][col[p]][s0 .. s0+1]
-template <class R, class Coef>
-__device__ inline void row_spmv(const Layout &L, int k, int64_t i, int s0, const int32_t *__restrict__ rowptr,
-                                const int32_t *__restrict__ col, const Coef &cf,
-                                const typename CT<R>::C *__restrict__ X, typename CT<R>::C y[2]) {
-  using C = typename CT<R>::C;
-  y[0] = czero<C>();
-  y[1] = czero<C>();
-  int b = __ldg(rowptr + i), e = __ldg(rowptr + i + 1);
-  const C *Xk = X + (int64_t)k * L.n * L.nsp + s0;
+// Operator descriptor handed to the SpMM kernel; make(k) gives harmonic k's coefficients.
+struct OpA32 {
+  const int32_t *rowptr;
+  const Rec32 *rec;
+  const float *omega;
+  __device__ CoefA32 make(int k) const { return CoefA32{rec, omega[k]}; }
+};
+struct OpG32 {
+  const int32_t *rowptr;
+  const Rec32 *rec;
+  int64_t nnz;
+  __device__ CoefG32 make(int k) const { return CoefG32{rec + (int64_t)k * nnz}; }
+};
+struct OpA64 {
+  const int32_t *rowptr, *col;
+  const double2 *KM;
+  const double *omega;
+  __device__ CoefA64 make(int k) const { return CoefA64{col, KM, omega[k]}; }
+};
+struct OpG64 {
+  const int32_t *rowptr, *col;
+  const double2 *G;
+  int64_t nnz;
+  __device__ CoefG64 make(int k) const { return CoefG64{col, G + (int64_t)k * nnz}; }
+};
+
+// y[0..VEC) = sum_p coef(p) * Xk[col(p)*nsp + s0 ..]   (32-bit offsets inside one harmonic plane)
+template <int VEC, class C, class Coef>
+__device__ inline void row_spmv(int nsp, const int32_t *__restrict__ rowptr, int64_t i, const Coef &cf,
+                                const C *__restrict__ Xk, C (&y)[VEC]) {
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) y[v] = czero<C>();
+  const int b = __ldg(rowptr + i), e = __ldg(rowptr + i + 1);
   int p = b;
   for (; p + 4 <= e; p += 4) {
-    int j0 = __ldg(col + p), j1 = __ldg(col + p + 1), j2 = __ldg(col + p + 2), j3 = __ldg(col + p + 3);
-    C a0 = cf.get(p), a1 = cf.get(p + 1), a2 = cf.get(p + 2), a3 = cf.get(p + 3);
-    C x0[2], x1[2], x2[2], x3[2];
-    ldg2(Xk + (int64_t)j0 * L.nsp, x0);
-    ldg2(Xk + (int64_t)j1 * L.nsp, x1);
-    ldg2(Xk + (int64_t)j2 * L.nsp, x2);
-    ldg2(Xk + (int64_t)j3 * L.nsp, x3);
+    int j0, j1, j2, j3;
+    C a0, a1, a2, a3;
+    cf.get(p, j0, a0);
+    cf.get(p + 1, j1, a1);
+    cf.get(p + 2, j2, a2);
+    cf.get(p + 3, j3, a3);
+    C x0[VEC], x1[VEC], x2[VEC], x3[VEC];
+    ldgv<VEC>(Xk + j0 * nsp, x0);
+    ldgv<VEC>(Xk + j1 * nsp, x1);
+    ldgv<VEC>(Xk + j2 * nsp, x2);
+    ldgv<VEC>(Xk + j3 * nsp, x3);
 #pragma unroll
-    for (int v = 0; v < 2; ++v) {
+    for (int v = 0; v < VEC; ++v) {
       y[v] = cfmaT(a0, x0[v], y[v]);
       y[v] = cfmaT(a1, x1[v], y[v]);
       y[v] = cfmaT(a2, x2[v], y[v]);
@@ -235,12 +300,13 @@ __device__ inline void row_spmv(const Layout &L, int k, int64_t i, int s0, const
     }
   }
   for (; p < e; ++p) {
-    int j = __ldg(col + p);
-    C a = cf.get(p);
-    C x[2];
-    ldg2(Xk + (int64_t)j * L.nsp, x);
-    y[0] = cfmaT(a, x[0], y[0]);
-    y[1] = cfmaT(a, x[1], y[1]);
+    int j;
+    C a;
+    cf.get(p, j, a);
+    C x[VEC];
+    ldgv<VEC>(Xk + j * nsp, x);
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) y[v] = cfmaT(a, x[v], y[v]);
   }
 }
 
@@ -250,134 +316,99 @@ __device__ inline bool halted(const Ctl *ctl, int need) {
   return need == ST_RUNNING ? (s != ST_RUNNING) : (s == ST_DONE);
 }
 
-// Y = A_k X, optionally dot(Y, W) into acc[D1]
-template <class R, bool DOT>
-__global__ void __launch_bounds__(BS) k_spmm_A(Layout L, const int32_t *__restrict__ rowptr,
-                                               const int32_t *__restrict__ col,
-                                               const typename CT<R>::KM *__restrict__ KM,
-                                               const R *__restrict__ omega, const typename CT<R>::C *__restrict__ X,
-                                               typename CT<R>::C *__restrict__ Y,
-                                               const typename CT<R>::C *__restrict__ W, Cols cols, const Ctl *ctl,
-                                               int gate) {
+// Y = Op_k X.  MODE 0: store.  MODE 1: store, acc[D1] += Y.W.
+// MODE 2: no store, acc[D2] += Y.W, acc[D3] += Y.Y.
+template <class R, int VEC, int MODE, class Op>
+__global__ void __launch_bounds__(BS) k_spmm(Layout L, Op op, const typename CT<R>::C *__restrict__ X,
+                                             typename CT<R>::C *__restrict__ Y,
+                                             const typename CT<R>::C *__restrict__ W, Cols cols, const Ctl *ctl) {
   using C = typename CT<R>::C;
-  if (ctl && halted(ctl, gate)) return;
+  if (ctl && halted(ctl, ST_RUNNING)) return;
   extern __shared__ double2 smem[];
   Lane ln(L);
-  CoefA<R> cf{KM, omega[ln.k]};
-  double2 part[2][2][1] = {};
+  const auto cf = op.make(ln.k);
+  const int s0 = ln.sub * VEC;
+  const C *Xk = X + (int64_t)ln.k * L.n * L.nsp + s0;
+  constexpr int NQ = MODE == 2 ? 2 : 1;
+  double2 part[VEC][NQ];
+#pragma unroll
+  for (int v = 0; v < VEC; ++v)
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) part[v][q] = make_double2(0, 0);
   for (int it = 0; it < L.ipb; ++it) {
-    int64_t i = ln.row(L, it);
+    const int64_t i = ln.row(L, it);
     if (i >= L.n) break;
-    for (int ch = 0; ch < L.nch; ++ch) {
-      int s0 = ln.s0(L, ch);
-      C y[2];
-      row_spmv<R>(L, ln.k, i, s0, rowptr, col, cf, X, y);
-      int64_t o = vidx(L, ln.k, i, s0);
-      st2(Y + o, y);
-      if (DOT) {
-        C w[2];
-        ld2(W + o, w);
-        acc_bil(part[ch][0][0], y[0], w[0]);
-        acc_bil(part[ch][1][0], y[1], w[1]);
+    C y[VEC];
+    row_spmv<VEC>(L.nsp, op.rowptr, i, cf, Xk, y);
+    const int64_t o = vidx(L, ln.k, i, s0);
+    if (MODE != 2) stv<VEC>(Y + o, y);
+    if (MODE != 0) {
+      C w[VEC];
+      ldv<VEC>(W + o, w);
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) {
+        acc_bil(part[v][0], y[v], w[v]);
+        if (MODE == 2) acc_bil(part[v][NQ - 1], y[v], y[v]);
       }
     }
   }
-  if (DOT) {
+  if constexpr (MODE == 1) {
     const int slot[1] = {ACC_D1};
-    block_reduce<1>(L, ln, part, cols.acc, cols.C, slot, smem);
-  }
-}
-
-// Y = G_k X (lower pattern) or G_k^T X (transposed pattern + values).
-// MODE 0: store Y.  MODE 1: no store; acc[D2] += Y.W, acc[D3] += Y.Y.
-template <class R, int MODE>
-__global__ void __launch_bounds__(BS) k_spmm_G(Layout L, const int32_t *__restrict__ rowptr,
-                                               const int32_t *__restrict__ col,
-                                               const typename CT<R>::C *__restrict__ G, int64_t nnzG,
-                                               const typename CT<R>::C *__restrict__ X,
-                                               typename CT<R>::C *__restrict__ Y,
-                                               const typename CT<R>::C *__restrict__ W, Cols cols, const Ctl *ctl,
-                                               int gate) {
-  using C = typename CT<R>::C;
-  if (ctl && halted(ctl, gate)) return;
-  extern __shared__ double2 smem[];
-  Lane ln(L);
-  CoefG<R> cf{G + (int64_t)ln.k * nnzG};
-  double2 part[2][2][2] = {};
-  for (int it = 0; it < L.ipb; ++it) {
-    int64_t i = ln.row(L, it);
-    if (i >= L.n) break;
-    for (int ch = 0; ch < L.nch; ++ch) {
-      int s0 = ln.s0(L, ch);
-      C y[2];
-      row_spmv<R>(L, ln.k, i, s0, rowptr, col, cf, X, y);
-      int64_t o = vidx(L, ln.k, i, s0);
-      if (MODE == 0) {
-        st2(Y + o, y);
-      } else {
-        C w[2];
-        ld2(W + o, w);
-        for (int v = 0; v < 2; ++v) {
-          acc_bil(part[ch][v][0], y[v], w[v]);
-          acc_bil(part[ch][v][1], y[v], y[v]);
-        }
-      }
-    }
-  }
-  if (MODE == 1) {
+    block_reduce<VEC, 1>(L, ln, part, cols.acc, cols.C, slot, smem);
+  } else if constexpr (MODE == 2) {
     const int slot[2] = {ACC_D2, ACC_D3};
-    block_reduce<2>(L, ln, part, cols.acc, cols.C, slot, smem);
+    block_reduce<VEC, 2>(L, ln, part, cols.acc, cols.C, slot, smem);
   }
 }
 
-// h = x + alpha*h ; s = r - alpha*v ; acc[NS] += |s|^2   (dMesh.m:1305-1307)
-template <class R>
-__global__ void __launch_bounds__(BS) k_update_hs(Layout L, const typename CT<R>::C *__restrict__ x,
-                                                  typename CT<R>::C *__restrict__ h,
-                                                  const typename CT<R>::C *__restrict__ r,
-                                                  const typename CT<R>::C *__restrict__ v,
-                                                  typename CT<R>::C *__restrict__ s, Cols cols, const Ctl *ctl) {
+// per-lane column scalars
+template <class R, int VEC>
+__device__ inline void lane_scalars(const Cols &cols, const Lane &ln, const Layout &L, const double2 *src,
+                                    typename CT<R>::C (&out)[VEC], int (&act)[VEC]) {
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) {
+    const int64_t c = (int64_t)ln.k * L.nsp + ln.sub * VEC + v;
+    act[v] = cols.active[c];
+    out[v] = cvt<R>(src[c]);
+  }
+}
+
+// s = r - alpha*v ; acc[NS] += |s|^2   (dMesh.m:1306-1307)
+template <class R, int VEC>
+__global__ void __launch_bounds__(BS) k_update_s(Layout L, const typename CT<R>::C *__restrict__ r,
+                                                 const typename CT<R>::C *__restrict__ v,
+                                                 typename CT<R>::C *__restrict__ s, Cols cols, const Ctl *ctl) {
   using C = typename CT<R>::C;
   if (halted(ctl, ST_RUNNING)) return;
   extern __shared__ double2 smem[];
   Lane ln(L);
-  double2 part[2][2][1] = {};
-  C al[2][2];
-  int act[2][2];
-  for (int ch = 0; ch < L.nch; ++ch)
-    for (int q = 0; q < 2; ++q) {
-      int64_t c = (int64_t)ln.k * L.nsp + ln.s0(L, ch) + q;
-      act[ch][q] = cols.active[c];
-      al[ch][q] = cvt<R>(cols.alpha[c]);
-    }
+  double2 part[VEC][1];
+  C al[VEC];
+  int act[VEC];
+  lane_scalars<R, VEC>(cols, ln, L, cols.alpha, al, act);
+#pragma unroll
+  for (int q = 0; q < VEC; ++q) part[q][0] = make_double2(0, 0);
   for (int it = 0; it < L.ipb; ++it) {
-    int64_t i = ln.row(L, it);
+    const int64_t i = ln.row(L, it);
     if (i >= L.n) break;
-    for (int ch = 0; ch < L.nch; ++ch) {
-      int64_t o = vidx(L, ln.k, i, ln.s0(L, ch));
-      C xx[2], hh[2], rr[2], vv[2], ss[2];
-      ld2(x + o, xx); ld2(h + o, hh); ld2(r + o, rr); ld2(v + o, vv);
-      for (int q = 0; q < 2; ++q) {
-        if (act[ch][q]) {
-          hh[q] = cfmaT(al[ch][q], hh[q], xx[q]);
-          ss[q] = cfmaT(mk(-al[ch][q].x, -al[ch][q].y), vv[q], rr[q]);
-          acc_abs2(part[ch][q][0].x, ss[q]);
-        } else {
-          hh[q] = xx[q];
-          ss[q] = rr[q];
-        }
-      }
-      st2(h + o, hh);
-      st2(s + o, ss);
+    const int64_t o = vidx(L, ln.k, i, ln.sub * VEC);
+    C rr[VEC], vv[VEC], ss[VEC];
+    ldv<VEC>(r + o, rr);
+    ldv<VEC>(v + o, vv);
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) {
+      ss[q] = act[q] ? cfmaT(cneg(al[q]), vv[q], rr[q]) : rr[q];
+      if (act[q]) acc_abs2(part[q][0].x, ss[q]);
     }
+    stv<VEC>(s + o, ss);
   }
   const int slot[1] = {ACC_NS};
-  block_reduce<1>(L, ln, part, cols.acc, cols.C, slot, smem);
+  block_reduce<VEC, 1>(L, ln, part, cols.acc, cols.C, slot, smem);
 }
 
-// x = h + omega*z ; r = s - omega*t ; p = p - omega*v ; acc[NR] += |r|^2 ;
-// acc[RHO] += r0^.r  (dMesh.m:1327-1337).  In the FINAL state: x = h (:1311).
-template <class R>
+// x = x + alpha*h + omega*z ; r = s - omega*t ; p = p - omega*v ; acc[NR] += |r|^2 ;
+// acc[RHO] += r0^.r  (dMesh.m:1305, :1327-1337).  In the FINAL state: x = x + alpha*h (:1311).
+template <class R, int VEC>
 __global__ void __launch_bounds__(BS) k_update_xrp(Layout L, typename CT<R>::C *__restrict__ x,
                                                    const typename CT<R>::C *__restrict__ h,
                                                    const typename CT<R>::C *__restrict__ z,
@@ -393,76 +424,79 @@ __global__ void __launch_bounds__(BS) k_update_xrp(Layout L, typename CT<R>::C *
   const bool final_ = *(volatile const int *)&ctl->state == ST_FINAL;
   extern __shared__ double2 smem[];
   Lane ln(L);
-  double2 part[2][2][2] = {};
-  C om[2][2];
-  int act[2][2];
-  for (int ch = 0; ch < L.nch; ++ch)
-    for (int q = 0; q < 2; ++q) {
-      int64_t c = (int64_t)ln.k * L.nsp + ln.s0(L, ch) + q;
-      act[ch][q] = cols.active[c];
-      om[ch][q] = cvt<R>(cols.omega[c]);
-    }
+  double2 part[VEC][2];
+  C al[VEC], om[VEC];
+  int act[VEC];
+  lane_scalars<R, VEC>(cols, ln, L, cols.omega, om, act);
+  lane_scalars<R, VEC>(cols, ln, L, cols.alpha, al, act);
+#pragma unroll
+  for (int q = 0; q < VEC; ++q) part[q][0] = part[q][1] = make_double2(0, 0);
   for (int it = 0; it < L.ipb; ++it) {
-    int64_t i = ln.row(L, it);
+    const int64_t i = ln.row(L, it);
     if (i >= L.n) break;
-    for (int ch = 0; ch < L.nch; ++ch) {
-      int64_t o = vidx(L, ln.k, i, ln.s0(L, ch));
-      if (final_) {
-        C hh[2], xx[2];
-        ld2(h + o, hh);
-        ld2(x + o, xx);
-        for (int q = 0; q < 2; ++q) xx[q] = act[ch][q] ? hh[q] : xx[q];
-        st2(x + o, xx);
+    const int64_t o = vidx(L, ln.k, i, ln.sub * VEC);
+    C xx[VEC], hh[VEC];
+    ldv<VEC>(x + o, xx);
+    ldv<VEC>(h + o, hh);
+    if (final_) {
+#pragma unroll
+      for (int q = 0; q < VEC; ++q)
+        if (act[q]) xx[q] = cfmaT(al[q], hh[q], xx[q]);
+      stv<VEC>(x + o, xx);
+      continue;
+    }
+    C zz[VEC], ss[VEC], tt[VEC], pp[VEC], vv[VEC], rh[VEC], rr[VEC];
+    ldv<VEC>(z + o, zz);
+    ldv<VEC>(s + o, ss);
+    ldv<VEC>(t + o, tt);
+    ldv<VEC>(p + o, pp);
+    ldv<VEC>(v + o, vv);
+    ldv<VEC>(rhat + o, rh);
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) {
+      if (!act[q]) {
+        rr[q] = ss[q];
         continue;
       }
-      C xx[2], hh[2], zz[2], rr[2], ss[2], tt[2], pp[2], vv[2], rh[2];
-      ld2(x + o, xx); ld2(h + o, hh); ld2(z + o, zz); ld2(r + o, rr); ld2(s + o, ss);
-      ld2(t + o, tt); ld2(p + o, pp); ld2(v + o, vv); ld2(rhat + o, rh);
-      for (int q = 0; q < 2; ++q) {
-        if (!act[ch][q]) continue;
-        C w = om[ch][q], mw = mk(-om[ch][q].x, -om[ch][q].y);
-        xx[q] = cfmaT(w, zz[q], hh[q]);
-        rr[q] = cfmaT(mw, tt[q], ss[q]);
-        pp[q] = cfmaT(mw, vv[q], pp[q]);
-        acc_abs2(part[ch][q][0].x, rr[q]);
-        acc_bil(part[ch][q][1], rh[q], rr[q]);
+      xx[q] = cfmaT(om[q], zz[q], cfmaT(al[q], hh[q], xx[q]));
+      rr[q] = cfmaT(cneg(om[q]), tt[q], ss[q]);
+      pp[q] = cfmaT(cneg(om[q]), vv[q], pp[q]);
+      if (act[q] == 1) {
+        acc_abs2(part[q][0].x, rr[q]);
+        acc_bil(part[q][1], rh[q], rr[q]);
       }
-      st2(x + o, xx); st2(r + o, rr); st2(p + o, pp);
     }
+    stv<VEC>(x + o, xx);
+    stv<VEC>(r + o, rr);
+    stv<VEC>(p + o, pp);
   }
   if (!final_) {
     const int slot[2] = {ACC_NR, ACC_RHO};
-    block_reduce<2>(L, ln, part, cols.acc, cols.C, slot, smem);
+    block_reduce<VEC, 2>(L, ln, part, cols.acc, cols.C, slot, smem);
   }
 }
 
 // p = r + beta*p  (dMesh.m:1340)
-template <class R>
+template <class R, int VEC>
 __global__ void __launch_bounds__(BS) k_update_p(Layout L, const typename CT<R>::C *__restrict__ r,
                                                  typename CT<R>::C *__restrict__ p, Cols cols, const Ctl *ctl) {
   using C = typename CT<R>::C;
   if (halted(ctl, ST_RUNNING)) return;
   Lane ln(L);
-  C be[2][2];
-  int act[2][2];
-  for (int ch = 0; ch < L.nch; ++ch)
-    for (int q = 0; q < 2; ++q) {
-      int64_t c = (int64_t)ln.k * L.nsp + ln.s0(L, ch) + q;
-      act[ch][q] = cols.active[c];
-      be[ch][q] = cvt<R>(cols.beta[c]);
-    }
+  C be[VEC];
+  int act[VEC];
+  lane_scalars<R, VEC>(cols, ln, L, cols.beta, be, act);
   for (int it = 0; it < L.ipb; ++it) {
-    int64_t i = ln.row(L, it);
+    const int64_t i = ln.row(L, it);
     if (i >= L.n) break;
-    for (int ch = 0; ch < L.nch; ++ch) {
-      int64_t o = vidx(L, ln.k, i, ln.s0(L, ch));
-      C rr[2], pp[2];
-      ld2(r + o, rr);
-      ld2(p + o, pp);
-      for (int q = 0; q < 2; ++q)
-        if (act[ch][q]) pp[q] = cfmaT(be[ch][q], pp[q], rr[q]);
-      st2(p + o, pp);
-    }
+    const int64_t o = vidx(L, ln.k, i, ln.sub * VEC);
+    C rr[VEC], pp[VEC];
+    ldv<VEC>(r + o, rr);
+    ldv<VEC>(p + o, pp);
+#pragma unroll
+    for (int q = 0; q < VEC; ++q)
+      if (act[q]) pp[q] = cfmaT(be[q], pp[q], rr[q]);
+    stv<VEC>(p + o, pp);
   }
 }
 
@@ -496,29 +530,35 @@ __global__ void __launch_bounds__(1024) k_stage_alpha(Cols c, Ctl *ctl) {
     c.acc[ACC_D1 * c.C + j] = make_double2(0, 0);
     if (!c.active[j]) continue;
     double2 a = cdiv(c.rho0[j], d1);
-    if (!(cabs2(d1) > 0.0) || !finite2(a) || !(cabs2(c.rho0[j]) > 0.0)) { freeze(c, j, DGP_COL_BREAKDOWN_RHO); continue; }
+    if (!(cabs2(d1) > 0.0) || !finite2(a) || !(cabs2(c.rho0[j]) > 0.0)) {
+      freeze(c, j, DGP_COL_BREAKDOWN_RHO);
+      continue;
+    }
     c.alpha[j] = a;
   }
 }
 
-// after s: err = max ||s||/||r0||; below tol -> FINAL (x = h), dMesh.m:1307-1313
+// after s: err = max ||s||/||r0||; below tol -> FINAL (x = x + alpha h), dMesh.m:1307-1313
 __global__ void __launch_bounds__(1024) k_stage_check_s(Cols c, Ctl *ctl) {
   if (ctl->state != ST_RUNNING) return;
   double m = 0.0;
-  int stop_rule = ctl->stop_rule;
-  double tol = ctl->tol;
+  const int stop_rule = ctl->stop_rule;
+  const double tol = ctl->tol;
   for (int64_t j = threadIdx.x; j < c.C; j += blockDim.x) {
     double ns = c.acc[ACC_NS * c.C + j].x;
     c.acc[ACC_NS * c.C + j] = make_double2(0, 0);
     if (!c.active[j]) continue;
     double e = sqrt(ns) / c.err0[j];
-    if (!isfinite(e)) { freeze(c, j, DGP_COL_NONFINITE); continue; }
+    if (!isfinite(e)) {
+      freeze(c, j, DGP_COL_NONFINITE);
+      continue;
+    }
     c.err[j] = e;
     if (stop_rule == DGP_STOP_PER_COLUMN && e < tol) {
-      // column done at s: take x = h now and stop updating it afterwards
+      // column done at s: x = x + alpha h in this iteration's update, then frozen
       c.omega[j] = make_double2(0, 0);
       c.status[j] = DGP_COL_CONVERGED;
-      c.active[j] = 2;  // 2 = finishing this iteration
+      c.active[j] = 2;
     } else {
       m = fmax(m, e);
     }
@@ -533,34 +573,42 @@ __global__ void __launch_bounds__(1024) k_stage_check_s(Cols c, Ctl *ctl) {
 // after G t: omega = (Gt.Gs)/(Gt.Gt), dMesh.m:1325
 __global__ void __launch_bounds__(1024) k_stage_omega(Cols c, Ctl *ctl) {
   if (ctl->state == ST_DONE) return;
-  bool fin = ctl->state == ST_FINAL;
+  const bool fin = ctl->state == ST_FINAL;
   for (int64_t j = threadIdx.x; j < c.C; j += blockDim.x) {
     double2 d2v = c.acc[ACC_D2 * c.C + j], d3 = c.acc[ACC_D3 * c.C + j];
     c.acc[ACC_D2 * c.C + j] = make_double2(0, 0);
     c.acc[ACC_D3 * c.C + j] = make_double2(0, 0);
-    if (c.active[j] != 1) continue;
-    if (fin) continue;
+    if (c.active[j] != 1 || fin) continue;
     double2 om = cdiv(d2v, d3);
-    if (!(cabs2(d3) > 0.0) || !finite2(om) || !(cabs2(om) > 0.0)) { freeze(c, j, DGP_COL_BREAKDOWN_OMEGA); continue; }
+    if (!(cabs2(d3) > 0.0) || !finite2(om) || !(cabs2(om) > 0.0)) {
+      freeze(c, j, DGP_COL_BREAKDOWN_OMEGA);
+      continue;
+    }
     c.omega[j] = om;
   }
 }
 
 // after x, r: err = max ||r||/||r0|| (dMesh.m:1330-1335); beta, rho0 (:1337-1339)
 __global__ void __launch_bounds__(1024) k_stage_check_r(Cols c, Ctl *ctl) {
-  int st = ctl->state;
+  const int st = ctl->state;
   if (st == ST_DONE) return;
   double m = 0.0;
-  double tol = ctl->tol;
+  const double tol = ctl->tol;
   for (int64_t j = threadIdx.x; j < c.C; j += blockDim.x) {
     double nr = c.acc[ACC_NR * c.C + j].x;
     double2 rho = c.acc[ACC_RHO * c.C + j];
     c.acc[ACC_NR * c.C + j] = make_double2(0, 0);
     c.acc[ACC_RHO * c.C + j] = make_double2(0, 0);
-    if (c.active[j] == 2) { c.active[j] = 0; continue; }  // finished at s this iteration
+    if (c.active[j] == 2) {  // finished at s this iteration
+      c.active[j] = 0;
+      continue;
+    }
     if (!c.active[j] || st == ST_FINAL) continue;
     double e = sqrt(nr) / c.err0[j];
-    if (!isfinite(e)) { freeze(c, j, DGP_COL_NONFINITE); continue; }
+    if (!isfinite(e)) {
+      freeze(c, j, DGP_COL_NONFINITE);
+      continue;
+    }
     c.err[j] = e;
     if (ctl->stop_rule == DGP_STOP_PER_COLUMN && e < tol) {
       c.active[j] = 0;
@@ -570,7 +618,10 @@ __global__ void __launch_bounds__(1024) k_stage_check_r(Cols c, Ctl *ctl) {
     m = fmax(m, e);
     // beta = rho/rho0 * (1/(alph*om)) = (rho/rho0) * (alpha/omega)
     double2 b = cmul(cdiv(rho, c.rho0[j]), cdiv(c.alpha[j], c.omega[j]));
-    if (!finite2(b) || !(cabs2(rho) > 0.0)) { freeze(c, j, DGP_COL_BREAKDOWN_RHO); continue; }
+    if (!finite2(b) || !(cabs2(rho) > 0.0)) {
+      freeze(c, j, DGP_COL_BREAKDOWN_RHO);
+      continue;
+    }
     c.beta[j] = b;
     c.rho0[j] = rho;
   }
@@ -583,8 +634,14 @@ __global__ void __launch_bounds__(1024) k_stage_check_r(Cols c, Ctl *ctl) {
     } else {
       ctl->max_err = m;
       // with the per-column rule the solve ends when no column is active (k_stage_count)
-      if (ctl->stop_rule == DGP_STOP_MAX_ALL && m < tol) { ctl->state = ST_DONE; ctl->reason = 0; }
-      if (ctl->state != ST_DONE && ctl->iters >= ctl->maxit) { ctl->state = ST_DONE; ctl->reason = 1; }
+      if (ctl->stop_rule == DGP_STOP_MAX_ALL && m < tol) {
+        ctl->state = ST_DONE;
+        ctl->reason = 0;
+      }
+      if (ctl->state != ST_DONE && ctl->iters >= ctl->maxit) {
+        ctl->state = ST_DONE;
+        ctl->reason = 1;
+      }
     }
   }
 }
@@ -599,39 +656,44 @@ __global__ void __launch_bounds__(1024) k_stage_count(Cols c, Ctl *ctl) {
   a = BR(tmp).Sum(a);
   if (threadIdx.x == 0) {
     ctl->n_active = a;
-    if (a == 0) { ctl->state = ST_DONE; ctl->reason = ctl->iters == 0 ? 2 : 0; }
+    if (a == 0) {
+      ctl->state = ST_DONE;
+      ctl->reason = ctl->iters == 0 ? 2 : 0;
+    }
   }
 }
 
 // --------------------------------------------------------- setup kernels
-// initial state: x = 0, r = r^0 = p = b (dMesh.m:1283-1290); err0, rho0 per column.
-template <class R>
-__global__ void __launch_bounds__(BS) k_init(Layout L, const typename CT<R>::C *__restrict__ b,
-                                             typename CT<R>::C *x, typename CT<R>::C *r, typename CT<R>::C *rhat,
-                                             typename CT<R>::C *p, Cols cols) {
+// initial state: x = 0, r = r^0 = p = b (dMesh.m:1283-1290); ||r0||^2 and r0.r0 per column.
+template <class R, int VEC>
+__global__ void __launch_bounds__(BS) k_init(Layout L, typename CT<R>::C *__restrict__ x,
+                                             const typename CT<R>::C *__restrict__ r,
+                                             typename CT<R>::C *__restrict__ rhat, typename CT<R>::C *__restrict__ p,
+                                             Cols cols) {
   using C = typename CT<R>::C;
   extern __shared__ double2 smem[];
   Lane ln(L);
-  double2 part[2][2][2] = {};
+  double2 part[VEC][2];
+#pragma unroll
+  for (int q = 0; q < VEC; ++q) part[q][0] = part[q][1] = make_double2(0, 0);
   for (int it = 0; it < L.ipb; ++it) {
-    int64_t i = ln.row(L, it);
+    const int64_t i = ln.row(L, it);
     if (i >= L.n) break;
-    for (int ch = 0; ch < L.nch; ++ch) {
-      int64_t o = vidx(L, ln.k, i, ln.s0(L, ch));
-      C bb[2], z[2] = {czero<C>(), czero<C>()};
-      ld2(b + o, bb);
-      if (x) st2(x + o, z);
-      if (r != b) st2(r + o, bb);
-      st2(rhat + o, bb);
-      st2(p + o, bb);
-      for (int q = 0; q < 2; ++q) {
-        acc_abs2(part[ch][q][0].x, bb[q]);
-        acc_bil(part[ch][q][1], bb[q], bb[q]);
-      }
+    const int64_t o = vidx(L, ln.k, i, ln.sub * VEC);
+    C bb[VEC], zz[VEC];
+    ldv<VEC>(r + o, bb);
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) {
+      zz[q] = czero<C>();
+      acc_abs2(part[q][0].x, bb[q]);
+      acc_bil(part[q][1], bb[q], bb[q]);
     }
+    stv<VEC>(x + o, zz);
+    stv<VEC>(rhat + o, bb);
+    stv<VEC>(p + o, bb);
   }
   const int slot[2] = {ACC_NR, ACC_RHO};
-  block_reduce<2>(L, ln, part, cols.acc, cols.C, slot, smem);
+  block_reduce<VEC, 2>(L, ln, part, cols.acc, cols.C, slot, smem);
 }
 
 // err0 = ||r0||, rho0 = r0.r0, activity from the column index and norm
@@ -644,12 +706,12 @@ __global__ void __launch_bounds__(1024) k_stage_init(Cols c, Ctl *ctl, int nsp, 
     double2 rho = c.acc[ACC_RHO * c.C + j];
     c.acc[ACC_NR * c.C + j] = make_double2(0, 0);
     c.acc[ACC_RHO * c.C + j] = make_double2(0, 0);
-    int s = (int)(j % nsp);
+    const int s = (int)(j % nsp);
     c.err0[j] = sqrt(nr);
     c.err[j] = 1.0;
     c.rho0[j] = rho;
     c.alpha[j] = c.omega[j] = c.beta[j] = make_double2(0, 0);
-    bool act = s < ns && nr > 0.0 && isfinite(nr);
+    const bool act = s < ns && nr > 0.0 && isfinite(nr);
     c.active[j] = act ? 1 : 0;
     c.status[j] = act ? DGP_COL_MAXIT : (s < ns && !isfinite(nr) ? DGP_COL_NONFINITE : DGP_COL_ZERO_RHS);
     if (!act) c.err[j] = 0.0;
@@ -667,7 +729,7 @@ __global__ void __launch_bounds__(1024) k_stage_init(Cols c, Ctl *ctl, int nsp, 
 
 // final statuses: active columns below tol are converged, the rest hit maxit
 __global__ void __launch_bounds__(1024) k_stage_final(Cols c, Ctl *ctl) {
-  double tol = ctl->tol;
+  const double tol = ctl->tol;
   for (int64_t j = threadIdx.x; j < c.C; j += blockDim.x) {
     if (c.status[j] == DGP_COL_MAXIT || c.active[j]) {
       c.status[j] = (c.err[j] < tol || (ctl->reason == 0 && ctl->stop_rule == DGP_STOP_MAX_ALL))
@@ -676,53 +738,73 @@ __global__ void __launch_bounds__(1024) k_stage_final(Cols c, Ctl *ctl) {
   }
 }
 
+// mixed precision: a column's status is decided by its FP64 residual
+__global__ void k_status_outer(Cols c, const double *__restrict__ outer_err, double tol, int nsp, int ns) {
+  int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j >= c.C) return;
+  const int s = (int)(j % nsp);
+  if (s >= ns) return;
+  const int st = c.status[j];
+  if (st == DGP_COL_BREAKDOWN_RHO || st == DGP_COL_BREAKDOWN_OMEGA || st == DGP_COL_NONFINITE) return;
+  if (st == DGP_COL_ZERO_RHS) return;
+  c.status[j] = outer_err[j] < tol ? DGP_COL_CONVERGED : DGP_COL_MAXIT;
+}
+
 // ------------------------------------------------ user layout <-> workspace
 // dst[k][i][s] (nsp) = (T) src[k][i][s] (ns), zero padding
 template <class R>
-__global__ void k_pack(Layout L, int ns, const double2 *__restrict__ src, typename CT<R>::C *__restrict__ dst) {
-  int64_t tot = (int64_t)L.nf * L.n * L.nsp;
+__global__ void k_pack(int64_t n, int nf, int nsp, int ns, const double2 *__restrict__ src,
+                       typename CT<R>::C *__restrict__ dst) {
+  const int64_t tot = (int64_t)nf * n * nsp;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
-    int s = (int)(e % L.nsp);
-    int64_t ki = e / L.nsp;
+    const int s = (int)(e % nsp);
+    const int64_t ki = e / nsp;
     double2 v = s < ns ? src[ki * ns + s] : make_double2(0, 0);
     dst[e] = cvt<R>(v);
   }
 }
 
 template <class R>
-__global__ void k_unpack(Layout L, int ns, const typename CT<R>::C *__restrict__ src, double2 *__restrict__ dst) {
-  int64_t tot = (int64_t)L.nf * L.n * ns;
+__global__ void k_unpack(int64_t n, int nf, int nsp, int ns, const typename CT<R>::C *__restrict__ src,
+                         double2 *__restrict__ dst) {
+  const int64_t tot = (int64_t)nf * n * ns;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
-    int s = (int)(e % ns);
-    int64_t ki = e / ns;
-    dst[e] = d2(src[ki * L.nsp + s]);
+    const int s = (int)(e % ns);
+    const int64_t ki = e / ns;
+    dst[e] = d2(src[ki * nsp + s]);
   }
 }
 
 // point-source right-hand sides (dMesh.m:124-129): b[k][node][s] = w * fpsf[k]
 template <class R>
-__global__ void k_sources(Layout L, int ns, const int32_t *__restrict__ nodes, const double *__restrict__ w,
-                          const double2 *__restrict__ fpsf, typename CT<R>::C *__restrict__ b) {
-  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (t >= (int64_t)L.nf * ns) return;
-  int k = (int)(t / ns), s = (int)(t % ns);
+__global__ void k_sources(int64_t n, int nf, int nsp, int ns, const int32_t *__restrict__ nodes,
+                          const double *__restrict__ w, const double2 *__restrict__ fpsf,
+                          typename CT<R>::C *__restrict__ b) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= (int64_t)nf * ns) return;
+  const int k = (int)(t / ns), s = (int)(t % ns);
   for (int l = 0; l < 4; ++l) {
-    int32_t nd = nodes[4 * s + l];
-    if (nd < 0 || nd >= L.n) continue;  // rejected on the host before the solve
+    const int32_t nd = nodes[4 * s + l];
+    if (nd < 0 || nd >= n) continue;  // rejected on the host before the solve
     // the reference assigns (not accumulates) the 4 weights of a tet's distinct nodes
     double2 v = make_double2(w[4 * s + l] * fpsf[k].x, w[4 * s + l] * fpsf[k].y);
-    b[vidx(L, k, nd, s)] = cvt<R>(v);
+    b[((int64_t)k * n + nd) * nsp + s] = cvt<R>(v);
   }
+}
+
+__global__ void k_check_nodes(const int32_t *__restrict__ nodes, int ns, int64_t n, int *bad) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < 4 * ns && (nodes[t] < 0 || nodes[t] >= n)) atomicOr(bad, 1);
 }
 
 // ------------------------------------------------- mixed precision kernels
 // X64[k][i][s] += x32[k][i][s] for s < ns (X64 is the caller's [nf][n][ns] buffer)
-__global__ void k_accum_x(Layout L, int ns, const float2 *__restrict__ x32, double2 *__restrict__ X) {
-  int64_t tot = (int64_t)L.nf * L.n * ns;
+__global__ void k_accum_x(int64_t n, int nf, int nsp, int ns, const float2 *__restrict__ x32, double2 *__restrict__ X) {
+  const int64_t tot = (int64_t)nf * n * ns;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
-    int s = (int)(e % ns);
-    int64_t ki = e / ns;
-    float2 d = x32[ki * L.nsp + s];
+    const int s = (int)(e % ns);
+    const int64_t ki = e / ns;
+    float2 d = x32[ki * nsp + s];
     double2 v = X[e];
     v.x += (double)d.x;
     v.y += (double)d.y;
@@ -730,10 +812,10 @@ __global__ void k_accum_x(Layout L, int ns, const float2 *__restrict__ x32, doub
   }
 }
 
-// FP64 residual r = b - A_k X (X in the caller's layout, stride ns), written
-// as FP32 into r32 (the next inner right-hand side) with FP64 norms into
-// acc[NR].  b is either a dense caller buffer (stride ns) or the point
-// sources (nodes, w, fpsf) generated on the fly.
+// FP64 residual r = b - A_k X (X in the caller's layout, stride ns), written as FP32 into
+// r32 (the next inner right-hand side) with FP64 norms into acc[NR].  b is a dense caller
+// buffer (stride ns) or the point sources (nodes, w, fpsf) generated on the fly.
+template <int VEC>
 __global__ void __launch_bounds__(BS) k_residual64(Layout L, int ns, const int32_t *__restrict__ rowptr,
                                                    const int32_t *__restrict__ col, const double2 *__restrict__ KM,
                                                    const double *__restrict__ omega, const double2 *__restrict__ X,
@@ -746,63 +828,66 @@ __global__ void __launch_bounds__(BS) k_residual64(Layout L, int ns, const int32
   Lane ln(L);
   if (snodes) {
     for (int t = threadIdx.x; t < 4 * L.nsp; t += blockDim.x) {
-      int s = t / 4;
+      const int s = t / 4;
       sn[t] = s < ns ? snodes[t] : -1;
       swt[t] = s < ns ? sw[t] : 0.0;
     }
-    __syncthreads();
   }
+  __syncthreads();
   const double om = omega[ln.k];
   const double2 fk = fpsf ? fpsf[ln.k] : make_double2(0, 0);
-  double2 part[2][2][1] = {};
+  double2 part[VEC][1];
+#pragma unroll
+  for (int q = 0; q < VEC; ++q) part[q][0] = make_double2(0, 0);
+  const double2 *Xk = X + (int64_t)ln.k * L.n * ns;
   for (int it = 0; it < L.ipb; ++it) {
-    int64_t i = ln.row(L, it);
+    const int64_t i = ln.row(L, it);
     if (i >= L.n) break;
-    for (int ch = 0; ch < L.nch; ++ch) {
-      int s0 = ln.s0(L, ch);
-      double2 y[2] = {make_double2(0, 0), make_double2(0, 0)};
-      int b = __ldg(rowptr + i), e = __ldg(rowptr + i + 1);
-      const double2 *Xk = X + (int64_t)ln.k * L.n * ns;
-      for (int p = b; p < e; ++p) {
-        int j = __ldg(col + p);
-        double2 km = __ldg(KM + p);
-        double2 a = make_double2(km.x, om * km.y);
-        for (int q = 0; q < 2; ++q)
-          if (s0 + q < ns) y[q] = cfma(a, __ldg(Xk + (int64_t)j * ns + s0 + q), y[q]);
-      }
-      float2 out[2];
-      for (int q = 0; q < 2; ++q) {
-        int s = s0 + q;
-        double2 bv = make_double2(0, 0);
-        if (s < ns) {
-          if (Bd) {
-            bv = Bd[((int64_t)ln.k * L.n + i) * ns + s];
-          } else {
-            for (int l = 0; l < 4; ++l)
-              if (sn[4 * s + l] == i) bv = make_double2(swt[4 * s + l] * fk.x, swt[4 * s + l] * fk.y);
-          }
-        }
-        double2 rr = make_double2(bv.x - y[q].x, bv.y - y[q].y);
-        if (s >= ns) rr = make_double2(0, 0);
-        acc_abs2(part[ch][q][0].x, rr);
-        out[q] = make_float2((float)rr.x, (float)rr.y);
-      }
-      st2(r32 + vidx(L, ln.k, i, s0), out);
+    const int s0 = ln.sub * VEC;
+    double2 y[VEC];
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) y[q] = make_double2(0, 0);
+    const int b = __ldg(rowptr + i), e = __ldg(rowptr + i + 1);
+    for (int p = b; p < e; ++p) {
+      const int j = __ldg(col + p);
+      const double2 km = __ldg(KM + p);
+      const double2 a = make_double2(km.x, om * km.y);
+#pragma unroll
+      for (int q = 0; q < VEC; ++q)
+        if (s0 + q < ns) y[q] = cfma(a, __ldg(Xk + (int64_t)j * ns + s0 + q), y[q]);
     }
+    float2 out[VEC];
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) {
+      const int s = s0 + q;
+      double2 bv = make_double2(0, 0);
+      if (s < ns) {
+        if (Bd) {
+          bv = Bd[((int64_t)ln.k * L.n + i) * ns + s];
+        } else {
+          for (int l = 0; l < 4; ++l)
+            if (sn[4 * s + l] == i) bv = make_double2(swt[4 * s + l] * fk.x, swt[4 * s + l] * fk.y);
+        }
+      }
+      double2 rr = make_double2(bv.x - y[q].x, bv.y - y[q].y);
+      if (s >= ns) rr = make_double2(0, 0);
+      acc_abs2(part[q][0].x, rr);
+      out[q] = make_float2((float)rr.x, (float)rr.y);
+    }
+    stv<VEC>(r32 + vidx(L, ln.k, i, s0), out);
   }
   const int slot[1] = {ACC_NR};
-  block_reduce<1>(L, ln, part, cols.acc, cols.C, slot, smem);
+  block_reduce<VEC, 1>(L, ln, part, cols.acc, cols.C, slot, smem);
 }
 
-// ||b|| per column for the outer relative residual, and the outer check
+// mode 0: ||b|| per column from acc[NR]; mode 1: outer_err = ||r||/||b||, ctl->max_err = max
 __global__ void __launch_bounds__(1024) k_outer_norms(Cols c, double *bnorm, double *outer_err, Ctl *ctl, int mode,
                                                       int nsp, int ns) {
-  // mode 0: store ||b|| from acc[NR]; mode 1: outer_err = ||r||/||b||, ctl->max_err = max
   double m = 0.0;
   for (int64_t j = threadIdx.x; j < c.C; j += blockDim.x) {
-    double nr = c.acc[ACC_NR * c.C + j].x;
+    const double nr = c.acc[ACC_NR * c.C + j].x;
     c.acc[ACC_NR * c.C + j] = make_double2(0, 0);
-    int s = (int)(j % nsp);
+    const int s = (int)(j % nsp);
     if (mode == 0) {
       bnorm[j] = sqrt(nr);
     } else {
@@ -816,33 +901,49 @@ __global__ void __launch_bounds__(1024) k_outer_norms(Cols c, double *bnorm, dou
   if (threadIdx.x == 0 && mode == 1) ctl->max_err = m;
 }
 
-__global__ void k_cvt_km(const double *__restrict__ K, const double *__restrict__ M, int64_t nnz, double2 *km64,
-                         float2 *km32) {
-  int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+__global__ void k_cvt_km(const double *__restrict__ K, const double *__restrict__ M, const int32_t *__restrict__ col,
+                         int64_t nnz, double2 *km64, Rec32 *rec) {
+  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (p >= nnz) return;
   km64[p] = make_double2(K[p], M[p]);
-  km32[p] = make_float2((float)K[p], (float)M[p]);
+  Rec32 r;
+  r.col = col[p];
+  r.a = (float)K[p];
+  r.b = (float)M[p];
+  r.pad = 0.f;
+  rec[p] = r;
 }
 
 __global__ void k_dfc_m(const double *__restrict__ M, double dfc, int64_t nnz, double *out) {
-  int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (p < nnz) out[p] = dfc * M[p];
 }
 
-__global__ void k_gather_gt(const double2 *__restrict__ G, const int32_t *__restrict__ perm, int64_t nnzG, int nf,
-                            double2 *GT, float2 *G32, float2 *GT32) {
-  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+// G^T values and the FP32 records of G and G^T
+__global__ void k_gather_gt(const double2 *__restrict__ G, const int32_t *__restrict__ perm,
+                            const int32_t *__restrict__ colG, const int32_t *__restrict__ colT, int64_t nnzG, int nf,
+                            double2 *GT, Rec32 *recG, Rec32 *recGT) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= nnzG * nf) return;
-  int64_t k = t / nnzG, q = t % nnzG;
-  double2 gt = G[k * nnzG + perm[q]];
+  const int64_t k = t / nnzG, q = t % nnzG;
+  const double2 gt = G[k * nnzG + perm[q]];
   GT[t] = gt;
-  double2 g = G[t];
-  G32[t] = make_float2((float)g.x, (float)g.y);
-  GT32[t] = make_float2((float)gt.x, (float)gt.y);
+  const double2 g = G[t];
+  Rec32 a, b;
+  a.col = colG[q];
+  a.a = (float)g.x;
+  a.b = (float)g.y;
+  a.pad = 0.f;
+  b.col = colT[q];
+  b.a = (float)gt.x;
+  b.b = (float)gt.y;
+  b.pad = 0.f;
+  recG[t] = a;
+  recGT[t] = b;
 }
 
 __global__ void k_omega(int nf, double dfc, double *om64, float *om32) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k < nf) {
     om64[k] = (double)k * dfc;
     om32[k] = (float)((double)k * dfc);
@@ -873,7 +974,7 @@ struct Work {
 
 Work work_views(SolverPlan *S) {
   Work w;
-  int64_t C = S->ws_cols;
+  const int64_t C = S->ws_cols;
   char *b = S->scal.as<char>();
   w.cols.C = C;
   w.cols.err0 = (double *)b; b += sizeof(double) * C;
@@ -885,7 +986,7 @@ Work work_views(SolverPlan *S) {
   w.cols.omega = (double2 *)b; b += sizeof(double2) * C;
   w.cols.beta = (double2 *)b; b += sizeof(double2) * C;
   w.cols.acc = (double2 *)b; b += sizeof(double2) * C * NACC;
-  w.cols.active = (int *)b; b += sizeof(int) * C;
+  w.cols.active = (int *)b;
   w.cols.status = S->status.as<int>();
   w.ctl = S->ctl.as<Ctl>();
   return w;
@@ -904,11 +1005,14 @@ template <class R> Vecs<R> vec_views(SolverPlan *S) {
 int ensure_workspace(SolverPlan *S, int prec) {
   if (S->ws_prec == prec) return DGP_OK;
   for (auto &g : S->graph)
-    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
   S->graph_iters[0] = S->graph_iters[1] = 0;
-  int64_t C = (int64_t)S->nf * S->nsp;
-  size_t esz = prec == DGP_PREC_FP64 ? sizeof(double2) : sizeof(float2);
-  size_t vb = esz * (size_t)C * S->n;
+  const int64_t C = (int64_t)S->nf * S->nsp;
+  const size_t esz = prec == DGP_PREC_FP64 ? sizeof(double2) : sizeof(float2);
+  const size_t vb = esz * (size_t)C * S->n;
   for (int q = 0; q < 10; ++q) {
     S->vec[q].release();
     DGP_TRY(S->vec[q].alloc(vb));
@@ -922,77 +1026,93 @@ int ensure_workspace(SolverPlan *S, int prec) {
   return DGP_OK;
 }
 
-// one BiCGSTAB iteration (dMesh.m:1295-1340) enqueued on st
-template <class R>
-int enqueue_iteration(SolverPlan *S, const Layout &L, const Layout &Ld, const Vecs<R> &V, const Work &W,
-                      cudaStream_t st) {
-  using C = typename CT<R>::C;
-  constexpr bool F32 = sizeof(R) == 4;
-  const auto *KM = F32 ? (const typename CT<R>::KM *)S->KM32.p : (const typename CT<R>::KM *)S->KM64.p;
-  const R *om = F32 ? (const R *)(S->omega.as<char>() + sizeof(double) * S->nf) : (const R *)S->omega.p;
-  const C *G = F32 ? (const C *)S->G32.p : (const C *)S->G64.p;
-  const C *GT = F32 ? (const C *)S->GT32.p : (const C *)S->GT64.p;
-  const int32_t *rp = S->rowptr.as<int32_t>(), *cl = S->col.as<int32_t>();
-  const int32_t *rg = S->P.rowptr.as<int32_t>(), *cg = S->P.col.as<int32_t>();
-  const int32_t *rt = S->P.rowptrT.as<int32_t>(), *ct = S->P.colT.as<int32_t>();
-  dim3 gr((unsigned)ceil_div(L.n, L.rows_per_block()), L.nf);
-  dim3 gd((unsigned)ceil_div(Ld.n, Ld.rows_per_block()), Ld.nf);
-  Ctl *ctl = W.ctl;
-  // T1 = G p ; h = G^T T1                                       (:1295-1296)
-  k_spmm_G<R, 0><<<gr, BS, 0, st>>>(L, rg, cg, G, S->nnzG, V.p, V.T1, nullptr, W.cols, ctl, ST_RUNNING);
-  k_spmm_G<R, 0><<<gr, BS, 0, st>>>(L, rt, ct, GT, S->nnzG, V.T1, V.h, nullptr, W.cols, ctl, ST_RUNNING);
-  // v = A h, d1 = v.r0^                                         (:1301, :1304)
-  k_spmm_A<R, true><<<gd, BS, red_smem(Ld, 1), st>>>(Ld, rp, cl, KM, om, V.h, V.v, V.rhat, W.cols, ctl, ST_RUNNING);
-  k_stage_alpha<<<1, 1024, 0, st>>>(W.cols, ctl);
-  // h = x + alpha h ; s = r - alpha v ; ||s||                   (:1305-1308)
-  k_update_hs<R><<<gd, BS, red_smem(Ld, 1), st>>>(Ld, V.x, V.h, V.r, V.v, V.s, W.cols, ctl);
-  k_stage_check_s<<<1, 1024, 0, st>>>(W.cols, ctl);
-  // Gs = G s ; z = G^T Gs ; t = A z ; (G t).Gs, (G t).(G t)     (:1315-1325)
-  k_spmm_G<R, 0><<<gr, BS, 0, st>>>(L, rg, cg, G, S->nnzG, V.s, V.T1, nullptr, W.cols, ctl, ST_RUNNING);
-  k_spmm_G<R, 0><<<gr, BS, 0, st>>>(L, rt, ct, GT, S->nnzG, V.T1, V.z, nullptr, W.cols, ctl, ST_RUNNING);
-  k_spmm_A<R, false><<<gr, BS, 0, st>>>(L, rp, cl, KM, om, V.z, V.t, nullptr, W.cols, ctl, ST_RUNNING);
-  k_spmm_G<R, 1><<<gd, BS, red_smem(Ld, 2), st>>>(Ld, rg, cg, G, S->nnzG, V.t, nullptr, V.T1, W.cols, ctl, ST_RUNNING);
-  k_stage_omega<<<1, 1024, 0, st>>>(W.cols, ctl);
-  // x = h + om z ; r = s - om t ; p = p - om v ; ||r|| ; r0^.r  (:1327-1337)
-  k_update_xrp<R><<<gd, BS, red_smem(Ld, 2), st>>>(Ld, V.x, V.h, V.z, V.r, V.s, V.t, V.p, V.v, V.rhat, W.cols, ctl);
-  k_stage_check_r<<<1, 1024, 0, st>>>(W.cols, ctl);
-  k_stage_count<<<1, 1024, 0, st>>>(W.cols, ctl);
-  // p = r + beta p                                              (:1340)
-  k_update_p<R><<<gr, BS, 0, st>>>(L, V.r, V.p, W.cols, ctl);
-  DGP_CHECK_LAUNCH();
-  return DGP_OK;
-}
-
 struct Layouts {
   Layout L, Ld;
 };
 
-Layouts layouts_for(SolverPlan *S) {
+// plain sweeps: ~64 rows per block; sweeps with dot products: 16x more rows per
+// block, so each block issues fewer FP64 atomics per column
+Layouts layouts_for(const SolverPlan *S, int vec) {
   Layouts x;
-  // plain sweeps: ~64 rows per block; sweeps with dot products: 4x more rows
-  // per block (fewer FP64 atomics per column)
-  int rpw = 32 / std::min(32, S->nsp / 2);
-  int ipb = std::max(1, 64 / (WARPS * rpw));
-  x.L = make_layout(S->n, S->nf, S->nsp, ipb);
-  x.Ld = make_layout(S->n, S->nf, S->nsp, ipb * 4);
+  const int lpr = S->nsp / vec;
+  const int rpw = 32 / lpr;
+  const int ipb = std::max(1, 64 / (WARPS * rpw));
+  x.L = Layout{S->n, S->nf, S->nsp, lpr, rpw, ipb};
+  x.Ld = Layout{S->n, S->nf, S->nsp, lpr, rpw, ipb * 16};
   return x;
+}
+
+inline int vec_for(const SolverPlan *S) { return S->nsp <= 64 ? 2 : 4; }
+
+dim3 grid_of(const Layout &L) { return dim3((unsigned)ceil_div(L.n, L.rows_per_block()), (unsigned)L.nf); }
+
+// one BiCGSTAB iteration (dMesh.m:1295-1340) enqueued on st: KERNELS_PER_ITER launches
+template <class R, int VEC, class OpA, class OpG>
+void enqueue_iteration(const Layouts &LL, const OpA &A, const OpG &G, const OpG &GT, const Vecs<R> &V,
+                       const Work &W, cudaStream_t st) {
+  const Layout &L = LL.L, &Ld = LL.Ld;
+  Ctl *ctl = W.ctl;
+  // T1 = G p ; h = G^T T1                                       (:1295-1296)
+  k_spmm<R, VEC, 0><<<grid_of(L), BS, 0, st>>>(L, G, V.p, V.T1, nullptr, W.cols, ctl);
+  k_spmm<R, VEC, 0><<<grid_of(L), BS, 0, st>>>(L, GT, V.T1, V.h, nullptr, W.cols, ctl);
+  // v = A h, d1 = v.r0^                                         (:1301, :1304)
+  k_spmm<R, VEC, 1><<<grid_of(Ld), BS, red_smem(Ld, 1), st>>>(Ld, A, V.h, V.v, V.rhat, W.cols, ctl);
+  k_stage_alpha<<<1, 1024, 0, st>>>(W.cols, ctl);
+  // s = r - alpha v ; ||s||                                     (:1306-1308)
+  k_update_s<R, VEC><<<grid_of(Ld), BS, red_smem(Ld, 1), st>>>(Ld, V.r, V.v, V.s, W.cols, ctl);
+  k_stage_check_s<<<1, 1024, 0, st>>>(W.cols, ctl);
+  // Gs = G s ; z = G^T Gs ; t = A z ; (G t).Gs, (G t).(G t)     (:1315-1325)
+  k_spmm<R, VEC, 0><<<grid_of(L), BS, 0, st>>>(L, G, V.s, V.T1, nullptr, W.cols, ctl);
+  k_spmm<R, VEC, 0><<<grid_of(L), BS, 0, st>>>(L, GT, V.T1, V.z, nullptr, W.cols, ctl);
+  k_spmm<R, VEC, 0><<<grid_of(L), BS, 0, st>>>(L, A, V.z, V.t, nullptr, W.cols, ctl);
+  k_spmm<R, VEC, 2><<<grid_of(Ld), BS, red_smem(Ld, 2), st>>>(Ld, G, V.t, nullptr, V.T1, W.cols, ctl);
+  k_stage_omega<<<1, 1024, 0, st>>>(W.cols, ctl);
+  // x += alpha h + om z ; r = s - om t ; p -= om v ; ||r|| ; r0^.r   (:1305, :1327-1337)
+  k_update_xrp<R, VEC><<<grid_of(Ld), BS, red_smem(Ld, 2), st>>>(Ld, V.x, V.h, V.z, V.r, V.s, V.t, V.p, V.v, V.rhat,
+                                                                 W.cols, ctl);
+  k_stage_check_r<<<1, 1024, 0, st>>>(W.cols, ctl);
+  k_stage_count<<<1, 1024, 0, st>>>(W.cols, ctl);
+  // p = r + beta p                                              (:1340)
+  k_update_p<R, VEC><<<grid_of(L), BS, 0, st>>>(L, V.r, V.p, W.cols, ctl);
+}
+
+template <class R, int VEC>
+int enqueue_for(SolverPlan *S, const Vecs<R> &V, const Work &W, cudaStream_t st) {
+  const Layouts LL = layouts_for(S, VEC);
+  const int32_t *rp = S->rowptr.as<int32_t>();
+  if constexpr (sizeof(R) == 4) {
+    OpA32 A{rp, S->RecA32.as<Rec32>(), (const float *)(S->omega.as<char>() + sizeof(double) * S->nf)};
+    OpG32 G{S->P.rowptr.as<int32_t>(), S->RecG32.as<Rec32>(), S->nnzG};
+    OpG32 GT{S->P.rowptrT.as<int32_t>(), S->RecGT32.as<Rec32>(), S->nnzG};
+    enqueue_iteration<R, VEC>(LL, A, G, GT, V, W, st);
+  } else {
+    OpA64 A{rp, S->col.as<int32_t>(), S->KM64.as<double2>(), S->omega.as<double>()};
+    OpG64 G{S->P.rowptr.as<int32_t>(), S->P.col.as<int32_t>(), S->G64.as<double2>(), S->nnzG};
+    OpG64 GT{S->P.rowptrT.as<int32_t>(), S->P.colT.as<int32_t>(), S->GT64.as<double2>(), S->nnzG};
+    enqueue_iteration<R, VEC>(LL, A, G, GT, V, W, st);
+  }
+  DGP_CUDA(cudaGetLastError());
+  return DGP_OK;
 }
 
 // run BiCGSTAB iterations (graph-captured blocks) until the control block says done
 template <class R>
 int run_iterations(SolverPlan *S, const Vecs<R> &V, const Work &W, int check_every, int maxit, cudaStream_t st,
                    int *iters_out) {
-  Layouts LL = layouts_for(S);
-  int gi = sizeof(R) == 4 ? 1 : 0;
+  const int gi = sizeof(R) == 4 ? 1 : 0;
   if (check_every < 1) check_every = 1;
   if (!S->graph[gi] || S->graph_iters[gi] != check_every) {
-    if (S->graph[gi]) { cudaGraphExecDestroy(S->graph[gi]); S->graph[gi] = nullptr; }
+    if (S->graph[gi]) {
+      cudaGraphExecDestroy(S->graph[gi]);
+      S->graph[gi] = nullptr;
+    }
     cudaStream_t cs;
     DGP_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     cudaGraph_t g;
     DGP_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
     int rc = DGP_OK;
-    for (int q = 0; q < check_every && rc == DGP_OK; ++q) rc = enqueue_iteration<R>(S, LL.L, LL.Ld, V, W, cs);
+    for (int q = 0; q < check_every && rc == DGP_OK; ++q)
+      rc = vec_for(S) == 2 ? enqueue_for<R, 2>(S, V, W, cs) : enqueue_for<R, 4>(S, V, W, cs);
     cudaError_t e = cudaStreamEndCapture(cs, &g);
     cudaStreamDestroy(cs);
     if (rc != DGP_OK) return rc;
@@ -1008,6 +1128,7 @@ int run_iterations(SolverPlan *S, const Vecs<R> &V, const Work &W, int check_eve
   for (int64_t launches = 0;; ++launches) {
     if (launches > max_launches) return fail(DGP_ERR_CUDA, "solver: control block never reached DONE");
     DGP_CUDA(cudaGraphLaunch(S->graph[gi], st));
+    count_launches((int64_t)KERNELS_PER_ITER * check_every);
     DGP_CUDA(cudaMemcpyAsync(h, W.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
     DGP_CUDA(cudaStreamSynchronize(st));
     if (h->state == ST_DONE) break;
@@ -1029,6 +1150,30 @@ int set_ctl(Ctl *d, double tol, int maxit, int stop_rule, cudaStream_t st, void 
   return DGP_OK;
 }
 
+template <class R, int VEC>
+void launch_init(const Layout &Ld, const Vecs<R> &V, const Work &W, cudaStream_t st) {
+  k_init<R, VEC><<<grid_of(Ld), BS, red_smem(Ld, 2), st>>>(Ld, V.x, V.r, V.rhat, V.p, W.cols);
+}
+
+// FP64 residual sweep b - A x with the solver's lane layout for its source count
+void launch_residual(SolverPlan *S, int ns, const double *d_X, const double *d_B, const int32_t *d_nodes,
+                     const double *d_w, const double *d_fpsf, float2 *r32, const Work &W, cudaStream_t st) {
+  const int vec = vec_for(S);
+  const Layout Ld = layouts_for(S, vec).Ld;
+  const size_t sm = red_smem(Ld, 1) + (sizeof(int32_t) + sizeof(double)) * 4 * Ld.nsp;
+  if (vec == 2)
+    k_residual64<2><<<grid_of(Ld), BS, sm, st>>>(Ld, ns, S->rowptr.as<int32_t>(), S->col.as<int32_t>(),
+                                                 S->KM64.as<double2>(), S->omega.as<double>(), (const double2 *)d_X,
+                                                 (const double2 *)d_B, d_nodes, d_w, (const double2 *)d_fpsf, r32,
+                                                 W.cols);
+  else
+    k_residual64<4><<<grid_of(Ld), BS, sm, st>>>(Ld, ns, S->rowptr.as<int32_t>(), S->col.as<int32_t>(),
+                                                 S->KM64.as<double2>(), S->omega.as<double>(), (const double2 *)d_X,
+                                                 (const double2 *)d_B, d_nodes, d_w, (const double2 *)d_fpsf, r32,
+                                                 W.cols);
+  count_launches(1);
+}
+
 }  // namespace
 
 SolverPlan::~SolverPlan() {
@@ -1039,7 +1184,8 @@ SolverPlan::~SolverPlan() {
 
 int solver_update(SolverPlan *S, const double *d_K, const double *d_M, cudaStream_t st) {
   const int64_t nnz = S->nnz;
-  k_cvt_km<<<g1(nnz, 256), 256, 0, st>>>(d_K, d_M, nnz, S->KM64.as<double2>(), S->KM32.as<float2>());
+  k_cvt_km<<<g1(nnz, 256), 256, 0, st>>>(d_K, d_M, S->col.as<int32_t>(), nnz, S->KM64.as<double2>(),
+                                          S->RecA32.as<Rec32>());
   DGP_CHECK_LAUNCH();
   // FSAI of tril(K + i*k*dfc*M) for every harmonic
   DevBuf im;
@@ -1049,9 +1195,10 @@ int solver_update(SolverPlan *S, const double *d_K, const double *d_M, cudaStrea
   DGP_TRY(fsai_factor_run(S->rowptr.as<int32_t>(), S->col.as<int32_t>(), d_K, im.as<double>(), S->n,
                           S->P.rowptr.as<int32_t>(), S->P.col.as<int32_t>(), S->P.mmax, S->nf,
                           S->G64.as<double2>(), 1, S->nnzG, st));
-  k_gather_gt<<<g1(S->nnzG * S->nf, 256), 256, 0, st>>>(S->G64.as<double2>(), S->P.permT.as<int32_t>(), S->nnzG,
-                                                       S->nf, S->GT64.as<double2>(), S->G32.as<float2>(),
-                                                       S->GT32.as<float2>());
+  k_gather_gt<<<g1(S->nnzG * S->nf, 256), 256, 0, st>>>(S->G64.as<double2>(), S->P.permT.as<int32_t>(),
+                                                       S->P.col.as<int32_t>(), S->P.colT.as<int32_t>(), S->nnzG,
+                                                       S->nf, S->GT64.as<double2>(), S->RecG32.as<Rec32>(),
+                                                       S->RecGT32.as<Rec32>());
   DGP_CHECK_LAUNCH();
   DGP_CUDA(cudaStreamSynchronize(st));
   return DGP_OK;
@@ -1062,7 +1209,7 @@ int solver_build(SolverPlan *S, const int32_t *d_rowptr, const int32_t *d_col, i
                  const dgp_solve_opts *opts, cudaStream_t st) {
   DGP_REQUIRE(n > 0 && nnz > 0 && nf > 0 && nf <= 65535, "solver: bad sizes");
   DGP_REQUIRE(ns_max >= 1 && ns_max <= 128, "solver: 1 <= ns_max <= 128 sources per harmonic");
-  DGP_REQUIRE(nnz < INT32_MAX, "solver: nnz must fit int32");
+  DGP_REQUIRE(nnz < INT32_MAX && n < (1 << 24), "solver: nnz must fit int32 and n < 2^24");
   S->n = n;
   S->nnz = nnz;
   S->nf = nf;
@@ -1075,7 +1222,7 @@ int solver_build(SolverPlan *S, const int32_t *d_rowptr, const int32_t *d_col, i
   DGP_CUDA(cudaMemcpyAsync(S->rowptr.p, d_rowptr, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToDevice, st));
   DGP_CUDA(cudaMemcpyAsync(S->col.p, d_col, sizeof(int32_t) * nnz, cudaMemcpyDeviceToDevice, st));
   DGP_TRY(S->KM64.alloc(sizeof(double2) * nnz));
-  DGP_TRY(S->KM32.alloc(sizeof(float2) * nnz));
+  DGP_TRY(S->RecA32.alloc(sizeof(Rec32) * nnz));
   DGP_TRY(S->omega.alloc((sizeof(double) + sizeof(float)) * nf));
   k_omega<<<g1(nf, 128), 128, 0, st>>>(nf, dfc, S->omega.as<double>(),
                                         (float *)(S->omega.as<char>() + sizeof(double) * nf));
@@ -1083,11 +1230,11 @@ int solver_build(SolverPlan *S, const int32_t *d_rowptr, const int32_t *d_col, i
   DGP_TRY(fsai_pattern_build(&S->P, S->rowptr.as<int32_t>(), S->col.as<int32_t>(), d_K, d_M, dfc, n,
                              S->opts.fsai_cap, st));
   S->nnzG = S->P.nnzG;
-  size_t gb = sizeof(double2) * (size_t)S->nnzG * nf;
-  DGP_TRY(S->G64.alloc(gb));
-  DGP_TRY(S->GT64.alloc(gb));
-  DGP_TRY(S->G32.alloc(gb / 2));
-  DGP_TRY(S->GT32.alloc(gb / 2));
+  const size_t gcount = (size_t)S->nnzG * nf;
+  DGP_TRY(S->G64.alloc(sizeof(double2) * gcount));
+  DGP_TRY(S->GT64.alloc(sizeof(double2) * gcount));
+  DGP_TRY(S->RecG32.alloc(sizeof(Rec32) * gcount));
+  DGP_TRY(S->RecGT32.alloc(sizeof(Rec32) * gcount));
   DGP_CUDA(cudaMallocHost(&S->h_ctl, sizeof(Ctl)));
   return solver_update(S, d_K, d_M, st);
 }
@@ -1099,46 +1246,43 @@ static int solve_fp64(SolverPlan *S, const double *d_B, const int32_t *d_nodes, 
   DGP_TRY(ensure_workspace(S, DGP_PREC_FP64));
   Work W = work_views(S);
   Vecs<double> V = vec_views<double>(S);
-  Layouts LL = layouts_for(S);
-  const Layout &L = LL.L;
-  size_t vbytes = sizeof(double2) * (size_t)S->ws_cols * S->n;
+  const int vec = vec_for(S);
+  const Layouts LL = layouts_for(S, vec);
+  const size_t vbytes = sizeof(double2) * (size_t)S->ws_cols * S->n;
   // b -> r (workspace layout)
   if (d_B) {
-    k_pack<double><<<g1((int64_t)S->ws_cols * S->n, 256), 256, 0, st>>>(L, ns, (const double2 *)d_B, V.r);
+    k_pack<double><<<g1((int64_t)S->ws_cols * S->n, 256), 256, 0, st>>>(S->n, S->nf, S->nsp, ns,
+                                                                         (const double2 *)d_B, V.r);
   } else {
     DGP_CUDA(cudaMemsetAsync(V.r, 0, vbytes, st));
-    k_sources<double><<<g1((int64_t)S->nf * ns, 128), 128, 0, st>>>(L, ns, d_nodes, d_w, (const double2 *)d_fpsf, V.r);
+    k_sources<double><<<g1((int64_t)S->nf * ns, 128), 128, 0, st>>>(S->n, S->nf, S->nsp, ns, d_nodes, d_w,
+                                                                      (const double2 *)d_fpsf, V.r);
   }
   DGP_CHECK_LAUNCH();
   DGP_TRY(set_ctl(W.ctl, o.tol, o.maxit, o.stop_rule, st, S->h_ctl));
-  dim3 gd((unsigned)ceil_div(LL.Ld.n, LL.Ld.rows_per_block()), LL.Ld.nf);
-  k_init<double><<<gd, BS, red_smem(LL.Ld, 2), st>>>(LL.Ld, V.r, V.x, V.r, V.rhat, V.p, W.cols);
+  if (vec == 2) launch_init<double, 2>(LL.Ld, V, W, st); else launch_init<double, 4>(LL.Ld, V, W, st);
+  DGP_CHECK_LAUNCH();
   k_stage_init<<<1, 1024, 0, st>>>(W.cols, W.ctl, S->nsp, ns);
   DGP_CHECK_LAUNCH();
   int iters = 0;
   DGP_TRY(run_iterations<double>(S, V, W, o.check_every, o.maxit, st, &iters));
   k_stage_final<<<1, 1024, 0, st>>>(W.cols, W.ctl);
-  k_unpack<double><<<g1((int64_t)S->nf * S->n * ns, 256), 256, 0, st>>>(L, ns, V.x, (double2 *)d_X);
   DGP_CHECK_LAUNCH();
-  // true FP64 residual of the returned solution, for the report
-  {
-    Layout Ld = LL.Ld;
-    size_t sm = red_smem(Ld, 1) + (sizeof(int32_t) + sizeof(double)) * 4 * Ld.nsp;
-    DGP_CUDA(cudaMemsetAsync(W.cols.acc + ACC_NR * W.cols.C, 0, sizeof(double2) * W.cols.C, st));
-    // ||b|| into bnorm
-    k_residual64<<<gd, BS, sm, st>>>(Ld, ns, S->rowptr.as<int32_t>(), S->col.as<int32_t>(), S->KM64.as<double2>(),
-                                     S->omega.as<double>(), (const double2 *)d_X, (const double2 *)d_B, d_nodes, d_w,
-                                     (const double2 *)d_fpsf, (float2 *)V.T1, W.cols);
-    DGP_CHECK_LAUNCH();
-  }
-  Ctl hc;
+  k_unpack<double><<<g1((int64_t)S->nf * S->n * ns, 256), 256, 0, st>>>(S->n, S->nf, S->nsp, ns, V.x,
+                                                                          (double2 *)d_X);
+  DGP_CHECK_LAUNCH();
+  // true FP64 residual of the returned solution, for the report (||b|| = ||r0|| since x0 = 0)
+  DGP_CUDA(cudaMemcpyAsync(W.bnorm, W.cols.err0, sizeof(double) * W.cols.C, cudaMemcpyDeviceToDevice, st));
+  DGP_CUDA(cudaMemsetAsync(W.cols.acc + ACC_NR * W.cols.C, 0, sizeof(double2) * W.cols.C, st));
+  launch_residual(S, ns, d_X, d_B, d_nodes, d_w, d_fpsf, (float2 *)V.T1, W, st);
   k_outer_norms<<<1, 1024, 0, st>>>(W.cols, W.bnorm, W.outer_err, W.ctl, 1, S->nsp, ns);
   DGP_CHECK_LAUNCH();
+  Ctl hc;
   DGP_CUDA(cudaMemcpyAsync(&hc, W.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
   DGP_CUDA(cudaStreamSynchronize(st));
   rep->iterations = iters;
   rep->refinements = 0;
-  rep->max_rel_residual = hc.max_err;  // ||b - Ax|| / ||r0|| with r0 = b (x0 = 0)
+  rep->max_rel_residual = hc.max_err;
   return hc.reason == 1 ? DGP_ERR_NOT_CONVERGED : DGP_OK;
 }
 
@@ -1149,27 +1293,25 @@ static int solve_mixed(SolverPlan *S, const double *d_B, const int32_t *d_nodes,
   DGP_TRY(ensure_workspace(S, DGP_PREC_MIXED));
   Work W = work_views(S);
   Vecs<float> V = vec_views<float>(S);
-  Layouts LL = layouts_for(S);
-  const Layout &Ld = LL.Ld;
-  dim3 gd((unsigned)ceil_div(Ld.n, Ld.rows_per_block()), Ld.nf);
-  size_t sm = red_smem(Ld, 1) + (sizeof(int32_t) + sizeof(double)) * 4 * Ld.nsp;
+  const int vec = vec_for(S);
+  const Layouts LL = layouts_for(S, vec);
   DGP_CUDA(cudaMemsetAsync(d_X, 0, sizeof(double2) * (size_t)S->nf * S->n * ns, st));
   DGP_CUDA(cudaMemsetAsync(W.cols.acc, 0, sizeof(double2) * W.cols.C * NACC, st));
   // r = b (x = 0): ||b|| per column
-  k_residual64<<<gd, BS, sm, st>>>(Ld, ns, S->rowptr.as<int32_t>(), S->col.as<int32_t>(), S->KM64.as<double2>(),
-                                   S->omega.as<double>(), (const double2 *)d_X, (const double2 *)d_B, d_nodes, d_w,
-                                   (const double2 *)d_fpsf, V.r, W.cols);
+  launch_residual(S, ns, d_X, d_B, d_nodes, d_w, d_fpsf, V.r, W, st);
   k_outer_norms<<<1, 1024, 0, st>>>(W.cols, W.bnorm, W.outer_err, W.ctl, 0, S->nsp, ns);
   DGP_CHECK_LAUNCH();
   int total_iters = 0, refinements = 0;
   double max_err = 1.0;
   Ctl *h = (Ctl *)S->h_ctl;
   int status = DGP_OK;
-  for (int ref = 0; ref < std::max(1, o.max_refine); ++ref) {
+  const int max_ref = std::max(1, o.max_refine);
+  for (int ref = 0; ref < max_ref; ++ref) {
     // inner FP32 solve on the current residual (already in V.r)
     const int inner_maxit = std::max(1, o.maxit - total_iters);
     DGP_TRY(set_ctl(W.ctl, o.inner_tol, inner_maxit, DGP_STOP_MAX_ALL, st, S->h_ctl));
-    k_init<float><<<gd, BS, red_smem(Ld, 2), st>>>(Ld, V.r, V.x, V.r, V.rhat, V.p, W.cols);
+    if (vec == 2) launch_init<float, 2>(LL.Ld, V, W, st); else launch_init<float, 4>(LL.Ld, V, W, st);
+    DGP_CHECK_LAUNCH();
     k_stage_init<<<1, 1024, 0, st>>>(W.cols, W.ctl, S->nsp, ns);
     DGP_CHECK_LAUNCH();
     int it = 0;
@@ -1177,19 +1319,22 @@ static int solve_mixed(SolverPlan *S, const double *d_B, const int32_t *d_nodes,
     total_iters += it;
     refinements += 1;
     // X += x32 ; r = b - A X in FP64
-    k_accum_x<<<g1((int64_t)S->nf * S->n * ns, 256), 256, 0, st>>>(Ld, ns, V.x, (double2 *)d_X);
-    k_residual64<<<gd, BS, sm, st>>>(Ld, ns, S->rowptr.as<int32_t>(), S->col.as<int32_t>(), S->KM64.as<double2>(),
-                                     S->omega.as<double>(), (const double2 *)d_X, (const double2 *)d_B, d_nodes, d_w,
-                                     (const double2 *)d_fpsf, V.r, W.cols);
+    k_accum_x<<<g1((int64_t)S->nf * S->n * ns, 256), 256, 0, st>>>(S->n, S->nf, S->nsp, ns, V.x, (double2 *)d_X);
+    DGP_CHECK_LAUNCH();
+    launch_residual(S, ns, d_X, d_B, d_nodes, d_w, d_fpsf, V.r, W, st);
     k_outer_norms<<<1, 1024, 0, st>>>(W.cols, W.bnorm, W.outer_err, W.ctl, 1, S->nsp, ns);
     DGP_CHECK_LAUNCH();
     DGP_CUDA(cudaMemcpyAsync(h, W.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
     DGP_CUDA(cudaStreamSynchronize(st));
     max_err = h->max_err;
     if (max_err < o.tol) break;
-    if (total_iters >= o.maxit) { status = DGP_ERR_NOT_CONVERGED; break; }
-    if (ref == std::max(1, o.max_refine) - 1) status = DGP_ERR_NOT_CONVERGED;
+    if (total_iters >= o.maxit || ref == max_ref - 1) {
+      status = DGP_ERR_NOT_CONVERGED;
+      break;
+    }
   }
+  k_status_outer<<<g1(W.cols.C, 256), 256, 0, st>>>(W.cols, W.outer_err, o.tol, S->nsp, ns);
+  DGP_CHECK_LAUNCH();
   rep->iterations = total_iters;
   rep->refinements = refinements;
   rep->max_rel_residual = max_err;
@@ -1205,10 +1350,21 @@ int solver_solve(SolverPlan *S, const double *d_B, const int32_t *d_nodes, const
   DGP_REQUIRE(o.tol > 0 && o.maxit >= 1, "solve: tol > 0 and maxit >= 1 required");
   DGP_REQUIRE(o.precision == DGP_PREC_FP64 || o.precision == DGP_PREC_MIXED, "solve: unknown precision");
   if (o.check_every < 1) o.check_every = 1;
+  if (d_nodes) {
+    DevBuf bad;
+    DGP_TRY(bad.alloc(sizeof(int)));
+    DGP_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), st));
+    k_check_nodes<<<g1(4 * ns, 128), 128, 0, st>>>(d_nodes, ns, S->n, bad.as<int>());
+    DGP_CHECK_LAUNCH();
+    int hb = 0;
+    DGP_CUDA(cudaMemcpyAsync(&hb, bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    DGP_CUDA(cudaStreamSynchronize(st));
+    if (hb) return fail(DGP_ERR_ARG, "solve: source node index out of range");
+  }
   dgp_solve_report local{};
   dgp_solve_report *r = rep ? rep : &local;
-  int rc = o.precision == DGP_PREC_FP64 ? solve_fp64(S, d_B, d_nodes, d_w, d_fpsf, d_X, ns, o, r, st)
-                                        : solve_mixed(S, d_B, d_nodes, d_w, d_fpsf, d_X, ns, o, r, st);
+  const int rc = o.precision == DGP_PREC_FP64 ? solve_fp64(S, d_B, d_nodes, d_w, d_fpsf, d_X, ns, o, r, st)
+                                              : solve_mixed(S, d_B, d_nodes, d_w, d_fpsf, d_X, ns, o, r, st);
   if (rc != DGP_OK && rc != DGP_ERR_NOT_CONVERGED) return rc;
   // per-column statuses for the caller (harmonic-major, ns columns per harmonic)
   std::vector<int> hs((size_t)S->ws_cols);
@@ -1219,7 +1375,6 @@ int solver_solve(SolverPlan *S, const double *d_B, const int32_t *d_nodes, const
   for (int k = 0; k < S->nf; ++k)
     for (int s = 0; s < ns; ++s) {
       int v = hs[(size_t)k * S->nsp + s];
-      if (o.precision == DGP_PREC_MIXED) v = (r->max_rel_residual < o.tol) ? DGP_COL_CONVERGED : v;
       if (v == DGP_COL_ZERO_RHS) v = DGP_COL_CONVERGED;  // x = 0 solves b = 0 exactly
       out[(size_t)k * ns + s] = v;
       bad += v != DGP_COL_CONVERGED;
@@ -1241,8 +1396,6 @@ int solver_profile(SolverPlan *S, int which, int reps, float *ms, double *bytes,
   DGP_REQUIRE(reps >= 1 && which >= 0 && which <= 3, "profile: bad arguments");
   Vecs<float> V = vec_views<float>(S);
   Work W = work_views(S);
-  Layouts LL = layouts_for(S);
-  const Layout &L = LL.L, &Ld = LL.Ld;
   DevBuf dctl;
   DGP_TRY(dctl.alloc(sizeof(Ctl)));
   Ctl hc{};
@@ -1250,37 +1403,30 @@ int solver_profile(SolverPlan *S, int which, int reps, float *ms, double *bytes,
   hc.maxit = 1 << 30;
   DGP_CUDA(cudaMemcpyAsync(dctl.p, &hc, sizeof(Ctl), cudaMemcpyHostToDevice, st));
   Ctl *ctl = dctl.as<Ctl>();
+  const Layouts LL = layouts_for(S, 2);
+  const Layout &L = LL.L, &Ld = LL.Ld;
   const float *om = (const float *)(S->omega.as<char>() + sizeof(double) * S->nf);
-  dim3 gr((unsigned)ceil_div(L.n, L.rows_per_block()), L.nf);
-  dim3 gd((unsigned)ceil_div(Ld.n, Ld.rows_per_block()), Ld.nf);
+  OpA32 A{S->rowptr.as<int32_t>(), S->RecA32.as<Rec32>(), om};
+  OpG32 G{S->P.rowptr.as<int32_t>(), S->RecG32.as<Rec32>(), S->nnzG};
   const double vec = 8.0 * (double)S->nf * S->n * S->nsp;
   auto launch = [&]() {
     switch (which) {
-      case 0:  // t = A z
-        k_spmm_A<float, false><<<gr, BS, 0, st>>>(L, S->rowptr.as<int32_t>(), S->col.as<int32_t>(),
-                                                  S->KM32.as<float2>(), om, V.z, V.t, nullptr, W.cols, ctl,
-                                                  ST_RUNNING);
-        break;
-      case 1:  // T1 = G p
-        k_spmm_G<float, 0><<<gr, BS, 0, st>>>(L, S->P.rowptr.as<int32_t>(), S->P.col.as<int32_t>(),
-                                              S->G32.as<float2>(), S->nnzG, V.p, V.T1, nullptr, W.cols, ctl,
-                                              ST_RUNNING);
-        break;
+      case 0: k_spmm<float, 2, 0><<<grid_of(L), BS, 0, st>>>(L, A, V.z, V.t, nullptr, W.cols, ctl); break;
+      case 1: k_spmm<float, 2, 0><<<grid_of(L), BS, 0, st>>>(L, G, V.p, V.T1, nullptr, W.cols, ctl); break;
       case 2:
-        k_update_xrp<float><<<gd, BS, red_smem(Ld, 2), st>>>(Ld, V.x, V.h, V.z, V.r, V.s, V.t, V.p, V.v, V.rhat,
-                                                             W.cols, ctl);
+        k_update_xrp<float, 2><<<grid_of(Ld), BS, red_smem(Ld, 2), st>>>(Ld, V.x, V.h, V.z, V.r, V.s, V.t, V.p, V.v,
+                                                                         V.rhat, W.cols, ctl);
         break;
-      default:
-        k_update_hs<float><<<gd, BS, red_smem(Ld, 1), st>>>(Ld, V.x, V.h, V.r, V.v, V.s, W.cols, ctl);
-        break;
+      default: k_update_s<float, 2><<<grid_of(Ld), BS, red_smem(Ld, 1), st>>>(Ld, V.r, V.v, V.s, W.cols, ctl); break;
     }
   };
   switch (which) {
-    case 0: *bytes = 2 * vec + (double)S->nf * (12.0 * S->nnz + 4.0 * (S->n + 1)); break;
-    case 1: *bytes = 2 * vec + (double)S->nf * (12.0 * S->nnzG + 4.0 * (S->n + 1)); break;
-    case 2: *bytes = 12 * vec; break;
-    default: *bytes = 6 * vec; break;
+    case 0: *bytes = 2 * vec + (double)S->nf * (16.0 * S->nnz + 4.0 * (S->n + 1)); break;
+    case 1: *bytes = 2 * vec + (double)S->nf * (16.0 * S->nnzG + 4.0 * (S->n + 1)); break;
+    case 2: *bytes = 11 * vec; break;
+    default: *bytes = 3 * vec; break;
   }
+  DGP_REQUIRE(S->nsp <= 64, "profile: the timed kernels use two sources per lane (nsp <= 64)");
   launch();  // warm
   DGP_CHECK_LAUNCH();
   cudaEvent_t e0, e1;
@@ -1295,6 +1441,7 @@ int solver_profile(SolverPlan *S, int which, int reps, float *ms, double *bytes,
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   DGP_CHECK_LAUNCH();
+  count_launches(reps + 1);
   DGP_CUDA(cudaMemsetAsync(W.cols.acc, 0, sizeof(double2) * W.cols.C * NACC, st));
   DGP_CUDA(cudaStreamSynchronize(st));
   *ms = t / reps;
@@ -1304,24 +1451,26 @@ int solver_profile(SolverPlan *S, int which, int reps, float *ms, double *bytes,
 // --------------------------------------------------- standalone operators
 int spmm_A_f64(const int32_t *rowptr, const int32_t *col, const double2 *KM, const double *omega, int64_t n,
                int32_t nf, int32_t ns, const double2 *X, double2 *Y, cudaStream_t st) {
-  DGP_REQUIRE(ns >= 2 && (ns & (ns - 1)) == 0 && ns <= 128,
-              "spmm_A: ns must be a power of two in 2..128 (pad the source axis)");
-  Layout L = make_layout(n, nf, ns, 4);
-  dim3 gr((unsigned)ceil_div(n, L.rows_per_block()), nf);
+  DGP_REQUIRE(ns >= 2 && (ns & (ns - 1)) == 0 && ns <= 64,
+              "spmm_A: ns must be a power of two in 2..64 (pad the source axis)");
+  const int lpr = ns / 2, rpw = 32 / lpr;
+  Layout L{n, nf, ns, lpr, rpw, std::max(1, 64 / (WARPS * rpw))};
   Cols c{};
-  k_spmm_A<double, false><<<gr, BS, 0, st>>>(L, rowptr, col, KM, omega, X, Y, nullptr, c, nullptr, 0);
+  OpA64 A{rowptr, col, KM, omega};
+  k_spmm<double, 2, 0><<<grid_of(L), BS, 0, st>>>(L, A, X, Y, nullptr, c, nullptr);
   DGP_CHECK_LAUNCH();
   return DGP_OK;
 }
 
 int fsai_apply_f64(const int32_t *rowptr, const int32_t *col, const double2 *G, int64_t n, int64_t nnzG, int32_t nf,
                    int32_t ns, const double2 *X, double2 *Y, cudaStream_t st) {
-  DGP_REQUIRE(ns >= 2 && (ns & (ns - 1)) == 0 && ns <= 128,
-              "fsai_apply: ns must be a power of two in 2..128 (pad the source axis)");
-  Layout L = make_layout(n, nf, ns, 4);
-  dim3 gr((unsigned)ceil_div(n, L.rows_per_block()), nf);
+  DGP_REQUIRE(ns >= 2 && (ns & (ns - 1)) == 0 && ns <= 64,
+              "fsai_apply: ns must be a power of two in 2..64 (pad the source axis)");
+  const int lpr = ns / 2, rpw = 32 / lpr;
+  Layout L{n, nf, ns, lpr, rpw, std::max(1, 64 / (WARPS * rpw))};
   Cols c{};
-  k_spmm_G<double, 0><<<gr, BS, 0, st>>>(L, rowptr, col, G, nnzG, X, Y, nullptr, c, nullptr, 0);
+  OpG64 Gop{rowptr, col, G, nnzG};
+  k_spmm<double, 2, 0><<<grid_of(L), BS, 0, st>>>(L, Gop, X, Y, nullptr, c, nullptr);
   DGP_CHECK_LAUNCH();
   return DGP_OK;
 }

@@ -1,6 +1,7 @@
 // C ABI of libdogpup_b200: argument checks, error reporting, plan handles.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -14,6 +15,10 @@
 namespace dgp {
 
 static thread_local std::string g_err;
+static std::atomic<int64_t> g_launches{0};
+
+void count_launches(int64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+int64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 void set_error(const std::string &msg) { g_err = msg; }
 
@@ -121,6 +126,8 @@ const char *dgp_status_string(int s) {
 }
 
 int dgp_version(void) { return 10000; }
+
+int64_t dgp_kernel_launches(void) { return launch_count(); }
 
 // ------------------------------------------------------------ mex layouts
 int dgp_smv_mex(double *d_out_real, double *d_out_imag, const double *d_x_real, const double *d_x_imag,
@@ -248,7 +255,7 @@ int dgp_solver_memory(dgp_solver_t s, int64_t *bytes) {
   if (!s || !bytes) return fail(DGP_ERR_ARG, "solver_memory: null pointer");
   const SolverPlan &p = s->plan;
   int64_t b = 0;
-  const DevBuf *bufs[] = {&p.rowptr, &p.col, &p.KM64, &p.KM32, &p.omega, &p.G64, &p.GT64, &p.G32, &p.GT32,
+  const DevBuf *bufs[] = {&p.rowptr, &p.col, &p.KM64, &p.RecA32, &p.omega, &p.G64, &p.GT64, &p.RecG32, &p.RecGT32,
                           &p.P.rowptr, &p.P.col, &p.P.rowptrT, &p.P.colT, &p.P.permT, &p.scal, &p.ctl, &p.status};
   for (auto *d : bufs) b += (int64_t)d->bytes;
   for (auto &v : p.vec) b += (int64_t)v.bytes;

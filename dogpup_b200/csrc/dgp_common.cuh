@@ -22,7 +22,15 @@ int cuda_fail(cudaError_t e, const char *what, const char *file, int line);
     if (e_ != cudaSuccess) return ::dgp::cuda_fail(e_, #call, __FILE__, __LINE__); \
   } while (0)
 
-#define DGP_CHECK_LAUNCH() DGP_CUDA(cudaGetLastError())
+// kernels launched by this library (graph-contained kernels included)
+void count_launches(int64_t n);
+int64_t launch_count();
+
+#define DGP_CHECK_LAUNCH()                                                     \
+  do {                                                                         \
+    ::dgp::count_launches(1);                                                  \
+    DGP_CUDA(cudaGetLastError());                                              \
+  } while (0)
 
 #define DGP_TRY(call)                                                          \
   do {                                                                         \

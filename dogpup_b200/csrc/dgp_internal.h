@@ -57,15 +57,16 @@ struct SolverPlan {
   double dfc = 0;
   dgp_solve_opts opts{};
   DevBuf rowptr, col;            // A pattern
-  DevBuf KM64, KM32;             // interleaved (K, M) per slot
+  DevBuf KM64;                   // interleaved (K, M) per slot, FP64
+  DevBuf RecA32;                 // FP32 path: one 16-byte (col, K, M) record per slot
   DevBuf omega;                  // [nf] k * dfc
   FsaiPattern P;
-  DevBuf G64, GT64, G32, GT32;   // [nf][nnzG] complex
+  DevBuf G64, GT64;              // [nf][nnzG] complex128
+  DevBuf RecG32, RecGT32;        // FP32 path: [nf][nnzG] 16-byte (col, Re, Im) records
   // workspace (allocated lazily per precision)
   int ws_prec = -1;
   int64_t ws_cols = 0;
   DevBuf vec[12];                // solver vectors
-  DevBuf x64, r64;               // mixed: FP64 solution and residual work
   DevBuf scal;                   // per-column scalars
   DevBuf ctl;                    // control block
   DevBuf status;                 // per-column status

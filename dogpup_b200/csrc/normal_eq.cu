@@ -518,6 +518,7 @@ int cholesky_solve_run(double *H, int64_t n, int64_t ldh, double *x, cudaStream_
     const int nb = (int)std::min<int64_t>(NB, n - k0);
     k_potrf_diag<<<1, 256, 0, st>>>(H, ldh, k0, nb, errb.as<int>());
     const int64_t rest = n - k0 - nb;
+    count_launches(rest > 0 ? 3 : 1);
     if (rest > 0) {
       k_trsm_panel<<<(unsigned)ceil_div(rest, 128), 128, 0, st>>>(H, ldh, k0, nb, n);
       const int64_t T = ceil_div(rest, NB);
@@ -528,12 +529,14 @@ int cholesky_solve_run(double *H, int64_t n, int64_t ldh, double *x, cudaStream_
   for (int64_t k0 = 0; k0 < n; k0 += NB) {  // L y = b
     const int nb = (int)std::min<int64_t>(NB, n - k0);
     k_trsv_diag<<<1, 32, 0, st>>>(H, ldh, k0, nb, x, 1);
+    count_launches(n - k0 - nb > 0 ? 2 : 1);
     if (n - k0 - nb > 0) k_trsv_fwd_update<<<(unsigned)ceil_div(n - k0 - nb, 256), 256, 0, st>>>(H, ldh, k0, nb, n, x);
   }
   for (int64_t k0 = ((n - 1) / NB) * NB; k0 >= 0; k0 -= NB) {  // L' x = y
     const int nb = (int)std::min<int64_t>(NB, n - k0);
     if (n - k0 - nb > 0) k_trsv_bwd_update<<<nb, 256, 0, st>>>(H, ldh, k0, nb, n, x);
     k_trsv_diag<<<1, 32, 0, st>>>(H, ldh, k0, nb, x, 0);
+    count_launches(n - k0 - nb > 0 ? 2 : 1);
   }
   DGP_CHECK_LAUNCH();
   int herr = 0;

@@ -54,6 +54,9 @@ enum {
 const char *dgp_last_error(void);
 const char *dgp_status_string(int status);
 int dgp_version(void);
+/* Number of kernels this library has launched in the process so far
+ * (kernels inside its CUDA graphs included). */
+int64_t dgp_kernel_launches(void);
 
 /* ====================================================================== *
  *  Drop-in host functions of the reference mex sources.  Same names,
