@@ -347,11 +347,11 @@ def run_ours(a, rank, world, local_rank):
                "ms_per_step": ems / a.steps}
 
     # ---- roofline: the dominant sweep kernel, CUDA-event timed on the solver's stream
-    launches = {0: 2, 1: 5, 2: 1, 3: 1}  # per BiCGSTAB iteration: A SpMM x2, G SpMM x5, x/r/p, h/s
+    per_iter = {0: 2, 1: 5, 2: 1, 3: 1}  # per BiCGSTAB iteration: A SpMM x2, G SpMM x5, x/r/p, s
     names = {0: "k_spmm_A<float> (K + i w M SpMM)", 1: "k_spmm_G<float> (FSAI apply)",
              2: "k_update_xrp<float>", 3: "k_update_s<float>"}
-    prof = {q: solver.profile_kernel(q, 5) for q in launches}
-    dom = max(prof, key=lambda q: prof[q][0] * launches[q])
+    prof = {q: solver.profile_kernel(q, 5) for q in per_iter}
+    dom = max(prof, key=lambda q: prof[q][0] * per_iter[q])
     pk = json.load(open(ROOT / "MEASURED_PEAKS.json")) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = pk.get("hbm_gbs", 6650.0)
     ach = prof[dom][1] / (prof[dom][0] * 1e-3) / 1e9

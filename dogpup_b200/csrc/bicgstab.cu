@@ -278,26 +278,21 @@ __device__ inline void row_spmv(int nsp, const int32_t *__restrict__ rowptr, int
 #pragma unroll
   for (int v = 0; v < VEC; ++v) y[v] = czero<C>();
   const int b = __ldg(rowptr + i), e = __ldg(rowptr + i + 1);
+  // gathers in flight per lane: UNR nonzeros x VEC complex (register budget bounds UNR*VEC)
+  constexpr int UNR = VEC >= 8 ? 2 : 4;
   int p = b;
-  for (; p + 4 <= e; p += 4) {
-    int j0, j1, j2, j3;
-    C a0, a1, a2, a3;
-    cf.get(p, j0, a0);
-    cf.get(p + 1, j1, a1);
-    cf.get(p + 2, j2, a2);
-    cf.get(p + 3, j3, a3);
-    C x0[VEC], x1[VEC], x2[VEC], x3[VEC];
-    ldgv<VEC>(Xk + j0 * nsp, x0);
-    ldgv<VEC>(Xk + j1 * nsp, x1);
-    ldgv<VEC>(Xk + j2 * nsp, x2);
-    ldgv<VEC>(Xk + j3 * nsp, x3);
+  for (; p + UNR <= e; p += UNR) {
+    int j[UNR];
+    C a[UNR];
 #pragma unroll
-    for (int v = 0; v < VEC; ++v) {
-      y[v] = cfmaT(a0, x0[v], y[v]);
-      y[v] = cfmaT(a1, x1[v], y[v]);
-      y[v] = cfmaT(a2, x2[v], y[v]);
-      y[v] = cfmaT(a3, x3[v], y[v]);
-    }
+    for (int u = 0; u < UNR; ++u) cf.get(p + u, j[u], a[u]);
+    C xs[UNR][VEC];
+#pragma unroll
+    for (int u = 0; u < UNR; ++u) ldgv<VEC>(Xk + j[u] * nsp, xs[u]);
+#pragma unroll
+    for (int u = 0; u < UNR; ++u)
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) y[v] = cfmaT(a[u], xs[u][v], y[v]);
   }
   for (; p < e; ++p) {
     int j;
@@ -1042,54 +1037,61 @@ Layouts layouts_for(const SolverPlan *S, int vec) {
   return x;
 }
 
-inline int vec_for(const SolverPlan *S) { return S->nsp <= 64 ? 2 : 4; }
+// complex values per lane: more per lane amortises each nonzero's coefficient load over more
+// right-hand sides (FP32 up to 8, FP64 up to 4 for register room)
+inline int vec_for(const SolverPlan *S, bool fp32) { return std::min(S->nsp, fp32 ? 8 : 4); }
 
 dim3 grid_of(const Layout &L) { return dim3((unsigned)ceil_div(L.n, L.rows_per_block()), (unsigned)L.nf); }
 
 // one BiCGSTAB iteration (dMesh.m:1295-1340) enqueued on st: KERNELS_PER_ITER launches
-template <class R, int VEC, class OpA, class OpG>
-void enqueue_iteration(const Layouts &LL, const OpA &A, const OpG &G, const OpG &GT, const Vecs<R> &V,
+// lane widths: plain SpMM sweeps VS, SpMM sweeps with dot products VD, vector updates 2
+constexpr int VU = 2;
+
+// one BiCGSTAB iteration (dMesh.m:1295-1340) enqueued on st: KERNELS_PER_ITER launches
+template <class R, int VS, int VD, class OpA, class OpG>
+void enqueue_iteration(const SolverPlan *S, const OpA &A, const OpG &G, const OpG &GT, const Vecs<R> &V,
                        const Work &W, cudaStream_t st) {
-  const Layout &L = LL.L, &Ld = LL.Ld;
+  const Layout Ls = layouts_for(S, VS).L, Lsd = layouts_for(S, VD).Ld;
+  const Layout Lu = layouts_for(S, VU).L, Lud = layouts_for(S, VU).Ld;
   Ctl *ctl = W.ctl;
   // T1 = G p ; h = G^T T1                                       (:1295-1296)
-  k_spmm<R, VEC, 0><<<grid_of(L), BS, 0, st>>>(L, G, V.p, V.T1, nullptr, W.cols, ctl);
-  k_spmm<R, VEC, 0><<<grid_of(L), BS, 0, st>>>(L, GT, V.T1, V.h, nullptr, W.cols, ctl);
+  k_spmm<R, VS, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, G, V.p, V.T1, nullptr, W.cols, ctl);
+  k_spmm<R, VS, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, GT, V.T1, V.h, nullptr, W.cols, ctl);
   // v = A h, d1 = v.r0^                                         (:1301, :1304)
-  k_spmm<R, VEC, 1><<<grid_of(Ld), BS, red_smem(Ld, 1), st>>>(Ld, A, V.h, V.v, V.rhat, W.cols, ctl);
+  k_spmm<R, VD, 1><<<grid_of(Lsd), BS, red_smem(Lsd, 1), st>>>(Lsd, A, V.h, V.v, V.rhat, W.cols, ctl);
   k_stage_alpha<<<1, 1024, 0, st>>>(W.cols, ctl);
   // s = r - alpha v ; ||s||                                     (:1306-1308)
-  k_update_s<R, VEC><<<grid_of(Ld), BS, red_smem(Ld, 1), st>>>(Ld, V.r, V.v, V.s, W.cols, ctl);
+  k_update_s<R, VU><<<grid_of(Lud), BS, red_smem(Lud, 1), st>>>(Lud, V.r, V.v, V.s, W.cols, ctl);
   k_stage_check_s<<<1, 1024, 0, st>>>(W.cols, ctl);
   // Gs = G s ; z = G^T Gs ; t = A z ; (G t).Gs, (G t).(G t)     (:1315-1325)
-  k_spmm<R, VEC, 0><<<grid_of(L), BS, 0, st>>>(L, G, V.s, V.T1, nullptr, W.cols, ctl);
-  k_spmm<R, VEC, 0><<<grid_of(L), BS, 0, st>>>(L, GT, V.T1, V.z, nullptr, W.cols, ctl);
-  k_spmm<R, VEC, 0><<<grid_of(L), BS, 0, st>>>(L, A, V.z, V.t, nullptr, W.cols, ctl);
-  k_spmm<R, VEC, 2><<<grid_of(Ld), BS, red_smem(Ld, 2), st>>>(Ld, G, V.t, nullptr, V.T1, W.cols, ctl);
+  k_spmm<R, VS, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, G, V.s, V.T1, nullptr, W.cols, ctl);
+  k_spmm<R, VS, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, GT, V.T1, V.z, nullptr, W.cols, ctl);
+  k_spmm<R, VS, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, A, V.z, V.t, nullptr, W.cols, ctl);
+  k_spmm<R, VD, 2><<<grid_of(Lsd), BS, red_smem(Lsd, 2), st>>>(Lsd, G, V.t, nullptr, V.T1, W.cols, ctl);
   k_stage_omega<<<1, 1024, 0, st>>>(W.cols, ctl);
   // x += alpha h + om z ; r = s - om t ; p -= om v ; ||r|| ; r0^.r   (:1305, :1327-1337)
-  k_update_xrp<R, VEC><<<grid_of(Ld), BS, red_smem(Ld, 2), st>>>(Ld, V.x, V.h, V.z, V.r, V.s, V.t, V.p, V.v, V.rhat,
-                                                                 W.cols, ctl);
+  k_update_xrp<R, VU><<<grid_of(Lud), BS, red_smem(Lud, 2), st>>>(Lud, V.x, V.h, V.z, V.r, V.s, V.t, V.p, V.v,
+                                                                  V.rhat, W.cols, ctl);
   k_stage_check_r<<<1, 1024, 0, st>>>(W.cols, ctl);
   k_stage_count<<<1, 1024, 0, st>>>(W.cols, ctl);
   // p = r + beta p                                              (:1340)
-  k_update_p<R, VEC><<<grid_of(L), BS, 0, st>>>(L, V.r, V.p, W.cols, ctl);
+  k_update_p<R, VU><<<grid_of(Lu), BS, 0, st>>>(Lu, V.r, V.p, W.cols, ctl);
 }
 
-template <class R, int VEC>
+template <class R, int VS>
 int enqueue_for(SolverPlan *S, const Vecs<R> &V, const Work &W, cudaStream_t st) {
-  const Layouts LL = layouts_for(S, VEC);
+  constexpr int VD = VS < 4 ? VS : 4;
   const int32_t *rp = S->rowptr.as<int32_t>();
   if constexpr (sizeof(R) == 4) {
     OpA32 A{rp, S->RecA32.as<Rec32>(), (const float *)(S->omega.as<char>() + sizeof(double) * S->nf)};
     OpG32 G{S->P.rowptr.as<int32_t>(), S->RecG32.as<Rec32>(), S->nnzG};
     OpG32 GT{S->P.rowptrT.as<int32_t>(), S->RecGT32.as<Rec32>(), S->nnzG};
-    enqueue_iteration<R, VEC>(LL, A, G, GT, V, W, st);
+    enqueue_iteration<R, VS, VD>(S, A, G, GT, V, W, st);
   } else {
     OpA64 A{rp, S->col.as<int32_t>(), S->KM64.as<double2>(), S->omega.as<double>()};
     OpG64 G{S->P.rowptr.as<int32_t>(), S->P.col.as<int32_t>(), S->G64.as<double2>(), S->nnzG};
     OpG64 GT{S->P.rowptrT.as<int32_t>(), S->P.colT.as<int32_t>(), S->GT64.as<double2>(), S->nnzG};
-    enqueue_iteration<R, VEC>(LL, A, G, GT, V, W, st);
+    enqueue_iteration<R, VS, VD>(S, A, G, GT, V, W, st);
   }
   DGP_CUDA(cudaGetLastError());
   return DGP_OK;
@@ -1112,7 +1114,13 @@ int run_iterations(SolverPlan *S, const Vecs<R> &V, const Work &W, int check_eve
     DGP_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
     int rc = DGP_OK;
     for (int q = 0; q < check_every && rc == DGP_OK; ++q)
-      rc = vec_for(S) == 2 ? enqueue_for<R, 2>(S, V, W, cs) : enqueue_for<R, 4>(S, V, W, cs);
+      switch (vec_for(S, sizeof(R) == 4)) {
+        case 2: rc = enqueue_for<R, 2>(S, V, W, cs); break;
+        case 4: rc = enqueue_for<R, 4>(S, V, W, cs); break;
+        default:
+          if constexpr (sizeof(R) == 4) rc = enqueue_for<R, 8>(S, V, W, cs);
+          break;
+      }
     cudaError_t e = cudaStreamEndCapture(cs, &g);
     cudaStreamDestroy(cs);
     if (rc != DGP_OK) return rc;
@@ -1158,7 +1166,7 @@ void launch_init(const Layout &Ld, const Vecs<R> &V, const Work &W, cudaStream_t
 // FP64 residual sweep b - A x with the solver's lane layout for its source count
 void launch_residual(SolverPlan *S, int ns, const double *d_X, const double *d_B, const int32_t *d_nodes,
                      const double *d_w, const double *d_fpsf, float2 *r32, const Work &W, cudaStream_t st) {
-  const int vec = vec_for(S);
+  const int vec = vec_for(S, false);
   const Layout Ld = layouts_for(S, vec).Ld;
   const size_t sm = red_smem(Ld, 1) + (sizeof(int32_t) + sizeof(double)) * 4 * Ld.nsp;
   if (vec == 2)
@@ -1246,7 +1254,7 @@ static int solve_fp64(SolverPlan *S, const double *d_B, const int32_t *d_nodes, 
   DGP_TRY(ensure_workspace(S, DGP_PREC_FP64));
   Work W = work_views(S);
   Vecs<double> V = vec_views<double>(S);
-  const int vec = vec_for(S);
+  const int vec = vec_for(S, false);
   const Layouts LL = layouts_for(S, vec);
   const size_t vbytes = sizeof(double2) * (size_t)S->ws_cols * S->n;
   // b -> r (workspace layout)
@@ -1260,7 +1268,7 @@ static int solve_fp64(SolverPlan *S, const double *d_B, const int32_t *d_nodes, 
   }
   DGP_CHECK_LAUNCH();
   DGP_TRY(set_ctl(W.ctl, o.tol, o.maxit, o.stop_rule, st, S->h_ctl));
-  if (vec == 2) launch_init<double, 2>(LL.Ld, V, W, st); else launch_init<double, 4>(LL.Ld, V, W, st);
+  launch_init<double, VU>(layouts_for(S, VU).Ld, V, W, st);
   DGP_CHECK_LAUNCH();
   k_stage_init<<<1, 1024, 0, st>>>(W.cols, W.ctl, S->nsp, ns);
   DGP_CHECK_LAUNCH();
@@ -1293,7 +1301,7 @@ static int solve_mixed(SolverPlan *S, const double *d_B, const int32_t *d_nodes,
   DGP_TRY(ensure_workspace(S, DGP_PREC_MIXED));
   Work W = work_views(S);
   Vecs<float> V = vec_views<float>(S);
-  const int vec = vec_for(S);
+  const int vec = vec_for(S, true);
   const Layouts LL = layouts_for(S, vec);
   DGP_CUDA(cudaMemsetAsync(d_X, 0, sizeof(double2) * (size_t)S->nf * S->n * ns, st));
   DGP_CUDA(cudaMemsetAsync(W.cols.acc, 0, sizeof(double2) * W.cols.C * NACC, st));
@@ -1310,7 +1318,7 @@ static int solve_mixed(SolverPlan *S, const double *d_B, const int32_t *d_nodes,
     // inner FP32 solve on the current residual (already in V.r)
     const int inner_maxit = std::max(1, o.maxit - total_iters);
     DGP_TRY(set_ctl(W.ctl, o.inner_tol, inner_maxit, DGP_STOP_MAX_ALL, st, S->h_ctl));
-    if (vec == 2) launch_init<float, 2>(LL.Ld, V, W, st); else launch_init<float, 4>(LL.Ld, V, W, st);
+    launch_init<float, VU>(layouts_for(S, VU).Ld, V, W, st);
     DGP_CHECK_LAUNCH();
     k_stage_init<<<1, 1024, 0, st>>>(W.cols, W.ctl, S->nsp, ns);
     DGP_CHECK_LAUNCH();
@@ -1388,6 +1396,25 @@ int solver_solve(SolverPlan *S, const double *d_B, const int32_t *d_nodes, const
 }
 
 // ------------------------------------------------------ kernel timing hook
+namespace {
+template <int VEC>
+void profile_launch(int which, const SolverPlan *S, const OpA32 &A, const OpG32 &G, const Vecs<float> &V,
+                    const Work &W, const Ctl *ctl, cudaStream_t st) {
+  const Layout L = layouts_for(S, VEC).L, Lud = layouts_for(S, VU).Ld;
+  switch (which) {
+    case 0: k_spmm<float, VEC, 0><<<grid_of(L), BS, 0, st>>>(L, A, V.z, V.t, nullptr, W.cols, ctl); break;
+    case 1: k_spmm<float, VEC, 0><<<grid_of(L), BS, 0, st>>>(L, G, V.p, V.T1, nullptr, W.cols, ctl); break;
+    case 2:
+      k_update_xrp<float, VU><<<grid_of(Lud), BS, red_smem(Lud, 2), st>>>(Lud, V.x, V.h, V.z, V.r, V.s, V.t, V.p,
+                                                                          V.v, V.rhat, W.cols, ctl);
+      break;
+    default:
+      k_update_s<float, VU><<<grid_of(Lud), BS, red_smem(Lud, 1), st>>>(Lud, V.r, V.v, V.s, W.cols, ctl);
+      break;
+  }
+}
+}  // namespace
+
 // Times one sweep kernel of the complex-FP32 iteration on the solver's own
 // workspace (same shapes and launch configuration as inside the solve) with
 // CUDA events on `st`, and returns its algorithmic bytes per launch.
@@ -1403,30 +1430,24 @@ int solver_profile(SolverPlan *S, int which, int reps, float *ms, double *bytes,
   hc.maxit = 1 << 30;
   DGP_CUDA(cudaMemcpyAsync(dctl.p, &hc, sizeof(Ctl), cudaMemcpyHostToDevice, st));
   Ctl *ctl = dctl.as<Ctl>();
-  const Layouts LL = layouts_for(S, 2);
-  const Layout &L = LL.L, &Ld = LL.Ld;
+  const int vec = vec_for(S, true);
   const float *om = (const float *)(S->omega.as<char>() + sizeof(double) * S->nf);
   OpA32 A{S->rowptr.as<int32_t>(), S->RecA32.as<Rec32>(), om};
   OpG32 G{S->P.rowptr.as<int32_t>(), S->RecG32.as<Rec32>(), S->nnzG};
-  const double vec = 8.0 * (double)S->nf * S->n * S->nsp;
+  const double pass = 8.0 * (double)S->nf * S->n * S->nsp;
   auto launch = [&]() {
-    switch (which) {
-      case 0: k_spmm<float, 2, 0><<<grid_of(L), BS, 0, st>>>(L, A, V.z, V.t, nullptr, W.cols, ctl); break;
-      case 1: k_spmm<float, 2, 0><<<grid_of(L), BS, 0, st>>>(L, G, V.p, V.T1, nullptr, W.cols, ctl); break;
-      case 2:
-        k_update_xrp<float, 2><<<grid_of(Ld), BS, red_smem(Ld, 2), st>>>(Ld, V.x, V.h, V.z, V.r, V.s, V.t, V.p, V.v,
-                                                                         V.rhat, W.cols, ctl);
-        break;
-      default: k_update_s<float, 2><<<grid_of(Ld), BS, red_smem(Ld, 1), st>>>(Ld, V.r, V.v, V.s, W.cols, ctl); break;
+    switch (vec) {
+      case 2: profile_launch<2>(which, S, A, G, V, W, ctl, st); break;
+      case 4: profile_launch<4>(which, S, A, G, V, W, ctl, st); break;
+      default: profile_launch<8>(which, S, A, G, V, W, ctl, st); break;
     }
   };
   switch (which) {
-    case 0: *bytes = 2 * vec + (double)S->nf * (16.0 * S->nnz + 4.0 * (S->n + 1)); break;
-    case 1: *bytes = 2 * vec + (double)S->nf * (16.0 * S->nnzG + 4.0 * (S->n + 1)); break;
-    case 2: *bytes = 11 * vec; break;
-    default: *bytes = 3 * vec; break;
+    case 0: *bytes = 2 * pass + (double)S->nf * (16.0 * S->nnz + 4.0 * (S->n + 1)); break;
+    case 1: *bytes = 2 * pass + (double)S->nf * (16.0 * S->nnzG + 4.0 * (S->n + 1)); break;
+    case 2: *bytes = 11 * pass; break;
+    default: *bytes = 3 * pass; break;
   }
-  DGP_REQUIRE(S->nsp <= 64, "profile: the timed kernels use two sources per lane (nsp <= 64)");
   launch();  // warm
   DGP_CHECK_LAUNCH();
   cudaEvent_t e0, e1;
