@@ -91,38 +91,46 @@ template <class R> struct CT;
 template <> struct CT<float> { using C = float2; };
 template <> struct CT<double> { using C = double2; };
 
-template <int VEC> __device__ inline void ldv(const float2 *p, float2 (&c)[VEC]) {
+// Lane I/O.  A lane owns VEC complex values of a row as VEC/E chunks of E
+// complex (16 bytes: E = 2 for complex FP32, 1 for complex FP64); chunk q
+// starts cs complex after chunk q-1, with cs = E * (lanes per row), so each
+// load instruction of a row group reads one contiguous run across its lanes.
+template <class C> struct Chunk;
+template <> struct Chunk<float2> { static constexpr int E = 2; };
+template <> struct Chunk<double2> { static constexpr int E = 1; };
+
+template <int VEC> __device__ inline void ldv(const float2 *p, int cs, float2 (&c)[VEC]) {
 #pragma unroll
   for (int q = 0; q < VEC; q += 2) {
-    float4 v = *reinterpret_cast<const float4 *>(p + q);
+    float4 v = *reinterpret_cast<const float4 *>(p + (q / 2) * cs);
     c[q] = make_float2(v.x, v.y);
     c[q + 1] = make_float2(v.z, v.w);
   }
 }
-template <int VEC> __device__ inline void ldv(const double2 *p, double2 (&c)[VEC]) {
+template <int VEC> __device__ inline void ldv(const double2 *p, int cs, double2 (&c)[VEC]) {
 #pragma unroll
-  for (int q = 0; q < VEC; ++q) c[q] = p[q];
+  for (int q = 0; q < VEC; ++q) c[q] = p[q * cs];
 }
-template <int VEC> __device__ inline void ldgv(const float2 *p, float2 (&c)[VEC]) {
+template <int VEC> __device__ inline void ldgv(const float2 *p, int cs, float2 (&c)[VEC]) {
 #pragma unroll
   for (int q = 0; q < VEC; q += 2) {
-    float4 v = __ldg(reinterpret_cast<const float4 *>(p + q));
+    float4 v = __ldg(reinterpret_cast<const float4 *>(p + (q / 2) * cs));
     c[q] = make_float2(v.x, v.y);
     c[q + 1] = make_float2(v.z, v.w);
   }
 }
-template <int VEC> __device__ inline void ldgv(const double2 *p, double2 (&c)[VEC]) {
+template <int VEC> __device__ inline void ldgv(const double2 *p, int cs, double2 (&c)[VEC]) {
 #pragma unroll
-  for (int q = 0; q < VEC; ++q) c[q] = __ldg(p + q);
+  for (int q = 0; q < VEC; ++q) c[q] = __ldg(p + q * cs);
 }
-template <int VEC> __device__ inline void stv(float2 *p, const float2 (&c)[VEC]) {
+template <int VEC> __device__ inline void stv(float2 *p, int cs, const float2 (&c)[VEC]) {
 #pragma unroll
   for (int q = 0; q < VEC; q += 2)
-    *reinterpret_cast<float4 *>(p + q) = make_float4(c[q].x, c[q].y, c[q + 1].x, c[q + 1].y);
+    *reinterpret_cast<float4 *>(p + (q / 2) * cs) = make_float4(c[q].x, c[q].y, c[q + 1].x, c[q + 1].y);
 }
-template <int VEC> __device__ inline void stv(double2 *p, const double2 (&c)[VEC]) {
+template <int VEC> __device__ inline void stv(double2 *p, int cs, const double2 (&c)[VEC]) {
 #pragma unroll
-  for (int q = 0; q < VEC; ++q) p[q] = c[q];
+  for (int q = 0; q < VEC; ++q) p[q * cs] = c[q];
 }
 
 template <class C> __device__ inline C czero();
@@ -164,6 +172,10 @@ struct Lane {
     k = blockIdx.y;
   }
   __device__ int64_t row(const Layout &L, int it) const { return row0 + ((int64_t)it * WARPS + warp) * L.rpw + rsub; }
+  // column of this lane's value v, its first column, and the stride between its chunks
+  template <int E> __device__ int col(const Layout &L, int v) const { return E * ((v / E) * L.lpr + sub) + v % E; }
+  template <int E> __device__ int col0() const { return E * sub; }
+  template <int E> __device__ int cs(const Layout &L) const { return E * L.lpr; }
 };
 
 __device__ inline int64_t vidx(const Layout &L, int k, int64_t i, int s) {
@@ -171,7 +183,7 @@ __device__ inline int64_t vidx(const Layout &L, int k, int64_t i, int s) {
 }
 
 // Block reduction of per-lane column partials into acc[slot[q]][k*nsp + s] (FP64 atomics).
-template <int VEC, int NQ>
+template <int VEC, int NQ, int E = 2>
 __device__ inline void block_reduce(const Layout &L, const Lane &ln, double2 (&part)[VEC][NQ], double2 *acc,
                                     int64_t C, const int (&slot)[NQ], double2 *sm /*[WARPS][nsp][NQ]*/) {
 #pragma unroll
@@ -188,7 +200,7 @@ __device__ inline void block_reduce(const Layout &L, const Lane &ln, double2 (&p
   if (ln.rsub == 0) {
 #pragma unroll
     for (int v = 0; v < VEC; ++v) {
-      const int s = ln.sub * VEC + v;
+      const int s = ln.template col<E>(L, v);
 #pragma unroll
       for (int q = 0; q < NQ; ++q) sm[((int64_t)ln.warp * L.nsp + s) * NQ + q] = part[v][q];
     }
@@ -273,7 +285,7 @@ struct OpG64 {
 
 // y[0..VEC) = sum_p coef(p) * Xk[col(p)*nsp + s0 ..]   (32-bit offsets inside one harmonic plane)
 template <int VEC, class C, class Coef>
-__device__ inline void row_spmv(int nsp, const int32_t *__restrict__ rowptr, int64_t i, const Coef &cf,
+__device__ inline void row_spmv(int nsp, int cs, const int32_t *__restrict__ rowptr, int64_t i, const Coef &cf,
                                 const C *__restrict__ Xk, C (&y)[VEC]) {
 #pragma unroll
   for (int v = 0; v < VEC; ++v) y[v] = czero<C>();
@@ -288,7 +300,7 @@ __device__ inline void row_spmv(int nsp, const int32_t *__restrict__ rowptr, int
     for (int u = 0; u < UNR; ++u) cf.get(p + u, j[u], a[u]);
     C xs[UNR][VEC];
 #pragma unroll
-    for (int u = 0; u < UNR; ++u) ldgv<VEC>(Xk + j[u] * nsp, xs[u]);
+    for (int u = 0; u < UNR; ++u) ldgv<VEC>(Xk + j[u] * nsp, cs, xs[u]);
 #pragma unroll
     for (int u = 0; u < UNR; ++u)
 #pragma unroll
@@ -299,7 +311,7 @@ __device__ inline void row_spmv(int nsp, const int32_t *__restrict__ rowptr, int
     C a;
     cf.get(p, j, a);
     C x[VEC];
-    ldgv<VEC>(Xk + j * nsp, x);
+    ldgv<VEC>(Xk + j * nsp, cs, x);
 #pragma unroll
     for (int v = 0; v < VEC; ++v) y[v] = cfmaT(a, x[v], y[v]);
   }
@@ -322,8 +334,9 @@ __global__ void __launch_bounds__(BS) k_spmm(Layout L, Op op, const typename CT<
   extern __shared__ double2 smem[];
   Lane ln(L);
   const auto cf = op.make(ln.k);
-  const int s0 = ln.sub * VEC;
-  const C *Xk = X + (int64_t)ln.k * L.n * L.nsp + s0;
+  constexpr int E = Chunk<C>::E;
+  const int c0 = ln.template col0<E>(), cs = ln.template cs<E>(L);
+  const C *Xk = X + (int64_t)ln.k * L.n * L.nsp + c0;
   constexpr int NQ = MODE == 2 ? 2 : 1;
   double2 part[VEC][NQ];
 #pragma unroll
@@ -334,12 +347,12 @@ __global__ void __launch_bounds__(BS) k_spmm(Layout L, Op op, const typename CT<
     const int64_t i = ln.row(L, it);
     if (i >= L.n) break;
     C y[VEC];
-    row_spmv<VEC>(L.nsp, op.rowptr, i, cf, Xk, y);
-    const int64_t o = vidx(L, ln.k, i, s0);
-    if (MODE != 2) stv<VEC>(Y + o, y);
+    row_spmv<VEC>(L.nsp, cs, op.rowptr, i, cf, Xk, y);
+    const int64_t o = vidx(L, ln.k, i, c0);
+    if (MODE != 2) stv<VEC>(Y + o, cs, y);
     if (MODE != 0) {
       C w[VEC];
-      ldv<VEC>(W + o, w);
+      ldv<VEC>(W + o, cs, w);
 #pragma unroll
       for (int v = 0; v < VEC; ++v) {
         acc_bil(part[v][0], y[v], w[v]);
@@ -349,10 +362,10 @@ __global__ void __launch_bounds__(BS) k_spmm(Layout L, Op op, const typename CT<
   }
   if constexpr (MODE == 1) {
     const int slot[1] = {ACC_D1};
-    block_reduce<VEC, 1>(L, ln, part, cols.acc, cols.C, slot, smem);
+    block_reduce<VEC, 1, E>(L, ln, part, cols.acc, cols.C, slot, smem);
   } else if constexpr (MODE == 2) {
     const int slot[2] = {ACC_D2, ACC_D3};
-    block_reduce<VEC, 2>(L, ln, part, cols.acc, cols.C, slot, smem);
+    block_reduce<VEC, 2, E>(L, ln, part, cols.acc, cols.C, slot, smem);
   }
 }
 
@@ -362,7 +375,7 @@ __device__ inline void lane_scalars(const Cols &cols, const Lane &ln, const Layo
                                     typename CT<R>::C (&out)[VEC], int (&act)[VEC]) {
 #pragma unroll
   for (int v = 0; v < VEC; ++v) {
-    const int64_t c = (int64_t)ln.k * L.nsp + ln.sub * VEC + v;
+    const int64_t c = (int64_t)ln.k * L.nsp + ln.template col<Chunk<typename CT<R>::C>::E>(L, v);
     act[v] = cols.active[c];
     out[v] = cvt<R>(src[c]);
   }
@@ -377,6 +390,8 @@ __global__ void __launch_bounds__(BS) k_update_s(Layout L, const typename CT<R>:
   if (halted(ctl, ST_RUNNING)) return;
   extern __shared__ double2 smem[];
   Lane ln(L);
+  constexpr int E = Chunk<typename CT<R>::C>::E;
+  const int c0 = ln.template col0<E>(), cs = ln.template cs<E>(L);
   double2 part[VEC][1];
   C al[VEC];
   int act[VEC];
@@ -386,19 +401,19 @@ __global__ void __launch_bounds__(BS) k_update_s(Layout L, const typename CT<R>:
   for (int it = 0; it < L.ipb; ++it) {
     const int64_t i = ln.row(L, it);
     if (i >= L.n) break;
-    const int64_t o = vidx(L, ln.k, i, ln.sub * VEC);
+    const int64_t o = vidx(L, ln.k, i, c0);
     C rr[VEC], vv[VEC], ss[VEC];
-    ldv<VEC>(r + o, rr);
-    ldv<VEC>(v + o, vv);
+    ldv<VEC>(r + o, cs, rr);
+    ldv<VEC>(v + o, cs, vv);
 #pragma unroll
     for (int q = 0; q < VEC; ++q) {
       ss[q] = act[q] ? cfmaT(cneg(al[q]), vv[q], rr[q]) : rr[q];
       if (act[q]) acc_abs2(part[q][0].x, ss[q]);
     }
-    stv<VEC>(s + o, ss);
+    stv<VEC>(s + o, cs, ss);
   }
   const int slot[1] = {ACC_NS};
-  block_reduce<VEC, 1>(L, ln, part, cols.acc, cols.C, slot, smem);
+  block_reduce<VEC, 1, E>(L, ln, part, cols.acc, cols.C, slot, smem);
 }
 
 // x = x + alpha*h + omega*z ; r = s - omega*t ; p = p - omega*v ; acc[NR] += |r|^2 ;
@@ -419,6 +434,8 @@ __global__ void __launch_bounds__(BS) k_update_xrp(Layout L, typename CT<R>::C *
   const bool final_ = *(volatile const int *)&ctl->state == ST_FINAL;
   extern __shared__ double2 smem[];
   Lane ln(L);
+  constexpr int E = Chunk<typename CT<R>::C>::E;
+  const int c0 = ln.template col0<E>(), cs = ln.template cs<E>(L);
   double2 part[VEC][2];
   C al[VEC], om[VEC];
   int act[VEC];
@@ -429,24 +446,24 @@ __global__ void __launch_bounds__(BS) k_update_xrp(Layout L, typename CT<R>::C *
   for (int it = 0; it < L.ipb; ++it) {
     const int64_t i = ln.row(L, it);
     if (i >= L.n) break;
-    const int64_t o = vidx(L, ln.k, i, ln.sub * VEC);
+    const int64_t o = vidx(L, ln.k, i, c0);
     C xx[VEC], hh[VEC];
-    ldv<VEC>(x + o, xx);
-    ldv<VEC>(h + o, hh);
+    ldv<VEC>(x + o, cs, xx);
+    ldv<VEC>(h + o, cs, hh);
     if (final_) {
 #pragma unroll
       for (int q = 0; q < VEC; ++q)
         if (act[q]) xx[q] = cfmaT(al[q], hh[q], xx[q]);
-      stv<VEC>(x + o, xx);
+      stv<VEC>(x + o, cs, xx);
       continue;
     }
     C zz[VEC], ss[VEC], tt[VEC], pp[VEC], vv[VEC], rh[VEC], rr[VEC];
-    ldv<VEC>(z + o, zz);
-    ldv<VEC>(s + o, ss);
-    ldv<VEC>(t + o, tt);
-    ldv<VEC>(p + o, pp);
-    ldv<VEC>(v + o, vv);
-    ldv<VEC>(rhat + o, rh);
+    ldv<VEC>(z + o, cs, zz);
+    ldv<VEC>(s + o, cs, ss);
+    ldv<VEC>(t + o, cs, tt);
+    ldv<VEC>(p + o, cs, pp);
+    ldv<VEC>(v + o, cs, vv);
+    ldv<VEC>(rhat + o, cs, rh);
 #pragma unroll
     for (int q = 0; q < VEC; ++q) {
       if (!act[q]) {
@@ -461,13 +478,13 @@ __global__ void __launch_bounds__(BS) k_update_xrp(Layout L, typename CT<R>::C *
         acc_bil(part[q][1], rh[q], rr[q]);
       }
     }
-    stv<VEC>(x + o, xx);
-    stv<VEC>(r + o, rr);
-    stv<VEC>(p + o, pp);
+    stv<VEC>(x + o, cs, xx);
+    stv<VEC>(r + o, cs, rr);
+    stv<VEC>(p + o, cs, pp);
   }
   if (!final_) {
     const int slot[2] = {ACC_NR, ACC_RHO};
-    block_reduce<VEC, 2>(L, ln, part, cols.acc, cols.C, slot, smem);
+    block_reduce<VEC, 2, E>(L, ln, part, cols.acc, cols.C, slot, smem);
   }
 }
 
@@ -478,20 +495,22 @@ __global__ void __launch_bounds__(BS) k_update_p(Layout L, const typename CT<R>:
   using C = typename CT<R>::C;
   if (halted(ctl, ST_RUNNING)) return;
   Lane ln(L);
+  constexpr int E = Chunk<typename CT<R>::C>::E;
+  const int c0 = ln.template col0<E>(), cs = ln.template cs<E>(L);
   C be[VEC];
   int act[VEC];
   lane_scalars<R, VEC>(cols, ln, L, cols.beta, be, act);
   for (int it = 0; it < L.ipb; ++it) {
     const int64_t i = ln.row(L, it);
     if (i >= L.n) break;
-    const int64_t o = vidx(L, ln.k, i, ln.sub * VEC);
+    const int64_t o = vidx(L, ln.k, i, c0);
     C rr[VEC], pp[VEC];
-    ldv<VEC>(r + o, rr);
-    ldv<VEC>(p + o, pp);
+    ldv<VEC>(r + o, cs, rr);
+    ldv<VEC>(p + o, cs, pp);
 #pragma unroll
     for (int q = 0; q < VEC; ++q)
       if (act[q]) pp[q] = cfmaT(be[q], pp[q], rr[q]);
-    stv<VEC>(p + o, pp);
+    stv<VEC>(p + o, cs, pp);
   }
 }
 
@@ -668,27 +687,29 @@ __global__ void __launch_bounds__(BS) k_init(Layout L, typename CT<R>::C *__rest
   using C = typename CT<R>::C;
   extern __shared__ double2 smem[];
   Lane ln(L);
+  constexpr int E = Chunk<typename CT<R>::C>::E;
+  const int c0 = ln.template col0<E>(), cs = ln.template cs<E>(L);
   double2 part[VEC][2];
 #pragma unroll
   for (int q = 0; q < VEC; ++q) part[q][0] = part[q][1] = make_double2(0, 0);
   for (int it = 0; it < L.ipb; ++it) {
     const int64_t i = ln.row(L, it);
     if (i >= L.n) break;
-    const int64_t o = vidx(L, ln.k, i, ln.sub * VEC);
+    const int64_t o = vidx(L, ln.k, i, c0);
     C bb[VEC], zz[VEC];
-    ldv<VEC>(r + o, bb);
+    ldv<VEC>(r + o, cs, bb);
 #pragma unroll
     for (int q = 0; q < VEC; ++q) {
       zz[q] = czero<C>();
       acc_abs2(part[q][0].x, bb[q]);
       acc_bil(part[q][1], bb[q], bb[q]);
     }
-    stv<VEC>(x + o, zz);
-    stv<VEC>(rhat + o, bb);
-    stv<VEC>(p + o, bb);
+    stv<VEC>(x + o, cs, zz);
+    stv<VEC>(rhat + o, cs, bb);
+    stv<VEC>(p + o, cs, bb);
   }
   const int slot[2] = {ACC_NR, ACC_RHO};
-  block_reduce<VEC, 2>(L, ln, part, cols.acc, cols.C, slot, smem);
+  block_reduce<VEC, 2, E>(L, ln, part, cols.acc, cols.C, slot, smem);
 }
 
 // err0 = ||r0||, rho0 = r0.r0, activity from the column index and norm
@@ -835,10 +856,13 @@ __global__ void __launch_bounds__(BS) k_residual64(Layout L, int ns, const int32
 #pragma unroll
   for (int q = 0; q < VEC; ++q) part[q][0] = make_double2(0, 0);
   const double2 *Xk = X + (int64_t)ln.k * L.n * ns;
+  // columns of this lane: the strided mapping of the FP32 vectors (E = 2) it writes
+  int scol[VEC];
+#pragma unroll
+  for (int q = 0; q < VEC; ++q) scol[q] = ln.template col<2>(L, q);
   for (int it = 0; it < L.ipb; ++it) {
     const int64_t i = ln.row(L, it);
     if (i >= L.n) break;
-    const int s0 = ln.sub * VEC;
     double2 y[VEC];
 #pragma unroll
     for (int q = 0; q < VEC; ++q) y[q] = make_double2(0, 0);
@@ -849,12 +873,12 @@ __global__ void __launch_bounds__(BS) k_residual64(Layout L, int ns, const int32
       const double2 a = make_double2(km.x, om * km.y);
 #pragma unroll
       for (int q = 0; q < VEC; ++q)
-        if (s0 + q < ns) y[q] = cfma(a, __ldg(Xk + (int64_t)j * ns + s0 + q), y[q]);
+        if (scol[q] < ns) y[q] = cfma(a, __ldg(Xk + (int64_t)j * ns + scol[q]), y[q]);
     }
     float2 out[VEC];
 #pragma unroll
     for (int q = 0; q < VEC; ++q) {
-      const int s = s0 + q;
+      const int s = scol[q];
       double2 bv = make_double2(0, 0);
       if (s < ns) {
         if (Bd) {
@@ -869,10 +893,10 @@ __global__ void __launch_bounds__(BS) k_residual64(Layout L, int ns, const int32
       acc_abs2(part[q][0].x, rr);
       out[q] = make_float2((float)rr.x, (float)rr.y);
     }
-    stv<VEC>(r32 + vidx(L, ln.k, i, s0), out);
+    stv<VEC>(r32 + vidx(L, ln.k, i, ln.template col0<2>()), ln.template cs<2>(L), out);
   }
   const int slot[1] = {ACC_NR};
-  block_reduce<VEC, 1>(L, ln, part, cols.acc, cols.C, slot, smem);
+  block_reduce<VEC, 1, 2>(L, ln, part, cols.acc, cols.C, slot, smem);
 }
 
 // mode 0: ||b|| per column from acc[NR]; mode 1: outer_err = ||r||/||b||, ctl->max_err = max
