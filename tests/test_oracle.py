@@ -120,3 +120,25 @@ def test_tik_inv_matches_normal_equations():
     uw = jacobian.tik_inv(J, 0.1, y, weights=w)
     Hw = J.T @ (w[:, None] * J) + 0.1 * np.max((w[:, None] * J ** 2).sum(0)) * np.eye(12)
     assert np.allclose(uw, np.linalg.solve(Hw, J.T @ (w * y)), rtol=1e-12)
+
+
+def test_c_port_matches_numpy_oracle(small_case):
+    """The C/OpenMP restatement used as the CPU baseline agrees with the numpy oracle."""
+    from oracle import cport
+    K, M = small_case["K"], small_case["M"]
+    dfc = 2 * np.pi / 10e-9 / (2.99792458e11 / 1.4)
+    k = 3
+    A = sp.tril(K + 1j * dfc * M).tocsr()
+    rg, cg = solver.fsai_pattern(A)
+    G = cport.fsai_factor(sp.tril(K).tocsr(), sp.tril(k * dfc * M).tocsr(), rg, cg)
+    G0 = solver.fsai_factor(sp.tril(K).tocsr(), sp.tril(dfc * M).tocsr(), rg, cg, k + 1)[:, k]
+    assert np.abs(G - G0).max() <= 1e-12 * np.abs(G0).max()
+    rt, ct, perm = solver.transpose_pattern(rg, cg, K.shape[0])
+    rng = np.random.default_rng(2)
+    B = np.zeros((K.shape[0], 3), complex)
+    for c in range(3):
+        B[rng.choice(K.shape[0], 4, replace=False), c] = rng.random(4)
+    X, it = cport.bicgstab(K, M, k * dfc, rg, cg, G, rt, ct, G[perm], B, 1e-12)
+    Xd = solver.direct_solve(K, M, k * dfc, np.stack([B, B], axis=2))[:, :, 1]   # harmonic 1 of k*dfc
+    assert np.linalg.norm(X - Xd) / np.linalg.norm(Xd) < 1e-9
+    assert (it > 3).all()
