@@ -48,6 +48,7 @@ _SIGS = {
     "dgp_fem_pattern": (C.c_int, [P, C.POINTER(P), C.POINTER(P)]),
     "dgp_fem_boundary": (C.c_int, [P, P, P]),
     "dgp_fem_assemble": (C.c_int, [P, P, P, P, P, P]),
+    "dgp_fem_adjoint_grad": (C.c_int, [P, P, P, P, P, I32, I32, P, P, P]),
     "dgp_solve_opts_default": (None, [C.POINTER(SolveOpts)]),
     "dgp_solver_create": (C.c_int, [C.POINTER(P), P, P, I64, I64, P, P, D, I32, I32, C.POINTER(SolveOpts), P]),
     "dgp_solver_update": (C.c_int, [P, P, P, P]),
@@ -64,6 +65,7 @@ _SIGS = {
     "dgp_td2fc": (C.c_int, [P, I64, I32, P, P, I32, P, P]),
     "dgp_fc2td": (C.c_int, [P, I64, I32, P, P, I32, P, P]),
     "dgp_fc2tg": (C.c_int, [P, I64, I32, P, I32, I32, P, P]),
+    "dgp_tg_adjoint_rhs": (C.c_int, [P, P, I32, P, I32, P, I32, I32, P, I64, I32, I32, P, P]),
     "dgp_normal_eq": (C.c_int, [P, I64, I64, P, P, D, I32, P, I64, P, P]),
     "dgp_cholesky_solve": (C.c_int, [P, I64, I64, P, P]),
     "dgp_jacobian_complex":(C.c_int, [P, P, P, I64, P, P, I32, P, I32, I64, I32, P, P, I32, P, P]),

@@ -257,3 +257,30 @@ def meas(det_nodes, det_w, link, phi) -> torch.Tensor:
     check(lib.dgp_meas(ptr(det_nodes), ptr(det_w), int(det_nodes.shape[0]), ptr(link), nm, ptr(as_real(phi)), n,
                        nf, ns, ptr(as_real(out)), stream_ptr()))
     return out
+
+
+# ------------------------------------------------------ reverse-mode pieces
+def tg_adjoint_rhs(det_nodes, det_w, link, gate_fc, nt, g, n, nf, ns) -> torch.Tensor:
+    """dL/dphi [NF][NN][NS] complex128 for L = sum g * fc2tg(meas(phi)), g [NM][NG]."""
+    gate = gate_fc.to(device="cuda", dtype=torch.complex128).contiguous()
+    g = g.to(device="cuda", dtype=torch.float64).contiguous()
+    link = link.to(device="cuda", dtype=torch.int32).contiguous()
+    B = torch.empty((nf, n, ns), dtype=torch.complex128, device="cuda")
+    check(lib.dgp_tg_adjoint_rhs(ptr(det_nodes), ptr(det_w), int(det_nodes.shape[0]), ptr(link), int(link.shape[0]),
+                                 ptr(as_real(gate)), int(gate.shape[0]), int(nt), ptr(g), n, nf, ns, ptr(as_real(B)),
+                                 stream_ptr()))
+    return B
+
+
+def fem_adjoint_grad(fem: Fem, mua, musp, phi, lam, want_musp=True):
+    """(dL/dmua, dL/dmusp or None) [NN] from forward fields phi and adjoint fields lam [NF][NN][NS]."""
+    nf, n, ns = phi.shape
+    if lam.shape != phi.shape:
+        raise ValueError("phi and lam must have the same shape")
+    mua = mua.to(device="cuda", dtype=torch.float64).contiguous()
+    musp = musp.to(device="cuda", dtype=torch.float64).contiguous()
+    gmua = torch.empty(n, dtype=torch.float64, device="cuda")
+    gmusp = torch.empty(n, dtype=torch.float64, device="cuda") if want_musp else None
+    check(lib.dgp_fem_adjoint_grad(fem._h, ptr(mua), ptr(musp), ptr(as_real(phi)), ptr(as_real(lam)), nf, ns,
+                                   ptr(gmua), None if gmusp is None else ptr(gmusp), stream_ptr()))
+    return gmua, gmusp

@@ -206,6 +206,14 @@ int dgp_fem_assemble(dgp_fem_t fem, const double *d_mua, const double *d_musp, d
   DGP_GUARD(fem_assemble(&fem->plan, d_mua, d_musp, d_K, d_M, (cudaStream_t)stream));
 }
 
+int dgp_fem_adjoint_grad(dgp_fem_t fem, const double *d_mua, const double *d_musp, const double *d_phi,
+                         const double *d_lam, int32_t nf, int32_t ns, double *d_gmua, double *d_gmusp,
+                         dgp_stream_t stream) {
+  if (!fem) return fail(DGP_ERR_ARG, "fem_adjoint_grad: null handle");
+  DGP_GUARD(fem_adjoint_grad(&fem->plan, d_mua, d_musp, d_phi, d_lam, nf, ns, d_gmua, d_gmusp,
+                             (cudaStream_t)stream));
+}
+
 // ----------------------------------------------------------------- solver
 void dgp_solve_opts_default(dgp_solve_opts *o) {
   if (!o) return;
@@ -358,6 +366,13 @@ int dgp_jacobian_tg_vjp(const int32_t *d_P_rowptr, const int32_t *d_P_col, const
                         double *d_out, dgp_stream_t stream) {
   DGP_GUARD(jacobian_run(2, d_P_rowptr, d_P_col, d_P_val, nv, d_w, d_phi, ns, d_phiA, nd, nn, nf, d_fpsf, d_link, nm,
                          d_gate_fc, ng, nt, d_data_tg, d_out, d_g, (cudaStream_t)stream));
+}
+
+int dgp_tg_adjoint_rhs(const int32_t *d_det_nodes, const double *d_det_w, int32_t nd, const int32_t *d_link,
+                       int32_t nm, const double *d_gate_fc, int32_t ng, int32_t nt, const double *d_g, int64_t n,
+                       int32_t nf, int32_t ns, double *d_B, dgp_stream_t stream) {
+  DGP_GUARD(tg_adjoint_rhs(d_det_nodes, d_det_w, nd, d_link, nm, d_gate_fc, ng, nt, d_g, n, nf, ns, d_B,
+                           (cudaStream_t)stream));
 }
 
 // -------------------------------------------------------- normal equations

@@ -24,6 +24,14 @@ int fem_create(FemPlan *F, const double *d_node, const int32_t *d_elem, int64_t 
                cudaStream_t st);
 int fem_assemble(FemPlan *F, const double *d_mua, const double *d_musp, double *d_K, double *d_M,
                  cudaStream_t st);
+// dL/dmua (and dL/dmusp when d_gmusp is not NULL) = -Re sum lam^T (dA/dp) phi
+int fem_adjoint_grad(FemPlan *F, const double *d_mua, const double *d_musp, const double *d_phi,
+                     const double *d_lam, int32_t nf, int32_t ns, double *d_gmua, double *d_gmusp,
+                     cudaStream_t st);
+// adjoint sources of L = sum g . fc2tg(meas(phi))
+int tg_adjoint_rhs(const int32_t *d_det_nodes, const double *d_det_w, int32_t nd, const int32_t *d_link, int32_t nm,
+                   const double *d_gate_fc, int32_t ng, int32_t nt, const double *d_g, int64_t n, int32_t nf,
+                   int32_t ns, double *d_B, cudaStream_t st);
 
 // ----------------------------------------------------------------- FSAI
 struct FsaiPattern {

@@ -54,7 +54,7 @@ __device__ inline Geo tet_geometry(const double *__restrict__ node, const int32_
   double det = cx * B[0][2] + cy * B[1][2] + cz * B[2][2];
   Geo G;
   G.vol = fabs(det / 6.0);
-  if (!(G.vol > 0.0)) atomicOr(bad, 1);
+  if (!(G.vol > 0.0) && bad) atomicOr(bad, 1);
   // inv(B^T) = cof(B) / det(B): (B^-T)_{ij} = cofactor_{ij}(B) / det
   double cof[3][3];
   cof[0][0] = B[1][1] * B[2][2] - B[1][2] * B[2][1];
@@ -337,6 +337,94 @@ __global__ void k_gather_slots(const int32_t *__restrict__ cstart, const int32_t
   M[u] = mv;
 }
 
+// Adjoint gradient of a real functional L(phi(mua, musp)) for every node:
+//   dL/dmua_v = -Re sum_{s,k} lam^T (dA_k/dmua_v) phi,  dL/dmusp_v likewise,
+// with dA/dp differentiated through exactly the element quadrature above:
+// absorption block vol sum_q w_q N_v N_i N_j, and the stiffness block
+// vol (grad N_i . grad N_j) d(ksum)/dp with ksum = sum_q w_q sum_l N_l kappa_l,
+// d(ksum)/dmua_v = d(ksum)/dmusp_v = -3 kappa_v^2 sum_q w_q N_v(x_q)
+// (kappa = 1/(3(mua + musp)), dMesh.m:74, :85).  One warp per element, lanes
+// over sources, all harmonics; the per-vertex sums leave by one FP64 atomic
+// per vertex and output.  Robin and M blocks do not depend on mua or musp.
+__global__ void __launch_bounds__(256) k_elem_grad(const double *__restrict__ node, const int32_t *__restrict__ elem,
+                                                   int64_t ne, const double2 *__restrict__ phi,
+                                                   const double2 *__restrict__ lam, int64_t n, int nf, int ns,
+                                                   const double *__restrict__ mua, const double *__restrict__ musp,
+                                                   double *gmua, double *gmusp) {
+  const int lane = threadIdx.x & 31;
+  const int64_t e = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  if (e >= ne) return;
+  int32_t v[4];
+#pragma unroll
+  for (int l = 0; l < 4; ++l) v[l] = elem[4 * e + l];
+  Geo G = tet_geometry(node, v, nullptr);
+  double dk[4];
+#pragma unroll
+  for (int l = 0; l < 4; ++l) {
+    double cv = 0.0;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) cv += c_tw[q] * c_tq[l][q];
+    double kap = 1.0 / (3.0 * (mua[v[l]] + musp[v[l]]));
+    dk[l] = -3.0 * kap * kap * cv * G.vol;
+  }
+  double acc_a[4] = {0, 0, 0, 0}, acc_k = 0.0;
+  for (int k = 0; k < nf; ++k) {
+    const int64_t base = (int64_t)k * n;
+    for (int s = lane; s < ns; s += 32) {
+      double2 f[4], a[4];
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        f[l] = phi[(base + v[l]) * ns + s];
+        a[l] = lam[(base + v[l]) * ns + s];
+      }
+      // absorption: sum_q w_q N_v(x_q) Re(lam(x_q) phi(x_q))
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        double fr = 0, fi = 0, ar = 0, ai = 0;
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+          fr += c_tq[l][q] * f[l].x;
+          fi += c_tq[l][q] * f[l].y;
+          ar += c_tq[l][q] * a[l].x;
+          ai += c_tq[l][q] * a[l].y;
+        }
+        const double pr = c_tw[q] * (ar * fr - ai * fi);
+#pragma unroll
+        for (int l = 0; l < 4; ++l) acc_a[l] += c_tq[l][q] * pr;
+      }
+      // stiffness: Re(grad lam . grad phi), shared by all four vertices
+      double dot = 0.0;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        double lr = 0, li = 0, pr = 0, pi = 0;
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+          lr += G.g[l][d] * a[l].x;
+          li += G.g[l][d] * a[l].y;
+          pr += G.g[l][d] * f[l].x;
+          pi += G.g[l][d] * f[l].y;
+        }
+        dot += lr * pr - li * pi;
+      }
+      acc_k += dot;
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+    for (int l = 0; l < 4; ++l) acc_a[l] += __shfl_xor_sync(0xffffffffu, acc_a[l], off);
+    acc_k += __shfl_xor_sync(0xffffffffu, acc_k, off);
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+      const double stiff = acc_k * dk[l];
+      atomicAdd(gmua + v[l], -(G.vol * acc_a[l] + stiff));
+      if (gmusp) atomicAdd(gmusp + v[l], -stiff);
+    }
+  }
+}
+
 double robin_factor(double nr) {
   double r0 = (nr - 1.0) * (nr - 1.0) / ((nr + 1.0) * (nr + 1.0));
   double ct = fabs(cos(asin(1.0 / nr)));
@@ -532,6 +620,21 @@ int fem_assemble(FemPlan *F, const double *d_mua, const double *d_musp, double *
                                                     F->nk, 16 * F->ne, F->elem.as<int32_t>(),
                                                     F->faces.as<int32_t>(), F->Ke.as<double>(), F->Me.as<double>(),
                                                     F->Be.as<double>(), d_K, d_M);
+  DGP_CHECK_LAUNCH();
+  return DGP_OK;
+}
+
+int fem_adjoint_grad(FemPlan *F, const double *d_mua, const double *d_musp, const double *d_phi,
+                     const double *d_lam, int32_t nf, int32_t ns, double *d_gmua, double *d_gmusp,
+                     cudaStream_t st) {
+  DGP_REQUIRE(d_mua && d_musp && d_phi && d_lam && d_gmua, "fem_adjoint_grad: null pointer");
+  DGP_REQUIRE(nf > 0 && ns > 0, "fem_adjoint_grad: nf and ns must be positive");
+  DGP_TRY(upload_quadrature());
+  DGP_CUDA(cudaMemsetAsync(d_gmua, 0, sizeof(double) * F->nn, st));
+  if (d_gmusp) DGP_CUDA(cudaMemsetAsync(d_gmusp, 0, sizeof(double) * F->nn, st));
+  k_elem_grad<<<grid1(F->ne * 32, 256), 256, 0, st>>>(F->node.as<double>(), F->elem.as<int32_t>(), F->ne,
+                                                      (const double2 *)d_phi, (const double2 *)d_lam, F->nn, nf, ns,
+                                                      d_mua, d_musp, d_gmua, d_gmusp);
   DGP_CHECK_LAUNCH();
   return DGP_OK;
 }

@@ -75,6 +75,7 @@ class DMesh:
             self.musp = torch.as_tensor(props[:, 1], device="cuda")
             self.musp_host = props[:, 1].copy()
         self.K, self.M = self.fem.assemble(self.mua, self.musp)
+        self.props_version = getattr(self, "props_version", 0) + 1
         if self._solver is not None:
             self._solver.update(self.K, self.M)
         return self

@@ -135,6 +135,20 @@ int dgp_fem_boundary(dgp_fem_t fem, int32_t *d_bnd, dgp_stream_t stream);
  * (mass) values on the pattern, float64, from nodal mua and musp. */
 int dgp_fem_assemble(dgp_fem_t fem, const double *d_mua, const double *d_musp,
                      double *d_K, double *d_M, dgp_stream_t stream);
+/* Reverse-mode gradient of a real functional L(phi) through the assembly:
+ *   d_gmua[v]  = dL/dmua_v  = -Re sum_{k,s} lam_{k,s}^T (dA_k/dmua_v)  phi_{k,s}
+ *   d_gmusp[v] = dL/dmusp_v = -Re sum_{k,s} lam_{k,s}^T (dA_k/dmusp_v) phi_{k,s}
+ * (d_gmusp may be NULL) where phi [nf][nn][ns] complex128 are the forward
+ * fields and lam the adjoint fields A_k^-1 (dL/dphi_{k,s}) of the same
+ * layout.  dA/dp follows the element quadrature of dgp_fem_assemble exactly,
+ * kappa's dependence on mua and musp included; the reference's absorption
+ * Jacobian (J_complex, dMesh.m:206-247) holds kappa fixed, which is
+ * d_gmua - d_gmusp here.  No reference counterpart as one call: the
+ * reference forms J explicitly and multiplies. */
+int dgp_fem_adjoint_grad(dgp_fem_t fem, const double *d_mua,
+                         const double *d_musp, const double *d_phi,
+                         const double *d_lam, int32_t nf, int32_t ns,
+                         double *d_gmua, double *d_gmusp, dgp_stream_t stream);
 
 /* ====================================================================== *
  *  Batched solver: FSAI setup + BiCGSTAB over every source x harmonic.
@@ -257,6 +271,17 @@ int dgp_fc2td(const double *d_c, int64_t nr, int32_t nf, const double *d_f,
 /* y[r][g] = nt * 2 Re sum_k conj(gate[g][k]) c~[r][k] (fc2tg.m:100-111). */
 int dgp_fc2tg(const double *d_c, int64_t nr, int32_t nf, const double *d_gate_fc,
               int32_t ng, int32_t nt, double *d_y, dgp_stream_t stream);
+/* Adjoint sources of L = sum_{m,g} d_g[m][g] * fc2tg(meas(phi))[m][g]:
+ * d_B[k][node][s] = dL/dphi_{k,s}[node] (complex128 [nf][n][ns], overwritten),
+ * c[m][k] = 2 nt h_k sum_g g[m][g] conj(gate[g][k]) (h_0 = 1/2, else 1)
+ * scattered through detector d's weights for every link m = (s, d).  Solving
+ * A_k lam = B (dgp_solve) gives the adjoint fields of dgp_fem_adjoint_grad.
+ * The chain rule of fc2tg.m:100-111 and meas_flu (dMesh.m:144-171). */
+int dgp_tg_adjoint_rhs(const int32_t *d_det_nodes, const double *d_det_w,
+                       int32_t nd, const int32_t *d_link, int32_t nm,
+                       const double *d_gate_fc, int32_t ng, int32_t nt,
+                       const double *d_g, int64_t n, int32_t nf, int32_t ns,
+                       double *d_B, dgp_stream_t stream);
 
 /* ====================================================================== *
  *  Absorption Jacobian (J_complex, dMesh.m:206-247) and its time-gated
