@@ -51,6 +51,8 @@ _SIGS = {
     "dgp_fem_adjoint_grad": (C.c_int, [P, P, P, P, P, I32, I32, P, P, P]),
     "dgp_solve_opts_default": (None, [C.POINTER(SolveOpts)]),
     "dgp_solver_create": (C.c_int, [C.POINTER(P), P, P, I64, I64, P, P, D, I32, I32, C.POINTER(SolveOpts), P]),
+    "dgp_solver_create_harmonics": (C.c_int, [C.POINTER(P), P, P, I64, I64, P, P, D, P, I32, I32,
+                                              C.POINTER(SolveOpts), P]),
     "dgp_solver_update": (C.c_int, [P, P, P, P]),
     "dgp_solver_destroy": (C.c_int, [P]),
     "dgp_solver_memory": (C.c_int, [P, C.POINTER(I64)]),

@@ -86,14 +86,27 @@ def _borrow(p: int, n: int, dtype) -> torch.Tensor:
 class Solver:
     """Batched FSAI-BiCGSTAB plan for A_k = K + i*k*dfc*M (gpuBicstab_FSAIP, dMesh.m:1247-1385)."""
 
-    def __init__(self, rowptr, col, K, M, dfc: float, nf: int, ns_max: int, opts: _lib.SolveOpts | None = None):
+    def __init__(self, rowptr, col, K, M, dfc: float, nf: int, ns_max: int, opts: _lib.SolveOpts | None = None,
+                 harmonics=None):
+        """harmonics: the harmonic index of each of the nf batch slots (default 0 .. nf-1)."""
         self.n = int(rowptr.numel() - 1)
         self.nnz = int(col.numel())
         self.nf, self.ns_max, self.dfc = int(nf), int(ns_max), float(dfc)
         o = opts or _lib.default_opts()
         h = C.c_void_p()
-        check(lib.dgp_solver_create(C.byref(h), ptr(rowptr), ptr(col), self.n, self.nnz, ptr(K), ptr(M),
-                                    self.dfc, self.nf, self.ns_max, C.byref(o), stream_ptr()))
+        if harmonics is None:
+            check(lib.dgp_solver_create(C.byref(h), ptr(rowptr), ptr(col), self.n, self.nnz, ptr(K), ptr(M),
+                                        self.dfc, self.nf, self.ns_max, C.byref(o), stream_ptr()))
+            self.harmonics = list(range(self.nf))
+        else:
+            hl = [int(x) for x in harmonics]
+            if len(hl) != self.nf:
+                raise ValueError("one harmonic index per batch slot")
+            arr = (C.c_int32 * self.nf)(*hl)
+            check(lib.dgp_solver_create_harmonics(C.byref(h), ptr(rowptr), ptr(col), self.n, self.nnz, ptr(K),
+                                                  ptr(M), self.dfc, arr, self.nf, self.ns_max, C.byref(o),
+                                                  stream_ptr()))
+            self.harmonics = hl
         self._h = h
 
     def update(self, K, M):

@@ -19,8 +19,11 @@ from . import api
 
 
 class TimeGatedForward:
-    def __init__(self, mesh, gate_fc, precision="fp64", tol=1e-12, maxit=1000, inner_tol=None):
+    def __init__(self, mesh, gate_fc, precision="fp64", tol=1e-12, maxit=1000, inner_tol=None, recompute=False):
+        """recompute=True keeps no fields between forward and backward: backward solves phi again
+        (one extra forward solve for NF x NN x NS x 16 bytes less memory held by the autograd graph)."""
         self.mesh = mesh
+        self.recompute = bool(recompute)
         self.gate_fc = torch.as_tensor(gate_fc, device="cuda", dtype=torch.complex128).contiguous()
         self.nt = len(mesh.optode.tAxis)
         self.opts = api.make_opts(tol=tol, maxit=maxit, precision=precision, inner_tol=inner_tol)
@@ -47,7 +50,9 @@ class TimeGatedForward:
 
     def gradient(self, mua, musp, phi, state, gy):
         """(dL/dmua, dL/dmusp) for L = sum gy * y at the properties the fields were solved for."""
-        if state != self.mesh.props_version:
+        if phi is None:
+            _, phi, state = self.forward_fields(mua, musp)
+        elif state != self.mesh.props_version:
             self._assemble(mua, musp)
         S = self.mesh.solver(ns_max=self.ns)
         nf, n, ns = phi.shape
@@ -64,7 +69,8 @@ class _TimeGated(torch.autograd.Function):
     @staticmethod
     def forward(ctx, mua, musp, model):
         y, phi, state = model.forward_fields(mua, musp)
-        ctx.model, ctx.phi, ctx.state = model, phi, state
+        ctx.model, ctx.state = model, state
+        ctx.phi = None if model.recompute else phi
         ctx.save_for_backward(mua, musp)
         return y
 

@@ -961,11 +961,11 @@ __global__ void k_gather_gt(const double2 *__restrict__ G, const int32_t *__rest
   recGT[t] = b;
 }
 
-__global__ void k_omega(int nf, double dfc, double *om64, float *om32) {
+__global__ void k_omega(int nf, double dfc, const int32_t *__restrict__ harm, double *om64, float *om32) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k < nf) {
-    om64[k] = (double)k * dfc;
-    om32[k] = (float)((double)k * dfc);
+    om64[k] = (double)harm[k] * dfc;
+    om32[k] = (float)((double)harm[k] * dfc);
   }
 }
 
@@ -1226,7 +1226,7 @@ int solver_update(SolverPlan *S, const double *d_K, const double *d_M, cudaStrea
   DGP_CHECK_LAUNCH();
   DGP_TRY(fsai_factor_run(S->rowptr.as<int32_t>(), S->col.as<int32_t>(), d_K, im.as<double>(), S->n,
                           S->P.rowptr.as<int32_t>(), S->P.col.as<int32_t>(), S->P.mmax, S->nf,
-                          S->G64.as<double2>(), 1, S->nnzG, st));
+                          S->G64.as<double2>(), 1, S->nnzG, st, S->harm.as<int32_t>()));
   k_gather_gt<<<g1(S->nnzG * S->nf, 256), 256, 0, st>>>(S->G64.as<double2>(), S->P.permT.as<int32_t>(),
                                                        S->P.col.as<int32_t>(), S->P.colT.as<int32_t>(), S->nnzG,
                                                        S->nf, S->GT64.as<double2>(), S->RecG32.as<Rec32>(),
@@ -1238,8 +1238,13 @@ int solver_update(SolverPlan *S, const double *d_K, const double *d_M, cudaStrea
 
 int solver_build(SolverPlan *S, const int32_t *d_rowptr, const int32_t *d_col, int64_t n, int64_t nnz,
                  const double *d_K, const double *d_M, double dfc, int32_t nf, int32_t ns_max,
-                 const dgp_solve_opts *opts, cudaStream_t st) {
+                 const dgp_solve_opts *opts, cudaStream_t st, const int32_t *h_harm) {
   DGP_REQUIRE(n > 0 && nnz > 0 && nf > 0 && nf <= 65535, "solver: bad sizes");
+  std::vector<int32_t> hl(nf);
+  for (int j = 0; j < nf; ++j) {
+    hl[j] = h_harm ? h_harm[j] : j;
+    DGP_REQUIRE(hl[j] >= 0, "solver: harmonic indices must be >= 0");
+  }
   DGP_REQUIRE(ns_max >= 1 && ns_max <= 128, "solver: 1 <= ns_max <= 128 sources per harmonic");
   DGP_REQUIRE(nnz < INT32_MAX && n < (1 << 24), "solver: nnz must fit int32 and n < 2^24");
   S->n = n;
@@ -1256,7 +1261,9 @@ int solver_build(SolverPlan *S, const int32_t *d_rowptr, const int32_t *d_col, i
   DGP_TRY(S->KM64.alloc(sizeof(double2) * nnz));
   DGP_TRY(S->RecA32.alloc(sizeof(Rec32) * nnz));
   DGP_TRY(S->omega.alloc((sizeof(double) + sizeof(float)) * nf));
-  k_omega<<<g1(nf, 128), 128, 0, st>>>(nf, dfc, S->omega.as<double>(),
+  DGP_TRY(S->harm.alloc(sizeof(int32_t) * nf));
+  DGP_CUDA(cudaMemcpyAsync(S->harm.p, hl.data(), sizeof(int32_t) * nf, cudaMemcpyHostToDevice, st));
+  k_omega<<<g1(nf, 128), 128, 0, st>>>(nf, dfc, S->harm.as<int32_t>(), S->omega.as<double>(),
                                         (float *)(S->omega.as<char>() + sizeof(double) * nf));
   DGP_CHECK_LAUNCH();
   DGP_TRY(fsai_pattern_build(&S->P, S->rowptr.as<int32_t>(), S->col.as<int32_t>(), d_K, d_M, dfc, n,

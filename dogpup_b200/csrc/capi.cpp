@@ -231,13 +231,22 @@ void dgp_solve_opts_default(dgp_solve_opts *o) {
 int dgp_solver_create(dgp_solver_t *solver, const int32_t *d_rowptr, const int32_t *d_col, int64_t n, int64_t nnz,
                       const double *d_K, const double *d_M, double dfc, int32_t nf, int32_t ns_max,
                       const dgp_solve_opts *opts, dgp_stream_t stream) {
+  return dgp_solver_create_harmonics(solver, d_rowptr, d_col, n, nnz, d_K, d_M, dfc, nullptr, nf, ns_max, opts,
+                                     stream);
+}
+
+int dgp_solver_create_harmonics(dgp_solver_t *solver, const int32_t *d_rowptr, const int32_t *d_col, int64_t n,
+                                int64_t nnz, const double *d_K, const double *d_M, double dfc,
+                                const int32_t *h_harmonics, int32_t nf, int32_t ns_max, const dgp_solve_opts *opts,
+                                dgp_stream_t stream) {
   if (!solver || !d_rowptr || !d_col || !d_K || !d_M) return fail(DGP_ERR_ARG, "solver_create: null pointer");
   *solver = nullptr;
   dgp_solver_s *h = new (std::nothrow) dgp_solver_s();
   if (!h) return fail(DGP_ERR_NOMEM, "solver_create: host allocation failed");
   int rc;
   try {
-    rc = solver_build(&h->plan, d_rowptr, d_col, n, nnz, d_K, d_M, dfc, nf, ns_max, opts, (cudaStream_t)stream);
+    rc = solver_build(&h->plan, d_rowptr, d_col, n, nnz, d_K, d_M, dfc, nf, ns_max, opts, (cudaStream_t)stream,
+                      h_harmonics);
   } catch (...) {
     rc = fail(DGP_ERR_NOMEM, "solver_create: exception");
   }

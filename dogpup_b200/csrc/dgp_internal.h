@@ -48,11 +48,12 @@ int fsai_pattern_build(FsaiPattern *P, const int32_t *d_rowptr, const int32_t *d
 int fsai_pattern_rows(const int32_t *d_rowptr, const int32_t *d_col, const double *d_K, const double *d_M,
                       double dfc, int64_t n, int32_t cap, int32_t *d_rowptrG, int32_t *d_colG,
                       int32_t *h_nnzG, int32_t *h_mmax, cudaStream_t st);
-// G values for harmonics k = k0 .. k0+nf-1 of A_k = Re + i*k*Im, written to
-// out[slot * s_slot + (k-k0) * s_k] (complex128 interleaved).
+// G values of A_h = Re + i*h*Im for the harmonics h = d_harm[j] (j = 0 .. nf-1;
+// h = j when d_harm is NULL), written to out[slot * s_slot + j * s_k]
+// (complex128 interleaved).
 int fsai_factor_run(const int32_t *d_rowptr, const int32_t *d_col, const double *d_re, const double *d_im,
                     int64_t n, const int32_t *d_rowptrG, const int32_t *d_colG, int32_t mmax, int32_t nf,
-                    double2 *d_out, int64_t s_slot, int64_t s_k, cudaStream_t st);
+                    double2 *d_out, int64_t s_slot, int64_t s_k, cudaStream_t st, const int32_t *d_harm = nullptr);
 int fsai_transpose_pattern(FsaiPattern *P, cudaStream_t st);
 int fsai_factor_full(const int32_t *d_rowptr, const int32_t *d_col, const double *d_K, const double *d_M, double dfc,
                      int64_t n, const int32_t *d_rowptrG, const int32_t *d_colG, int32_t nf, double2 *d_G,
@@ -67,7 +68,8 @@ struct SolverPlan {
   DevBuf rowptr, col;            // A pattern
   DevBuf KM64;                   // interleaved (K, M) per slot, FP64
   DevBuf RecA32;                 // FP32 path: one 16-byte (col, K, M) record per slot
-  DevBuf omega;                  // [nf] k * dfc
+  DevBuf omega;                  // [nf] h_j * dfc (FP64), then [nf] FP32
+  DevBuf harm;                   // [nf] harmonic index h_j of batch slot j
   FsaiPattern P;
   DevBuf G64, GT64;              // [nf][nnzG] complex128
   DevBuf RecG32, RecGT32;        // FP32 path: [nf][nnzG] 16-byte (col, Re, Im) records
@@ -85,9 +87,10 @@ struct SolverPlan {
   ~SolverPlan();
 };
 
+// h_harm: host list of the nf harmonic indices the plan solves (NULL = 0 .. nf-1)
 int solver_build(SolverPlan *S, const int32_t *d_rowptr, const int32_t *d_col, int64_t n, int64_t nnz,
                  const double *d_K, const double *d_M, double dfc, int32_t nf, int32_t ns_max,
-                 const dgp_solve_opts *opts, cudaStream_t st);
+                 const dgp_solve_opts *opts, cudaStream_t st, const int32_t *h_harm = nullptr);
 int solver_update(SolverPlan *S, const double *d_K, const double *d_M, cudaStream_t st);
 int solver_solve(SolverPlan *S, const double *d_B, const int32_t *d_nodes, const double *d_w,
                  const double *d_fpsf, double *d_X, int32_t ns, const dgp_solve_opts *opts,

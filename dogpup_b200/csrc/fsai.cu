@@ -77,7 +77,8 @@ __global__ void __launch_bounds__(128) k_fsai_factor(const int32_t *__restrict__
                                                      const double *__restrict__ Aim, int64_t n,
                                                      const int32_t *__restrict__ rowptrG,
                                                      const int32_t *__restrict__ colG, int nf,
-                                                     double2 *__restrict__ out, int64_t s_slot, int64_t s_k) {
+                                                     double2 *__restrict__ out, int64_t s_slot, int64_t s_k,
+                                                     const int32_t *__restrict__ harm) {
   constexpr int RB = 4, KT = 32;
   extern __shared__ double sh[];  // [RB][2][MMAX][MMAX]
   const int tr = threadIdx.x / KT, tk = threadIdx.x % KT;
@@ -113,7 +114,7 @@ __global__ void __launch_bounds__(128) k_fsai_factor(const int32_t *__restrict__
   const int gb = rowptrG[i], m = rowptrG[i + 1] - gb;
   const double *s0 = sh + (size_t)tr * 2 * MMAX * MMAX;
   const double *s1 = s0 + MMAX * MMAX;
-  const double kk = (double)k;
+  const double kk = (double)(harm ? harm[k] : k);
   double2 a[MMAX][MMAX];
   double2 y[MMAX];
   for (int r = 0; r < m; ++r) {
@@ -218,20 +219,20 @@ int fsai_pattern_rows(const int32_t *d_rowptr, const int32_t *d_col, const doubl
 
 int fsai_factor_run(const int32_t *d_rowptr, const int32_t *d_col, const double *d_re, const double *d_im,
                     int64_t n, const int32_t *d_rowptrG, const int32_t *d_colG, int32_t mmax, int32_t nf,
-                    double2 *d_out, int64_t s_slot, int64_t s_k, cudaStream_t st) {
+                    double2 *d_out, int64_t s_slot, int64_t s_k, cudaStream_t st, const int32_t *d_harm) {
   DGP_REQUIRE(mmax >= 1 && mmax <= 32, "fsai factor: pattern rows must hold 1..32 entries");
   DGP_REQUIRE(nf >= 1 && nf <= 65535 * 32, "fsai factor: bad number of harmonics");
   dim3 grid((unsigned)ceil_div(n, 4), (unsigned)ceil_div(nf, 32));
   if (mmax <= 8) {
     size_t sm = 4 * 2 * 8 * 8 * sizeof(double);
-    k_fsai_factor<8><<<grid, 128, sm, st>>>(d_rowptr, d_col, d_re, d_im, n, d_rowptrG, d_colG, nf, d_out, s_slot, s_k);
+    k_fsai_factor<8><<<grid, 128, sm, st>>>(d_rowptr, d_col, d_re, d_im, n, d_rowptrG, d_colG, nf, d_out, s_slot, s_k, d_harm);
   } else if (mmax <= 16) {
     size_t sm = 4 * 2 * 16 * 16 * sizeof(double);
-    k_fsai_factor<16><<<grid, 128, sm, st>>>(d_rowptr, d_col, d_re, d_im, n, d_rowptrG, d_colG, nf, d_out, s_slot, s_k);
+    k_fsai_factor<16><<<grid, 128, sm, st>>>(d_rowptr, d_col, d_re, d_im, n, d_rowptrG, d_colG, nf, d_out, s_slot, s_k, d_harm);
   } else {
     size_t sm = 4 * 2 * 32 * 32 * sizeof(double);
     DGP_CUDA(cudaFuncSetAttribute(k_fsai_factor<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_fsai_factor<32><<<grid, 128, sm, st>>>(d_rowptr, d_col, d_re, d_im, n, d_rowptrG, d_colG, nf, d_out, s_slot, s_k);
+    k_fsai_factor<32><<<grid, 128, sm, st>>>(d_rowptr, d_col, d_re, d_im, n, d_rowptrG, d_colG, nf, d_out, s_slot, s_k, d_harm);
   }
   DGP_CHECK_LAUNCH();
   return DGP_OK;

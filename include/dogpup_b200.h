@@ -190,6 +190,19 @@ int dgp_solver_create(dgp_solver_t *solver, const int32_t *d_rowptr,
                       const double *d_K, const double *d_M, double dfc,
                       int32_t nf, int32_t ns_max, const dgp_solve_opts *opts,
                       dgp_stream_t stream);
+/* As dgp_solver_create for an arbitrary set of harmonics: batch slot j
+ * solves A_h = K + i*h*dfc*M with h = h_harmonics[j] (a host array of nf
+ * indices >= 0; NULL = 0 .. nf-1, which is dgp_solver_create).  Right-hand
+ * sides, d_fpsf and solutions are then indexed by slot j.  Used to shard the
+ * harmonics of one mesh over several GPUs and to solve one harmonic alone;
+ * the reference always solves harmonics 0 .. NF-1 together (dMesh.m:1243). */
+int dgp_solver_create_harmonics(dgp_solver_t *solver, const int32_t *d_rowptr,
+                                const int32_t *d_col, int64_t n, int64_t nnz,
+                                const double *d_K, const double *d_M,
+                                double dfc, const int32_t *h_harmonics,
+                                int32_t nf, int32_t ns_max,
+                                const dgp_solve_opts *opts,
+                                dgp_stream_t stream);
 /* New K, M values on the same pattern (e.g. after a property update):
  * re-copies them and refactors FSAI. */
 int dgp_solver_update(dgp_solver_t solver, const double *d_K, const double *d_M,

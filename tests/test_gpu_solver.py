@@ -199,3 +199,30 @@ def test_solver_reports_maxit(small_case, gpu_case, torch):
     assert rep.iterations == 2
     assert (status.cpu().numpy() == 1).all()
     assert np.isfinite(X.cpu().numpy()).all()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_solver_harmonic_subset(small_case, gpu_case, torch, precision):
+    """A plan over harmonics [5, 0, 9] solves slot j at harmonic h_j: same as the full plan's columns."""
+    from dogpup_b200 import api
+    from oracle import solver as osv
+    K0, M0 = small_case["K"], small_case["M"]
+    harm = [5, 0, 9]
+    ns = 3
+    dfc = 2 * np.pi / 10e-9 / (C_VAC / 1.4)
+    nodes, w = _point_sources(small_case, ns, 21)
+    fpsf_all = np.exp(-0.25j * np.arange(10)) * (1.0 + 0.05 * np.arange(10))
+    fem = gpu_case["fem"]
+    S = api.Solver(fem.rowptr, fem.col, gpu_case["K"], gpu_case["M"], dfc, len(harm), ns, harmonics=harm)
+    opts = api.make_opts(tol=1e-12 if precision == "fp64" else 1e-10, precision=precision)
+    X, rep = S.solve_sources(torch.as_tensor(nodes, device="cuda"), torch.as_tensor(w, device="cuda"),
+                             torch.as_tensor(fpsf_all[harm], device="cuda"), opts)
+    Q = np.zeros((K0.shape[0], ns, 10), complex)
+    for s in range(ns):
+        Q[nodes[s], s, :] = w[s][:, None] * fpsf_all[None, :]
+    xd = osv.direct_solve(K0, M0, dfc, Q)[:, :, harm]
+    Xh = np.transpose(X.cpu().numpy(), (1, 2, 0))
+    err = np.linalg.norm(Xh - xd, axis=0) / np.linalg.norm(xd, axis=0)
+    assert err.max() < (1e-9 if precision == "fp64" else 1e-6), err.max()
+    with pytest.raises(ValueError):
+        api.Solver(fem.rowptr, fem.col, gpu_case["K"], gpu_case["M"], dfc, 2, ns, harmonics=[1])

@@ -167,6 +167,20 @@ def test_device_autograd_matches_finite_differences(dev_case):
 
 
 @pytest.mark.gpu
+def test_device_autograd_recompute_equals_stored(dev_case):
+    from dogpup_b200.autograd import TimeGatedForward
+    rec = TimeGatedForward(dev_case["mesh"], dev_case["gfc"], precision="fp64", tol=1e-13, recompute=True)
+    out = []
+    for model in (dev_case["model"], rec):
+        mua = dev_case["mua"].clone().requires_grad_(True)
+        musp = dev_case["musp"].clone().requires_grad_(True)
+        (model(mua, musp) * dev_case["g"]).sum().backward()
+        out.append((mua.grad.cpu().numpy(), musp.grad.cpu().numpy()))
+    # same solves in the same order on the same matrices: identical results
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+@pytest.mark.gpu
 def test_device_autograd_mixed_precision(dev_case):
     import torch
     from dogpup_b200.autograd import TimeGatedForward
