@@ -48,6 +48,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-secondary", action="store_true", help="skip the TG Jacobian / LM / plain-FP64 timings")
+    ap.add_argument("--only", choices=["tg", "lm"], default=None,
+                    help="run one secondary timing alone and print its JSON (profiling cases)")
+    ap.add_argument("--lm-grid-mm", type=float, default=2.0, help="voxel pitch of the LM step's Jacobian basis")
     return ap.parse_args()
 
 
@@ -233,9 +236,9 @@ def tg_jacobian_bench(reps=3):
             "tg_loss_gradient_s": round(t_grad, 3)}
 
 
-def lm_step_bench(reps=2):
+def lm_step_bench(reps=2, grid_mm=2.0):
     """Weighted LM normal-equation step of the 50k-node configuration: cylinder r30 h60 @1.5 mm,
-    32 x 32 optodes, 10 gates (10240 measurements), J on the in-mesh voxels of a 2 mm grid."""
+    32 x 32 optodes, 10 gates (10240 measurements), J on the in-mesh voxels of a grid_mm grid."""
     import ctypes as C
     import torch
     from dogpup_b200 import api, workloads
@@ -243,7 +246,7 @@ def lm_step_bench(reps=2):
     w = workloads.cylinder_fwd(seed=4, ns=32, nd=32, nf=32)
     mesh = workloads.build_dmesh(w)
     lo, hi = w["mesh"].node.min(0), w["mesh"].node.max(0)
-    mesh.mesh2grid(*[np.arange(lo[d], hi[d] + 1e-9, 2.0) for d in range(3)])
+    mesh.mesh2grid(*[np.arange(lo[d], hi[d] + 1e-9, grid_mm) for d in range(3)])
     P = mesh.m2g[mesh.gridinmesh]
     basis = api.Basis(P, np.full(P.shape[0], mesh.dxyz ** 3))
     phi, data = mesh.flu_solve(precision="mixed", tol=1e-8)
@@ -255,6 +258,8 @@ def lm_step_bench(reps=2):
     J = api.jacobian_tg(basis, phi, phiA, mesh.optode.s_fpsf, mesh._link(), gfc, nt, data_tg)  # Rytov
     nv, nmeas = J.shape[0], J.shape[1] * J.shape[2]
     Jt = J.reshape(nv, nmeas).contiguous()
+    del J, phi, phiA
+    mesh._solver = None          # release the solver workspace before the dense step
     rng = np.random.default_rng(9)
     W = torch.as_tensor(1.0 / (0.01 * (1 + rng.random(nmeas))) ** 2, device="cuda")
     y = torch.as_tensor(rng.standard_normal(nmeas) * 0.01, device="cuda")
@@ -272,7 +277,8 @@ def lm_step_bench(reps=2):
         check(lib.dgp_cholesky_solve(v(Hc), nv, nv, v(xc), api.stream_ptr()))
     ms_chol = _event_ms(chol, reps)
     syrk_flops = 3 * 2.0 * nmeas * nv * (nv + 128) / 2
-    return {"workload": f"cylinder r30 h60 @1.5mm, {mesh.nn} nodes, 32x32 optodes, 10 gates, {nv} voxels (2 mm)",
+    return {"workload": f"cylinder r30 h60 @1.5mm, {mesh.nn} nodes, 32x32 optodes, 10 gates, {nv} voxels "
+                        f"({grid_mm:g} mm)",
             "nmeas": nmeas, "nv": nv, "normal_eq_ms": round(ms_ne, 3), "cholesky_solve_ms": round(ms_chol, 3),
             "syrk_tflops_bf16_lower_bound": round(syrk_flops / (ms_ne * 1e-3) / 1e12, 1),
             "cholesky_tflops_fp64": round(nv ** 3 / 3 / (ms_chol * 1e-3) / 1e12, 2)}
@@ -404,7 +410,7 @@ def run_ours(a, rank, world, local_rank):
         log(f"[rank 0] plain FP64 per-RHS: {res['plain']}")
         res["tg"] = tg_jacobian_bench()
         log(f"[rank 0] TG Jacobian: {res['tg']}")
-        res["lm"] = lm_step_bench()
+        res["lm"] = lm_step_bench(grid_mm=a.lm_grid_mm)
         log(f"[rank 0] LM step: {res['lm']}")
     return res
 
@@ -439,6 +445,11 @@ def main():
         return
     import torch
     import torch.distributed as dist
+    if a.only:
+        torch.cuda.set_device(local_rank)
+        out = tg_jacobian_bench() if a.only == "tg" else lm_step_bench(grid_mm=a.lm_grid_mm)
+        print(json.dumps(out))
+        return
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local_rank))

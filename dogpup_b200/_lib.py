@@ -41,6 +41,9 @@ _SIGS = {
     "dgp_smv_mex": (C.c_int, [P, P, P, P, P, P, P, P, P, C.c_int, C.c_int, C.c_int, P]),
     "dgp_fsaimv_mex": (C.c_int, [P, P, P, P, P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, P]),
     "dgp_fsaip_mex": (C.c_int, [P, P, P, P, P, P, P, P, C.c_int, C.c_int, P]),
+    "dgp_smv_mex_ic": (C.c_int, [P, P, P, P, P, P, C.c_int, C.c_int, C.c_int, P]),
+    "dgp_fsaimv_mex_ic": (C.c_int, [P, P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, P]),
+    "dgp_fsaip_mex_ic": (C.c_int, [P, P, P, P, P, P, C.c_int, C.c_int, P]),
     "dgp_fsaip_mex_noalloc": (C.c_int, [P, P, P, P, P, P, P, P, C.c_int, C.c_int, P]),
     "dgp_fem_create": (C.c_int, [C.POINTER(P), P, P, I64, I64, D, P]),
     "dgp_fem_destroy": (C.c_int, [P]),
@@ -57,6 +60,7 @@ _SIGS = {
     "dgp_solver_destroy": (C.c_int, [P]),
     "dgp_solver_memory": (C.c_int, [P, C.POINTER(I64)]),
     "dgp_solve": (C.c_int, [P, P, P, I32, C.POINTER(SolveOpts), C.POINTER(SolveReport), P]),
+    "dgp_solve_mex": (C.c_int, [P, P, P, I32, I32, C.POINTER(SolveOpts), C.POINTER(SolveReport), P]),
     "dgp_solve_sources": (C.c_int, [P, P, P, P, I32, P, C.POINTER(SolveOpts), C.POINTER(SolveReport), P]),
     "dgp_solver_profile_kernel": (C.c_int, [P, I32, I32, C.POINTER(C.c_float), C.POINTER(D), P]),
     "dgp_spmm_A": (C.c_int, [P, P, P, P, I64, I32, I32, P, P, P]),

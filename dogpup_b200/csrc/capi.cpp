@@ -69,7 +69,7 @@ int sm_count() {
 
 int mex_spmv(int mode, double *out_re, double *out_im, const double *x_re, const double *x_im, const double *fAxis,
              const double *v_re, const double *v_im, const int *rPtr, const int *cPtr, int64_t nnz, int nrows,
-             int ncols, int nfreqs, cudaStream_t st);
+             int ncols, int nfreqs, cudaStream_t st, int es = 1);
 int td2fc_run(const double *x, int64_t nr, int nt, const double *t, const double *f, int nf, double *c,
               cudaStream_t st);
 int fc2td_run(const double *c, int64_t nr, int nf, const double *f, const double *t, int nt, double *x,
@@ -78,7 +78,8 @@ int fc2tg_run(const double *c, int64_t nr, int nf, const double *gate, int ng, i
 int meas_run(const int32_t *dn, const double *dw, int nd, const int32_t *link, int nm, const double *phi, int64_t n,
              int nf, int ns, double *data, cudaStream_t st);
 int mex_fsaip(double *out_re, double *out_im, const double *A_re, const double *A_im, const int *rPtrA,
-              const int *cPtrA, const int *rPtrG, const int *cPtrG, int nfreqs, int nrows, cudaStream_t st);
+              const int *cPtrA, const int *rPtrG, const int *cPtrG, int nfreqs, int nrows, cudaStream_t st,
+              int es = 1);
 int jacobian_run(int mode, const int32_t *prow, const int32_t *pcol, const double *pval, int64_t nv, const double *w,
                  const double *phi, int ns, const double *phiA, int nd, int64_t nn, int nf, const double *fpsf,
                  const int32_t *link, int nm, const double *gate, int ng, int nt, const double *rytov, void *out,
@@ -149,6 +150,27 @@ int dgp_fsaip_mex(double *d_out_real, double *d_out_imag, const double *d_valA_r
                   int nrows, dgp_stream_t stream) {
   DGP_GUARD(mex_fsaip(d_out_real, d_out_imag, d_valA_real, d_valA_imag, d_rPtrA, d_cPtrA, d_rPtrG, d_cPtrG, nfreqs,
                       nrows, (cudaStream_t)stream));
+}
+
+int dgp_smv_mex_ic(double *d_out, const double *d_x, const double *d_fAxis, const double *d_valA, const int *d_rPtr,
+                   const int *d_cPtr, int nrows, int ncols, int nfreqs, dgp_stream_t stream) {
+  if (!d_out || !d_x || !d_valA) return fail(DGP_ERR_ARG, "smv_mex_ic: null pointer");
+  DGP_GUARD(mex_spmv(0, d_out, d_out + 1, d_x, d_x + 1, d_fAxis, d_valA, d_valA + 1, d_rPtr, d_cPtr, 0, nrows, ncols,
+                     nfreqs, (cudaStream_t)stream, 2));
+}
+
+int dgp_fsaimv_mex_ic(double *d_out, const double *d_x, const double *d_valG, const int *d_rPtr, const int *d_cPtr,
+                      int nnz, int nrows, int ncols, int nfreqs, dgp_stream_t stream) {
+  if (!d_out || !d_x || !d_valG) return fail(DGP_ERR_ARG, "FSAImv_mex_ic: null pointer");
+  DGP_GUARD(mex_spmv(1, d_out, d_out + 1, d_x, d_x + 1, nullptr, d_valG, d_valG + 1, d_rPtr, d_cPtr, nnz, nrows,
+                     ncols, nfreqs, (cudaStream_t)stream, 2));
+}
+
+int dgp_fsaip_mex_ic(double *d_out, const double *d_valA, const int *d_rPtrA, const int *d_cPtrA, const int *d_rPtrG,
+                     const int *d_cPtrG, int nfreqs, int nrows, dgp_stream_t stream) {
+  if (!d_out || !d_valA) return fail(DGP_ERR_ARG, "FSAIP_mex_ic: null pointer");
+  DGP_GUARD(mex_fsaip(d_out, d_out + 1, d_valA, d_valA + 1, d_rPtrA, d_cPtrA, d_rPtrG, d_cPtrG, nfreqs, nrows,
+                      (cudaStream_t)stream, 2));
 }
 
 // -------------------------------------------------------------------- FEM
@@ -284,6 +306,12 @@ int dgp_solve(dgp_solver_t s, const double *d_B, double *d_X, int32_t ns, const 
               dgp_solve_report *report, dgp_stream_t stream) {
   if (!s || !d_B || !d_X) return fail(DGP_ERR_ARG, "solve: null pointer");
   DGP_GUARD(solver_solve(&s->plan, d_B, nullptr, nullptr, nullptr, d_X, ns, opts, report, (cudaStream_t)stream));
+}
+
+int dgp_solve_mex(dgp_solver_t s, const double *d_Q, double *d_X, int32_t ns, int32_t layout,
+                  const dgp_solve_opts *opts, dgp_solve_report *report, dgp_stream_t stream) {
+  if (!s) return fail(DGP_ERR_ARG, "solve_mex: null handle");
+  DGP_GUARD(solve_mexlayout(&s->plan, d_Q, d_X, ns, layout, opts, report, (cudaStream_t)stream));
 }
 
 int dgp_solve_sources(dgp_solver_t s, const int32_t *d_nodes, const double *d_w, const double *d_fpsf, int32_t ns,

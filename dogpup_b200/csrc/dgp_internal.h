@@ -96,6 +96,10 @@ int solver_solve(SolverPlan *S, const double *d_B, const int32_t *d_nodes, const
                  const double *d_fpsf, double *d_X, int32_t ns, const dgp_solve_opts *opts,
                  dgp_solve_report *rep, cudaStream_t st);
 
+// gpuBicstab_FSAIP on MATLAB's [N x NS x NF] interleaved layout (transposes around solver_solve)
+int solve_mexlayout(SolverPlan *S, const double *d_Q, double *d_X, int32_t ns, int32_t layout,
+                    const dgp_solve_opts *opts, dgp_solve_report *rep, cudaStream_t st);
+
 int solver_profile(SolverPlan *S, int which, int reps, float *ms, double *bytes, cudaStream_t st);
 
 // batched operators (layout [nf][n][ns] complex)

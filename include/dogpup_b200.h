@@ -91,6 +91,20 @@ int dgp_fsaip_mex(double *d_out_real, double *d_out_imag,
                   const int *d_cPtrG, int nfreqs, int nrows,
                   dgp_stream_t stream);
 
+/* The same three operations on interleaved complex data (MATLAB's
+ * interleaved-complex API, R2018a+): each complex array is one pointer to
+ * (re, im) pairs in the layout above, which saves the gateways the
+ * real/imaginary split copies the reference makes (mxGPUCopyReal/Imag). */
+int dgp_smv_mex_ic(double *d_out, const double *d_x, const double *d_fAxis,
+                   const double *d_valA, const int *d_rPtr, const int *d_cPtr,
+                   int nrows, int ncols, int nfreqs, dgp_stream_t stream);
+int dgp_fsaimv_mex_ic(double *d_out, const double *d_x, const double *d_valG,
+                      const int *d_rPtr, const int *d_cPtr, int nnz, int nrows,
+                      int ncols, int nfreqs, dgp_stream_t stream);
+int dgp_fsaip_mex_ic(double *d_out, const double *d_valA, const int *d_rPtrA,
+                     const int *d_cPtrA, const int *d_rPtrG, const int *d_cPtrG,
+                     int nfreqs, int nrows, dgp_stream_t stream);
+
 /* No counterpart in the reference.  dgp_fsaip_mex for callers that must not
  * allocate device memory -- a MATLAB mex gateway whose device memory has to
  * come from MATLAB's gpuArray pool, or an application whose own pooling
@@ -217,6 +231,20 @@ int dgp_solver_memory(dgp_solver_t solver, int64_t *bytes);
 int dgp_solve(dgp_solver_t solver, const double *d_B, double *d_X, int32_t ns,
               const dgp_solve_opts *opts, dgp_solve_report *report,
               dgp_stream_t stream);
+
+/* dgp_solve on MATLAB's layouts: d_Q and d_X are column-major complex128
+ * with interleaved real/imaginary parts (the data of a complex array under
+ * MATLAB's interleaved-complex API):
+ *   DGP_LAYOUT_N_NS_NF: [N x NS x NF] (x of smv_mex, gpuBicstab_FSAIP's
+ *                       working layout, dMesh.m:1264)
+ *   DGP_LAYOUT_N_NF_NS: [N x NF x NS] (fluGPU's Q and phi, dMesh.m:1238-1243)
+ * This is the entry the bicgstab_fsai_mex gateway calls; the reference has
+ * no single-call counterpart (it drives smv_mex / FSAImv_mex from a MATLAB
+ * loop, dMesh.m:1247-1348). */
+enum { DGP_LAYOUT_N_NS_NF = 0, DGP_LAYOUT_N_NF_NS = 1 };
+int dgp_solve_mex(dgp_solver_t solver, const double *d_Q, double *d_X,
+                  int32_t ns, int32_t layout, const dgp_solve_opts *opts,
+                  dgp_solve_report *report, dgp_stream_t stream);
 
 /* Same solve with the point-source right-hand sides of flu_solve /
  * adj_flu_solve (dMesh.m:124-129, :191-196) generated on the device:
