@@ -76,12 +76,35 @@ def build_library(verbose: bool = False, jobs: int | None = None) -> Path:
     return LIB
 
 
+DRIVER_SRC = PKG / "driver" / "dgp_forward.cpp"
+DRIVER = PKG / "dgp_forward"
+
+
+def build_driver(verbose: bool = False) -> Path:
+    """The standalone C++ driver, linked against the in-tree library (rpath = this folder)."""
+    lib = build_library(verbose)
+    deps = [DRIVER_SRC, lib, ROOT / "include" / "dogpup_b200.h"]
+    if DRIVER.exists() and DRIVER.stat().st_mtime >= max(d.stat().st_mtime for d in deps):
+        return DRIVER
+    cuda = Path(nvcc()).resolve().parent.parent
+    cmd = ["g++", "-O2", "-std=c++17", f"-I{ROOT / 'include'}", f"-I{cuda / 'include'}", str(DRIVER_SRC),
+           f"-L{PKG}", "-ldogpup_b200", f"-Wl,-rpath,{PKG}", f"-L{cuda / 'lib64'}", "-lcudart",
+           f"-Wl,-rpath,{cuda / 'lib64'}", "-o", str(DRIVER)]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"driver build failed:\n{r.stdout}\n{r.stderr}")
+    return DRIVER
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--all", action="store_true", help="also build the oracle C code and reference kernels")
     ap.add_argument("-v", "--verbose", action="store_true")
     a = ap.parse_args(argv)
     print(build_library(a.verbose))
+    print(build_driver(a.verbose))
     if a.all:
         subprocess.run(["make", "-C", str(ROOT / "oracle")], check=True)
 
