@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--only", choices=["tg", "lm"], default=None,
                     help="run one secondary timing alone and print its JSON (profiling cases)")
     ap.add_argument("--lm-grid-mm", type=float, default=2.0, help="voxel pitch of the LM step's Jacobian basis")
+    ap.add_argument("--order", choices=["morton", "lattice"], default="morton", help="mesh node numbering")
     return ap.parse_args()
 
 
@@ -58,12 +59,12 @@ def log(msg):
     print(msg, file=sys.stderr, flush=True)
 
 
-def workload(name, seed=1):
+def workload(name, seed=1, order="morton"):
     from dogpup_b200 import workloads
     if name == "medium":  # same shape family at a coarser lattice: 19k nodes, 64 x 32 RHS (profiling case)
-        return workloads.ellipsoid_fwd(seed=seed, h=2.4, nf=32)
+        return workloads.ellipsoid_fwd(seed=seed, h=2.4, nf=32, order=order)
     return {"ellipsoid": workloads.ellipsoid_fwd, "cylinder": workloads.cylinder_fwd,
-            "small": workloads.small_fwd}[name](seed=seed)
+            "small": workloads.small_fwd}[name](seed=seed, order=order)
 
 
 # ------------------------------------------------------------------ clocks
@@ -317,7 +318,7 @@ def run_ours(a, rank, world, local_rank):
     import torch.distributed as dist
     from dogpup_b200 import workloads
     torch.cuda.set_device(local_rank)
-    w = workload(a.workload, seed=1 + rank)
+    w = workload(a.workload, seed=1 + rank, order=a.order)
     mesh = workloads.build_dmesh(w)
     ns, nf = len(w["src"]), w["nf"]
     solver = mesh.solver()
@@ -423,7 +424,7 @@ def main():
     if a.impl == "reference":
         if rank != 0:
             return
-        w = workload(a.workload)
+        w = workload(a.workload, order=a.order)
         for _ in range(a.warmup):
             cpu_sample(w, tol=a.tol)
         vals = []
@@ -470,7 +471,7 @@ def main():
                        "sources": len(w["src"]), "harmonics": w["nf"], "tol": a.tol, "inner_tol": a.inner_tol,
                        "iterations": rep.iterations, "refinements": rep.refinements,
                        "max_rel_residual": rep.max_rel_residual, "l2": "inputs larger than L2 (vectors ~GB)",
-                       "parallelism": f"replicas x{world}"},
+                       "parallelism": f"replicas x{world}", "node_order": a.order},
             "e2e": r["e2e"], "roofline": r["roof"], "cpu_baseline": cpu, "clocks": r["clocks"],
             "gpu_launches": r["launches"],
             "plain_fp64_per_rhs": r.get("plain"), "tg_jacobian": r.get("tg"), "lm_step": r.get("lm"),

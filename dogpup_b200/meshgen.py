@@ -4,9 +4,13 @@ These generators produce the inputs of the forward/sensitivity path: a
 regular cube lattice clipped to a shape, each cube split into 6 linear
 tetrahedra around its main diagonal (the conforming Kuhn split, the same
 lattice family as iso2mesh ``meshgrid6``), and interior nodes jittered by a
-seeded uniform offset.  Nodes are numbered in lattice order (x fastest, z
-slowest), which keeps the FEM matrix bandwidth near one lattice plane and the
-sparse gathers of the solver cache-friendly.
+seeded uniform offset.  Nodes are numbered either in lattice order (x
+fastest, z slowest: FEM matrix bandwidth of about one lattice plane) or in
+Morton (Z-curve) order of their lattice coordinates, which puts each run of
+64 consecutive nodes in a compact 4x4x4 region, so a block of SpMM rows
+gathers mostly from nodes that other rows of the same block also read (the
+locality ``sortmesh`` aims at in the reference's meshing stack,
+meshing/iso2mesh/sortmesh.m).
 
 The reference builds its meshes with iso2mesh (``meshabox`` + ``sortmesh``,
 tutorials/tut_1_meshing.m:5-7); that meshing stack is third-party and out of
@@ -65,12 +69,29 @@ def boundary_nodes(elem: np.ndarray, nn: int) -> np.ndarray:
     return bnd
 
 
-def lattice_mesh(inside, lo, hi, h, jitter=0.0, seed=0) -> TetMesh:
+def _spread_bits(v: np.ndarray) -> np.ndarray:
+    """Bits 0..20 of v moved to bits 0, 3, 6, ... (3-D Morton interleave)."""
+    v = v.astype(np.uint64) & np.uint64(0x1FFFFF)
+    for shift, mask in ((32, 0x1F00000000FFFF), (16, 0x1F0000FF0000FF), (8, 0x100F00F00F00F00F),
+                        (4, 0x10C30C30C30C30C3), (2, 0x1249249249249249)):
+        v = (v | (v << np.uint64(shift))) & np.uint64(mask)
+    return v
+
+
+def morton_order(lat: np.ndarray) -> np.ndarray:
+    """Permutation sorting lattice coordinates [N, 3] (each < 2^21) along the Z-curve."""
+    key = _spread_bits(lat[:, 0]) | (_spread_bits(lat[:, 1]) << np.uint64(1)) | (_spread_bits(lat[:, 2]) << np.uint64(2))
+    return np.argsort(key, kind="stable")
+
+
+def lattice_mesh(inside, lo, hi, h, jitter=0.0, seed=0, order="morton") -> TetMesh:
     """Cube lattice of spacing ``h`` over the box [lo, hi], keeping cubes whose
     centre satisfies ``inside(xyz) -> bool``; 6 tets per kept cube.
 
     Interior nodes are moved by an independent uniform offset in
-    [-jitter, jitter] per coordinate drawn from ``numpy.random.default_rng(seed)``.
+    [-jitter, jitter] per coordinate drawn from ``numpy.random.default_rng(seed)``
+    in lattice order, so both node orders ("lattice", "morton") give the same
+    geometry.
     """
     lo = np.asarray(lo, dtype=np.float64)
     hi = np.asarray(hi, dtype=np.float64)
@@ -102,10 +123,17 @@ def lattice_mesh(inside, lo, hi, h, jitter=0.0, seed=0) -> TetMesh:
         d = rng.uniform(-jitter, jitter, size=node.shape)
         d[bnd] = 0.0
         node = node + d
+    if order == "morton":
+        perm = morton_order(lat)
+        new_id = np.empty_like(perm)
+        new_id[perm] = np.arange(perm.shape[0])
+        node, bnd, lat, elem = node[perm], bnd[perm], lat[perm], new_id[elem]
+    elif order != "lattice":
+        raise ValueError("order must be 'lattice' or 'morton'")
     return TetMesh(node=node, elem=elem.astype(np.int32), bnd=bnd, lattice=lat, h=float(h), origin=lo)
 
 
-def cylinder_mesh(radius, height, h, jitter=0.0, seed=0, centre=(0.0, 0.0, 0.0)) -> TetMesh:
+def cylinder_mesh(radius, height, h, jitter=0.0, seed=0, centre=(0.0, 0.0, 0.0), order="morton") -> TetMesh:
     """Cylinder with its axis along z, base at ``centre[2]``."""
     cx, cy, cz = centre
 
@@ -114,10 +142,10 @@ def cylinder_mesh(radius, height, h, jitter=0.0, seed=0, centre=(0.0, 0.0, 0.0))
 
     lo = (cx - radius, cy - radius, cz)
     hi = (cx + radius, cy + radius, cz + height)
-    return lattice_mesh(inside, lo, hi, h, jitter, seed)
+    return lattice_mesh(inside, lo, hi, h, jitter, seed, order)
 
 
-def ellipsoid_mesh(axes, h, jitter=0.0, seed=0, centre=(0.0, 0.0, 0.0)) -> TetMesh:
+def ellipsoid_mesh(axes, h, jitter=0.0, seed=0, centre=(0.0, 0.0, 0.0), order="morton") -> TetMesh:
     """Ellipsoid with full axis lengths ``axes`` (mm) along x, y, z."""
     a = np.asarray(axes, dtype=np.float64) / 2.0
     c = np.asarray(centre, dtype=np.float64)
@@ -125,11 +153,11 @@ def ellipsoid_mesh(axes, h, jitter=0.0, seed=0, centre=(0.0, 0.0, 0.0)) -> TetMe
     def inside(p):
         return (((p - c) / a) ** 2).sum(axis=1) <= 1.0
 
-    return lattice_mesh(inside, c - a, c + a, h, jitter, seed)
+    return lattice_mesh(inside, c - a, c + a, h, jitter, seed, order)
 
 
-def box_mesh(size, h, jitter=0.0, seed=0) -> TetMesh:
-    return lattice_mesh(lambda p: np.ones(p.shape[0], dtype=bool), (0, 0, 0), size, h, jitter, seed)
+def box_mesh(size, h, jitter=0.0, seed=0, order="morton") -> TetMesh:
+    return lattice_mesh(lambda p: np.ones(p.shape[0], dtype=bool), (0, 0, 0), size, h, jitter, seed, order)
 
 
 def smooth_random_field(mesh: TetMesh, corr_mm: float, seed: int) -> np.ndarray:

@@ -34,9 +34,9 @@ def all_pairs(ns, nd):
     return np.stack([s.ravel(), d.ravel()], axis=1)
 
 
-def cylinder_fwd(seed=1, h=1.5, ns=16, nd=16, nf=32):
+def cylinder_fwd(seed=1, h=1.5, ns=16, nd=16, nf=32, order="morton"):
     """Plain FP64 forward, small: cylinder r=30 h=60 mm at 1.5 mm, 16+16 optodes on the mid ring, 32 harmonics."""
-    m = meshgen.cylinder_mesh(30.0, 60.0, h, jitter=0.2, seed=seed)
+    m = meshgen.cylinder_mesh(30.0, 60.0, h, jitter=0.2, seed=seed, order=order)
     c = np.array([0.0, 0.0, 30.0])
     src = ring(ns, c, (30.0, 30.0), 30.0)
     det = ring(nd, c, (30.0, 30.0), 30.0, phase=np.pi / nd)
@@ -44,9 +44,9 @@ def cylinder_fwd(seed=1, h=1.5, ns=16, nd=16, nf=32):
                 nr=1.4, src=src, det=det, link=all_pairs(ns, nd), t=time_axis(10e-9), nf=nf)
 
 
-def ellipsoid_fwd(seed=1, axes=(90.0, 75.0, 70.0), h=1.2, ns=64, nd=64, nf=128, grf_corr_mm=8.0):
+def ellipsoid_fwd(seed=1, axes=(90.0, 75.0, 70.0), h=1.2, ns=64, nd=64, nf=128, grf_corr_mm=8.0, order="morton"):
     """Batched mixed forward: ellipsoid head phantom, mua = 0.01 (1 + 0.2 GRF), 64 sources x 128 harmonics."""
-    m = meshgen.ellipsoid_mesh(axes, h, jitter=0.2, seed=seed)
+    m = meshgen.ellipsoid_mesh(axes, h, jitter=0.2, seed=seed, order=order)
     grf = meshgen.smooth_random_field(m, grf_corr_mm, seed + 100)
     mua = 0.01 * (1.0 + 0.2 * grf)
     a = np.asarray(axes) / 2
@@ -64,9 +64,9 @@ def ellipsoid_fwd(seed=1, axes=(90.0, 75.0, 70.0), h=1.2, ns=64, nd=64, nf=128, 
                 t=time_axis(10e-9), nf=nf)
 
 
-def small_fwd(seed=1, ns=8, nd=8, nf=8):
+def small_fwd(seed=1, ns=8, nd=8, nf=8, order="morton"):
     """A few-thousand-node cylinder for smoke tests."""
-    m = meshgen.cylinder_mesh(10.0, 16.0, 1.5, jitter=0.2, seed=seed)
+    m = meshgen.cylinder_mesh(10.0, 16.0, 1.5, jitter=0.2, seed=seed, order=order)
     c = np.array([0.0, 0.0, 8.0])
     src = ring(ns, c, (10.0, 10.0), 8.0)
     det = ring(nd, c, (10.0, 10.0), 8.0, phase=np.pi / nd)

@@ -142,3 +142,20 @@ def test_c_port_matches_numpy_oracle(small_case):
     Xd = solver.direct_solve(K, M, k * dfc, np.stack([B, B], axis=2))[:, :, 1]   # harmonic 1 of k*dfc
     assert np.linalg.norm(X - Xd) / np.linalg.norm(Xd) < 1e-9
     assert (it > 3).all()
+
+
+def test_morton_and_lattice_orders_are_the_same_mesh():
+    a = cylinder_mesh(5, 6, 1.5, jitter=0.2, seed=4, order="lattice")
+    b = cylinder_mesh(5, 6, 1.5, jitter=0.2, seed=4, order="morton")
+    assert a.nn == b.nn and a.ne == b.ne
+    # same node positions under the permutation given by the lattice coordinates
+    ka = {tuple(x): i for i, x in enumerate(a.lattice)}
+    perm = np.array([ka[tuple(x)] for x in b.lattice])
+    assert np.array_equal(a.node[perm], b.node)
+    assert np.array_equal(a.bnd[perm], b.bnd)
+    ea = {tuple(sorted(e)) for e in a.elem.tolist()}
+    eb = {tuple(sorted(perm[e])) for e in b.elem.tolist()}
+    assert ea == eb
+    # Morton order: consecutive runs of 64 nodes span compact lattice boxes
+    spans = [np.ptp(b.lattice[i:i + 64], axis=0).max() for i in range(0, b.nn - 64, 64)]
+    assert np.median(spans) <= 7
