@@ -66,7 +66,9 @@ def build_library(verbose: bool = False, jobs: int | None = None) -> Path:
     if LIB.exists() and LIB.stat().st_mtime >= max(o.stat().st_mtime for o in objs):
         return LIB
     tmp = LIB.with_suffix(".so.tmp")
-    cmd = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", *map(str, objs), "-o", str(tmp)]
+    cuda_lib = Path(nvcc()).resolve().parent.parent / "lib64"
+    cmd = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", *map(str, objs), f"-L{cuda_lib}", "-lcublas",
+           "-Xlinker", "-rpath", "-Xlinker", str(cuda_lib), "-o", str(tmp)]
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -154,6 +154,12 @@ template <class C> __device__ inline void acc_bil(double2 &s, C a, C b) {
   s.x += x.x * y.x - x.y * y.y;
   s.y += x.x * y.y + x.y * y.x;
 }
+// FP32 partials of the FP32 solver's SpMM dots: each lane sums at most one
+// block's rows (<= 32) in FP32 before the FP64 lane / warp / block reduction
+__device__ inline void acc_bil(float2 &s, float2 a, float2 b) {
+  s.x = fmaf(a.x, b.x, fmaf(-a.y, b.y, s.x));
+  s.y = fmaf(a.x, b.y, fmaf(a.y, b.x, s.y));
+}
 template <class C> __device__ inline void acc_abs2(double &s, C a) {
   double2 x = d2(a);
   s += x.x * x.x + x.y * x.y;
@@ -338,11 +344,11 @@ __global__ void __launch_bounds__(BS) k_spmm(Layout L, Op op, const typename CT<
   const int c0 = ln.template col0<E>(), cs = ln.template cs<E>(L);
   const C *Xk = X + (int64_t)ln.k * L.n * L.nsp + c0;
   constexpr int NQ = MODE == 2 ? 2 : 1;
-  double2 part[VEC][NQ];
+  C part[VEC][NQ];  // per-lane partial sums in the sweep's precision (FP32 lanes: <= 32 rows each)
 #pragma unroll
   for (int v = 0; v < VEC; ++v)
 #pragma unroll
-    for (int q = 0; q < NQ; ++q) part[v][q] = make_double2(0, 0);
+    for (int q = 0; q < NQ; ++q) part[v][q] = czero<C>();
   for (int it = 0; it < L.ipb; ++it) {
     const int64_t i = ln.row(L, it);
     if (i >= L.n) break;
@@ -360,12 +366,19 @@ __global__ void __launch_bounds__(BS) k_spmm(Layout L, Op op, const typename CT<
       }
     }
   }
-  if constexpr (MODE == 1) {
-    const int slot[1] = {ACC_D1};
-    block_reduce<VEC, 1, E>(L, ln, part, cols.acc, cols.C, slot, smem);
-  } else if constexpr (MODE == 2) {
-    const int slot[2] = {ACC_D2, ACC_D3};
-    block_reduce<VEC, 2, E>(L, ln, part, cols.acc, cols.C, slot, smem);
+  if constexpr (MODE != 0) {
+    double2 pd[VEC][NQ];
+#pragma unroll
+    for (int v = 0; v < VEC; ++v)
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) pd[v][q] = d2(part[v][q]);
+    if constexpr (MODE == 1) {
+      const int slot[1] = {ACC_D1};
+      block_reduce<VEC, 1, E>(L, ln, pd, cols.acc, cols.C, slot, smem);
+    } else {
+      const int slot[2] = {ACC_D2, ACC_D3};
+      block_reduce<VEC, 2, E>(L, ln, pd, cols.acc, cols.C, slot, smem);
+    }
   }
 }
 
@@ -1104,7 +1117,9 @@ void enqueue_iteration(const SolverPlan *S, const OpA &A, const OpG &G, const Op
 
 template <class R, int VS>
 int enqueue_for(SolverPlan *S, const Vecs<R> &V, const Work &W, cudaStream_t st) {
-  constexpr int VD = VS < 4 ? VS : 4;
+  // lane width of the SpMM sweeps with dot products: the FP32 sweeps keep their
+  // partials in FP32 and afford the plain sweeps' width; FP64 ones cap at 4
+  constexpr int VD = sizeof(R) == 4 ? VS : (VS < 4 ? VS : 4);
   const int32_t *rp = S->rowptr.as<int32_t>();
   if constexpr (sizeof(R) == 4) {
     OpA32 A{rp, S->RecA32.as<Rec32>(), (const float *)(S->omega.as<char>() + sizeof(double) * S->nf)};

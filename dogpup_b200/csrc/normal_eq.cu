@@ -10,6 +10,13 @@
 //   r = J' W y                         FP64
 //   H = L L', solve L L' x = r         FP64 blocked Cholesky + triangular solves
 //
+// Cholesky: right-looking over 256-column block steps.  The 256 x 256
+// diagonal block is factored by this file's kernels (64-column steps: one
+// CTA per 64 x 64 diagonal factor, a thread per panel row for the triangular
+// solve, 64 x 64 tiles for the update inside the block); the panel below it
+// is a cuBLAS DTRSM and the trailing update a cuBLAS DSYRK (plain BLAS-3,
+// where n^3/3 of the flops are).
+//
 // Input J is given transposed, Jt [nv][nmeas] float32 row-major -- the layout
 // the TG Jacobian kernel writes -- so both GEMM operands are K-major.
 //
@@ -30,8 +37,11 @@
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
+#include <cublas_v2.h>
+
 #include <algorithm>
 #include <cmath>
+#include <map>
 #include <mutex>
 
 #include "dgp_common.cuh"
@@ -509,22 +519,62 @@ int normal_eq_run(const float *Jt, int64_t nv, int64_t nm, const double *W, cons
   return DGP_OK;
 }
 
+// one cuBLAS handle per device, created on first use and kept for the process
+cublasHandle_t blas_handle(std::unique_lock<std::mutex> &lk) {
+  static std::mutex mu;
+  static std::map<int, cublasHandle_t> handles;
+  lk = std::unique_lock<std::mutex>(mu);
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  auto it = handles.find(dev);
+  if (it != handles.end()) return it->second;
+  cublasHandle_t h = nullptr;
+  if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) return nullptr;
+  handles[dev] = h;
+  return h;
+}
+
 int cholesky_solve_run(double *H, int64_t n, int64_t ldh, double *x, cudaStream_t st) {
   DGP_REQUIRE(H && x && n > 0 && ldh >= n, "cholesky: bad arguments");
+  DGP_REQUIRE(n <= INT32_MAX && ldh <= INT32_MAX, "cholesky: n and ldh must fit int32 (cuBLAS)");
   DevBuf errb;
   DGP_TRY(errb.alloc(sizeof(int)));
   DGP_CUDA(cudaMemsetAsync(errb.p, 0, sizeof(int), st));
-  for (int64_t k0 = 0; k0 < n; k0 += NB) {
-    const int nb = (int)std::min<int64_t>(NB, n - k0);
-    k_potrf_diag<<<1, 256, 0, st>>>(H, ldh, k0, nb, errb.as<int>());
-    const int64_t rest = n - k0 - nb;
-    count_launches(rest > 0 ? 3 : 1);
-    if (rest > 0) {
-      k_trsm_panel<<<(unsigned)ceil_div(rest, 128), 128, 0, st>>>(H, ldh, k0, nb, n);
-      const int64_t T = ceil_div(rest, NB);
-      k_chol_update<<<(unsigned)(T * (T + 1) / 2), 256, 0, st>>>(H, ldh, k0, nb, n);
+  constexpr int64_t NBO = 256;  // outer block step: DTRSM panel + DSYRK trailing update
+  std::unique_lock<std::mutex> lk;
+  cublasHandle_t hb = blas_handle(lk);
+  if (!hb) return fail(DGP_ERR_CUDA, "cholesky: cuBLAS handle creation failed");
+  if (cublasSetStream(hb, st) != CUBLAS_STATUS_SUCCESS) return fail(DGP_ERR_CUDA, "cholesky: cublasSetStream failed");
+  const double one = 1.0, minus_one = -1.0;
+  for (int64_t k0 = 0; k0 < n; k0 += NBO) {
+    const int64_t kend = std::min(n, k0 + NBO);
+    // factor the diagonal block [k0, kend) in 64-column steps
+    for (int64_t j0 = k0; j0 < kend; j0 += NB) {
+      const int nb = (int)std::min<int64_t>(NB, kend - j0);
+      k_potrf_diag<<<1, 256, 0, st>>>(H, ldh, j0, nb, errb.as<int>());
+      const int64_t rest = kend - j0 - nb;
+      count_launches(rest > 0 ? 3 : 1);
+      if (rest > 0) {
+        k_trsm_panel<<<(unsigned)ceil_div(rest, 128), 128, 0, st>>>(H, ldh, j0, nb, kend);
+        const int64_t T = ceil_div(rest, NB);
+        k_chol_update<<<(unsigned)(T * (T + 1) / 2), 256, 0, st>>>(H, ldh, j0, nb, kend);
+      }
     }
+    DGP_CHECK_LAUNCH();
+    const int64_t rest = n - kend, nb = kend - k0;
+    if (rest <= 0) break;
+    // Column-major view of the row-major lower triangle: Hc = H^T (upper), leading dimension ldh.
+    // Panel rows [kend, n) x cols [k0, kend):  P <- P L^-T   <=>  Pc <- (Lc^T)^-1 Pc
+    if (cublasDtrsm(hb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, (int)nb,
+                    (int)rest, &one, H + k0 * ldh + k0, (int)ldh, H + kend * ldh + k0,
+                    (int)ldh) != CUBLAS_STATUS_SUCCESS)
+      return fail(DGP_ERR_CUDA, "cholesky: cublasDtrsm failed");
+    // Trailing lower triangle: H[i][l] -= sum_j P[i][j] P[l][j]  <=>  upper(Cc) -= Pc^T Pc
+    if (cublasDsyrk(hb, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, (int)rest, (int)nb, &minus_one, H + kend * ldh + k0,
+                    (int)ldh, &one, H + kend * ldh + kend, (int)ldh) != CUBLAS_STATUS_SUCCESS)
+      return fail(DGP_ERR_CUDA, "cholesky: cublasDsyrk failed");
   }
+  lk.unlock();
   DGP_CHECK_LAUNCH();
   for (int64_t k0 = 0; k0 < n; k0 += NB) {  // L y = b
     const int nb = (int)std::min<int64_t>(NB, n - k0);

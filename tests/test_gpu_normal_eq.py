@@ -48,28 +48,35 @@ def test_normal_equations_match_fp64(nv, nm):
     assert np.linalg.norm(rhs.cpu().numpy() - r0) / np.linalg.norm(r0) < 1e-12
 
 
-def test_cholesky_solve_exact_matrix():
+@pytest.mark.parametrize("n,pad", [(333, 0), (1100, 7)])
+def test_cholesky_solve_exact_matrix(n, pad):
+    """n > 256 crosses the 256-column block steps (DTRSM panel + DSYRK update); pad > 0 tests ldh > n."""
     import torch
     from dogpup_b200._lib import lib, check
     rng = np.random.default_rng(3)
-    n = 333
     A = rng.standard_normal((n, n))
     H0 = A @ A.T + n * np.eye(n)
     b = rng.standard_normal(n)
-    H = torch.as_tensor(np.tril(H0), device="cuda").contiguous()
+    ldh = n + pad
+    Hp = np.full((n, ldh), np.nan)
+    Hp[:, :n] = np.tril(H0)
+    Hp[:, :n][np.triu_indices(n, 1)] = np.nan        # the strict upper triangle is never read
+    H = torch.as_tensor(Hp, device="cuda").contiguous()
     x = torch.as_tensor(b, device="cuda").clone()
-    check(lib.dgp_cholesky_solve(_v(H), n, n, _v(x), None))
+    check(lib.dgp_cholesky_solve(_v(H), n, ldh, _v(x), None))
     x0 = np.linalg.solve(H0, b)
     assert np.linalg.norm(x.cpu().numpy() - x0) / np.linalg.norm(x0) < 1e-10
-    L = np.tril(H.cpu().numpy())
+    L = np.tril(H.cpu().numpy()[:, :n])
     assert np.linalg.norm(L @ L.T - H0) / np.linalg.norm(H0) < 1e-13
 
 
-def test_cholesky_rejects_indefinite_matrix():
+@pytest.mark.parametrize("n,bad", [(70, 0), (600, 530)])
+def test_cholesky_rejects_indefinite_matrix(n, bad):
     import torch
     from dogpup_b200._lib import lib
-    n = 70
-    H = torch.as_tensor(-np.eye(n), device="cuda").contiguous()
+    d = np.ones(n)
+    d[bad] = -1.0
+    H = torch.as_tensor(np.diag(d), device="cuda").contiguous()
     x = torch.ones(n, dtype=torch.float64, device="cuda")
     assert lib.dgp_cholesky_solve(_v(H), n, n, _v(x), None) == 1
 

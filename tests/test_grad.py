@@ -176,8 +176,10 @@ def test_device_autograd_recompute_equals_stored(dev_case):
         musp = dev_case["musp"].clone().requires_grad_(True)
         (model(mua, musp) * dev_case["g"]).sum().backward()
         out.append((mua.grad.cpu().numpy(), musp.grad.cpu().numpy()))
-    # same solves in the same order on the same matrices: identical results
-    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    # the same solves on the same matrices; only the order of the FP64 atomic
+    # partial sums inside the solver's dot products may differ between runs
+    for a, b in zip(out[0], out[1]):
+        assert np.abs(a - b).max() <= 1e-10 * np.abs(a).max()
 
 
 @pytest.mark.gpu
