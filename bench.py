@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-secondary", action="store_true", help="skip the TG Jacobian / LM / plain-FP64 timings")
-    ap.add_argument("--only", choices=["tg", "lm"], default=None,
+    ap.add_argument("--only", choices=["tg", "lm", "recon"], default=None,
                     help="run one secondary timing alone and print its JSON (profiling cases)")
     ap.add_argument("--lm-grid-mm", type=float, default=2.0, help="voxel pitch of the LM step's Jacobian basis")
     ap.add_argument("--order", choices=["morton", "lattice"], default="morton", help="mesh node numbering")
@@ -285,6 +285,61 @@ def lm_step_bench(reps=2, grid_mm=2.0):
             "cholesky_tflops_fp64": round(nv ** 3 / 3 / (ms_chol * 1e-3) / 1e12, 2)}
 
 
+def lm_recon_bench(max_iter=10, grid_mm=2.0, seed=7):
+    """Weighted LM reconstruction: cylinder r30 h60 @1.5 mm, 32 x 32 optodes, 10 gates of 500 ps;
+    truth = two spheres of r = 8 mm with 2x mua at seeded positions; data with 1 % count-scaled
+    noise (sigma = 1 % x sqrt(data x the curve's peak)), W = 1/sigma^2.  Runs the loop with
+    mixed-precision solves + split-BF16 normal equations, and again all-FP64 (FP64 solves, FP64
+    J^T W J); reports per-iteration mua error vs truth and vs the FP64 run, and the time."""
+    import torch
+    from dogpup_b200 import api, workloads
+    from dogpup_b200.recon import LMRecon
+    rng = np.random.default_rng(seed)
+    w = workloads.cylinder_fwd(seed=4, ns=32, nd=32, nf=32)
+    node = w["mesh"].node
+    truth = np.full(w["mesh"].nn, 0.01)
+    centres = []
+    while len(centres) < 2:
+        p = np.array([rng.uniform(-12, 12), rng.uniform(-12, 12), rng.uniform(20, 40)])
+        if p[0] ** 2 + p[1] ** 2 < 14 ** 2 and all(np.linalg.norm(p - q) > 18 for q in centres):
+            centres.append(p)
+    for p in centres:
+        truth[((node - p) ** 2).sum(1) < 8.0 ** 2] = 0.02
+    w["mua"] = truth
+    mesh = workloads.build_dmesh(w)
+    nt = len(w["t"])
+    gfc = api.td2fc(torch.as_tensor(_gates(w["t"], 10, 500e-12, 0.5e-9, 500e-12), device="cuda"),
+                    torch.as_tensor(mesh.optode.fAxis), torch.as_tensor(w["t"]))
+    _, data = mesh.flu_solve(precision="fp64", tol=1e-12)
+    clean = api.fc2tg(data, gfc, nt).cpu().numpy()
+    sigma = 0.01 * np.sqrt(np.abs(clean) * np.abs(clean).max(axis=1, keepdims=True))
+    data_m = np.abs(clean + sigma * rng.standard_normal(clean.shape))
+    lo, hi = node.min(0), node.max(0)
+    mesh.mesh2grid(*[np.arange(lo[d], hi[d] + 1e-9, grid_mm) for d in range(3)])
+    truth_d = torch.as_tensor(truth, device="cuda")
+    out = {}
+    for tag, prec, ne in (("mixed_split_bf16", "mixed", "split_bf16"), ("fp64", "fp64", "fp64")):
+        mesh.mua = torch.full((mesh.nn,), 0.01, dtype=torch.float64, device="cuda")
+        mesh.update_properties()
+        rec = LMRecon(mesh, gfc, precision=prec, tol=1e-8 if prec == "mixed" else 1e-10, normal_eq=ne)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        h = rec.run(data_m, lam=(1.0, 0.0), sigma=sigma, thresh=0.8, max_iter=max_iter, truth=truth_d)
+        torch.cuda.synchronize()
+        out[tag] = dict(seconds=time.perf_counter() - t0, hist=h)
+        mesh._solver = None
+    a, b = out["mixed_split_bf16"]["hist"], out["fp64"]["hist"]
+    vs64 = [float(torch.linalg.vector_norm(x - y) / torch.linalg.vector_norm(y)) for x, y in zip(a["mua"], b["mua"])]
+    return {"workload": f"cylinder r30 h60 @1.5mm, {mesh.nn} nodes, 32x32 optodes, 10 gates, "
+                        f"{int(np.asarray(mesh.gridinmesh).sum())} voxels ({grid_mm:g} mm), 2 absorbers r=8 mm 2x",
+            "iterations": a["iterations"], "seconds_mixed": round(out["mixed_split_bf16"]["seconds"], 2),
+            "seconds_fp64": round(out["fp64"]["seconds"], 2),
+            "mua_rel_err_vs_truth_mixed": [round(x, 5) for x in a["err_truth"]],
+            "mua_rel_err_vs_truth_fp64": [round(x, 5) for x in b["err_truth"]],
+            "mua_rel_diff_mixed_vs_fp64": [float(f"{x:.3e}") for x in vs64],
+            "data_misfit_perc_mixed": [round(x, 3) for x in a["err_perc"]]}
+
+
 def plain_fp64_per_rhs(mesh, nsample=4, tol=1e-8):
     """The plain baseline of the path: FP64 BiCGSTAB (reference arithmetic) on ONE right-hand side per
     call (one source at one harmonic), through the same library, on the bench mesh.  Harmonics are
@@ -448,7 +503,8 @@ def main():
     import torch.distributed as dist
     if a.only:
         torch.cuda.set_device(local_rank)
-        out = tg_jacobian_bench() if a.only == "tg" else lm_step_bench(grid_mm=a.lm_grid_mm)
+        out = {"tg": tg_jacobian_bench, "lm": lambda: lm_step_bench(grid_mm=a.lm_grid_mm),
+               "recon": lambda: lm_recon_bench(grid_mm=a.lm_grid_mm)}[a.only]()
         print(json.dumps(out))
         return
     if world > 1:

@@ -1,0 +1,173 @@
+"""Weighted Levenberg-Marquardt reconstruction of nodal absorption on the device.
+
+Restates wghtd_LM_recon (DOGPUP/reconstruction/wghtd_LM_recon.m:1-168) with
+its helpers id_thresh (DOGPUP/id_thresh.m:1-27) and tik_inv
+(DOGPUP/reconstruction/tik_inv.m:1-20), on the library's kernels:
+
+  per iteration   forward + adjoint solves (batched, mixed or FP64)
+                  TG Jacobian with Rytov normalisation (dgp_jacobian_tg)
+                  H = J^T W J + lam * max diag, r = J^T W y (dgp_normal_eq,
+                  split-BF16 tcgen05) and the FP64 Cholesky solve
+                  (dgp_cholesky_solve), or all of it in FP64 for comparison
+  host            the loop's scalar logic (lambda schedule, step-back on a
+                  rising error, exit conditions) on [NM x NG]-sized data
+
+Data weighting: the reference weights rows by reshape_J's dense w
+(wghtd_LM_recon.m:74-76) when target spots are given, else by 1; here a
+diagonal W = 1/sigma^2 (the north-star weighting) or 1.  The spot-reshaping
+branch (target_spots / reshape_J) is not restated.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import api
+from ._lib import lib, check
+
+
+def id_thresh(data, thresh):
+    """Mask of the gated data used by the fit (DOGPUP/id_thresh.m:13-27), data [NM x NG].
+
+    'all': range-normalised value > 1 %.  A number t: on the falling edge
+    (gate index >= the curve's maximum) with normalised value in (1 %, t]."""
+    d = np.asarray(data, dtype=np.float64)
+    lo = d.min(axis=1, keepdims=True)
+    rng = d.max(axis=1, keepdims=True) - lo
+    rng[rng == 0] = 1.0
+    dn = (d - lo) / rng                                        # normalize(data, 2, 'range')
+    if isinstance(thresh, str):
+        if thresh != "all":
+            raise ValueError("thresh must be a number or 'all'")
+        return dn > 0.01
+    idx = np.arange(d.shape[1])[None, :]
+    after = idx >= np.argmax(dn, axis=1)[:, None]
+    return after & (dn <= thresh) & (dn > 0.01)
+
+
+def _flat(x_nm_ng: torch.Tensor) -> torch.Tensor:
+    """[NM][NG] -> MATLAB's x(:) order (measurement fastest): index g*NM + m."""
+    return x_nm_ng.transpose(0, 1).reshape(-1)
+
+
+class LMRecon:
+    """wghtd_LM_recon on a DMesh with a voxel basis (mesh.mesh2grid called beforehand)."""
+
+    def __init__(self, mesh, gate_fc, precision="mixed", tol=1e-8, normal_eq="split_bf16"):
+        if normal_eq not in ("split_bf16", "fp64"):
+            raise ValueError("normal_eq must be 'split_bf16' or 'fp64'")
+        self.mesh = mesh
+        self.gate_fc = torch.as_tensor(gate_fc, device="cuda", dtype=torch.complex128).contiguous()
+        self.nt = len(mesh.optode.tAxis)
+        self.solve_kw = dict(precision=precision, tol=tol)
+        self.normal_eq = normal_eq
+        inmesh = np.asarray(mesh.gridinmesh)
+        P = mesh.m2g[inmesh]
+        self.basis = api.Basis(P, np.full(P.shape[0], mesh.dxyz ** 3))
+        self.m2g_in = P.tocsr()
+        self.g2m_in = mesh.g2m[:, np.nonzero(inmesh)[0]].tocsr()
+        self.nv = P.shape[0]
+
+    # ----------------------------------------------------------- one model
+    def model(self):
+        """Time-gated data [NM][NG] and the Rytov-normalised TG Jacobian^T [NV][NG*NM]."""
+        m = self.mesh
+        phi, data = m.flu_solve(**self.solve_kw)
+        phiA = m.adj_flu_solve(**self.solve_kw)
+        data_tg = api.fc2tg(data, self.gate_fc, self.nt)
+        if self.normal_eq == "split_bf16":
+            J = api.jacobian_tg(self.basis, phi, phiA, m.optode.s_fpsf, m._link(), self.gate_fc, self.nt, data_tg)
+            Jt = J.reshape(self.nv, -1)
+        else:
+            Jc = api.jacobian_complex(self.basis, phi, phiA, m.optode.s_fpsf, m._link())   # [NV][NF][NM]
+            Jc[:, 0, :] *= 0.5
+            Jtg = self.nt * 2.0 * torch.einsum("gk,vkm->vgm", self.gate_fc.conj(), Jc).real   # fc2tg.m:100-111
+            del Jc
+            Jt = (Jtg / data_tg.transpose(0, 1)[None]).reshape(self.nv, -1)
+        return data_tg, Jt
+
+    # --------------------------------------------------------------- step
+    def _tik(self, Jt, lam, y, w):
+        """update = (J^T W J + lam * max diag)^-1 J^T W y  (tik_inv.m:13-20)."""
+        nv = Jt.shape[0]
+        if self.normal_eq == "split_bf16":
+            Jf = Jt.to(torch.float32).contiguous()
+            H = torch.empty((nv, nv), dtype=torch.float64, device="cuda")
+            x = torch.empty(nv, dtype=torch.float64, device="cuda")
+            v = lambda t: C.c_void_p(t.data_ptr())
+            check(lib.dgp_normal_eq(v(Jf), nv, Jf.shape[1], None if w is None else v(w), v(y), float(lam), 0, v(H),
+                                    nv, v(x), api.stream_ptr()))
+        else:
+            Jd = Jt.to(torch.float64)
+            Jw = Jd if w is None else Jd * w[None, :]
+            H = Jw @ Jd.T
+            H.diagonal().add_(lam * H.diagonal().max())
+            x = Jw @ y
+            H = H.contiguous()
+        check(lib.dgp_cholesky_solve(C.c_void_p(H.data_ptr()), nv, nv, C.c_void_p(x.data_ptr()), api.stream_ptr()))
+        return x
+
+    def run(self, data_m, lam=(1.0, 0.0), sigma=None, thresh=0.8, max_iter=10, truth=None, callback=None):
+        """Iterates from the mesh's current mua (wghtd_LM_recon.m:25-168); data_m [NM][NG] measured TG data.
+
+        sigma [NM][NG] (or None): data standard deviations; the fit is on log
+        data, so W = (data / sigma)^2 to first order.  Returns a history dict."""
+        m = self.mesh
+        data_m = np.asarray(data_m, dtype=np.float64)
+        incl = torch.as_tensor(np.nonzero(id_thresh(data_m, thresh).T.ravel())[0], device="cuda")  # x(:) order
+        dm = torch.log(_flat(torch.as_tensor(data_m, device="cuda")))[incl]
+        w = None
+        if sigma is not None:
+            rel = np.asarray(sigma, dtype=np.float64) / data_m        # sigma of log data
+            w = (1.0 / _flat(torch.as_tensor(rel, device="cuda")) ** 2)[incl].contiguous()
+        k = 10 ** 0.25
+        lam1 = lam[0] * k                                             # :38-39
+        hist = dict(err=[], err_perc=[], err_del=[], lam=[], mua=[], err_truth=[])
+        wn = torch.ones_like(dm) if w is None else w
+        count, d_mu, y_prev, J_prev = 0, None, None, None
+        while True:
+            data_c, Jt = self.model()
+            Jt = Jt[:, incl] if incl.numel() != Jt.shape[1] else Jt
+            y = dm - torch.log(_flat(data_c))[incl]                   # :60-64
+            err = float(torch.sqrt((wn * y * y).sum()))
+            hist["err"].append(err)
+            hist["err_perc"].append(100 * err / float(torch.sqrt((wn * dm * dm).sum())))
+            if truth is not None:
+                hist["err_truth"].append(float(torch.linalg.vector_norm(m.mua - truth) /
+                                               torch.linalg.vector_norm(truth)))
+            if count > 0:
+                hist["err_del"].append(hist["err_perc"][-1] - hist["err_perc"][-2])
+            if callback:
+                callback(count, hist)
+            if count > 1 and hist["err_del"][-1] < 0 and (abs(hist["err_del"][-1]) < 0.12 or
+                                                           hist["err_perc"][-1] < 1.5):      # :91-95
+                break
+            count += 1
+            if count == 1 or hist["err_del"][-1] < 0:                 # :100-106
+                G = torch.as_tensor(self.m2g_in @ m.mua.cpu().numpy(), device="cuda")
+                lam1 = lam1 / k
+            else:                                                     # step back (:107-115)
+                G = torch.as_tensor(self.m2g_in @ (m.mua - d_mu).cpu().numpy(), device="cuda")
+                y, Jt = y_prev, J_prev
+                lam1 = lam1 * k
+            lam1 = max(lam1, err)                                     # :118-120
+            hist["lam"].append(lam1)
+            Jg = (Jt * G[:, None].to(Jt.dtype)).contiguous()          # J .* G.' (property normalisation)
+            upd = self._tik(Jg, lam1, y.contiguous(), w)              # :125-127
+            x = G * upd                                               # :131
+            d_mu = torch.as_tensor(self.g2m_in @ x.cpu().numpy(), device="cuda")   # :132
+            if torch.isnan(d_mu).any():
+                break
+            new_mu = m.mua + d_mu
+            if (new_mu < 0).any():
+                break
+            m.mua = new_mu.contiguous()
+            m.update_properties()                                     # :153
+            hist["mua"].append(m.mua.clone())
+            if count > max_iter - 1:
+                break
+            y_prev, J_prev = y, Jt
+        hist["iterations"] = count
+        return hist
