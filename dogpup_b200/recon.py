@@ -116,7 +116,10 @@ class LMRecon:
         data, so W = (data / sigma)^2 to first order.  Returns a history dict."""
         m = self.mesh
         data_m = np.asarray(data_m, dtype=np.float64)
-        incl = torch.as_tensor(np.nonzero(id_thresh(data_m, thresh).T.ravel())[0], device="cuda")  # x(:) order
+        # gates in the id_thresh window whose measured value has a logarithm (a truncated Fourier
+        # series can ring below zero before the pulse arrives; log() of those is undefined)
+        mask = id_thresh(data_m, thresh) & (data_m > 0)
+        incl = torch.as_tensor(np.nonzero(mask.T.ravel())[0], device="cuda")               # x(:) order
         dm = torch.log(_flat(torch.as_tensor(data_m, device="cuda")))[incl]
         w = None
         if sigma is not None:
@@ -131,6 +134,9 @@ class LMRecon:
             data_c, Jt = self.model()
             Jt = Jt[:, incl] if incl.numel() != Jt.shape[1] else Jt
             y = dm - torch.log(_flat(data_c))[incl]                   # :60-64
+            if not bool(torch.isfinite(y).all()):
+                hist["stopped"] = "model data not positive on an included gate"
+                break
             err = float(torch.sqrt((wn * y * y).sum()))
             hist["err"].append(err)
             hist["err_perc"].append(100 * err / float(torch.sqrt((wn * dm * dm).sum())))

@@ -31,14 +31,14 @@ def test_lm_recon_reduces_error_and_split_bf16_tracks_fp64():
     from dogpup_b200 import api, workloads
     from dogpup_b200.autograd import gate_coefficients
     from dogpup_b200.recon import LMRecon
-    w = workloads.small_fwd(ns=8, nd=8, nf=16)
+    w = workloads.small_fwd(ns=8, nd=8, nf=32)
     node = w["mesh"].node
     c = node.mean(0)
     truth = np.full(w["mesh"].nn, 0.01)
     truth[((node - c) ** 2).sum(1) < 4.0 ** 2] = 0.02
     w["mua"] = truth
     mesh = workloads.build_dmesh(w)
-    gfc = gate_coefficients(w["t"], 0.3e-9 + 0.25e-9 * np.arange(8), 250e-12, mesh.optode.fAxis)
+    gfc = gate_coefficients(w["t"], 0.6e-9 + 0.25e-9 * np.arange(8), 250e-12, mesh.optode.fAxis)
     _, data = mesh.flu_solve(precision="fp64", tol=1e-12)
     data_m = api.fc2tg(data, gfc, len(w["t"])).cpu().numpy()
     lo, hi = node.min(0), node.max(0)
@@ -51,6 +51,7 @@ def test_lm_recon_reduces_error_and_split_bf16_tracks_fp64():
         runs[ne] = rec.run(data_m, lam=(1e-2, 0), thresh="all", max_iter=3,
                            truth=torch.as_tensor(truth, device="cuda"))
     h = runs["split_bf16"]
+    assert "stopped" not in h and len(h["mua"]) >= 2
     assert h["err"][-1] < 0.5 * h["err"][0]
     assert h["err_truth"][-1] < h["err_truth"][0]
     for a, b in zip(runs["split_bf16"]["mua"], runs["fp64"]["mua"]):
