@@ -117,6 +117,12 @@ class Solver:
         check(lib.dgp_solver_memory(self._h, C.byref(b)))
         return b.value
 
+    def autotune(self) -> dict:
+        """Pick the complex-FP32 SpMM lane width and rows per block for this plan (dgp_solver_autotune)."""
+        v, r, ms = C.c_int32(), C.c_int32(), C.c_float()
+        check(lib.dgp_solver_autotune(self._h, C.byref(v), C.byref(r), C.byref(ms), stream_ptr()))
+        return {"vec": v.value, "rows": r.value, "spmm_ms_per_iteration": round(ms.value, 3)}
+
     def profile_kernel(self, which: int, reps: int = 10):
         """(ms per launch, algorithmic bytes per launch) of one sweep kernel, CUDA-event timed."""
         ms, b = C.c_float(), C.c_double()

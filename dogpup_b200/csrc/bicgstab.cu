@@ -1064,19 +1064,31 @@ struct Layouts {
 
 // plain sweeps: ~64 rows per block; sweeps with dot products: 16x more rows per
 // block, so each block issues fewer FP64 atomics per column
-Layouts layouts_for(const SolverPlan *S, int vec) {
+Layouts layouts_for(const SolverPlan *S, int vec, int rows = 64) {
   Layouts x;
   const int lpr = S->nsp / vec;
   const int rpw = 32 / lpr;
-  const int ipb = std::max(1, 64 / (WARPS * rpw));
+  const int ipb = std::max(1, rows / (WARPS * rpw));
   x.L = Layout{S->n, S->nf, S->nsp, lpr, rpw, ipb};
+  // sweeps with dot products take 16x the rows per block: fewer block partials and FP64 atomics
   x.Ld = Layout{S->n, S->nf, S->nsp, lpr, rpw, ipb * 16};
+  return x;
+}
+
+// SpMM layouts: rows per block from the autotuner when it has run; the complex-FP32 dot
+// sweeps keep at most 32 rows per lane, the bound of their FP32 per-lane partial sums
+Layouts spmm_layouts(const SolverPlan *S, int vec, bool fp32) {
+  Layouts x = layouts_for(S, vec, (fp32 && S->tune_rows) ? S->tune_rows : 64);
+  if (fp32) x.Ld.ipb = std::max(x.L.ipb, std::min(x.L.ipb * 16, 32));
   return x;
 }
 
 // complex values per lane: more per lane amortises each nonzero's coefficient load over more
 // right-hand sides (FP32 up to 8, FP64 up to 4 for register room)
-inline int vec_for(const SolverPlan *S, bool fp32) { return std::min(S->nsp, fp32 ? 8 : 4); }
+inline int vec_for(const SolverPlan *S, bool fp32) {
+  if (fp32 && S->tune_vec) return S->tune_vec;
+  return std::min(S->nsp, fp32 ? 8 : 4);
+}
 
 dim3 grid_of(const Layout &L) { return dim3((unsigned)ceil_div(L.n, L.rows_per_block()), (unsigned)L.nf); }
 
@@ -1088,7 +1100,7 @@ constexpr int VU = 2;
 template <class R, int VS, int VD, class OpA, class OpG>
 void enqueue_iteration(const SolverPlan *S, const OpA &A, const OpG &G, const OpG &GT, const Vecs<R> &V,
                        const Work &W, cudaStream_t st) {
-  const Layout Ls = layouts_for(S, VS).L, Lsd = layouts_for(S, VD).Ld;
+  const Layout Ls = spmm_layouts(S, VS, sizeof(R) == 4).L, Lsd = spmm_layouts(S, VD, sizeof(R) == 4).Ld;
   const Layout Lu = layouts_for(S, VU).L, Lud = layouts_for(S, VU).Ld;
   Ctl *ctl = W.ctl;
   // T1 = G p ; h = G^T T1                                       (:1295-1296)
@@ -1446,7 +1458,7 @@ namespace {
 template <int VEC>
 void profile_launch(int which, const SolverPlan *S, const OpA32 &A, const OpG32 &G, const Vecs<float> &V,
                     const Work &W, const Ctl *ctl, cudaStream_t st) {
-  const Layout L = layouts_for(S, VEC).L, Lud = layouts_for(S, VU).Ld;
+  const Layout L = spmm_layouts(S, VEC, true).L, Lud = layouts_for(S, VU).Ld;
   switch (which) {
     case 0: k_spmm<float, VEC, 0><<<grid_of(L), BS, 0, st>>>(L, A, V.z, V.t, nullptr, W.cols, ctl); break;
     case 1: k_spmm<float, VEC, 0><<<grid_of(L), BS, 0, st>>>(L, G, V.p, V.T1, nullptr, W.cols, ctl); break;
@@ -1512,6 +1524,116 @@ int solver_profile(SolverPlan *S, int which, int reps, float *ms, double *bytes,
   DGP_CUDA(cudaMemsetAsync(W.cols.acc, 0, sizeof(double2) * W.cols.C * NACC, st));
   DGP_CUDA(cudaStreamSynchronize(st));
   *ms = t / reps;
+  return DGP_OK;
+}
+
+// ------------------------------------------------------------ autotuner
+namespace {
+// the complex-FP32 SpMM sweeps of one iteration (enqueue_iteration's 7 SpMM launches)
+template <int VEC>
+void spmm_set(const SolverPlan *S, const OpA32 &A, const OpG32 &G, const OpG32 &GT, const Vecs<float> &V,
+              const Work &W, const Ctl *ctl, cudaStream_t st) {
+  const Layouts LL = spmm_layouts(S, VEC, true);
+  const Layout Ls = LL.L, Lsd = LL.Ld;
+  k_spmm<float, VEC, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, G, V.p, V.T1, nullptr, W.cols, ctl);
+  k_spmm<float, VEC, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, GT, V.T1, V.h, nullptr, W.cols, ctl);
+  k_spmm<float, VEC, 1><<<grid_of(Lsd), BS, red_smem(Lsd, 1), st>>>(Lsd, A, V.h, V.v, V.rhat, W.cols, ctl);
+  k_spmm<float, VEC, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, G, V.s, V.T1, nullptr, W.cols, ctl);
+  k_spmm<float, VEC, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, GT, V.T1, V.z, nullptr, W.cols, ctl);
+  k_spmm<float, VEC, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, A, V.z, V.t, nullptr, W.cols, ctl);
+  k_spmm<float, VEC, 2><<<grid_of(Lsd), BS, red_smem(Lsd, 2), st>>>(Lsd, G, V.t, nullptr, V.T1, W.cols, ctl);
+}
+}  // namespace
+
+// Chooses the lane width (complex values per lane) and the rows per block of
+// the complex-FP32 SpMM sweeps for this plan's shape by timing the seven
+// SpMM launches of one iteration, with CUDA events on `st`, for every
+// candidate on the plan's own workspace; keeps the fastest and drops captured
+// graphs so the next solve records the new launch shapes.  The vector
+// contents are scratch here (every solve re-initialises them).
+int solver_autotune(SolverPlan *S, int32_t *vec_out, int32_t *rows_out, float *ms_out, cudaStream_t st) {
+  DGP_TRY(ensure_workspace(S, DGP_PREC_MIXED));
+  Vecs<float> V = vec_views<float>(S);
+  Work W = work_views(S);
+  DevBuf dctl;
+  DGP_TRY(dctl.alloc(sizeof(Ctl)));
+  Ctl hc{};
+  hc.state = ST_RUNNING;
+  hc.maxit = 1 << 30;
+  DGP_CUDA(cudaMemcpyAsync(dctl.p, &hc, sizeof(Ctl), cudaMemcpyHostToDevice, st));
+  const Ctl *ctl = dctl.as<Ctl>();
+  const float *om = (const float *)(S->omega.as<char>() + sizeof(double) * S->nf);
+  OpA32 A{S->rowptr.as<int32_t>(), S->RecA32.as<Rec32>(), om};
+  OpG32 G{S->P.rowptr.as<int32_t>(), S->RecG32.as<Rec32>(), S->nnzG};
+  OpG32 GT{S->P.rowptrT.as<int32_t>(), S->RecGT32.as<Rec32>(), S->nnzG};
+  cudaEvent_t e0, e1;
+  DGP_CUDA(cudaEventCreate(&e0));
+  DGP_CUDA(cudaEventCreate(&e1));
+  const int32_t old_vec = S->tune_vec, old_rows = S->tune_rows;
+  float best = 3.4e38f;
+  int32_t bv = 0, br = 0;
+  int launches = 0;
+  int rc = DGP_OK;
+  for (int vec : {8, 4, 2}) {
+    if (vec > S->nsp || S->nsp / vec > 32) continue;
+    int last_ipb = -1;
+    for (int rows : {32, 64, 128, 256}) {
+      S->tune_vec = vec;
+      S->tune_rows = rows;
+      const int ipb = spmm_layouts(S, vec, true).L.ipb;
+      if (ipb == last_ipb) continue;  // same launch shape as the previous candidate
+      last_ipb = ipb;
+      auto run = [&]() {
+        switch (vec) {
+          case 2: spmm_set<2>(S, A, G, GT, V, W, ctl, st); break;
+          case 4: spmm_set<4>(S, A, G, GT, V, W, ctl, st); break;
+          default: spmm_set<8>(S, A, G, GT, V, W, ctl, st); break;
+        }
+      };
+      run();  // warm
+      cudaEventRecord(e0, st);
+      run();
+      run();
+      cudaEventRecord(e1, st);
+      launches += 21;
+      cudaError_t e = cudaEventSynchronize(e1);
+      if (e != cudaSuccess) {
+        rc = cuda_fail(e, "autotune", __FILE__, __LINE__);
+        break;
+      }
+      float t = 0;
+      cudaEventElapsedTime(&t, e0, e1);
+      t *= 0.5f;
+      if (t < best) {
+        best = t;
+        bv = vec;
+        br = rows;
+      }
+    }
+    if (rc != DGP_OK) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  count_launches(launches);
+  if (rc != DGP_OK || bv == 0) {
+    S->tune_vec = old_vec;
+    S->tune_rows = old_rows;
+    return rc != DGP_OK ? rc : fail(DGP_ERR_UNSUPPORTED, "autotune: no launch shape fits this plan");
+  }
+  DGP_CHECK_LAUNCH();
+  S->tune_vec = bv;
+  S->tune_rows = br;
+  for (auto &g : S->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  S->graph_iters[0] = S->graph_iters[1] = 0;
+  DGP_CUDA(cudaMemsetAsync(W.cols.acc, 0, sizeof(double2) * W.cols.C * NACC, st));
+  DGP_CUDA(cudaStreamSynchronize(st));
+  if (vec_out) *vec_out = bv;
+  if (rows_out) *rows_out = br;
+  if (ms_out) *ms_out = best;
   return DGP_OK;
 }
 

@@ -83,6 +83,8 @@ struct SolverPlan {
   void *h_ctl = nullptr;         // pinned mirror of the control block
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   int graph_iters[2] = {0, 0};
+  // SpMM launch shape of the complex-FP32 sweeps chosen by solver_autotune (0 = built-in default)
+  int32_t tune_vec = 0, tune_rows = 0;
   int64_t bytes = 0;
   ~SolverPlan();
 };
@@ -101,6 +103,9 @@ int solve_mexlayout(SolverPlan *S, const double *d_Q, double *d_X, int32_t ns, i
                     const dgp_solve_opts *opts, dgp_solve_report *rep, cudaStream_t st);
 
 int solver_profile(SolverPlan *S, int which, int reps, float *ms, double *bytes, cudaStream_t st);
+// times the complex-FP32 SpMM sweeps of one iteration for each candidate lane width x rows per
+// block on the plan's own workspace and keeps the fastest (tune_vec, tune_rows)
+int solver_autotune(SolverPlan *S, int32_t *vec, int32_t *rows, float *ms, cudaStream_t st);
 
 // batched operators (layout [nf][n][ns] complex)
 int spmm_A_f64(const int32_t *rowptr, const int32_t *col, const double2 *KM, const double *omega, int64_t n,

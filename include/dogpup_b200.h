@@ -224,6 +224,16 @@ int dgp_solver_update(dgp_solver_t solver, const double *d_K, const double *d_M,
 int dgp_solver_destroy(dgp_solver_t solver);
 /* Bytes of device memory the solver holds. */
 int dgp_solver_memory(dgp_solver_t solver, int64_t *bytes);
+/* Autotuner of the complex-FP32 (DGP_PREC_MIXED) sweeps: times the seven
+ * SpMM launches of one BiCGSTAB iteration for each lane width (8, 4, 2
+ * complex values per lane) x rows per block (32 .. 256) that fits the plan,
+ * on the plan's own workspace (allocating it if needed), and keeps the
+ * fastest for later solves.  Outputs (each may be NULL): the chosen lane
+ * width and rows per block, and the time of the seven launches in ms.
+ * Synchronises the stream.  No reference counterpart (the reference's
+ * launch shapes are fixed, smv_CUDA.cu:57-82). */
+int dgp_solver_autotune(dgp_solver_t solver, int32_t *vec, int32_t *rows,
+                        float *ms, dgp_stream_t stream);
 
 /* Solves A_k X[k] = B[k] for every harmonic, B and X complex128
  * [NF][NN][NS] with ns <= ns_max.  Synchronises the stream; returns

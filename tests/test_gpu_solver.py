@@ -226,3 +226,27 @@ def test_solver_harmonic_subset(small_case, gpu_case, torch, precision):
     assert err.max() < (1e-9 if precision == "fp64" else 1e-6), err.max()
     with pytest.raises(ValueError):
         api.Solver(fem.rowptr, fem.col, gpu_case["K"], gpu_case["M"], dfc, 2, ns, harmonics=[1])
+
+
+def test_solver_autotune_then_mixed_accuracy(small_case, gpu_case, torch):
+    """The autotuner picks a fitting launch shape; solves after it keep the mixed accuracy bar."""
+    from dogpup_b200 import api
+    from oracle import solver as osv
+    K0, M0 = small_case["K"], small_case["M"]
+    nf, ns = 6, 16
+    dfc = 2 * np.pi / 10e-9 / (C_VAC / 1.4)
+    nodes, w = _point_sources(small_case, ns, 31)
+    fpsf = np.exp(-0.2j * np.arange(nf))
+    fem = gpu_case["fem"]
+    S = api.Solver(fem.rowptr, fem.col, gpu_case["K"], gpu_case["M"], dfc, nf, ns)
+    t = S.autotune()
+    assert t["vec"] in (2, 4, 8) and t["rows"] in (32, 64, 128, 256) and t["spmm_ms_per_iteration"] > 0
+    opts = api.make_opts(tol=1e-10, precision="mixed")
+    X, rep = S.solve_sources(torch.as_tensor(nodes, device="cuda"), torch.as_tensor(w, device="cuda"),
+                             torch.as_tensor(fpsf, device="cuda"), opts)
+    Q = np.zeros((K0.shape[0], ns, nf), complex)
+    for s in range(ns):
+        Q[nodes[s], s, :] = w[s][:, None] * fpsf[None, :]
+    xd = osv.direct_solve(K0, M0, dfc, Q)
+    err = np.linalg.norm(np.transpose(X.cpu().numpy(), (1, 2, 0)) - xd, axis=0) / np.linalg.norm(xd, axis=0)
+    assert err.max() < 1e-6, err.max()
