@@ -113,7 +113,11 @@ class LMRecon:
         """Iterates from the mesh's current mua (wghtd_LM_recon.m:25-168); data_m [NM][NG] measured TG data.
 
         sigma [NM][NG] (or None): data standard deviations; the fit is on log
-        data, so W = (data / sigma)^2 to first order.  Returns a history dict."""
+        data, so W = (data / sigma)^2 to first order, scaled to unit mean over
+        the fitted gates: the reference's damping rule floors lambda at the
+        residual norm (wghtd_LM_recon.m:118-120), which keeps its meaning only
+        when the weighted norm is on the scale of the unweighted one.
+        Returns a history dict."""
         m = self.mesh
         data_m = np.asarray(data_m, dtype=np.float64)
         # gates in the id_thresh window whose measured value has a logarithm (a truncated Fourier
@@ -124,7 +128,8 @@ class LMRecon:
         w = None
         if sigma is not None:
             rel = np.asarray(sigma, dtype=np.float64) / data_m        # sigma of log data
-            w = (1.0 / _flat(torch.as_tensor(rel, device="cuda")) ** 2)[incl].contiguous()
+            w = (1.0 / _flat(torch.as_tensor(rel, device="cuda")) ** 2)[incl]
+            w = (w / w.mean()).contiguous()
         k = 10 ** 0.25
         lam1 = lam[0] * k                                             # :38-39
         hist = dict(err=[], err_perc=[], err_del=[], lam=[], mua=[], err_truth=[])
