@@ -118,10 +118,20 @@ class Solver:
         return b.value
 
     def autotune(self) -> dict:
-        """Pick the complex-FP32 SpMM lane width and rows per block for this plan (dgp_solver_autotune)."""
-        v, r, ms = C.c_int32(), C.c_int32(), C.c_float()
-        check(lib.dgp_solver_autotune(self._h, C.byref(v), C.byref(r), C.byref(ms), stream_ptr()))
-        return {"vec": v.value, "rows": r.value, "spmm_ms_per_iteration": round(ms.value, 3)}
+        """Pick the complex-FP32 SpMM kind and launch shape for this plan (dgp_solver_autotune)."""
+        tl, v, r, ms = C.c_int32(), C.c_int32(), C.c_int32(), C.c_float()
+        check(lib.dgp_solver_autotune(self._h, C.byref(tl), C.byref(v), C.byref(r), C.byref(ms), stream_ptr()))
+        return {"spmm": "tiled" if tl.value else "gather", "vec": v.value, "rows": r.value,
+                "spmm_ms_per_iteration": round(ms.value, 3)}
+
+    def set_spmm(self, tiled: bool, vec: int = 0, rows: int = 0):
+        check(lib.dgp_solver_set_spmm(self._h, int(tiled), int(vec), int(rows)))
+
+    def check_spmm(self) -> float:
+        """max |tiled - gather| / max |value| over A, G, G^T on a test pattern."""
+        d = C.c_double()
+        check(lib.dgp_solver_check_spmm(self._h, C.byref(d), stream_ptr()))
+        return d.value
 
     def profile_kernel(self, which: int, reps: int = 10):
         """(ms per launch, algorithmic bytes per launch) of one sweep kernel, CUDA-event timed."""

@@ -290,6 +290,10 @@ struct OpG64 {
 };
 
 // y[0..VEC) = sum_p coef(p) * Xk[col(p)*nsp + s0 ..]   (32-bit offsets inside one harmonic plane)
+//
+// Software-pipelined: the coefficient records (column, value) of batch b+1 are
+// loaded before the x gathers of batch b are consumed, so the record -> column
+// -> x dependency costs one memory latency per batch instead of two.
 template <int VEC, class C, class Coef>
 __device__ inline void row_spmv(int nsp, int cs, const int32_t *__restrict__ rowptr, int64_t i, const Coef &cf,
                                 const C *__restrict__ Xk, C (&y)[VEC]) {
@@ -299,18 +303,35 @@ __device__ inline void row_spmv(int nsp, int cs, const int32_t *__restrict__ row
   // gathers in flight per lane: UNR nonzeros x VEC complex (register budget bounds UNR*VEC)
   constexpr int UNR = VEC >= 8 ? 2 : 4;
   int p = b;
-  for (; p + UNR <= e; p += UNR) {
+  if (p + UNR <= e) {
     int j[UNR];
     C a[UNR];
 #pragma unroll
     for (int u = 0; u < UNR; ++u) cf.get(p + u, j[u], a[u]);
-    C xs[UNR][VEC];
+    for (;;) {
+      C xs[UNR][VEC];
 #pragma unroll
-    for (int u = 0; u < UNR; ++u) ldgv<VEC>(Xk + j[u] * nsp, cs, xs[u]);
+      for (int u = 0; u < UNR; ++u) ldgv<VEC>(Xk + j[u] * nsp, cs, xs[u]);
+      const int pn = p + UNR;
+      const bool more = pn + UNR <= e;
+      int jn[UNR];
+      C an[UNR];
+      if (more) {
 #pragma unroll
-    for (int u = 0; u < UNR; ++u)
+        for (int u = 0; u < UNR; ++u) cf.get(pn + u, jn[u], an[u]);
+      }
 #pragma unroll
-      for (int v = 0; v < VEC; ++v) y[v] = cfmaT(a[u], xs[u][v], y[v]);
+      for (int u = 0; u < UNR; ++u)
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) y[v] = cfmaT(a[u], xs[u][v], y[v]);
+      p = pn;
+      if (!more) break;
+#pragma unroll
+      for (int u = 0; u < UNR; ++u) {
+        j[u] = jn[u];
+        a[u] = an[u];
+      }
+    }
   }
   for (; p < e; ++p) {
     int j;
@@ -378,6 +399,154 @@ __global__ void __launch_bounds__(BS) k_spmm(Layout L, Op op, const typename CT<
     } else {
       const int slot[2] = {ACC_D2, ACC_D3};
       block_reduce<VEC, 2, E>(L, ln, pd, cols.acc, cols.C, slot, smem);
+    }
+  }
+}
+
+// ------------------------------------------------------- tiled SpMM
+// Y = Op_k X with the x rows a block needs staged in shared memory first.
+// Block (b, k, z) owns rows [b*rb, b*rb + rb) of harmonic k and sources
+// [z*SW, z*SW + SW): it copies its halo rows (the distinct columns of its
+// rows, hcols[hptr[b] ..]) and its nonzeros' 16-byte records into shared
+// memory with cp.async (all copies in flight at once, no dependent global
+// loads), then each lane accumulates VEC consecutive sources of a row from
+// shared memory (the record's pad word holds the column's halo position).
+// MODE as k_spmm: 0 store, 1 store + Y.W, 2 Y.W and Y.Y without the store.
+struct TLayout {
+  int64_t n;
+  int nf, nsp, rb;
+  const int32_t *hptr, *hcols, *rowptr;
+};
+
+__device__ inline void cp_async16(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ inline void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+template <class Op> struct TCoef;
+template <> struct TCoef<OpA32> {
+  float om;
+  const Rec32 *rec;
+  __device__ TCoef(const OpA32 &op, int k) : om(op.omega[k]), rec(op.rec) {}
+  __device__ float2 of(const Rec32 &r) const { return make_float2(r.a, om * r.b); }
+};
+template <> struct TCoef<OpG32> {
+  const Rec32 *rec;
+  __device__ TCoef(const OpG32 &op, int k) : rec(op.rec + (int64_t)k * op.nnz) {}
+  __device__ float2 of(const Rec32 &r) const { return make_float2(r.a, r.b); }
+};
+
+template <int MODE, int SW, class Op>
+__global__ void __launch_bounds__(BS) k_tspmm(TLayout T, Op op, const float2 *__restrict__ X, float2 *__restrict__ Y,
+                                              const float2 *__restrict__ W, Cols cols, const Ctl *ctl, int hcap) {
+  constexpr int VEC = SW < 4 ? SW : 4;  // complex values per lane
+  constexpr int LPR = SW / VEC;         // lanes per row
+  constexpr int RPW = 32 / LPR;         // rows per warp
+  constexpr int NQ = MODE == 2 ? 2 : 1;
+  if (ctl && halted(ctl, ST_RUNNING)) return;
+  extern __shared__ float4 tsm[];
+  float2 *tile = reinterpret_cast<float2 *>(tsm);                      // [hcap][SW]
+  Rec32 *srec = reinterpret_cast<Rec32 *>(tile + (size_t)hcap * SW);   // [zcap]
+  const int b = blockIdx.x, k = blockIdx.y, s0 = blockIdx.z * SW;
+  const int64_t r0 = (int64_t)b * T.rb;
+  const int64_t r1 = min(T.n, r0 + T.rb);
+  const int h0 = T.hptr[b], nh = T.hptr[b + 1] - h0;
+  const int p0 = T.rowptr[r0], np = T.rowptr[r1] - p0;
+  const TCoef<Op> cf(op, k);
+  const float2 *Xk = X + (int64_t)k * T.n * T.nsp + s0;
+  constexpr int CPR = SW / 2;  // 16-byte chunks per halo row
+  for (int t = threadIdx.x; t < nh * CPR; t += BS) {
+    const int hr = t / CPR, c = t - hr * CPR;
+    const int64_t j = T.hcols[h0 + hr];
+    cp_async16(tile + hr * SW + 2 * c, Xk + j * T.nsp + 2 * c);
+  }
+  for (int t = threadIdx.x; t < np; t += BS) cp_async16(srec + t, cf.rec + p0 + t);
+  cp_async_wait_all();
+  __syncthreads();
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int sub = lane % LPR, rsub = lane / LPR;
+  float2 part[VEC][NQ];
+#pragma unroll
+  for (int v = 0; v < VEC; ++v)
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) part[v][q] = make_float2(0.f, 0.f);
+  for (int lr0 = 0; lr0 < T.rb; lr0 += WARPS * RPW) {
+    const int64_t i = r0 + lr0 + warp * RPW + rsub;
+    if (i >= r1) continue;
+    float2 y[VEC];
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) y[v] = make_float2(0.f, 0.f);
+    const int pb = __ldg(T.rowptr + i) - p0, pe = __ldg(T.rowptr + i + 1) - p0;
+    for (int p = pb; p < pe; ++p) {
+      const Rec32 rc = srec[p];
+      const float2 a = cf.of(rc);
+      const float2 *xr = tile + __float_as_int(rc.pad) * SW + sub * VEC;
+#pragma unroll
+      for (int v = 0; v < VEC; v += 2) {
+        const float4 xv = *reinterpret_cast<const float4 *>(xr + v);
+        y[v] = cfmaf(a, make_float2(xv.x, xv.y), y[v]);
+        if (VEC > 1) y[v + 1] = cfmaf(a, make_float2(xv.z, xv.w), y[v + 1]);
+      }
+    }
+    const int64_t o = ((int64_t)k * T.n + i) * T.nsp + s0 + sub * VEC;
+    if (MODE != 2) {
+#pragma unroll
+      for (int v = 0; v < VEC; v += 2)
+        *reinterpret_cast<float4 *>(Y + o + v) = make_float4(y[v].x, y[v].y, y[v + 1].x, y[v + 1].y);
+    }
+    if (MODE != 0) {
+#pragma unroll
+      for (int v = 0; v < VEC; v += 2) {
+        const float4 wv = *reinterpret_cast<const float4 *>(W + o + v);
+        acc_bil(part[v][0], y[v], make_float2(wv.x, wv.y));
+        acc_bil(part[v + 1][0], y[v + 1], make_float2(wv.z, wv.w));
+        if (MODE == 2) {
+          acc_bil(part[v][NQ - 1], y[v], y[v]);
+          acc_bil(part[v + 1][NQ - 1], y[v + 1], y[v + 1]);
+        }
+      }
+    }
+  }
+  if constexpr (MODE != 0) {
+    // lanes with the same sub hold the same columns: shuffle, then warps through shared memory
+    double2 pd[VEC][NQ];
+#pragma unroll
+    for (int v = 0; v < VEC; ++v)
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        double2 x = d2(part[v][q]);
+        for (int off = LPR; off < 32; off <<= 1) {
+          x.x += __shfl_xor_sync(0xffffffffu, x.x, off);
+          x.y += __shfl_xor_sync(0xffffffffu, x.y, off);
+        }
+        pd[v][q] = x;
+      }
+    __syncthreads();  // the tile is no longer read: reuse its space for the warp partials
+    double2 *red = reinterpret_cast<double2 *>(tsm);  // [WARPS][SW][NQ]
+    if (rsub == 0) {
+#pragma unroll
+      for (int v = 0; v < VEC; ++v)
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) red[(warp * SW + sub * VEC + v) * NQ + q] = pd[v][q];
+    }
+    __syncthreads();
+    const int slot[2] = {MODE == 1 ? ACC_D1 : ACC_D2, ACC_D3};
+    for (int t = threadIdx.x; t < SW * NQ; t += BS) {
+      const int sc = t / NQ, q = t % NQ;
+      double2 x = make_double2(0.0, 0.0);
+      for (int w = 0; w < WARPS; ++w) {
+        const double2 yv = red[(w * SW + sc) * NQ + q];
+        x.x += yv.x;
+        x.y += yv.y;
+      }
+      double2 *dst = cols.acc + (int64_t)slot[q] * cols.C + (int64_t)k * T.nsp + s0 + sc;
+      atomicAdd(&dst->x, x.x);
+      atomicAdd(&dst->y, x.y);
     }
   }
 }
@@ -934,7 +1103,7 @@ __global__ void __launch_bounds__(1024) k_outer_norms(Cols c, double *bnorm, dou
 }
 
 __global__ void k_cvt_km(const double *__restrict__ K, const double *__restrict__ M, const int32_t *__restrict__ col,
-                         int64_t nnz, double2 *km64, Rec32 *rec) {
+                         int64_t nnz, double2 *km64, Rec32 *rec, const int32_t *__restrict__ lcol) {
   const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (p >= nnz) return;
   km64[p] = make_double2(K[p], M[p]);
@@ -942,7 +1111,7 @@ __global__ void k_cvt_km(const double *__restrict__ K, const double *__restrict_
   r.col = col[p];
   r.a = (float)K[p];
   r.b = (float)M[p];
-  r.pad = 0.f;
+  r.pad = __int_as_float(lcol ? lcol[p] : 0);  // halo position for the tiled SpMM
   rec[p] = r;
 }
 
@@ -954,7 +1123,8 @@ __global__ void k_dfc_m(const double *__restrict__ M, double dfc, int64_t nnz, d
 // G^T values and the FP32 records of G and G^T
 __global__ void k_gather_gt(const double2 *__restrict__ G, const int32_t *__restrict__ perm,
                             const int32_t *__restrict__ colG, const int32_t *__restrict__ colT, int64_t nnzG, int nf,
-                            double2 *GT, Rec32 *recG, Rec32 *recGT) {
+                            double2 *GT, Rec32 *recG, Rec32 *recGT, const int32_t *__restrict__ lcolG,
+                            const int32_t *__restrict__ lcolT) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= nnzG * nf) return;
   const int64_t k = t / nnzG, q = t % nnzG;
@@ -965,11 +1135,11 @@ __global__ void k_gather_gt(const double2 *__restrict__ G, const int32_t *__rest
   a.col = colG[q];
   a.a = (float)g.x;
   a.b = (float)g.y;
-  a.pad = 0.f;
+  a.pad = __int_as_float(lcolG ? lcolG[q] : 0);
   b.col = colT[q];
   b.a = (float)gt.x;
   b.b = (float)gt.y;
-  b.pad = 0.f;
+  b.pad = __int_as_float(lcolT ? lcolT[q] : 0);
   recG[t] = a;
   recGT[t] = b;
 }
@@ -992,6 +1162,124 @@ int pad_sources(int ns) {
 }
 
 size_t red_smem(const Layout &L, int nq) { return sizeof(double2) * WARPS * L.nsp * nq; }
+
+// ------------------------------------------------------- tiled SpMM plans
+constexpr int TILE_RB = 32;                 // rows per block of the tiled SpMM
+constexpr size_t TILE_SMEM_MAX = 200 * 1024;
+
+inline int tile_sw(const SolverPlan *S) { return std::min(S->nsp, 32); }
+
+// halo lists of the row blocks of one CSR pattern (host; once per plan)
+int tiled_build(TiledPlan *T, const int32_t *d_rowptr, const int32_t *d_col, int64_t n, int64_t nnz, int rb,
+                cudaStream_t st) {
+  std::vector<int32_t> rp(n + 1), cl(nnz);
+  DGP_CUDA(cudaMemcpyAsync(rp.data(), d_rowptr, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost, st));
+  DGP_CUDA(cudaMemcpyAsync(cl.data(), d_col, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, st));
+  DGP_CUDA(cudaStreamSynchronize(st));
+  const int64_t nblk = ceil_div(n, (int64_t)rb);
+  std::vector<int32_t> hptr(nblk + 1, 0), hcols, lcol(nnz), tmp;
+  hcols.reserve((size_t)nnz / 2);
+  int32_t hmax = 0, zmax = 0;
+  for (int64_t b = 0; b < nblk; ++b) {
+    const int64_t r0 = b * rb, r1 = std::min(n, r0 + rb);
+    const int32_t p0 = rp[r0], p1 = rp[r1];
+    tmp.assign(cl.begin() + p0, cl.begin() + p1);
+    std::sort(tmp.begin(), tmp.end());
+    tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+    for (int32_t p = p0; p < p1; ++p)
+      lcol[p] = (int32_t)(std::lower_bound(tmp.begin(), tmp.end(), cl[p]) - tmp.begin());
+    hcols.insert(hcols.end(), tmp.begin(), tmp.end());
+    hptr[b + 1] = (int32_t)hcols.size();
+    hmax = std::max(hmax, (int32_t)tmp.size());
+    zmax = std::max(zmax, p1 - p0);
+  }
+  T->rb = rb;
+  T->nblk = nblk;
+  T->hmax = hmax;
+  T->zmax = zmax;
+  DGP_TRY(T->hptr.alloc(sizeof(int32_t) * hptr.size()));
+  DGP_TRY(T->hcols.alloc(sizeof(int32_t) * std::max<size_t>(1, hcols.size())));
+  DGP_TRY(T->lcol.alloc(sizeof(int32_t) * std::max<int64_t>(1, nnz)));
+  DGP_CUDA(cudaMemcpyAsync(T->hptr.p, hptr.data(), sizeof(int32_t) * hptr.size(), cudaMemcpyHostToDevice, st));
+  DGP_CUDA(cudaMemcpyAsync(T->hcols.p, hcols.data(), sizeof(int32_t) * hcols.size(), cudaMemcpyHostToDevice, st));
+  DGP_CUDA(cudaMemcpyAsync(T->lcol.p, lcol.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, st));
+  DGP_CUDA(cudaStreamSynchronize(st));
+  return DGP_OK;
+}
+
+size_t tile_smem(const TiledPlan &T, int sw, int mode) {
+  const size_t main = (size_t)T.hmax * sw * sizeof(float2) + (size_t)T.zmax * sizeof(Rec32);
+  const size_t red = mode == 0 ? 0 : (size_t)WARPS * sw * (mode == 2 ? 2 : 1) * sizeof(double2);
+  return std::max(main, red);
+}
+
+template <int MODE, int SW, class Op>
+void tspmm_launch(const SolverPlan *S, const TiledPlan &T, const int32_t *rowptr, const Op &op, const float2 *X,
+                  float2 *Y, const float2 *Wv, const Cols &cols, const Ctl *ctl, cudaStream_t st) {
+  const TLayout L{S->n, S->nf, S->nsp, T.rb, T.hptr.as<int32_t>(), T.hcols.as<int32_t>(), rowptr};
+  const dim3 grid((unsigned)T.nblk, (unsigned)S->nf, (unsigned)(S->nsp / SW));
+  k_tspmm<MODE, SW, Op><<<grid, BS, tile_smem(T, SW, MODE), st>>>(L, op, X, Y, Wv, cols, ctl, T.hmax);
+}
+
+template <int SW, class Op>
+int tspmm_attrs(const TiledPlan &T) {
+  DGP_CUDA(cudaFuncSetAttribute(k_tspmm<0, SW, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)tile_smem(T, SW, 0)));
+  DGP_CUDA(cudaFuncSetAttribute(k_tspmm<1, SW, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)tile_smem(T, SW, 1)));
+  DGP_CUDA(cudaFuncSetAttribute(k_tspmm<2, SW, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)tile_smem(T, SW, 2)));
+  return DGP_OK;
+}
+
+// the tiled SpMM launch of sweep `what` (0 A, 1 G, 2 G^T) in mode MODE, dispatched on the source tile width
+template <int MODE>
+void tspmm(const SolverPlan *S, int what, const float2 *X, float2 *Y, const float2 *Wv, const Cols &cols,
+           const Ctl *ctl, cudaStream_t st) {
+  const float *om = (const float *)(S->omega.as<char>() + sizeof(double) * S->nf);
+  const OpA32 A{S->rowptr.as<int32_t>(), S->RecA32.as<Rec32>(), om};
+  const OpG32 G{S->P.rowptr.as<int32_t>(), S->RecG32.as<Rec32>(), S->nnzG};
+  const OpG32 GT{S->P.rowptrT.as<int32_t>(), S->RecGT32.as<Rec32>(), S->nnzG};
+  auto go = [&](auto sw) {
+    constexpr int W_ = decltype(sw)::value;
+    if (what == 0) tspmm_launch<MODE, W_>(S, S->tA, A.rowptr, A, X, Y, Wv, cols, ctl, st);
+    else if (what == 1) tspmm_launch<MODE, W_>(S, S->tG, G.rowptr, G, X, Y, Wv, cols, ctl, st);
+    else tspmm_launch<MODE, W_>(S, S->tGT, GT.rowptr, GT, X, Y, Wv, cols, ctl, st);
+  };
+  switch (tile_sw(S)) {
+    case 2: go(std::integral_constant<int, 2>()); break;
+    case 4: go(std::integral_constant<int, 4>()); break;
+    case 8: go(std::integral_constant<int, 8>()); break;
+    case 16: go(std::integral_constant<int, 16>()); break;
+    default: go(std::integral_constant<int, 32>()); break;
+  }
+}
+
+// builds the three halo plans and sets the kernels' shared-memory limits; tiled_ok = 1 when they fit
+int tiled_setup(SolverPlan *S, cudaStream_t st) {
+  DGP_TRY(tiled_build(&S->tA, S->rowptr.as<int32_t>(), S->col.as<int32_t>(), S->n, S->nnz, TILE_RB, st));
+  DGP_TRY(tiled_build(&S->tG, S->P.rowptr.as<int32_t>(), S->P.col.as<int32_t>(), S->n, S->nnzG, TILE_RB, st));
+  DGP_TRY(tiled_build(&S->tGT, S->P.rowptrT.as<int32_t>(), S->P.colT.as<int32_t>(), S->n, S->nnzG, TILE_RB, st));
+  const int sw = tile_sw(S);
+  size_t need = 0;
+  for (const TiledPlan *T : {&S->tA, &S->tG, &S->tGT})
+    for (int m = 0; m < 3; ++m) need = std::max(need, tile_smem(*T, sw, m));
+  S->tiled_ok = need <= TILE_SMEM_MAX && S->nsp % sw == 0;
+  if (!S->tiled_ok) return DGP_OK;
+  auto attrs = [&](auto w) {
+    constexpr int W_ = decltype(w)::value;
+    int rc = tspmm_attrs<W_, OpA32>(S->tA);
+    if (rc == DGP_OK) rc = tspmm_attrs<W_, OpG32>(S->tG.hmax >= S->tGT.hmax ? S->tG : S->tGT);
+    return rc;
+  };
+  switch (sw) {
+    case 2: return attrs(std::integral_constant<int, 2>());
+    case 4: return attrs(std::integral_constant<int, 4>());
+    case 8: return attrs(std::integral_constant<int, 8>());
+    case 16: return attrs(std::integral_constant<int, 16>());
+    default: return attrs(std::integral_constant<int, 32>());
+  }
+}
 
 template <class R> struct Vecs {
   using C = typename CT<R>::C;
@@ -1097,12 +1385,40 @@ dim3 grid_of(const Layout &L) { return dim3((unsigned)ceil_div(L.n, L.rows_per_b
 constexpr int VU = 2;
 
 // one BiCGSTAB iteration (dMesh.m:1295-1340) enqueued on st: KERNELS_PER_ITER launches
+// one complex-FP32 iteration with the tiled SpMM (same kernel sequence as enqueue_iteration)
+void enqueue_iteration_tiled(const SolverPlan *S, const Vecs<float> &V, const Work &W, cudaStream_t st) {
+  const Layout Lu = layouts_for(S, VU).L, Lud = layouts_for(S, VU).Ld;
+  Ctl *ctl = W.ctl;
+  tspmm<0>(S, 1, V.p, V.T1, nullptr, W.cols, ctl, st);
+  tspmm<0>(S, 2, V.T1, V.h, nullptr, W.cols, ctl, st);
+  tspmm<1>(S, 0, V.h, V.v, V.rhat, W.cols, ctl, st);
+  k_stage_alpha<<<1, 1024, 0, st>>>(W.cols, ctl);
+  k_update_s<float, VU><<<grid_of(Lud), BS, red_smem(Lud, 1), st>>>(Lud, V.r, V.v, V.s, W.cols, ctl);
+  k_stage_check_s<<<1, 1024, 0, st>>>(W.cols, ctl);
+  tspmm<0>(S, 1, V.s, V.T1, nullptr, W.cols, ctl, st);
+  tspmm<0>(S, 2, V.T1, V.z, nullptr, W.cols, ctl, st);
+  tspmm<0>(S, 0, V.z, V.t, nullptr, W.cols, ctl, st);
+  tspmm<2>(S, 1, V.t, nullptr, V.T1, W.cols, ctl, st);
+  k_stage_omega<<<1, 1024, 0, st>>>(W.cols, ctl);
+  k_update_xrp<float, VU><<<grid_of(Lud), BS, red_smem(Lud, 2), st>>>(Lud, V.x, V.h, V.z, V.r, V.s, V.t, V.p, V.v,
+                                                                      V.rhat, W.cols, ctl);
+  k_stage_check_r<<<1, 1024, 0, st>>>(W.cols, ctl);
+  k_stage_count<<<1, 1024, 0, st>>>(W.cols, ctl);
+  k_update_p<float, VU><<<grid_of(Lu), BS, 0, st>>>(Lu, V.r, V.p, W.cols, ctl);
+}
+
 template <class R, int VS, int VD, class OpA, class OpG>
 void enqueue_iteration(const SolverPlan *S, const OpA &A, const OpG &G, const OpG &GT, const Vecs<R> &V,
                        const Work &W, cudaStream_t st) {
   const Layout Ls = spmm_layouts(S, VS, sizeof(R) == 4).L, Lsd = spmm_layouts(S, VD, sizeof(R) == 4).Ld;
   const Layout Lu = layouts_for(S, VU).L, Lud = layouts_for(S, VU).Ld;
   Ctl *ctl = W.ctl;
+  if constexpr (sizeof(R) == 4) {
+    if (S->tiled) {
+      enqueue_iteration_tiled(S, V, W, st);
+      return;
+    }
+  }
   // T1 = G p ; h = G^T T1                                       (:1295-1296)
   k_spmm<R, VS, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, G, V.p, V.T1, nullptr, W.cols, ctl);
   k_spmm<R, VS, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, GT, V.T1, V.h, nullptr, W.cols, ctl);
@@ -1244,7 +1560,7 @@ SolverPlan::~SolverPlan() {
 int solver_update(SolverPlan *S, const double *d_K, const double *d_M, cudaStream_t st) {
   const int64_t nnz = S->nnz;
   k_cvt_km<<<g1(nnz, 256), 256, 0, st>>>(d_K, d_M, S->col.as<int32_t>(), nnz, S->KM64.as<double2>(),
-                                          S->RecA32.as<Rec32>());
+                                          S->RecA32.as<Rec32>(), S->tA.lcol.as<int32_t>());
   DGP_CHECK_LAUNCH();
   // FSAI of tril(K + i*k*dfc*M) for every harmonic
   DevBuf im;
@@ -1257,7 +1573,8 @@ int solver_update(SolverPlan *S, const double *d_K, const double *d_M, cudaStrea
   k_gather_gt<<<g1(S->nnzG * S->nf, 256), 256, 0, st>>>(S->G64.as<double2>(), S->P.permT.as<int32_t>(),
                                                        S->P.col.as<int32_t>(), S->P.colT.as<int32_t>(), S->nnzG,
                                                        S->nf, S->GT64.as<double2>(), S->RecG32.as<Rec32>(),
-                                                       S->RecGT32.as<Rec32>());
+                                                       S->RecGT32.as<Rec32>(), S->tG.lcol.as<int32_t>(),
+                                                       S->tGT.lcol.as<int32_t>());
   DGP_CHECK_LAUNCH();
   DGP_CUDA(cudaStreamSynchronize(st));
   return DGP_OK;
@@ -1302,6 +1619,7 @@ int solver_build(SolverPlan *S, const int32_t *d_rowptr, const int32_t *d_col, i
   DGP_TRY(S->RecG32.alloc(sizeof(Rec32) * gcount));
   DGP_TRY(S->RecGT32.alloc(sizeof(Rec32) * gcount));
   DGP_CUDA(cudaMallocHost(&S->h_ctl, sizeof(Ctl)));
+  DGP_TRY(tiled_setup(S, st));
   return solver_update(S, d_K, d_M, st);
 }
 
@@ -1545,13 +1863,54 @@ void spmm_set(const SolverPlan *S, const OpA32 &A, const OpG32 &G, const OpG32 &
 }
 }  // namespace
 
+void tspmm_set(const SolverPlan *S, const Vecs<float> &V, const Work &W, const Ctl *ctl, cudaStream_t st) {
+  tspmm<0>(S, 1, V.p, V.T1, nullptr, W.cols, ctl, st);
+  tspmm<0>(S, 2, V.T1, V.h, nullptr, W.cols, ctl, st);
+  tspmm<1>(S, 0, V.h, V.v, V.rhat, W.cols, ctl, st);
+  tspmm<0>(S, 1, V.s, V.T1, nullptr, W.cols, ctl, st);
+  tspmm<0>(S, 2, V.T1, V.z, nullptr, W.cols, ctl, st);
+  tspmm<0>(S, 0, V.z, V.t, nullptr, W.cols, ctl, st);
+  tspmm<2>(S, 1, V.t, nullptr, V.T1, W.cols, ctl, st);
+}
+
+// deterministic test pattern in [-1, 1) for the operator self-check
+__global__ void k_fill_pattern(float2 *x, int64_t n, uint32_t seed) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t h = (uint32_t)i * 2654435761u ^ seed;
+  h ^= h >> 15;
+  h *= 2246822519u;
+  h ^= h >> 13;
+  const float a = (float)(h & 0xffff) / 32768.f - 1.f, b = (float)(h >> 16) / 32768.f - 1.f;
+  x[i] = make_float2(a, b);
+}
+
+// out[0] = max |a - b|, out[1] = max |b| as float bits (non-negative floats order like their bits)
+__global__ void k_maxdiff(const float2 *__restrict__ a, const float2 *__restrict__ b, int64_t n, unsigned *out) {
+  float d = 0.f, m = 0.f;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float2 u = a[i], v = b[i];
+    d = fmaxf(d, fmaxf(fabsf(u.x - v.x), fabsf(u.y - v.y)));
+    m = fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y)));
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    d = fmaxf(d, __shfl_xor_sync(0xffffffffu, d, off));
+    m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(out, __float_as_uint(d));
+    atomicMax(out + 1, __float_as_uint(m));
+  }
+}
+
 // Chooses the lane width (complex values per lane) and the rows per block of
 // the complex-FP32 SpMM sweeps for this plan's shape by timing the seven
 // SpMM launches of one iteration, with CUDA events on `st`, for every
 // candidate on the plan's own workspace; keeps the fastest and drops captured
 // graphs so the next solve records the new launch shapes.  The vector
 // contents are scratch here (every solve re-initialises them).
-int solver_autotune(SolverPlan *S, int32_t *vec_out, int32_t *rows_out, float *ms_out, cudaStream_t st) {
+int solver_autotune(SolverPlan *S, int32_t *tiled_out, int32_t *vec_out, int32_t *rows_out, float *ms_out,
+                    cudaStream_t st) {
   DGP_TRY(ensure_workspace(S, DGP_PREC_MIXED));
   Vecs<float> V = vec_views<float>(S);
   Work W = work_views(S);
@@ -1569,7 +1928,8 @@ int solver_autotune(SolverPlan *S, int32_t *vec_out, int32_t *rows_out, float *m
   cudaEvent_t e0, e1;
   DGP_CUDA(cudaEventCreate(&e0));
   DGP_CUDA(cudaEventCreate(&e1));
-  const int32_t old_vec = S->tune_vec, old_rows = S->tune_rows;
+  const int32_t old_vec = S->tune_vec, old_rows = S->tune_rows, old_tiled = S->tiled;
+  S->tiled = 0;
   float best = 3.4e38f;
   int32_t bv = 0, br = 0;
   int launches = 0;
@@ -1612,17 +1972,42 @@ int solver_autotune(SolverPlan *S, int32_t *vec_out, int32_t *rows_out, float *m
     }
     if (rc != DGP_OK) break;
   }
+  int32_t bt = 0;
+  if (rc == DGP_OK && S->tiled_ok) {  // the tiled SpMM as one more candidate
+    S->tiled = 1;
+    tspmm_set(S, V, W, ctl, st);
+    cudaEventRecord(e0, st);
+    tspmm_set(S, V, W, ctl, st);
+    tspmm_set(S, V, W, ctl, st);
+    cudaEventRecord(e1, st);
+    launches += 21;
+    cudaError_t e = cudaEventSynchronize(e1);
+    if (e != cudaSuccess) {
+      rc = cuda_fail(e, "autotune", __FILE__, __LINE__);
+    } else {
+      float t = 0;
+      cudaEventElapsedTime(&t, e0, e1);
+      t *= 0.5f;
+      if (t < best) {
+        best = t;
+        bt = 1;
+      }
+    }
+    S->tiled = 0;
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   count_launches(launches);
   if (rc != DGP_OK || bv == 0) {
     S->tune_vec = old_vec;
     S->tune_rows = old_rows;
+    S->tiled = old_tiled;
     return rc != DGP_OK ? rc : fail(DGP_ERR_UNSUPPORTED, "autotune: no launch shape fits this plan");
   }
   DGP_CHECK_LAUNCH();
   S->tune_vec = bv;
   S->tune_rows = br;
+  S->tiled = bt;
   for (auto &g : S->graph)
     if (g) {
       cudaGraphExecDestroy(g);
@@ -1631,9 +2016,85 @@ int solver_autotune(SolverPlan *S, int32_t *vec_out, int32_t *rows_out, float *m
   S->graph_iters[0] = S->graph_iters[1] = 0;
   DGP_CUDA(cudaMemsetAsync(W.cols.acc, 0, sizeof(double2) * W.cols.C * NACC, st));
   DGP_CUDA(cudaStreamSynchronize(st));
+  if (tiled_out) *tiled_out = bt;
   if (vec_out) *vec_out = bv;
   if (rows_out) *rows_out = br;
   if (ms_out) *ms_out = best;
+  return DGP_OK;
+}
+
+int solver_set_spmm(SolverPlan *S, int32_t tiled, int32_t vec, int32_t rows) {
+  DGP_REQUIRE(tiled == 0 || tiled == 1, "set_spmm: tiled must be 0 or 1");
+  DGP_REQUIRE(!tiled || S->tiled_ok, "set_spmm: the tiled SpMM does not fit this plan's shared memory");
+  if (!tiled && vec != 0) {
+    DGP_REQUIRE((vec == 2 || vec == 4 || vec == 8) && vec <= S->nsp && S->nsp / vec <= 32,
+                "set_spmm: vec must be 2, 4 or 8, at most the padded source count and at least nsp/32");
+    DGP_REQUIRE(rows == 0 || rows == 32 || rows == 64 || rows == 128 || rows == 256,
+                "set_spmm: rows must be 0 (default), 32, 64, 128 or 256");
+  }
+  S->tiled = tiled;
+  if (!tiled) {
+    S->tune_vec = vec;
+    S->tune_rows = vec ? rows : 0;
+  }
+  for (auto &g : S->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  S->graph_iters[0] = S->graph_iters[1] = 0;
+  return DGP_OK;
+}
+
+// Runs the gather and the tiled SpMM of A, G and G^T on one test pattern and
+// returns the largest |difference| over the largest |value| (FP32 roundoff:
+// only the summation order differs).
+int solver_check_spmm(SolverPlan *S, double *max_rel, cudaStream_t st) {
+  DGP_REQUIRE(max_rel, "check_spmm: null output");
+  DGP_REQUIRE(S->tiled_ok, "check_spmm: the tiled SpMM does not fit this plan");
+  DGP_TRY(ensure_workspace(S, DGP_PREC_MIXED));
+  Vecs<float> V = vec_views<float>(S);
+  Work W = work_views(S);
+  DevBuf dctl, dm;
+  DGP_TRY(dctl.alloc(sizeof(Ctl)));
+  DGP_TRY(dm.alloc(2 * sizeof(unsigned)));
+  Ctl hc{};
+  hc.state = ST_RUNNING;
+  hc.maxit = 1 << 30;
+  DGP_CUDA(cudaMemcpyAsync(dctl.p, &hc, sizeof(Ctl), cudaMemcpyHostToDevice, st));
+  const Ctl *ctl = dctl.as<Ctl>();
+  const int64_t cnt = (int64_t)S->nf * S->n * S->nsp;
+  k_fill_pattern<<<g1(cnt, 256), 256, 0, st>>>(V.p, cnt, 12345u);
+  const float *om = (const float *)(S->omega.as<char>() + sizeof(double) * S->nf);
+  const OpA32 A{S->rowptr.as<int32_t>(), S->RecA32.as<Rec32>(), om};
+  const OpG32 G{S->P.rowptr.as<int32_t>(), S->RecG32.as<Rec32>(), S->nnzG};
+  const OpG32 GT{S->P.rowptrT.as<int32_t>(), S->RecGT32.as<Rec32>(), S->nnzG};
+  const int gv = std::min(S->nsp, 8);  // gather kernel at its built-in shape
+  auto gather = [&](auto vv, int what) {
+    constexpr int VV = decltype(vv)::value;
+    const Layout L = layouts_for(S, VV).L;
+    if (what == 0) k_spmm<float, VV, 0><<<grid_of(L), BS, 0, st>>>(L, A, V.p, V.T1, nullptr, W.cols, ctl);
+    else k_spmm<float, VV, 0><<<grid_of(L), BS, 0, st>>>(L, what == 1 ? G : GT, V.p, V.T1, nullptr, W.cols, ctl);
+  };
+  double worst = 0.0;
+  for (int what = 0; what < 3; ++what) {
+    if (gv == 2) gather(std::integral_constant<int, 2>(), what);
+    else if (gv == 4) gather(std::integral_constant<int, 4>(), what);
+    else gather(std::integral_constant<int, 8>(), what);
+    tspmm<0>(S, what, V.p, V.h, nullptr, W.cols, ctl, st);
+    DGP_CUDA(cudaMemsetAsync(dm.p, 0, 2 * sizeof(unsigned), st));
+    k_maxdiff<<<1184, 256, 0, st>>>(V.h, V.T1, cnt, dm.as<unsigned>());
+    unsigned h[2] = {0, 0};
+    DGP_CUDA(cudaMemcpyAsync(h, dm.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+    DGP_CUDA(cudaStreamSynchronize(st));
+    float d, m;
+    memcpy(&d, &h[0], 4);
+    memcpy(&m, &h[1], 4);
+    worst = std::max(worst, m > 0 ? (double)d / m : (double)d);
+  }
+  count_launches(3 * 3 + 1);
+  DGP_CHECK_LAUNCH();
+  *max_rel = worst;
   return DGP_OK;
 }
 

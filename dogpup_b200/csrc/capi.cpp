@@ -308,9 +308,20 @@ int dgp_solve(dgp_solver_t s, const double *d_B, double *d_X, int32_t ns, const 
   DGP_GUARD(solver_solve(&s->plan, d_B, nullptr, nullptr, nullptr, d_X, ns, opts, report, (cudaStream_t)stream));
 }
 
-int dgp_solver_autotune(dgp_solver_t s, int32_t *vec, int32_t *rows, float *ms, dgp_stream_t stream) {
+int dgp_solver_autotune(dgp_solver_t s, int32_t *tiled, int32_t *vec, int32_t *rows, float *ms,
+                        dgp_stream_t stream) {
   if (!s) return fail(DGP_ERR_ARG, "solver_autotune: null handle");
-  DGP_GUARD(solver_autotune(&s->plan, vec, rows, ms, (cudaStream_t)stream));
+  DGP_GUARD(solver_autotune(&s->plan, tiled, vec, rows, ms, (cudaStream_t)stream));
+}
+
+int dgp_solver_set_spmm(dgp_solver_t s, int32_t tiled, int32_t vec, int32_t rows) {
+  if (!s) return fail(DGP_ERR_ARG, "solver_set_spmm: null handle");
+  DGP_GUARD(solver_set_spmm(&s->plan, tiled, vec, rows));
+}
+
+int dgp_solver_check_spmm(dgp_solver_t s, double *max_rel, dgp_stream_t stream) {
+  if (!s) return fail(DGP_ERR_ARG, "solver_check_spmm: null handle");
+  DGP_GUARD(solver_check_spmm(&s->plan, max_rel, (cudaStream_t)stream));
 }
 
 int dgp_solve_mex(dgp_solver_t s, const double *d_Q, double *d_X, int32_t ns, int32_t layout,

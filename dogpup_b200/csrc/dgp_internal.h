@@ -60,6 +60,16 @@ int fsai_factor_full(const int32_t *d_rowptr, const int32_t *d_col, const double
                      cudaStream_t st);
 
 // ---------------------------------------------------------------- solver
+// Row-block halo plan of the tiled SpMM (complex-FP32 sweeps): rows are cut
+// into blocks of rb consecutive rows; block b stages the distinct columns
+// hcols[hptr[b] .. hptr[b+1]) of its rows in shared memory, and each nonzero
+// p carries its column's position in that list, lcol[p].
+struct TiledPlan {
+  int32_t rb = 0, hmax = 0, zmax = 0;  // rows per block, largest halo, most nonzeros in a block
+  int64_t nblk = 0;
+  DevBuf hptr, hcols, lcol;
+};
+
 struct SolverPlan {
   int64_t n = 0, nnz = 0, nnzG = 0;
   int32_t nf = 0, ns_max = 0, nsp = 0;  // nsp: padded sources per harmonic
@@ -85,6 +95,9 @@ struct SolverPlan {
   int graph_iters[2] = {0, 0};
   // SpMM launch shape of the complex-FP32 sweeps chosen by solver_autotune (0 = built-in default)
   int32_t tune_vec = 0, tune_rows = 0;
+  // tiled SpMM (halo rows staged in shared memory) for A, G and G^T; tiled = 1 selects it
+  TiledPlan tA, tG, tGT;
+  int32_t tiled_ok = 0, tiled = 0;
   int64_t bytes = 0;
   ~SolverPlan();
 };
@@ -105,7 +118,11 @@ int solve_mexlayout(SolverPlan *S, const double *d_Q, double *d_X, int32_t ns, i
 int solver_profile(SolverPlan *S, int which, int reps, float *ms, double *bytes, cudaStream_t st);
 // times the complex-FP32 SpMM sweeps of one iteration for each candidate lane width x rows per
 // block on the plan's own workspace and keeps the fastest (tune_vec, tune_rows)
-int solver_autotune(SolverPlan *S, int32_t *vec, int32_t *rows, float *ms, cudaStream_t st);
+int solver_autotune(SolverPlan *S, int32_t *tiled, int32_t *vec, int32_t *rows, float *ms, cudaStream_t st);
+// sets the SpMM kind / shape explicitly (tiled 0: gather kernel with vec, rows; 1: tiled)
+int solver_set_spmm(SolverPlan *S, int32_t tiled, int32_t vec, int32_t rows);
+// largest relative difference between the tiled and the gather SpMM on the plan's operators
+int solver_check_spmm(SolverPlan *S, double *max_rel, cudaStream_t st);
 
 // batched operators (layout [nf][n][ns] complex)
 int spmm_A_f64(const int32_t *rowptr, const int32_t *col, const double2 *KM, const double *omega, int64_t n,

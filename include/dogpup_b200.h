@@ -225,15 +225,29 @@ int dgp_solver_destroy(dgp_solver_t solver);
 /* Bytes of device memory the solver holds. */
 int dgp_solver_memory(dgp_solver_t solver, int64_t *bytes);
 /* Autotuner of the complex-FP32 (DGP_PREC_MIXED) sweeps: times the seven
- * SpMM launches of one BiCGSTAB iteration for each lane width (8, 4, 2
- * complex values per lane) x rows per block (32 .. 256) that fits the plan,
- * on the plan's own workspace (allocating it if needed), and keeps the
- * fastest for later solves.  Outputs (each may be NULL): the chosen lane
- * width and rows per block, and the time of the seven launches in ms.
- * Synchronises the stream.  No reference counterpart (the reference's
- * launch shapes are fixed, smv_CUDA.cu:57-82). */
-int dgp_solver_autotune(dgp_solver_t solver, int32_t *vec, int32_t *rows,
-                        float *ms, dgp_stream_t stream);
+ * SpMM launches of one BiCGSTAB iteration for each candidate -- the gather
+ * SpMM at each lane width (8, 4, 2 complex values per lane) x rows per block
+ * (32 .. 256) that fits the plan, and the tiled SpMM (32-row blocks whose
+ * halo rows are staged in shared memory) when it fits -- on the plan's own
+ * workspace (allocating it if needed), and keeps the fastest for later
+ * solves.  Outputs (each may be NULL): 1 if the tiled SpMM won, the best
+ * gather lane width and rows per block, and the winner's time for the seven
+ * launches in ms.  Synchronises the stream.  No reference counterpart (the
+ * reference's launch shapes are fixed, smv_CUDA.cu:57-82). */
+int dgp_solver_autotune(dgp_solver_t solver, int32_t *tiled, int32_t *vec,
+                        int32_t *rows, float *ms, dgp_stream_t stream);
+/* Sets the complex-FP32 SpMM explicitly: tiled = 1 selects the tiled SpMM
+ * (DGP_ERR_ARG if it does not fit the plan); tiled = 0 the gather SpMM with
+ * vec complex values per lane (2, 4, 8; 0 = built-in default) and rows per
+ * block (32, 64, 128, 256; 0 = 64). */
+int dgp_solver_set_spmm(dgp_solver_t solver, int32_t tiled, int32_t vec,
+                        int32_t rows);
+/* Self-check of the two SpMM kinds: applies A_k, G_k and G_k^T to one
+ * deterministic test pattern with the gather and with the tiled kernel and
+ * returns max |difference| / max |value| over all three (FP32 roundoff
+ * from the different summation order, ~1e-7).  Synchronises the stream. */
+int dgp_solver_check_spmm(dgp_solver_t solver, double *max_rel,
+                          dgp_stream_t stream);
 
 /* Solves A_k X[k] = B[k] for every harmonic, B and X complex128
  * [NF][NN][NS] with ns <= ns_max.  Synchronises the stream; returns
