@@ -32,6 +32,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <initializer_list>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -1221,14 +1222,15 @@ void tspmm_launch(const SolverPlan *S, const TiledPlan &T, const int32_t *rowptr
   k_tspmm<MODE, SW, Op><<<grid, BS, tile_smem(T, SW, MODE), st>>>(L, op, X, Y, Wv, cols, ctl, T.hmax);
 }
 
+// dynamic shared-memory limits of the three modes, large enough for every plan in Ts
 template <int SW, class Op>
-int tspmm_attrs(const TiledPlan &T) {
-  DGP_CUDA(cudaFuncSetAttribute(k_tspmm<0, SW, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)tile_smem(T, SW, 0)));
-  DGP_CUDA(cudaFuncSetAttribute(k_tspmm<1, SW, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)tile_smem(T, SW, 1)));
-  DGP_CUDA(cudaFuncSetAttribute(k_tspmm<2, SW, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)tile_smem(T, SW, 2)));
+int tspmm_attrs(std::initializer_list<const TiledPlan *> Ts) {
+  size_t b[3] = {0, 0, 0};
+  for (const TiledPlan *T : Ts)
+    for (int m = 0; m < 3; ++m) b[m] = std::max(b[m], tile_smem(*T, SW, m));
+  DGP_CUDA(cudaFuncSetAttribute(k_tspmm<0, SW, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b[0]));
+  DGP_CUDA(cudaFuncSetAttribute(k_tspmm<1, SW, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b[1]));
+  DGP_CUDA(cudaFuncSetAttribute(k_tspmm<2, SW, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b[2]));
   return DGP_OK;
 }
 
@@ -1268,8 +1270,8 @@ int tiled_setup(SolverPlan *S, cudaStream_t st) {
   if (!S->tiled_ok) return DGP_OK;
   auto attrs = [&](auto w) {
     constexpr int W_ = decltype(w)::value;
-    int rc = tspmm_attrs<W_, OpA32>(S->tA);
-    if (rc == DGP_OK) rc = tspmm_attrs<W_, OpG32>(S->tG.hmax >= S->tGT.hmax ? S->tG : S->tGT);
+    int rc = tspmm_attrs<W_, OpA32>({&S->tA});
+    if (rc == DGP_OK) rc = tspmm_attrs<W_, OpG32>({&S->tG, &S->tGT});
     return rc;
   };
   switch (sw) {
