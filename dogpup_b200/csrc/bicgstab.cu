@@ -1469,7 +1469,7 @@ int enqueue_for(SolverPlan *S, const Vecs<R> &V, const Work &W, cudaStream_t st)
 // run BiCGSTAB iterations (graph-captured blocks) until the control block says done
 template <class R>
 int run_iterations(SolverPlan *S, const Vecs<R> &V, const Work &W, int check_every, int maxit, cudaStream_t st,
-                   int *iters_out) {
+                   int *iters_out, bool stall_guard = false) {
   const int gi = sizeof(R) == 4 ? 1 : 0;
   if (check_every < 1) check_every = 1;
   if (!S->graph[gi] || S->graph_iters[gi] != check_every) {
@@ -1502,6 +1502,13 @@ int run_iterations(SolverPlan *S, const Vecs<R> &V, const Work &W, int check_eve
   Ctl *h = (Ctl *)S->h_ctl;
   // the device stops at maxit; the host bound only guards against a logic error
   const int64_t max_launches = maxit / check_every + 3;
+  // stall guard (inner solves of the mixed path): stop when the largest residual among the
+  // still-active columns has not halved for ~40 iterations -- complex-FP32 BiCGSTAB can
+  // stall at its rounding floor, and the FP64 refinement that follows restarts from the
+  // true residual, so stopping there loses nothing
+  const int patience = std::max(3, 40 / check_every);
+  double ref_err = 0.0;
+  int since = 0;
   for (int64_t launches = 0;; ++launches) {
     if (launches > max_launches) return fail(DGP_ERR_CUDA, "solver: control block never reached DONE");
     DGP_CUDA(cudaGraphLaunch(S->graph[gi], st));
@@ -1509,6 +1516,14 @@ int run_iterations(SolverPlan *S, const Vecs<R> &V, const Work &W, int check_eve
     DGP_CUDA(cudaMemcpyAsync(h, W.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
     DGP_CUDA(cudaStreamSynchronize(st));
     if (h->state == ST_DONE) break;
+    if (stall_guard) {
+      if (ref_err == 0.0 || h->max_err < 0.5 * ref_err) {
+        ref_err = h->max_err;
+        since = 0;
+      } else if (++since >= patience) {
+        break;
+      }
+    }
   }
   *iters_out = h->iters;
   return DGP_OK;
@@ -1695,13 +1710,16 @@ static int solve_mixed(SolverPlan *S, const double *d_B, const int32_t *d_nodes,
   for (int ref = 0; ref < max_ref; ++ref) {
     // inner FP32 solve on the current residual (already in V.r)
     const int inner_maxit = std::max(1, o.maxit - total_iters);
+    // all columns iterate until the largest residual reaches inner_tol (columns that converge
+    // early keep improving, which the next refinement step gains from); the stall guard of
+    // run_iterations ends inner solves that stop making progress in FP32
     DGP_TRY(set_ctl(W.ctl, o.inner_tol, inner_maxit, DGP_STOP_MAX_ALL, st, S->h_ctl));
     launch_init<float, VU>(layouts_for(S, VU).Ld, V, W, st);
     DGP_CHECK_LAUNCH();
     k_stage_init<<<1, 1024, 0, st>>>(W.cols, W.ctl, S->nsp, ns);
     DGP_CHECK_LAUNCH();
     int it = 0;
-    DGP_TRY(run_iterations<float>(S, V, W, o.check_every, inner_maxit, st, &it));
+    DGP_TRY(run_iterations<float>(S, V, W, o.check_every, inner_maxit, st, &it, true));
     total_iters += it;
     refinements += 1;
     // X += x32 ; r = b - A X in FP64
