@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-secondary", action="store_true", help="skip the TG Jacobian / LM / plain-FP64 timings")
-    ap.add_argument("--only", choices=["tg", "lm", "recon"], default=None,
+    ap.add_argument("--only", choices=["tg", "lm", "recon", "uneven", "grad500k"], default=None,
                     help="run one secondary timing alone and print its JSON (profiling cases)")
     ap.add_argument("--lm-grid-mm", type=float, default=2.0, help="voxel pitch of the LM step's Jacobian basis")
     ap.add_argument("--order", choices=["morton", "lattice"], default="morton", help="mesh node numbering")
@@ -341,6 +341,92 @@ def lm_recon_bench(max_iter=10, grid_mm=2.0, seed=7):
             "data_misfit_perc_mixed": [round(x, 3) for x in a["err_perc"]]}
 
 
+def uneven_bench(count=24, seed=11, streams=4):
+    """Uneven batch: `count` seeded ellipsoid / cylinder meshes of 5k-300k nodes (log-uniform),
+    8-64 sources and detectors, 16-128 harmonics; forward + TG vjp (10 gates of 500 ps, seeded
+    upstream gradient) for all of them through the batch executor (mixed precision to 1e-8)."""
+    import torch
+    from dogpup_b200 import meshgen, workloads
+    from dogpup_b200.autograd import gate_coefficients
+    from dogpup_b200.batch import UnevenBatch
+    rng = np.random.default_rng(seed)
+    t0 = time.perf_counter()
+    meshes, gates, ups, sizes = [], [], [], []
+    for i in range(count):
+        target = float(np.exp(rng.uniform(np.log(5e3), np.log(3e5))))
+        ns, nd, nf = int(rng.integers(8, 65)), int(rng.integers(8, 65)), int(rng.integers(16, 129))
+        t = workloads.time_axis(10e-9)
+        if i % 2 == 0:
+            h = (4 / 3 * np.pi * 45 * 37.5 * 35 / target) ** (1 / 3)
+            m = meshgen.ellipsoid_mesh((90.0, 75.0, 70.0), h, jitter=0.2 * h / 1.2, seed=seed + i)
+            src = workloads.ring(ns, np.zeros(3), (45.0, 37.5), 0.0)
+            det = workloads.ring(nd, np.zeros(3), (45.0, 37.5), 0.0, phase=np.pi / nd)
+        else:
+            h = (np.pi * 30 ** 2 * 60 / target) ** (1 / 3)
+            m = meshgen.cylinder_mesh(30.0, 60.0, h, jitter=0.2 * h / 1.5, seed=seed + i)
+            src = workloads.ring(ns, np.array([0.0, 0.0, 30.0]), (30.0, 30.0), 30.0)
+            det = workloads.ring(nd, np.array([0.0, 0.0, 30.0]), (30.0, 30.0), 30.0, phase=np.pi / nd)
+        w = dict(name=f"uneven {i}", mesh=m, mua=np.full(m.nn, 0.01), musp=np.full(m.nn, 1.0), nr=1.4, src=src,
+                 det=det, link=workloads.all_pairs(ns, nd), t=t, nf=nf)
+        mesh = workloads.build_dmesh(w)
+        meshes.append(mesh)
+        gates.append(gate_coefficients(t, 0.5e-9 + 0.5e-9 * np.arange(10), 500e-12, mesh.optode.fAxis))
+        ups.append(rng.standard_normal((ns * nd, 10)))
+        sizes.append((m.nn, ns, nd, nf))
+    setup_s = time.perf_counter() - t0
+    B = UnevenBatch(meshes, streams=streams, precision="mixed", tol=1e-8, gates=gates, upstream=ups)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = B.run()
+    torch.cuda.synchronize()
+    run_s = time.perf_counter() - t0
+    solves = sum((ns + nd) * nf for _, ns, nd, nf in sizes)
+    return {"workload": f"{count} meshes, {min(s[0] for s in sizes)}-{max(s[0] for s in sizes)} nodes "
+                        f"(total {sum(s[0] for s in sizes)}), 8-64 sources/detectors, 16-128 harmonics, "
+                        "forward + adjoint + TG vjp (10 gates)",
+            "tasks": len(B.tasks), "streams": streams, "budget_gb": round(B.budget / 1e9, 1),
+            "seconds": round(run_s, 2), "src_freq_solves": solves,
+            "src_freq_solves_per_s": round(solves / run_s, 1), "host_setup_s": round(setup_s, 1),
+            "vjp_finite": bool(all(torch.isfinite(r.vjp).all() for r in res))}
+
+
+def grad_big_bench(target_nodes=500_000, ns=32, nd=32, nf=32):
+    """End-to-end gradient of a TG least-squares loss w.r.t. nodal mua on a ~500k-node ellipsoid,
+    fields recomputed in backward instead of stored; mixed precision vs plain FP64 solves."""
+    import torch
+    from dogpup_b200 import workloads
+    from dogpup_b200.autograd import TimeGatedForward, gate_coefficients
+    h = (4 / 3 * np.pi * 45 * 37.5 * 35 / target_nodes) ** (1 / 3)
+    w = workloads.ellipsoid_fwd(seed=5, h=h, ns=ns, nd=nd, nf=nf)
+    mesh = workloads.build_dmesh(w)
+    gfc = gate_coefficients(w["t"], 0.5e-9 + 0.5e-9 * np.arange(10), 500e-12, mesh.optode.fAxis)
+    rng = np.random.default_rng(2)
+    target = None
+    out = {}
+    for prec, tol in (("mixed", 1e-8), ("fp64", 1e-8)):
+        model = TimeGatedForward(mesh, gfc, precision=prec, tol=tol, recompute=True)
+        mua = torch.as_tensor(w["mua"], device="cuda").clone().requires_grad_(True)
+        musp = torch.as_tensor(w["musp"], device="cuda")
+        if target is None:
+            with torch.no_grad():
+                target = model(mua, musp) * torch.as_tensor(1 + 0.01 * rng.standard_normal((ns * nd, 10)),
+                                                            device="cuda")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        y = model(mua, musp)
+        loss = ((torch.log(y.clamp_min(1e-300)) - torch.log(target.clamp_min(1e-300))) ** 2).sum()
+        loss.backward()
+        torch.cuda.synchronize()
+        out[prec] = dict(seconds=time.perf_counter() - t0, grad=mua.grad.clone())
+        mesh._solver = None
+    g64, gm = out["fp64"]["grad"], out["mixed"]["grad"]
+    return {"workload": f"ellipsoid 90x75x70 @{h:.2f}mm, {mesh.nn} nodes, {ns}x{nd} optodes, {nf} harmonics, "
+                        "10 gates, TG log-data least squares, fields recomputed in backward",
+            "seconds_mixed": round(out["mixed"]["seconds"], 2), "seconds_fp64": round(out["fp64"]["seconds"], 2),
+            "speedup": round(out["fp64"]["seconds"] / out["mixed"]["seconds"], 2),
+            "grad_rel_diff_mixed_vs_fp64": float(torch.linalg.vector_norm(gm - g64) / torch.linalg.vector_norm(g64))}
+
+
 def plain_fp64_per_rhs(mesh, nsample=4, tol=1e-8):
     """The plain baseline of the path: FP64 BiCGSTAB (reference arithmetic) on ONE right-hand side per
     call (one source at one harmonic), through the same library, on the bench mesh.  Harmonics are
@@ -511,7 +597,8 @@ def main():
     if a.only:
         torch.cuda.set_device(local_rank)
         out = {"tg": tg_jacobian_bench, "lm": lambda: lm_step_bench(grid_mm=a.lm_grid_mm),
-               "recon": lambda: lm_recon_bench(grid_mm=a.lm_grid_mm)}[a.only]()
+               "recon": lambda: lm_recon_bench(grid_mm=a.lm_grid_mm), "uneven": uneven_bench,
+               "grad500k": grad_big_bench}[a.only]()
         print(json.dumps(out))
         return
     if world > 1:
