@@ -157,7 +157,7 @@ __global__ void k_ctab(const double2 *__restrict__ gate, const double2 *__restri
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < nf) finv[t] = cdiv(make_double2(-1.0, 0.0), fpsf[t]);
   if (t >= ng * nf || !gate) return;
-  int g = t / nf, k = t % nf;
+  const int k = t % nf;  // t = g * nf + k
   double h = k == 0 ? 0.5 : 1.0;
   double2 gc = make_double2(gate[t].x, -gate[t].y);
   double2 r = cdiv(gc, fpsf[k]);

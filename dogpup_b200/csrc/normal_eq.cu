@@ -307,6 +307,9 @@ __global__ void k_damp(double *H, int64_t ldh, const double *__restrict__ diag, 
 
 // ------------------------------------------------------- FP64 Cholesky
 constexpr int NB = 64;
+#ifndef DGP_CHOL_NBO
+#define DGP_CHOL_NBO 256
+#endif
 
 // factor the diagonal block in place (unblocked right-looking, shared memory)
 __global__ void __launch_bounds__(256) k_potrf_diag(double *H, int64_t ldh, int64_t k0, int nb, int *err) {
@@ -540,7 +543,7 @@ int cholesky_solve_run(double *H, int64_t n, int64_t ldh, double *x, cudaStream_
   DevBuf errb;
   DGP_TRY(errb.alloc(sizeof(int)));
   DGP_CUDA(cudaMemsetAsync(errb.p, 0, sizeof(int), st));
-  constexpr int64_t NBO = 256;  // outer block step: DTRSM panel + DSYRK trailing update
+  constexpr int64_t NBO = DGP_CHOL_NBO;  // outer block step: DTRSM panel + DSYRK trailing update
   std::unique_lock<std::mutex> lk;
   cublasHandle_t hb = blas_handle(lk);
   if (!hb) return fail(DGP_ERR_CUDA, "cholesky: cuBLAS handle creation failed");
