@@ -345,6 +345,39 @@ __device__ inline void row_spmv(int nsp, int cs, const int32_t *__restrict__ row
   }
 }
 
+// FP32 rows: the lanes of a row load the row's records in parallel (one
+// coalesced 16-byte load per lane and LPR nonzeros) and hand each nonzero's
+// column and coefficient to the row's lanes with shuffles, instead of every
+// lane loading every record (a broadcast load costs the L1 return bandwidth
+// of a full vector load); the x gathers then depend on one record load per
+// LPR nonzeros.  Rows of a warp loop to the warp's longest row (masked).
+template <int VEC, class Coef>
+__device__ inline void row_spmv_shfl(int nsp, int cs, const int32_t *__restrict__ rowptr, int64_t i, const Coef &cf,
+                                     const float2 *__restrict__ Xk, float2 (&y)[VEC], int lpr, int sub) {
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) y[v] = make_float2(0.f, 0.f);
+  const unsigned mask = __activemask();  // lanes past the last row have left the row loop
+  const int b = __ldg(rowptr + i), e = __ldg(rowptr + i + 1);
+  const int cmax = __reduce_max_sync(mask, e - b);
+  for (int base = 0; base < cmax; base += lpr) {
+    int j0 = 0;
+    float2 a0 = make_float2(0.f, 0.f);
+    if (b + base + sub < e) cf.get(b + base + sub, j0, a0);
+    const int cnt = min(lpr, cmax - base);
+    for (int u = 0; u < cnt; ++u) {
+      const int j = __shfl_sync(mask, j0, u, lpr);
+      const float ax = __shfl_sync(mask, a0.x, u, lpr), ay = __shfl_sync(mask, a0.y, u, lpr);
+      if (b + base + u < e) {
+        float2 x[VEC];
+        ldgv<VEC>(Xk + j * nsp, cs, x);
+        const float2 a = make_float2(ax, ay);
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) y[v] = cfmaf(a, x[v], y[v]);
+      }
+    }
+  }
+}
+
 __device__ inline bool halted(const Ctl *ctl, int need) {
   // need = ST_RUNNING: skip unless running; ST_FINAL: skip only when done
   int s = *(volatile const int *)&ctl->state;
@@ -375,7 +408,8 @@ __global__ void __launch_bounds__(BS) k_spmm(Layout L, Op op, const typename CT<
     const int64_t i = ln.row(L, it);
     if (i >= L.n) break;
     C y[VEC];
-    row_spmv<VEC>(L.nsp, cs, op.rowptr, i, cf, Xk, y);
+    if constexpr (sizeof(R) == 4) row_spmv_shfl<VEC>(L.nsp, cs, op.rowptr, i, cf, Xk, y, L.lpr, ln.sub);
+    else row_spmv<VEC>(L.nsp, cs, op.rowptr, i, cf, Xk, y);
     const int64_t o = vidx(L, ln.k, i, c0);
     if (MODE != 2) stv<VEC>(Y + o, cs, y);
     if (MODE != 0) {

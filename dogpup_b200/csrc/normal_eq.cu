@@ -10,12 +10,12 @@
 //   r = J' W y                         FP64
 //   H = L L', solve L L' x = r         FP64 blocked Cholesky + triangular solves
 //
-// Cholesky: right-looking over 256-column block steps.  The 256 x 256
-// diagonal block is factored by this file's kernels (64-column steps: one
-// CTA per 64 x 64 diagonal factor, a thread per panel row for the triangular
-// solve, 64 x 64 tiles for the update inside the block); the panel below it
-// is a cuBLAS DTRSM and the trailing update a cuBLAS DSYRK (plain BLAS-3,
-// where n^3/3 of the flops are).
+// Cholesky: right-looking over 256-column block steps.  Inside the 256 x 256
+// diagonal block, 64-column steps: this file's one-warp factor of the 64 x 64
+// diagonal, then DTRSM / DSYRK for the rest of the block; below the block the
+// panel is a cuBLAS DTRSM and the trailing update a cuBLAS DSYRK (plain
+// BLAS-3, where n^3/3 of the flops are); the two triangular solves are cuBLAS
+// DTRSV.
 //
 // Input J is given transposed, Jt [nv][nmeas] float32 row-major -- the layout
 // the TG Jacobian kernel writes -- so both GEMM operands are K-major.
@@ -311,142 +311,35 @@ constexpr int NB = 64;
 #define DGP_CHOL_NBO 256
 #endif
 
-// factor the diagonal block in place (unblocked right-looking, shared memory)
-__global__ void __launch_bounds__(256) k_potrf_diag(double *H, int64_t ldh, int64_t k0, int nb, int *err) {
+// Factors the nb x nb (nb <= 64) diagonal block at k0 in place, one warp,
+// right-looking in shared memory: each column is scaled by 1/sqrt(pivot) and
+// every lane updates the rows it owns (rows j+1+lane, j+33+lane) -- only warp
+// barriers between columns.  A non-positive or non-finite pivot sets err bit 8.
+__global__ void __launch_bounds__(32) k_potrf_diag(double *H, int64_t ldh, int64_t k0, int nb, int *err) {
   __shared__ double A[NB][NB + 1];
-  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
-    int i = t / nb, j = t % nb;
-    A[i][j] = j <= i ? H[(k0 + i) * ldh + k0 + j] : 0.0;
-  }
-  __syncthreads();
+  const int lane = threadIdx.x;
+  for (int i = 0; i < nb; ++i)
+    for (int j = lane; j <= i; j += 32) A[i][j] = H[(k0 + i) * ldh + k0 + j];
+  __syncwarp();
   for (int j = 0; j < nb; ++j) {
-    if (threadIdx.x == 0) {
-      double d = A[j][j];
-      if (!(d > 0.0) || !isfinite(d)) { atomicOr(err, 8); d = 1.0; }
-      A[j][j] = sqrt(d);
+    double d = A[j][j];
+    if (!(d > 0.0) || !isfinite(d)) {
+      d = 1.0;
+      if (lane == 0) atomicOr(err, 8);
     }
-    __syncthreads();
-    for (int i = j + 1 + threadIdx.x; i < nb; i += blockDim.x) A[i][j] /= A[j][j];
-    __syncthreads();
-    for (int t = threadIdx.x; t < (nb - j - 1) * (nb - j - 1); t += blockDim.x) {
-      int i = j + 1 + t / (nb - j - 1), l = j + 1 + t % (nb - j - 1);
-      if (l <= i) A[i][l] -= A[i][j] * A[l][j];
+    const double sd = sqrt(d), inv = 1.0 / sd;
+    __syncwarp();
+    if (lane == 0) A[j][j] = sd;
+    for (int i = j + 1 + lane; i < nb; i += 32) A[i][j] *= inv;
+    __syncwarp();
+    for (int i = j + 1 + lane; i < nb; i += 32) {
+      const double aij = A[i][j];
+      for (int l = j + 1; l <= i; ++l) A[i][l] -= aij * A[l][j];
     }
-    __syncthreads();
+    __syncwarp();
   }
-  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
-    int i = t / nb, j = t % nb;
-    if (j <= i) H[(k0 + i) * ldh + k0 + j] = A[i][j];
-  }
-}
-
-// panel rows i >= k0 + nb: x L_kk^T = a  (forward substitution per row)
-__global__ void __launch_bounds__(128) k_trsm_panel(double *H, int64_t ldh, int64_t k0, int nb, int64_t n) {
-  __shared__ double L[NB][NB + 1];
-  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
-    int i = t / nb, j = t % nb;
-    L[i][j] = j <= i ? H[(k0 + i) * ldh + k0 + j] : 0.0;
-  }
-  __syncthreads();
-  int64_t i = k0 + nb + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  double x[NB];
-  double *row = H + i * ldh + k0;
-  for (int j = 0; j < nb; ++j) {
-    double a = row[j];
-    for (int l = 0; l < j; ++l) a -= x[l] * L[j][l];
-    x[j] = a / L[j][j];
-  }
-  for (int j = 0; j < nb; ++j) row[j] = x[j];
-}
-
-// trailing update of the lower triangle: H[i][l] -= sum_j L[i][j] L[l][j], one 64x64 tile per block
-__global__ void __launch_bounds__(256) k_chol_update(double *H, int64_t ldh, int64_t k0, int nb, int64_t n) {
-  constexpr int KC = 32;  // K chunk staged in shared memory
-  __shared__ double As[NB][KC + 1], Bs[NB][KC + 1];
-  const int64_t b = blockIdx.x;
-  int64_t ti = (int64_t)((sqrt(8.0 * (double)b + 1.0) - 1.0) * 0.5);
-  while (ti * (ti + 1) / 2 > b) --ti;
-  while ((ti + 1) * (ti + 2) / 2 <= b) ++ti;
-  const int64_t tl = b - ti * (ti + 1) / 2;
-  const int64_t r0 = k0 + nb + ti * NB, c0 = k0 + nb + tl * NB;
-  const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;  // 4x4 outputs per thread
-  double acc[4][4] = {};
-  for (int j0 = 0; j0 < nb; j0 += KC) {
-    const int kc = min(KC, nb - j0);
-    __syncthreads();
-    for (int t = threadIdx.x; t < NB * KC; t += blockDim.x) {
-      int i = t / KC, j = t % KC;
-      bool in = j < kc;
-      As[i][j] = (in && r0 + i < n) ? H[(r0 + i) * ldh + k0 + j0 + j] : 0.0;
-      Bs[i][j] = (in && c0 + i < n) ? H[(c0 + i) * ldh + k0 + j0 + j] : 0.0;
-    }
-    __syncthreads();
-    for (int j = 0; j < kc; ++j) {
-      double a[4], c[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        a[q] = As[ty + 16 * q][j];
-        c[q] = Bs[tx + 16 * q][j];
-      }
-#pragma unroll
-      for (int p = 0; p < 4; ++p)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) acc[p][q] = fma(a[p], c[q], acc[p][q]);
-    }
-  }
-#pragma unroll
-  for (int p = 0; p < 4; ++p)
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      int64_t i = r0 + ty + 16 * p, l = c0 + tx + 16 * q;
-      if (i < n && l <= i) H[i * ldh + l] -= acc[p][q];
-    }
-}
-
-// forward / backward substitution on one diagonal block (one block of threads)
-__global__ void k_trsv_diag(const double *H, int64_t ldh, int64_t k0, int nb, double *x, int lower) {
-  __shared__ double xs[NB];
-  if (threadIdx.x == 0) {
-    if (lower) {
-      for (int j = 0; j < nb; ++j) {
-        double a = x[k0 + j];
-        for (int l = 0; l < j; ++l) a -= H[(k0 + j) * ldh + k0 + l] * xs[l];
-        xs[j] = a / H[(k0 + j) * ldh + k0 + j];
-      }
-    } else {
-      for (int j = nb - 1; j >= 0; --j) {
-        double a = x[k0 + j];
-        for (int l = j + 1; l < nb; ++l) a -= H[(k0 + l) * ldh + k0 + j] * xs[l];
-        xs[j] = a / H[(k0 + j) * ldh + k0 + j];
-      }
-    }
-    for (int j = 0; j < nb; ++j) x[k0 + j] = xs[j];
-  }
-}
-
-// forward: x[i] -= sum_{j in block} L[i][j] x[j] for i below the block
-__global__ void k_trsv_fwd_update(const double *H, int64_t ldh, int64_t k0, int nb, int64_t n, double *x) {
-  int64_t i = k0 + nb + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  double a = 0;
-  for (int j = 0; j < nb; ++j) a += H[i * ldh + k0 + j] * x[k0 + j];
-  x[i] -= a;
-}
-
-// backward: x[k0+j] -= sum_{i >= k0+nb} L[i][k0+j] x[i]   (column reduction)
-__global__ void k_trsv_bwd_update(const double *H, int64_t ldh, int64_t k0, int nb, int64_t n, double *x) {
-  __shared__ double part[256];
-  const int j = blockIdx.x;
-  double a = 0;
-  for (int64_t i = k0 + nb + threadIdx.x; i < n; i += blockDim.x) a += H[i * ldh + k0 + j] * x[i];
-  part[threadIdx.x] = a;
-  __syncthreads();
-  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-    if (threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) x[k0 + j] -= part[0];
+  for (int i = 0; i < nb; ++i)
+    for (int j = lane; j <= i; j += 32) H[(k0 + i) * ldh + k0 + j] = A[i][j];
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
@@ -551,17 +444,19 @@ int cholesky_solve_run(double *H, int64_t n, int64_t ldh, double *x, cudaStream_
   const double one = 1.0, minus_one = -1.0;
   for (int64_t k0 = 0; k0 < n; k0 += NBO) {
     const int64_t kend = std::min(n, k0 + NBO);
-    // factor the diagonal block [k0, kend) in 64-column steps
+    // factor the diagonal block [k0, kend) in 64-column steps: warp factor of the 64 x 64
+    // diagonal, then DTRSM / DSYRK for the rest of the block (same column-major view as below)
     for (int64_t j0 = k0; j0 < kend; j0 += NB) {
-      const int nb = (int)std::min<int64_t>(NB, kend - j0);
-      k_potrf_diag<<<1, 256, 0, st>>>(H, ldh, j0, nb, errb.as<int>());
-      const int64_t rest = kend - j0 - nb;
-      count_launches(rest > 0 ? 3 : 1);
-      if (rest > 0) {
-        k_trsm_panel<<<(unsigned)ceil_div(rest, 128), 128, 0, st>>>(H, ldh, j0, nb, kend);
-        const int64_t T = ceil_div(rest, NB);
-        k_chol_update<<<(unsigned)(T * (T + 1) / 2), 256, 0, st>>>(H, ldh, j0, nb, kend);
-      }
+      const int64_t jb = std::min<int64_t>(NB, kend - j0), jend = j0 + jb, jr = kend - jend;
+      k_potrf_diag<<<1, 32, 0, st>>>(H, ldh, j0, (int)jb, errb.as<int>());
+      count_launches(1);
+      if (jr <= 0) continue;
+      if (cublasDtrsm(hb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, (int)jb,
+                      (int)jr, &one, H + j0 * ldh + j0, (int)ldh, H + jend * ldh + j0,
+                      (int)ldh) != CUBLAS_STATUS_SUCCESS ||
+          cublasDsyrk(hb, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, (int)jr, (int)jb, &minus_one, H + jend * ldh + j0,
+                      (int)ldh, &one, H + jend * ldh + jend, (int)ldh) != CUBLAS_STATUS_SUCCESS)
+        return fail(DGP_ERR_CUDA, "cholesky: cuBLAS call in the diagonal block failed");
     }
     DGP_CHECK_LAUNCH();
     const int64_t rest = n - kend, nb = kend - k0;
@@ -577,21 +472,14 @@ int cholesky_solve_run(double *H, int64_t n, int64_t ldh, double *x, cudaStream_
                     (int)ldh, &one, H + kend * ldh + kend, (int)ldh) != CUBLAS_STATUS_SUCCESS)
       return fail(DGP_ERR_CUDA, "cholesky: cublasDsyrk failed");
   }
+  DGP_CHECK_LAUNCH();
+  // L y = b, then L^T x = y (cuBLAS DTRSV on the column-major view Hc = L^T, upper)
+  if (cublasDtrsv(hb, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, (int)n, H, (int)ldh, x, 1) !=
+          CUBLAS_STATUS_SUCCESS ||
+      cublasDtrsv(hb, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, (int)n, H, (int)ldh, x, 1) !=
+          CUBLAS_STATUS_SUCCESS)
+    return fail(DGP_ERR_CUDA, "cholesky: cublasDtrsv failed");
   lk.unlock();
-  DGP_CHECK_LAUNCH();
-  for (int64_t k0 = 0; k0 < n; k0 += NB) {  // L y = b
-    const int nb = (int)std::min<int64_t>(NB, n - k0);
-    k_trsv_diag<<<1, 32, 0, st>>>(H, ldh, k0, nb, x, 1);
-    count_launches(n - k0 - nb > 0 ? 2 : 1);
-    if (n - k0 - nb > 0) k_trsv_fwd_update<<<(unsigned)ceil_div(n - k0 - nb, 256), 256, 0, st>>>(H, ldh, k0, nb, n, x);
-  }
-  for (int64_t k0 = ((n - 1) / NB) * NB; k0 >= 0; k0 -= NB) {  // L' x = y
-    const int nb = (int)std::min<int64_t>(NB, n - k0);
-    if (n - k0 - nb > 0) k_trsv_bwd_update<<<nb, 256, 0, st>>>(H, ldh, k0, nb, n, x);
-    k_trsv_diag<<<1, 32, 0, st>>>(H, ldh, k0, nb, x, 0);
-    count_launches(n - k0 - nb > 0 ? 2 : 1);
-  }
-  DGP_CHECK_LAUNCH();
   int herr = 0;
   DGP_CUDA(cudaMemcpyAsync(&herr, errb.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   DGP_CUDA(cudaStreamSynchronize(st));
