@@ -353,10 +353,10 @@ __device__ inline void row_spmv(int nsp, int cs, const int32_t *__restrict__ row
 // LPR nonzeros.  Rows of a warp loop to the warp's longest row (masked).
 template <int VEC, class Coef>
 __device__ inline void row_spmv_shfl(int nsp, int cs, const int32_t *__restrict__ rowptr, int64_t i, const Coef &cf,
-                                     const float2 *__restrict__ Xk, float2 (&y)[VEC], int lpr, int sub) {
+                                     const float2 *__restrict__ Xk, float2 (&y)[VEC], int lpr, int sub,
+                                     unsigned mask /* lanes of the warp's rows that exist */) {
 #pragma unroll
   for (int v = 0; v < VEC; ++v) y[v] = make_float2(0.f, 0.f);
-  const unsigned mask = __activemask();  // lanes past the last row have left the row loop
   const int b = __ldg(rowptr + i), e = __ldg(rowptr + i + 1);
   const int cmax = __reduce_max_sync(mask, e - b);
   for (int base = 0; base < cmax; base += lpr) {
@@ -406,9 +406,14 @@ __global__ void __launch_bounds__(BS) k_spmm(Layout L, Op op, const typename CT<
     for (int q = 0; q < NQ; ++q) part[v][q] = czero<C>();
   for (int it = 0; it < L.ipb; ++it) {
     const int64_t i = ln.row(L, it);
-    if (i >= L.n) break;
+    // every lane reaches this ballot each step (rows past n only `continue`), so the FP32
+    // row's shuffles run on an exact mask of the warp's valid rows
+    const bool valid = i < L.n;
+    const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+    if (vmask == 0u) break;
+    if (!valid) continue;
     C y[VEC];
-    if constexpr (sizeof(R) == 4) row_spmv_shfl<VEC>(L.nsp, cs, op.rowptr, i, cf, Xk, y, L.lpr, ln.sub);
+    if constexpr (sizeof(R) == 4) row_spmv_shfl<VEC>(L.nsp, cs, op.rowptr, i, cf, Xk, y, L.lpr, ln.sub, vmask);
     else row_spmv<VEC>(L.nsp, cs, op.rowptr, i, cf, Xk, y);
     const int64_t o = vidx(L, ln.k, i, c0);
     if (MODE != 2) stv<VEC>(Y + o, cs, y);
