@@ -70,7 +70,23 @@ struct Cols {
   double2 *acc;     // [NACC][C]
   int *active;      // 1 iterating, 2 converged at s this iteration, 0 frozen
   int *status;      // DGP_COL_*
+  int *hact;        // [nf] 1 while any column of harmonic k iterates; sweeps skip the others (NULL: none skipped)
+  int nsp;
 };
+
+// a sweep block of harmonic k has nothing to do once all of k's columns are frozen
+__device__ inline bool harmonic_done(const Cols &c, int k) { return c.hact && !c.hact[k]; }
+
+// hact[k] = 1 while any column of harmonic k is active (one block; call after active[] is final)
+__device__ inline void update_hact(const Cols &c) {
+  if (!c.hact) return;
+  const int nf = (int)(c.C / c.nsp);
+  for (int k = threadIdx.x; k < nf; k += blockDim.x) {
+    int any = 0;
+    for (int s = 0; s < c.nsp && !any; ++s) any = c.active[(int64_t)k * c.nsp + s] != 0;
+    c.hact[k] = any;
+  }
+}
 
 struct Layout {
   int64_t n;
@@ -392,6 +408,7 @@ __global__ void __launch_bounds__(BS) k_spmm(Layout L, Op op, const typename CT<
                                              const typename CT<R>::C *__restrict__ W, Cols cols, const Ctl *ctl) {
   using C = typename CT<R>::C;
   if (ctl && halted(ctl, ST_RUNNING)) return;
+  if (harmonic_done(cols, blockIdx.y)) return;
   extern __shared__ double2 smem[];
   Lane ln(L);
   const auto cf = op.make(ln.k);
@@ -488,6 +505,7 @@ __global__ void __launch_bounds__(BS) k_tspmm(TLayout T, Op op, const float2 *__
   constexpr int RPW = 32 / LPR;         // rows per warp
   constexpr int NQ = MODE == 2 ? 2 : 1;
   if (ctl && halted(ctl, ST_RUNNING)) return;
+  if (harmonic_done(cols, blockIdx.y)) return;
   extern __shared__ float4 tsm[];
   float2 *tile = reinterpret_cast<float2 *>(tsm);                      // [hcap][SW]
   Rec32 *srec = reinterpret_cast<Rec32 *>(tile + (size_t)hcap * SW);   // [zcap]
@@ -610,6 +628,7 @@ __global__ void __launch_bounds__(BS) k_update_s(Layout L, const typename CT<R>:
                                                  typename CT<R>::C *__restrict__ s, Cols cols, const Ctl *ctl) {
   using C = typename CT<R>::C;
   if (halted(ctl, ST_RUNNING)) return;
+  if (harmonic_done(cols, blockIdx.y)) return;
   extern __shared__ double2 smem[];
   Lane ln(L);
   constexpr int E = Chunk<typename CT<R>::C>::E;
@@ -653,6 +672,7 @@ __global__ void __launch_bounds__(BS) k_update_xrp(Layout L, typename CT<R>::C *
                                                    const Ctl *ctl) {
   using C = typename CT<R>::C;
   if (halted(ctl, ST_FINAL)) return;
+  if (harmonic_done(cols, blockIdx.y)) return;
   const bool final_ = *(volatile const int *)&ctl->state == ST_FINAL;
   extern __shared__ double2 smem[];
   Lane ln(L);
@@ -716,6 +736,7 @@ __global__ void __launch_bounds__(BS) k_update_p(Layout L, const typename CT<R>:
                                                  typename CT<R>::C *__restrict__ p, Cols cols, const Ctl *ctl) {
   using C = typename CT<R>::C;
   if (halted(ctl, ST_RUNNING)) return;
+  if (harmonic_done(cols, blockIdx.y)) return;
   Lane ln(L);
   constexpr int E = Chunk<typename CT<R>::C>::E;
   const int c0 = ln.template col0<E>(), cs = ln.template cs<E>(L);
@@ -890,6 +911,7 @@ __global__ void __launch_bounds__(1024) k_stage_count(Cols c, Ctl *ctl) {
   int a = 0;
   for (int64_t j = threadIdx.x; j < c.C; j += blockDim.x) a += c.active[j] != 0;
   a = BR(tmp).Sum(a);
+  update_hact(c);
   if (threadIdx.x == 0) {
     ctl->n_active = a;
     if (a == 0) {
@@ -955,7 +977,8 @@ __global__ void __launch_bounds__(1024) k_stage_init(Cols c, Ctl *ctl, int nsp, 
     if (!act) c.err[j] = 0.0;
     a += act;
   }
-  a = BR(tmp).Sum(a);
+  a = BR(tmp).Sum(a);  // (its barrier also orders the active[] writes before the loop below)
+  update_hact(c);
   if (threadIdx.x == 0) {
     ctl->n_active = a;
     ctl->iters = 0;
@@ -1348,12 +1371,14 @@ Work work_views(SolverPlan *S) {
   w.cols.beta = (double2 *)b; b += sizeof(double2) * C;
   w.cols.acc = (double2 *)b; b += sizeof(double2) * C * NACC;
   w.cols.active = (int *)b;
+  w.cols.hact = w.cols.active + C;
+  w.cols.nsp = S->nsp;
   w.cols.status = S->status.as<int>();
   w.ctl = S->ctl.as<Ctl>();
   return w;
 }
 
-size_t scal_bytes(int64_t C) { return (sizeof(double) * 4 + sizeof(double2) * (4 + NACC) + sizeof(int)) * C + 256; }
+size_t scal_bytes(int64_t C) { return (sizeof(double) * 4 + sizeof(double2) * (4 + NACC) + 2 * sizeof(int)) * C + 256; }
 
 template <class R> Vecs<R> vec_views(SolverPlan *S) {
   using C = typename CT<R>::C;
@@ -1749,10 +1774,12 @@ static int solve_mixed(SolverPlan *S, const double *d_B, const int32_t *d_nodes,
   for (int ref = 0; ref < max_ref; ++ref) {
     // inner FP32 solve on the current residual (already in V.r)
     const int inner_maxit = std::max(1, o.maxit - total_iters);
-    // all columns iterate until the largest residual reaches inner_tol (columns that converge
-    // early keep improving, which the next refinement step gains from); the stall guard of
-    // run_iterations ends inner solves that stop making progress in FP32
-    DGP_TRY(set_ctl(W.ctl, o.inner_tol, inner_maxit, DGP_STOP_MAX_ALL, st, S->h_ctl));
+    // inner columns stop individually: each column freezes at inner_tol and a harmonic whose
+    // columns are all frozen drops out of every sweep (low harmonics need ~4x the iterations of
+    // high ones, so this halves the inner work); the FP64 residual of every column is checked
+    // against tol after each inner solve.  The stall guard of run_iterations ends inner solves
+    // that stop making progress in FP32.
+    DGP_TRY(set_ctl(W.ctl, o.inner_tol, inner_maxit, DGP_STOP_PER_COLUMN, st, S->h_ctl));
     launch_init<float, VU>(layouts_for(S, VU).Ld, V, W, st);
     DGP_CHECK_LAUNCH();
     k_stage_init<<<1, 1024, 0, st>>>(W.cols, W.ctl, S->nsp, ns);
@@ -1858,6 +1885,7 @@ int solver_profile(SolverPlan *S, int which, int reps, float *ms, double *bytes,
   DGP_REQUIRE(reps >= 1 && which >= 0 && which <= 3, "profile: bad arguments");
   Vecs<float> V = vec_views<float>(S);
   Work W = work_views(S);
+  W.cols.hact = nullptr;  // timing / checking runs sweep every harmonic
   DevBuf dctl;
   DGP_TRY(dctl.alloc(sizeof(Ctl)));
   Ctl hc{};
@@ -1973,6 +2001,7 @@ int solver_autotune(SolverPlan *S, int32_t *tiled_out, int32_t *vec_out, int32_t
   DGP_TRY(ensure_workspace(S, DGP_PREC_MIXED));
   Vecs<float> V = vec_views<float>(S);
   Work W = work_views(S);
+  W.cols.hact = nullptr;  // timing / checking runs sweep every harmonic
   DevBuf dctl;
   DGP_TRY(dctl.alloc(sizeof(Ctl)));
   Ctl hc{};
@@ -2114,6 +2143,7 @@ int solver_check_spmm(SolverPlan *S, double *max_rel, cudaStream_t st) {
   DGP_TRY(ensure_workspace(S, DGP_PREC_MIXED));
   Vecs<float> V = vec_views<float>(S);
   Work W = work_views(S);
+  W.cols.hact = nullptr;  // timing / checking runs sweep every harmonic
   DevBuf dctl, dm;
   DGP_TRY(dctl.alloc(sizeof(Ctl)));
   DGP_TRY(dm.alloc(2 * sizeof(unsigned)));

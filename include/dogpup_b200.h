@@ -179,7 +179,13 @@ typedef struct dgp_solve_opts {
   double inner_tol;    /* mixed: complex-FP32 inner target per refinement  */
   int32_t max_refine;  /* mixed: maximum FP64 refinement steps             */
   int32_t fsai_cap;    /* FSAI pattern cap per row (reference: 30)         */
-  int32_t stop_rule;   /* DGP_STOP_MAX_ALL (reference) | PER_COLUMN        */
+  int32_t stop_rule;   /* FP64: DGP_STOP_MAX_ALL (reference: every column
+                        * iterates until the largest residual is below tol)
+                        * | PER_COLUMN (each column freezes at tol; sweeps
+                        * skip harmonics whose columns are all frozen).
+                        * Mixed: the inner complex-FP32 solves always stop
+                        * per column; every column's FP64 residual must
+                        * reach tol. */
   int32_t check_every; /* iterations per host convergence poll (>= 1)      */
 } dgp_solve_opts;
 
