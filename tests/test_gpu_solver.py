@@ -278,3 +278,28 @@ def test_tiled_spmm_matches_gather_and_solves(small_case, gpu_case, torch, ns):
     assert err.max() < 1e-6, err.max()
     with pytest.raises(Exception):
         S.set_spmm(False, vec=3)
+
+
+def test_solver_fp64_per_column_skips_finished_harmonics(small_case, gpu_case, torch):
+    """Per-column stopping (columns freeze at tol, finished harmonics leave the sweeps): every column
+    still meets tol against the sparse-direct solution, and every status word says converged."""
+    from dogpup_b200 import api
+    from oracle import solver as osv
+    K0, M0 = small_case["K"], small_case["M"]
+    nf, ns = 8, 5
+    dfc = 2 * np.pi / 10e-9 / (C_VAC / 1.4)
+    nodes, w = _point_sources(small_case, ns, 51)
+    fpsf = np.exp(-0.3j * np.arange(nf))
+    fem = gpu_case["fem"]
+    S = api.Solver(fem.rowptr, fem.col, gpu_case["K"], gpu_case["M"], dfc, nf, ns)
+    status = torch.full((nf * ns,), -1, dtype=torch.int32, device="cuda")
+    X, rep = S.solve_sources(torch.as_tensor(nodes, device="cuda"), torch.as_tensor(w, device="cuda"),
+                             torch.as_tensor(fpsf, device="cuda"),
+                             api.make_opts(tol=1e-11, precision="fp64", stop_rule="per_column"), status=status)
+    Q = np.zeros((K0.shape[0], ns, nf), complex)
+    for s in range(ns):
+        Q[nodes[s], s, :] = w[s][:, None] * fpsf[None, :]
+    xd = osv.direct_solve(K0, M0, dfc, Q)
+    err = np.linalg.norm(np.transpose(X.cpu().numpy(), (1, 2, 0)) - xd, axis=0) / np.linalg.norm(xd, axis=0)
+    assert err.max() < 1e-8, err.max()
+    assert (status.cpu().numpy() == 0).all()
