@@ -243,7 +243,7 @@ void dgp_solve_opts_default(dgp_solve_opts *o) {
   o->tol = 1e-12;       // dMesh.m:1243
   o->maxit = 1000;      // dMesh.m:1243
   o->precision = DGP_PREC_FP64;
-  o->inner_tol = 1e-4;
+  o->inner_tol = 3e-5;  // per-column inner stop: final FP64 residual ~10x below tol
   o->max_refine = 8;
   o->fsai_cap = 30;     // dMesh.m:1363
   o->stop_rule = DGP_STOP_MAX_ALL;
