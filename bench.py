@@ -499,10 +499,13 @@ def run_ours(a, rank, world, local_rank):
         rep = step()
         log(f"[rank {rank}] warmup {q}: {time.perf_counter() - t0:.2f}s, {rep.iterations} it, "
             f"{rep.refinements} ref, res {rep.max_rel_residual:.2e}, mem {solver.memory() / 1e9:.1f} GB")
+    # the sampler starts before the timed region (nvidia-smi's start-up talks to the driver and
+    # would stall the first timed launches) and keeps sampling through it
+    clk = Clocks(torch.cuda.current_device()) if rank == 0 else None
+    time.sleep(1.5)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    clk = Clocks(torch.cuda.current_device()) if rank == 0 else None
     from dogpup_b200._lib import lib as _dlib
     n_launch0 = _dlib.dgp_kernel_launches()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
