@@ -21,6 +21,7 @@ step time is the maximum over ranks.
 from __future__ import annotations
 
 import argparse
+import datetime
 import json
 import os
 import statistics
@@ -73,7 +74,7 @@ def workload(name, seed=1, order="morton"):
 # ------------------------------------------------------------------ clocks
 class Clocks:
     """nvidia-smi sampling during the timed region (read-only queries)."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -87,6 +88,10 @@ class Clocks:
         except FileNotFoundError:
             self.p = None
 
+    def mark(self):
+        """Start of the timed region: samples before it are not reported."""
+        self.t0 = datetime.datetime.now()
+
     def stop(self):
         if self.p is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
@@ -94,10 +99,17 @@ class Clocks:
         self.p.wait(timeout=10)
         self.f.flush()
         rows = []
+        t0 = getattr(self, "t0", None)
         for line in open(self.f.name):
             parts = [x.strip() for x in line.split(",")]
-            if len(parts) >= 9:
-                rows.append(parts)
+            if len(parts) < 10:
+                continue
+            try:
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f")
+            except ValueError:
+                continue
+            if t0 is None or ts >= t0:
+                rows.append(parts[1:])
         os.unlink(self.f.name)
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
@@ -507,6 +519,8 @@ def run_ours(a, rank, world, local_rank):
         dist.barrier()
     torch.cuda.synchronize()
     from dogpup_b200._lib import lib as _dlib
+    if clk:
+        clk.mark()
     n_launch0 = _dlib.dgp_kernel_launches()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(st)
