@@ -46,11 +46,10 @@ namespace {
 
 constexpr int BS = 256;
 constexpr int WARPS = BS / 32;
-constexpr int KERNELS_PER_ITER = 15;  // FP64; the fused complex-FP32 iteration has one fewer
+constexpr int KERNELS_PER_ITER = 15;
 
 enum { ST_RUNNING = 0, ST_FINAL = 1, ST_DONE = 2 };
-// dot-product slots; RS = r0^.s and RT = r0^.t feed the fused p update of the FP32 sweeps
-enum { ACC_D1 = 0, ACC_NS = 1, ACC_D2 = 2, ACC_D3 = 3, ACC_NR = 4, ACC_RHO = 5, ACC_RS = 6, ACC_RT = 7, NACC = 8 };
+enum { ACC_D1 = 0, ACC_NS = 1, ACC_D2 = 2, ACC_D3 = 3, ACC_NR = 4, ACC_RHO = 5, NACC = 6 };
 
 struct Ctl {
   int state;
@@ -402,7 +401,7 @@ __device__ inline bool halted(const Ctl *ctl, int need) {
 }
 
 // Y = Op_k X.  MODE 0: store.  MODE 1: store, acc[D1] += Y.W.
-// MODE 2: no store, acc[D2] += Y.W, acc[D3] += Y.Y.  MODE 3: store, acc[RT] += Y.W.
+// MODE 2: no store, acc[D2] += Y.W, acc[D3] += Y.Y.
 template <class R, int VEC, int MODE, class Op>
 __global__ void __launch_bounds__(BS) k_spmm(Layout L, Op op, const typename CT<R>::C *__restrict__ X,
                                              typename CT<R>::C *__restrict__ Y,
@@ -451,8 +450,8 @@ __global__ void __launch_bounds__(BS) k_spmm(Layout L, Op op, const typename CT<
     for (int v = 0; v < VEC; ++v)
 #pragma unroll
       for (int q = 0; q < NQ; ++q) pd[v][q] = d2(part[v][q]);
-    if constexpr (MODE == 1 || MODE == 3) {
-      const int slot[1] = {MODE == 1 ? ACC_D1 : ACC_RT};
+    if constexpr (MODE == 1) {
+      const int slot[1] = {ACC_D1};
       block_reduce<VEC, 1, E>(L, ln, pd, cols.acc, cols.C, slot, smem);
     } else {
       const int slot[2] = {ACC_D2, ACC_D3};
@@ -469,8 +468,7 @@ __global__ void __launch_bounds__(BS) k_spmm(Layout L, Op op, const typename CT<
 // memory with cp.async (all copies in flight at once, no dependent global
 // loads), then each lane accumulates VEC consecutive sources of a row from
 // shared memory (the record's pad word holds the column's halo position).
-// MODE as k_spmm: 0 store, 1 store + Y.W, 2 Y.W and Y.Y without the store, 3 store + Y.W
-// into the r0^.t slot.
+// MODE as k_spmm: 0 store, 1 store + Y.W, 2 Y.W and Y.Y without the store.
 struct TLayout {
   int64_t n;
   int nf, nsp, rb;
@@ -595,7 +593,7 @@ __global__ void __launch_bounds__(BS) k_tspmm(TLayout T, Op op, const float2 *__
         for (int q = 0; q < NQ; ++q) red[(warp * SW + sub * VEC + v) * NQ + q] = pd[v][q];
     }
     __syncthreads();
-    const int slot[2] = {MODE == 1 ? ACC_D1 : (MODE == 3 ? ACC_RT : ACC_D2), ACC_D3};
+    const int slot[2] = {MODE == 1 ? ACC_D1 : ACC_D2, ACC_D3};
     for (int t = threadIdx.x; t < SW * NQ; t += BS) {
       const int sc = t / NQ, q = t % NQ;
       double2 x = make_double2(0.0, 0.0);
@@ -624,12 +622,10 @@ __device__ inline void lane_scalars(const Cols &cols, const Lane &ln, const Layo
 }
 
 // s = r - alpha*v ; acc[NS] += |s|^2   (dMesh.m:1306-1307)
-// s = r - alpha*v ; acc[NS] += |s|^2  (dMesh.m:1306-1308); FUSE: also acc[RS] += r0^.s
-template <class R, int VEC, bool FUSE = false>
+template <class R, int VEC>
 __global__ void __launch_bounds__(BS) k_update_s(Layout L, const typename CT<R>::C *__restrict__ r,
                                                  const typename CT<R>::C *__restrict__ v,
-                                                 typename CT<R>::C *__restrict__ s, Cols cols, const Ctl *ctl,
-                                                 const typename CT<R>::C *__restrict__ rhat = nullptr) {
+                                                 typename CT<R>::C *__restrict__ s, Cols cols, const Ctl *ctl) {
   using C = typename CT<R>::C;
   if (halted(ctl, ST_RUNNING)) return;
   if (harmonic_done(cols, blockIdx.y)) return;
@@ -637,15 +633,12 @@ __global__ void __launch_bounds__(BS) k_update_s(Layout L, const typename CT<R>:
   Lane ln(L);
   constexpr int E = Chunk<typename CT<R>::C>::E;
   const int c0 = ln.template col0<E>(), cs = ln.template cs<E>(L);
-  constexpr int NQ = FUSE ? 2 : 1;
-  double2 part[VEC][NQ];
+  double2 part[VEC][1];
   C al[VEC];
   int act[VEC];
   lane_scalars<R, VEC>(cols, ln, L, cols.alpha, al, act);
 #pragma unroll
-  for (int q = 0; q < VEC; ++q)
-#pragma unroll
-    for (int u = 0; u < NQ; ++u) part[q][u] = make_double2(0, 0);
+  for (int q = 0; q < VEC; ++q) part[q][0] = make_double2(0, 0);
   for (int it = 0; it < L.ipb; ++it) {
     const int64_t i = ln.row(L, it);
     if (i >= L.n) break;
@@ -658,27 +651,15 @@ __global__ void __launch_bounds__(BS) k_update_s(Layout L, const typename CT<R>:
       ss[q] = act[q] ? cfmaT(cneg(al[q]), vv[q], rr[q]) : rr[q];
       if (act[q]) acc_abs2(part[q][0].x, ss[q]);
     }
-    if constexpr (FUSE) {
-      C rh[VEC];
-      ldv<VEC>(rhat + o, cs, rh);
-#pragma unroll
-      for (int q = 0; q < VEC; ++q)
-        if (act[q]) acc_bil(part[q][NQ - 1], rh[q], ss[q]);
-    }
     stv<VEC>(s + o, cs, ss);
   }
-  int slot[NQ];
-  slot[0] = ACC_NS;
-  if constexpr (NQ == 2) slot[1] = ACC_RS;
-  block_reduce<VEC, NQ, E>(L, ln, part, cols.acc, cols.C, slot, smem);
+  const int slot[1] = {ACC_NS};
+  block_reduce<VEC, 1, E>(L, ln, part, cols.acc, cols.C, slot, smem);
 }
 
 // x = x + alpha*h + omega*z ; r = s - omega*t ; p = p - omega*v ; acc[NR] += |r|^2 ;
 // acc[RHO] += r0^.r  (dMesh.m:1305, :1327-1337).  In the FINAL state: x = x + alpha*h (:1311).
-// FUSE (complex-FP32 sweeps): beta is already known -- rho = r0^.r = r0^.s - omega r0^.t from
-// the RS / RT dots -- so p = r + beta (p - omega v) (:1340) is written here, without r0^.r
-// and without the separate p update.
-template <class R, int VEC, bool FUSE = false>
+template <class R, int VEC>
 __global__ void __launch_bounds__(BS) k_update_xrp(Layout L, typename CT<R>::C *__restrict__ x,
                                                    const typename CT<R>::C *__restrict__ h,
                                                    const typename CT<R>::C *__restrict__ z,
@@ -697,17 +678,13 @@ __global__ void __launch_bounds__(BS) k_update_xrp(Layout L, typename CT<R>::C *
   Lane ln(L);
   constexpr int E = Chunk<typename CT<R>::C>::E;
   const int c0 = ln.template col0<E>(), cs = ln.template cs<E>(L);
-  constexpr int NQ = FUSE ? 1 : 2;
-  double2 part[VEC][NQ];
-  C al[VEC], om[VEC], be[VEC];
+  double2 part[VEC][2];
+  C al[VEC], om[VEC];
   int act[VEC];
   lane_scalars<R, VEC>(cols, ln, L, cols.omega, om, act);
   lane_scalars<R, VEC>(cols, ln, L, cols.alpha, al, act);
-  if constexpr (FUSE) lane_scalars<R, VEC>(cols, ln, L, cols.beta, be, act);
 #pragma unroll
-  for (int q = 0; q < VEC; ++q)
-#pragma unroll
-    for (int u = 0; u < NQ; ++u) part[q][u] = make_double2(0, 0);
+  for (int q = 0; q < VEC; ++q) part[q][0] = part[q][1] = make_double2(0, 0);
   for (int it = 0; it < L.ipb; ++it) {
     const int64_t i = ln.row(L, it);
     if (i >= L.n) break;
@@ -728,7 +705,7 @@ __global__ void __launch_bounds__(BS) k_update_xrp(Layout L, typename CT<R>::C *
     ldv<VEC>(t + o, cs, tt);
     ldv<VEC>(p + o, cs, pp);
     ldv<VEC>(v + o, cs, vv);
-    if constexpr (!FUSE) ldv<VEC>(rhat + o, cs, rh);
+    ldv<VEC>(rhat + o, cs, rh);
 #pragma unroll
     for (int q = 0; q < VEC; ++q) {
       if (!act[q]) {
@@ -738,12 +715,9 @@ __global__ void __launch_bounds__(BS) k_update_xrp(Layout L, typename CT<R>::C *
       xx[q] = cfmaT(om[q], zz[q], cfmaT(al[q], hh[q], xx[q]));
       rr[q] = cfmaT(cneg(om[q]), tt[q], ss[q]);
       pp[q] = cfmaT(cneg(om[q]), vv[q], pp[q]);
-      if constexpr (FUSE) {
-        if (act[q] == 1) pp[q] = cfmaT(be[q], pp[q], rr[q]);
-      }
       if (act[q] == 1) {
         acc_abs2(part[q][0].x, rr[q]);
-        if constexpr (!FUSE) acc_bil(part[q][NQ - 1], rh[q], rr[q]);
+        acc_bil(part[q][1], rh[q], rr[q]);
       }
     }
     stv<VEC>(x + o, cs, xx);
@@ -751,10 +725,8 @@ __global__ void __launch_bounds__(BS) k_update_xrp(Layout L, typename CT<R>::C *
     stv<VEC>(p + o, cs, pp);
   }
   if (!final_) {
-    int slot[NQ];
-    slot[0] = ACC_NR;
-    if constexpr (NQ == 2) slot[1] = ACC_RHO;
-    block_reduce<VEC, NQ, E>(L, ln, part, cols.acc, cols.C, slot, smem);
+    const int slot[2] = {ACC_NR, ACC_RHO};
+    block_reduce<VEC, 2, E>(L, ln, part, cols.acc, cols.C, slot, smem);
   }
 }
 
@@ -856,9 +828,6 @@ __global__ void __launch_bounds__(1024) k_stage_check_s(Cols c, Ctl *ctl) {
 }
 
 // after G t: omega = (Gt.Gs)/(Gt.Gt), dMesh.m:1325
-// FUSE: also rho = r0^.r = r0^.s - omega r0^.t into acc[RHO] (read by k_stage_check_r as
-// if k_update_xrp had summed it) and beta = rho/rho0 * (alpha/omega) for the fused p update
-template <bool FUSE = false>
 __global__ void __launch_bounds__(1024) k_stage_omega(Cols c, Ctl *ctl) {
   if (ctl->state == ST_DONE) return;
   const bool fin = ctl->state == ST_FINAL;
@@ -866,13 +835,6 @@ __global__ void __launch_bounds__(1024) k_stage_omega(Cols c, Ctl *ctl) {
     double2 d2v = c.acc[ACC_D2 * c.C + j], d3 = c.acc[ACC_D3 * c.C + j];
     c.acc[ACC_D2 * c.C + j] = make_double2(0, 0);
     c.acc[ACC_D3 * c.C + j] = make_double2(0, 0);
-    double2 rs = make_double2(0, 0), rt = make_double2(0, 0);
-    if (FUSE) {
-      rs = c.acc[ACC_RS * c.C + j];
-      rt = c.acc[ACC_RT * c.C + j];
-      c.acc[ACC_RS * c.C + j] = make_double2(0, 0);
-      c.acc[ACC_RT * c.C + j] = make_double2(0, 0);
-    }
     if (c.active[j] != 1 || fin) continue;
     double2 om = cdiv(d2v, d3);
     if (!(cabs2(d3) > 0.0) || !finite2(om) || !(cabs2(om) > 0.0)) {
@@ -880,11 +842,6 @@ __global__ void __launch_bounds__(1024) k_stage_omega(Cols c, Ctl *ctl) {
       continue;
     }
     c.omega[j] = om;
-    if (FUSE) {
-      const double2 rho = csub(rs, cmul(om, rt));
-      c.acc[ACC_RHO * c.C + j] = rho;
-      c.beta[j] = cmul(cdiv(rho, c.rho0[j]), cdiv(c.alpha[j], om));
-    }
   }
 }
 
@@ -1330,13 +1287,12 @@ void tspmm_launch(const SolverPlan *S, const TiledPlan &T, const int32_t *rowptr
 // dynamic shared-memory limits of the three modes, large enough for every plan in Ts
 template <int SW, class Op>
 int tspmm_attrs(std::initializer_list<const TiledPlan *> Ts) {
-  size_t b[4] = {0, 0, 0, 0};
+  size_t b[3] = {0, 0, 0};
   for (const TiledPlan *T : Ts)
-    for (int m = 0; m < 4; ++m) b[m] = std::max(b[m], tile_smem(*T, SW, m));
+    for (int m = 0; m < 3; ++m) b[m] = std::max(b[m], tile_smem(*T, SW, m));
   DGP_CUDA(cudaFuncSetAttribute(k_tspmm<0, SW, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b[0]));
   DGP_CUDA(cudaFuncSetAttribute(k_tspmm<1, SW, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b[1]));
   DGP_CUDA(cudaFuncSetAttribute(k_tspmm<2, SW, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b[2]));
-  DGP_CUDA(cudaFuncSetAttribute(k_tspmm<3, SW, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b[3]));
   return DGP_OK;
 }
 
@@ -1371,7 +1327,7 @@ int tiled_setup(SolverPlan *S, cudaStream_t st) {
   const int sw = tile_sw(S);
   size_t need = 0;
   for (const TiledPlan *T : {&S->tA, &S->tG, &S->tGT})
-    for (int m = 0; m < 4; ++m) need = std::max(need, tile_smem(*T, sw, m));
+    for (int m = 0; m < 3; ++m) need = std::max(need, tile_smem(*T, sw, m));
   S->tiled_ok = need <= TILE_SMEM_MAX && S->nsp % sw == 0;
   if (!S->tiled_ok) return DGP_OK;
   auto attrs = [&](auto w) {
@@ -1490,34 +1446,31 @@ inline int vec_for(const SolverPlan *S, bool fp32) {
 
 dim3 grid_of(const Layout &L) { return dim3((unsigned)ceil_div(L.n, L.rows_per_block()), (unsigned)L.nf); }
 
+// one BiCGSTAB iteration (dMesh.m:1295-1340) enqueued on st: KERNELS_PER_ITER launches
 // lane widths: plain SpMM sweeps VS, SpMM sweeps with dot products VD, vector updates 2
 constexpr int VU = 2;
 
-// one BiCGSTAB iteration (dMesh.m:1295-1340) enqueued on st: KERNELS_PER_ITER launches (FP64)
-// or one fewer (complex FP32).
-// The complex-FP32 iteration fuses the p update (:1340) into the x / r update: r0^.r is
-// formed as r0^.s - omega r0^.t from dots taken in the s update and in t = A z, so beta is
-// known before x, r, p are written (two vector passes and one launch fewer per iteration).
-
-// complex-FP32 iteration with the tiled SpMM (same kernel sequence as the gather one)
+// one BiCGSTAB iteration (dMesh.m:1295-1340) enqueued on st: KERNELS_PER_ITER launches
+// one complex-FP32 iteration with the tiled SpMM (same kernel sequence as enqueue_iteration)
 void enqueue_iteration_tiled(const SolverPlan *S, const Vecs<float> &V, const Work &W, cudaStream_t st) {
-  const Layout Lud = layouts_for(S, VU).Ld;
+  const Layout Lu = layouts_for(S, VU).L, Lud = layouts_for(S, VU).Ld;
   Ctl *ctl = W.ctl;
   tspmm<0>(S, 1, V.p, V.T1, nullptr, W.cols, ctl, st);
   tspmm<0>(S, 2, V.T1, V.h, nullptr, W.cols, ctl, st);
   tspmm<1>(S, 0, V.h, V.v, V.rhat, W.cols, ctl, st);
   k_stage_alpha<<<1, 1024, 0, st>>>(W.cols, ctl);
-  k_update_s<float, VU, true><<<grid_of(Lud), BS, red_smem(Lud, 2), st>>>(Lud, V.r, V.v, V.s, W.cols, ctl, V.rhat);
+  k_update_s<float, VU><<<grid_of(Lud), BS, red_smem(Lud, 1), st>>>(Lud, V.r, V.v, V.s, W.cols, ctl);
   k_stage_check_s<<<1, 1024, 0, st>>>(W.cols, ctl);
   tspmm<0>(S, 1, V.s, V.T1, nullptr, W.cols, ctl, st);
   tspmm<0>(S, 2, V.T1, V.z, nullptr, W.cols, ctl, st);
-  tspmm<3>(S, 0, V.z, V.t, V.rhat, W.cols, ctl, st);
+  tspmm<0>(S, 0, V.z, V.t, nullptr, W.cols, ctl, st);
   tspmm<2>(S, 1, V.t, nullptr, V.T1, W.cols, ctl, st);
-  k_stage_omega<true><<<1, 1024, 0, st>>>(W.cols, ctl);
-  k_update_xrp<float, VU, true><<<grid_of(Lud), BS, red_smem(Lud, 1), st>>>(Lud, V.x, V.h, V.z, V.r, V.s, V.t,
-                                                                            V.p, V.v, V.rhat, W.cols, ctl);
+  k_stage_omega<<<1, 1024, 0, st>>>(W.cols, ctl);
+  k_update_xrp<float, VU><<<grid_of(Lud), BS, red_smem(Lud, 2), st>>>(Lud, V.x, V.h, V.z, V.r, V.s, V.t, V.p, V.v,
+                                                                      V.rhat, W.cols, ctl);
   k_stage_check_r<<<1, 1024, 0, st>>>(W.cols, ctl);
   k_stage_count<<<1, 1024, 0, st>>>(W.cols, ctl);
+  k_update_p<float, VU><<<grid_of(Lu), BS, 0, st>>>(Lu, V.r, V.p, W.cols, ctl);
 }
 
 template <class R, int VS, int VD, class OpA, class OpG>
@@ -1526,8 +1479,7 @@ void enqueue_iteration(const SolverPlan *S, const OpA &A, const OpG &G, const Op
   const Layout Ls = spmm_layouts(S, VS, sizeof(R) == 4).L, Lsd = spmm_layouts(S, VD, sizeof(R) == 4).Ld;
   const Layout Lu = layouts_for(S, VU).L, Lud = layouts_for(S, VU).Ld;
   Ctl *ctl = W.ctl;
-  constexpr bool F = sizeof(R) == 4;  // fused p update
-  if constexpr (F) {
+  if constexpr (sizeof(R) == 4) {
     if (S->tiled) {
       enqueue_iteration_tiled(S, V, W, st);
       return;
@@ -1539,28 +1491,22 @@ void enqueue_iteration(const SolverPlan *S, const OpA &A, const OpG &G, const Op
   // v = A h, d1 = v.r0^                                         (:1301, :1304)
   k_spmm<R, VD, 1><<<grid_of(Lsd), BS, red_smem(Lsd, 1), st>>>(Lsd, A, V.h, V.v, V.rhat, W.cols, ctl);
   k_stage_alpha<<<1, 1024, 0, st>>>(W.cols, ctl);
-  // s = r - alpha v ; ||s|| (; r0^.s)                            (:1306-1308)
-  k_update_s<R, VU, F><<<grid_of(Lud), BS, red_smem(Lud, F ? 2 : 1), st>>>(Lud, V.r, V.v, V.s, W.cols, ctl,
-                                                                           V.rhat);
+  // s = r - alpha v ; ||s||                                     (:1306-1308)
+  k_update_s<R, VU><<<grid_of(Lud), BS, red_smem(Lud, 1), st>>>(Lud, V.r, V.v, V.s, W.cols, ctl);
   k_stage_check_s<<<1, 1024, 0, st>>>(W.cols, ctl);
-  // Gs = G s ; z = G^T Gs ; t = A z (; r0^.t) ; (G t).Gs, (G t).(G t)   (:1315-1325)
+  // Gs = G s ; z = G^T Gs ; t = A z ; (G t).Gs, (G t).(G t)     (:1315-1325)
   k_spmm<R, VS, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, G, V.s, V.T1, nullptr, W.cols, ctl);
   k_spmm<R, VS, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, GT, V.T1, V.z, nullptr, W.cols, ctl);
-  if constexpr (F) {
-    const Layout Lsd3 = spmm_layouts(S, VS, true).Ld;
-    k_spmm<R, VS, 3><<<grid_of(Lsd3), BS, red_smem(Lsd3, 1), st>>>(Lsd3, A, V.z, V.t, V.rhat, W.cols, ctl);
-  } else {
-    k_spmm<R, VS, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, A, V.z, V.t, nullptr, W.cols, ctl);
-  }
+  k_spmm<R, VS, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, A, V.z, V.t, nullptr, W.cols, ctl);
   k_spmm<R, VD, 2><<<grid_of(Lsd), BS, red_smem(Lsd, 2), st>>>(Lsd, G, V.t, nullptr, V.T1, W.cols, ctl);
-  k_stage_omega<F><<<1, 1024, 0, st>>>(W.cols, ctl);
-  // x += alpha h + om z ; r = s - om t ; p -= om v (FP32: p = r + beta p) ; ||r|| (; r0^.r)
-  k_update_xrp<R, VU, F><<<grid_of(Lud), BS, red_smem(Lud, F ? 1 : 2), st>>>(Lud, V.x, V.h, V.z, V.r, V.s, V.t,
-                                                                              V.p, V.v, V.rhat, W.cols, ctl);
+  k_stage_omega<<<1, 1024, 0, st>>>(W.cols, ctl);
+  // x += alpha h + om z ; r = s - om t ; p -= om v ; ||r|| ; r0^.r   (:1305, :1327-1337)
+  k_update_xrp<R, VU><<<grid_of(Lud), BS, red_smem(Lud, 2), st>>>(Lud, V.x, V.h, V.z, V.r, V.s, V.t, V.p, V.v,
+                                                                  V.rhat, W.cols, ctl);
   k_stage_check_r<<<1, 1024, 0, st>>>(W.cols, ctl);
   k_stage_count<<<1, 1024, 0, st>>>(W.cols, ctl);
   // p = r + beta p                                              (:1340)
-  if constexpr (!F) k_update_p<R, VU><<<grid_of(Lu), BS, 0, st>>>(Lu, V.r, V.p, W.cols, ctl);
+  k_update_p<R, VU><<<grid_of(Lu), BS, 0, st>>>(Lu, V.r, V.p, W.cols, ctl);
 }
 
 template <class R, int VS>
@@ -1630,7 +1576,7 @@ int run_iterations(SolverPlan *S, const Vecs<R> &V, const Work &W, int check_eve
   for (int64_t launches = 0;; ++launches) {
     if (launches > max_launches) return fail(DGP_ERR_CUDA, "solver: control block never reached DONE");
     DGP_CUDA(cudaGraphLaunch(S->graph[gi], st));
-    count_launches((int64_t)(KERNELS_PER_ITER - (sizeof(R) == 4 ? 1 : 0)) * check_every);
+    count_launches((int64_t)KERNELS_PER_ITER * check_every);
     DGP_CUDA(cudaMemcpyAsync(h, W.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
     DGP_CUDA(cudaStreamSynchronize(st));
     if (h->state == ST_DONE) break;
@@ -1999,7 +1945,7 @@ void spmm_set(const SolverPlan *S, const OpA32 &A, const OpG32 &G, const OpG32 &
   k_spmm<float, VEC, 1><<<grid_of(Lsd), BS, red_smem(Lsd, 1), st>>>(Lsd, A, V.h, V.v, V.rhat, W.cols, ctl);
   k_spmm<float, VEC, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, G, V.s, V.T1, nullptr, W.cols, ctl);
   k_spmm<float, VEC, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, GT, V.T1, V.z, nullptr, W.cols, ctl);
-  k_spmm<float, VEC, 3><<<grid_of(Lsd), BS, red_smem(Lsd, 1), st>>>(Lsd, A, V.z, V.t, V.rhat, W.cols, ctl);
+  k_spmm<float, VEC, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, A, V.z, V.t, nullptr, W.cols, ctl);
   k_spmm<float, VEC, 2><<<grid_of(Lsd), BS, red_smem(Lsd, 2), st>>>(Lsd, G, V.t, nullptr, V.T1, W.cols, ctl);
 }
 }  // namespace
@@ -2010,7 +1956,7 @@ void tspmm_set(const SolverPlan *S, const Vecs<float> &V, const Work &W, const C
   tspmm<1>(S, 0, V.h, V.v, V.rhat, W.cols, ctl, st);
   tspmm<0>(S, 1, V.s, V.T1, nullptr, W.cols, ctl, st);
   tspmm<0>(S, 2, V.T1, V.z, nullptr, W.cols, ctl, st);
-  tspmm<3>(S, 0, V.z, V.t, V.rhat, W.cols, ctl, st);
+  tspmm<0>(S, 0, V.z, V.t, nullptr, W.cols, ctl, st);
   tspmm<2>(S, 1, V.t, nullptr, V.T1, W.cols, ctl, st);
 }
 
