@@ -288,6 +288,19 @@ def meas(det_nodes, det_w, link, phi) -> torch.Tensor:
     return out
 
 
+def locate_points(node: torch.Tensor, elem: torch.Tensor, pts, eps: float = 1e-12):
+    """(elem id [NP] int64, -1 outside; barycentric weights [NP][4]) of points [NP][3] on the device."""
+    node = torch.as_tensor(node).to(device="cuda", dtype=torch.float64).contiguous()
+    elem = torch.as_tensor(elem).to(device="cuda", dtype=torch.int32).contiguous()
+    pts = torch.as_tensor(pts).to(device="cuda", dtype=torch.float64).reshape(-1, 3).contiguous()
+    n = int(pts.shape[0])
+    eid = torch.empty(n, dtype=torch.int32, device="cuda")
+    w = torch.empty((n, 4), dtype=torch.float64, device="cuda")
+    check(lib.dgp_locate_points(ptr(node), ptr(elem), int(node.shape[0]), int(elem.shape[0]), ptr(pts), n,
+                                float(eps), ptr(eid), ptr(w), stream_ptr()))
+    return eid.long(), w
+
+
 # ------------------------------------------------------ reverse-mode pieces
 def tg_adjoint_rhs(det_nodes, det_w, link, gate_fc, nt, g, n, nf, ns) -> torch.Tensor:
     """dL/dphi [NF][NN][NS] complex128 for L = sum g * fc2tg(meas(phi)), g [NM][NG]."""

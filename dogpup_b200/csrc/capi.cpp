@@ -428,6 +428,12 @@ int dgp_tg_adjoint_rhs(const int32_t *d_det_nodes, const double *d_det_w, int32_
                            (cudaStream_t)stream));
 }
 
+// ----------------------------------------------------------- point location
+int dgp_locate_points(const double *d_node, const int32_t *d_elem, int64_t nn, int64_t ne, const double *d_pts,
+                      int64_t np, double eps, int32_t *d_eid, double *d_w, dgp_stream_t stream) {
+  DGP_GUARD(locate_points(d_node, d_elem, nn, ne, d_pts, np, eps, d_eid, d_w, (cudaStream_t)stream));
+}
+
 // -------------------------------------------------------- normal equations
 int dgp_normal_eq(const float *d_Jt, int64_t nv, int64_t nmeas, const double *d_w, const double *d_y, double lambda,
                   int32_t damping, double *d_H, int64_t ldh, double *d_rhs, dgp_stream_t stream) {

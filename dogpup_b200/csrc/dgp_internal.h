@@ -124,6 +124,10 @@ int solver_set_spmm(SolverPlan *S, int32_t tiled, int32_t vec, int32_t rows);
 // largest relative difference between the tiled and the gather SpMM on the plan's operators
 int solver_check_spmm(SolverPlan *S, double *max_rel, cudaStream_t st);
 
+// containing tetrahedron (-1: none) and barycentric weights [np][4] of points [np][3]
+int locate_points(const double *d_node, const int32_t *d_elem, int64_t nn, int64_t ne, const double *d_pts,
+                  int64_t np, double eps, int32_t *d_eid, double *d_w, cudaStream_t st);
+
 // batched operators (layout [nf][n][ns] complex)
 int spmm_A_f64(const int32_t *rowptr, const int32_t *col, const double2 *KM, const double *omega, int64_t n,
                int32_t nf, int32_t ns, const double2 *X, double2 *Y, cudaStream_t st);

@@ -131,10 +131,12 @@ class DMesh:
         return api.meas(nodes, w, link, phi)
 
     # ------------------------------------------------------------ Jacobian
-    def mesh2grid(self, x, y, z):
-        """Voxel basis of the Jacobian (dMesh.m:286-380): m2g, g2m, gridinmesh, dxyz."""
+    def mesh2grid(self, x, y, z, device=True):
+        """Voxel basis of the Jacobian (dMesh.m:286-380): m2g, g2m, gridinmesh, dxyz.
+        device=False locates the voxel centres on the host instead of the GPU."""
         from .grid import mesh2grid
-        g = mesh2grid(self.node_host, self.elem_host, np.asarray(x), np.asarray(y), np.asarray(z), self.locator())
+        g = mesh2grid(self.node_host, self.elem_host, np.asarray(x), np.asarray(y), np.asarray(z),
+                      None if device else self.locator(), device=device)
         self.grid, self.m2g, self.g2m = g["grid"], g["m2g"], g["g2m"]
         self.gridinmesh, self.dxyz, self.gridSize = g["gridinmesh"], g["dxyz"], g["size"]
         self.grid_basis = api.Basis(self.m2g, np.full(self.m2g.shape[0], self.dxyz ** 3))

@@ -397,6 +397,20 @@ int dgp_jacobian_tg_vjp(const int32_t *d_P_rowptr, const int32_t *d_P_col,
                         double *d_out, dgp_stream_t stream);
 
 /* ====================================================================== *
+ *  Point location for the voxel basis (mesh2grid, dMesh.m:286-327; the
+ *  reference uses MATLAB's pointLocation on the host).
+ * ====================================================================== */
+/* For each point d_pts[i][0..2]: d_eid[i] = the element whose smallest
+ * barycentric weight is largest (ties: lower element id) when that weight is
+ * >= -eps, else -1; d_w[i][0..3] its barycentric weights for the vertices
+ * d_elem[e][0..3] (zeros when d_eid[i] == -1).  d_node [nn][3] float64,
+ * d_elem [ne][4] int32 (0-based).  Bins the elements on the device; the
+ * call synchronises the stream. */
+int dgp_locate_points(const double *d_node, const int32_t *d_elem, int64_t nn,
+                      int64_t ne, const double *d_pts, int64_t np, double eps,
+                      int32_t *d_eid, double *d_w, dgp_stream_t stream);
+
+/* ====================================================================== *
  *  Levenberg-Marquardt normal equations (tik_inv, reconstruction/
  *  tik_inv.m:1-20, with a diagonal data weight W = 1/sigma^2).
  * ====================================================================== */

@@ -14,6 +14,44 @@ import scipy.sparse as sp
 from .transforms import fc2tg
 
 
+def point_location(node, elem, pts, eps=1e-12, chunk=64):
+    """Containing tetrahedron and barycentric weights of each point, by testing
+    every element (MATLAB ``pointLocation`` in mesh2grid, dMesh.m:311-313).
+
+    The element whose smallest barycentric weight is largest wins (ties: lower
+    id); it is accepted when that weight is >= -eps, else the point is outside
+    (-1, zero weights).  Returns (eid [NP] int64, w [NP, 4])."""
+    node = np.asarray(node, dtype=np.float64)
+    elem = np.asarray(elem, dtype=np.int64)
+    pts = np.atleast_2d(np.asarray(pts, dtype=np.float64))
+    v = node[elem]                                                   # [NE, 4, 3]
+    T = np.stack([v[:, 1] - v[:, 0], v[:, 2] - v[:, 0], v[:, 3] - v[:, 0]], axis=-1)
+    Ti = np.linalg.inv(T)                                            # [NE, 3, 3]
+    eid = np.full(pts.shape[0], -1, dtype=np.int64)
+    w = np.zeros((pts.shape[0], 4))
+    for c0 in range(0, pts.shape[0], chunk):
+        p = pts[c0:c0 + chunk]
+        l = np.einsum("eij,pej->pei", Ti, p[:, None, :] - v[None, :, 0])   # [P, NE, 3]
+        lam = np.concatenate([1.0 - l.sum(-1, keepdims=True), l], axis=-1)
+        score = lam.min(-1)
+        j = np.argmax(score, axis=1)                                 # first maximum: lowest id
+        best = score[np.arange(p.shape[0]), j]
+        ok = best >= -eps
+        rows = np.arange(c0, c0 + p.shape[0])[ok]
+        eid[rows] = j[ok]
+        w[rows] = lam[ok, j[ok]]
+    return eid, w
+
+
+def m2g_matrix(node, elem, grid, eps=1e-12):
+    """mesh-to-grid interpolation [NV, NN] and the in-mesh mask (dMesh.m:311-327)."""
+    eid, w = point_location(node, elem, grid, eps)
+    inm = eid >= 0
+    ii = np.repeat(np.nonzero(inm)[0], 4)
+    jj = np.asarray(elem, dtype=np.int64)[eid[inm]].ravel()
+    return sp.csr_matrix((w[inm].ravel(), (ii, jj)), shape=(grid.shape[0], node.shape[0])), inm
+
+
 def j_complex(P, w, phi, phiA, link, fpsf):
     """J[m, k, v] = -(P phi_s)[v,k] * (P phiA_d)[v,k] * w[v] / s_fpsf[k], dMesh.m:239-245.
 

@@ -1,0 +1,91 @@
+"""Device point location (dgp_locate_points) against the oracle's brute-force
+point location (every element tested), and the device mesh2grid basis.
+
+Element ids must agree wherever the containing element is unique (the
+oracle's best score above 1e-9); elsewhere -- points on shared faces, edges
+or vertices -- any of the tied elements is correct, so the interpolation of a
+linear field is compared instead (1e-11 absolute on O(10) values).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+LIN = np.array([0.3, -1.1, 0.7])
+
+
+def _oracle_scores(node, elem, pts, eid):
+    from oracle.jacobian import point_location
+    e0, w0 = point_location(node, elem, pts)
+    return e0, w0
+
+
+def _check(node, elem, pts):
+    from dogpup_b200 import api
+    e_d, w_d = api.locate_points(node, elem, pts)
+    eid, w = e_d.cpu().numpy(), w_d.cpu().numpy()
+    e0, w0 = _oracle_scores(node, elem, pts, eid)
+    assert np.array_equal(eid >= 0, e0 >= 0)
+    inm = e0 >= 0
+    unique = inm & (w0.min(axis=1) > 1e-9)
+    assert np.array_equal(eid[unique], e0[unique])
+    assert np.abs(w[unique] - w0[unique]).max(initial=0) < 1e-12
+    # any tied element interpolates a linear field exactly
+    f = node @ LIN + 2.0
+    fi = (w[inm] * f[elem[eid[inm]]]).sum(axis=1)
+    assert np.abs(fi - (pts[inm] @ LIN + 2.0)).max(initial=0) < 1e-11
+    assert not w[~inm].any()
+    assert np.abs(w[inm].sum(axis=1) - 1).max(initial=0) < 1e-12
+    return eid, inm
+
+
+def test_locate_ellipsoid_grid_inside_and_outside():
+    from dogpup_b200.meshgen import ellipsoid_mesh
+    m = ellipsoid_mesh((12, 10, 8), 1.0, 0.15, 7)
+    lo, hi = m.node.min(0), m.node.max(0)
+    xs = [np.arange(lo[d] - 1.3, hi[d] + 1.31, 0.7) for d in range(3)]
+    X, Y, Z = np.meshgrid(*xs, indexing="ij")
+    pts = np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1)
+    _, inm = _check(m.node, m.elem.astype(np.int64), pts)
+    assert inm.sum() > 200 and (~inm).sum() > 200
+
+
+def test_locate_points_on_vertices_faces_and_far_away():
+    from dogpup_b200.meshgen import box_mesh
+    m = box_mesh((4, 3, 5), 1.0)                     # lattice: grid points hit vertices, edges and faces
+    xs = [np.arange(-0.5, s + 0.51, 0.5) for s in (4, 3, 5)]
+    X, Y, Z = np.meshgrid(*xs, indexing="ij")
+    pts = np.concatenate([np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1),
+                          [[1e6, 0, 0], [-3, -3, -3], [2, 1.5, 1e3], [np.nan, 1, 1]]])
+    # the NaN point is outside for the device and the oracle alike
+    eid, inm = _check(m.node, m.elem.astype(np.int64), np.nan_to_num(pts, nan=-7.0))
+    from dogpup_b200 import api
+    e_nan, w_nan = api.locate_points(m.node, m.elem.astype(np.int64), pts[-1:])
+    assert int(e_nan[0]) == -1 and not w_nan.any()
+    assert (eid[-4:] == -1).all()
+
+
+def test_locate_empty_and_single_point():
+    from dogpup_b200 import api
+    from dogpup_b200.meshgen import box_mesh
+    m = box_mesh((2, 2, 2), 1.0)
+    e, w = api.locate_points(m.node, m.elem.astype(np.int64), np.zeros((0, 3)))
+    assert e.shape == (0,) and w.shape == (0, 4)
+    _check(m.node, m.elem.astype(np.int64), np.array([[0.25, 0.5, 0.75]]))
+
+
+def test_dmesh_mesh2grid_device_equals_host():
+    from dogpup_b200 import workloads
+    w = workloads.small_fwd(ns=2, nd=2, nf=4)
+    mesh = workloads.build_dmesh(w)
+    lo, hi = w["mesh"].node.min(0), w["mesh"].node.max(0)
+    xs = [np.arange(lo[d] - 2, hi[d] + 2.001, 1.5) for d in range(3)]
+    mesh.mesh2grid(*xs, device=False)
+    P_host, inm_host = mesh.m2g.copy(), mesh.gridinmesh.copy()
+    mesh.mesh2grid(*xs, device=True)
+    assert np.array_equal(mesh.gridinmesh, inm_host)
+    f = mesh.node_host @ LIN + 2.0
+    assert np.abs(mesh.m2g @ f - P_host @ f).max() < 1e-11
+    assert mesh.m2g.nnz == P_host.nnz
+    g = mesh.grid @ LIN + 2.0
+    assert np.abs((mesh.m2g @ f)[mesh.gridinmesh] - g[mesh.gridinmesh]).max() < 1e-11

@@ -159,3 +159,23 @@ def test_morton_and_lattice_orders_are_the_same_mesh():
     # Morton order: consecutive runs of 64 nodes span compact lattice boxes
     spans = [np.ptp(b.lattice[i:i + 64], axis=0).max() for i in range(0, b.nn - 64, 64)]
     assert np.median(spans) <= 7
+
+
+def test_point_location_oracle_against_host_locator():
+    """Brute-force point location (oracle) vs the package's k-d tree host locator:
+    the same in-mesh mask and the same interpolation of a linear field."""
+    from dogpup_b200.grid import mesh2grid
+    m = ellipsoid_mesh((8, 7, 6), 1.2, 0.15, 3)
+    lo, hi = m.node.min(0), m.node.max(0)
+    xs = [np.arange(lo[d] - 0.7, hi[d] + 0.71, 0.9) for d in range(3)]
+    g = mesh2grid(m.node, m.elem, *xs)
+    P, inm = jacobian.m2g_matrix(m.node, m.elem, g["grid"])
+    assert inm.sum() > 100 and (~inm).sum() > 100
+    assert np.array_equal(inm, g["gridinmesh"])
+    f = m.node @ np.array([0.3, -1.1, 0.7]) + 2.0
+    fg = g["grid"] @ np.array([0.3, -1.1, 0.7]) + 2.0
+    assert np.abs(P @ f - np.where(inm, fg, 0)).max() < 1e-11
+    assert np.abs(g["m2g"] @ f - P @ f).max() < 1e-11
+    # rows sum to one inside, empty outside
+    rs = np.asarray(P.sum(axis=1)).ravel()
+    assert np.abs(rs[inm] - 1).max() < 1e-12 and not rs[~inm].any()
