@@ -7,6 +7,7 @@ from __future__ import annotations
 
 import ctypes as C
 
+import numpy as np
 import torch
 
 from . import _lib
@@ -299,6 +300,28 @@ def locate_points(node: torch.Tensor, elem: torch.Tensor, pts, eps: float = 1e-1
     check(lib.dgp_locate_points(ptr(node), ptr(elem), int(node.shape[0]), int(elem.shape[0]), ptr(pts), n,
                                 float(eps), ptr(eid), ptr(w), stream_ptr()))
     return eid.long(), w
+
+
+def grid_to_mesh(node: torch.Tensor, axes, inmesh):
+    """g2m rows (voxel index [NN][4], -1 = empty; weight [NN][4]) for the lattice of
+    voxel centres ``ndgrid(*axes)`` (each axis uniformly spaced) and the in-mesh mask."""
+    node = torch.as_tensor(node).to(device="cuda", dtype=torch.float64).contiguous()
+    inm = torch.as_tensor(np.asarray(inmesh, dtype=np.uint8)).to("cuda").contiguous()
+    o, d, n = [], [], []
+    for a in axes:
+        a = np.asarray(a, dtype=np.float64).ravel()
+        step = a[1] - a[0] if a.size > 1 else 1.0
+        if a.size > 1 and np.abs(np.diff(a) - step).max() > 1e-9 * abs(step):
+            raise ValueError("grid axes must be uniformly spaced")
+        o.append(a[0]); d.append(step); n.append(a.size)
+    if int(np.prod(n)) != inm.numel():
+        raise ValueError("inmesh must have one flag per voxel")
+    o, d, n = (C.c_double * 3)(*o), (C.c_double * 3)(*d), (C.c_int32 * 3)(*n)
+    nn = int(node.shape[0])
+    col = torch.empty((nn, 4), dtype=torch.int32, device="cuda")
+    val = torch.empty((nn, 4), dtype=torch.float64, device="cuda")
+    check(lib.dgp_grid_to_mesh(ptr(node), nn, o, d, n, ptr(inm), ptr(col), ptr(val), stream_ptr()))
+    return col.long(), val
 
 
 # ------------------------------------------------------ reverse-mode pieces

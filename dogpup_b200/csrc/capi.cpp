@@ -434,6 +434,12 @@ int dgp_locate_points(const double *d_node, const int32_t *d_elem, int64_t nn, i
   DGP_GUARD(locate_points(d_node, d_elem, nn, ne, d_pts, np, eps, d_eid, d_w, (cudaStream_t)stream));
 }
 
+int dgp_grid_to_mesh(const double *d_node, int64_t nn, const double *origin, const double *spacing, const int32_t *n,
+                     const uint8_t *d_inmesh, int32_t *d_col, double *d_val, dgp_stream_t stream) {
+  if (!origin || !spacing || !n) return fail(DGP_ERR_ARG, "grid_to_mesh: null lattice description");
+  DGP_GUARD(grid_to_mesh(d_node, nn, origin, spacing, n, d_inmesh, d_col, d_val, (cudaStream_t)stream));
+}
+
 // -------------------------------------------------------- normal equations
 int dgp_normal_eq(const float *d_Jt, int64_t nv, int64_t nmeas, const double *d_w, const double *d_y, double lambda,
                   int32_t damping, double *d_H, int64_t ldh, double *d_rhs, dgp_stream_t stream) {

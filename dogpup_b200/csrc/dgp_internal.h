@@ -128,6 +128,10 @@ int solver_check_spmm(SolverPlan *S, double *max_rel, cudaStream_t st);
 int locate_points(const double *d_node, const int32_t *d_elem, int64_t nn, int64_t ne, const double *d_pts,
                   int64_t np, double eps, int32_t *d_eid, double *d_w, cudaStream_t st);
 
+// grid-to-mesh interpolation rows [nn][4] (voxel index or -1, weight) on a rectilinear lattice
+int grid_to_mesh(const double *d_node, int64_t nn, const double origin[3], const double spacing[3], const int32_t n[3],
+                 const uint8_t *d_inmesh, int32_t *d_col, double *d_val, cudaStream_t st);
+
 // batched operators (layout [nf][n][ns] complex)
 int spmm_A_f64(const int32_t *rowptr, const int32_t *col, const double2 *KM, const double *omega, int64_t n,
                int32_t nf, int32_t ns, const double2 *X, double2 *Y, cudaStream_t st);

@@ -193,4 +193,159 @@ int locate_points(const double *d_node, const int32_t *d_elem, int64_t nn, int64
   return DGP_OK;
 }
 
+
+// ---------------------------------------------------------------------------
+// Grid-to-mesh interpolation g2m [nn x nv] (dMesh.m:330-373).
+//
+// The reference triangulates the voxel centres (delaunay), locates every node
+// in that triangulation and keeps the barycentric weights of in-mesh voxels;
+// a node none of whose four voxels is in the mesh takes its nearest in-mesh
+// voxel with weight 1; rows are normalised to sum 1 (rows summing to 0 stay
+// 0).  The Delaunay triangulation of a rectilinear lattice is not unique
+// (the eight corners of a cell are cospherical); the Kuhn split is used:
+// cell corner c, fractional offsets sorted t_a >= t_b >= t_c (ties by axis
+// order) give the simplex c, c+e_a, c+e_a+e_b, c+1 with weights 1-t_a,
+// t_a-t_b, t_b-t_c, t_c.  No search is needed for the simplex; the nearest
+// in-mesh voxel is found by expanding shells around the nearest lattice point.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct Lattice {
+  double o[3], d[3];
+  int n[3];
+  __device__ int64_t index(int i, int j, int k) const { return ((int64_t)k * n[1] + j) * n[0] + i; }
+};
+
+__device__ inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// nearest in-mesh voxel of p (ties: lower voxel index); -1 if the grid has none
+__device__ int64_t nearest_inmesh(const Lattice &L, const uint8_t *__restrict__ inmesh, const double p[3]) {
+  double f[3];
+  int c[3];
+  double e = 0.0, dmin = 1e300;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    f[d] = (p[d] - L.o[d]) / L.d[d];
+    const double r = rint(fmin(fmax(f[d], -1.0), (double)L.n[d]));
+    c[d] = clampi((int)r, 0, L.n[d] - 1);
+    e = fmax(e, fabs(f[d] - c[d]));
+    dmin = fmin(dmin, fabs(L.d[d]));
+  }
+  const int rmax = max(L.n[0], max(L.n[1], L.n[2]));
+  int64_t best = -1;
+  double bd = 1e300;
+  for (int r = 0; r <= rmax; ++r) {
+    // every voxel of shell r is at least dmin * (r - e) away
+    if (best >= 0 && (r - e) * dmin > sqrt(bd)) break;
+    const int k0 = max(c[2] - r, 0), k1 = min(c[2] + r, L.n[2] - 1);
+    const int j0 = max(c[1] - r, 0), j1 = min(c[1] + r, L.n[1] - 1);
+    for (int k = k0; k <= k1; ++k)
+      for (int j = j0; j <= j1; ++j) {
+        const bool face = abs(k - c[2]) == r || abs(j - c[1]) == r;
+        const int step = face ? 1 : 2 * r;
+        for (int i = c[0] - r; i <= c[0] + r; i += (r == 0 ? 1 : step)) {
+          if (i < 0 || i >= L.n[0]) continue;
+          const int64_t v = L.index(i, j, k);
+          if (!inmesh[v]) continue;
+          // voxel centre o + i*d and squared distance rounded step by step (no contraction),
+          // so that equal distances compare equal whatever the compiler fuses
+          const double dx = p[0] - __dadd_rn(L.o[0], __dmul_rn((double)i, L.d[0]));
+          const double dy = p[1] - __dadd_rn(L.o[1], __dmul_rn((double)j, L.d[1]));
+          const double dz = p[2] - __dadd_rn(L.o[2], __dmul_rn((double)k, L.d[2]));
+          const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+          if (d2 < bd || (d2 == bd && v < best)) {
+            bd = d2;
+            best = v;
+          }
+        }
+      }
+  }
+  return best;
+}
+
+__global__ void k_grid_to_mesh(const double *__restrict__ node, int64_t nn, Lattice L,
+                               const uint8_t *__restrict__ inmesh, int32_t *__restrict__ col,
+                               double *__restrict__ val) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= nn) return;
+  const double p[3] = {node[3 * t], node[3 * t + 1], node[3 * t + 2]};
+  int32_t vc[4] = {-1, -1, -1, -1};
+  double vw[4] = {0, 0, 0, 0};
+  bool in_grid = true;
+  int cell[3];
+  double fr[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double f = (p[d] - L.o[d]) / L.d[d];
+    if (!(f >= 0.0 && f <= (double)(L.n[d] - 1))) in_grid = false;   // also NaN
+    const int hi = max(L.n[d] - 2, 0);
+    cell[d] = in_grid ? clampi((int)floor(f), 0, hi) : 0;
+    fr[d] = in_grid ? f - cell[d] : 0.0;
+    if (L.n[d] == 1) fr[d] = 0.0;                                     // flat axis: stay on the plane
+  }
+  int kept = 0;
+  if (in_grid) {
+    // axis order by descending fraction (stable in x, y, z)
+    int a = 0, b = 1, c = 2;
+    if (fr[b] > fr[a]) { int s = a; a = b; b = s; }
+    if (fr[c] > fr[b]) { int s = b; b = c; c = s; }
+    if (fr[b] > fr[a]) { int s = a; a = b; b = s; }
+    const double w[4] = {1.0 - fr[a], fr[a] - fr[b], fr[b] - fr[c], fr[c]};
+    int v[3] = {cell[0], cell[1], cell[2]};
+    const int ax[3] = {a, b, c};
+    double sum = 0.0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (q > 0) v[ax[q - 1]] = min(v[ax[q - 1]] + 1, L.n[ax[q - 1]] - 1);
+      const int64_t vox = L.index(v[0], v[1], v[2]);
+      if (inmesh[vox]) {
+        ++kept;
+        if (w[q] != 0.0) {
+          vc[q] = (int32_t)vox;
+          vw[q] = w[q];
+          sum += w[q];
+        }
+      }
+    }
+    if (kept > 0 && sum != 0.0) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) vw[q] = vw[q] / sum;
+    }
+  }
+  if (kept == 0) {
+    const int64_t v = nearest_inmesh(L, inmesh, p);
+    if (v >= 0) {
+      vc[0] = (int32_t)v;
+      vw[0] = 1.0;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    col[4 * t + q] = vc[q];
+    val[4 * t + q] = vw[q];
+  }
+}
+
+}  // namespace
+
+int grid_to_mesh(const double *d_node, int64_t nn, const double origin[3], const double spacing[3], const int32_t n[3],
+                 const uint8_t *d_inmesh, int32_t *d_col, double *d_val, cudaStream_t st) {
+  DGP_REQUIRE(d_node && d_inmesh && d_col && d_val, "grid_to_mesh: null pointer");
+  DGP_REQUIRE(nn > 0, "grid_to_mesh: no nodes");
+  Lattice L;
+  int64_t nv = 1;
+  for (int d = 0; d < 3; ++d) {
+    DGP_REQUIRE(n[d] >= 1 && spacing[d] != 0.0 && std::isfinite(spacing[d]) && std::isfinite(origin[d]),
+                "grid_to_mesh: bad lattice");
+    L.o[d] = origin[d];
+    L.d[d] = spacing[d];
+    L.n[d] = n[d];
+    nv *= n[d];
+  }
+  DGP_REQUIRE(nv < (int64_t)INT32_MAX, "grid_to_mesh: more than 2^31-1 voxels");
+  k_grid_to_mesh<<<(unsigned)ceil_div(nn, 128), 128, 0, st>>>(d_node, nn, L, d_inmesh, d_col, d_val);
+  DGP_CHECK_LAUNCH();
+  return DGP_OK;
+}
+
 }  // namespace dgp

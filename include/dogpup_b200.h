@@ -410,6 +410,22 @@ int dgp_locate_points(const double *d_node, const int32_t *d_elem, int64_t nn,
                       int64_t ne, const double *d_pts, int64_t np, double eps,
                       int32_t *d_eid, double *d_w, dgp_stream_t stream);
 
+/* Grid-to-mesh interpolation g2m (dMesh.m:330-373) on the lattice of voxel
+ * centres origin[d] + i*spacing[d], i < n[d], spacing != 0 (host arrays of 3;
+ * voxel index
+ * i + n0*(j + n1*k), MATLAB's ndgrid order).  Row r of g2m is written to
+ * d_col[r][0..3] (voxel index, -1 = empty) and d_val[r][0..3]: the
+ * barycentric weights of node r in the lattice's Kuhn triangulation (one of
+ * the Delaunay triangulations of a rectilinear lattice), restricted to voxels
+ * with d_inmesh[v] != 0 and normalised to sum 1; a node none of whose four
+ * voxels is in the mesh (or that lies outside the lattice) gets its nearest
+ * in-mesh voxel with weight 1 (ties: lower index).  Zero weights are
+ * dropped. */
+int dgp_grid_to_mesh(const double *d_node, int64_t nn, const double *origin,
+                     const double *spacing, const int32_t *n,
+                     const uint8_t *d_inmesh, int32_t *d_col, double *d_val,
+                     dgp_stream_t stream);
+
 /* ====================================================================== *
  *  Levenberg-Marquardt normal equations (tik_inv, reconstruction/
  *  tik_inv.m:1-20, with a diagonal data weight W = 1/sigma^2).

@@ -52,6 +52,63 @@ def m2g_matrix(node, elem, grid, eps=1e-12):
     return sp.csr_matrix((w[inm].ravel(), (ii, jj)), shape=(grid.shape[0], node.shape[0])), inm
 
 
+def g2m_matrix(node, axes, inmesh):
+    """Grid-to-mesh interpolation [NN, NV] (dMesh.m:330-373).
+
+    The reference locates every node in ``delaunay(grid)`` and keeps the
+    barycentric weights of in-mesh voxels (:332-348); a node none of whose
+    four voxels is in the mesh takes its nearest in-mesh voxel with weight 1
+    (:351-367); rows are normalised (:369-372).  A rectilinear lattice has
+    many Delaunay triangulations; this restatement uses the Kuhn split (cell
+    corner c, fractions sorted t_a >= t_b >= t_c with ties in axis order,
+    simplex c, c+e_a, c+e_a+e_b, c+1).  Nodes outside the lattice take the
+    nearest in-mesh voxel.  Nearest ties: lower voxel index."""
+    node = np.asarray(node, dtype=np.float64)
+    axes = [np.asarray(a, dtype=np.float64).ravel() for a in axes]
+    n = [a.size for a in axes]
+    o = [a[0] for a in axes]
+    d = [a[1] - a[0] if a.size > 1 else 1.0 for a in axes]
+    inmesh = np.asarray(inmesh, dtype=bool)
+    X, Y, Z = np.meshgrid(*axes, indexing="ij")
+    grid = np.stack([X.ravel(order="F"), Y.ravel(order="F"), Z.ravel(order="F")], axis=1)
+    inm_idx = np.nonzero(inmesh)[0]
+    rows, cols, vals = [], [], []
+    for r in range(node.shape[0]):
+        p = node[r]
+        f = [(p[k] - o[k]) / d[k] for k in range(3)]
+        in_grid = all(0.0 <= f[k] <= n[k] - 1 for k in range(3))
+        kept, ent = 0, []
+        if in_grid:
+            cell = [min(max(int(np.floor(f[k])), 0), max(n[k] - 2, 0)) for k in range(3)]
+            fr = [0.0 if n[k] == 1 else f[k] - cell[k] for k in range(3)]
+            order = sorted(range(3), key=lambda k: -fr[k])            # stable: ties keep axis order
+            a, b, c = order
+            w = [1.0 - fr[a], fr[a] - fr[b], fr[b] - fr[c], fr[c]]
+            v = list(cell)
+            for q in range(4):
+                if q > 0:
+                    ax = order[q - 1]
+                    v[ax] = min(v[ax] + 1, n[ax] - 1)
+                vox = v[0] + n[0] * (v[1] + n[1] * v[2])
+                if inmesh[vox]:
+                    kept += 1
+                    if w[q] != 0.0:
+                        ent.append((vox, w[q]))
+            s = 0.0
+            for _, wq in ent:
+                s += wq
+            if s != 0.0:
+                ent = [(vox, wq / s) for vox, wq in ent]
+        if kept == 0 and inm_idx.size:
+            d2 = ((grid[inm_idx] - p) ** 2).sum(axis=1)
+            ent = [(int(inm_idx[int(np.argmin(d2))]), 1.0)]
+        for vox, wq in ent:
+            rows.append(r)
+            cols.append(vox)
+            vals.append(wq)
+    return sp.csr_matrix((vals, (rows, cols)), shape=(node.shape[0], grid.shape[0]))
+
+
 def j_complex(P, w, phi, phiA, link, fpsf):
     """J[m, k, v] = -(P phi_s)[v,k] * (P phiA_d)[v,k] * w[v] / s_fpsf[k], dMesh.m:239-245.
 

@@ -1,5 +1,6 @@
 """Device point location (dgp_locate_points) against the oracle's brute-force
-point location (every element tested), and the device mesh2grid basis.
+point location (every element tested), the device grid-to-mesh map
+(dgp_grid_to_mesh) against the oracle's g2m, and the device mesh2grid basis.
 
 Element ids must agree wherever the containing element is unique (the
 oracle's best score above 1e-9); elsewhere -- points on shared faces, edges
@@ -86,6 +87,72 @@ def test_dmesh_mesh2grid_device_equals_host():
     assert np.array_equal(mesh.gridinmesh, inm_host)
     f = mesh.node_host @ LIN + 2.0
     assert np.abs(mesh.m2g @ f - P_host @ f).max() < 1e-11
-    assert mesh.m2g.nnz == P_host.nnz
     g = mesh.grid @ LIN + 2.0
     assert np.abs((mesh.m2g @ f)[mesh.gridinmesh] - g[mesh.gridinmesh]).max() < 1e-11
+
+
+def _g2m_check(node, axes, inm):
+    """Device g2m rows vs the oracle's g2m: same pattern, weights to 1e-15;
+    nearest-voxel rows may differ only between voxels at equal distance."""
+    from dogpup_b200 import api
+    from dogpup_b200.grid import g2m_from_rows
+    from oracle.jacobian import g2m_matrix
+    col, val = api.grid_to_mesh(node, axes, inm)
+    nv = int(np.prod([len(a) for a in axes]))
+    G = g2m_from_rows(col.cpu().numpy(), val.cpu().numpy(), nv)
+    _g2m_compare(G, g2m_matrix(node, axes, inm), node, axes)
+    return G
+
+
+def _g2m_compare(G, G0, node, axes):
+    # rows sum to 1, or to 0 where the only in-mesh voxels of the node's simplex
+    # carry weight 0 (the reference's rule then adds no nearest voxel either)
+    rs = np.asarray(G.sum(axis=1)).ravel()
+    assert np.minimum(np.abs(rs - 1), np.abs(rs)).max() < 1e-14
+    diff = abs(G - G0).tocsr()
+    bad = np.nonzero(np.asarray(diff.max(axis=1).todense()).ravel() > 1e-15)[0]
+    X, Y, Z = np.meshgrid(*axes, indexing="ij")
+    grid = np.stack([X.ravel(order="F"), Y.ravel(order="F"), Z.ravel(order="F")], axis=1)
+    for r in bad:                                   # only nearest-voxel ties may differ
+        assert G.indptr[r + 1] - G.indptr[r] == 1 and G0.indptr[r + 1] - G0.indptr[r] == 1
+        v, v0 = G.indices[G.indptr[r]], G0.indices[G0.indptr[r]]
+        d, d0 = ((grid[v] - node[r]) ** 2).sum(), ((grid[v0] - node[r]) ** 2).sum()
+        assert abs(d - d0) <= 1e-12 * max(d0, 1.0)
+
+
+def test_g2m_ellipsoid_partial_grid():
+    """Lattice that stops short of the mesh on two sides: nodes outside it and
+    nodes with no in-mesh voxel take the nearest in-mesh voxel."""
+    from dogpup_b200.meshgen import ellipsoid_mesh
+    from oracle.jacobian import m2g_matrix
+    m = ellipsoid_mesh((12, 10, 8), 1.0, 0.15, 9)
+    lo, hi = m.node.min(0), m.node.max(0)
+    axes = [np.arange(lo[0] + 1.1, hi[0] + 0.8, 0.75), np.arange(lo[1] - 0.4, hi[1] - 0.9, 0.75),
+            np.arange(lo[2] - 0.4, hi[2] + 0.8, 0.75)]
+    X, Y, Z = np.meshgrid(*axes, indexing="ij")
+    grid = np.stack([X.ravel(order="F"), Y.ravel(order="F"), Z.ravel(order="F")], axis=1)
+    _, inm = m2g_matrix(m.node, m.elem, grid)
+    G = _g2m_check(m.node, axes, inm)
+    assert (np.diff(G.indptr) == 1).sum() > 20      # the nearest-voxel rule was exercised
+
+
+def test_g2m_nodes_on_lattice_points_and_descending_axis():
+    from dogpup_b200.meshgen import box_mesh
+    from oracle.jacobian import m2g_matrix
+    m = box_mesh((4, 3, 5), 1.0)
+    axes = [np.arange(4.5, -0.51, -0.5), np.arange(0.0, 3.01, 1.0), np.arange(-0.5, 5.51, 0.5)]
+    X, Y, Z = np.meshgrid(*axes, indexing="ij")
+    grid = np.stack([X.ravel(order="F"), Y.ravel(order="F"), Z.ravel(order="F")], axis=1)
+    _, inm = m2g_matrix(m.node, m.elem, grid)
+    _g2m_check(m.node, axes, inm)
+
+
+def test_dmesh_g2m_is_the_oracle_g2m():
+    from dogpup_b200 import workloads
+    from oracle.jacobian import g2m_matrix
+    w = workloads.small_fwd(ns=2, nd=2, nf=4)
+    mesh = workloads.build_dmesh(w)
+    lo, hi = w["mesh"].node.min(0), w["mesh"].node.max(0)
+    xs = [np.arange(lo[d] - 2, hi[d] + 2.001, 1.5) for d in range(3)]
+    mesh.mesh2grid(*xs)
+    _g2m_compare(mesh.g2m, g2m_matrix(mesh.node_host, xs, mesh.gridinmesh), mesh.node_host, xs)

@@ -164,18 +164,51 @@ def test_morton_and_lattice_orders_are_the_same_mesh():
 def test_point_location_oracle_against_host_locator():
     """Brute-force point location (oracle) vs the package's k-d tree host locator:
     the same in-mesh mask and the same interpolation of a linear field."""
-    from dogpup_b200.grid import mesh2grid
+    from dogpup_b200.grid import locate_host, m2g_from_location
     m = ellipsoid_mesh((8, 7, 6), 1.2, 0.15, 3)
     lo, hi = m.node.min(0), m.node.max(0)
     xs = [np.arange(lo[d] - 0.7, hi[d] + 0.71, 0.9) for d in range(3)]
-    g = mesh2grid(m.node, m.elem, *xs)
-    P, inm = jacobian.m2g_matrix(m.node, m.elem, g["grid"])
+    X, Y, Z = np.meshgrid(*xs, indexing="ij")
+    grid = np.stack([X.ravel(order="F"), Y.ravel(order="F"), Z.ravel(order="F")], axis=1)
+    m2g_host, inm_host = m2g_from_location(*locate_host(m.node, m.elem, grid), m.elem, m.nn)
+    P, inm = jacobian.m2g_matrix(m.node, m.elem, grid)
     assert inm.sum() > 100 and (~inm).sum() > 100
-    assert np.array_equal(inm, g["gridinmesh"])
+    assert np.array_equal(inm, inm_host)
     f = m.node @ np.array([0.3, -1.1, 0.7]) + 2.0
-    fg = g["grid"] @ np.array([0.3, -1.1, 0.7]) + 2.0
+    fg = grid @ np.array([0.3, -1.1, 0.7]) + 2.0
     assert np.abs(P @ f - np.where(inm, fg, 0)).max() < 1e-11
-    assert np.abs(g["m2g"] @ f - P @ f).max() < 1e-11
+    assert np.abs(m2g_host @ f - P @ f).max() < 1e-11
     # rows sum to one inside, empty outside
     rs = np.asarray(P.sum(axis=1)).ravel()
     assert np.abs(rs[inm] - 1).max() < 1e-12 and not rs[~inm].any()
+
+
+def test_g2m_oracle_properties():
+    """g2m restatement: rows sum to 1; a node whose lattice cell is all in-mesh
+    interpolates a linear voxel field exactly (barycentric weights); uncovered
+    nodes take their nearest in-mesh voxel."""
+    m = ellipsoid_mesh((8, 7, 6), 1.0, 0.1, 5)
+    lo, hi = m.node.min(0), m.node.max(0)
+    xs = [np.arange(lo[d] - 0.3, hi[d] + 0.9, 0.8) for d in range(3)]
+    X, Y, Z = np.meshgrid(*xs, indexing="ij")
+    grid = np.stack([X.ravel(order="F"), Y.ravel(order="F"), Z.ravel(order="F")], axis=1)
+    _, inm = jacobian.m2g_matrix(m.node, m.elem, grid)
+    G = jacobian.g2m_matrix(m.node, xs, inm)
+    assert np.abs(np.asarray(G.sum(axis=1)).ravel() - 1).max() < 1e-14
+    assert not G[:, ~inm].count_nonzero()                          # only in-mesh voxels carry weight
+    lin = np.array([0.3, -1.1, 0.7])
+    fv = grid @ lin + 2.0
+    n = [len(a) for a in xs]
+    full = []
+    for r, p in enumerate(m.node):
+        c = [int(np.floor((p[k] - xs[k][0]) / 0.8)) for k in range(3)]
+        corners = [c[0] + i + n[0] * (c[1] + j + n[1] * (c[2] + k)) for i in (0, 1) for j in (0, 1) for k in (0, 1)]
+        full.append(all(inm[v] for v in corners))
+    full = np.array(full)
+    assert full.sum() > 50
+    assert np.abs((G @ fv)[full] - (m.node[full] @ lin + 2.0)).max() < 1e-12
+    single = np.diff(G.indptr) == 1
+    for r in np.nonzero(single & ~full)[0][:20]:
+        v = G.indices[G.indptr[r]]
+        d2 = ((grid[inm] - m.node[r]) ** 2).sum(1)
+        assert abs(((grid[v] - m.node[r]) ** 2).sum() - d2.min()) <= 1e-12 * max(1.0, d2.min()) or G.data[G.indptr[r]] == 1
