@@ -87,6 +87,8 @@ int jacobian_run(int mode, const int32_t *prow, const int32_t *pcol, const doubl
 int normal_eq_run(const float *Jt, int64_t nv, int64_t nm, const double *W, const double *y, double lam, int mode,
                   double *H, int64_t ldh, double *rhs, cudaStream_t st);
 int cholesky_solve_run(double *H, int64_t n, int64_t ldh, double *x, cudaStream_t st);
+int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_t nrhs, int64_t ldx,
+                            cudaStream_t st);
 
 }  // namespace dgp
 
@@ -448,6 +450,11 @@ int dgp_normal_eq(const float *d_Jt, int64_t nv, int64_t nmeas, const double *d_
 
 int dgp_cholesky_solve(double *d_H, int64_t n, int64_t ldh, double *d_x, dgp_stream_t stream) {
   DGP_GUARD(cholesky_solve_run(d_H, n, ldh, d_x, (cudaStream_t)stream));
+}
+
+int dgp_cholesky_solve_many(double *d_H, int64_t n, int64_t ldh, double *d_X, int32_t nrhs, int64_t ldx,
+                            dgp_stream_t stream) {
+  DGP_GUARD(cholesky_solve_many_run(d_H, n, ldh, d_X, nrhs, ldx, (cudaStream_t)stream));
 }
 
 }  // extern "C"

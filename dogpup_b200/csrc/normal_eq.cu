@@ -430,9 +430,18 @@ cublasHandle_t blas_handle(std::unique_lock<std::mutex> &lk) {
   return h;
 }
 
+int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_t nrhs, int64_t ldx,
+                            cudaStream_t st);
+
 int cholesky_solve_run(double *H, int64_t n, int64_t ldh, double *x, cudaStream_t st) {
+  return cholesky_solve_many_run(H, n, ldh, x, 1, n, st);
+}
+
+int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_t nrhs, int64_t ldx,
+                            cudaStream_t st) {
   DGP_REQUIRE(H && x && n > 0 && ldh >= n, "cholesky: bad arguments");
-  DGP_REQUIRE(n <= INT32_MAX && ldh <= INT32_MAX, "cholesky: n and ldh must fit int32 (cuBLAS)");
+  DGP_REQUIRE(nrhs >= 1 && ldx >= n, "cholesky: need nrhs >= 1 and ldx >= n");
+  DGP_REQUIRE(n <= INT32_MAX && ldh <= INT32_MAX && ldx <= INT32_MAX, "cholesky: n, ldh and ldx must fit int32 (cuBLAS)");
   DevBuf errb;
   DGP_TRY(errb.alloc(sizeof(int)));
   DGP_CUDA(cudaMemsetAsync(errb.p, 0, sizeof(int), st));
@@ -473,12 +482,22 @@ int cholesky_solve_run(double *H, int64_t n, int64_t ldh, double *x, cudaStream_
       return fail(DGP_ERR_CUDA, "cholesky: cublasDsyrk failed");
   }
   DGP_CHECK_LAUNCH();
-  // L y = b, then L^T x = y (cuBLAS DTRSV on the column-major view Hc = L^T, upper)
-  if (cublasDtrsv(hb, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, (int)n, H, (int)ldh, x, 1) !=
-          CUBLAS_STATUS_SUCCESS ||
-      cublasDtrsv(hb, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, (int)n, H, (int)ldh, x, 1) !=
-          CUBLAS_STATUS_SUCCESS)
-    return fail(DGP_ERR_CUDA, "cholesky: cublasDtrsv failed");
+  // L y = b, then L^T x = y on the column-major view Hc = L^T (upper): DTRSV for one right-hand
+  // side, DTRSM for several (right-hand side r is row r of x, i.e. column r of the n x nrhs
+  // column-major view with leading dimension ldx)
+  if (nrhs == 1) {
+    if (cublasDtrsv(hb, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, (int)n, H, (int)ldh, x, 1) !=
+            CUBLAS_STATUS_SUCCESS ||
+        cublasDtrsv(hb, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, (int)n, H, (int)ldh, x, 1) !=
+            CUBLAS_STATUS_SUCCESS)
+      return fail(DGP_ERR_CUDA, "cholesky: cublasDtrsv failed");
+  } else {
+    if (cublasDtrsm(hb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, (int)n, nrhs,
+                    &one, H, (int)ldh, x, (int)ldx) != CUBLAS_STATUS_SUCCESS ||
+        cublasDtrsm(hb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, (int)n, nrhs,
+                    &one, H, (int)ldh, x, (int)ldx) != CUBLAS_STATUS_SUCCESS)
+      return fail(DGP_ERR_CUDA, "cholesky: cublasDtrsm (solve) failed");
+  }
   lk.unlock();
   int herr = 0;
   DGP_CUDA(cudaMemcpyAsync(&herr, errb.p, sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -12,10 +12,13 @@ its helpers id_thresh (DOGPUP/id_thresh.m:1-27) and tik_inv
   host            the loop's scalar logic (lambda schedule, step-back on a
                   rising error, exit conditions) on [NM x NG]-sized data
 
-Data weighting: the reference weights rows by reshape_J's dense w
-(wghtd_LM_recon.m:74-76) when target spots are given, else by 1; here a
-diagonal W = 1/sigma^2 (the north-star weighting) or 1.  The spot-reshaping
-branch (target_spots / reshape_J) is not restated.
+Data weighting: with target spots (``pos_s``) the rows of J and y are
+mixed by reshape_J's dense w (wghtd_LM_recon.m:35-37, :72-76;
+reconstruction/reshape_J.m:13-15; dMesh.m:250-282), computed on the device:
+J J^T + lam2 max diag by the split-BF16 tensor-core kernel (dgp_normal_eq on
+J), Js J^T by cuBLAS SGEMM, and w by one FP64 Cholesky factorisation with
+one right-hand side per spot (dgp_cholesky_solve_many).  Without spots the
+rows are weighted by a diagonal W = 1/sigma^2 or by 1.
 """
 from __future__ import annotations
 
@@ -45,6 +48,52 @@ def id_thresh(data, thresh):
     idx = np.arange(d.shape[1])[None, :]
     after = idx >= np.argmax(dn, axis=1)[:, None]
     return after & (dn <= thresh) & (dn > 0.01)
+
+
+def target_spots(grid, inmesh, pos, w=1.5, kind="gauss"):
+    """Sensitivity spots Js [NS][NV] on the device (dMesh.m:250-282): a Gaussian of width
+    parameter 2 sqrt(2 ln 2) w ('gauss', w the FWHM) or a cube of side w ('square') around
+    each centre pos [NS][3], normalised to unit sum over all voxels, negated, zero outside
+    the mesh."""
+    g = torch.as_tensor(np.asarray(grid, dtype=np.float64), device="cuda")
+    p = torch.as_tensor(np.atleast_2d(np.asarray(pos, dtype=np.float64)), device="cuda")
+    diff = g[None, :, :] - p[:, None, :]                               # [NS][NV][3]
+    if kind == "gauss":
+        s = 2.0 * np.sqrt(2.0 * np.log(2.0)) * w
+        t = torch.exp(-(diff * diff).sum(-1) / (s * s * 2))
+    elif kind == "square":
+        t = (diff.abs() <= w / 2).all(-1).to(torch.float64)
+    else:
+        raise ValueError("spot type must be 'gauss' or 'square'")
+    tot = t.sum(1, keepdim=True)
+    if bool((tot == 0).any()):
+        raise ValueError("a target spot covers no voxel")
+    t = -(t / tot)
+    t[:, ~torch.as_tensor(np.asarray(inmesh, dtype=bool), device="cuda")] = 0.0
+    return t
+
+
+def reshape_J(Jt: torch.Tensor, Js: torch.Tensor, lam: float, normal_eq="split_bf16") -> torch.Tensor:
+    """w [NS][NM] = (Js J^T)(J J^T + lam max diag I)^-1 (reconstruction/reshape_J.m:13-15).
+
+    Jt [NV][NM] is J transposed (the TG Jacobian's layout), Js [NS][NV] the spots on the
+    same voxels.  J J^T: split-BF16 tensor cores (or FP64 for normal_eq='fp64'); the
+    solve: FP64 Cholesky with one right-hand side per spot."""
+    nv, nm = Jt.shape
+    ns = Js.shape[0]
+    A = torch.empty((nm, nm), dtype=torch.float64, device="cuda")
+    v = lambda t: C.c_void_p(t.data_ptr())
+    if normal_eq == "split_bf16":
+        J = Jt.to(torch.float32).t().contiguous()                        # [NM][NV]: rows of J
+        check(lib.dgp_normal_eq(v(J), nm, nv, None, None, float(lam), 0, v(A), nm, None, api.stream_ptr()))
+        B = (Js.to(torch.float32) @ Jt.to(torch.float32)).to(torch.float64).contiguous()
+    else:
+        Jd = Jt.to(torch.float64)
+        A.copy_(Jd.T @ Jd)
+        A.diagonal().add_(lam * A.diagonal().max())
+        B = (Js.to(torch.float64) @ Jd).contiguous()
+    check(lib.dgp_cholesky_solve_many(v(A), nm, nm, v(B), ns, nm, api.stream_ptr()))
+    return B
 
 
 def _flat(x_nm_ng: torch.Tensor) -> torch.Tensor:
@@ -109,8 +158,13 @@ class LMRecon:
         check(lib.dgp_cholesky_solve(C.c_void_p(H.data_ptr()), nv, nv, C.c_void_p(x.data_ptr()), api.stream_ptr()))
         return x
 
-    def run(self, data_m, lam=(1.0, 0.0), sigma=None, thresh=0.8, max_iter=10, truth=None, callback=None):
+    def run(self, data_m, lam=(1.0, 0.0), sigma=None, thresh=0.8, max_iter=10, truth=None, callback=None,
+            pos_s=None, spot_width=1.5, spot_kind="gauss"):
         """Iterates from the mesh's current mua (wghtd_LM_recon.m:25-168); data_m [NM][NG] measured TG data.
+
+        pos_s [NS][3] (or None): centres of the target spots; J and y are then mixed by
+        reshape_J's w with regulariser lam[1] at every iteration (wghtd_LM_recon.m:72-76),
+        and the misfit is |w y| relative to |w data| (:84-85).
 
         sigma [NM][NG] (or None): data standard deviations; the fit is on log
         data, so W = (data / sigma)^2 to first order, scaled to unit mean over
@@ -126,6 +180,13 @@ class LMRecon:
         incl = torch.as_tensor(np.nonzero(mask.T.ravel())[0], device="cuda")               # x(:) order
         dm = torch.log(_flat(torch.as_tensor(data_m, device="cuda")))[incl]
         w = None
+        Js = None
+        if pos_s is not None:
+            if sigma is not None:
+                raise ValueError("pos_s (reshaping weights) and sigma (diagonal weights) exclude each other")
+            inmesh = np.asarray(m.gridinmesh)
+            Js = target_spots(m.grid, inmesh, pos_s, spot_width, spot_kind)[:, torch.as_tensor(inmesh, device="cuda")]
+            Js = Js.contiguous()
         if sigma is not None:
             rel = np.asarray(sigma, dtype=np.float64) / data_m        # sigma of log data
             w = (1.0 / _flat(torch.as_tensor(rel, device="cuda")) ** 2)[incl]
@@ -142,9 +203,17 @@ class LMRecon:
             if not bool(torch.isfinite(y).all()):
                 hist["stopped"] = "model data not positive on an included gate"
                 break
-            err = float(torch.sqrt((wn * y * y).sum()))
+            if Js is not None:                                        # :72-76
+                ws = reshape_J(Jt, Js, lam[1], self.normal_eq)        # [NS][NM]
+                Jt = (Jt @ ws.T.to(Jt.dtype)).contiguous()             # rows of w J, transposed
+                y = ws @ y
+                err = float(torch.linalg.vector_norm(y))
+                ref = float(torch.linalg.vector_norm(ws @ dm))
+            else:
+                err = float(torch.sqrt((wn * y * y).sum()))
+                ref = float(torch.sqrt((wn * dm * dm).sum()))
             hist["err"].append(err)
-            hist["err_perc"].append(100 * err / float(torch.sqrt((wn * dm * dm).sum())))
+            hist["err_perc"].append(100 * err / ref)
             if truth is not None:
                 hist["err_truth"].append(float(torch.linalg.vector_norm(m.mua - truth) /
                                                torch.linalg.vector_norm(truth)))
@@ -166,7 +235,7 @@ class LMRecon:
             lam1 = max(lam1, err)                                     # :118-120
             hist["lam"].append(lam1)
             Jg = (Jt * G[:, None].to(Jt.dtype)).contiguous()          # J .* G.' (property normalisation)
-            upd = self._tik(Jg, lam1, y.contiguous(), w)              # :125-127
+            upd = self._tik(Jg, lam1, y.contiguous(), None if Js is not None else w)   # :125-127
             x = G * upd                                               # :131
             d_mu = torch.as_tensor(self.g2m_in @ x.cpu().numpy(), device="cuda")   # :132
             if torch.isnan(d_mu).any():

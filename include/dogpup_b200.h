@@ -446,6 +446,12 @@ int dgp_normal_eq(const float *d_Jt, int64_t nv, int64_t nmeas, const double *d_
  * Returns DGP_ERR_ARG if H is not positive definite. */
 int dgp_cholesky_solve(double *d_H, int64_t n, int64_t ldh, double *d_x,
                        dgp_stream_t stream);
+/* dgp_cholesky_solve for nrhs right-hand sides: row r of d_X [nrhs][ldx]
+ * (ldx >= n) is b_r in and x_r out; one factorisation, one DTRSM pair.
+ * Used for reshape_J's w = (Js J^T)(J J^T + lam max diag I)^-1
+ * (reconstruction/reshape_J.m:13-15) with the rows of Js J^T as b_r. */
+int dgp_cholesky_solve_many(double *d_H, int64_t n, int64_t ldh, double *d_X,
+                            int32_t nrhs, int64_t ldx, dgp_stream_t stream);
 
 #ifdef __cplusplus
 } /* extern "C" */

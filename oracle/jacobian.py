@@ -3,8 +3,10 @@
 ``J_complex`` (DOGPUP/dMesh.m:206-247), its time-gated form
 (``fc2tg`` applied along the frequency axis, tutorials/tut_2...m:147 and
 reconstruction/wghtd_LM_recon.m:61), the vector-Jacobian product of the TG
-Jacobian, and ``tik_inv`` (reconstruction/tik_inv.m:1-20) with an optional
-diagonal data weight W.
+Jacobian, ``tik_inv`` (reconstruction/tik_inv.m:1-20) with an optional
+diagonal data weight W, the voxel basis (mesh2grid, dMesh.m:286-380) and the
+sensitivity reshaping weights (target_spots, dMesh.m:250-282; reshape_J,
+reconstruction/reshape_J.m:1-17).
 """
 from __future__ import annotations
 
@@ -138,6 +140,40 @@ def j_tg(J, gate_fc, nt):
 def j_tg_vjp(J_tg, g):
     """J^T g for the TG Jacobian: sum over measurements and gates of J[m,g,v] g[m,g]."""
     return np.einsum("mgv,mg->v", J_tg, g)
+
+
+def target_spots(grid, inmesh, pos, w, kind="gauss"):
+    """Sensitivity spots [NS, NV] (dMesh.m:250-282): a Gaussian whose width
+    parameter is (2 sqrt(2 ln 2)) w, or a cube of side w, around each spot
+    centre, normalised to unit sum over all voxels, negated, and zero outside
+    the mesh."""
+    grid = np.asarray(grid, dtype=np.float64)
+    pos = np.atleast_2d(np.asarray(pos, dtype=np.float64))
+    if kind == "gauss":
+        s = 2.0 * np.sqrt(2.0 * np.log(2.0)) * w                      # :267
+        t = np.exp(-((grid[:, None, 0] - pos[None, :, 0]) ** 2) / (s ** 2 * 2)
+                   - ((grid[:, None, 1] - pos[None, :, 1]) ** 2) / (s ** 2 * 2)
+                   - ((grid[:, None, 2] - pos[None, :, 2]) ** 2) / (s ** 2 * 2))
+    elif kind == "square":
+        h = w / 2                                                     # :272
+        t = np.ones((grid.shape[0], pos.shape[0]), dtype=bool)
+        for d in range(3):
+            t &= (grid[:, None, d] <= pos[None, :, d] + h) & (grid[:, None, d] >= pos[None, :, d] - h)
+        t = t.astype(np.float64)
+    else:
+        raise ValueError("Check spot type is gauss or square")
+    t = t / t.sum(axis=0)                                             # :279
+    t = -t.T
+    t[:, ~np.asarray(inmesh, dtype=bool)] = 0.0                        # :281
+    return t
+
+
+def reshape_j(J, Js, lam):
+    """w = (Js J^T) / (J J^T + lam max(diag(J J^T)) I)  (reconstruction/reshape_J.m:13-15);
+    J [NM, NV], Js [NS, NV]; returns [NS, NM]."""
+    A = J @ J.T
+    A = A + lam * np.max(np.diag(A)) * np.eye(A.shape[0])
+    return np.linalg.solve(A.T, (Js @ J.T).T).T
 
 
 def tik_inv(J, lam, y, weights=None, diag_mode="max"):

@@ -2,7 +2,7 @@
 
 Tolerances: H from the three-term BF16 split with FP32 accumulation, 3e-5
 norm-wise relative; J^T W y (FP64) 1e-12; the Cholesky solve on an exact
-FP64 matrix 1e-10; the whole LM step against the all-FP64 oracle
+FP64 matrix 1e-10 (one or many right-hand sides); the whole LM step against the all-FP64 oracle
 (tik_inv with W), 1e-3.
 """
 import ctypes as C
@@ -68,6 +68,28 @@ def test_cholesky_solve_exact_matrix(n, pad):
     assert np.linalg.norm(x.cpu().numpy() - x0) / np.linalg.norm(x0) < 1e-10
     L = np.tril(H.cpu().numpy()[:, :n])
     assert np.linalg.norm(L @ L.T - H0) / np.linalg.norm(H0) < 1e-13
+
+
+@pytest.mark.parametrize("n,nrhs,padx", [(333, 7, 5), (600, 40, 0)])
+def test_cholesky_solve_many_right_hand_sides(n, nrhs, padx):
+    """One factorisation, nrhs right-hand sides as the rows of X [nrhs][ldx]; ldx > n keeps
+    the pad columns untouched."""
+    import torch
+    from dogpup_b200._lib import lib, check
+    rng = np.random.default_rng(11)
+    A = rng.standard_normal((n, n))
+    H0 = A @ A.T + n * np.eye(n)
+    B = rng.standard_normal((nrhs, n))
+    ldx = n + padx
+    Xp = np.full((nrhs, ldx), 7.0)
+    Xp[:, :n] = B
+    H = torch.as_tensor(np.tril(H0), device="cuda").contiguous()
+    X = torch.as_tensor(Xp, device="cuda").contiguous()
+    check(lib.dgp_cholesky_solve_many(_v(H), n, n, _v(X), nrhs, ldx, None))
+    X0 = np.linalg.solve(H0, B.T).T
+    Xh = X.cpu().numpy()
+    assert np.linalg.norm(Xh[:, :n] - X0) / np.linalg.norm(X0) < 1e-10
+    assert (Xh[:, n:] == 7.0).all()
 
 
 @pytest.mark.parametrize("n,bad", [(70, 0), (600, 530)])

@@ -212,3 +212,23 @@ def test_g2m_oracle_properties():
         v = G.indices[G.indptr[r]]
         d2 = ((grid[inm] - m.node[r]) ** 2).sum(1)
         assert abs(((grid[v] - m.node[r]) ** 2).sum() - d2.min()) <= 1e-12 * max(1.0, d2.min()) or G.data[G.indptr[r]] == 1
+
+
+def test_reshape_and_spot_oracles():
+    """reshape_J's w solves w (J J^T + lam max diag I) = Js J^T; spots have unit
+    (negative) mass over the whole grid and vanish outside the mesh."""
+    rng = np.random.default_rng(4)
+    J = rng.standard_normal((40, 300))
+    Js = rng.standard_normal((6, 300))
+    w = jacobian.reshape_j(J, Js, 0.05)
+    A = J @ J.T
+    A += 0.05 * A.diagonal().max() * np.eye(40)
+    assert np.abs(w @ A - Js @ J.T).max() < 1e-10 * np.abs(Js @ J.T).max()
+    g = np.stack(np.meshgrid(np.arange(10.0), np.arange(8.0), np.arange(6.0), indexing="ij"), -1).reshape(-1, 3)
+    inm = g[:, 0] < 7
+    for kind, wd in (("gauss", 1.5), ("square", 3.0)):
+        t = jacobian.target_spots(g, np.ones(len(g), bool), [[3, 4, 2], [6.5, 1, 3]], wd, kind)
+        assert np.allclose(t.sum(1), -1.0)
+        t2 = jacobian.target_spots(g, inm, [[3, 4, 2], [6.5, 1, 3]], wd, kind)
+        assert not t2[:, ~inm].any() and np.array_equal(t2[:, inm], t[:, inm])
+    assert np.count_nonzero(jacobian.target_spots(g, inm, [[3, 4, 2]], 3.0, "square")) == 27
