@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--workload", default="ellipsoid", choices=["ellipsoid", "medium", "cylinder", "small"])
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--inner-tol", type=float, default=3e-5)
+    ap.add_argument("--inner", choices=["cocg", "bicgstab"], default="cocg",
+                    help="complex-FP32 inner solver of the mixed solve")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-secondary", action="store_true", help="skip the TG Jacobian / LM / plain-FP64 timings")
@@ -491,9 +493,11 @@ def run_ours(a, rank, world, local_rank):
     st = torch.cuda.current_stream()
     res = {}
 
+    prec = "mixed" if a.inner == "cocg" else "mixed_bicgstab"
+
     def step():
         mesh.update_properties()                         # K, M re-assembly + FSAI refactor
-        phi, data, rep = mesh.flu_solve(precision="mixed", tol=a.tol, inner_tol=a.inner_tol, return_report=True)
+        phi, data, rep = mesh.flu_solve(precision=prec, tol=a.tol, inner_tol=a.inner_tol, return_report=True)
         return rep
 
     log(f"[rank {rank}] setup done: {mesh.nn} nodes, nnz {mesh.fem.nnz}, solver {solver.memory() / 1e9:.1f} GB")
@@ -550,7 +554,7 @@ def run_ours(a, rank, world, local_rank):
             mesh.mua = mua_h.to("cuda", non_blocking=True)
             mesh.musp = musp_h.to("cuda", non_blocking=True)
             mesh.update_properties()
-            phi, data = mesh.flu_solve(precision="mixed", tol=a.tol, inner_tol=a.inner_tol)
+            phi, data = mesh.flu_solve(precision=prec, tol=a.tol, inner_tol=a.inner_tol)
             data_h.copy_(data, non_blocking=True)
 
         step_e2e()
@@ -572,7 +576,8 @@ def run_ours(a, rank, world, local_rank):
                "ms_per_step": ems / a.steps}
 
     # ---- roofline: the dominant sweep kernel, CUDA-event timed on the solver's stream
-    per_iter = {0: 2, 1: 5, 2: 1, 3: 1}  # per BiCGSTAB iteration: A SpMM x2, G SpMM x5, x/r/p, s
+    # sweeps per inner iteration -- BiCGSTAB: A SpMM x2, G SpMM x5, x/r/p, s; COCG: A x1, G x2
+    per_iter = {0: 2, 1: 5, 2: 1, 3: 1} if a.inner == "bicgstab" else {0: 1, 1: 2}
     names = {0: "k_spmm_A<float> (K + i w M SpMM)", 1: "k_spmm_G<float> (FSAI apply)",
              2: "k_update_xrp<float>", 3: "k_update_s<float>"}
     prof = {q: solver.profile_kernel(q, 5) for q in per_iter}
@@ -651,6 +656,7 @@ def main():
             "data": "synthetic",
             "config": {"workload": w["name"], "nodes": mesh.nn, "tets": int(w["mesh"].ne), "nnz": mesh.fem.nnz,
                        "sources": len(w["src"]), "harmonics": w["nf"], "tol": a.tol, "inner_tol": a.inner_tol,
+                       "inner_solver": a.inner,
                        "iterations": rep.iterations, "refinements": rep.refinements,
                        "max_rel_residual": rep.max_rel_residual, "l2": "inputs larger than L2 (vectors ~GB)",
                        "parallelism": f"replicas x{world}", "node_order": a.order, "autotuned": r["tuned"]},

@@ -27,7 +27,7 @@ class SolveReport(C.Structure):
                 ("d_status", P)]
 
 
-PREC_FP64, PREC_MIXED = 0, 1
+PREC_FP64, PREC_MIXED, PREC_MIXED_BICGSTAB = 0, 1, 2
 STOP_MAX_ALL, STOP_PER_COLUMN = 0, 1
 OK, ERR_NOT_CONVERGED = 0, 5
 COL_STATUS = {0: "converged", 1: "maxit", 2: "breakdown_rho", 3: "breakdown_omega", 4: "nonfinite", 5: "zero_rhs"}

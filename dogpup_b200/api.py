@@ -178,7 +178,7 @@ def make_opts(**kw) -> _lib.SolveOpts:
         if v is None:
             continue
         if k == "precision" and isinstance(v, str):
-            v = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}[v]
+            v = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED, "mixed_bicgstab": _lib.PREC_MIXED_BICGSTAB}[v]
         if k == "stop_rule" and isinstance(v, str):
             v = {"max_all": _lib.STOP_MAX_ALL, "per_column": _lib.STOP_PER_COLUMN}[v]
         setattr(o, k, v)

@@ -91,8 +91,8 @@ struct SolverPlan {
   DevBuf ctl;                    // control block
   DevBuf status;                 // per-column status
   void *h_ctl = nullptr;         // pinned mirror of the control block
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};
-  int graph_iters[2] = {0, 0};
+  cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};  // FP64 BiCGSTAB, FP32 BiCGSTAB, FP32 COCG
+  int graph_iters[3] = {0, 0, 0};
   // SpMM launch shape of the complex-FP32 sweeps chosen by solver_autotune (0 = built-in default)
   int32_t tune_vec = 0, tune_rows = 0;
   // tiled SpMM (halo rows staged in shared memory) for A, G and G^T; tiled = 1 selects it

@@ -1,7 +1,7 @@
 // dgp_forward: standalone C++ driver of the forward hot path through the C ABI
 // (include/dogpup_b200.h), no Python or MATLAB involved.
 //
-//   dgp_forward CASE OUT [--precision fp64|mixed] [--tol T] [--maxit N] [--repeat R]
+//   dgp_forward CASE OUT [--precision fp64|mixed|mixed_bicgstab] [--tol T] [--maxit N] [--repeat R]
 //
 // Reads a case file (mesh, nodal mua / musp, optode barycentrics, links,
 // source spectrum; format below), then on the GPU: builds the FEM plan,
@@ -106,7 +106,7 @@ float elapsed(cudaEvent_t a, cudaEvent_t b) {
 
 int main(int argc, char **argv) {
   if (argc < 3) {
-    fprintf(stderr, "usage: %s CASE OUT [--precision fp64|mixed] [--tol T] [--maxit N] [--repeat R]\n", argv[0]);
+    fprintf(stderr, "usage: %s CASE OUT [--precision fp64|mixed|mixed_bicgstab] [--tol T] [--maxit N] [--repeat R]\n", argv[0]);
     return 2;
   }
   dgp_solve_opts o;
@@ -114,7 +114,8 @@ int main(int argc, char **argv) {
   int repeat = 0;
   for (int i = 3; i + 1 < argc; i += 2) {
     const std::string k = argv[i], v = argv[i + 1];
-    if (k == "--precision") o.precision = v == "mixed" ? DGP_PREC_MIXED : DGP_PREC_FP64;
+    if (k == "--precision")
+      o.precision = v == "mixed" ? DGP_PREC_MIXED : v == "mixed_bicgstab" ? DGP_PREC_MIXED_BICGSTAB : DGP_PREC_FP64;
     else if (k == "--tol") o.tol = atof(v.c_str());
     else if (k == "--maxit") o.maxit = atoi(v.c_str());
     else if (k == "--repeat") repeat = atoi(v.c_str());
@@ -186,7 +187,8 @@ int main(int argc, char **argv) {
          "\"iterations\": %d, \"refinements\": %d, \"max_rel_residual\": %.3e, \"not_converged\": %d, "
          "\"setup_ms\": %.3f, \"solve_ms\": %.3f, \"step_ms\": %.3f, \"solves_per_s\": %.1f}\n",
          (long long)c.nn, (long long)nnz, (long long)c.ns, (long long)c.nf,
-         o.precision == DGP_PREC_MIXED ? "mixed" : "fp64", rep.iterations, rep.refinements, rep.max_rel_residual,
+         o.precision == DGP_PREC_MIXED ? "mixed" : o.precision == DGP_PREC_MIXED_BICGSTAB ? "mixed_bicgstab" : "fp64",
+         rep.iterations, rep.refinements, rep.max_rel_residual,
          rep.n_not_converged, setup_ms, solve_ms, step_ms, c.ns * c.nf / (solve_ms * 1e-3));
   dgp_solver_destroy(S);
   dgp_fem_destroy(fem);

@@ -113,9 +113,10 @@ void mexFunction(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
       const std::string s(buf);
       if (s == "fp64") o.precision = DGP_PREC_FP64;
       else if (s == "mixed") o.precision = DGP_PREC_MIXED;
-      else dgp_mex::fail(GW, "precision", "precision must be 'fp64' or 'mixed'");
+      else if (s == "mixed_bicgstab") o.precision = DGP_PREC_MIXED_BICGSTAB;
+      else dgp_mex::fail(GW, "precision", "precision must be 'fp64', 'mixed' or 'mixed_bicgstab'");
     } else {
-      o.precision = (int32_t)dgp_mex::scalar(GW, "precision must be 'fp64' or 'mixed'", p);
+      o.precision = (int32_t)dgp_mex::scalar(GW, "precision must be 'fp64', 'mixed' or 'mixed_bicgstab'", p);
     }
   }
   dgp_mex::Handles H;

@@ -169,13 +169,19 @@ int dgp_fem_adjoint_grad(dgp_fem_t fem, const double *d_mua,
  *  Replaces fluGPU + gpuBicstab_FSAIP + FSAIP_gen, dMesh.m:1238-1385,
  *  as one call instead of a MATLAB loop over mex mat-vecs.
  * ====================================================================== */
-enum { DGP_PREC_FP64 = 0, DGP_PREC_MIXED = 1 };
+/* FP64: the reference's BiCGSTAB in FP64.  MIXED: complex-FP32 COCG
+ * (conjugate-orthogonal CG: A_k and the FSAI preconditioner G^T G are
+ * complex symmetric; one A and one G^T G application per iteration) inside
+ * FP64 iterative refinement.  MIXED_BICGSTAB: as MIXED with complex-FP32
+ * BiCGSTAB (the reference's recurrences) as the inner solver. */
+enum { DGP_PREC_FP64 = 0, DGP_PREC_MIXED = 1, DGP_PREC_MIXED_BICGSTAB = 2 };
 enum { DGP_STOP_MAX_ALL = 0, DGP_STOP_PER_COLUMN = 1 };
 
 typedef struct dgp_solve_opts {
   double tol;          /* relative residual target (reference: 1e-12)      */
-  int32_t maxit;       /* BiCGSTAB iterations (reference: 1000)            */
-  int32_t precision;   /* DGP_PREC_FP64 | DGP_PREC_MIXED                   */
+  int32_t maxit;       /* iterations (reference: 1000; mixed: summed over
+                        * the inner solves)                                */
+  int32_t precision;   /* DGP_PREC_FP64 | _MIXED | _MIXED_BICGSTAB         */
   double inner_tol;    /* mixed: complex-FP32 inner target per refinement  */
   int32_t max_refine;  /* mixed: maximum FP64 refinement steps             */
   int32_t fsai_cap;    /* FSAI pattern cap per row (reference: 30)         */
@@ -192,7 +198,7 @@ typedef struct dgp_solve_opts {
 void dgp_solve_opts_default(dgp_solve_opts *opts);
 
 typedef struct dgp_solve_report {
-  int32_t iterations;       /* BiCGSTAB iterations (summed over refinement) */
+  int32_t iterations;       /* inner iterations (summed over refinement)    */
   int32_t refinements;      /* FP64 refinement steps (mixed)                */
   double max_rel_residual;  /* max over columns of ||b-Ax||/||b|| (FP64)    */
   int32_t n_not_converged;  /* columns whose status is not CONVERGED        */

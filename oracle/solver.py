@@ -239,6 +239,36 @@ def bicgstab_fsai(pc: FsaiPrecond, Q, tol=1e-12, maxit=1000, history=None):
     return x, it
 
 
+def cocg_fsai(pc: FsaiPrecond, Q, tol=1e-12, maxit=4000):
+    """Preconditioned COCG (conjugate-orthogonal CG) on the same systems and
+    preconditioner as ``bicgstab_fsai``: A_k and M = G^T G are complex
+    symmetric, so CG with bilinear dots applies.  Restates the library's
+    mixed-precision inner solver (not a reference algorithm): per column
+    alpha = (r.z)/(p.Ap), x += alpha p, r -= alpha Ap, z = M r,
+    beta = (r.z)'/(r.z), p = z + beta p; stop when the largest relative
+    residual is below tol.  Returns (x, iterations)."""
+    x = np.zeros_like(Q)
+    r = Q.copy()
+    with np.errstate(invalid="ignore", divide="ignore"):
+        e0 = np.sqrt(_colsum(np.abs(r) ** 2))
+        z = pc.GTm(pc.Gm(r))
+        p = z.copy()
+        rho = _colsum(r * z)
+        it = 0
+        for it in range(1, maxit + 1):
+            q = pc.A(p)
+            alpha = rho / _colsum(p * q)
+            x = x + alpha * p
+            r = r - alpha * q
+            if _maxerr(np.sqrt(_colsum(np.abs(r) ** 2)) / e0) < tol:
+                break
+            z = pc.GTm(pc.Gm(r))
+            rn = _colsum(r * z)
+            p = z + (rn / rho) * p
+            rho = rn
+    return x, it
+
+
 # ------------------------------------------------------- sources / detectors
 def source_vectors(elem, bary, fpsf, nn):
     """Q[:, s, k] = barycentric weights of optode s at its tet's nodes times

@@ -161,7 +161,10 @@ def test_solver_dense_rhs_and_status(small_case, gpu_case, torch):
     assert np.abs(X[:, :, 2].cpu().numpy()).max() == 0.0
 
 
-def test_solver_mixed_precision_accuracy(small_case, gpu_case, torch):
+@pytest.mark.parametrize("precision", ["mixed", "mixed_bicgstab"])
+def test_solver_mixed_precision_accuracy(small_case, gpu_case, torch, precision):
+    """Both complex-FP32 inner solvers (COCG, BiCGSTAB) refined in FP64 reach the
+    sparse-direct solution."""
     from dogpup_b200 import api
     from oracle import solver as osv
     K0, M0 = small_case["K"], small_case["M"]
@@ -171,7 +174,7 @@ def test_solver_mixed_precision_accuracy(small_case, gpu_case, torch):
     fpsf = np.exp(-0.3j * np.arange(nf))
     fem = gpu_case["fem"]
     S = api.Solver(fem.rowptr, fem.col, gpu_case["K"], gpu_case["M"], dfc, nf, ns)
-    opts = api.make_opts(tol=1e-10, precision="mixed", inner_tol=1e-4)
+    opts = api.make_opts(tol=1e-10, precision=precision, inner_tol=1e-4)
     X, rep = S.solve_sources(torch.as_tensor(nodes, device="cuda"), torch.as_tensor(w, device="cuda"),
                              torch.as_tensor(fpsf, device="cuda"), opts)
     Q = np.zeros((K0.shape[0], ns, nf), complex)
@@ -201,7 +204,7 @@ def test_solver_reports_maxit(small_case, gpu_case, torch):
     assert np.isfinite(X.cpu().numpy()).all()
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "mixed_bicgstab"])
 def test_solver_harmonic_subset(small_case, gpu_case, torch, precision):
     """A plan over harmonics [5, 0, 9] solves slot j at harmonic h_j: same as the full plan's columns."""
     from dogpup_b200 import api

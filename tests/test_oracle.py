@@ -92,6 +92,25 @@ def test_bicgstab_matches_direct(small_case):
     assert 5 < it < 200
 
 
+def test_cocg_matches_direct_and_bicgstab_iterations(small_case):
+    """COCG (the mixed solver's inner method) on the same systems reaches the direct
+    solution; per iteration it applies A and G^T G once (BiCGSTAB: twice), and needs
+    fewer than twice BiCGSTAB's iterations."""
+    K, M = small_case["K"], small_case["M"]
+    dfc = 2 * np.pi / 10e-9 / (2.99792458e11 / 1.4)
+    pc = solver.FsaiPrecond(K, M, dfc, 4)
+    rng = np.random.default_rng(0)
+    Q = np.zeros((K.shape[0], 3, 4), complex)
+    for s in range(3):
+        idx = rng.choice(K.shape[0], 4, replace=False)
+        Q[idx, s, :] = rng.random(4)[:, None] * np.exp(0.3j * np.arange(4))[None]
+    x, it = solver.cocg_fsai(pc, Q, 1e-12)
+    xd = solver.direct_solve(K, M, dfc, Q)
+    assert np.linalg.norm(x - xd) / np.linalg.norm(xd) < 1e-9
+    _, itb = solver.bicgstab_fsai(pc, Q, 1e-12, 1000)
+    assert it < 2 * itb
+
+
 def test_transform_round_trip_and_gates():
     t = np.arange(0, 141) * 50e-12
     T = t[-1]
