@@ -527,12 +527,16 @@ def run_ours(a, rank, world, local_rank):
         clk.mark()
     n_launch0 = _dlib.dgp_kernel_launches()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
     e0.record(st)
-    for _ in range(a.steps):
+    for q in range(a.steps):
         rep = step()
+        marks[q].record(st)
     e1.record(st)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
+    step_ms = [e0.elapsed_time(marks[0])] + [marks[q - 1].elapsed_time(marks[q]) for q in range(1, a.steps)]
+    log(f"[rank {rank}] timed steps (ms): {[round(x, 1) for x in step_ms]}")
     launches = _dlib.dgp_kernel_launches() - n_launch0
     clocks = clk.stop() if clk else None
     if world > 1:

@@ -77,6 +77,7 @@ struct Cols {
   int *active;      // 1 iterating, 2 converged at s this iteration, 0 frozen
   int *status;      // DGP_COL_*
   int *hact;        // [nf] 1 while any column of harmonic k iterates; sweeps skip the others (NULL: none skipped)
+  double *tolc;     // per-column relative target of the per-column stop rule
   int nsp;
 };
 
@@ -861,7 +862,7 @@ __global__ void __launch_bounds__(1024) k_stage_check_s(Cols c, Ctl *ctl) {
       continue;
     }
     c.err[j] = e;
-    if (stop_rule == DGP_STOP_PER_COLUMN && e < tol) {
+    if (stop_rule == DGP_STOP_PER_COLUMN && e < c.tolc[j]) {
       // column done at s: x = x + alpha h in this iteration's update, then frozen
       c.omega[j] = make_double2(0, 0);
       c.status[j] = DGP_COL_CONVERGED;
@@ -917,7 +918,7 @@ __global__ void __launch_bounds__(1024) k_stage_check_r(Cols c, Ctl *ctl) {
       continue;
     }
     c.err[j] = e;
-    if (ctl->stop_rule == DGP_STOP_PER_COLUMN && e < tol) {
+    if (ctl->stop_rule == DGP_STOP_PER_COLUMN && e < c.tolc[j]) {
       c.active[j] = 0;
       c.status[j] = DGP_COL_CONVERGED;
       continue;
@@ -1004,7 +1005,7 @@ __global__ void __launch_bounds__(1024) k_cocg_check(Cols c, Ctl *ctl) {
       continue;
     }
     c.err[j] = e;
-    if (stop_rule == DGP_STOP_PER_COLUMN && e < tol) {
+    if (stop_rule == DGP_STOP_PER_COLUMN && e < c.tolc[j]) {
       c.active[j] = 0;
       c.status[j] = DGP_COL_CONVERGED;
       continue;
@@ -1077,8 +1078,12 @@ __global__ void __launch_bounds__(BS) k_init(Layout L, typename CT<R>::C *__rest
   block_reduce<VEC, 2, E>(L, ln, part, cols.acc, cols.C, slot, smem);
 }
 
-// err0 = ||r0||, rho0 = r0.r0, activity from the column index and norm
-__global__ void __launch_bounds__(1024) k_stage_init(Cols c, Ctl *ctl, int nsp, int ns) {
+// err0 = ||r0||, rho0 = r0.r0, activity from the column index and norm.  Per-column targets:
+// ctl->tol, or -- inside FP64 refinement, outer_err[j] = ||b_j - A X_j|| / ||b_j|| -- the
+// larger of ctl->tol and the reduction the column still needs, 0.3 outer_tol / outer_err[j]
+// (the last inner solve stops once the FP64 target is within reach instead of at ctl->tol)
+__global__ void __launch_bounds__(1024) k_stage_init(Cols c, Ctl *ctl, int nsp, int ns,
+                                                     const double *outer_err = nullptr, double outer_tol = 0.0) {
   typedef cub::BlockReduce<int, 1024> BR;
   __shared__ typename BR::TempStorage tmp;
   int a = 0;
@@ -1090,6 +1095,7 @@ __global__ void __launch_bounds__(1024) k_stage_init(Cols c, Ctl *ctl, int nsp, 
     const int s = (int)(j % nsp);
     c.err0[j] = sqrt(nr);
     c.err[j] = 1.0;
+    c.tolc[j] = outer_err ? fmax(ctl->tol, 0.3 * outer_tol / outer_err[j]) : ctl->tol;
     c.rho0[j] = rho;
     c.alpha[j] = c.omega[j] = c.beta[j] = make_double2(0, 0);
     const bool act = s < ns && nr > 0.0 && isfinite(nr);
@@ -1486,6 +1492,7 @@ Work work_views(SolverPlan *S) {
   w.cols.err = (double *)b; b += sizeof(double) * C;
   w.bnorm = (double *)b; b += sizeof(double) * C;
   w.outer_err = (double *)b; b += sizeof(double) * C;
+  w.cols.tolc = (double *)b; b += sizeof(double) * C;
   w.cols.rho0 = (double2 *)b; b += sizeof(double2) * C;
   w.cols.alpha = (double2 *)b; b += sizeof(double2) * C;
   w.cols.omega = (double2 *)b; b += sizeof(double2) * C;
@@ -1499,7 +1506,7 @@ Work work_views(SolverPlan *S) {
   return w;
 }
 
-size_t scal_bytes(int64_t C) { return (sizeof(double) * 4 + sizeof(double2) * (4 + NACC) + 2 * sizeof(int)) * C + 256; }
+size_t scal_bytes(int64_t C) { return (sizeof(double) * 5 + sizeof(double2) * (4 + NACC) + 2 * sizeof(int)) * C + 256; }
 
 template <class R> Vecs<R> vec_views(SolverPlan *S) {
   using C = typename CT<R>::C;
@@ -1976,7 +1983,7 @@ static int solve_mixed(SolverPlan *S, const double *d_B, const int32_t *d_nodes,
     DGP_TRY(set_ctl(W.ctl, o.inner_tol, inner_maxit, DGP_STOP_PER_COLUMN, st, S->h_ctl));
     launch_init<float, VU>(layouts_for(S, VU).Ld, V, W, st);
     DGP_CHECK_LAUNCH();
-    k_stage_init<<<1, 1024, 0, st>>>(W.cols, W.ctl, S->nsp, ns);
+    k_stage_init<<<1, 1024, 0, st>>>(W.cols, W.ctl, S->nsp, ns, ref > 0 ? W.outer_err : nullptr, o.tol);
     DGP_CHECK_LAUNCH();
     if (cocg) {
       DGP_TRY(enqueue_vec<float>(S, V, W, st, ENQ_COCG_START));
