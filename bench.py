@@ -81,14 +81,33 @@ class Clocks:
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index):
-        self.index = index
+        # nvidia-smi numbers the physical GPUs; CUDA numbers the visible ones
+        vis = [v.strip() for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
+        self.index = vis[index] if index < len(vis) else str(index)
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
-            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), f"--query-gpu={self.Q}",
+            self.p = subprocess.Popen(["nvidia-smi", "-i", self.index, f"--query-gpu={self.Q}",
                                        "--format=csv,noheader,nounits", "-lms", "200"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except FileNotFoundError:
             self.p = None
+
+    def wait_ready(self, samples=5, timeout=30.0):
+        """Blocks until nvidia-smi has written `samples` lines: its start-up (device
+        enumeration) stalls running GPU work, so it must be over before the timed region."""
+        if self.p is None:
+            return
+        t_end = time.perf_counter() + timeout
+        while time.perf_counter() < t_end:
+            self.f.flush()
+            try:
+                n = sum(1 for _ in open(self.f.name))
+            except OSError:
+                n = 0
+            if n >= samples or self.p.poll() is not None:
+                break
+            time.sleep(0.1)
+        time.sleep(0.5)
 
     def mark(self):
         """Start of the timed region: samples before it are not reported."""
@@ -518,7 +537,8 @@ def run_ours(a, rank, world, local_rank):
     # the sampler starts before the timed region (nvidia-smi's start-up talks to the driver and
     # would stall the first timed launches) and keeps sampling through it
     clk = Clocks(torch.cuda.current_device()) if rank == 0 else None
-    time.sleep(1.5)
+    if clk:
+        clk.wait_ready()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()

@@ -77,6 +77,7 @@ _SIGS = {
     "dgp_tg_adjoint_rhs": (C.c_int, [P, P, I32, P, I32, P, I32, I32, P, I64, I32, I32, P, P]),
     "dgp_locate_points": (C.c_int, [P, P, I64, I64, P, I64, D, P, P, P]),
     "dgp_grid_to_mesh": (C.c_int, [P, I64, P, P, P, P, P, P, P]),
+    "dgp_snap_to_surface": (C.c_int, [P, I64, P, P, I64, P, I64, P, P, P, P]),
     "dgp_normal_eq": (C.c_int, [P, I64, I64, P, P, D, I32, P, I64, P, P]),
     "dgp_cholesky_solve": (C.c_int, [P, I64, I64, P, P]),
     "dgp_cholesky_solve_many": (C.c_int, [P, I64, I64, P, I32, I64, P]),

@@ -302,6 +302,22 @@ def locate_points(node: torch.Tensor, elem: torch.Tensor, pts, eps: float = 1e-1
     return eid.long(), w
 
 
+def snap_to_surface(node, bnd, face, pos):
+    """(surface point [N][3], inward normal [N][3], face id [N]) of positions [N][3] on the device
+    (snap_pos, dOptode.m:155-190); bnd [NN] flags, face [NF][3] 0-based surface triangles."""
+    node = torch.as_tensor(node).to(device="cuda", dtype=torch.float64).contiguous()
+    bnd = torch.as_tensor(bnd).to(device="cuda", dtype=torch.int32).contiguous()
+    face = torch.as_tensor(face).to(device="cuda", dtype=torch.int32).contiguous()
+    pos = torch.as_tensor(pos).to(device="cuda", dtype=torch.float64).reshape(-1, 3).contiguous()
+    n = int(pos.shape[0])
+    out = torch.empty((n, 3), dtype=torch.float64, device="cuda")
+    dirs = torch.empty((n, 3), dtype=torch.float64, device="cuda")
+    fid = torch.empty(n, dtype=torch.int32, device="cuda")
+    check(lib.dgp_snap_to_surface(ptr(node), int(node.shape[0]), ptr(bnd), ptr(face), int(face.shape[0]), ptr(pos),
+                                  n, ptr(out), ptr(dirs), ptr(fid), stream_ptr()))
+    return out, dirs, fid.long()
+
+
 def grid_to_mesh(node: torch.Tensor, axes, inmesh):
     """g2m rows (voxel index [NN][4], -1 = empty; weight [NN][4]) for the lattice of
     voxel centres ``ndgrid(*axes)`` (each axis uniformly spaced) and the in-mesh mask."""

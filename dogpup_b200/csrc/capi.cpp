@@ -442,6 +442,13 @@ int dgp_grid_to_mesh(const double *d_node, int64_t nn, const double *origin, con
   DGP_GUARD(grid_to_mesh(d_node, nn, origin, spacing, n, d_inmesh, d_col, d_val, (cudaStream_t)stream));
 }
 
+int dgp_snap_to_surface(const double *d_node, int64_t nn, const int32_t *d_bnd, const int32_t *d_face,
+                        int64_t nface, const double *d_pos, int64_t n, double *d_out_pos, double *d_out_dir,
+                        int32_t *d_out_face, dgp_stream_t stream) {
+  DGP_GUARD(snap_to_surface(d_node, nn, d_bnd, d_face, nface, d_pos, n, d_out_pos, d_out_dir, d_out_face,
+                            (cudaStream_t)stream));
+}
+
 // -------------------------------------------------------- normal equations
 int dgp_normal_eq(const float *d_Jt, int64_t nv, int64_t nmeas, const double *d_w, const double *d_y, double lambda,
                   int32_t damping, double *d_H, int64_t ldh, double *d_rhs, dgp_stream_t stream) {

@@ -132,6 +132,11 @@ int locate_points(const double *d_node, const int32_t *d_elem, int64_t nn, int64
 int grid_to_mesh(const double *d_node, int64_t nn, const double origin[3], const double spacing[3], const int32_t n[3],
                  const uint8_t *d_inmesh, int32_t *d_col, double *d_val, cudaStream_t st);
 
+// optode snapping: closest surface point, inward normal and face of each position
+int snap_to_surface(const double *d_node, int64_t nn, const int32_t *d_bnd, const int32_t *d_face, int64_t nface,
+                    const double *d_pos, int64_t n, double *d_out_pos, double *d_out_dir, int32_t *d_out_face,
+                    cudaStream_t st);
+
 // batched operators (layout [nf][n][ns] complex)
 int spmm_A_f64(const int32_t *rowptr, const int32_t *col, const double2 *KM, const double *omega, int64_t n,
                int32_t nf, int32_t ns, const double2 *X, double2 *Y, cudaStream_t st);

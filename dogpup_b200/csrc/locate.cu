@@ -348,4 +348,145 @@ int grid_to_mesh(const double *d_node, int64_t nn, const double origin[3], const
   return DGP_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Optode snapping (snap_pos, dOptode.m:155-190): nearest boundary node
+// (dsearchn), then the closest point on the surface triangles that contain
+// that node (ties: lower face index) and the face's normal -cross(b-a, c-a)
+// normalised.  One block per optode; both searches are block-wide argmins.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct D3 {
+  double x, y, z;
+};
+__device__ inline D3 ld3(const double *p, int64_t i) { return D3{p[3 * i], p[3 * i + 1], p[3 * i + 2]}; }
+__device__ inline D3 sub3(D3 a, D3 b) { return D3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ inline D3 axpy3(double s, D3 a, D3 b) { return D3{b.x + s * a.x, b.y + s * a.y, b.z + s * a.z}; }
+__device__ inline double dot3(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+// closest point of triangle abc to p: Voronoi-region walk over the vertices, edges and the
+// face (Ericson, Real-Time Collision Detection, sec. 5.1.5)
+__device__ D3 closest_on_triangle(D3 p, D3 a, D3 b, D3 c) {
+  const D3 ab = sub3(b, a), ac = sub3(c, a), ap = sub3(p, a);
+  const double d1 = dot3(ab, ap), d2 = dot3(ac, ap);
+  if (d1 <= 0 && d2 <= 0) return a;
+  const D3 bp = sub3(p, b);
+  const double d3 = dot3(ab, bp), d4 = dot3(ac, bp);
+  if (d3 >= 0 && d4 <= d3) return b;
+  const double vc = d1 * d4 - d3 * d2;
+  if (vc <= 0 && d1 >= 0 && d3 <= 0) return axpy3(d1 / (d1 - d3), ab, a);
+  const D3 cp = sub3(p, c);
+  const double d5 = dot3(ab, cp), d6 = dot3(ac, cp);
+  if (d6 >= 0 && d5 <= d6) return c;
+  const double vb = d5 * d2 - d1 * d6;
+  if (vb <= 0 && d2 >= 0 && d6 <= 0) return axpy3(d2 / (d2 - d6), ac, a);
+  const double va = d3 * d6 - d5 * d4;
+  if (va <= 0 && (d4 - d3) >= 0 && (d5 - d6) >= 0)
+    return axpy3((d4 - d3) / ((d4 - d3) + (d5 - d6)), sub3(c, b), b);
+  const double den = 1.0 / (va + vb + vc);
+  return axpy3(vc * den, ac, axpy3(vb * den, ab, a));
+}
+
+// block argmin of (value, index): smaller value, then smaller index; result in thread 0's return
+template <int NT>
+__device__ void block_argmin(double &v, int64_t &i) {
+  __shared__ double sv[NT];
+  __shared__ int64_t si[NT];
+  sv[threadIdx.x] = v;
+  si[threadIdx.x] = i;
+  __syncthreads();
+  for (int o = NT / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      const double w = sv[threadIdx.x + o];
+      const int64_t j = si[threadIdx.x + o];
+      if (w < sv[threadIdx.x] || (w == sv[threadIdx.x] && j >= 0 && (si[threadIdx.x] < 0 || j < si[threadIdx.x]))) {
+        sv[threadIdx.x] = w;
+        si[threadIdx.x] = j;
+      }
+    }
+    __syncthreads();
+  }
+  v = sv[0];
+  i = si[0];
+  __syncthreads();
+}
+
+constexpr int SNAP_NT = 256;
+
+__global__ void __launch_bounds__(SNAP_NT) k_snap(const double *__restrict__ node, int64_t nn,
+                                                  const int32_t *__restrict__ bnd, const int32_t *__restrict__ face,
+                                                  int64_t nface, const double *__restrict__ pos,
+                                                  double *__restrict__ out_pos, double *__restrict__ out_dir,
+                                                  int32_t *__restrict__ out_face) {
+  const int64_t o = blockIdx.x;
+  const D3 p = ld3(pos, o);
+  // nearest boundary node
+  double bd = INFINITY;
+  int64_t bi = -1;
+  for (int64_t i = threadIdx.x; i < nn; i += SNAP_NT) {
+    if (!bnd[i]) continue;
+    const D3 d = sub3(ld3(node, i), p);
+    const double d2 = dot3(d, d);
+    if (d2 < bd) {  // ascending i per thread: the first minimum is kept
+      bd = d2;
+      bi = i;
+    }
+  }
+  block_argmin<SNAP_NT>(bd, bi);
+  // closest point over the faces that contain that node
+  double fd = INFINITY;
+  int64_t fi = -1;
+  if (bi >= 0) {
+    for (int64_t f = threadIdx.x; f < nface; f += SNAP_NT) {
+      const int32_t v0 = face[3 * f], v1 = face[3 * f + 1], v2 = face[3 * f + 2];
+      if (v0 != bi && v1 != bi && v2 != bi) continue;
+      const D3 q = closest_on_triangle(p, ld3(node, v0), ld3(node, v1), ld3(node, v2));
+      const D3 d = sub3(q, p);
+      const double dist = sqrt(dot3(d, d));
+      if (dist < fd) {
+        fd = dist;
+        fi = f;
+      }
+    }
+  }
+  block_argmin<SNAP_NT>(fd, fi);
+  if (threadIdx.x != 0) return;
+  out_face[o] = (int32_t)fi;
+  if (fi < 0) {
+    for (int d = 0; d < 3; ++d) out_pos[3 * o + d] = out_dir[3 * o + d] = NAN;
+    return;
+  }
+  const D3 a = ld3(node, face[3 * fi]), b = ld3(node, face[3 * fi + 1]), c = ld3(node, face[3 * fi + 2]);
+  const D3 q = closest_on_triangle(p, a, b, c);
+  const D3 u = sub3(b, a), w = sub3(c, a);
+  D3 nv{-(u.y * w.z - u.z * w.y), -(u.z * w.x - u.x * w.z), -(u.x * w.y - u.y * w.x)};
+  const double len = sqrt(dot3(nv, nv));
+  out_pos[3 * o] = q.x;
+  out_pos[3 * o + 1] = q.y;
+  out_pos[3 * o + 2] = q.z;
+  out_dir[3 * o] = nv.x / len;
+  out_dir[3 * o + 1] = nv.y / len;
+  out_dir[3 * o + 2] = nv.z / len;
+}
+
+}  // namespace
+
+int snap_to_surface(const double *d_node, int64_t nn, const int32_t *d_bnd, const int32_t *d_face, int64_t nface,
+                    const double *d_pos, int64_t n, double *d_out_pos, double *d_out_dir, int32_t *d_out_face,
+                    cudaStream_t st) {
+  DGP_REQUIRE(nn > 0 && nface > 0 && n >= 0, "snap_to_surface: bad sizes");
+  if (n == 0) return DGP_OK;
+  DGP_REQUIRE(d_node && d_bnd && d_face && d_pos && d_out_pos && d_out_dir && d_out_face,
+              "snap_to_surface: null pointer");
+  DGP_REQUIRE(n <= INT32_MAX, "snap_to_surface: too many optodes");
+  k_snap<<<(unsigned)n, SNAP_NT, 0, st>>>(d_node, nn, d_bnd, d_face, nface, d_pos, d_out_pos, d_out_dir, d_out_face);
+  DGP_CHECK_LAUNCH();
+  std::vector<int32_t> hf((size_t)n);
+  DGP_CUDA(cudaMemcpyAsync(hf.data(), d_out_face, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st));
+  DGP_CUDA(cudaStreamSynchronize(st));
+  for (int64_t i = 0; i < n; ++i)
+    if (hf[i] < 0) return fail(DGP_ERR_ARG, "snap_to_surface: no boundary node or no face on it");
+  return DGP_OK;
+}
+
 }  // namespace dgp

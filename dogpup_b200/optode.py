@@ -2,8 +2,9 @@
 
 Mirrors the ``dOptode`` class (DOGPUP/dOptode.m:34-199).  The Fourier
 coefficients of the source pulse come from the device ``td2fc`` kernel; the
-geometry (nearest surface point, containing tetrahedron) is host set-up code,
-as in the reference, where it runs once per optode in MATLAB.
+geometry (nearest surface point, containing tetrahedron) runs on the device
+(``dgp_snap_to_surface``, ``dgp_locate_points``), or on the host with k-d
+tree candidates (``snap2mesh(mesh, device=False)``).
 """
 from __future__ import annotations
 
@@ -40,13 +41,39 @@ class DOptode:
         self.s_bary = self.d_bary = None
         self.s_dirs = self.d_dirs = None
 
-    def snap2mesh(self, mesh):
-        """Snap optodes to the surface, move sources 1/min(musp) inward (dOptode.m:77-97)."""
+    def snap2mesh(self, mesh, device=True):
+        """Snap optodes to the surface, move sources 1/min(musp) inward (dOptode.m:77-97).
+
+        device=True: surface search (``dgp_snap_to_surface``) and point location
+        (``dgp_locate_points``) on the GPU; device=False: the host k-d tree path."""
+        if device:
+            return self._snap2mesh_device(mesh)
         self.d_positions, self.d_bary, self.d_dirs = snap_pos(mesh, self.d_positions)
         self.s_positions, _, self.s_dirs = snap_pos(mesh, self.s_positions)
         inset = self.s_positions + (1.0 / float(np.min(mesh.musp_host))) * self.s_dirs   # :89
         eid, w = locate_points(mesh.node_host, mesh.elem_host, inset, mesh.locator())
         self.s_bary = _clean_bary(eid, w)
+        return self
+
+
+    def _snap2mesh_device(self, mesh):
+        node = torch.as_tensor(mesh.node_host, device="cuda")
+        elem = torch.as_tensor(mesh.elem_host, device="cuda", dtype=torch.int32)
+        face = torch.as_tensor(mesh.face_host, device="cuda", dtype=torch.int32)
+
+        def locate(pts):
+            eid, w = api.locate_points(node, elem, pts, eps=1e-9)          # pointLocation, :88-92, :188
+            eid, w = eid.cpu().numpy(), w.cpu().numpy()
+            if (eid < 0).any():
+                raise ValueError(f"point {pts[int(np.nonzero(eid < 0)[0][0])].tolist()} lies outside the mesh")
+            return _clean_bary(eid, w)
+
+        dpos, ddir, _ = api.snap_to_surface(node, mesh.fem.bnd, face, self.d_positions)
+        spos, sdir, _ = api.snap_to_surface(node, mesh.fem.bnd, face, self.s_positions)
+        self.d_positions, self.d_dirs = dpos.cpu().numpy(), ddir.cpu().numpy()
+        self.s_positions, self.s_dirs = spos.cpu().numpy(), sdir.cpu().numpy()
+        self.d_bary = locate(dpos)
+        self.s_bary = locate(spos + (1.0 / float(np.min(mesh.musp_host))) * sdir)   # :89
         return self
 
 

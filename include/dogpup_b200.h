@@ -416,6 +416,19 @@ int dgp_locate_points(const double *d_node, const int32_t *d_elem, int64_t nn,
                       int64_t ne, const double *d_pts, int64_t np, double eps,
                       int32_t *d_eid, double *d_w, dgp_stream_t stream);
 
+/* Optode snapping (snap_pos, dOptode.m:155-190): for each position
+ * d_pos[i][0..2], the nearest boundary node (d_bnd[v] != 0; ties: lower
+ * index), then the closest point on the surface triangles d_face[f][0..2]
+ * (int32, 0-based) that contain that node (ties: lower face index):
+ * d_out_pos[i] = that point, d_out_dir[i] = the face's normal
+ * -cross(b - a, c - a) normalised (inward for outward-ordered faces),
+ * d_out_face[i] = the face.  DGP_ERR_ARG when a position finds no boundary
+ * node or face.  Synchronises the stream. */
+int dgp_snap_to_surface(const double *d_node, int64_t nn, const int32_t *d_bnd,
+                        const int32_t *d_face, int64_t nface, const double *d_pos,
+                        int64_t n, double *d_out_pos, double *d_out_dir,
+                        int32_t *d_out_face, dgp_stream_t stream);
+
 /* Grid-to-mesh interpolation g2m (dMesh.m:330-373) on the lattice of voxel
  * centres origin[d] + i*spacing[d], i < n[d], spacing != 0 (host arrays of 3;
  * voxel index

@@ -156,3 +156,60 @@ def test_dmesh_g2m_is_the_oracle_g2m():
     xs = [np.arange(lo[d] - 2, hi[d] + 2.001, 1.5) for d in range(3)]
     mesh.mesh2grid(*xs)
     _g2m_compare(mesh.g2m, g2m_matrix(mesh.node_host, xs, mesh.gridinmesh), mesh.node_host, xs)
+
+
+def _snap_case(with_w=False):
+    from dogpup_b200 import workloads
+    w = workloads.small_fwd(ns=8, nd=8, nf=4)
+    mesh = workloads.build_dmesh(w)
+    if with_w:
+        return mesh, w
+    rng = np.random.default_rng(5)
+    c = w["mesh"].node.mean(0)
+    pos = np.concatenate([w["src"], w["det"], c + rng.standard_normal((40, 3)) * [14, 14, 10],
+                          mesh.node_host[np.nonzero(mesh.bnd_host)[0][:5]]])      # exactly on boundary nodes
+    return mesh, pos
+
+
+def test_snap_to_surface_against_oracle():
+    """Surface points to 1e-12 and normals to 1e-12; where two candidate faces are equally
+    close (the point lands on their shared edge) either face's normal is accepted."""
+    from dogpup_b200 import api
+    from oracle.optode import snap_pos
+    mesh, pos = _snap_case()
+    q, d, f = api.snap_to_surface(mesh.node_host, mesh.fem.bnd, mesh.face_host, pos)
+    q, d, f = q.cpu().numpy(), d.cpu().numpy(), f.cpu().numpy()
+    q0, d0, f0, dists = snap_pos(mesh.node_host, mesh.bnd_host, mesh.face_host, pos)
+    assert np.abs(q - q0).max() < 1e-12
+    for i in range(len(pos)):
+        tie = len(dists[i]) > 1 and dists[i][1] - dists[i][0] <= 1e-12 * max(1.0, dists[i][0])
+        if not tie:
+            assert f[i] == f0[i]
+            assert np.abs(d[i] - d0[i]).max() < 1e-12
+    assert np.allclose(np.linalg.norm(d, axis=1), 1.0)
+
+
+def test_snap_rejects_a_mesh_without_boundary():
+    from dogpup_b200 import api
+    from dogpup_b200._lib import DgpError
+    mesh, pos = _snap_case()
+    with pytest.raises(DgpError):
+        api.snap_to_surface(mesh.node_host, np.zeros(mesh.nn, np.int32), mesh.face_host, pos[:3])
+
+
+def test_optode_snap_device_equals_host():
+    """DOptode.snap2mesh on the device and on the host: same surface points, normals and
+    source/detector points (the weighted vertices of the located elements)."""
+    from dogpup_b200.optode import DOptode
+    from dogpup_b200.workloads import gaussian_pulse
+    mesh, w = _snap_case(with_w=True)
+    t = w["t"]
+    o_dev, o_host = (DOptode(w["src"], w["det"], w["link"], 1e3, gaussian_pulse(t), t, w["nf"]) for _ in range(2))
+    o_dev.snap2mesh(mesh)
+    o_host.snap2mesh(mesh, device=False)
+    assert np.abs(o_host.s_positions - o_dev.s_positions).max() < 1e-12
+    assert np.abs(o_host.d_positions - o_dev.d_positions).max() < 1e-12
+    assert np.abs(o_host.s_dirs - o_dev.s_dirs).max() < 1e-12
+    for b_dev, b_host in ((o_dev.s_bary, o_host.s_bary), (o_dev.d_bary, o_host.d_bary)):
+        pt = lambda b: (b[:, 1:, None] * mesh.node_host[mesh.elem_host[b[:, 0].astype(int)]]).sum(1)
+        assert np.abs(pt(b_dev) - pt(b_host)).max() < 1e-9

@@ -251,3 +251,14 @@ def test_reshape_and_spot_oracles():
         t2 = jacobian.target_spots(g, inm, [[3, 4, 2], [6.5, 1, 3]], wd, kind)
         assert not t2[:, ~inm].any() and np.array_equal(t2[:, inm], t[:, inm])
     assert np.count_nonzero(jacobian.target_spots(g, inm, [[3, 4, 2]], 3.0, "square")) == 27
+
+
+def test_closest_point_on_triangle_two_methods():
+    """The package's Voronoi-region walk and the oracle's projection-or-edges route agree."""
+    from dogpup_b200.optode import closest_point_on_triangle as walk
+    from oracle.optode import closest_point_on_triangle as proj
+    rng = np.random.default_rng(8)
+    for _ in range(400):
+        a, b, c = rng.standard_normal((3, 3))
+        p = rng.standard_normal(3) * 2
+        assert np.abs(walk(p, a, b, c) - proj(p, a, b, c)).max() < 1e-12
