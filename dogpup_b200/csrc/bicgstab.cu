@@ -408,7 +408,7 @@ __device__ inline bool halted(const Ctl *ctl, int need) {
 }
 
 // Y = Op_k X.  MODE 0: store.  MODE 1: store, acc[D1] += Y.W.
-// MODE 2: no store, acc[D2] += Y.W, acc[D3] += Y.Y.
+// MODE 2: no store, acc[D2] += Y.W, acc[D3] += Y.Y.  MODE 3: store, acc[D1] += Y.Y.
 template <class R, int VEC, int MODE, class Op>
 __global__ void __launch_bounds__(BS) k_spmm(Layout L, Op op, const typename CT<R>::C *__restrict__ X,
                                              typename CT<R>::C *__restrict__ Y,
@@ -441,7 +441,10 @@ __global__ void __launch_bounds__(BS) k_spmm(Layout L, Op op, const typename CT<
     else row_spmv<VEC>(L.nsp, cs, op.rowptr, i, cf, Xk, y);
     const int64_t o = vidx(L, ln.k, i, c0);
     if (MODE != 2) stv<VEC>(Y + o, cs, y);
-    if (MODE != 0) {
+    if constexpr (MODE == 3) {
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) acc_bil(part[v][0], y[v], y[v]);
+    } else if (MODE != 0) {
       C w[VEC];
       ldv<VEC>(W + o, cs, w);
 #pragma unroll
@@ -457,7 +460,7 @@ __global__ void __launch_bounds__(BS) k_spmm(Layout L, Op op, const typename CT<
     for (int v = 0; v < VEC; ++v)
 #pragma unroll
       for (int q = 0; q < NQ; ++q) pd[v][q] = d2(part[v][q]);
-    if constexpr (MODE == 1) {
+    if constexpr (MODE == 1 || MODE == 3) {
       const int slot[1] = {ACC_D1};
       block_reduce<VEC, 1, E>(L, ln, pd, cols.acc, cols.C, slot, smem);
     } else {
@@ -1637,7 +1640,9 @@ void enqueue_iteration(const SolverPlan *S, const OpA &A, const OpG &G, const Op
   k_update_p<R, VU><<<grid_of(Lu), BS, 0, st>>>(Lu, V.r, V.p, W.cols, ctl);
 }
 
-// COCG preconditioner step: T1 = G r ; z = G^T T1 with acc[D1] = r.z ; rho, beta
+// COCG preconditioner step: T1 = G r ; z = G^T T1 ; acc[D1] = r.z ; rho, beta.  The gather
+// path takes r.z = r^T G^T G r as T1.T1 in the G sweep (no second read of r); the tiled path
+// takes it as r.z in the G^T sweep.
 template <class R, int VS, int VD, class OpG>
 void enqueue_cocg_precond(const SolverPlan *S, const OpG &G, const OpG &GT, const Vecs<R> &V, const Work &W,
                           int first, cudaStream_t st) {
@@ -1652,8 +1657,8 @@ void enqueue_cocg_precond(const SolverPlan *S, const OpG &G, const OpG &GT, cons
   }
   if (!done) {
     const Layout Ls = spmm_layouts(S, VS, sizeof(R) == 4).L, Lsd = spmm_layouts(S, VD, sizeof(R) == 4).Ld;
-    k_spmm<R, VS, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, G, V.r, V.T1, nullptr, W.cols, ctl);
-    k_spmm<R, VD, 1><<<grid_of(Lsd), BS, red_smem(Lsd, 1), st>>>(Lsd, GT, V.T1, V.z, V.r, W.cols, ctl);
+    k_spmm<R, VD, 3><<<grid_of(Lsd), BS, red_smem(Lsd, 1), st>>>(Lsd, G, V.r, V.T1, nullptr, W.cols, ctl);
+    k_spmm<R, VS, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, GT, V.T1, V.z, nullptr, W.cols, ctl);
   }
   k_cocg_rho<<<1, 1024, 0, st>>>(W.cols, ctl, first);
 }
