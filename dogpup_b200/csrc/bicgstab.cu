@@ -1203,8 +1203,9 @@ __global__ void k_accum_x(int64_t n, int nf, int nsp, int ns, const float2 *__re
   }
 }
 
-// FP64 residual r = b - A_k X (X in the caller's layout, stride ns), written as FP32 into
-// r32 (the next inner right-hand side) with FP64 norms into acc[NR].  b is a dense caller
+// FP64 residual r = b - A_k X (X in the caller's layout, stride ns; X = NULL: X = 0, no
+// mat-vec), written as FP32 into r32 (the next inner right-hand side) with FP64 norms into
+// acc[NR].  b is a dense caller
 // buffer (stride ns) or the point sources (nodes, w, fpsf) generated on the fly.
 template <int VEC>
 __global__ void __launch_bounds__(BS) k_residual64(Layout L, int ns, const int32_t *__restrict__ rowptr,
@@ -1230,7 +1231,7 @@ __global__ void __launch_bounds__(BS) k_residual64(Layout L, int ns, const int32
   double2 part[VEC][1];
 #pragma unroll
   for (int q = 0; q < VEC; ++q) part[q][0] = make_double2(0, 0);
-  const double2 *Xk = X + (int64_t)ln.k * L.n * ns;
+  const double2 *Xk = X ? X + (int64_t)ln.k * L.n * ns : nullptr;
   // columns of this lane: the strided mapping of the FP32 vectors (E = 2) it writes
   int scol[VEC];
 #pragma unroll
@@ -1241,7 +1242,7 @@ __global__ void __launch_bounds__(BS) k_residual64(Layout L, int ns, const int32
     double2 y[VEC];
 #pragma unroll
     for (int q = 0; q < VEC; ++q) y[q] = make_double2(0, 0);
-    const int b = __ldg(rowptr + i), e = __ldg(rowptr + i + 1);
+    const int b = X ? __ldg(rowptr + i) : 0, e = X ? __ldg(rowptr + i + 1) : 0;
     for (int p = b; p < e; ++p) {
       const int j = __ldg(col + p);
       const double2 km = __ldg(KM + p);
@@ -1968,8 +1969,8 @@ static int solve_mixed(SolverPlan *S, const double *d_B, const int32_t *d_nodes,
   const Layouts LL = layouts_for(S, vec);
   DGP_CUDA(cudaMemsetAsync(d_X, 0, sizeof(double2) * (size_t)S->nf * S->n * ns, st));
   DGP_CUDA(cudaMemsetAsync(W.cols.acc, 0, sizeof(double2) * W.cols.C * NACC, st));
-  // r = b (x = 0): ||b|| per column
-  launch_residual(S, ns, d_X, d_B, d_nodes, d_w, d_fpsf, V.r, W, st);
+  // r = b (x = 0, no mat-vec): ||b|| per column
+  launch_residual(S, ns, nullptr, d_B, d_nodes, d_w, d_fpsf, V.r, W, st);
   k_outer_norms<<<1, 1024, 0, st>>>(W.cols, W.bnorm, W.outer_err, W.ctl, 0, S->nsp, ns);
   DGP_CHECK_LAUNCH();
   int total_iters = 0, refinements = 0;
