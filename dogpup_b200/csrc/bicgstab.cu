@@ -768,13 +768,11 @@ __global__ void __launch_bounds__(BS) k_update_p(Layout L, const typename CT<R>:
 }
 
 // ------------------------------------------------ COCG (mixed inner solve)
-// x = x + alpha p ; r = r - alpha q ; acc[NR] += |r|^2
+// r = r - alpha q ; acc[NR] += |r|^2   (iterating columns)
 template <class R, int VEC>
-__global__ void __launch_bounds__(BS) k_update_xr(Layout L, typename CT<R>::C *__restrict__ x,
-                                                  const typename CT<R>::C *__restrict__ p,
-                                                  typename CT<R>::C *__restrict__ r,
-                                                  const typename CT<R>::C *__restrict__ q, Cols cols,
-                                                  const Ctl *ctl) {
+__global__ void __launch_bounds__(BS) k_update_r(Layout L, typename CT<R>::C *__restrict__ r,
+                                                 const typename CT<R>::C *__restrict__ q, Cols cols,
+                                                 const Ctl *ctl) {
   using C = typename CT<R>::C;
   if (halted(ctl, ST_RUNNING)) return;
   if (harmonic_done(cols, blockIdx.y)) return;
@@ -792,23 +790,60 @@ __global__ void __launch_bounds__(BS) k_update_xr(Layout L, typename CT<R>::C *_
     const int64_t i = ln.row(L, it);
     if (i >= L.n) break;
     const int64_t o = vidx(L, ln.k, i, c0);
-    C xx[VEC], pp[VEC], rr[VEC], qq[VEC];
-    ldv<VEC>(x + o, cs, xx);
-    ldv<VEC>(p + o, cs, pp);
+    C rr[VEC], qq[VEC];
     ldv<VEC>(r + o, cs, rr);
     ldv<VEC>(q + o, cs, qq);
 #pragma unroll
     for (int v = 0; v < VEC; ++v) {
-      if (!act[v]) continue;
-      xx[v] = cfmaT(al[v], pp[v], xx[v]);
+      if (act[v] != 1) continue;
       rr[v] = cfmaT(cneg(al[v]), qq[v], rr[v]);
       acc_abs2(part[v][0].x, rr[v]);
     }
-    stv<VEC>(x + o, cs, xx);
     stv<VEC>(r + o, cs, rr);
   }
   const int slot[1] = {ACC_NR};
   block_reduce<VEC, 1, E>(L, ln, part, cols.acc, cols.C, slot, smem);
+}
+
+// x = x + alpha p (columns iterating or pending: active 1 or 2), then p = z + beta p (columns
+// still iterating, RUNNING state); in the FINAL state only the x update.  The x update of
+// iteration k is taken here, before p changes, so p is read once per iteration.
+template <class R, int VEC>
+__global__ void __launch_bounds__(BS) k_update_px(Layout L, typename CT<R>::C *__restrict__ x,
+                                                  typename CT<R>::C *__restrict__ p,
+                                                  const typename CT<R>::C *__restrict__ z, Cols cols,
+                                                  const Ctl *ctl) {
+  using C = typename CT<R>::C;
+  if (halted(ctl, ST_FINAL)) return;
+  if (harmonic_done(cols, blockIdx.y)) return;
+  const bool run = *(volatile const int *)&ctl->state == ST_RUNNING;
+  Lane ln(L);
+  constexpr int E = Chunk<typename CT<R>::C>::E;
+  const int c0 = ln.template col0<E>(), cs = ln.template cs<E>(L);
+  C al[VEC], be[VEC];
+  int act[VEC], actb[VEC];
+  lane_scalars<R, VEC>(cols, ln, L, cols.alpha, al, act);
+  lane_scalars<R, VEC>(cols, ln, L, cols.beta, be, actb);
+  bool any_p = false;
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) any_p |= run && act[v] == 1;
+  for (int it = 0; it < L.ipb; ++it) {
+    const int64_t i = ln.row(L, it);
+    if (i >= L.n) break;
+    const int64_t o = vidx(L, ln.k, i, c0);
+    C xx[VEC], pp[VEC], zz[VEC];
+    ldv<VEC>(x + o, cs, xx);
+    ldv<VEC>(p + o, cs, pp);
+    if (any_p) ldv<VEC>(z + o, cs, zz);
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) {
+      if (!act[v]) continue;
+      xx[v] = cfmaT(al[v], pp[v], xx[v]);
+      if (run && act[v] == 1) pp[v] = cfmaT(be[v], pp[v], zz[v]);
+    }
+    stv<VEC>(x + o, cs, xx);
+    if (any_p) stv<VEC>(p + o, cs, pp);
+  }
 }
 
 // ------------------------------------------------------------ scalar stages
@@ -1009,7 +1044,7 @@ __global__ void __launch_bounds__(1024) k_cocg_check(Cols c, Ctl *ctl) {
     }
     c.err[j] = e;
     if (stop_rule == DGP_STOP_PER_COLUMN && e < c.tolc[j]) {
-      c.active[j] = 0;
+      c.active[j] = 2;  // converged: its last x update is still pending (k_update_px)
       c.status[j] = DGP_COL_CONVERGED;
       continue;
     }
@@ -1019,12 +1054,38 @@ __global__ void __launch_bounds__(1024) k_cocg_check(Cols c, Ctl *ctl) {
   if (threadIdx.x == 0) {
     ctl->iters += 1;
     ctl->max_err = m;
+    // FINAL: the rest of this iteration applies the pending x updates only, k_cocg_count ends it
     if (stop_rule == DGP_STOP_MAX_ALL && m < tol) {
-      ctl->state = ST_DONE;
+      ctl->state = ST_FINAL;
       ctl->reason = 0;
     } else if (ctl->iters >= ctl->maxit) {
-      ctl->state = ST_DONE;
+      ctl->state = ST_FINAL;
       ctl->reason = 1;
+    }
+  }
+}
+
+// end of a COCG iteration: pending columns (x updated) are frozen, active columns counted,
+// harmonic activity refreshed; FINAL or no active column -> DONE
+__global__ void __launch_bounds__(1024) k_cocg_count(Cols c, Ctl *ctl) {
+  const int st = ctl->state;
+  if (st == ST_DONE) return;
+  typedef cub::BlockReduce<int, 1024> BR;
+  __shared__ typename BR::TempStorage tmp;
+  int a = 0;
+  for (int64_t j = threadIdx.x; j < c.C; j += blockDim.x) {
+    if (c.active[j] == 2) c.active[j] = 0;
+    a += c.active[j] == 1;
+  }
+  a = BR(tmp).Sum(a);  // (its barrier also orders the active[] writes before update_hact)
+  update_hact(c);
+  if (threadIdx.x == 0) {
+    ctl->n_active = a;
+    if (st == ST_FINAL) {
+      ctl->state = ST_DONE;
+    } else if (a == 0) {
+      ctl->state = ST_DONE;
+      ctl->reason = ctl->iters == 0 ? 2 : 0;
     }
   }
 }
@@ -1035,10 +1096,13 @@ __global__ void __launch_bounds__(1024) k_cocg_rho(Cols c, Ctl *ctl, int first) 
   for (int64_t j = threadIdx.x; j < c.C; j += blockDim.x) {
     double2 d = c.acc[ACC_D1 * c.C + j];
     c.acc[ACC_D1 * c.C + j] = make_double2(0, 0);
-    if (!c.active[j]) continue;
+    if (c.active[j] != 1) continue;
     const double2 b = first ? make_double2(0, 0) : cdiv(d, c.rho0[j]);
     if (!(cabs2(d) > 0.0) || !finite2(d) || !finite2(b)) {
-      freeze(c, j, DGP_COL_BREAKDOWN_RHO);
+      // r already holds this iteration's update: keep alpha so that x takes it too, then stop
+      c.active[j] = 2;
+      c.status[j] = DGP_COL_BREAKDOWN_RHO;
+      c.beta[j] = make_double2(0, 0);
       continue;
     }
     c.beta[j] = b;
@@ -1675,8 +1739,8 @@ void enqueue_cocg_start(const SolverPlan *S, const OpG &G, const OpG &GT, const 
 
 // one preconditioned COCG iteration (conjugate-orthogonal CG for the complex-symmetric A_k with
 // the complex-symmetric FSAI preconditioner G^T G), KERNELS_PER_ITER_COCG launches:
-//   q = A p, p.q ; alpha = rho/(p.q) ; x += alpha p, r -= alpha q, ||r|| ; stop checks ;
-//   z = G^T G r, rho' = r.z, beta = rho'/rho ; p = z + beta p
+//   q = A p, p.q ; alpha = rho/(p.q) ; r -= alpha q, ||r|| ; stop checks ;
+//   z = G^T G r, rho' = r.z, beta = rho'/rho ; x += alpha p, p = z + beta p ; count
 template <class R, int VS, int VD, class OpA, class OpG>
 void enqueue_cocg(const SolverPlan *S, const OpA &A, const OpG &G, const OpG &GT, const Vecs<R> &V, const Work &W,
                   cudaStream_t st) {
@@ -1694,11 +1758,11 @@ void enqueue_cocg(const SolverPlan *S, const OpA &A, const OpG &G, const OpG &GT
     k_spmm<R, VD, 1><<<grid_of(Lsd), BS, red_smem(Lsd, 1), st>>>(Lsd, A, V.p, V.v, V.p, W.cols, ctl);
   }
   k_cocg_alpha<<<1, 1024, 0, st>>>(W.cols, ctl);
-  k_update_xr<R, VU><<<grid_of(Lud), BS, red_smem(Lud, 1), st>>>(Lud, V.x, V.p, V.r, V.v, W.cols, ctl);
+  k_update_r<R, VU><<<grid_of(Lud), BS, red_smem(Lud, 1), st>>>(Lud, V.r, V.v, W.cols, ctl);
   k_cocg_check<<<1, 1024, 0, st>>>(W.cols, ctl);
-  k_stage_count<<<1, 1024, 0, st>>>(W.cols, ctl);
   enqueue_cocg_precond<R, VS, VD>(S, G, GT, V, W, 0, st);
-  k_update_p<R, VU><<<grid_of(Lu), BS, 0, st>>>(Lu, V.z, V.p, W.cols, ctl);
+  k_update_px<R, VU><<<grid_of(Lu), BS, 0, st>>>(Lu, V.x, V.p, V.z, W.cols, ctl);
+  k_cocg_count<<<1, 1024, 0, st>>>(W.cols, ctl);
 }
 
 enum { ENQ_BICGSTAB = 0, ENQ_COCG = 1, ENQ_COCG_START = 2 };

@@ -204,6 +204,27 @@ def test_solver_reports_maxit(small_case, gpu_case, torch):
     assert np.isfinite(X.cpu().numpy()).all()
 
 
+@pytest.mark.parametrize("precision", ["mixed", "mixed_bicgstab"])
+def test_mixed_solver_stops_at_maxit_with_progress(small_case, gpu_case, torch, precision):
+    """maxit reached inside an inner solve: the iterations done so far still enter X (for
+    COCG the last x update is applied after the stop), the statuses say maxit and the true
+    FP64 residual has fallen."""
+    from dogpup_b200 import api
+    nf, ns = 4, 4
+    dfc = 2 * np.pi / 10e-9 / (C_VAC / 1.4)
+    fem = gpu_case["fem"]
+    S = api.Solver(fem.rowptr, fem.col, gpu_case["K"], gpu_case["M"], dfc, nf, ns)
+    nodes, w = _point_sources(small_case, ns, 3)
+    status = torch.full((nf * ns,), -1, dtype=torch.int32, device="cuda")
+    X, rep = S.solve_sources(torch.as_tensor(nodes, device="cuda"), torch.as_tensor(w, device="cuda"),
+                             torch.ones(nf, dtype=torch.complex128, device="cuda"),
+                             api.make_opts(tol=1e-12, maxit=5, precision=precision, check_every=1), status=status)
+    assert rep.iterations == 5
+    assert (status.cpu().numpy() == 1).all()
+    assert np.isfinite(X.cpu().numpy()).all() and np.abs(X.cpu().numpy()).max() > 0
+    assert rep.max_rel_residual < 0.5
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed", "mixed_bicgstab"])
 def test_solver_harmonic_subset(small_case, gpu_case, torch, precision):
     """A plan over harmonics [5, 0, 9] solves slot j at harmonic h_j: same as the full plan's columns."""
