@@ -78,6 +78,7 @@ _SIGS = {
     "dgp_locate_points": (C.c_int, [P, P, I64, I64, P, I64, D, P, P, P]),
     "dgp_grid_to_mesh": (C.c_int, [P, I64, P, P, P, P, P, P, P]),
     "dgp_snap_to_surface": (C.c_int, [P, I64, P, P, I64, P, I64, P, P, P, P]),
+    "dgp_solver_set_dot_rows": (C.c_int, [P, I32]),
     "dgp_normal_eq": (C.c_int, [P, I64, I64, P, P, D, I32, P, I64, P, P]),
     "dgp_cholesky_solve": (C.c_int, [P, I64, I64, P, P]),
     "dgp_cholesky_solve_many": (C.c_int, [P, I64, I64, P, I32, I64, P]),

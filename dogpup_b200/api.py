@@ -128,6 +128,10 @@ class Solver:
     def set_spmm(self, tiled: bool, vec: int = 0, rows: int = 0):
         check(lib.dgp_solver_set_spmm(self._h, int(tiled), int(vec), int(rows)))
 
+    def set_dot_rows(self, mult: int):
+        """Rows per block of the dot-product SpMM sweeps as a multiple of the plain ones (0 = 4)."""
+        check(lib.dgp_solver_set_dot_rows(self._h, int(mult)))
+
     def check_spmm(self) -> float:
         """max |tiled - gather| / max |value| over A, G, G^T on a test pattern."""
         d = C.c_double()

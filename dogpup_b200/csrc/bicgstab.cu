@@ -1626,10 +1626,11 @@ Layouts layouts_for(const SolverPlan *S, int vec, int rows = 64) {
 }
 
 // SpMM layouts: rows per block from the autotuner when it has run; the complex-FP32 dot
-// sweeps keep at most 32 rows per lane, the bound of their FP32 per-lane partial sums
+// sweeps take tune_dot (default 4) times those rows per block and at most 32 rows per
+// lane, the bound of their FP32 per-lane partial sums
 Layouts spmm_layouts(const SolverPlan *S, int vec, bool fp32) {
   Layouts x = layouts_for(S, vec, (fp32 && S->tune_rows) ? S->tune_rows : 64);
-  if (fp32) x.Ld.ipb = std::max(x.L.ipb, std::min(x.L.ipb * 16, 32));
+  if (fp32) x.Ld.ipb = std::max(x.L.ipb, std::min(x.L.ipb * (S->tune_dot ? S->tune_dot : 4), 32));
   return x;
 }
 
@@ -2138,10 +2139,15 @@ namespace {
 template <int VEC>
 void profile_launch(int which, const SolverPlan *S, const OpA32 &A, const OpG32 &G, const Vecs<float> &V,
                     const Work &W, const Ctl *ctl, cudaStream_t st) {
-  const Layout L = spmm_layouts(S, VEC, true).L, Lud = layouts_for(S, VU).Ld;
+  const Layout L = spmm_layouts(S, VEC, true).L, Ld = spmm_layouts(S, VEC, true).Ld;
+  const Layout Lu = layouts_for(S, VU).L, Lud = layouts_for(S, VU).Ld;
   switch (which) {
     case 0: k_spmm<float, VEC, 0><<<grid_of(L), BS, 0, st>>>(L, A, V.z, V.t, nullptr, W.cols, ctl); break;
     case 1: k_spmm<float, VEC, 0><<<grid_of(L), BS, 0, st>>>(L, G, V.p, V.T1, nullptr, W.cols, ctl); break;
+    case 4: k_spmm<float, VEC, 1><<<grid_of(Ld), BS, red_smem(Ld, 1), st>>>(Ld, A, V.p, V.v, V.p, W.cols, ctl); break;
+    case 5: k_spmm<float, VEC, 3><<<grid_of(Ld), BS, red_smem(Ld, 1), st>>>(Ld, G, V.r, V.T1, nullptr, W.cols, ctl); break;
+    case 6: k_update_r<float, VU><<<grid_of(Lud), BS, red_smem(Lud, 1), st>>>(Lud, V.r, V.v, W.cols, ctl); break;
+    case 7: k_update_px<float, VU><<<grid_of(Lu), BS, 0, st>>>(Lu, V.x, V.p, V.z, W.cols, ctl); break;
     case 2:
       k_update_xrp<float, VU><<<grid_of(Lud), BS, red_smem(Lud, 2), st>>>(Lud, V.x, V.h, V.z, V.r, V.s, V.t, V.p,
                                                                           V.v, V.rhat, W.cols, ctl);
@@ -2158,7 +2164,7 @@ void profile_launch(int which, const SolverPlan *S, const OpA32 &A, const OpG32 
 // CUDA events on `st`, and returns its algorithmic bytes per launch.
 int solver_profile(SolverPlan *S, int which, int reps, float *ms, double *bytes, cudaStream_t st) {
   DGP_REQUIRE(S->ws_prec == DGP_PREC_MIXED, "profile: run a mixed-precision solve first");
-  DGP_REQUIRE(reps >= 1 && which >= 0 && which <= 3, "profile: bad arguments");
+  DGP_REQUIRE(reps >= 1 && which >= 0 && which <= 7, "profile: bad arguments");
   Vecs<float> V = vec_views<float>(S);
   Work W = work_views(S);
   W.cols.hact = nullptr;  // timing / checking runs sweep every harmonic
@@ -2185,6 +2191,9 @@ int solver_profile(SolverPlan *S, int which, int reps, float *ms, double *bytes,
     case 0: *bytes = 2 * pass + (double)S->nf * (16.0 * S->nnz + 4.0 * (S->n + 1)); break;
     case 1: *bytes = 2 * pass + (double)S->nf * (16.0 * S->nnzG + 4.0 * (S->n + 1)); break;
     case 2: *bytes = 11 * pass; break;
+    case 4: *bytes = 3 * pass + (double)S->nf * (16.0 * S->nnz + 4.0 * (S->n + 1)); break;
+    case 5: *bytes = 2 * pass + (double)S->nf * (16.0 * S->nnzG + 4.0 * (S->n + 1)); break;
+    case 7: *bytes = 5 * pass; break;
     default: *bytes = 3 * pass; break;
   }
   launch();  // warm
@@ -2401,6 +2410,19 @@ int solver_set_spmm(SolverPlan *S, int32_t tiled, int32_t vec, int32_t rows) {
     S->tune_vec = vec;
     S->tune_rows = vec ? rows : 0;
   }
+  for (auto &g : S->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  for (int &gi : S->graph_iters) gi = 0;
+  return DGP_OK;
+}
+
+int solver_set_dot_rows(SolverPlan *S, int32_t mult) {
+  DGP_REQUIRE(mult == 0 || mult == 1 || mult == 2 || mult == 4 || mult == 8 || mult == 16,
+              "set_dot_rows: multiple must be 0 (default 16), 1, 2, 4, 8 or 16");
+  S->tune_dot = mult;
   for (auto &g : S->graph)
     if (g) {
       cudaGraphExecDestroy(g);

@@ -321,6 +321,11 @@ int dgp_solver_set_spmm(dgp_solver_t s, int32_t tiled, int32_t vec, int32_t rows
   DGP_GUARD(solver_set_spmm(&s->plan, tiled, vec, rows));
 }
 
+int dgp_solver_set_dot_rows(dgp_solver_t s, int32_t mult) {
+  if (!s) return fail(DGP_ERR_ARG, "solver_set_dot_rows: null handle");
+  DGP_GUARD(solver_set_dot_rows(&s->plan, mult));
+}
+
 int dgp_solver_check_spmm(dgp_solver_t s, double *max_rel, dgp_stream_t stream) {
   if (!s) return fail(DGP_ERR_ARG, "solver_check_spmm: null handle");
   DGP_GUARD(solver_check_spmm(&s->plan, max_rel, (cudaStream_t)stream));

@@ -254,6 +254,14 @@ int dgp_solver_autotune(dgp_solver_t solver, int32_t *tiled, int32_t *vec,
  * block (32, 64, 128, 256; 0 = 64). */
 int dgp_solver_set_spmm(dgp_solver_t solver, int32_t tiled, int32_t vec,
                         int32_t rows);
+/* Rows per block of the complex-FP32 SpMM sweeps that also reduce a dot
+ * product (v = A h with v.r^, the COCG sweeps q = A p with p.q and T = G r
+ * with T.T), as a multiple of the plain sweeps' rows per block: 1, 2, 4, 8
+ * or 16 (0 = default 4; at most 32 warp steps per block).  Taller blocks
+ * issue fewer FP64 atomics, shorter ones more blocks (at 153k nodes x 128
+ * harmonics: 4 and 2 give the shortest solve, 16 is 1 % slower, 1 is 6 %
+ * slower). */
+int dgp_solver_set_dot_rows(dgp_solver_t solver, int32_t mult);
 /* Self-check of the two SpMM kinds: applies A_k, G_k and G_k^T to one
  * deterministic test pattern with the gather and with the tiled kernel and
  * returns max |difference| / max |value| over all three (FP32 roundoff
@@ -293,7 +301,9 @@ int dgp_solve_sources(dgp_solver_t solver, const int32_t *d_nodes,
 
 /* Times one sweep kernel of the complex-FP32 iteration on the solver's
  * workspace with CUDA events on `stream` (which: 0 = t = A z SpMM,
- * 1 = G p SpMM, 2 = x/r/p update, 3 = h/s update) and returns the average
+ * 1 = G p SpMM, 2 = BiCGSTAB x/r/p update, 3 = h/s update, 4 = q = A p SpMM
+ * with p.q, 5 = T = G r SpMM with T.T, 6 = COCG r update, 7 = COCG x/p
+ * update) and returns the average
  * milliseconds per launch and the kernel's algorithmic bytes per launch.
  * Needs a prior DGP_PREC_MIXED solve; overwrites workspace vectors. */
 int dgp_solver_profile_kernel(dgp_solver_t solver, int32_t which, int32_t reps,
