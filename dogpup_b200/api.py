@@ -64,7 +64,7 @@ class Fem:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and lib is not None:  # lib is None during interpreter shutdown
             lib.dgp_fem_destroy(h)
             self._h = None
 
@@ -171,7 +171,7 @@ class Solver:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and lib is not None:  # lib is None during interpreter shutdown
             lib.dgp_solver_destroy(h)
             self._h = None
 
