@@ -240,7 +240,38 @@ def tg_jacobian_bench(reps=3):
     S64 = api.Solver(mesh.fem.rowptr, mesh.fem.col, mesh.K, mesh.M, mesh.optode.df / mesh.c, nf, 2)
     ref, _ = S64.solve_sources(nodes, wts, fpsf.contiguous(), api.make_opts(tol=1e-12, precision="fp64"))
     err = (torch.linalg.vector_norm(phi[:, :, :2] - ref, dim=1) / torch.linalg.vector_norm(ref, dim=1)).max()
-    del S64, ref
+    # detector data, TG data (2 sources x all detectors) and TG J entries (2 sources x 4
+    # detectors) of the mixed solve against FP64 fields to 1e-12
+    dn, dw = mesh._sources(mesh.optode.d_bary)
+    S64A = api.Solver(mesh.fem.rowptr, mesh.fem.col, mesh.K, mesh.M, mesh.optode.df / mesh.c, nf, 4)
+    dnodes4, dw4 = mesh._sources(mesh.optode.d_bary[:4])
+    refA, _ = S64A.solve_sources(dnodes4, dw4, fpsf.contiguous(), api.make_opts(tol=1e-12, precision="fp64"))
+    del S64A
+    lk = np.array([(s_, d_) for s_ in range(2) for d_ in range(nd)], dtype=np.int32)
+    lk_t = torch.as_tensor(lk, device="cuda")
+    phi2 = phi[:, :, :2].contiguous()
+    dm, dr = api.meas(dn, dw, lk_t, phi2), api.meas(dn, dw, lk_t, ref)
+    det_err = (torch.linalg.vector_norm(dm - dr, dim=1) / torch.linalg.vector_norm(dr, dim=1)).cpu().numpy()
+    tm, tr = api.fc2tg(dm, gfc, nt), api.fc2tg(dr, gfc, nt)
+    tg_err = (torch.linalg.vector_norm(tm - tr, dim=1) / torch.linalg.vector_norm(tr, dim=1)).cpu().numpy()
+    lj = torch.as_tensor(np.array([(s_, d_) for s_ in range(2) for d_ in range(4)], dtype=np.int32), device="cuda")
+    Jm = api.jacobian_tg(nb, phi2, phiA[:, :, :4].contiguous(), fpsf, lj, gfc, nt)
+    Jr = api.jacobian_tg(nb, ref, refA, fpsf, lj, gfc, nt)
+    j_err = float(torch.linalg.vector_norm(Jm.double() - Jr.double()) / torch.linalg.vector_norm(Jr.double()))
+    S8 = api.Solver(mesh.fem.rowptr, mesh.fem.col, mesh.K, mesh.M, mesh.optode.df / mesh.c, nf, 2)
+    ref8, _ = S8.solve_sources(nodes, wts, fpsf.contiguous(), api.make_opts(tol=1e-8, precision="fp64"))
+    d8 = api.meas(dn, dw, lk_t, ref8)
+    det_err8 = (torch.linalg.vector_norm(d8 - dr, dim=1) / torch.linalg.vector_norm(dr, dim=1)).cpu().numpy()
+    del S8, ref8
+    accuracy = {"fluence_per_rhs_max": float(err),
+                "fp64_to_1e-8_detector_data_per_link_median": float(np.median(det_err8)),
+                "fp64_to_1e-8_detector_data_per_link_max": float(det_err8.max()),
+                "detector_data_per_link_median": float(np.median(det_err)),
+                "detector_data_per_link_max": float(det_err.max()),
+                "tg_data_per_link_median": float(np.median(tg_err)), "tg_data_per_link_max": float(tg_err.max()),
+                "tg_jacobian_entries": j_err,
+                "sample": "sources 0-1 x all 32 detectors (J: detectors 0-3); mixed to 1e-8 vs FP64 to 1e-12"}
+    del S64, ref, refA, Jm, Jr
 
     # plain FP64, one right-hand side per solve, on this mesh (sampled harmonics, projected)
     plain = plain_fp64_per_rhs(mesh, nsample=4)
@@ -264,7 +295,7 @@ def tg_jacobian_bench(reps=3):
             "forward_and_adjoint_solve_s": round(t_solve, 3),
             "achieved_gbs": round((field_bytes + j_bytes) / (ms * 1e-3) / 1e9, 1),
             "achieved_tflops_fp32": round(flops / (ms * 1e-3) / 1e12, 2),
-            "mixed_fluence_rel_err_vs_fp64": float(err),
+            "mixed_fluence_rel_err_vs_fp64": float(err), "mixed_vs_fp64": accuracy,
             "headline": {"batched_mixed_forward_adjoint_tgJ_s": round(batched_s, 3),
                          "plain_fp64_per_rhs_s": round(plain_s, 3),
                          "plain_fp64_per_rhs_solves_per_s": round(plain_rate, 1),
@@ -314,11 +345,35 @@ def lm_step_bench(reps=2, grid_mm=2.0):
         check(lib.dgp_cholesky_solve(v(Hc), nv, nv, v(xc), api.stream_ptr()))
     ms_chol = _event_ms(chol, reps)
     syrk_flops = 3 * 2.0 * nmeas * nv * (nv + 128) / 2
+    # the same LM update from all-FP64 normal equations (cuBLAS DGEMM) and the FP64 Cholesky
+    Jd = Jt.double()
+    Jw = Jd * W[None, :]
+    H64 = Jw @ Jd.T
+    H64.diagonal().add_(1e-2 * H64.diagonal().max())
+    x64 = (Jw @ y).contiguous()
+    del Jw, Jd
+    H64 = H64.contiguous()
+    check(lib.dgp_cholesky_solve(v(H64), nv, nv, v(x64), api.stream_ptr()))
+    upd_err = float(torch.linalg.vector_norm(xc - x64) / torch.linalg.vector_norm(x64))
+    del H64
+    # DGEMM peak measured here: the denominator of the Cholesky's FP64 fraction
+    a = torch.randn((8192, 8192), dtype=torch.float64, device="cuda")
+    ms_dgemm = _event_ms(lambda: a @ a, 3)
+    dgemm_tf = 2.0 * 8192 ** 3 / (ms_dgemm * 1e-3) / 1e12
+    del a
+    pk = json.load(open(ROOT / "MEASURED_PEAKS.json")) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    bf16 = pk.get("bf16_tflops", 1590.0)
+    chol_tf = nv ** 3 / 3 / (ms_chol * 1e-3) / 1e12
+    syrk_tf = syrk_flops / (ms_ne * 1e-3) / 1e12
     return {"workload": f"cylinder r30 h60 @1.5mm, {mesh.nn} nodes, 32x32 optodes, 10 gates, {nv} voxels "
                         f"({grid_mm:g} mm)",
             "nmeas": nmeas, "nv": nv, "normal_eq_ms": round(ms_ne, 3), "cholesky_solve_ms": round(ms_chol, 3),
-            "syrk_tflops_bf16_lower_bound": round(syrk_flops / (ms_ne * 1e-3) / 1e12, 1),
-            "cholesky_tflops_fp64": round(nv ** 3 / 3 / (ms_chol * 1e-3) / 1e12, 2)}
+            "syrk_tflops_bf16_lower_bound": round(syrk_tf, 1),
+            "syrk_frac_of_bf16_peak": round(syrk_tf / bf16, 3),
+            "bf16_peak_source": "measured" if "bf16_tflops" in pk else "fallback",
+            "cholesky_tflops_fp64": round(chol_tf, 2), "dgemm_tflops_fp64_measured": round(dgemm_tf, 2),
+            "cholesky_frac_of_dgemm": round(chol_tf / dgemm_tf, 3),
+            "lm_update_rel_err_vs_fp64": upd_err}
 
 
 def lm_recon_bench(max_iter=10, grid_mm=2.0, seed=7):
