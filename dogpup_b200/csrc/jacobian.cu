@@ -21,7 +21,10 @@
 // all harmonics and optodes into shared memory once (FP64 sums, stored as
 // complex FP32), then each thread owns measurements m and accumulates all NG
 // gates in registers; consecutive threads write consecutive m (coalesced).
+// The time-gated form (k_jacobian_tg) blocks MT measurements per thread so that
+// each gate coefficient read from shared memory feeds MT complex products.
 #include <algorithm>
+#include <type_traits>
 
 #include "dgp_common.cuh"
 #include "dgp_internal.h"
@@ -151,6 +154,85 @@ __global__ void __launch_bounds__(JBS) k_jacobian(JArgs a, const float2 *__restr
   }
 }
 
+// Time-gated Jacobian with register blocking: a thread owns MT measurements (m = m0 + j*JBS)
+// and all NGC (>= ng, zero-padded) gates of each; per harmonic it forms the MT products
+// a_k(m) once and reads the gate coefficients C[k][0..NGC) as 128-bit shared loads, each
+// used for MT complex products (the DFT over harmonics is 2*MT*NGC FMAs per harmonic).
+template <int MT, int NGC>
+__global__ void __launch_bounds__(JBS) k_jacobian_tg(JArgs a, const float2 *__restrict__ Ckg /*[nf][NGC]*/,
+                                                     const double *__restrict__ rytov, float *__restrict__ Jtg) {
+  extern __shared__ float2 sh[];
+  float2 *Ps = sh;                         // [nf][ns]
+  float2 *Pd = Ps + a.nf * a.ns;           // [nf][nd]
+  float2 *Cs = Pd + a.nf * a.nd;           // [nf][NGC], 16-byte aligned (offset is even)
+  for (int t = threadIdx.x; t < a.nf * NGC; t += blockDim.x) Cs[t] = Ckg[t];
+  for (int64_t v = blockIdx.x; v < a.nv; v += gridDim.x) {
+    __syncthreads();
+    stage_field(a, v, a.phi, a.ns, Ps);
+    stage_field(a, v, a.phiA, a.nd, Pd);
+    __syncthreads();
+    const double wv = a.w ? a.w[v] : 1.0;
+    for (int m0 = 0; m0 < a.nm; m0 += JBS * MT) {
+      int sj[MT], dj[MT];
+#pragma unroll
+      for (int j = 0; j < MT; ++j) {
+        const int m = m0 + j * JBS + threadIdx.x;
+        const bool ok = m < a.nm;
+        sj[j] = ok ? a.link[2 * m] : 0;
+        dj[j] = ok ? a.link[2 * m + 1] : 0;
+      }
+      float acc[MT][NGC];
+#pragma unroll
+      for (int j = 0; j < MT; ++j)
+#pragma unroll
+        for (int g = 0; g < NGC; ++g) acc[j][g] = 0.f;
+#pragma unroll 1
+      for (int k = 0; k < a.nf; ++k) {
+        float ar[MT], ai[MT];
+#pragma unroll
+        for (int j = 0; j < MT; ++j) {
+          const float2 x = Ps[k * a.ns + sj[j]], y = Pd[k * a.nd + dj[j]];
+          ar[j] = x.x * y.x - x.y * y.y;
+          ai[j] = x.x * y.y + x.y * y.x;
+        }
+        const float4 *c4 = reinterpret_cast<const float4 *>(Cs + k * NGC);
+#pragma unroll
+        for (int g2 = 0; g2 < NGC / 2; ++g2) {
+          const float4 c = c4[g2];  // (C[k][2 g2], C[k][2 g2 + 1])
+#pragma unroll
+          for (int j = 0; j < MT; ++j) {
+            acc[j][2 * g2] = fmaf(c.x, ar[j], fmaf(-c.y, ai[j], acc[j][2 * g2]));
+            acc[j][2 * g2 + 1] = fmaf(c.z, ar[j], fmaf(-c.w, ai[j], acc[j][2 * g2 + 1]));
+          }
+        }
+      }
+      // epilogue in FP32 (the output precision): w_v scaling and the Rytov division
+      const float wf = (float)wv;
+#pragma unroll
+      for (int j = 0; j < MT; ++j) {
+        const int m = m0 + j * JBS + threadIdx.x;
+        if (m >= a.nm) continue;
+#pragma unroll
+        for (int g = 0; g < NGC; ++g) {
+          if (g < a.ng) {
+            float val = wf * acc[j][g];
+            if (rytov) val = val / (float)rytov[(int64_t)m * a.ng + g];
+            Jtg[((int64_t)v * a.ng + g) * a.nm + m] = val;
+          }
+        }
+      }
+    }
+  }
+}
+
+// Ckg[k][g] = C[g][k] for g < ng, 0 for ng <= g < ngc (the register-blocked kernel's layout)
+__global__ void k_ctab_kg(const float2 *__restrict__ C, int ng, int nf, int ngc, float2 *Ckg) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nf * ngc) return;
+  const int k = t / ngc, g = t % ngc;
+  Ckg[t] = g < ng ? C[g * nf + k] : make_float2(0.f, 0.f);
+}
+
 // C[g,k] = -2 Nt h_k conj(gate[g,k]) / fpsf[k]; also -1/fpsf[k] for the FD form
 __global__ void k_ctab(const double2 *__restrict__ gate, const double2 *__restrict__ fpsf, int ng, int nf, int nt,
                        float2 *C, double2 *finv) {
@@ -217,8 +299,35 @@ int jacobian_run(int mode, const int32_t *prow, const int32_t *pcol, const doubl
     DGP_CUDA(cudaFuncSetAttribute(k_jacobian<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   }
   if (mode == 0) {
-    k_jacobian<0><<<grid, JBS, smem, st>>>(a, ctab.as<float2>(), finv.as<double2>(), rytov, (float *)out, nullptr,
-                                           nullptr, nullptr);
+    // register-blocked TG kernel: gates padded to 8/16/24/32, MT measurements per thread
+    const int ngc = ng <= 8 ? 8 : ng <= 16 ? 16 : ng <= 24 ? 24 : 32;
+    // measurements per thread: 4 while the accumulators fit two blocks per SM (<= 16 gates), else 2
+    const int mt = (nm > 2 * JBS && ngc <= 16) ? 4 : nm > JBS ? 2 : 1;
+    DevBuf ckg;
+    DGP_TRY(ckg.alloc(sizeof(float2) * (size_t)nf * ngc));
+    k_ctab_kg<<<(unsigned)ceil_div((int64_t)nf * ngc, 256), 256, 0, st>>>(ctab.as<float2>(), ng, nf, ngc,
+                                                                          ckg.as<float2>());
+    DGP_CHECK_LAUNCH();
+    const size_t smem_tg = sizeof(float2) * ((size_t)nf * (ns + nd) + (size_t)nf * ngc);
+    DGP_REQUIRE(smem_tg <= 200 * 1024, "jacobian: NF*(NS+ND+NG) too large for one block's shared memory");
+    auto go = [&](auto mtc, auto ngcc) {
+      constexpr int MT_ = decltype(mtc)::value, NGC_ = decltype(ngcc)::value;
+      cudaFuncSetAttribute(k_jacobian_tg<MT_, NGC_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tg);
+      k_jacobian_tg<MT_, NGC_><<<grid, JBS, smem_tg, st>>>(a, ckg.as<float2>(), rytov, (float *)out);
+    };
+    auto by_ngc = [&](auto mtc) {
+      switch (ngc) {
+        case 8: go(mtc, std::integral_constant<int, 8>()); break;
+        case 16: go(mtc, std::integral_constant<int, 16>()); break;
+        case 24: go(mtc, std::integral_constant<int, 24>()); break;
+        default: go(mtc, std::integral_constant<int, 32>()); break;
+      }
+    };
+    if (mt == 4) by_ngc(std::integral_constant<int, 4>());
+    else if (mt == 2) by_ngc(std::integral_constant<int, 2>());
+    else by_ngc(std::integral_constant<int, 1>());
+    DGP_CHECK_LAUNCH();
+    DGP_CUDA(cudaStreamSynchronize(st));  // ckg is released on return
   } else if (mode == 1) {
     k_jacobian<1><<<grid, JBS, smem, st>>>(a, ctab.as<float2>(), finv.as<double2>(), nullptr, nullptr,
                                            (double2 *)out, nullptr, nullptr);

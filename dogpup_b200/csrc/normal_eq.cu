@@ -307,8 +307,10 @@ __global__ void k_damp(double *H, int64_t ldh, const double *__restrict__ diag, 
 
 // ------------------------------------------------------- FP64 Cholesky
 constexpr int NB = 64;
+// outer block width: the trailing DSYRK is rank-NBO (n = 22,971: 225.6 / 217.9 / 214.2 ms for
+// 256 / 512 / 1024)
 #ifndef DGP_CHOL_NBO
-#define DGP_CHOL_NBO 256
+#define DGP_CHOL_NBO 1024
 #endif
 
 // Factors the nb x nb (nb <= 64) diagonal block at k0 in place, one warp,
