@@ -76,79 +76,25 @@ __device__ void stage_field(const JArgs &a, int64_t v, const double2 *__restrict
   }
 }
 
-// MODE 0: time-gated Jacobian (float [nv][ng][nm]); MODE 1: complex FD Jacobian
-// (double2 [nv][nf][nm]); MODE 2: vector-Jacobian product out[v] (FP64).
-template <int MODE>
-__global__ void __launch_bounds__(JBS) k_jacobian(JArgs a, const float2 *__restrict__ Ctab,
-                                                  const double2 *__restrict__ fpsf_inv,
-                                                  const double *__restrict__ rytov, float *__restrict__ Jtg,
-                                                  double2 *__restrict__ Jfd, const float2 *__restrict__ Chat,
-                                                  double *__restrict__ vjp) {
+// Complex Jacobian J[v][k][m] (double2 [nv][nf][nm]): one block per voxel, threads over m.
+__global__ void __launch_bounds__(JBS) k_jacobian_complex(JArgs a, const double2 *__restrict__ fpsf_inv,
+                                                          double2 *__restrict__ Jfd) {
   extern __shared__ float2 sh[];
   float2 *Ps = sh;                         // [nf][ns]
   float2 *Pd = Ps + a.nf * a.ns;           // [nf][nd]
-  float2 *Cs = Pd + a.nf * a.nd;           // [ng][nf] (MODE 0)
-  if (MODE == 0)
-    for (int t = threadIdx.x; t < a.ng * a.nf; t += blockDim.x) Cs[t] = Ctab[t];
-  __shared__ double red[JBS / 32];
   for (int64_t v = blockIdx.x; v < a.nv; v += gridDim.x) {
     __syncthreads();
     stage_field(a, v, a.phi, a.ns, Ps);
     stage_field(a, v, a.phiA, a.nd, Pd);
     __syncthreads();
     const double wv = a.w ? a.w[v] : 1.0;
-    double part = 0.0;
     for (int m = threadIdx.x; m < a.nm; m += blockDim.x) {
       const int s = a.link[2 * m], d = a.link[2 * m + 1];
-      if (MODE == 0) {
-        float acc[NGMAX];
-#pragma unroll
-        for (int g = 0; g < NGMAX; ++g) acc[g] = 0.f;
-        for (int k = 0; k < a.nf; ++k) {
-          float2 x = Ps[k * a.ns + s], y = Pd[k * a.nd + d];
-          float ar = x.x * y.x - x.y * y.y, ai = x.x * y.y + x.y * y.x;
-#pragma unroll
-          for (int g = 0; g < NGMAX; ++g) {
-            if (g < a.ng) {
-              float2 c = Cs[g * a.nf + k];
-              acc[g] = fmaf(c.x, ar, fmaf(-c.y, ai, acc[g]));
-            }
-          }
-        }
-#pragma unroll
-        for (int g = 0; g < NGMAX; ++g) {
-          if (g < a.ng) {
-            double val = wv * (double)acc[g];
-            if (rytov) val /= rytov[(int64_t)m * a.ng + g];
-            Jtg[((int64_t)v * a.ng + g) * a.nm + m] = (float)val;
-          }
-        }
-      } else if (MODE == 1) {
-        for (int k = 0; k < a.nf; ++k) {
-          float2 x = Ps[k * a.ns + s], y = Pd[k * a.nd + d];
-          double2 p = make_double2((double)x.x * y.x - (double)x.y * y.y, (double)x.x * y.y + (double)x.y * y.x);
-          double2 r = cmul(p, fpsf_inv[k]);  // -1 / s_fpsf[k]
-          Jfd[((int64_t)v * a.nf + k) * a.nm + m] = make_double2(wv * r.x, wv * r.y);
-        }
-      } else {
-        double acc = 0.0;
-        for (int k = 0; k < a.nf; ++k) {
-          float2 x = Ps[k * a.ns + s], y = Pd[k * a.nd + d];
-          float ar = x.x * y.x - x.y * y.y, ai = x.x * y.y + x.y * y.x;
-          float2 c = Chat[(int64_t)m * a.nf + k];
-          acc += (double)(c.x * ar - c.y * ai);
-        }
-        part += acc;
-      }
-    }
-    if (MODE == 2) {
-      for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(0xffffffffu, part, off);
-      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        double tot = 0.0;
-        for (int q = 0; q < JBS / 32; ++q) tot += red[q];
-        vjp[v] = wv * tot;
+      for (int k = 0; k < a.nf; ++k) {
+        float2 x = Ps[k * a.ns + s], y = Pd[k * a.nd + d];
+        double2 p = make_double2((double)x.x * y.x - (double)x.y * y.y, (double)x.x * y.y + (double)x.y * y.x);
+        double2 r = cmul(p, fpsf_inv[k]);  // -1 / s_fpsf[k]
+        Jfd[((int64_t)v * a.nf + k) * a.nm + m] = make_double2(wv * r.x, wv * r.y);
       }
     }
   }
@@ -225,6 +171,59 @@ __global__ void __launch_bounds__(JBS) k_jacobian_tg(JArgs a, const float2 *__re
   }
 }
 
+// Vector-Jacobian product out[v] = w_v sum_m sum_k Re(Chat[m,k] a_k(m)) for VB voxels per block
+// pass: the fields of VB voxels are staged together, so each Chat[m,k] read from global memory
+// (L2) serves VB voxels.
+template <int VB>
+__global__ void __launch_bounds__(JBS) k_jacobian_vjp(JArgs a, const float2 *__restrict__ Chat,
+                                                      double *__restrict__ vjp) {
+  extern __shared__ float2 sh[];
+  const int per = a.nf * (a.ns + a.nd);
+  __shared__ double red[JBS / 32][VB];
+  for (int64_t v0 = (int64_t)blockIdx.x * VB; v0 < a.nv; v0 += (int64_t)gridDim.x * VB) {
+    __syncthreads();
+#pragma unroll
+    for (int b = 0; b < VB; ++b) {
+      if (v0 + b >= a.nv) break;
+      stage_field(a, v0 + b, a.phi, a.ns, sh + b * per);
+      stage_field(a, v0 + b, a.phiA, a.nd, sh + b * per + a.nf * a.ns);
+    }
+    __syncthreads();
+    double part[VB];
+#pragma unroll
+    for (int b = 0; b < VB; ++b) part[b] = 0.0;
+    for (int m = threadIdx.x; m < a.nm; m += blockDim.x) {
+      const int s = a.link[2 * m], d = a.link[2 * m + 1];
+      double acc[VB];
+#pragma unroll
+      for (int b = 0; b < VB; ++b) acc[b] = 0.0;
+      for (int k = 0; k < a.nf; ++k) {
+        const float2 c = Chat[(int64_t)m * a.nf + k];
+#pragma unroll
+        for (int b = 0; b < VB; ++b) {
+          const float2 x = sh[b * per + k * a.ns + s], y = sh[b * per + a.nf * a.ns + k * a.nd + d];
+          const float ar = x.x * y.x - x.y * y.y, ai = x.x * y.y + x.y * y.x;
+          acc[b] += (double)(c.x * ar - c.y * ai);
+        }
+      }
+#pragma unroll
+      for (int b = 0; b < VB; ++b) part[b] += acc[b];
+    }
+#pragma unroll
+    for (int b = 0; b < VB; ++b) {
+      double q = part[b];
+      for (int off = 16; off > 0; off >>= 1) q += __shfl_xor_sync(0xffffffffu, q, off);
+      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][b] = q;
+    }
+    __syncthreads();
+    if (threadIdx.x < VB && v0 + threadIdx.x < a.nv) {
+      double tot = 0.0;
+      for (int q = 0; q < JBS / 32; ++q) tot += red[q][threadIdx.x];
+      vjp[v0 + threadIdx.x] = (a.w ? a.w[v0 + threadIdx.x] : 1.0) * tot;
+    }
+  }
+}
+
 // Ckg[k][g] = C[g][k] for g < ng, 0 for ng <= g < ngc (the register-blocked kernel's layout)
 __global__ void k_ctab_kg(const float2 *__restrict__ C, int ng, int nf, int ngc, float2 *Ckg) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -293,11 +292,8 @@ int jacobian_run(int mode, const int32_t *prow, const int32_t *pcol, const doubl
   k_ctab<<<(unsigned)ceil_div(nt_, 256), 256, 0, st>>>((const double2 *)gate, (const double2 *)fpsf, mode == 1 ? 0 : ng,
                                                         nf, nt, ctab.as<float2>(), finv.as<double2>());
   DGP_CHECK_LAUNCH();
-  if (smem > 48 * 1024) {
-    DGP_CUDA(cudaFuncSetAttribute(k_jacobian<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    DGP_CUDA(cudaFuncSetAttribute(k_jacobian<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    DGP_CUDA(cudaFuncSetAttribute(k_jacobian<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  }
+  if (smem > 48 * 1024)
+    DGP_CUDA(cudaFuncSetAttribute(k_jacobian_complex, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   if (mode == 0) {
     // register-blocked TG kernel: gates padded to 8/16/24/32, MT measurements per thread
     const int ngc = ng <= 8 ? 8 : ng <= 16 ? 16 : ng <= 24 ? 24 : 32;
@@ -329,16 +325,27 @@ int jacobian_run(int mode, const int32_t *prow, const int32_t *pcol, const doubl
     DGP_CHECK_LAUNCH();
     DGP_CUDA(cudaStreamSynchronize(st));  // ckg is released on return
   } else if (mode == 1) {
-    k_jacobian<1><<<grid, JBS, smem, st>>>(a, ctab.as<float2>(), finv.as<double2>(), nullptr, nullptr,
-                                           (double2 *)out, nullptr, nullptr);
+    k_jacobian_complex<<<grid, JBS, smem, st>>>(a, finv.as<double2>(), (double2 *)out);
   } else {
     DGP_REQUIRE(gin, "jacobian vjp: null upstream gradient");
     DGP_TRY(chat.alloc(sizeof(float2) * (size_t)nm * nf));
     k_chat<<<(unsigned)ceil_div((int64_t)nm * nf, 256), 256, 0, st>>>(gin, ctab.as<float2>(), rytov, nm, ng, nf,
                                                                       chat.as<float2>());
     DGP_CHECK_LAUNCH();
-    k_jacobian<2><<<grid, JBS, smem, st>>>(a, ctab.as<float2>(), finv.as<double2>(), nullptr, nullptr, nullptr,
-                                           chat.as<float2>(), (double *)out);
+    // voxels per block pass: as many as 200 KB of staged fields allow, up to 4
+    const size_t per = sizeof(float2) * (size_t)nf * (ns + nd);
+    const int vb = (int)std::min<size_t>(4, std::max<size_t>(1, (200 * 1024) / per));
+    const size_t smem_v = per * vb;
+    auto go = [&](auto vbc) {
+      constexpr int VB_ = decltype(vbc)::value;
+      cudaFuncSetAttribute(k_jacobian_vjp<VB_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_v);
+      const int gv = (int)std::min<int64_t>(ceil_div(nv, VB_), (int64_t)sm_count() * 8);
+      k_jacobian_vjp<VB_><<<gv, JBS, smem_v, st>>>(a, chat.as<float2>(), (double *)out);
+    };
+    if (vb >= 4) go(std::integral_constant<int, 4>());
+    else if (vb == 3) go(std::integral_constant<int, 3>());
+    else if (vb == 2) go(std::integral_constant<int, 2>());
+    else go(std::integral_constant<int, 1>());
   }
   DGP_CHECK_LAUNCH();
   DGP_CUDA(cudaStreamSynchronize(st));  // scratch tables are released on return
