@@ -142,6 +142,7 @@ class Clocks:
 
 # ------------------------------------------------------------- CPU baseline
 def cpu_sample(w, harmonics=(1, 64), tol=1e-8):
+    harmonics = tuple(sorted({min(k, w["nf"] - 1) for k in harmonics}))
     """The reference algorithm on the host: FP64 FSAI + BiCGSTAB (dMesh.m:1247-1385)
     restated in C with OpenMP (oracle/cport), on a bounded sample of the workload --
     all sources x the given harmonics on the same mesh and properties.  The FSAI
@@ -149,6 +150,8 @@ def cpu_sample(w, harmonics=(1, 64), tol=1e-8):
     workload's NS*NF right-hand sides, as in one GPU step."""
     import scipy.sparse as sp
     from oracle import cport, fem, solver
+    from oracle.optode import snap_pos
+    from dogpup_b200.dmesh import surface_faces
     from dogpup_b200.optode import locate_points
     m = w["mesh"]
     t0 = time.perf_counter()
@@ -157,8 +160,12 @@ def cpu_sample(w, harmonics=(1, 64), tol=1e-8):
     t_asm = time.perf_counter() - t0
     dfc = (2 * np.pi / w["t"][-1]) / geo["c"]
     ns = len(w["src"])
-    c = m.node.mean(axis=0)
-    eid, bw = locate_points(m.node, m.elem, c + 0.97 * (w["src"] - c))   # sources just inside the surface
+    # sources as snap2mesh places them (dOptode.m:77-97): nearest surface point, moved
+    # 1/min(musp) inward along the face normal, then located
+    spos, sdir, _, _ = snap_pos(m.node, geo["bnd"], surface_faces(m.node, m.elem), w["src"])
+    eid, bw = locate_points(m.node, m.elem, spos + (1.0 / float(np.min(w["musp"]))) * sdir)
+    bw = np.where(bw < 1e-10, 0.0, bw)
+    bw = bw / bw.sum(axis=1, keepdims=True)
     rg, cg = solver.fsai_pattern(sp.tril(K + 1j * dfc * M).tocsr())
     rt, ct, perm = solver.transpose_pattern(rg, cg, K.shape[0])
     Kt = sp.tril(K).tocsr()
