@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--lm-grid-mm", type=float, default=2.0, help="voxel pitch of the LM step's Jacobian basis")
     ap.add_argument("--order", choices=["morton", "lattice"], default="morton", help="mesh node numbering")
     ap.add_argument("--no-autotune", action="store_true", help="keep the built-in SpMM launch shape")
+    ap.add_argument("--clock-ms", type=int, default=200, help="nvidia-smi sampling interval in the timed region")
     ap.add_argument("--spmm-vec", type=int, default=0, help="with --no-autotune: gather SpMM complex values per lane")
     ap.add_argument("--spmm-rows", type=int, default=0, help="with --no-autotune: gather SpMM rows per block")
     return ap.parse_args()
@@ -80,14 +81,14 @@ class Clocks:
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index):
+    def __init__(self, index, interval_ms=200):
         # nvidia-smi numbers the physical GPUs; CUDA numbers the visible ones
         vis = [v.strip() for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
         self.index = vis[index] if index < len(vis) else str(index)
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", self.index, f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                       "--format=csv,noheader,nounits", "-lms", str(int(interval_ms))],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except FileNotFoundError:
             self.p = None
@@ -598,7 +599,7 @@ def run_ours(a, rank, world, local_rank):
             f"{rep.refinements} ref, res {rep.max_rel_residual:.2e}, mem {solver.memory() / 1e9:.1f} GB")
     # the sampler starts before the timed region (nvidia-smi's start-up talks to the driver and
     # would stall the first timed launches) and keeps sampling through it
-    clk = Clocks(torch.cuda.current_device()) if rank == 0 else None
+    clk = Clocks(torch.cuda.current_device(), a.clock_ms) if rank == 0 else None
     if clk:
         clk.wait_ready()
     if world > 1:
