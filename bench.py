@@ -364,6 +364,12 @@ def lm_step_bench(reps=2, grid_mm=2.0):
     check(lib.dgp_cholesky_solve(v(H64), nv, nv, v(x64), api.stream_ptr()))
     upd_err = float(torch.linalg.vector_norm(xc - x64) / torch.linalg.vector_norm(x64))
     del H64
+    # the same update in one call in the smaller (measurements') form: dgp_lm_update
+    xu = torch.empty(nv, dtype=torch.float64, device="cuda")
+    used = C.c_int32(0)
+    ms_upd = _event_ms(lambda: check(lib.dgp_lm_update(v(Jt), nv, nmeas, v(W), v(y), 1e-2, v(xu), 0, C.byref(used),
+                                                       api.stream_ptr())), reps)
+    upd_err_u = float(torch.linalg.vector_norm(xu - x64) / torch.linalg.vector_norm(x64))
     # DGEMM peak measured here: the denominator of the Cholesky's FP64 fraction
     a = torch.randn((8192, 8192), dtype=torch.float64, device="cuda")
     ms_dgemm = _event_ms(lambda: a @ a, 3)
@@ -381,7 +387,11 @@ def lm_step_bench(reps=2, grid_mm=2.0):
             "bf16_peak_source": "measured" if "bf16_tflops" in pk else "fallback",
             "cholesky_tflops_fp64": round(chol_tf, 2), "dgemm_tflops_fp64_measured": round(dgemm_tf, 2),
             "cholesky_frac_of_dgemm": round(chol_tf / dgemm_tf, 3),
-            "lm_update_rel_err_vs_fp64": upd_err}
+            "lm_update_rel_err_vs_fp64": upd_err,
+            "lm_update_one_call": {"ms": round(ms_upd, 3), "form": "measurements" if used.value == 2 else "unknowns",
+                                   "rel_err_vs_fp64": upd_err_u,
+                                   "note": "dgp_lm_update: J_w^T (J_w J_w^T + mu I)^-1 W^1/2 y, the same update "
+                                           "as the nv x nv normal equations above"}}
 
 
 def lm_recon_bench(max_iter=10, grid_mm=2.0, seed=7):

@@ -82,6 +82,8 @@ _SIGS = {
     "dgp_normal_eq": (C.c_int, [P, I64, I64, P, P, D, I32, P, I64, P, P]),
     "dgp_cholesky_solve": (C.c_int, [P, I64, I64, P, P]),
     "dgp_cholesky_solve_many": (C.c_int, [P, I64, I64, P, I32, I64, P]),
+    "dgp_row_dots": (C.c_int, [P, I64, I64, P, P, P, P, P]),
+    "dgp_lm_update": (C.c_int, [P, I64, I64, P, P, D, P, I32, P, P]),
     "dgp_jacobian_complex":(C.c_int, [P, P, P, I64, P, P, I32, P, I32, I64, I32, P, P, I32, P, P]),
     "dgp_jacobian_tg": (C.c_int, [P, P, P, I64, P, P, I32, P, I32, I64, I32, P, P, I32, P, I32, I32, P, P, P]),
     "dgp_jacobian_tg_vjp": (C.c_int, [P, P, P, I64, P, P, I32, P, I32, I64, I32, P, P, I32, P, I32, I32, P, P, P,

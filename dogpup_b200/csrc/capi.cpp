@@ -87,6 +87,10 @@ int jacobian_run(int mode, const int32_t *prow, const int32_t *pcol, const doubl
 int normal_eq_run(const float *Jt, int64_t nv, int64_t nm, const double *W, const double *y, double lam, int mode,
                   double *H, int64_t ldh, double *rhs, cudaStream_t st);
 int cholesky_solve_run(double *H, int64_t n, int64_t ldh, double *x, cudaStream_t st);
+int row_dots_run(const float *Jt, int64_t nv, int64_t nm, const double *W, const double *y, double *diag, double *rhs,
+                 cudaStream_t st);
+int lm_update_run(const float *Jt, int64_t nv, int64_t nm, const double *W, const double *y, double lam, double *x,
+                  int32_t form, int32_t *form_used, cudaStream_t st);
 int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_t nrhs, int64_t ldx,
                             cudaStream_t st);
 
@@ -462,6 +466,16 @@ int dgp_normal_eq(const float *d_Jt, int64_t nv, int64_t nmeas, const double *d_
 
 int dgp_cholesky_solve(double *d_H, int64_t n, int64_t ldh, double *d_x, dgp_stream_t stream) {
   DGP_GUARD(cholesky_solve_run(d_H, n, ldh, d_x, (cudaStream_t)stream));
+}
+
+int dgp_row_dots(const float *d_Jt, int64_t nv, int64_t nmeas, const double *d_w, const double *d_y, double *d_diag,
+                 double *d_rhs, dgp_stream_t stream) {
+  DGP_GUARD(row_dots_run(d_Jt, nv, nmeas, d_w, d_y, d_diag, d_rhs, (cudaStream_t)stream));
+}
+
+int dgp_lm_update(const float *d_Jt, int64_t nv, int64_t nmeas, const double *d_w, const double *d_y, double lambda,
+                  double *d_x, int32_t form, int32_t *form_used, dgp_stream_t stream) {
+  DGP_GUARD(lm_update_run(d_Jt, nv, nmeas, d_w, d_y, lambda, d_x, form, form_used, (cudaStream_t)stream));
 }
 
 int dgp_cholesky_solve_many(double *d_H, int64_t n, int64_t ldh, double *d_X, int32_t nrhs, int64_t ldx,

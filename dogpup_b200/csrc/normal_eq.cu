@@ -43,6 +43,7 @@
 #include <cmath>
 #include <map>
 #include <mutex>
+#include <vector>
 
 #include "dgp_common.cuh"
 #include "dgp_internal.h"
@@ -292,7 +293,7 @@ __global__ void k_row_dots(const float *__restrict__ Jt, const double *__restric
   }
 }
 
-// H_ii = d_i + lam * (mode 0: max_j d_j, the tik_inv rule; mode 1: d_i)
+// H_ii = d_i + lam * (mode 0: max_j d_j, the tik_inv rule; mode 1: d_i; mode 2: 1)
 __global__ void k_damp(double *H, int64_t ldh, const double *__restrict__ diag, int64_t nv, double lam, int mode) {
   __shared__ double smax;
   if (threadIdx.x == 0) {
@@ -302,7 +303,7 @@ __global__ void k_damp(double *H, int64_t ldh, const double *__restrict__ diag, 
   }
   __syncthreads();
   for (int64_t i = threadIdx.x; i < nv; i += blockDim.x)
-    H[i * ldh + i] = diag[i] + lam * (mode == 0 ? smax : diag[i]);
+    H[i * ldh + i] = diag[i] + lam * (mode == 0 ? smax : mode == 1 ? diag[i] : 1.0);
 }
 
 // ------------------------------------------------------- FP64 Cholesky
@@ -377,7 +378,8 @@ int normal_eq_run(const float *Jt, int64_t nv, int64_t nm, const double *W, cons
                   double *H, int64_t ldh, double *rhs, cudaStream_t st) {
   DGP_REQUIRE(Jt && H, "normal_eq: null pointer");
   DGP_REQUIRE(nv > 0 && nm > 0 && ldh >= nv, "normal_eq: bad sizes");
-  DGP_REQUIRE(mode == 0 || mode == 1, "normal_eq: damping mode is 0 (lam*max diag) or 1 (lam*diag)");
+  DGP_REQUIRE(mode == 0 || mode == 1 || mode == 2,
+              "normal_eq: damping mode is 0 (lam*max diag), 1 (lam*diag) or 2 (lam)");
   const int64_t nvp = ceil_div(nv, TM) * TM, nmp = ceil_div(nm, TK) * TK;
   DGP_REQUIRE(nmp < (int64_t)INT32_MAX && nvp < (int64_t)INT32_MAX, "normal_eq: sizes exceed TMA coordinates");
   DevBuf hi, lo, diag, errb;
@@ -505,6 +507,86 @@ int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_
   DGP_CUDA(cudaMemcpyAsync(&herr, errb.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   DGP_CUDA(cudaStreamSynchronize(st));
   if (herr) return fail(DGP_ERR_ARG, "cholesky: matrix is not positive definite");
+  return DGP_OK;
+}
+
+// ----------------------------------------------------- tik_inv update
+namespace {
+
+// Jw[m][v] = sqrt(W[m]) Jt[v][m]: 32 x 32 tiles through shared memory
+__global__ void k_scale_transpose(const float *__restrict__ Jt, const double *__restrict__ W, int64_t nv, int64_t nm,
+                                  float *__restrict__ Jw) {
+  __shared__ float t[32][33];
+  const int64_t v0 = (int64_t)blockIdx.y * 32, m0 = (int64_t)blockIdx.x * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int64_t v = v0 + r, m = m0 + threadIdx.x;
+    t[r][threadIdx.x] = (v < nv && m < nm) ? Jt[v * nm + m] : 0.f;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int64_t m = m0 + r, v = v0 + threadIdx.x;
+    if (m < nm && v < nv) Jw[m * nv + v] = (W ? (float)sqrt(W[m]) : 1.f) * t[threadIdx.x][r];
+  }
+}
+
+// out[m] = sqrt(W[m]) in[m]
+__global__ void k_scale_sqrtw(const double *in, const double *__restrict__ W, int64_t nm, double *out) {
+  const int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (m < nm) out[m] = (W ? sqrt(W[m]) : 1.0) * in[m];
+}
+
+}  // namespace
+
+int row_dots_run(const float *Jt, int64_t nv, int64_t nm, const double *W, const double *y, double *diag, double *rhs,
+                 cudaStream_t st) {
+  DGP_REQUIRE(Jt && diag && nv > 0 && nm > 0, "row_dots: bad arguments");
+  k_row_dots<<<(unsigned)std::min<int64_t>(nv, 4096), 256, 0, st>>>(Jt, W, y, nv, nm, diag, rhs);
+  DGP_CHECK_LAUNCH();
+  return DGP_OK;
+}
+
+// update = (J^T W J + lam max_i (J^T W J)_ii I)^-1 J^T W y  (tik_inv.m:13-20 with W).  With fewer
+// measurements than unknowns the same update is J_w^T (J_w J_w^T + mu I)^-1 W^1/2 y with
+// J_w = W^1/2 J and mu = lam max_i (J^T W J)_ii: the Gram matrix and the factorisation are
+// nmeas x nmeas instead of nv x nv.
+int lm_update_run(const float *Jt, int64_t nv, int64_t nm, const double *W, const double *y, double lam, double *x,
+                  int32_t form, int32_t *form_used, cudaStream_t st) {
+  DGP_REQUIRE(Jt && y && x && nv > 0 && nm > 0, "lm_update: bad arguments");
+  DGP_REQUIRE(form >= 0 && form <= 2, "lm_update: form is 0 (auto), 1 (unknowns) or 2 (measurements)");
+  const bool dual = form == 2 || (form == 0 && nm < nv);
+  if (form_used) *form_used = dual ? 2 : 1;
+  if (!dual) {
+    DevBuf H;
+    DGP_TRY(H.alloc(sizeof(double) * (size_t)nv * nv));
+    DGP_TRY(normal_eq_run(Jt, nv, nm, W, y, lam, 0, H.as<double>(), nv, x, st));
+    return cholesky_solve_run(H.as<double>(), nv, nv, x, st);
+  }
+  DevBuf diag, Jw, G, z;
+  DGP_TRY(diag.alloc(sizeof(double) * nv));
+  DGP_TRY(Jw.alloc(sizeof(float) * (size_t)nm * nv));
+  DGP_TRY(G.alloc(sizeof(double) * (size_t)nm * nm));
+  DGP_TRY(z.alloc(sizeof(double) * nm));
+  DGP_TRY(row_dots_run(Jt, nv, nm, W, nullptr, diag.as<double>(), nullptr, st));
+  std::vector<double> hd((size_t)nv);
+  DGP_CUDA(cudaMemcpyAsync(hd.data(), diag.p, sizeof(double) * nv, cudaMemcpyDeviceToHost, st));
+  DGP_CUDA(cudaStreamSynchronize(st));
+  double dmax = 0.0;
+  for (double d : hd) dmax = std::max(dmax, d);
+  const double mu = lam * dmax;
+  dim3 tb(32, 8), tg((unsigned)ceil_div(nm, 32), (unsigned)ceil_div(nv, 32));
+  DGP_REQUIRE(tg.y <= 65535u, "lm_update: too many unknowns for the transpose grid");
+  k_scale_transpose<<<tg, tb, 0, st>>>(Jt, W, nv, nm, Jw.as<float>());
+  DGP_CHECK_LAUNCH();
+  // G = J_w J_w^T + mu I: the split-BF16 Gram kernel on J_w (rows = measurements)
+  DGP_TRY(normal_eq_run(Jw.as<float>(), nm, nv, nullptr, nullptr, mu, 2, G.as<double>(), nm, nullptr, st));
+  k_scale_sqrtw<<<(unsigned)ceil_div(nm, 256), 256, 0, st>>>(y, W, nm, z.as<double>());
+  DGP_CHECK_LAUNCH();
+  DGP_TRY(cholesky_solve_run(G.as<double>(), nm, nm, z.as<double>(), st));
+  k_scale_sqrtw<<<(unsigned)ceil_div(nm, 256), 256, 0, st>>>(z.as<double>(), W, nm, z.as<double>());
+  DGP_CHECK_LAUNCH();
+  // x = J^T (W^1/2 z)
+  DGP_TRY(row_dots_run(Jt, nv, nm, nullptr, z.as<double>(), diag.as<double>(), x, st));
+  DGP_CUDA(cudaStreamSynchronize(st));
   return DGP_OK;
 }
 

@@ -142,12 +142,13 @@ class LMRecon:
         """update = (J^T W J + lam * max diag)^-1 J^T W y  (tik_inv.m:13-20)."""
         nv = Jt.shape[0]
         if self.normal_eq == "split_bf16":
+            # split-BF16 Gram + FP64 Cholesky of the smaller of the two equivalent systems
             Jf = Jt.to(torch.float32).contiguous()
-            H = torch.empty((nv, nv), dtype=torch.float64, device="cuda")
             x = torch.empty(nv, dtype=torch.float64, device="cuda")
             v = lambda t: C.c_void_p(t.data_ptr())
-            check(lib.dgp_normal_eq(v(Jf), nv, Jf.shape[1], None if w is None else v(w), v(y), float(lam), 0, v(H),
-                                    nv, v(x), api.stream_ptr()))
+            check(lib.dgp_lm_update(v(Jf), nv, Jf.shape[1], None if w is None else v(w), v(y), float(lam), v(x), 0,
+                                    None, api.stream_ptr()))
+            return x
         else:
             Jd = Jt.to(torch.float64)
             Jw = Jd if w is None else Jd * w[None, :]

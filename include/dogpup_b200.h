@@ -459,11 +459,11 @@ int dgp_grid_to_mesh(const double *d_node, int64_t nn, const double *origin,
  *  Levenberg-Marquardt normal equations (tik_inv, reconstruction/
  *  tik_inv.m:1-20, with a diagonal data weight W = 1/sigma^2).
  * ====================================================================== */
-enum { DGP_DAMP_MAX_DIAG = 0, DGP_DAMP_DIAG = 1 };
+enum { DGP_DAMP_MAX_DIAG = 0, DGP_DAMP_DIAG = 1, DGP_DAMP_ADD = 2 };
 /* H = J^T W J (lower triangle of d_H [nv][ldh] in FP64, from split-BF16
  * tensor-core products with FP32 accumulation), H_ii = (J^T W J)_ii (exact
  * FP64) + lambda * (max_j (J^T W J)_jj for DGP_DAMP_MAX_DIAG, the tik_inv
- * rule; (J^T W J)_ii for DGP_DAMP_DIAG), and d_rhs = J^T W y (FP64) when
+ * rule; (J^T W J)_ii for DGP_DAMP_DIAG; 1 for DGP_DAMP_ADD), and d_rhs = J^T W y (FP64) when
  * d_y and d_rhs are not NULL.  d_Jt is J transposed, [nv][nmeas] float32
  * (the dgp_jacobian_tg output); d_w [nmeas] or NULL (W = I).  The strict
  * upper triangle of d_H is not written. */
@@ -475,6 +475,21 @@ int dgp_normal_eq(const float *d_Jt, int64_t nv, int64_t nmeas, const double *d_
  * Returns DGP_ERR_ARG if H is not positive definite. */
 int dgp_cholesky_solve(double *d_H, int64_t n, int64_t ldh, double *d_x,
                        dgp_stream_t stream);
+/* d_diag[v] = sum_m w_m Jt[v][m]^2 and, when d_y and d_rhs are not NULL,
+ * d_rhs[v] = sum_m Jt[v][m] w_m y_m (FP64 sums; d_w NULL = 1): the diagonal of
+ * J^T W J and J^T W y without forming J^T W J. */
+int dgp_row_dots(const float *d_Jt, int64_t nv, int64_t nmeas, const double *d_w,
+                 const double *d_y, double *d_diag, double *d_rhs, dgp_stream_t stream);
+/* The tik_inv update (reconstruction/tik_inv.m:13-20, with a diagonal data
+ * weight W): d_x = (J^T W J + lambda max_i (J^T W J)_ii I)^-1 J^T W y.
+ * form 1 factors the nv x nv system (dgp_normal_eq + dgp_cholesky_solve);
+ * form 2 the nmeas x nmeas one, J_w^T (J_w J_w^T + mu I)^-1 W^1/2 y with
+ * J_w = W^1/2 J and mu = lambda max_i (J^T W J)_ii (the same update, far less
+ * work when nmeas < nv); form 0 picks the smaller.  *form_used (may be NULL)
+ * reports 1 or 2.  Allocates its work arrays; synchronises the stream. */
+int dgp_lm_update(const float *d_Jt, int64_t nv, int64_t nmeas, const double *d_w,
+                  const double *d_y, double lambda, double *d_x, int32_t form,
+                  int32_t *form_used, dgp_stream_t stream);
 /* dgp_cholesky_solve for nrhs right-hand sides: row r of d_X [nrhs][ldx]
  * (ldx >= n) is b_r in and x_r out; one factorisation, one DTRSM pair.
  * Used for reshape_J's w = (Js J^T)(J J^T + lam max diag I)^-1

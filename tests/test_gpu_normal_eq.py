@@ -119,3 +119,26 @@ def test_lm_step_against_fp64_tik_inv():
     check(lib.dgp_cholesky_solve(_v(H), nv, nv, _v(x), None))
     u0 = tik_inv(Jt.cpu().numpy().T.astype(np.float64), lam, y, weights=W)
     assert np.linalg.norm(x.cpu().numpy() - u0) / np.linalg.norm(u0) < 1e-3
+
+
+@pytest.mark.parametrize("nv,nm", [(1500, 700), (400, 2048)])
+def test_lm_update_both_forms_match_tik_inv(nv, nm):
+    """dgp_lm_update in the unknowns' form (nv x nv) and the measurements' form
+    (nmeas x nmeas, J_w^T (J_w J_w^T + mu I)^-1 W^1/2 y) gives tik_inv's update
+    with W within 1e-3; form 0 picks the smaller system."""
+    import ctypes as C
+    import torch
+    from dogpup_b200._lib import lib, check
+    from oracle.jacobian import tik_inv
+    J, W, y = _case(nv, nm, 11)
+    Jt = torch.as_tensor(np.ascontiguousarray(J.T), dtype=torch.float32, device="cuda")
+    Wd = torch.as_tensor(W, device="cuda")
+    yd = torch.as_tensor(y, device="cuda")
+    lam = 1e-2
+    u0 = tik_inv(Jt.cpu().numpy().T.astype(np.float64), lam, y, weights=W)
+    for form in (1, 2, 0):
+        x = torch.zeros(nv, dtype=torch.float64, device="cuda")
+        used = C.c_int32(-1)
+        check(lib.dgp_lm_update(_v(Jt), nv, nm, _v(Wd), _v(yd), lam, _v(x), form, C.byref(used), None))
+        assert used.value == (form if form else (2 if nm < nv else 1))
+        assert np.linalg.norm(x.cpu().numpy() - u0) / np.linalg.norm(u0) < 1e-3, form
