@@ -110,7 +110,8 @@ __global__ void __launch_bounds__(JBS) k_jacobian_tg(JArgs a, const float2 *__re
   extern __shared__ float2 sh[];
   float2 *Ps = sh;                         // [nf][ns]
   float2 *Pd = Ps + a.nf * a.ns;           // [nf][nd]
-  float2 *Cs = Pd + a.nf * a.nd;           // [nf][NGC], 16-byte aligned (offset is even)
+  // [nf][NGC], read as float4: start at an even float2 offset (16-byte aligned)
+  float2 *Cs = Pd + a.nf * a.nd + ((a.nf * (a.ns + a.nd)) & 1);
   for (int t = threadIdx.x; t < a.nf * NGC; t += blockDim.x) Cs[t] = Ckg[t];
   for (int64_t v = blockIdx.x; v < a.nv; v += gridDim.x) {
     __syncthreads();
@@ -304,7 +305,7 @@ int jacobian_run(int mode, const int32_t *prow, const int32_t *pcol, const doubl
     k_ctab_kg<<<(unsigned)ceil_div((int64_t)nf * ngc, 256), 256, 0, st>>>(ctab.as<float2>(), ng, nf, ngc,
                                                                           ckg.as<float2>());
     DGP_CHECK_LAUNCH();
-    const size_t smem_tg = sizeof(float2) * ((size_t)nf * (ns + nd) + (size_t)nf * ngc);
+    const size_t smem_tg = sizeof(float2) * ((size_t)nf * (ns + nd) + 1 + (size_t)nf * ngc);
     DGP_REQUIRE(smem_tg <= 200 * 1024, "jacobian: NF*(NS+ND+NG) too large for one block's shared memory");
     auto go = [&](auto mtc, auto ngcc) {
       constexpr int MT_ = decltype(mtc)::value, NGC_ = decltype(ngcc)::value;

@@ -83,3 +83,34 @@ def test_vjp_matches_explicit_jacobian_nodal(jac_case):
     from oracle.jacobian import j_tg
     J0 = j_tg(_oracle_J(jac_case, sp.identity(mesh.nn, format="csr"), lump), jac_case["gfc"], nt)
     assert rel(np.transpose(Jt.cpu().numpy(), (2, 1, 0)), J0) < 1e-5
+
+
+@pytest.mark.parametrize("ng", [3, 20, 29])
+def test_tg_jacobian_odd_sizes(ng):
+    """Odd harmonic x optode counts (the staged fields end at an odd complex offset) and gate
+    counts that pad to 8, 24 and 32: TG Jacobian and vjp against the oracle."""
+    import scipy.sparse as sp
+    import torch
+    from dogpup_b200 import api, workloads
+    from oracle.jacobian import j_complex, j_tg
+    from oracle.transforms import td2fc
+    w = workloads.small_fwd(ns=3, nd=4, nf=5)
+    mesh = workloads.build_dmesh(w)
+    phi, _ = mesh.flu_solve(precision="fp64", tol=1e-12)
+    phiA = mesh.adj_flu_solve(precision="fp64", tol=1e-12)
+    t = w["t"]
+    gates = np.stack([np.exp(-(t - (0.3e-9 + q * 150e-12)) ** 2 / (2 * (100e-12) ** 2)) for q in range(ng)])
+    gfc = td2fc(gates, mesh.optode.fAxis, t)
+    nb = mesh.nodal_basis()
+    link = mesh._link()
+    nt = len(t)
+    Jt = api.jacobian_tg(nb, phi, phiA, mesh.optode.s_fpsf, link, torch.as_tensor(gfc, device="cuda"), nt)
+    P = sp.identity(mesh.nn, format="csr")
+    J0 = j_tg(j_complex(P, nb.w.cpu().numpy(), np.transpose(phi.cpu().numpy(), (1, 2, 0)),
+                        np.transpose(phiA.cpu().numpy(), (1, 2, 0)), mesh.optode.link,
+                        mesh.optode.s_fpsf.cpu().numpy()), gfc, nt)
+    assert rel(np.transpose(Jt.cpu().numpy(), (2, 1, 0)), J0) < 1e-5
+    g = np.random.default_rng(1).standard_normal((link.shape[0], ng))
+    v = api.jacobian_tg_vjp(nb, phi, phiA, mesh.optode.s_fpsf, link, torch.as_tensor(gfc, device="cuda"), nt,
+                            torch.as_tensor(g))
+    assert rel(v.cpu().numpy(), np.einsum("mgv,mg->v", J0, g)) < 1e-5
