@@ -1635,10 +1635,13 @@ Layouts spmm_layouts(const SolverPlan *S, int vec, bool fp32) {
 }
 
 // complex values per lane: more per lane amortises each nonzero's coefficient load over more
-// right-hand sides (FP32 up to 8, FP64 up to 4 for register room)
+// right-hand sides, fewer keep more rows in flight (FP64 up to 4 for register room)
 inline int vec_for(const SolverPlan *S, bool fp32) {
   if (fp32 && S->tune_vec) return S->tune_vec;
-  return std::min(S->nsp, fp32 ? 8 : 4);
+  // untuned FP32 default: 4 per lane from 8 padded sources up, 2 below (the autotuner's choice
+  // at 34,680 nodes x 32 harmonics for 3-64 sources; 8 per lane was 16-27 % slower)
+  if (fp32) return S->nsp >= 8 ? 4 : 2;
+  return std::min(S->nsp, 4);
 }
 
 dim3 grid_of(const Layout &L) { return dim3((unsigned)ceil_div(L.n, L.rows_per_block()), (unsigned)L.nf); }
