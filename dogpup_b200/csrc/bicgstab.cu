@@ -1836,9 +1836,30 @@ int run_iterations(SolverPlan *S, const Vecs<R> &V, const Work &W, int check_eve
     DGP_CUDA(e2);
     S->graph_iters[gi] = check_every;
   }
-  Ctl *h = (Ctl *)S->h_ctl;
+  // two pinned mirrors of the control block: while the host waits for one block of iterations'
+  // state, the next block is already queued, so the GPU never idles on the host's poll (after the
+  // stop the queued block's kernels return at once)
+  Ctl *hb = (Ctl *)S->h_ctl;
+  cudaEvent_t ev[2];
+  DGP_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+  if (cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming) != cudaSuccess) {
+    cudaEventDestroy(ev[0]);
+    return fail(DGP_ERR_CUDA, "solver: cudaEventCreate failed");
+  }
+  auto launch_block = [&](int slot) -> cudaError_t {
+    cudaError_t e = cudaGraphLaunch(S->graph[gi], st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&hb[slot], W.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[slot], st);
+    count_launches((int64_t)per_iter * check_every);
+    return e;
+  };
+  auto done = [&](int rc) {
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    return rc;
+  };
   // the device stops at maxit; the host bound only guards against a logic error
-  const int64_t max_launches = maxit / check_every + 3;
+  const int64_t max_launches = maxit / check_every + 4;
   // stall guard (inner solves of the mixed path): stop when the largest residual among the
   // still-active columns has not halved for ~40 iterations -- complex-FP32 BiCGSTAB can
   // stall at its rounding floor, and the FP64 refinement that follows restarts from the
@@ -1846,23 +1867,33 @@ int run_iterations(SolverPlan *S, const Vecs<R> &V, const Work &W, int check_eve
   const int patience = std::max(3, 40 / check_every);
   double ref_err = 0.0;
   int since = 0;
-  for (int64_t launches = 0;; ++launches) {
-    if (launches > max_launches) return fail(DGP_ERR_CUDA, "solver: control block never reached DONE");
-    DGP_CUDA(cudaGraphLaunch(S->graph[gi], st));
-    count_launches((int64_t)per_iter * check_every);
-    DGP_CUDA(cudaMemcpyAsync(h, W.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
-    DGP_CUDA(cudaStreamSynchronize(st));
-    if (h->state == ST_DONE) break;
+  cudaError_t e = launch_block(0);
+  if (e != cudaSuccess) return done(cuda_fail(e, "solver: graph launch", __FILE__, __LINE__));
+  int cur = 0;
+  for (int64_t launches = 1;; ++launches) {
+    if (launches > max_launches) return done(fail(DGP_ERR_CUDA, "solver: control block never reached DONE"));
+    e = launch_block(cur ^ 1);  // the next block of iterations, queued before this poll
+    if (e == cudaSuccess) e = cudaEventSynchronize(ev[cur]);
+    if (e != cudaSuccess) return done(cuda_fail(e, "solver: iteration block", __FILE__, __LINE__));
+    const Ctl &h = hb[cur];
+    if (h.state == ST_DONE) break;
     if (stall_guard) {
-      if (ref_err == 0.0 || h->max_err < 0.5 * ref_err) {
-        ref_err = h->max_err;
+      if (ref_err == 0.0 || h.max_err < 0.5 * ref_err) {
+        ref_err = h.max_err;
         since = 0;
       } else if (++since >= patience) {
         break;
       }
     }
+    cur ^= 1;
   }
-  *iters_out = h->iters;
+  // wait for the queued block (it returns at once after a stop on the device, or runs one more
+  // block of iterations after a stall-guard stop) and report the final count
+  e = cudaMemcpyAsync(&hb[0], W.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return done(cuda_fail(e, "solver: iteration block", __FILE__, __LINE__));
+  *iters_out = hb[0].iters;
+  done(DGP_OK);
   return DGP_OK;
 }
 
@@ -1972,7 +2003,7 @@ int solver_build(SolverPlan *S, const int32_t *d_rowptr, const int32_t *d_col, i
   DGP_TRY(S->GT64.alloc(sizeof(double2) * gcount));
   DGP_TRY(S->RecG32.alloc(sizeof(Rec32) * gcount));
   DGP_TRY(S->RecGT32.alloc(sizeof(Rec32) * gcount));
-  DGP_CUDA(cudaMallocHost(&S->h_ctl, sizeof(Ctl)));
+  DGP_CUDA(cudaMallocHost(&S->h_ctl, 2 * sizeof(Ctl)));  // two mirrors (run_iterations' pipelined polls)
   DGP_TRY(tiled_setup(S, st));
   return solver_update(S, d_K, d_M, st);
 }
@@ -2424,7 +2455,7 @@ int solver_set_spmm(SolverPlan *S, int32_t tiled, int32_t vec, int32_t rows) {
 
 int solver_set_dot_rows(SolverPlan *S, int32_t mult) {
   DGP_REQUIRE(mult == 0 || mult == 1 || mult == 2 || mult == 4 || mult == 8 || mult == 16,
-              "set_dot_rows: multiple must be 0 (default 16), 1, 2, 4, 8 or 16");
+              "set_dot_rows: multiple must be 0 (default 4), 1, 2, 4, 8 or 16");
   S->tune_dot = mult;
   for (auto &g : S->graph)
     if (g) {
