@@ -532,7 +532,7 @@ def grad_big_bench(target_nodes=500_000, ns=32, nd=32, nf=32):
         loss = (r ** 2).sum()
         loss.backward()
         torch.cuda.synchronize()
-        out[prec] = dict(seconds=time.perf_counter() - t0, grad=mua.grad.clone(), loss=float(loss),
+        out[prec] = dict(seconds=time.perf_counter() - t0, grad=mua.grad.clone(), loss=float(loss.detach()),
                          iterations=[(rep.iterations, rep.refinements) for rep in model.last_reports])
         mesh._solver = None
     g64, gm = out["fp64"]["grad"], out["mixed"]["grad"]
