@@ -262,3 +262,21 @@ def test_closest_point_on_triangle_two_methods():
         a, b, c = rng.standard_normal((3, 3))
         p = rng.standard_normal(3) * 2
         assert np.abs(walk(p, a, b, c) - proj(p, a, b, c)).max() < 1e-12
+
+
+def test_grid_matrix_assembly_helpers():
+    """m2g from (element, weights) drops zero weights as MATLAB's sparse does and leaves
+    out-of-mesh rows empty; g2m from device rows skips -1 slots and zero weights."""
+    from dogpup_b200.grid import g2m_from_rows, m2g_from_location
+    elem = np.array([[0, 1, 2, 3], [1, 2, 3, 4]])
+    eid = np.array([0, -1, 1])
+    w = np.array([[0.25, 0.25, 0.5, 0.0], [0, 0, 0, 0], [0.1, 0.2, 0.3, 0.4]])
+    P, inm = m2g_from_location(eid, w, elem, 5)
+    assert P.shape == (3, 5) and np.array_equal(inm, [True, False, True])
+    assert P.nnz == 3 + 4 and P[1].nnz == 0
+    assert np.allclose(P.toarray()[2], [0, 0.1, 0.2, 0.3, 0.4]) and np.allclose(P.toarray()[0], [0.25, 0.25, 0.5, 0, 0])
+    col = np.array([[3, -1, 5, 7], [-1, -1, -1, -1], [2, 4, 6, 8]])
+    val = np.array([[0.5, 0.0, 0.5, 0.0], [0, 0, 0, 0], [0.25, 0.25, 0.25, 0.25]])
+    G = g2m_from_rows(col, val, 10)
+    assert G.shape == (3, 10) and G.nnz == 2 + 4
+    assert np.allclose(G.toarray()[0], np.eye(10)[3] * 0.5 + np.eye(10)[5] * 0.5)
