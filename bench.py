@@ -198,6 +198,7 @@ def _event_ms(fn, reps):
     import torch
     st = torch.cuda.current_stream()
     fn()
+    fn()  # twice: a call that allocates its output while the previous one lives needs two blocks
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(st)
@@ -700,11 +701,20 @@ def run_ours(a, rank, world, local_rank):
             "per_kernel_gbs": {names[q]: round(prof[q][1] / (prof[q][0] * 1e-3) / 1e9, 1) for q in prof}}
     res.update(ms_per_step=ms_step, value=value, e2e=e2e, rep=rep, clocks=clocks, roof=roof, mesh=mesh, w=w,
                launches=launches, tuned=tuned)
+    # the secondary measurements build plans of their own: release this one's workspace (~110 GB
+    # of library allocations) first, and the previous measurement's objects between them
+    import gc
+    mesh._solver = None
+    del solver
+    gc.collect()
     if rank == 0 and not a.no_secondary:
         res["plain"] = plain_fp64_per_rhs(mesh)
         log(f"[rank 0] plain FP64 per-RHS: {res['plain']}")
+        gc.collect()
         res["tg"] = tg_jacobian_bench()
         log(f"[rank 0] TG Jacobian: {res['tg']}")
+        gc.collect()
+        torch.cuda.empty_cache()  # the LM step's library calls allocate their work arrays themselves
         res["lm"] = lm_step_bench(grid_mm=a.lm_grid_mm)
         log(f"[rank 0] LM step: {res['lm']}")
     return res
