@@ -674,10 +674,13 @@ def run_ours(a, rank, world, local_rank):
                "ms_per_step": ems / a.steps}
 
     # ---- roofline: the dominant sweep kernel, CUDA-event timed on the solver's stream
-    # sweeps per inner iteration -- BiCGSTAB: A SpMM x2, G SpMM x5, x/r/p, s; COCG: A x1, G x2
-    per_iter = {0: 2, 1: 5, 2: 1, 3: 1} if a.inner == "bicgstab" else {0: 1, 1: 2}
+    # sweeps per inner iteration -- BiCGSTAB: A SpMM x2, G SpMM x5, x/r/p, s; COCG: q = A p with p.q,
+    # T = G r with T.T, z = G^T T (the plain G kernel on the G^T records), r update, x/p update
+    per_iter = {0: 2, 1: 5, 2: 1, 3: 1} if a.inner == "bicgstab" else {4: 1, 5: 1, 1: 1, 6: 1, 7: 1}
     names = {0: "k_spmm_A<float> (K + i w M SpMM)", 1: "k_spmm_G<float> (FSAI apply)",
-             2: "k_update_xrp<float>", 3: "k_update_s<float>"}
+             2: "k_update_xrp<float>", 3: "k_update_s<float>",
+             4: "k_spmm<float,4,1,OpA32> (q = A p, p.q)", 5: "k_spmm<float,4,3,OpG32> (T = G r, T.T)",
+             6: "k_update_r<float>", 7: "k_update_px<float>"}
     prof = {q: solver.profile_kernel(q, 5) for q in per_iter}
     dom = max(prof, key=lambda q: prof[q][0] * per_iter[q])
     pk = json.load(open(ROOT / "MEASURED_PEAKS.json")) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
@@ -686,7 +689,7 @@ def run_ours(a, rank, world, local_rank):
     # DRAM bytes (read + write) per launch from one ncu capture of the same kernel and launch
     # shape on the 20,497-node, 32-harmonic ellipsoid, scaled to this launch by nodes x harmonics
     # (the records and vectors all scale with both)
-    captured = {0: 659.7e6, 1: 716.4e6}
+    captured = {0: 659.7e6, 1: 716.4e6, 4: 804.8e6, 5: 797.1e6, 6: 966.3e6, 7: 1626.1e6}
     traffic = traffic_bytes = None
     if dom in captured and a.workload == "ellipsoid":
         traffic_bytes = captured[dom] * (mesh.nn * nf) / (20497 * 32)

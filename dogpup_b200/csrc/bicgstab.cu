@@ -2170,6 +2170,12 @@ int solver_solve(SolverPlan *S, const double *d_B, const int32_t *d_nodes, const
 
 // ------------------------------------------------------ kernel timing hook
 namespace {
+// every column iterating (the update kernels skip frozen columns' work)
+__global__ void k_all_active(Cols c) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < c.C; j += (int64_t)gridDim.x * blockDim.x)
+    c.active[j] = 1;
+}
+
 template <int VEC>
 void profile_launch(int which, const SolverPlan *S, const OpA32 &A, const OpG32 &G, const Vecs<float> &V,
                     const Work &W, const Ctl *ctl, cudaStream_t st) {
@@ -2221,6 +2227,10 @@ int solver_profile(SolverPlan *S, int which, int reps, float *ms, double *bytes,
       default: profile_launch<8>(which, S, A, G, V, W, ctl, st); break;
     }
   };
+  if (which == 2 || which == 3 || which == 6 || which == 7) {  // update kernels: time full work
+    k_all_active<<<g1(W.cols.C, 256), 256, 0, st>>>(W.cols);
+    count_launches(1);
+  }
   switch (which) {
     case 0: *bytes = 2 * pass + (double)S->nf * (16.0 * S->nnz + 4.0 * (S->n + 1)); break;
     case 1: *bytes = 2 * pass + (double)S->nf * (16.0 * S->nnzG + 4.0 * (S->n + 1)); break;
