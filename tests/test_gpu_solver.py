@@ -4,7 +4,7 @@ Tolerances: integer/index data (CSR pattern, boundary flags, FSAI pattern)
 must match exactly; FP64 values to 1e-12 relative (different summation
 order); the FP64 solver to 1e-9 of the oracle's own BiCGSTAB; the
 mixed-precision solver to 1e-6 relative fluence error against a sparse-direct
-complex128 solve (the north-star accuracy bar).
+complex128 solve (the accuracy bar of the mixed mode).
 """
 import numpy as np
 import pytest
