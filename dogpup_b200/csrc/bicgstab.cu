@@ -1576,35 +1576,43 @@ Work work_views(SolverPlan *S) {
 
 size_t scal_bytes(int64_t C) { return (sizeof(double) * 5 + sizeof(double2) * (4 + NACC) + 2 * sizeof(int)) * C + 256; }
 
+// vector slots: COCG uses the first NVEC_COCG (x, r, r^ written by k_init, p, q, T, z),
+// BiCGSTAB all NVEC_ALL; a slot that is not allocated yet views as NULL
+constexpr int NVEC_COCG = 7, NVEC_ALL = 10;
+
 template <class R> Vecs<R> vec_views(SolverPlan *S) {
   using C = typename CT<R>::C;
   Vecs<R> V;
-  C **slots[10] = {&V.x, &V.r, &V.rhat, &V.p, &V.v, &V.h, &V.s, &V.T1, &V.z, &V.t};
-  for (int q = 0; q < 10; ++q) *slots[q] = S->vec[q].as<C>();
+  C **slots[NVEC_ALL] = {&V.x, &V.r, &V.rhat, &V.p, &V.v, &V.T1, &V.z, &V.h, &V.s, &V.t};
+  for (int q = 0; q < NVEC_ALL; ++q) *slots[q] = S->vec[q].as<C>();
   return V;
 }
 
-int ensure_workspace(SolverPlan *S, int prec) {
-  if (S->ws_prec == prec) return DGP_OK;
-  for (auto &g : S->graph)
-    if (g) {
-      cudaGraphExecDestroy(g);
-      g = nullptr;
-    }
-  for (int &gi : S->graph_iters) gi = 0;
+// Workspace of precision `prec` with at least `nvec` vectors.  A change of precision
+// reallocates everything; more vectors for the same precision are added without moving the
+// existing ones (graphs captured on them stay valid).  The mixed solve with the COCG inner
+// solver needs 7 of the 10 vectors (70 instead of 100 GB at 153k nodes x 64 x 128).
+int ensure_workspace(SolverPlan *S, int prec, int nvec = NVEC_ALL) {
   const int64_t C = (int64_t)S->nf * S->nsp;
   const size_t esz = prec == DGP_PREC_FP64 ? sizeof(double2) : sizeof(float2);
   const size_t vb = esz * (size_t)C * S->n;
-  for (int q = 0; q < 10; ++q) {
-    S->vec[q].release();
-    DGP_TRY(S->vec[q].alloc(vb));
+  if (S->ws_prec != prec) {
+    for (auto &g : S->graph)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
+    for (int &gi : S->graph_iters) gi = 0;
+    for (auto &v : S->vec) v.release();
+    DGP_TRY(S->scal.alloc(scal_bytes(C)));
+    DGP_TRY(S->status.alloc(sizeof(int) * C));
+    DGP_TRY(S->ctl.alloc(sizeof(Ctl)));
+    DGP_CUDA(cudaMemset(S->scal.p, 0, scal_bytes(C)));
+    S->ws_prec = prec;
+    S->ws_cols = C;
   }
-  DGP_TRY(S->scal.alloc(scal_bytes(C)));
-  DGP_TRY(S->status.alloc(sizeof(int) * C));
-  DGP_TRY(S->ctl.alloc(sizeof(Ctl)));
-  DGP_CUDA(cudaMemset(S->scal.p, 0, scal_bytes(C)));
-  S->ws_prec = prec;
-  S->ws_cols = C;
+  for (int q = 0; q < nvec; ++q)
+    if (!S->vec[q].p) DGP_TRY(S->vec[q].alloc(vb));
   return DGP_OK;
 }
 
@@ -2061,7 +2069,7 @@ static int solve_mixed(SolverPlan *S, const double *d_B, const int32_t *d_nodes,
                        const double *d_fpsf, double *d_X, int ns, const dgp_solve_opts &o, dgp_solve_report *rep,
                        cudaStream_t st) {
   const bool cocg = o.precision == DGP_PREC_MIXED;
-  DGP_TRY(ensure_workspace(S, DGP_PREC_MIXED));
+  DGP_TRY(ensure_workspace(S, DGP_PREC_MIXED, cocg ? NVEC_COCG : NVEC_ALL));
   Work W = work_views(S);
   Vecs<float> V = vec_views<float>(S);
   const int vec = vec_for(S, true);
@@ -2182,7 +2190,7 @@ void profile_launch(int which, const SolverPlan *S, const OpA32 &A, const OpG32 
   const Layout L = spmm_layouts(S, VEC, true).L, Ld = spmm_layouts(S, VEC, true).Ld;
   const Layout Lu = layouts_for(S, VU).L, Lud = layouts_for(S, VU).Ld;
   switch (which) {
-    case 0: k_spmm<float, VEC, 0><<<grid_of(L), BS, 0, st>>>(L, A, V.z, V.t, nullptr, W.cols, ctl); break;
+    case 0: k_spmm<float, VEC, 0><<<grid_of(L), BS, 0, st>>>(L, A, V.z, V.x, nullptr, W.cols, ctl); break;
     case 1: k_spmm<float, VEC, 0><<<grid_of(L), BS, 0, st>>>(L, G, V.p, V.T1, nullptr, W.cols, ctl); break;
     case 4: k_spmm<float, VEC, 1><<<grid_of(Ld), BS, red_smem(Ld, 1), st>>>(Ld, A, V.p, V.v, V.p, W.cols, ctl); break;
     case 5: k_spmm<float, VEC, 3><<<grid_of(Ld), BS, red_smem(Ld, 1), st>>>(Ld, G, V.r, V.T1, nullptr, W.cols, ctl); break;
@@ -2205,6 +2213,7 @@ void profile_launch(int which, const SolverPlan *S, const OpA32 &A, const OpG32 
 int solver_profile(SolverPlan *S, int which, int reps, float *ms, double *bytes, cudaStream_t st) {
   DGP_REQUIRE(S->ws_prec == DGP_PREC_MIXED, "profile: run a mixed-precision solve first");
   DGP_REQUIRE(reps >= 1 && which >= 0 && which <= 7, "profile: bad arguments");
+  if (which == 2 || which == 3) DGP_TRY(ensure_workspace(S, DGP_PREC_MIXED, NVEC_ALL));  // BiCGSTAB updates
   Vecs<float> V = vec_views<float>(S);
   Work W = work_views(S);
   W.cols.hact = nullptr;  // timing / checking runs sweep every harmonic
@@ -2269,24 +2278,25 @@ void spmm_set(const SolverPlan *S, const OpA32 &A, const OpG32 &G, const OpG32 &
               const Work &W, const Ctl *ctl, cudaStream_t st) {
   const Layouts LL = spmm_layouts(S, VEC, true);
   const Layout Ls = LL.L, Lsd = LL.Ld;
+  // scratch vectors from the first NVEC_COCG slots only (x, r and r^ stand in for h, s and t)
   k_spmm<float, VEC, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, G, V.p, V.T1, nullptr, W.cols, ctl);
-  k_spmm<float, VEC, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, GT, V.T1, V.h, nullptr, W.cols, ctl);
-  k_spmm<float, VEC, 1><<<grid_of(Lsd), BS, red_smem(Lsd, 1), st>>>(Lsd, A, V.h, V.v, V.rhat, W.cols, ctl);
-  k_spmm<float, VEC, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, G, V.s, V.T1, nullptr, W.cols, ctl);
+  k_spmm<float, VEC, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, GT, V.T1, V.x, nullptr, W.cols, ctl);
+  k_spmm<float, VEC, 1><<<grid_of(Lsd), BS, red_smem(Lsd, 1), st>>>(Lsd, A, V.x, V.v, V.rhat, W.cols, ctl);
+  k_spmm<float, VEC, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, G, V.r, V.T1, nullptr, W.cols, ctl);
   k_spmm<float, VEC, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, GT, V.T1, V.z, nullptr, W.cols, ctl);
-  k_spmm<float, VEC, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, A, V.z, V.t, nullptr, W.cols, ctl);
-  k_spmm<float, VEC, 2><<<grid_of(Lsd), BS, red_smem(Lsd, 2), st>>>(Lsd, G, V.t, nullptr, V.T1, W.cols, ctl);
+  k_spmm<float, VEC, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, A, V.z, V.rhat, nullptr, W.cols, ctl);
+  k_spmm<float, VEC, 2><<<grid_of(Lsd), BS, red_smem(Lsd, 2), st>>>(Lsd, G, V.rhat, nullptr, V.T1, W.cols, ctl);
 }
 }  // namespace
 
 void tspmm_set(const SolverPlan *S, const Vecs<float> &V, const Work &W, const Ctl *ctl, cudaStream_t st) {
   tspmm<0>(S, 1, V.p, V.T1, nullptr, W.cols, ctl, st);
-  tspmm<0>(S, 2, V.T1, V.h, nullptr, W.cols, ctl, st);
-  tspmm<1>(S, 0, V.h, V.v, V.rhat, W.cols, ctl, st);
-  tspmm<0>(S, 1, V.s, V.T1, nullptr, W.cols, ctl, st);
+  tspmm<0>(S, 2, V.T1, V.x, nullptr, W.cols, ctl, st);
+  tspmm<1>(S, 0, V.x, V.v, V.rhat, W.cols, ctl, st);
+  tspmm<0>(S, 1, V.r, V.T1, nullptr, W.cols, ctl, st);
   tspmm<0>(S, 2, V.T1, V.z, nullptr, W.cols, ctl, st);
-  tspmm<0>(S, 0, V.z, V.t, nullptr, W.cols, ctl, st);
-  tspmm<2>(S, 1, V.t, nullptr, V.T1, W.cols, ctl, st);
+  tspmm<0>(S, 0, V.z, V.rhat, nullptr, W.cols, ctl, st);
+  tspmm<2>(S, 1, V.rhat, nullptr, V.T1, W.cols, ctl, st);
 }
 
 // deterministic test pattern in [-1, 1) for the operator self-check
@@ -2327,7 +2337,7 @@ __global__ void k_maxdiff(const float2 *__restrict__ a, const float2 *__restrict
 // contents are scratch here (every solve re-initialises them).
 int solver_autotune(SolverPlan *S, int32_t *tiled_out, int32_t *vec_out, int32_t *rows_out, float *ms_out,
                     cudaStream_t st) {
-  DGP_TRY(ensure_workspace(S, DGP_PREC_MIXED));
+  DGP_TRY(ensure_workspace(S, DGP_PREC_MIXED, NVEC_COCG));
   Vecs<float> V = vec_views<float>(S);
   Work W = work_views(S);
   W.cols.hact = nullptr;  // timing / checking runs sweep every harmonic
@@ -2482,7 +2492,7 @@ int solver_set_dot_rows(SolverPlan *S, int32_t mult) {
 int solver_check_spmm(SolverPlan *S, double *max_rel, cudaStream_t st) {
   DGP_REQUIRE(max_rel, "check_spmm: null output");
   DGP_REQUIRE(S->tiled_ok, "check_spmm: the tiled SpMM does not fit this plan");
-  DGP_TRY(ensure_workspace(S, DGP_PREC_MIXED));
+  DGP_TRY(ensure_workspace(S, DGP_PREC_MIXED, NVEC_COCG));
   Vecs<float> V = vec_views<float>(S);
   Work W = work_views(S);
   W.cols.hact = nullptr;  // timing / checking runs sweep every harmonic
@@ -2512,9 +2522,9 @@ int solver_check_spmm(SolverPlan *S, double *max_rel, cudaStream_t st) {
     if (gv == 2) gather(std::integral_constant<int, 2>(), what);
     else if (gv == 4) gather(std::integral_constant<int, 4>(), what);
     else gather(std::integral_constant<int, 8>(), what);
-    tspmm<0>(S, what, V.p, V.h, nullptr, W.cols, ctl, st);
+    tspmm<0>(S, what, V.p, V.x, nullptr, W.cols, ctl, st);
     DGP_CUDA(cudaMemsetAsync(dm.p, 0, 2 * sizeof(unsigned), st));
-    k_maxdiff<<<1184, 256, 0, st>>>(V.h, V.T1, cnt, dm.as<unsigned>());
+    k_maxdiff<<<1184, 256, 0, st>>>(V.x, V.T1, cnt, dm.as<unsigned>());
     unsigned h[2] = {0, 0};
     DGP_CUDA(cudaMemcpyAsync(h, dm.p, sizeof(h), cudaMemcpyDeviceToHost, st));
     DGP_CUDA(cudaStreamSynchronize(st));
