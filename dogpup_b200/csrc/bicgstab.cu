@@ -1848,12 +1848,9 @@ int run_iterations(SolverPlan *S, const Vecs<R> &V, const Work &W, int check_eve
   // state, the next block is already queued, so the GPU never idles on the host's poll (after the
   // stop the queued block's kernels return at once)
   Ctl *hb = (Ctl *)S->h_ctl;
-  cudaEvent_t ev[2];
-  DGP_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
-  if (cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming) != cudaSuccess) {
-    cudaEventDestroy(ev[0]);
-    return fail(DGP_ERR_CUDA, "solver: cudaEventCreate failed");
-  }
+  for (auto &pe : S->poll_ev)
+    if (!pe) DGP_CUDA(cudaEventCreateWithFlags(&pe, cudaEventDisableTiming));
+  cudaEvent_t *ev = S->poll_ev;
   auto launch_block = [&](int slot) -> cudaError_t {
     cudaError_t e = cudaGraphLaunch(S->graph[gi], st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&hb[slot], W.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st);
@@ -1861,11 +1858,7 @@ int run_iterations(SolverPlan *S, const Vecs<R> &V, const Work &W, int check_eve
     count_launches((int64_t)per_iter * check_every);
     return e;
   };
-  auto done = [&](int rc) {
-    cudaEventDestroy(ev[0]);
-    cudaEventDestroy(ev[1]);
-    return rc;
-  };
+  auto done = [](int rc) { return rc; };
   // the device stops at maxit; the host bound only guards against a logic error
   const int64_t max_launches = maxit / check_every + 4;
   // stall guard (inner solves of the mixed path): stop when the largest residual among the
@@ -1947,6 +1940,8 @@ void launch_residual(SolverPlan *S, int ns, const double *d_X, const double *d_B
 SolverPlan::~SolverPlan() {
   for (auto &g : graph)
     if (g) cudaGraphExecDestroy(g);
+  for (auto &e : poll_ev)
+    if (e) cudaEventDestroy(e);
   if (h_ctl) cudaFreeHost(h_ctl);
 }
 
@@ -1955,12 +1950,11 @@ int solver_update(SolverPlan *S, const double *d_K, const double *d_M, cudaStrea
   k_cvt_km<<<g1(nnz, 256), 256, 0, st>>>(d_K, d_M, S->col.as<int32_t>(), nnz, S->KM64.as<double2>(),
                                           S->RecA32.as<Rec32>(), S->tA.lcol.as<int32_t>());
   DGP_CHECK_LAUNCH();
-  // FSAI of tril(K + i*k*dfc*M) for every harmonic
-  DevBuf im;
-  DGP_TRY(im.alloc(sizeof(double) * nnz));
-  k_dfc_m<<<g1(nnz, 256), 256, 0, st>>>(d_M, S->dfc, nnz, im.as<double>());
+  // FSAI of tril(K + i*k*dfc*M) for every harmonic (scratch kept in the plan: no allocation per update)
+  if (!S->dfcM.p) DGP_TRY(S->dfcM.alloc(sizeof(double) * nnz));
+  k_dfc_m<<<g1(nnz, 256), 256, 0, st>>>(d_M, S->dfc, nnz, S->dfcM.as<double>());
   DGP_CHECK_LAUNCH();
-  DGP_TRY(fsai_factor_run(S->rowptr.as<int32_t>(), S->col.as<int32_t>(), d_K, im.as<double>(), S->n,
+  DGP_TRY(fsai_factor_run(S->rowptr.as<int32_t>(), S->col.as<int32_t>(), d_K, S->dfcM.as<double>(), S->n,
                           S->P.rowptr.as<int32_t>(), S->P.col.as<int32_t>(), S->P.mmax, S->nf,
                           S->G64.as<double2>(), 1, S->nnzG, st, S->harm.as<int32_t>()));
   k_gather_gt<<<g1(S->nnzG * S->nf, 256), 256, 0, st>>>(S->G64.as<double2>(), S->P.permT.as<int32_t>(),
@@ -2140,13 +2134,12 @@ int solver_solve(SolverPlan *S, const double *d_B, const int32_t *d_nodes, const
               "solve: unknown precision");
   if (o.check_every < 1) o.check_every = 1;
   if (d_nodes) {
-    DevBuf bad;
-    DGP_TRY(bad.alloc(sizeof(int)));
-    DGP_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), st));
-    k_check_nodes<<<g1(4 * ns, 128), 128, 0, st>>>(d_nodes, ns, S->n, bad.as<int>());
+    if (!S->node_flag.p) DGP_TRY(S->node_flag.alloc(sizeof(int)));
+    DGP_CUDA(cudaMemsetAsync(S->node_flag.p, 0, sizeof(int), st));
+    k_check_nodes<<<g1(4 * ns, 128), 128, 0, st>>>(d_nodes, ns, S->n, S->node_flag.as<int>());
     DGP_CHECK_LAUNCH();
     int hb = 0;
-    DGP_CUDA(cudaMemcpyAsync(&hb, bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    DGP_CUDA(cudaMemcpyAsync(&hb, S->node_flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     DGP_CUDA(cudaStreamSynchronize(st));
     if (hb) return fail(DGP_ERR_ARG, "solve: source node index out of range");
   }

@@ -300,7 +300,7 @@ int dgp_solver_memory(dgp_solver_t s, int64_t *bytes) {
   if (!s || !bytes) return fail(DGP_ERR_ARG, "solver_memory: null pointer");
   const SolverPlan &p = s->plan;
   int64_t b = 0;
-  const DevBuf *bufs[] = {&p.rowptr, &p.col, &p.KM64, &p.RecA32, &p.omega, &p.G64, &p.GT64, &p.RecG32, &p.RecGT32,
+  const DevBuf *bufs[] = {&p.rowptr, &p.col, &p.KM64, &p.RecA32, &p.dfcM, &p.omega, &p.G64, &p.GT64, &p.RecG32, &p.RecGT32,
                           &p.P.rowptr, &p.P.col, &p.P.rowptrT, &p.P.colT, &p.P.permT, &p.scal, &p.ctl, &p.status};
   for (auto *d : bufs) b += (int64_t)d->bytes;
   for (auto &v : p.vec) b += (int64_t)v.bytes;

@@ -18,6 +18,7 @@ struct FemPlan {
   DevBuf rowptr, col;     // int32 CSR pattern (full symmetric)
   DevBuf cstart, payload; // per-slot contribution lists
   DevBuf Ke, Me, Be;      // element / face blocks (scratch of every assembly)
+  DevBuf flag;            // int: degenerate-element flag of the element kernel (kept: no per-call allocation)
 };
 
 int fem_create(FemPlan *F, const double *d_node, const int32_t *d_elem, int64_t nn, int64_t ne, double nr,
@@ -78,6 +79,8 @@ struct SolverPlan {
   DevBuf rowptr, col;            // A pattern
   DevBuf KM64;                   // interleaved (K, M) per slot, FP64
   DevBuf RecA32;                 // FP32 path: one 16-byte (col, K, M) record per slot
+  DevBuf dfcM;                   // [nnz] dfc * M, the imaginary part of the FSAI input (update scratch)
+  DevBuf node_flag;              // int: out-of-range source node flag (solve scratch)
   DevBuf omega;                  // [nf] h_j * dfc (FP64), then [nf] FP32
   DevBuf harm;                   // [nf] harmonic index h_j of batch slot j
   FsaiPattern P;
@@ -90,7 +93,8 @@ struct SolverPlan {
   DevBuf scal;                   // per-column scalars
   DevBuf ctl;                    // control block
   DevBuf status;                 // per-column status
-  void *h_ctl = nullptr;         // pinned mirror of the control block
+  void *h_ctl = nullptr;         // pinned mirrors of the control block (two)
+  cudaEvent_t poll_ev[2] = {nullptr, nullptr};  // the two mirrors' copy-done events
   cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};  // FP64 BiCGSTAB, FP32 BiCGSTAB, FP32 COCG
   int graph_iters[3] = {0, 0, 0};
   // SpMM launch shape of the complex-FP32 sweeps chosen by solver_autotune (0 = built-in default)

@@ -605,11 +605,10 @@ int fem_assemble(FemPlan *F, const double *d_mua, const double *d_musp, double *
                  cudaStream_t st) {
   DGP_REQUIRE(d_mua && d_musp && d_K && d_M, "fem_assemble: null pointer");
   const int bs = 128;
-  DevBuf flag;
-  DGP_TRY(flag.alloc(sizeof(int)));
-  DGP_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), st));
+  if (!F->flag.p) DGP_TRY(F->flag.alloc(sizeof(int)));
+  DGP_CUDA(cudaMemsetAsync(F->flag.p, 0, sizeof(int), st));
   k_element_blocks<<<grid1(F->ne, bs), bs, 0, st>>>(F->node.as<double>(), F->elem.as<int32_t>(), F->ne, d_mua,
-                                                   d_musp, F->Ke.as<double>(), F->Me.as<double>(), flag.as<int>());
+                                                   d_musp, F->Ke.as<double>(), F->Me.as<double>(), F->flag.as<int>());
   DGP_CHECK_LAUNCH();
   if (F->nfaces > 0) {
     k_face_blocks<<<grid1(F->nfaces, bs), bs, 0, st>>>(F->node.as<double>(), F->faces.as<int32_t>(), F->nfaces,
