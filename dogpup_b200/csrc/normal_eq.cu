@@ -372,6 +372,17 @@ int make_map(CUtensorMap *map, void *base, int64_t rows, int64_t cols) {
   return DGP_OK;
 }
 
+// DGP_ERR_ARG unless every data weight W[0..nm) is finite and non-negative; errb is a zeroed device int.
+int check_weights(const double *W, int64_t nm, int *errb, const char *who, cudaStream_t st) {
+  k_check_weights<<<(unsigned)ceil_div(nm, 256), 256, 0, st>>>(W, nm, errb);
+  DGP_CHECK_LAUNCH();
+  int werr = 0;
+  DGP_CUDA(cudaMemcpyAsync(&werr, errb, sizeof(int), cudaMemcpyDeviceToHost, st));
+  DGP_CUDA(cudaStreamSynchronize(st));
+  if (werr) return fail(DGP_ERR_ARG, std::string(who) + ": data weights must be finite and non-negative");
+  return DGP_OK;
+}
+
 }  // namespace
 
 int normal_eq_run(const float *Jt, int64_t nv, int64_t nm, const double *W, const double *y, double lam, int mode,
@@ -388,14 +399,7 @@ int normal_eq_run(const float *Jt, int64_t nv, int64_t nm, const double *W, cons
   DGP_TRY(diag.alloc(sizeof(double) * nv));
   DGP_TRY(errb.alloc(sizeof(int)));
   DGP_CUDA(cudaMemsetAsync(errb.p, 0, sizeof(int), st));
-  if (W) {
-    k_check_weights<<<(unsigned)ceil_div(nm, 256), 256, 0, st>>>(W, nm, errb.as<int>());
-    DGP_CHECK_LAUNCH();
-    int werr = 0;
-    DGP_CUDA(cudaMemcpyAsync(&werr, errb.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-    DGP_CUDA(cudaStreamSynchronize(st));
-    if (werr) return fail(DGP_ERR_ARG, "normal_eq: data weights must be finite and non-negative");
-  }
+  if (W) DGP_TRY(check_weights(W, nm, errb.as<int>(), "normal_eq", st));
   k_split<<<(unsigned)ceil_div(nvp * nmp, 256), 256, 0, st>>>(Jt, W, nv, nm, nvp, nmp, hi.as<__nv_bfloat16>(),
                                                                lo.as<__nv_bfloat16>());
   DGP_CHECK_LAUNCH();
@@ -561,7 +565,12 @@ int lm_update_run(const float *Jt, int64_t nv, int64_t nm, const double *W, cons
     DGP_TRY(normal_eq_run(Jt, nv, nm, W, y, lam, 0, H.as<double>(), nv, x, st));
     return cholesky_solve_run(H.as<double>(), nv, nv, x, st);
   }
-  DevBuf diag, Jw, G, z;
+  DevBuf diag, Jw, G, z, errb;
+  if (W) {
+    DGP_TRY(errb.alloc(sizeof(int)));
+    DGP_CUDA(cudaMemsetAsync(errb.p, 0, sizeof(int), st));
+    DGP_TRY(check_weights(W, nm, errb.as<int>(), "lm_update", st));
+  }
   DGP_TRY(diag.alloc(sizeof(double) * nv));
   DGP_TRY(Jw.alloc(sizeof(float) * (size_t)nm * nv));
   DGP_TRY(G.alloc(sizeof(double) * (size_t)nm * nm));

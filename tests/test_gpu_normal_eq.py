@@ -142,3 +142,22 @@ def test_lm_update_both_forms_match_tik_inv(nv, nm):
         check(lib.dgp_lm_update(_v(Jt), nv, nm, _v(Wd), _v(yd), lam, _v(x), form, C.byref(used), None))
         assert used.value == (form if form else (2 if nm < nv else 1))
         assert np.linalg.norm(x.cpu().numpy() - u0) / np.linalg.norm(u0) < 1e-3, form
+
+
+def test_lm_update_rejects_bad_weights_in_both_forms():
+    """A negative or non-finite data weight is DGP_ERR_ARG in the unknowns' form
+    and in the measurements' form alike (the latter takes W^1/2, so an unchecked
+    weight would surface as NaN instead)."""
+    import torch
+    from dogpup_b200._lib import lib
+    nv, nm = 300, 200
+    J, W, y = _case(nv, nm, 3)
+    Jt = torch.as_tensor(np.ascontiguousarray(J.T), dtype=torch.float32, device="cuda")
+    yd = torch.as_tensor(y, device="cuda")
+    for bad in (-1.0, float("nan")):
+        Wb = W.copy()
+        Wb[17] = bad
+        Wd = torch.as_tensor(Wb, device="cuda")
+        for form in (1, 2):
+            x = torch.zeros(nv, dtype=torch.float64, device="cuda")
+            assert lib.dgp_lm_update(_v(Jt), nv, nm, _v(Wd), _v(yd), 1e-2, _v(x), form, None, None) == 1, (bad, form)
