@@ -420,8 +420,9 @@ int dgp_jacobian_tg_vjp(const int32_t *d_P_rowptr, const int32_t *d_P_col,
  * barycentric weight is largest (ties: lower element id) when that weight is
  * >= -eps, else -1; d_w[i][0..3] its barycentric weights for the vertices
  * d_elem[e][0..3] (zeros when d_eid[i] == -1).  d_node [nn][3] float64,
- * d_elem [ne][4] int32 (0-based).  Bins the elements on the device; the
- * call synchronises the stream. */
+ * d_elem [ne][4] int32 (0-based; DGP_ERR_MESH when an id is outside
+ * [0, nn)).  Bins the elements on the device; the call synchronises the
+ * stream. */
 int dgp_locate_points(const double *d_node, const int32_t *d_elem, int64_t nn,
                       int64_t ne, const double *d_pts, int64_t np, double eps,
                       int32_t *d_eid, double *d_w, dgp_stream_t stream);
@@ -432,8 +433,9 @@ int dgp_locate_points(const double *d_node, const int32_t *d_elem, int64_t nn,
  * (int32, 0-based) that contain that node (ties: lower face index):
  * d_out_pos[i] = that point, d_out_dir[i] = the face's normal
  * -cross(b - a, c - a) normalised (inward for outward-ordered faces),
- * d_out_face[i] = the face.  DGP_ERR_ARG when a position finds no boundary
- * node or face.  Synchronises the stream. */
+ * d_out_face[i] = the face.  DGP_ERR_MESH when a face node id is outside
+ * [0, nn); DGP_ERR_ARG when a position finds no boundary node or face.
+ * Synchronises the stream. */
 int dgp_snap_to_surface(const double *d_node, int64_t nn, const int32_t *d_bnd,
                         const int32_t *d_face, int64_t nface, const double *d_pos,
                         int64_t n, double *d_out_pos, double *d_out_dir,
@@ -486,7 +488,8 @@ int dgp_row_dots(const float *d_Jt, int64_t nv, int64_t nmeas, const double *d_w
  * form 2 the nmeas x nmeas one, J_w^T (J_w J_w^T + mu I)^-1 W^1/2 y with
  * J_w = W^1/2 J and mu = lambda max_i (J^T W J)_ii (the same update, far less
  * work when nmeas < nv); form 0 picks the smaller.  *form_used (may be NULL)
- * reports 1 or 2.  Allocates its work arrays; synchronises the stream. */
+ * reports 1 or 2.  Both forms return DGP_ERR_ARG unless every weight is finite
+ * and non-negative.  Allocates its work arrays; synchronises the stream. */
 int dgp_lm_update(const float *d_Jt, int64_t nv, int64_t nmeas, const double *d_w,
                   const double *d_y, double lambda, double *d_x, int32_t form,
                   int32_t *form_used, dgp_stream_t stream);

@@ -213,3 +213,28 @@ def test_optode_snap_device_equals_host():
     for b_dev, b_host in ((o_dev.s_bary, o_host.s_bary), (o_dev.d_bary, o_host.d_bary)):
         pt = lambda b: (b[:, 1:, None] * mesh.node_host[mesh.elem_host[b[:, 0].astype(int)]]).sum(1)
         assert np.abs(pt(b_dev) - pt(b_host)).max() < 1e-9
+
+
+def test_locate_and_snap_reject_out_of_range_node_ids():
+    """An element or face node id outside [0, nn) is DGP_ERR_MESH, raised before any
+    kernel indexes the node array with it; a valid call afterwards still works."""
+    from dogpup_b200 import api
+    from dogpup_b200._lib import DgpError
+    from dogpup_b200.meshgen import box_mesh
+    m = box_mesh((3, 3, 3), 1.0)
+    pts = np.array([[1.5, 1.5, 1.5]])
+    for bad in (m.node.shape[0], -1):
+        elem = m.elem.astype(np.int64).copy()
+        elem[5, 2] = bad
+        with pytest.raises(DgpError) as ei:
+            api.locate_points(m.node, elem, pts)
+        assert ei.value.code == 4 and "node index out of range" in str(ei.value)
+    eid, _ = api.locate_points(m.node, m.elem.astype(np.int64), pts)
+    assert int(eid[0]) >= 0
+    mesh, pos = _snap_case()
+    for bad in (mesh.nn, -7):
+        face = np.array(mesh.face_host, copy=True)
+        face[3, 1] = bad
+        with pytest.raises(DgpError) as ei:
+            api.snap_to_surface(mesh.node_host, mesh.fem.bnd, face, pos[:3])
+        assert ei.value.code == 4 and "node index out of range" in str(ei.value)
