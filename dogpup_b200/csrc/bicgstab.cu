@@ -1978,6 +1978,7 @@ int solver_build(SolverPlan *S, const int32_t *d_rowptr, const int32_t *d_col, i
   }
   DGP_REQUIRE(ns_max >= 1 && ns_max <= 128, "solver: 1 <= ns_max <= 128 sources per harmonic");
   DGP_REQUIRE(nnz < INT32_MAX && n < (1 << 24), "solver: nnz must fit int32 and n < 2^24");
+  DGP_TRY(csr_in_range(d_rowptr, d_col, n, n, nnz, 0, "solver: pattern", st));
   S->n = n;
   S->nnz = nnz;
   S->nf = nf;

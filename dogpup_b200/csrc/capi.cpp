@@ -364,8 +364,12 @@ int dgp_spmm_A(const int32_t *d_rowptr, const int32_t *d_col, const double *d_KM
 int dgp_fsai_pattern(const int32_t *d_rowptr, const int32_t *d_col, const double *d_K, const double *d_M, double dfc,
                      int64_t n, int32_t cap, int32_t *d_rowptrG, int32_t *d_colG, dgp_stream_t stream) {
   if (!d_rowptr || !d_col || !d_K || !d_M || !d_rowptrG) return fail(DGP_ERR_ARG, "fsai_pattern: null pointer");
-  DGP_GUARD(fsai_pattern_rows(d_rowptr, d_col, d_K, d_M, dfc, n, cap, d_rowptrG, d_colG, nullptr, nullptr,
-                              (cudaStream_t)stream));
+  if (n <= 0) return fail(DGP_ERR_ARG, "fsai pattern: need n > 0 and 1 <= cap <= 32");
+  DGP_GUARD([&] {
+    DGP_TRY(csr_in_range(d_rowptr, d_col, n, n, -1, 0, "fsai_pattern: A", (cudaStream_t)stream));
+    return fsai_pattern_rows(d_rowptr, d_col, d_K, d_M, dfc, n, cap, d_rowptrG, d_colG, nullptr, nullptr,
+                             (cudaStream_t)stream);
+  }());
 }
 
 int dgp_fsai_factor(const int32_t *d_rowptr, const int32_t *d_col, const double *d_K, const double *d_M, double dfc,

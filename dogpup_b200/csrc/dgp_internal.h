@@ -130,6 +130,14 @@ int solver_set_dot_rows(SolverPlan *S, int32_t mult);
 // largest relative difference between the tiled and the gather SpMM on the plan's operators
 int solver_check_spmm(SolverPlan *S, double *max_rel, cudaStream_t st);
 
+// DGP_ERR_MESH unless every id in d_ids[0..count) lies in [0, limit) (synchronises the stream)
+int ids_in_range(const int32_t *d_ids, int64_t count, int64_t limit, const char *who, cudaStream_t st);
+// DGP_ERR_MESH unless d_rowptr[0..nrows] starts at 0, never decreases and (nnz >= 0) ends at nnz, no
+// row holds more than max_row entries (max_row > 0), and every column id lies in [0, ncols)
+// (synchronises the stream)
+int csr_in_range(const int32_t *d_rowptr, const int32_t *d_col, int64_t nrows, int64_t ncols, int64_t nnz,
+                 int64_t max_row, const char *who, cudaStream_t st);
+
 // containing tetrahedron (-1: none) and barycentric weights [np][4] of points [np][3]
 int locate_points(const double *d_node, const int32_t *d_elem, int64_t nn, int64_t ne, const double *d_pts,
                   int64_t np, double eps, int32_t *d_eid, double *d_w, cudaStream_t st);

@@ -282,6 +282,8 @@ int fsai_factor_full(const int32_t *d_rowptr, const int32_t *d_col, const double
                      int64_t n, const int32_t *d_rowptrG, const int32_t *d_colG, int32_t nf, double2 *d_G,
                      cudaStream_t st) {
   DGP_REQUIRE(n > 0 && nf > 0, "fsai_factor: sizes must be positive");
+  DGP_TRY(csr_in_range(d_rowptr, d_col, n, n, -1, 0, "fsai_factor: A", st));
+  DGP_TRY(csr_in_range(d_rowptrG, d_colG, n, n, -1, 0, "fsai_factor: G pattern", st));
   DevBuf m, im;
   DGP_TRY(m.alloc(sizeof(int)));
   DGP_CUDA(cudaMemsetAsync(m.p, 0, sizeof(int), st));

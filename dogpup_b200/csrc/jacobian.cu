@@ -25,6 +25,7 @@
 // each gate coefficient read from shared memory feeds MT complex products.
 #include <algorithm>
 #include <type_traits>
+#include <vector>
 
 #include "dgp_common.cuh"
 #include "dgp_internal.h"
@@ -286,6 +287,20 @@ int jacobian_run(int mode, const int32_t *prow, const int32_t *pcol, const doubl
   size_t smem;
   int grid;
   DGP_TRY(launch_common(a, smem, grid));
+  // the link table addresses the staged fields in shared memory and P's columns address the
+  // fields in HBM: both are checked before the first kernel uses them
+  {
+    std::vector<int32_t> hl(2 * (size_t)nm);
+    DGP_CUDA(cudaMemcpyAsync(hl.data(), link, sizeof(int32_t) * 2 * nm, cudaMemcpyDeviceToHost, st));
+    DGP_CUDA(cudaStreamSynchronize(st));
+    for (int m = 0; m < nm; ++m)
+      if (hl[2 * m] < 0 || hl[2 * m] >= ns || hl[2 * m + 1] < 0 || hl[2 * m + 1] >= nd)
+        return fail(DGP_ERR_ARG, "jacobian: link index out of range");
+  }
+  if (prow) {
+    DGP_REQUIRE(pcol && pval, "jacobian: null basis column or value array");
+    DGP_TRY(csr_in_range(prow, pcol, nv, nn, -1, PMAX, "jacobian basis", st));
+  }
   DevBuf ctab, finv, chat;
   DGP_TRY(ctab.alloc(sizeof(float2) * (size_t)std::max(1, ng) * nf));
   DGP_TRY(finv.alloc(sizeof(double2) * nf));

@@ -137,29 +137,7 @@ __global__ void k_locate(const double *__restrict__ node, const int32_t *__restr
   for (int l = 0; l < 4; ++l) wout[4 * t + l] = ok ? bw[l] : 0.0;
 }
 
-// *err = 1 when any of ids[0..count) lies outside [0, limit)
-__global__ void k_ids_in_range(const int32_t *__restrict__ ids, int64_t count, int64_t limit, int *err) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
-    if (ids[i] < 0 || ids[i] >= limit) atomicOr(err, 1);
-}
-
 }  // namespace
-
-// DGP_ERR_MESH unless every node id in ids[0..count) (count > 0) is in [0, nn): the kernels below index
-// the node array with them unchecked.
-static int node_ids_in_range(const int32_t *ids, int64_t count, int64_t nn, const char *who, cudaStream_t st) {
-  DevBuf err;
-  DGP_TRY(err.alloc(sizeof(int)));
-  DGP_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), st));
-  k_ids_in_range<<<(unsigned)std::min<int64_t>(ceil_div(count, 256), 148 * 16), 256, 0, st>>>(ids, count, nn,
-                                                                                             err.as<int>());
-  DGP_CHECK_LAUNCH();
-  int h = 0;
-  DGP_CUDA(cudaMemcpyAsync(&h, err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-  DGP_CUDA(cudaStreamSynchronize(st));
-  if (h) return fail(DGP_ERR_MESH, std::string(who) + ": node index out of range");
-  return DGP_OK;
-}
 
 int locate_points(const double *d_node, const int32_t *d_elem, int64_t nn, int64_t ne, const double *d_pts,
                   int64_t np, double eps, int32_t *d_eid, double *d_w, cudaStream_t st) {
@@ -167,7 +145,7 @@ int locate_points(const double *d_node, const int32_t *d_elem, int64_t nn, int64
   DGP_REQUIRE(nn > 0 && ne > 0 && np >= 0, "locate_points: bad sizes");
   if (np == 0) return DGP_OK;
   DGP_REQUIRE(d_pts && d_eid && d_w, "locate_points: null point pointer");
-  DGP_TRY(node_ids_in_range(d_elem, 4 * ne, nn, "locate_points", st));
+  DGP_TRY(ids_in_range(d_elem, 4 * ne, nn, "locate_points", st));
   // bins: bounding box of the nodes, cells of about two mean element edges
   std::vector<double> h((size_t)3 * nn);
   DGP_CUDA(cudaMemcpyAsync(h.data(), d_node, sizeof(double) * 3 * nn, cudaMemcpyDeviceToHost, st));
@@ -502,7 +480,7 @@ int snap_to_surface(const double *d_node, int64_t nn, const int32_t *d_bnd, cons
   DGP_REQUIRE(d_node && d_bnd && d_face && d_pos && d_out_pos && d_out_dir && d_out_face,
               "snap_to_surface: null pointer");
   DGP_REQUIRE(n <= INT32_MAX, "snap_to_surface: too many optodes");
-  DGP_TRY(node_ids_in_range(d_face, 3 * nface, nn, "snap_to_surface", st));
+  DGP_TRY(ids_in_range(d_face, 3 * nface, nn, "snap_to_surface", st));
   k_snap<<<(unsigned)n, SNAP_NT, 0, st>>>(d_node, nn, d_bnd, d_face, nface, d_pos, d_out_pos, d_out_dir, d_out_face);
   DGP_CHECK_LAUNCH();
   std::vector<int32_t> hf((size_t)n);

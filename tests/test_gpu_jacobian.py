@@ -114,3 +114,38 @@ def test_tg_jacobian_odd_sizes(ng):
     v = api.jacobian_tg_vjp(nb, phi, phiA, mesh.optode.s_fpsf, link, torch.as_tensor(gfc, device="cuda"), nt,
                             torch.as_tensor(g))
     assert rel(v.cpu().numpy(), np.einsum("mgv,mg->v", J0, g)) < 1e-5
+
+
+def test_jacobian_rejects_bad_link_and_basis(jac_case):
+    """Link entries outside [0, ns) x [0, nd) are DGP_ERR_ARG; basis columns outside [0, nn)
+    and basis rows of more than 8 entries are DGP_ERR_MESH -- all raised before a kernel
+    addresses shared memory or the fields with them."""
+    import scipy.sparse as sp
+    import torch
+    from dogpup_b200 import api
+    from dogpup_b200._lib import DgpError
+    mesh = jac_case["mesh"]
+    phi, phiA = jac_case["phi"], jac_case["phiA"]
+    nt = len(mesh.optode.tAxis)
+    nn, ns, nd = phi.shape[1], phi.shape[2], phiA.shape[2]
+    link = mesh._link()
+    nb = mesh.nodal_basis()
+    for j, bad in ((0, ns), (1, nd), (0, -1)):
+        lk = link.clone()
+        lk[2, j] = bad
+        with pytest.raises(DgpError) as ei:
+            api.jacobian_tg(nb, phi, phiA, mesh.optode.s_fpsf, lk, jac_case["gfc_d"], nt)
+        assert ei.value.code == 1 and "link index out of range" in str(ei.value)
+    P = sp.csr_matrix((np.full(3, 1 / 3), ([0, 1, 2], [0, 1, 2])), shape=(3, nn))
+    b = api.Basis(P, np.ones(3))
+    b.col[1] = nn
+    with pytest.raises(DgpError) as ei:
+        api.jacobian_complex(b, phi, phiA, mesh.optode.s_fpsf, link)
+    assert ei.value.code == 4 and "column index out of range" in str(ei.value)
+    P9 = sp.csr_matrix((np.full(9, 1 / 9), (np.zeros(9, int), np.arange(9))), shape=(2, nn))
+    gin = torch.zeros((link.shape[0], jac_case["gfc_d"].shape[0]), dtype=torch.float64)
+    with pytest.raises(DgpError) as ei:
+        api.jacobian_tg_vjp(api.Basis(P9, np.ones(2)), phi, phiA, mesh.optode.s_fpsf, link, jac_case["gfc_d"], nt, gin)
+    assert ei.value.code == 4 and "more than 8 entries" in str(ei.value)
+    J = api.jacobian_complex(api.Basis(P, np.ones(3)), phi, phiA, mesh.optode.s_fpsf, link)
+    assert torch.isfinite(torch.view_as_real(J)).all()

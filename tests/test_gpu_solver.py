@@ -58,6 +58,35 @@ def test_fem_rejects_degenerate_tet(torch):
         api.Fem(node, elem, 1.4)
 
 
+def test_solver_and_fsai_reject_a_bad_pattern(gpu_case, torch):
+    """A CSR column outside [0, n) or a decreasing row pointer is DGP_ERR_MESH at solver
+    creation, in dgp_fsai_pattern and in dgp_fsai_factor (G pattern), before any kernel
+    indexes with it; a row pointer that does not end at nnz is DGP_ERR_MESH at creation."""
+    from dogpup_b200 import api, DgpError
+    from dogpup_b200._lib import lib
+    fem = gpu_case["fem"]
+    n = fem.nn
+    K, M = gpu_case["K"], gpu_case["M"]
+    dfc = 2 * np.pi / 10e-9 / (C_VAC / 1.4)
+    bad_col = fem.col.clone()
+    bad_col[5] = n
+    bad_row = fem.rowptr.clone()
+    bad_row[3] = bad_row[4] + 1
+    for rp, cl, msg in ((fem.rowptr, bad_col, "column index out of range"), (bad_row, fem.col, "must start at 0")):
+        with pytest.raises(DgpError) as ei:
+            api.Solver(rp, cl, K, M, dfc, 2, 2)
+        assert ei.value.code == 4 and msg in str(ei.value)
+        rpg = torch.empty(n + 1, dtype=torch.int32, device="cuda")
+        assert lib.dgp_fsai_pattern(api.ptr(rp), api.ptr(cl), api.ptr(K), api.ptr(M), dfc, n, 30, api.ptr(rpg), None,
+                                    api.stream_ptr()) == 4
+        G = torch.empty((1, int(cl.numel())), dtype=torch.complex128, device="cuda")
+        assert lib.dgp_fsai_factor(api.ptr(fem.rowptr), api.ptr(fem.col), api.ptr(K), api.ptr(M), dfc, n, api.ptr(rp),
+                                   api.ptr(cl), 1, api.ptr(torch.view_as_real(G)), api.stream_ptr()) == 4
+    with pytest.raises(DgpError) as ei:
+        api.Solver(fem.rowptr, fem.col[:-1].contiguous(), K, M, dfc, 2, 2)
+    assert ei.value.code == 4 and "not at nnz" in str(ei.value)
+
+
 def test_fsai_pattern_and_factor(small_case, gpu_case, torch):
     from dogpup_b200 import api
     from dogpup_b200._lib import lib, check
