@@ -210,7 +210,9 @@ typedef struct dgp_solver_s *dgp_solver_t;
 /* Creates a solver for A_k = K + i*k*dfc*M, k = 0..nf-1, on the CSR pattern
  * (d_rowptr, d_col) with values d_K, d_M (float64, copied), for up to
  * ns_max sources per harmonic.  dfc = df/c (rad/s over mm/s).  Builds the
- * FSAI pattern and factors for all harmonics and allocates the workspace. */
+ * FSAI pattern and factors for all harmonics and allocates the workspace.
+ * DGP_ERR_MESH unless d_rowptr starts at 0, never decreases and ends at nnz
+ * and every column lies in [0, n). */
 int dgp_solver_create(dgp_solver_t *solver, const int32_t *d_rowptr,
                       const int32_t *d_col, int64_t n, int64_t nnz,
                       const double *d_K, const double *d_M, double dfc,
@@ -320,13 +322,15 @@ int dgp_spmm_A(const int32_t *d_rowptr, const int32_t *d_col,
                dgp_stream_t stream);
 /* FSAI pattern (rule of dMesh.m:1361-1380) of tril(K + i*dfc*M): counts
  * rows first (d_rowptrG [n+1]), then fills columns with a second call that
- * passes d_colG (size from d_rowptrG[n]). */
+ * passes d_colG (size from d_rowptrG[n]).  DGP_ERR_MESH for a malformed CSR
+ * (row pointer not starting at 0 or decreasing, column outside [0, n)). */
 int dgp_fsai_pattern(const int32_t *d_rowptr, const int32_t *d_col,
                      const double *d_K, const double *d_M, double dfc,
                      int64_t n, int32_t cap, int32_t *d_rowptrG,
                      int32_t *d_colG, dgp_stream_t stream);
 /* FSAI factor values G[k][slot] (complex128) for k = 0..nf-1 of
- * A_k = K + i*k*dfc*M on the pattern (arithmetic of FSAIP_CUDA.cu:92-160). */
+ * A_k = K + i*k*dfc*M on the pattern (arithmetic of FSAIP_CUDA.cu:92-160).
+ * DGP_ERR_MESH when the CSR of A or of the G pattern is malformed. */
 int dgp_fsai_factor(const int32_t *d_rowptr, const int32_t *d_col,
                     const double *d_K, const double *d_M, double dfc,
                     int64_t n, const int32_t *d_rowptrG, const int32_t *d_colG,
@@ -382,6 +386,9 @@ int dgp_tg_adjoint_rhs(const int32_t *d_det_nodes, const double *d_det_w,
  *  adjoint fluence as dgp_solve writes them); d_fpsf [nf] complex128;
  *  d_link [nm][2] (source, detector).  Outputs use the reference's memory
  *  order: voxel slowest, measurement fastest.
+ *  Checked before any kernel runs: a link entry outside [0, ns) x [0, nd) is
+ *  DGP_ERR_ARG; a malformed P (row pointer not starting at 0 or decreasing,
+ *  a row of more than 8 entries, a column outside [0, nn)) is DGP_ERR_MESH.
  * ====================================================================== */
 /* J[v][k][m] complex128 = -(P phi_s)(P phiA_d) w_v / s_fpsf[k]. */
 int dgp_jacobian_complex(const int32_t *d_P_rowptr, const int32_t *d_P_col,
