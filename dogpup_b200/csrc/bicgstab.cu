@@ -2166,7 +2166,10 @@ int solver_solve(SolverPlan *S, const double *d_B, const int32_t *d_nodes, const
   if (r->d_status)
     DGP_CUDA(cudaMemcpyAsync(r->d_status, out.data(), sizeof(int) * out.size(), cudaMemcpyHostToDevice, st));
   DGP_CUDA(cudaStreamSynchronize(st));
-  if (rc == DGP_ERR_NOT_CONVERGED) return fail(DGP_ERR_NOT_CONVERGED, "solve: tolerance not reached within maxit");
+  // any column that missed tol -- maxit, a breakdown or a non-finite value -- makes the call NOT_CONVERGED
+  if (rc == DGP_ERR_NOT_CONVERGED || bad > 0)
+    return fail(DGP_ERR_NOT_CONVERGED, "solve: " + std::to_string(bad) + " of " + std::to_string(out.size()) +
+                                           " columns did not reach tol (per-column status in the report)");
   return DGP_OK;
 }
 

@@ -37,7 +37,8 @@ typedef enum dgp_status {
   DGP_ERR_NOMEM = 3,      /* device allocation failed                       */
   DGP_ERR_MESH = 4,       /* degenerate mesh / pattern (e.g. zero volume)   */
   DGP_ERR_NOT_CONVERGED = 5, /* solver hit maxit before tol (x still valid) */
-  DGP_ERR_BREAKDOWN = 6,  /* BiCGSTAB breakdown (rho or omega = 0 / non-finite) */
+  DGP_ERR_BREAKDOWN = 6,  /* reserved: solves report a breakdown per column
+                           (DGP_COL_BREAKDOWN_*) under DGP_ERR_NOT_CONVERGED */
   DGP_ERR_UNSUPPORTED = 7
 } dgp_status;
 
@@ -273,7 +274,9 @@ int dgp_solver_check_spmm(dgp_solver_t solver, double *max_rel,
 
 /* Solves A_k X[k] = B[k] for every harmonic, B and X complex128
  * [NF][NN][NS] with ns <= ns_max.  Synchronises the stream; returns
- * DGP_ERR_NOT_CONVERGED if any column missed tol (X is still written). */
+ * DGP_ERR_NOT_CONVERGED if any column missed tol -- maxit, a breakdown or a
+ * non-finite value, told apart by the per-column status words (X is still
+ * written). */
 int dgp_solve(dgp_solver_t solver, const double *d_B, double *d_X, int32_t ns,
               const dgp_solve_opts *opts, dgp_solve_report *report,
               dgp_stream_t stream);

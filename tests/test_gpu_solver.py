@@ -190,6 +190,48 @@ def test_solver_dense_rhs_and_status(small_case, gpu_case, torch):
     assert np.abs(X[:, :, 2].cpu().numpy()).max() == 0.0
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_solver_flags_a_nonfinite_column(small_case, gpu_case, torch, precision):
+    """A right-hand side column holding a NaN is frozen as DGP_COL_NONFINITE and the call
+    returns DGP_ERR_NOT_CONVERGED (reported with the status words, not raised); the other
+    columns are unaffected and converge; tol = 0 and maxit = 0 are DGP_ERR_ARG."""
+    from dogpup_b200 import api, DgpError
+    from dogpup_b200._lib import lib
+    from oracle import solver as osv
+    K0, M0 = small_case["K"], small_case["M"]
+    nf, ns = 2, 3
+    dfc = 2 * np.pi / 10e-9 / (C_VAC / 1.4)
+    n = K0.shape[0]
+    rng = np.random.default_rng(4)
+    B = rng.standard_normal((nf, n, ns)) + 1j * rng.standard_normal((nf, n, ns))
+    B[1, 17, 1] = np.nan
+    fem = gpu_case["fem"]
+    S = api.Solver(fem.rowptr, fem.col, gpu_case["K"], gpu_case["M"], dfc, nf, ns)
+    status = torch.full((nf * ns,), -1, dtype=torch.int32, device="cuda")
+    Bd = torch.as_tensor(B, device="cuda")
+    X = torch.empty_like(Bd)
+    rep = api._lib.SolveReport()
+    rep.d_status = api.ptr(status)
+    o = api.make_opts(tol=1e-10, precision=precision)
+    rc = lib.dgp_solve(S._h, api.ptr(api.as_real(Bd)), api.ptr(api.as_real(X)), ns, api.C.byref(o),
+                       api.C.byref(rep), api.stream_ptr())
+    assert rc == 5 and rep.n_not_converged == 1
+    st = status.cpu().numpy().reshape(nf, ns)
+    assert st[1, 1] == 4 and (np.delete(st.ravel(), ns + 1) == 0).all()
+    B2 = B.copy()
+    B2[1, :, 1] = 0
+    xd = np.transpose(osv.direct_solve(K0, M0, dfc, np.transpose(B2, (1, 2, 0))), (2, 0, 1))
+    Xh = X.cpu().numpy()
+    for k in range(nf):
+        for s in range(ns):
+            if (k, s) != (1, 1):
+                assert rel(Xh[k, :, s], xd[k, :, s]) < 1e-6, (k, s)
+    for bad in (dict(tol=0.0), dict(tol=1e-10, maxit=0)):
+        with pytest.raises(DgpError) as ei:
+            S.solve(torch.as_tensor(np.nan_to_num(B), device="cuda"), api.make_opts(precision=precision, **bad))
+        assert ei.value.code == 1
+
+
 @pytest.mark.parametrize("precision", ["mixed", "mixed_bicgstab"])
 def test_solver_mixed_precision_accuracy(small_case, gpu_case, torch, precision):
     """Both complex-FP32 inner solvers (COCG, BiCGSTAB) refined in FP64 reach the
