@@ -23,6 +23,7 @@ rows are weighted by a diagonal W = 1/sigma^2 or by 1.
 from __future__ import annotations
 
 import ctypes as C
+import warnings
 
 import numpy as np
 import torch
@@ -172,7 +173,11 @@ class LMRecon:
         the fitted gates: the reference's damping rule floors lambda at the
         residual norm (wghtd_LM_recon.m:118-120), which keeps its meaning only
         when the weighted norm is on the scale of the unweighted one.
-        Returns a history dict."""
+        Returns a history dict; its "exit" names the rule that ended the loop:
+        "converged" (:91-95), "max_iter" (:158-161), "nan_update" (:136-141) or
+        "negative_mua" (:146-152; both warn and leave mua at the last accepted
+        update, as the reference does), or "model_data" (a model gate without a
+        logarithm, also recorded under "stopped")."""
         m = self.mesh
         data_m = np.asarray(data_m, dtype=np.float64)
         # gates in the id_thresh window whose measured value has a logarithm (a truncated Fourier
@@ -203,6 +208,7 @@ class LMRecon:
             y = dm - torch.log(_flat(data_c))[incl]                   # :60-64
             if not bool(torch.isfinite(y).all()):
                 hist["stopped"] = "model data not positive on an included gate"
+                hist["exit"] = "model_data"
                 break
             if Js is not None:                                        # :72-76
                 ws = reshape_J(Jt, Js, lam[1], self.normal_eq)        # [NS][NM]
@@ -224,6 +230,7 @@ class LMRecon:
                 callback(count, hist)
             if count > 1 and hist["err_del"][-1] < 0 and (abs(hist["err_del"][-1]) < 0.12 or
                                                            hist["err_perc"][-1] < 1.5):      # :91-95
+                hist["exit"] = "converged"
                 break
             count += 1
             if count == 1 or hist["err_del"][-1] < 0:                 # :100-106
@@ -239,15 +246,20 @@ class LMRecon:
             upd = self._tik(Jg, lam1, y.contiguous(), None if Js is not None else w)   # :125-127
             x = G * upd                                               # :131
             d_mu = torch.as_tensor(self.g2m_in @ x.cpu().numpy(), device="cuda")   # :132
-            if torch.isnan(d_mu).any():
+            if torch.isnan(d_mu).any():                               # :136-141
+                hist["exit"] = "nan_update"
+                warnings.warn("LM: NaN absorption update, stopping the reconstruction")
                 break
             new_mu = m.mua + d_mu
-            if (new_mu < 0).any():
+            if (new_mu < 0).any():                                    # :146-152: the update is not applied
+                hist["exit"] = "negative_mua"
+                warnings.warn("LM: negative absorption update, stopping the reconstruction")
                 break
             m.mua = new_mu.contiguous()
             m.update_properties()                                     # :153
             hist["mua"].append(m.mua.clone())
             if count > max_iter - 1:
+                hist["exit"] = "max_iter"
                 break
             y_prev, J_prev = y, Jt
         hist["iterations"] = count
