@@ -38,6 +38,7 @@ _SIGS = {
     "dgp_status_string": (C.c_char_p, [C.c_int]),
     "dgp_version": (C.c_int, []),
     "dgp_kernel_launches": (I64, []),
+    "dgp_device_allocations": (I64, []),
     "dgp_smv_mex": (C.c_int, [P, P, P, P, P, P, P, P, P, C.c_int, C.c_int, C.c_int, P]),
     "dgp_fsaimv_mex": (C.c_int, [P, P, P, P, P, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, P]),
     "dgp_fsaip_mex": (C.c_int, [P, P, P, P, P, P, P, P, C.c_int, C.c_int, P]),
@@ -74,6 +75,7 @@ _SIGS = {
     "dgp_td2fc": (C.c_int, [P, I64, I32, P, P, I32, P, P]),
     "dgp_fc2td": (C.c_int, [P, I64, I32, P, P, I32, P, P]),
     "dgp_fc2tg": (C.c_int, [P, I64, I32, P, I32, I32, P, P]),
+    "dgp_csr_spmv": (C.c_int, [P, P, P, I64, I64, P, P, P]),
     "dgp_tg_adjoint_rhs": (C.c_int, [P, P, I32, P, I32, P, I32, I32, P, I64, I32, I32, P, P]),
     "dgp_locate_points": (C.c_int, [P, P, I64, I64, P, I64, D, P, P, P]),
     "dgp_grid_to_mesh": (C.c_int, [P, I64, P, P, P, P, P, P, P]),

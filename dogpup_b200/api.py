@@ -202,7 +202,7 @@ def td2fc(x: torch.Tensor, f: torch.Tensor, t: torch.Tensor) -> torch.Tensor:
 
 
 def fc2td(c: torch.Tensor, f: torch.Tensor, t: torch.Tensor) -> torch.Tensor:
-    """Time-domain signal from coefficients along the last axis (fc2td.m:60-71)."""
+    """Time-domain signal from coefficients along the last axis (fc2td.m:24-31)."""
     c2 = c.to(torch.complex128).reshape(-1, c.shape[-1]).contiguous()
     f = f.to(device="cuda", dtype=torch.float64).contiguous()
     t = t.to(device="cuda", dtype=torch.float64).contiguous()
@@ -213,13 +213,42 @@ def fc2td(c: torch.Tensor, f: torch.Tensor, t: torch.Tensor) -> torch.Tensor:
 
 
 def fc2tg(c: torch.Tensor, gate_fc: torch.Tensor, nt: int) -> torch.Tensor:
-    """Time-gated data from coefficients along the last axis (fc2tg.m:100-111)."""
+    """Time-gated data from coefficients along the last axis (fc2tg.m:25-32)."""
     c2 = c.to(torch.complex128).reshape(-1, c.shape[-1]).contiguous()
     g = gate_fc.to(device="cuda", dtype=torch.complex128).contiguous()
     out = torch.empty((c2.shape[0], g.shape[0]), dtype=torch.float64, device="cuda")
     check(lib.dgp_fc2tg(ptr(as_real(c2)), c2.shape[0], c2.shape[1], ptr(as_real(g)), g.shape[0], int(nt),
                         ptr(out), stream_ptr()))
     return out.reshape(*c.shape[:-1], g.shape[0])
+
+
+class DeviceCsr:
+    """A real FP64 CSR matrix on the device with ``A @ x`` through ``dgp_csr_spmv``.
+
+    Built from a SciPy sparse matrix; the pattern is checked once here (row pointer
+    from 0, non-decreasing, ending at nnz; columns in range) so the kernel gets a
+    well-formed matrix."""
+
+    def __init__(self, A):
+        A = A.tocsr()
+        A.sort_indices()
+        ip, ix = np.asarray(A.indptr, dtype=np.int64), np.asarray(A.indices, dtype=np.int64)
+        if ip[0] != 0 or ip[-1] != ix.size or (np.diff(ip) < 0).any() or (ix.size and (ix.min() < 0 or
+                                                                                      ix.max() >= A.shape[1])):
+            raise ValueError("DeviceCsr: malformed CSR pattern")
+        self.shape = A.shape
+        self.rowptr = torch.as_tensor(ip.astype(np.int32), device="cuda")
+        self.col = torch.as_tensor(ix.astype(np.int32), device="cuda")
+        self.val = torch.as_tensor(np.asarray(A.data, dtype=np.float64), device="cuda")
+
+    def __matmul__(self, x: torch.Tensor) -> torch.Tensor:
+        x = x.to(device="cuda", dtype=torch.float64).contiguous()
+        if x.numel() != self.shape[1]:
+            raise ValueError(f"DeviceCsr: x has {x.numel()} entries, the matrix {self.shape[1]} columns")
+        y = torch.empty(self.shape[0], dtype=torch.float64, device="cuda")
+        check(lib.dgp_csr_spmv(ptr(self.rowptr), ptr(self.col), ptr(self.val), self.shape[0], self.shape[1], ptr(x),
+                               ptr(y), stream_ptr()))
+        return y
 
 
 class Basis:

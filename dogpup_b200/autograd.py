@@ -2,7 +2,7 @@
 
 ``TimeGatedForward(mesh, gate_fc)(mua, musp)`` returns the time-gated detector
 data y[m][g] = fc2tg(meas_flu(phi))  (DOGPUP/dMesh.m:80-171 then
-DOGPUP/fc2tg.m:100-111) as a torch tensor with a backward pass.  The reference
+DOGPUP/fc2tg.m:25-32) as a torch tensor with a backward pass.  The reference
 gets sensitivities from the explicit absorption Jacobian (J_complex,
 dMesh.m:206-247, kappa held fixed); here backward is the adjoint method:
 one batched solve of A_k lam = dL/dphi per source x harmonic (the same batch

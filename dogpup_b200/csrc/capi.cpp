@@ -16,6 +16,7 @@ namespace dgp {
 
 static thread_local std::string g_err;
 static std::atomic<int64_t> g_launches{0};
+static std::atomic<int64_t> g_device_allocs{0};
 
 void count_launches(int64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 int64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
@@ -39,6 +40,7 @@ int DevBuf::alloc(size_t n) {
   release();
   if (n == 0) n = 16;
   cudaError_t e = cudaMalloc(&p, n);
+  g_device_allocs.fetch_add(1, std::memory_order_relaxed);
   if (e != cudaSuccess) {
     p = nullptr;
     cudaGetLastError();
@@ -77,6 +79,8 @@ int fc2td_run(const double *c, int64_t nr, int nf, const double *f, const double
 int fc2tg_run(const double *c, int64_t nr, int nf, const double *gate, int ng, int nt, double *y, cudaStream_t st);
 int meas_run(const int32_t *dn, const double *dw, int nd, const int32_t *link, int nm, const double *phi, int64_t n,
              int nf, int ns, double *data, cudaStream_t st);
+int csr_spmv_run(const int32_t *rowptr, const int32_t *col, const double *val, int64_t nrows, int64_t ncols,
+                 const double *x, double *y, cudaStream_t st);
 int mex_fsaip(double *out_re, double *out_im, const double *A_re, const double *A_im, const int *rPtrA,
               const int *cPtrA, const int *rPtrG, const int *cPtrG, int nfreqs, int nrows, cudaStream_t st,
               int es = 1);
@@ -135,6 +139,8 @@ const char *dgp_status_string(int s) {
 int dgp_version(void) { return 10000; }
 
 int64_t dgp_kernel_launches(void) { return launch_count(); }
+
+int64_t dgp_device_allocations(void) { return g_device_allocs.load(std::memory_order_relaxed); }
 
 // ------------------------------------------------------------ mex layouts
 int dgp_smv_mex(double *d_out_real, double *d_out_imag, const double *d_x_real, const double *d_x_imag,
@@ -393,6 +399,11 @@ int dgp_fsai_apply(const int32_t *d_rowptrG, const int32_t *d_colG, const double
 int dgp_meas(const int32_t *d_det_nodes, const double *d_det_w, int32_t nd, const int32_t *d_link, int32_t nm,
              const double *d_phi, int64_t n, int32_t nf, int32_t ns, double *d_data, dgp_stream_t stream) {
   DGP_GUARD(meas_run(d_det_nodes, d_det_w, nd, d_link, nm, d_phi, n, nf, ns, d_data, (cudaStream_t)stream));
+}
+
+int dgp_csr_spmv(const int32_t *d_rowptr, const int32_t *d_col, const double *d_val, int64_t nrows, int64_t ncols,
+                 const double *d_x, double *d_y, dgp_stream_t stream) {
+  DGP_GUARD(csr_spmv_run(d_rowptr, d_col, d_val, nrows, ncols, d_x, d_y, (cudaStream_t)stream));
 }
 
 int dgp_td2fc(const double *d_x, int64_t nr, int32_t nt, const double *d_t, const double *d_f, int32_t nf,

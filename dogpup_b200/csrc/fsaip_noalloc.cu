@@ -10,19 +10,27 @@
 // entry point therefore uses no allocation of any kind: its only scratch is
 // the fixed file-scope device array below.
 //
-// The scratch holds a 256-byte header (the longest pattern row, reset on every
-// call) and a staging area of 2^20 complex128 values (16 MiB).  The factor of a
-// block of rows is staged there as interleaved complex and then split into the
-// caller's real / imaginary output planes; blocks are sized so that one block
-// of rows x all harmonics fits.  Limit: nfreqs * (longest pattern row) must not
-// exceed 2^20; larger requests are rejected with DGP_ERR_ARG.
+// The scratch holds a 256-byte header (the longest pattern row and a flag for
+// a malformed row pointer, both reset on every call) and a staging area of
+// 2^20 complex128 values (16 MiB).  The factor of a block of rows is staged
+// there as interleaved complex and then split into the caller's real /
+// imaginary output planes; blocks are sized so that one block of rows x all
+// harmonics fits.  Limit: nfreqs * (longest pattern row) must not exceed 2^20;
+// larger requests are rejected with DGP_ERR_ARG.  A G row pointer that does
+// not start at 0 or decreases is rejected with DGP_ERR_MESH before anything is
+// staged (a decreasing pointer would place a block's rows outside the array).
 //
 // Every GPU that loads the library keeps this 16 MiB array until the process
 // exits.  All calls share it, so two calls whose work overlaps on the GPU (on
 // different streams, or from different host threads) race on it: serialise
-// them.  The first call on a device looks up the array's device address
-// (cudaGetSymbolAddress) with that device current; make that first call
-// before any stream capture is started.
+// them.  The array's device address belongs to the CUDA context the library's
+// module is loaded in: the first call in a context looks it up
+// (cudaGetSymbolAddress, with that context's device current) and keeps it
+// with the context's id, so a context created after a device reset (MATLAB's
+// reset(gpuDevice) destroys the context) gets the address looked up again.
+// Make the first call in each context before any stream capture is started.
+#include <cuda.h>
+
 #include <algorithm>
 #include <cstdint>
 #include <mutex>
@@ -40,9 +48,15 @@ constexpr size_t kScratchBytes = kHeaderBytes + sizeof(double2) * (size_t)kStage
 
 static __device__ __align__(256) unsigned char g_fsaip_scratch[kScratchBytes];
 
-__global__ void k_noalloc_rowmax(const int *__restrict__ rptr, int n, int *m) {
+// hdr[0] = longest row of the pattern, hdr[1] = 1 when the row pointer does not start
+// at 0 or decreases somewhere
+__global__ void k_noalloc_rowmax(const int *__restrict__ rptr, int n, int *hdr) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) atomicMax(m, rptr[i + 1] - rptr[i]);
+  if (i < n) {
+    const int a = rptr[i], b = rptr[i + 1];
+    if (b < a || (i == 0 && a != 0)) atomicOr(hdr + 1, 1);
+    atomicMax(hdr, b - a);
+  }
 }
 
 __global__ void k_noalloc_split(const double2 *__restrict__ stage, int64_t count, double *__restrict__ re,
@@ -55,23 +69,64 @@ __global__ void k_noalloc_split(const double2 *__restrict__ stage, int64_t count
   }
 }
 
-constexpr int kMaxDevices = 128;
-std::mutex g_addr_mutex;
-void *g_addr[kMaxDevices] = {};
+// Driver entry points for the current context and its id (cuCtxGetId: unique for the
+// process's lifetime, also when a destroyed context's handle is reused), fetched
+// through the runtime so the library needs no link against libcuda.
+using PfnCtxGetCurrent = CUresult (*)(CUcontext *);
+using PfnCtxGetId = CUresult (*)(CUcontext, unsigned long long *);
+std::once_flag g_pfn_once;
+PfnCtxGetCurrent g_ctx_current = nullptr;
+PfnCtxGetId g_ctx_id = nullptr;
 
-// device address of the scratch array for the current device, looked up once
+int current_context_id(unsigned long long *id) {
+  std::call_once(g_pfn_once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_ctx_current = reinterpret_cast<PfnCtxGetCurrent>(p);
+    p = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_ctx_id = reinterpret_cast<PfnCtxGetId>(p);
+  });
+  DGP_REQUIRE(g_ctx_current && g_ctx_id, "fsaip_noalloc: driver entry points cuCtxGetCurrent / cuCtxGetId unavailable");
+  CUcontext ctx = nullptr;
+  if (g_ctx_current(&ctx) != CUDA_SUCCESS || !ctx) return fail(DGP_ERR_CUDA, "fsaip_noalloc: no current CUDA context");
+  if (g_ctx_id(ctx, id) != CUDA_SUCCESS) return fail(DGP_ERR_CUDA, "fsaip_noalloc: cuCtxGetId failed");
+  return DGP_OK;
+}
+
+constexpr int kMaxDevices = 128;
+struct ScratchAddr {
+  unsigned long long ctx_id = 0;  // context the address was looked up in (0: none yet)
+  void *addr = nullptr;
+};
+std::mutex g_addr_mutex;
+ScratchAddr g_addr[kMaxDevices];
+
+// device address of the scratch array in the current context, looked up once per
+// (device, context)
 int scratch_address(void **out) {
   int dev = 0;
   DGP_CUDA(cudaGetDevice(&dev));
   DGP_REQUIRE(dev >= 0 && dev < kMaxDevices, "fsaip_noalloc: device ordinal out of range");
+  void *p = nullptr;
+  unsigned long long id = 0;
   std::lock_guard<std::mutex> lock(g_addr_mutex);
-  if (!g_addr[dev]) {
-    void *p = nullptr;
+  if (current_context_id(&id) != DGP_OK) {
+    // no context is current on this thread yet: the symbol lookup makes the device's
+    // primary context current, after which its id can be read
     cudaError_t e = cudaGetSymbolAddress(&p, g_fsaip_scratch);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_fsaip_scratch)", __FILE__, __LINE__);
-    g_addr[dev] = p;
+    DGP_TRY(current_context_id(&id));
+    g_addr[dev] = ScratchAddr{id, p};
+  } else if (g_addr[dev].ctx_id != id || !g_addr[dev].addr) {
+    cudaError_t e = cudaGetSymbolAddress(&p, g_fsaip_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_fsaip_scratch)", __FILE__, __LINE__);
+    g_addr[dev] = ScratchAddr{id, p};
   }
-  *out = g_addr[dev];
+  *out = g_addr[dev].addr;
   return DGP_OK;
 }
 
@@ -84,16 +139,17 @@ int fsaip_noalloc(double *out_re, double *out_im, const double *A_re, const doub
   DGP_REQUIRE(nrows > 0 && nfreqs > 0, "fsaip_noalloc: sizes must be positive");
   void *base = nullptr;
   DGP_TRY(scratch_address(&base));
-  int *d_rowmax = static_cast<int *>(base);
+  int *d_hdr = static_cast<int *>(base);
   double2 *stage = reinterpret_cast<double2 *>(static_cast<char *>(base) + kHeaderBytes);
-  // the array keeps the previous call's contents: the maximum must restart at zero
-  DGP_CUDA(cudaMemsetAsync(d_rowmax, 0, sizeof(int), st));
-  k_noalloc_rowmax<<<(unsigned)ceil_div(nrows, 256), 256, 0, st>>>(rPtrG, nrows, d_rowmax);
+  // the array keeps the previous call's contents: the maximum and the flag restart at zero
+  DGP_CUDA(cudaMemsetAsync(d_hdr, 0, 2 * sizeof(int), st));
+  k_noalloc_rowmax<<<(unsigned)ceil_div(nrows, 256), 256, 0, st>>>(rPtrG, nrows, d_hdr);
   DGP_CHECK_LAUNCH();
-  int mmax = 0, nnzG = 0;
-  DGP_CUDA(cudaMemcpyAsync(&mmax, d_rowmax, sizeof(int), cudaMemcpyDeviceToHost, st));
-  DGP_CUDA(cudaMemcpyAsync(&nnzG, rPtrG + nrows, sizeof(int), cudaMemcpyDeviceToHost, st));
+  int hdr[2] = {0, 0};
+  DGP_CUDA(cudaMemcpyAsync(hdr, d_hdr, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
   DGP_CUDA(cudaStreamSynchronize(st));
+  if (hdr[1]) return fail(DGP_ERR_MESH, "fsaip_noalloc: G row pointer does not start at 0 or decreases");
+  const int mmax = hdr[0];
   DGP_REQUIRE(mmax >= 1 && mmax <= 32, "fsaip_noalloc: pattern rows must hold 1..32 entries");
   if ((int64_t)nfreqs * mmax > kStageSlots)
     return fail(DGP_ERR_ARG, "fsaip_noalloc: nfreqs * longest pattern row exceeds the 1048576-value "

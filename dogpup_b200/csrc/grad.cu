@@ -3,7 +3,7 @@
 // The reference differentiates its forward model through the explicit
 // absorption Jacobian (J_complex, DOGPUP/dMesh.m:206-247, then fc2tg); the
 // reverse-mode path here needs no J.  For a real functional
-//   L = sum_{m,g} g[m][g] y[m][g],   y = fc2tg(meas(phi))     (fc2tg.m:100-111)
+//   L = sum_{m,g} g[m][g] y[m][g],   y = fc2tg(meas(phi))     (fc2tg.m:25-32)
 // the chain rule through fc2tg and meas_flu (dMesh.m:144-171) gives
 //   c[m][k]   = 2 Nt h_k sum_g g[m][g] conj(gate[g][k])       (h_0 = 1/2, else 1)
 //   B[k][:,s] = sum_{m = (s, d)} c[m][k] D_d                  (D_d: detector d's weights)

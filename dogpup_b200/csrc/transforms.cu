@@ -1,9 +1,11 @@
 // Fourier-series transforms and detector read-out on the device.
 //
 //   td2fc  DOGPUP/td2fc.m:26-32  c_k = dt/t_end * sum_t exp(-i f_k t) x(t)
-//   fc2td  DOGPUP/fc2td.m:60-71  x(t) = 2 Re sum_k exp(i f_k t) c~_k, c~_0 = c_0/2
-//   fc2tg  DOGPUP/fc2tg.m:100-111 y_g = Nt * 2 Re sum_k conj(gate_gk) c~_k
+//   fc2td  DOGPUP/fc2td.m:24-31  x(t) = 2 Re sum_k exp(i f_k t) c~_k, c~_0 = c_0/2
+//   fc2tg  DOGPUP/fc2tg.m:25-32  y_g = Nt * 2 Re sum_k conj(gate_gk) c~_k
 //   meas   DOGPUP/dMesh.m:144-171 data[m,k] = sum_l w_dl phi[k, node_dl, s_m]
+//   csr    y = A x for a real FP64 CSR A: the voxel-basis maps of the LM update,
+//          G = m2g * mua and d_mu = g2m * x (wghtd_LM_recon.m:105, :133)
 //
 // These act on detector-sized data (NM x NF); the large Jacobian-sized
 // fc2tg is fused into the Jacobian kernels.  One thread per output element,
@@ -87,6 +89,21 @@ __global__ void k_meas(const int32_t *__restrict__ dn, const double *__restrict_
   data[e] = acc;
 }
 
+// one thread per row (the basis maps hold <= 8 entries per row); entries whose column
+// lies outside [0, ncols) are skipped, so a malformed matrix cannot read past x
+__global__ void k_csr_spmv(const int32_t *__restrict__ rowptr, const int32_t *__restrict__ col,
+                           const double *__restrict__ val, int64_t nrows, int64_t ncols, const double *__restrict__ x,
+                           double *__restrict__ y) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= nrows) return;
+  double acc = 0.0;
+  for (int p = rowptr[i], e = rowptr[i + 1]; p < e; ++p) {
+    const int j = col[p];
+    if (j >= 0 && j < ncols) acc = fma(val[p], x[j], acc);
+  }
+  y[i] = acc;
+}
+
 inline unsigned g1(int64_t n, int bs) { return (unsigned)ceil_div(n, bs); }
 
 }  // namespace
@@ -113,6 +130,15 @@ int fc2tg_run(const double *c, int64_t nr, int nf, const double *gate, int ng, i
   DGP_REQUIRE(c && gate && y, "fc2tg: null pointer");
   DGP_REQUIRE(nr > 0 && ng > 0 && nf > 0, "fc2tg: sizes must be positive");
   k_fc2tg<<<g1(nr * ng, 128), 128, 0, st>>>((const double2 *)c, nr, nf, (const double2 *)gate, ng, nt, y);
+  DGP_CHECK_LAUNCH();
+  return DGP_OK;
+}
+
+int csr_spmv_run(const int32_t *rowptr, const int32_t *col, const double *val, int64_t nrows, int64_t ncols,
+                 const double *x, double *y, cudaStream_t st) {
+  DGP_REQUIRE(rowptr && col && val && x && y, "csr_spmv: null pointer");
+  DGP_REQUIRE(nrows > 0 && ncols > 0, "csr_spmv: sizes must be positive");
+  k_csr_spmv<<<g1(nrows, 256), 256, 0, st>>>(rowptr, col, val, nrows, ncols, x, y);
   DGP_CHECK_LAUNCH();
   return DGP_OK;
 }

@@ -12,7 +12,6 @@ from __future__ import annotations
 
 import numpy as np
 import torch
-from scipy.spatial import cKDTree
 
 from . import api
 
@@ -49,7 +48,6 @@ class DMesh:
         self.c = self.fem.c
         self.bnd_host = self.fem.bnd.cpu().numpy().astype(bool)
         self.face_host = surface_faces(self.node_host, self.elem_host)
-        self._locator = None
         self.optode = None
         self._solver = None
         self._solver_key = None
@@ -59,11 +57,6 @@ class DMesh:
     @property
     def nn(self):
         return self.node_host.shape[0]
-
-    def locator(self):
-        if self._locator is None:
-            self._locator = cKDTree(self.node_host[self.elem_host].mean(axis=1))
-        return self._locator
 
     def update_properties(self, props=None):
         """Re-assemble K, M on the device (dMesh.m:80-88)."""
@@ -131,12 +124,11 @@ class DMesh:
         return api.meas(nodes, w, link, phi)
 
     # ------------------------------------------------------------ Jacobian
-    def mesh2grid(self, x, y, z, device=True):
-        """Voxel basis of the Jacobian (dMesh.m:286-380): m2g, g2m, gridinmesh, dxyz.
-        device=False locates the voxel centres on the host instead of the GPU."""
+    def mesh2grid(self, x, y, z):
+        """Voxel basis of the Jacobian (dMesh.m:286-380): m2g, g2m, gridinmesh, dxyz,
+        with the voxel centres located on the device."""
         from .grid import mesh2grid
-        g = mesh2grid(self.node_host, self.elem_host, np.asarray(x), np.asarray(y), np.asarray(z),
-                      None if device else self.locator(), device=device)
+        g = mesh2grid(self.node_host, self.elem_host, np.asarray(x), np.asarray(y), np.asarray(z))
         self.grid, self.m2g, self.g2m = g["grid"], g["m2g"], g["g2m"]
         self.gridinmesh, self.dxyz, self.gridSize = g["gridinmesh"], g["dxyz"], g["size"]
         self.grid_basis = api.Basis(self.m2g, np.full(self.m2g.shape[0], self.dxyz ** 3))

@@ -3,41 +3,13 @@
 Builds m2g (mesh -> voxel barycentric interpolation, <= 4 entries per row),
 the in-mesh mask, the voxel size and g2m (voxel -> node interpolation), as
 the reference does once per mesh with MATLAB's ``pointLocation`` and
-``delaunay``.  The point location runs on the device (``dgp_locate_points``)
-or on the host (k-d tree candidates); g2m on the device
-(``dgp_grid_to_mesh``).
+``delaunay``.  The point location (``dgp_locate_points``) and g2m
+(``dgp_grid_to_mesh``) run on the device.
 """
 from __future__ import annotations
 
 import numpy as np
 import scipy.sparse as sp
-from scipy.spatial import cKDTree
-
-from .optode import barycentric
-
-
-def locate_host(node, elem, grid, tree=None, eps=1e-12):
-    """Containing element (-1: none) and barycentric weights of each grid point, on the host
-    (candidates: the 32 elements with the nearest centroids)."""
-    nv = grid.shape[0]
-    if tree is None:
-        tree = cKDTree(node[elem].mean(axis=1))
-    k = min(32, elem.shape[0])
-    _, cand = tree.query(grid, k=k)
-    eid = np.full(nv, -1, dtype=np.int64)
-    w = np.zeros((nv, 4))
-    for c0 in range(0, nv, 4096):
-        sl = slice(c0, min(nv, c0 + 4096))
-        cc = cand[sl]                                                   # [B, k]
-        lam = barycentric(node, elem, cc, np.broadcast_to(grid[sl][:, None, :], cc.shape + (3,)))
-        score = lam.min(axis=2)
-        j = np.argmax(score, axis=1)
-        best = score[np.arange(cc.shape[0]), j]
-        ok = best >= -eps
-        rows = np.arange(sl.start, sl.stop)[ok]
-        eid[rows] = cc[ok, j[ok]]
-        w[rows] = lam[ok, j[ok]]
-    return eid, w
 
 
 def m2g_from_location(eid, w, elem, nn):
@@ -63,11 +35,10 @@ def g2m_from_rows(col, val, nv):
     return g2m
 
 
-def mesh2grid(node, elem, x, y, z, tree=None, device=True):
+def mesh2grid(node, elem, x, y, z):
     """Returns dict(grid [NV,3], m2g CSR [NV x NN], g2m CSR [NN x NV], gridinmesh [NV], dxyz, size).
 
-    The voxel centres are located with ``dgp_locate_points`` (device=True) or
-    with the k-d tree host locator; g2m is built on the device
+    The voxel centres are located with ``dgp_locate_points``; g2m is built on the device
     (``dgp_grid_to_mesh``: Kuhn triangulation of the lattice, in-mesh voxels,
     nearest in-mesh voxel for uncovered nodes, rows normalised)."""
     from . import api
@@ -76,11 +47,8 @@ def mesh2grid(node, elem, x, y, z, tree=None, device=True):
     X, Y, Z = np.meshgrid(x, y, z, indexing="ij")                      # ndgrid, :308
     grid = np.stack([X.ravel(order="F"), Y.ravel(order="F"), Z.ravel(order="F")], axis=1)
     nv = grid.shape[0]
-    if device:
-        e_d, w_d = api.locate_points(node, elem, grid, eps=1e-12)
-        eid, w = e_d.cpu().numpy(), w_d.cpu().numpy()
-    else:
-        eid, w = locate_host(node, elem, grid, tree)
+    e_d, w_d = api.locate_points(node, elem, grid, eps=1e-12)
+    eid, w = e_d.cpu().numpy(), w_d.cpu().numpy()
     m2g, inmesh = m2g_from_location(eid, w, elem, node.shape[0])
     col, val = api.grid_to_mesh(node, (x, y, z), inmesh)               # :330-373
     g2m = g2m_from_rows(col.cpu().numpy(), val.cpu().numpy(), nv)

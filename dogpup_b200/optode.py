@@ -3,14 +3,12 @@
 Mirrors the ``dOptode`` class (DOGPUP/dOptode.m:34-199).  The Fourier
 coefficients of the source pulse come from the device ``td2fc`` kernel; the
 geometry (nearest surface point, containing tetrahedron) runs on the device
-(``dgp_snap_to_surface``, ``dgp_locate_points``), or on the host with k-d
-tree candidates (``snap2mesh(mesh, device=False)``).
+(``dgp_snap_to_surface``, ``dgp_locate_points``).
 """
 from __future__ import annotations
 
 import numpy as np
 import torch
-from scipy.spatial import cKDTree
 
 from . import api
 
@@ -41,22 +39,10 @@ class DOptode:
         self.s_bary = self.d_bary = None
         self.s_dirs = self.d_dirs = None
 
-    def snap2mesh(self, mesh, device=True):
-        """Snap optodes to the surface, move sources 1/min(musp) inward (dOptode.m:77-97).
-
-        device=True: surface search (``dgp_snap_to_surface``) and point location
-        (``dgp_locate_points``) on the GPU; device=False: the host k-d tree path."""
-        if device:
-            return self._snap2mesh_device(mesh)
-        self.d_positions, self.d_bary, self.d_dirs = snap_pos(mesh, self.d_positions)
-        self.s_positions, _, self.s_dirs = snap_pos(mesh, self.s_positions)
-        inset = self.s_positions + (1.0 / float(np.min(mesh.musp_host))) * self.s_dirs   # :89
-        eid, w = locate_points(mesh.node_host, mesh.elem_host, inset, mesh.locator())
-        self.s_bary = _clean_bary(eid, w)
-        return self
-
-
-    def _snap2mesh_device(self, mesh):
+    def snap2mesh(self, mesh):
+        """Snap optodes to the surface, move sources 1/min(musp) inward (dOptode.m:77-97):
+        surface search (``dgp_snap_to_surface``) and point location (``dgp_locate_points``)
+        on the GPU."""
         node = torch.as_tensor(mesh.node_host, device="cuda")
         elem = torch.as_tensor(mesh.elem_host, device="cuda", dtype=torch.int32)
         face = torch.as_tensor(mesh.face_host, device="cuda", dtype=torch.int32)
@@ -82,88 +68,3 @@ def _clean_bary(eid, w):
     w = np.where(w < 1e-10, 0.0, w)
     w = w / w.sum(axis=1, keepdims=True)
     return np.concatenate([eid[:, None].astype(np.float64), w], axis=1)
-
-
-def closest_point_on_triangle(p, a, b, c):
-    """Closest point of triangle abc to p (Voronoi-region walk over vertices,
-    edges and face, as in Ericson, Real-Time Collision Detection, sec. 5.1.5)."""
-    ab, ac, ap = b - a, c - a, p - a
-    d1, d2 = ab @ ap, ac @ ap
-    if d1 <= 0 and d2 <= 0:
-        return a
-    bp = p - b
-    d3, d4 = ab @ bp, ac @ bp
-    if d3 >= 0 and d4 <= d3:
-        return b
-    vc = d1 * d4 - d3 * d2
-    if vc <= 0 and d1 >= 0 and d3 <= 0:
-        return a + (d1 / (d1 - d3)) * ab
-    cp = p - c
-    d5, d6 = ab @ cp, ac @ cp
-    if d6 >= 0 and d5 <= d6:
-        return c
-    vb = d5 * d2 - d1 * d6
-    if vb <= 0 and d2 >= 0 and d6 <= 0:
-        return a + (d2 / (d2 - d6)) * ac
-    va = d3 * d6 - d5 * d4
-    if va <= 0 and (d4 - d3) >= 0 and (d5 - d6) >= 0:
-        return b + ((d4 - d3) / ((d4 - d3) + (d5 - d6))) * (c - b)
-    den = 1.0 / (va + vb + vc)
-    return a + ab * (vb * den) + ac * (vc * den)
-
-
-def snap_pos(mesh, pos):
-    """Nearest surface point, inward normal and barycentric weights (dOptode.m:155-199)."""
-    node = mesh.node_host
-    face = mesh.face_host
-    bidx = np.nonzero(mesh.bnd_host)[0]
-    tree = cKDTree(node[bidx])
-    _, nb = tree.query(pos)                                                  # dsearchn, :162
-    ids = bidx[nb]
-    out = np.empty_like(pos)
-    norm = np.empty_like(pos)
-    for i in range(pos.shape[0]):
-        fi = np.nonzero((face == ids[i]).any(axis=1))[0]                   # :171
-        best, bpt, bf = np.inf, None, -1
-        for f in fi:
-            a, b, c = node[face[f]]
-            q = closest_point_on_triangle(pos[i], a, b, c)
-            d = np.linalg.norm(q - pos[i])
-            if d < best:
-                best, bpt, bf = d, q, f
-        out[i] = bpt                                                        # :180
-        a, b, c = node[face[bf]]
-        nv = -np.cross(b - a, c - a)                                        # :181-184
-        norm[i] = nv / np.linalg.norm(nv)
-    eid, w = locate_points(node, mesh.elem_host, out, mesh.locator())
-    return out, _clean_bary(eid, w), norm
-
-
-def barycentric(node, elem, e, p):
-    v = node[elem[e]]                                                       # [.., 4, 3]
-    T = np.stack([v[..., 0, :] - v[..., 3, :], v[..., 1, :] - v[..., 3, :], v[..., 2, :] - v[..., 3, :]], axis=-1)
-    l3 = np.linalg.solve(T, (p - v[..., 3, :])[..., None])[..., 0]
-    return np.concatenate([l3, 1.0 - l3.sum(axis=-1, keepdims=True)], axis=-1)
-
-
-def locate_points(node, elem, pts, tree=None, k=48):
-    """Containing tetrahedron and barycentric weights of each point
-    (MATLAB ``pointLocation``); points within 1e-9 outside the closest tet are
-    accepted (surface points).  Returns (elem_id, weights[., 4])."""
-    pts = np.atleast_2d(pts)
-    if tree is None:
-        tree = cKDTree(node[elem].mean(axis=1))
-    k = min(k, elem.shape[0])
-    _, cand = tree.query(pts, k=k)
-    cand = np.atleast_2d(cand)
-    eid = np.empty(pts.shape[0], dtype=np.int64)
-    w = np.empty((pts.shape[0], 4))
-    for i in range(pts.shape[0]):
-        lam = barycentric(node, elem, cand[i], np.broadcast_to(pts[i], (cand.shape[1], 3)))
-        score = lam.min(axis=1)
-        j = int(np.argmax(score))
-        if score[j] < -1e-9:
-            raise ValueError(f"point {pts[i]} lies outside the mesh")
-        eid[i] = cand[i, j]
-        w[i] = lam[j]
-    return eid, w

@@ -9,6 +9,8 @@ its helpers id_thresh (DOGPUP/id_thresh.m:1-27) and tik_inv
                   H = J^T W J + lam * max diag, r = J^T W y (dgp_normal_eq,
                   split-BF16 tcgen05) and the FP64 Cholesky solve
                   (dgp_cholesky_solve), or all of it in FP64 for comparison
+                  property normalisation G = m2g mua and the update map
+                  d_mu = g2m (G x) by the library's CSR SpMV (dgp_csr_spmv)
   host            the loop's scalar logic (lambda schedule, step-back on a
                   rising error, exit conditions) on [NM x NG]-sized data
 
@@ -116,8 +118,8 @@ class LMRecon:
         inmesh = np.asarray(mesh.gridinmesh)
         P = mesh.m2g[inmesh]
         self.basis = api.Basis(P, np.full(P.shape[0], mesh.dxyz ** 3))
-        self.m2g_in = P.tocsr()
-        self.g2m_in = mesh.g2m[:, np.nonzero(inmesh)[0]].tocsr()
+        self.m2g_in = api.DeviceCsr(P)                                  # in-mesh voxels x nodes
+        self.g2m_in = api.DeviceCsr(mesh.g2m[:, np.nonzero(inmesh)[0]])   # nodes x in-mesh voxels
         self.nv = P.shape[0]
 
     # ----------------------------------------------------------- one model
@@ -133,7 +135,7 @@ class LMRecon:
         else:
             Jc = api.jacobian_complex(self.basis, phi, phiA, m.optode.s_fpsf, m._link())   # [NV][NF][NM]
             Jc[:, 0, :] *= 0.5
-            Jtg = self.nt * 2.0 * torch.einsum("gk,vkm->vgm", self.gate_fc.conj(), Jc).real   # fc2tg.m:100-111
+            Jtg = self.nt * 2.0 * torch.einsum("gk,vkm->vgm", self.gate_fc.conj(), Jc).real   # fc2tg.m:25-32
             del Jc
             Jt = (Jtg / data_tg.transpose(0, 1)[None]).reshape(self.nv, -1)
         return data_tg, Jt
@@ -234,18 +236,20 @@ class LMRecon:
                 break
             count += 1
             if count == 1 or hist["err_del"][-1] < 0:                 # :100-106
-                G = torch.as_tensor(self.m2g_in @ m.mua.cpu().numpy(), device="cuda")
+                G = self.m2g_in @ m.mua
+                Jt = (Jt * G[:, None].to(Jt.dtype)).contiguous()      # J .* G.' (property normalisation)
                 lam1 = lam1 / k
             else:                                                     # step back (:107-115)
-                G = torch.as_tensor(self.m2g_in @ (m.mua - d_mu).cpu().numpy(), device="cuda")
+                # the cached J is used as cached, normalised by the G of its own iteration;
+                # the new G only rescales the update
+                G = self.m2g_in @ (m.mua - d_mu)
                 y, Jt = y_prev, J_prev
                 lam1 = lam1 * k
             lam1 = max(lam1, err)                                     # :118-120
             hist["lam"].append(lam1)
-            Jg = (Jt * G[:, None].to(Jt.dtype)).contiguous()          # J .* G.' (property normalisation)
-            upd = self._tik(Jg, lam1, y.contiguous(), None if Js is not None else w)   # :125-127
+            upd = self._tik(Jt, lam1, y.contiguous(), None if Js is not None else w)   # :125-127
             x = G * upd                                               # :131
-            d_mu = torch.as_tensor(self.g2m_in @ x.cpu().numpy(), device="cuda")   # :132
+            d_mu = self.g2m_in @ x                                    # :132
             if torch.isnan(d_mu).any():                               # :136-141
                 hist["exit"] = "nan_update"
                 warnings.warn("LM: NaN absorption update, stopping the reconstruction")

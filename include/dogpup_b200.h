@@ -58,6 +58,10 @@ int dgp_version(void);
 /* Number of kernels this library has launched in the process so far
  * (kernels inside its CUDA graphs included). */
 int64_t dgp_kernel_launches(void);
+/* Number of device allocations (cudaMalloc calls, failed ones included) this
+ * library's own code has made in the process so far; allocations made inside
+ * cuBLAS are not counted. */
+int64_t dgp_device_allocations(void);
 
 /* ====================================================================== *
  *  Drop-in host functions of the reference mex sources.  Same names,
@@ -112,10 +116,11 @@ int dgp_fsaip_mex_ic(double *d_out, const double *d_valA, const int *d_rPtrA,
  * allocator owns the GPU.  Same arguments and output; it allocates nothing
  * and stages its work in one fixed 16 MiB device array that every GPU loading
  * the library keeps until exit.  Limit: nfreqs * (longest pattern row)
- * <= 1048576, else DGP_ERR_ARG.  All calls share that array: calls that
- * overlap on the GPU race, so serialise them.  The first call on a device
- * looks the array up; make it before any stream capture.  Synchronises the
- * stream. */
+ * <= 1048576, else DGP_ERR_ARG; a G row pointer that does not start at 0 or
+ * decreases is DGP_ERR_MESH.  All calls share that array: calls that overlap
+ * on the GPU race, so serialise them.  The first call in each CUDA context
+ * (a new one after a device reset included) looks the array up; make it
+ * before any stream capture.  Synchronises the stream. */
 int dgp_fsaip_mex_noalloc(double *d_out_real, double *d_out_imag,
                           const double *d_valA_real, const double *d_valA_imag,
                           const int *d_rPtrA, const int *d_cPtrA,
@@ -355,14 +360,22 @@ int dgp_meas(const int32_t *d_det_nodes, const double *d_det_w, int32_t nd,
              int64_t n, int32_t nf, int32_t ns, double *d_data,
              dgp_stream_t stream);
 
+/* y = A x for a real FP64 CSR matrix A [nrows x ncols] (int32 0-based
+ * row pointer and columns).  The voxel-basis maps of the LM update use it:
+ * G = m2g * mua and d_mu = g2m * x (wghtd_LM_recon.m:105, :133).  Entries
+ * whose column lies outside [0, ncols) are skipped. */
+int dgp_csr_spmv(const int32_t *d_rowptr, const int32_t *d_col,
+                 const double *d_val, int64_t nrows, int64_t ncols,
+                 const double *d_x, double *d_y, dgp_stream_t stream);
+
 /* Fourier coefficients of sampled signals: c[r][k] = dt/t_end *
  * sum_t exp(-i f_k t) x[r][t]  (td2fc.m:26-32).  x [nr][nt] f64. */
 int dgp_td2fc(const double *d_x, int64_t nr, int32_t nt, const double *d_t,
               const double *d_f, int32_t nf, double *d_c, dgp_stream_t stream);
-/* x[r][t] = 2 Re sum_k exp(i f_k t) c~[r][k], c~_0 = c_0/2 (fc2td.m:60-71). */
+/* x[r][t] = 2 Re sum_k exp(i f_k t) c~[r][k], c~_0 = c_0/2 (fc2td.m:24-31). */
 int dgp_fc2td(const double *d_c, int64_t nr, int32_t nf, const double *d_f,
               const double *d_t, int32_t nt, double *d_x, dgp_stream_t stream);
-/* y[r][g] = nt * 2 Re sum_k conj(gate[g][k]) c~[r][k] (fc2tg.m:100-111). */
+/* y[r][g] = nt * 2 Re sum_k conj(gate[g][k]) c~[r][k] (fc2tg.m:25-32). */
 int dgp_fc2tg(const double *d_c, int64_t nr, int32_t nf, const double *d_gate_fc,
               int32_t ng, int32_t nt, double *d_y, dgp_stream_t stream);
 /* Adjoint sources of L = sum_{m,g} d_g[m][g] * fc2tg(meas(phi))[m][g]:
@@ -370,7 +383,7 @@ int dgp_fc2tg(const double *d_c, int64_t nr, int32_t nf, const double *d_gate_fc
  * c[m][k] = 2 nt h_k sum_g g[m][g] conj(gate[g][k]) (h_0 = 1/2, else 1)
  * scattered through detector d's weights for every link m = (s, d).  Solving
  * A_k lam = B (dgp_solve) gives the adjoint fields of dgp_fem_adjoint_grad.
- * The chain rule of fc2tg.m:100-111 and meas_flu (dMesh.m:144-171). */
+ * The chain rule of fc2tg.m:25-32 and meas_flu (dMesh.m:144-171). */
 int dgp_tg_adjoint_rhs(const int32_t *d_det_nodes, const double *d_det_w,
                        int32_t nd, const int32_t *d_link, int32_t nm,
                        const double *d_gate_fc, int32_t ng, int32_t nt,

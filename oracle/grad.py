@@ -1,7 +1,7 @@
 """Float64 restatement of the reverse-mode gradient of time-gated data (test infrastructure).
 
 The reference forms the absorption Jacobian explicitly (J_complex,
-DOGPUP/dMesh.m:206-247) and time-gates it with fc2tg (DOGPUP/fc2tg.m:100-111);
+DOGPUP/dMesh.m:206-247) and time-gates it with fc2tg (DOGPUP/fc2tg.m:25-32);
 its J holds kappa fixed.  The library's backward pass computes the exact
 discrete gradient of
 

@@ -20,7 +20,7 @@ def td2fc(fun_td, f, t):
 
 
 def fc2td(fun_fc, f, t):
-    """x(t) = 2 Re sum_k exp(i f_k t) c~_k with c~_0 = c_0/2, fc2td.m:60-71."""
+    """x(t) = 2 Re sum_k exp(i f_k t) c~_k with c~_0 = c_0/2, fc2td.m:24-31."""
     c = np.array(fun_fc, dtype=np.complex128, copy=True)
     c[..., 0] = c[..., 0] / 2
     T = np.exp(1j * np.asarray(f)[None, :] * np.asarray(t)[:, None])   # [NT, NF]
@@ -28,7 +28,7 @@ def fc2td(fun_fc, f, t):
 
 
 def fc2tg(fun_fc, gate_fc, f, nt):
-    """y[g] = Nt * 2 Re sum_k conj(gate_fc[g,k]) c~_k, c~_0 = c_0/2, fc2tg.m:100-111."""
+    """y[g] = Nt * 2 Re sum_k conj(gate_fc[g,k]) c~_k, c~_0 = c_0/2, fc2tg.m:25-32."""
     c = np.array(fun_fc, dtype=np.complex128, copy=True)
     c[..., 0] = c[..., 0] / 2
     G = np.conj(np.asarray(gate_fc))                   # [NG, NF]

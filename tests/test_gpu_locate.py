@@ -75,15 +75,19 @@ def test_locate_empty_and_single_point():
     _check(m.node, m.elem.astype(np.int64), np.array([[0.25, 0.5, 0.75]]))
 
 
-def test_dmesh_mesh2grid_device_equals_host():
+def test_dmesh_mesh2grid_device_equals_oracle():
+    """DMesh.mesh2grid (device point location) against the oracle's k-d tree host locator:
+    the same in-mesh mask and the same interpolation of a linear field."""
     from dogpup_b200 import workloads
+    from dogpup_b200.grid import m2g_from_location
+    from oracle.jacobian import point_location
     w = workloads.small_fwd(ns=2, nd=2, nf=4)
     mesh = workloads.build_dmesh(w)
     lo, hi = w["mesh"].node.min(0), w["mesh"].node.max(0)
     xs = [np.arange(lo[d] - 2, hi[d] + 2.001, 1.5) for d in range(3)]
-    mesh.mesh2grid(*xs, device=False)
-    P_host, inm_host = mesh.m2g.copy(), mesh.gridinmesh.copy()
-    mesh.mesh2grid(*xs, device=True)
+    mesh.mesh2grid(*xs)
+    P_host, inm_host = m2g_from_location(*point_location(mesh.node_host, mesh.elem_host, mesh.grid, chunk=8),
+                                         mesh.elem_host, mesh.nn)
     assert np.array_equal(mesh.gridinmesh, inm_host)
     f = mesh.node_host @ LIN + 2.0
     assert np.abs(mesh.m2g @ f - P_host @ f).max() < 1e-11
@@ -197,20 +201,23 @@ def test_snap_rejects_a_mesh_without_boundary():
         api.snap_to_surface(mesh.node_host, np.zeros(mesh.nn, np.int32), mesh.face_host, pos[:3])
 
 
-def test_optode_snap_device_equals_host():
-    """DOptode.snap2mesh on the device and on the host: same surface points, normals and
-    source/detector points (the weighted vertices of the located elements)."""
+def test_optode_snap_device_equals_oracle():
+    """DOptode.snap2mesh on the device against the oracle's snap2mesh on the host: same
+    surface points, normals and source/detector points (the weighted vertices of the
+    located elements)."""
     from dogpup_b200.optode import DOptode
     from dogpup_b200.workloads import gaussian_pulse
+    from oracle.optode import snap2mesh
     mesh, w = _snap_case(with_w=True)
     t = w["t"]
-    o_dev, o_host = (DOptode(w["src"], w["det"], w["link"], 1e3, gaussian_pulse(t), t, w["nf"]) for _ in range(2))
+    o_dev = DOptode(w["src"], w["det"], w["link"], 1e3, gaussian_pulse(t), t, w["nf"])
     o_dev.snap2mesh(mesh)
-    o_host.snap2mesh(mesh, device=False)
-    assert np.abs(o_host.s_positions - o_dev.s_positions).max() < 1e-12
-    assert np.abs(o_host.d_positions - o_dev.d_positions).max() < 1e-12
-    assert np.abs(o_host.s_dirs - o_dev.s_dirs).max() < 1e-12
-    for b_dev, b_host in ((o_dev.s_bary, o_host.s_bary), (o_dev.d_bary, o_host.d_bary)):
+    sq, sn, s_bary, dq, dn, d_bary = snap2mesh(mesh.node_host, mesh.elem_host, mesh.bnd_host, mesh.face_host,
+                                               mesh.musp_host, w["src"], w["det"])
+    assert np.abs(sq - o_dev.s_positions).max() < 1e-12
+    assert np.abs(dq - o_dev.d_positions).max() < 1e-12
+    assert np.abs(sn - o_dev.s_dirs).max() < 1e-12
+    for b_dev, b_host in ((o_dev.s_bary, s_bary), (o_dev.d_bary, d_bary)):
         pt = lambda b: (b[:, 1:, None] * mesh.node_host[mesh.elem_host[b[:, 0].astype(int)]]).sum(1)
         assert np.abs(pt(b_dev) - pt(b_host)).max() < 1e-9
 

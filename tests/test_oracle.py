@@ -180,16 +180,25 @@ def test_morton_and_lattice_orders_are_the_same_mesh():
     assert np.median(spans) <= 7
 
 
-def test_point_location_oracle_against_host_locator():
-    """Brute-force point location (oracle) vs the package's k-d tree host locator:
+def test_point_location_oracle_against_kdtree_locator():
+    """Brute-force point location vs the oracle's k-d tree candidate locator (two routes):
     the same in-mesh mask and the same interpolation of a linear field."""
-    from dogpup_b200.grid import locate_host, m2g_from_location
+    from dogpup_b200.grid import m2g_from_location
+    from oracle.optode import locate_points
     m = ellipsoid_mesh((8, 7, 6), 1.2, 0.15, 3)
     lo, hi = m.node.min(0), m.node.max(0)
     xs = [np.arange(lo[d] - 0.7, hi[d] + 0.71, 0.9) for d in range(3)]
     X, Y, Z = np.meshgrid(*xs, indexing="ij")
     grid = np.stack([X.ravel(order="F"), Y.ravel(order="F"), Z.ravel(order="F")], axis=1)
-    m2g_host, inm_host = m2g_from_location(*locate_host(m.node, m.elem, grid), m.elem, m.nn)
+    eid = np.full(len(grid), -1)
+    wts = np.zeros((len(grid), 4))
+    for i, p in enumerate(grid):
+        try:
+            e, wi = locate_points(m.node, m.elem, p, k=32, eps=1e-12)
+            eid[i], wts[i] = e[0], wi[0]
+        except ValueError:
+            pass
+    m2g_host, inm_host = m2g_from_location(eid, wts, m.elem, m.nn)
     P, inm = jacobian.m2g_matrix(m.node, m.elem, grid)
     assert inm.sum() > 100 and (~inm).sum() > 100
     assert np.array_equal(inm, inm_host)
@@ -254,8 +263,9 @@ def test_reshape_and_spot_oracles():
 
 
 def test_closest_point_on_triangle_two_methods():
-    """The package's Voronoi-region walk and the oracle's projection-or-edges route agree."""
-    from dogpup_b200.optode import closest_point_on_triangle as walk
+    """The Voronoi-region walk (the device kernel's method) and the projection-or-edges
+    route agree."""
+    from oracle.optode import closest_point_on_triangle_walk as walk
     from oracle.optode import closest_point_on_triangle as proj
     rng = np.random.default_rng(8)
     for _ in range(400):

@@ -116,3 +116,64 @@ def test_lm_recon_with_target_spots():
     assert all(torch.isfinite(m).all() for m in h["mua"])
     for a, b in zip(runs["split_bf16"]["mua"], runs["fp64"]["mua"]):
         assert (torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)).item() < 2e-2
+
+
+@pytest.mark.gpu
+def test_lm_loop_against_oracle_with_two_step_backs_in_a_row():
+    """The LM loop's control flow against the oracle's restatement of wghtd_LM_recon
+    (oracle/recon.py) on a scripted model whose misfit falls, rises twice in a row, then
+    falls: both step-back iterations reuse the Jacobian cached at the last accepted step,
+    normalised by that step's G (wghtd_LM_recon.m:103-116, :165-166), and rescale the update
+    by the new G.  FP64 normal equations; the device maps m2g / g2m (dgp_csr_spmv) and the
+    FP64 Cholesky against NumPy: mua after every update to 1e-10, lambda and misfit exactly
+    as the oracle's up to rounding."""
+    import types
+
+    import scipy.sparse as sp
+    import torch
+    from dogpup_b200.recon import LMRecon, _flat
+    from oracle.recon import lm_loop
+
+    rng = np.random.default_rng(17)
+    nn, nv, nm, ng = 60, 40, 12, 4
+    m2g = sp.random(nv, nn, density=0.08, random_state=3, format="csr") + sp.eye(nv, nn, format="csr")
+    m2g = sp.diags(1.0 / np.asarray(m2g.sum(1)).ravel()) @ m2g                    # rows sum to 1
+    g2m = sp.random(nn, nv, density=0.1, random_state=4, format="csr") + sp.eye(nn, nv, format="csr")
+    g2m = sp.diags(1.0 / np.maximum(np.asarray(g2m.sum(1)).ravel(), 1e-300)) @ g2m
+    data_m = np.exp(5.0 + 0.5 * rng.standard_normal((nm, ng)))
+    r = rng.standard_normal((nm, ng))
+    eps = [1.0, 0.6, 0.8, 0.9, 0.4, 0.3, 0.25]           # misfit scale per model call
+    Js = [300.0 * rng.standard_normal((nv, ng * nm)) for _ in eps]   # normalised J ~ 3: small steps
+    mua0 = 0.01 + 0.002 * rng.random(nn)
+
+    def scripted(q):
+        return data_m * np.exp(-eps[q] * r), Js[q]      # data [NM][NG], J^T [NV][NG*NM] in x(:) order
+
+    mesh = types.SimpleNamespace(
+        mua=torch.as_tensor(mua0, device="cuda"), gridinmesh=np.ones(nv, bool), m2g=m2g, g2m=g2m, dxyz=1.0,
+        optode=types.SimpleNamespace(tAxis=np.arange(11.0)), update_properties=lambda: None)
+
+    class Scripted(LMRecon):
+        calls = 0
+
+        def model(self):
+            d, J = scripted(self.calls)
+            self.calls += 1
+            return torch.as_tensor(d, device="cuda"), torch.as_tensor(J, device="cuda")
+
+    rec = Scripted(mesh, np.ones((ng, 8), complex), precision="fp64", normal_eq="fp64")
+    h = rec.run(data_m, lam=(1.0, 0.0), thresh="all", max_iter=5)
+
+    mask = id_thresh(data_m, "all") & (data_m > 0)
+    incl = np.nonzero(mask.T.ravel())[0]
+    dm = np.log(_flat(torch.as_tensor(data_m)).numpy())[incl]
+    h0 = lm_loop(lambda q: (_flat(torch.as_tensor(scripted(q)[0])).numpy(), scripted(q)[1].T),
+                 mua0, m2g, g2m, dm, incl, 1.0, max_iter=5)
+    deltas = np.sign(h0["err_del"])
+    assert list(deltas[:3]) == [-1, 1, 1]                # fall, then two rises in a row
+    assert h["exit"] == h0["exit"] == "max_iter" and h["iterations"] == h0["iterations"] == 5
+    assert np.allclose(h["err"], h0["err"], rtol=1e-12, atol=0)
+    assert np.allclose(h["lam"], h0["lam"], rtol=1e-12, atol=0)
+    assert len(h["mua"]) == len(h0["mua"]) == 5
+    for a, b in zip(h["mua"], h0["mua"]):
+        assert np.abs(a.cpu().numpy() - b).max() <= 1e-10 * np.abs(b).max()

@@ -9,6 +9,11 @@ harmonic count below makes the rows go through the scratch array in several
 blocks.  This file is named to run last.
 """
 import ctypes as C
+import json
+import os
+import subprocess
+import sys
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -16,65 +21,137 @@ import scipy.sparse as sp
 
 pytestmark = pytest.mark.gpu
 
-DGP_ERR_ARG = 1
+DGP_ERR_ARG, DGP_ERR_MESH = 1, 4
+HERE = Path(__file__).resolve().parent
+MODULE_IMAGE_BYTES = 16 * 2 ** 20 + 4 * 2 ** 20   # the fixed scratch array + the module's code and page rounding
 
 
 def _vp(t):
     return C.c_void_p(t.data_ptr())
 
 
-def test_noalloc_factor_matches_allocating_entry_point(small_case):
-    import torch
-    from dogpup_b200._lib import lib, check
+def _case(small_case, dfc=2 * np.pi / 10e-9 / (2.99792458e11 / 1.4)):
+    """tril(K + i dfc M) of the small cylinder and its FSAI pattern (dfc: the harmonic step
+    of a 10 ns period over the speed of light at n = 1.4, in 1/mm)."""
     from oracle import solver as osv
-
     K, M = small_case["K"], small_case["M"]
-    dfc = 2 * np.pi / 10e-9 / (2.99792458e11 / 1.4)
     A = sp.tril(K + 1j * dfc * M).tocsr()
     A.sort_indices()
     rg, cg = osv.fsai_pattern(A)
-    n, nnzG, nf = A.shape[0], cg.shape[0], 64   # 64 harmonics x 8-entry rows: 2048 rows per scratch block
+    return A, rg, cg
+
+
+def _inputs(A, rg, cg):
+    import torch
 
     def dev(a, dt):
         return torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device="cuda")
 
-    ins = [dev(A.data.real, torch.float64), dev(A.data.imag, torch.float64), dev(A.indptr, torch.int32),
-           dev(A.indices, torch.int32), dev(rg, torch.int32), dev(cg, torch.int32)]
+    return [dev(A.data.real, torch.float64), dev(A.data.imag, torch.float64), dev(A.indptr, torch.int32),
+            dev(A.indices, torch.int32), dev(rg, torch.int32), dev(cg, torch.int32)]
+
+
+def test_noalloc_factor_matches_allocating_entry_point(small_case):
+    """Three calls in a row equal dgp_fsaip_mex to 1e-12.  No call -- the first one
+    included -- makes a device allocation through the library (its own allocation
+    counter), and no call after the first changes the device's free memory.  The first
+    call may load the library's module for this entry point, which places the fixed
+    scratch array in device memory; that is the driver loading code and static data,
+    bounded here by the array's size plus the module's code."""
+    import torch
+    from dogpup_b200._lib import lib, check
+
+    A, rg, cg = _case(small_case)
+    n, nnzG, nf = A.shape[0], cg.shape[0], 64   # 64 harmonics x 8-entry rows: 2048 rows per scratch block
+    ins = _inputs(A, rg, cg)
+    ptrs = [_vp(t) for t in ins]
+    re = torch.empty((nnzG * nf,), dtype=torch.float64, device="cuda")
+    im = torch.empty_like(re)
 
     def run(fn):
-        re = torch.full((nnzG * nf,), np.nan, dtype=torch.float64, device="cuda")
-        im = torch.full_like(re, np.nan)
-        check(fn(_vp(re), _vp(im), *[_vp(t) for t in ins], nf, n, None))
+        re.fill_(np.nan)
+        im.fill_(np.nan)
         torch.cuda.synchronize()
-        return re.cpu().numpy() + 1j * im.cpu().numpy()
+        a0, free0 = lib.dgp_device_allocations(), torch.cuda.mem_get_info()[0]
+        check(fn(_vp(re), _vp(im), *ptrs, nf, n, None))
+        torch.cuda.synchronize()
+        a1, free1 = lib.dgp_device_allocations(), torch.cuda.mem_get_info()[0]
+        return re.cpu().numpy() + 1j * im.cpu().numpy(), a1 - a0, free0 - free1
 
-    expected = run(lib.dgp_fsaip_mex)
+    expected, allocs, _ = run(lib.dgp_fsaip_mex)
     assert np.isfinite(expected).all()
-    free = []
+    assert allocs > 0                     # the allocating entry point is seen by the counter
     for call in range(3):
-        got = run(lib.dgp_fsaip_mex_noalloc)
-        free.append(torch.cuda.mem_get_info()[0])
+        got, allocs, used = run(lib.dgp_fsaip_mex_noalloc)
         err = np.linalg.norm(got - expected) / np.linalg.norm(expected)
         assert err <= 1e-12, (call, err)
-    # after the first call (which may load the module) no call changes free device memory
-    assert free[1] == free[2]
+        assert allocs == 0, (call, allocs)
+        if call == 0:
+            assert 0 <= used <= MODULE_IMAGE_BYTES, used
+        else:
+            assert used == 0, (call, used)
 
 
 def test_noalloc_rejects_requests_beyond_its_scratch(small_case):
     import torch
     from dogpup_b200._lib import lib, last_error
-    from oracle import solver as osv
 
-    K, M = small_case["K"], small_case["M"]
-    A = sp.tril(K + 1j * 1e-3 * M).tocsr()
-    A.sort_indices()
-    rg, cg = osv.fsai_pattern(A)
+    A, rg, cg = _case(small_case, dfc=1e-3)
     mmax = int(np.diff(rg).max())
     nf = (1 << 20) // mmax + 1
-    dev = lambda a, dt: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device="cuda")
-    ins = [dev(A.data.real, torch.float64), dev(A.data.imag, torch.float64), dev(A.indptr, torch.int32),
-           dev(A.indices, torch.int32), dev(rg, torch.int32), dev(cg, torch.int32)]
+    ins = _inputs(A, rg, cg)
     dummy = torch.zeros(1, dtype=torch.float64, device="cuda")
     rc = lib.dgp_fsaip_mex_noalloc(_vp(dummy), _vp(dummy), *[_vp(t) for t in ins], nf, A.shape[0], None)
     assert rc == DGP_ERR_ARG
     assert "scratch" in last_error()
+
+
+@pytest.mark.parametrize("fault", ["decreasing", "nonzero_start"])
+def test_noalloc_rejects_a_malformed_row_pointer(small_case, fault):
+    """A G row pointer that decreases (or does not start at 0) would place a block's rows
+    outside the fixed array; it is DGP_ERR_MESH before anything is staged, and a valid
+    call afterwards still matches the allocating entry point."""
+    import torch
+    from dogpup_b200._lib import lib, last_error, check
+
+    A, rg, cg = _case(small_case)
+    n, nnzG, nf = A.shape[0], cg.shape[0], 4
+    bad = rg.copy()
+    if fault == "decreasing":
+        bad[n // 2] = bad[n // 2 + 1] + 3                   # row n/2 - 1 grows, row n/2 has negative length
+    else:
+        bad = bad + 1
+    ins = _inputs(A, bad, cg)
+    out = torch.zeros(nnzG * nf, dtype=torch.float64, device="cuda")
+    rc = lib.dgp_fsaip_mex_noalloc(_vp(out), _vp(out), *[_vp(t) for t in ins], nf, n, None)
+    assert rc == DGP_ERR_MESH, rc
+    assert "row pointer" in last_error()
+    ins = _inputs(A, rg, cg)
+    re, im = torch.empty_like(out), torch.empty_like(out)
+    check(lib.dgp_fsaip_mex_noalloc(_vp(re), _vp(im), *[_vp(t) for t in ins], nf, n, None))
+    e_re, e_im = torch.empty_like(out), torch.empty_like(out)
+    check(lib.dgp_fsaip_mex(_vp(e_re), _vp(e_im), *[_vp(t) for t in ins], nf, n, None))
+    torch.cuda.synchronize()
+    got, exp = (re + 1j * im).cpu().numpy(), (e_re + 1j * e_im).cpu().numpy()
+    assert np.linalg.norm(got - exp) <= 1e-12 * np.linalg.norm(exp)
+
+
+def test_noalloc_in_a_new_context_after_the_old_one_is_destroyed(small_case, tmp_path):
+    """MATLAB's reset(gpuDevice) destroys the CUDA context between mex calls; the next call
+    runs in a new context, where the fixed array may sit at another address.  A child
+    process (no torch) makes a context with the driver API, calls both entry points,
+    destroys it, and does the same in a second context: both rounds match to 1e-12, and
+    only the allocating entry point allocates."""
+    A, rg, cg = _case(small_case)
+    case = tmp_path / "case.npz"
+    np.savez(case, re=A.data.real, im=A.data.imag, rp=A.indptr, cl=A.indices, rg=rg, cg=cg, n=A.shape[0])
+    env = dict(os.environ)
+    r = subprocess.run([sys.executable, str(HERE / "noalloc_contexts_child.py"), str(case), "16"],
+                       capture_output=True, text=True, timeout=300, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    rounds = json.loads(r.stdout.strip().splitlines()[-1])
+    assert len(rounds) == 2
+    for rd in rounds:
+        assert rd["rc_alloc"] == 0 and rd["rc_noalloc"] == 0, rd
+        assert rd["finite"] and rd["rel_err"] <= 1e-12, rd
+        assert rd["allocs_noalloc"] == 0 and rd["allocs_alloc"] > 0, rd
