@@ -122,11 +122,20 @@ class Solver:
         """Pick the complex-FP32 SpMM kind and launch shape for this plan (dgp_solver_autotune)."""
         tl, v, r, ms = C.c_int32(), C.c_int32(), C.c_int32(), C.c_float()
         check(lib.dgp_solver_autotune(self._h, C.byref(tl), C.byref(v), C.byref(r), C.byref(ms), stream_ptr()))
-        return {"spmm": "tiled" if tl.value else "gather", "vec": v.value, "rows": r.value,
-                "spmm_ms_per_iteration": round(ms.value, 3)}
+        return dict(self.spmm_shape(), spmm_ms_per_iteration=round(ms.value, 3))
+
+    def spmm_shape(self) -> dict:
+        """The plan's complex-FP32 SpMM: tiled or gather, lane width, rows per block, inner-loop kind."""
+        tl, v, r, k = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        check(lib.dgp_solver_spmm_shape(self._h, C.byref(tl), C.byref(v), C.byref(r), C.byref(k)))
+        return {"spmm": "tiled" if tl.value else "gather", "vec": v.value, "rows": r.value, "kind": k.value}
 
     def set_spmm(self, tiled: bool, vec: int = 0, rows: int = 0):
         check(lib.dgp_solver_set_spmm(self._h, int(tiled), int(vec), int(rows)))
+
+    def set_spmm_kind(self, kind: int):
+        """Inner loop of the gather SpMM: 0 one nonzero per step, 1 two, 2 four, 3 four with packed FMAs."""
+        check(lib.dgp_solver_set_spmm_kind(self._h, int(kind)))
 
     def set_dot_rows(self, mult: int):
         """Rows per block of the dot-product SpMM sweeps as a multiple of the plain ones (0 = 4)."""

@@ -401,6 +401,73 @@ __device__ inline void row_spmv_shfl(int nsp, int cs, const int32_t *__restrict_
   }
 }
 
+// FP32 rows, U nonzeros per step (KIND 1: U = 2, KIND 2: U = 4, KIND 3: U = 4 with packed
+// FP32 FMAs).  As row_spmv_shfl, but the lanes past a row's end hold a padding record
+// (the row's own column, coefficient 0), so the U shuffles, U x gathers and U * VEC
+// complex FMAs of a step are issued without per-nonzero predicates and the U gathers
+// are in flight together.  A padding term adds 0 * x_i (exactly 0 for finite x_i).
+// KIND 3 accumulates sum a.re * x and sum a.im * x as float2 pairs with one packed FMA
+// each (__ffma2_rn) and combines them once per row: 2 instead of 4 FMA instructions
+// per complex product.
+template <int VEC, int KIND, class Coef>
+__device__ inline void row_spmv_shfl_u(int nsp, int cs, const int32_t *__restrict__ rowptr, int64_t i,
+                                       const Coef &cf, const float2 *__restrict__ Xk, float2 (&y)[VEC], int lpr,
+                                       int sub, unsigned mask) {
+  constexpr int U = KIND == 1 ? 2 : 4;
+  constexpr bool PACKED = KIND == 3;
+  float2 ac[VEC], as[PACKED ? VEC : 1];
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) ac[v] = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int v = 0; v < (PACKED ? VEC : 1); ++v) as[v] = make_float2(0.f, 0.f);
+  const int b = __ldg(rowptr + i), e = __ldg(rowptr + i + 1);
+  const int cmax = __reduce_max_sync(mask, e - b);
+  const int step = min(U, lpr);  // lpr is a power of two: every step stays inside the row's lanes
+  for (int base = 0; base < cmax; base += lpr) {
+    int j0 = (int)i;
+    float2 a0 = make_float2(0.f, 0.f);
+    if (b + base + sub < e) cf.get(b + base + sub, j0, a0);
+    const int cnt = min(lpr, cmax - base);
+    for (int u = 0; u < cnt; u += step) {
+      int j[U];
+      float2 a[U];
+#pragma unroll
+      for (int q = 0; q < U; ++q) {
+        if (q < step) {
+          j[q] = __shfl_sync(mask, j0, u + q, lpr);
+          a[q].x = __shfl_sync(mask, a0.x, u + q, lpr);
+          a[q].y = __shfl_sync(mask, a0.y, u + q, lpr);
+        }
+      }
+      float2 x[U][VEC];
+#pragma unroll
+      for (int q = 0; q < U; ++q)
+        if (q < step) ldgv<VEC>(Xk + j[q] * nsp, cs, x[q]);
+#pragma unroll
+      for (int q = 0; q < U; ++q) {
+        if (q < step) {
+          if constexpr (PACKED) {
+            const float2 re = make_float2(a[q].x, a[q].x), im = make_float2(a[q].y, a[q].y);
+#pragma unroll
+            for (int v = 0; v < VEC; ++v) {
+              ac[v] = __ffma2_rn(re, x[q][v], ac[v]);
+              as[v] = __ffma2_rn(im, x[q][v], as[v]);
+            }
+          } else {
+#pragma unroll
+            for (int v = 0; v < VEC; ++v) ac[v] = cfmaf(a[q], x[q][v], ac[v]);
+          }
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) {
+    if constexpr (PACKED) y[v] = make_float2(ac[v].x - as[v].y, ac[v].y + as[v].x);
+    else y[v] = ac[v];
+  }
+}
+
 __device__ inline bool halted(const Ctl *ctl, int need) {
   // need = ST_RUNNING: skip unless running; ST_FINAL: skip only when done
   int s = *(volatile const int *)&ctl->state;
@@ -409,7 +476,8 @@ __device__ inline bool halted(const Ctl *ctl, int need) {
 
 // Y = Op_k X.  MODE 0: store.  MODE 1: store, acc[D1] += Y.W.
 // MODE 2: no store, acc[D2] += Y.W, acc[D3] += Y.Y.  MODE 3: store, acc[D1] += Y.Y.
-template <class R, int VEC, int MODE, class Op>
+// KIND (complex FP32 only): 0 one nonzero per step (row_spmv_shfl), 1-3 row_spmv_shfl_u.
+template <class R, int VEC, int MODE, class Op, int KIND = 0>
 __global__ void __launch_bounds__(BS) k_spmm(Layout L, Op op, const typename CT<R>::C *__restrict__ X,
                                              typename CT<R>::C *__restrict__ Y,
                                              const typename CT<R>::C *__restrict__ W, Cols cols, const Ctl *ctl) {
@@ -437,8 +505,12 @@ __global__ void __launch_bounds__(BS) k_spmm(Layout L, Op op, const typename CT<
     if (vmask == 0u) break;
     if (!valid) continue;
     C y[VEC];
-    if constexpr (sizeof(R) == 4) row_spmv_shfl<VEC>(L.nsp, cs, op.rowptr, i, cf, Xk, y, L.lpr, ln.sub, vmask);
-    else row_spmv<VEC>(L.nsp, cs, op.rowptr, i, cf, Xk, y);
+    if constexpr (sizeof(R) == 4) {
+      if constexpr (KIND == 0) row_spmv_shfl<VEC>(L.nsp, cs, op.rowptr, i, cf, Xk, y, L.lpr, ln.sub, vmask);
+      else row_spmv_shfl_u<VEC, KIND>(L.nsp, cs, op.rowptr, i, cf, Xk, y, L.lpr, ln.sub, vmask);
+    } else {
+      row_spmv<VEC>(L.nsp, cs, op.rowptr, i, cf, Xk, y);
+    }
     const int64_t o = vidx(L, ln.k, i, c0);
     if (MODE != 2) stv<VEC>(Y + o, cs, y);
     if constexpr (MODE == 3) {
@@ -1654,6 +1726,22 @@ inline int vec_for(const SolverPlan *S, bool fp32) {
 
 dim3 grid_of(const Layout &L) { return dim3((unsigned)ceil_div(L.n, L.rows_per_block()), (unsigned)L.nf); }
 
+// k_spmm launch with the plan's gather kind (complex FP32: S->tune_kind; FP64: kind 0)
+template <class R, int VEC, int MODE, class Op>
+void spmm_go(const SolverPlan *S, const Layout &L, size_t smem, cudaStream_t st, const Op &op,
+             const typename CT<R>::C *X, typename CT<R>::C *Y, const typename CT<R>::C *W, const Cols &cols,
+             const Ctl *ctl) {
+  if constexpr (sizeof(R) == 4) {
+    switch (S->tune_kind) {
+      case 1: k_spmm<R, VEC, MODE, Op, 1><<<grid_of(L), BS, smem, st>>>(L, op, X, Y, W, cols, ctl); return;
+      case 2: k_spmm<R, VEC, MODE, Op, 2><<<grid_of(L), BS, smem, st>>>(L, op, X, Y, W, cols, ctl); return;
+      case 3: k_spmm<R, VEC, MODE, Op, 3><<<grid_of(L), BS, smem, st>>>(L, op, X, Y, W, cols, ctl); return;
+      default: break;
+    }
+  }
+  k_spmm<R, VEC, MODE, Op, 0><<<grid_of(L), BS, smem, st>>>(L, op, X, Y, W, cols, ctl);
+}
+
 // one BiCGSTAB iteration (dMesh.m:1295-1340) enqueued on st: KERNELS_PER_ITER launches
 // lane widths: plain SpMM sweeps VS, SpMM sweeps with dot products VD, vector updates 2
 constexpr int VU = 2;
@@ -1694,19 +1782,19 @@ void enqueue_iteration(const SolverPlan *S, const OpA &A, const OpG &G, const Op
     }
   }
   // T1 = G p ; h = G^T T1                                       (:1295-1296)
-  k_spmm<R, VS, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, G, V.p, V.T1, nullptr, W.cols, ctl);
-  k_spmm<R, VS, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, GT, V.T1, V.h, nullptr, W.cols, ctl);
+  spmm_go<R, VS, 0>(S, Ls, 0, st, G, V.p, V.T1, nullptr, W.cols, ctl);
+  spmm_go<R, VS, 0>(S, Ls, 0, st, GT, V.T1, V.h, nullptr, W.cols, ctl);
   // v = A h, d1 = v.r0^                                         (:1301, :1304)
-  k_spmm<R, VD, 1><<<grid_of(Lsd), BS, red_smem(Lsd, 1), st>>>(Lsd, A, V.h, V.v, V.rhat, W.cols, ctl);
+  spmm_go<R, VD, 1>(S, Lsd, red_smem(Lsd, 1), st, A, V.h, V.v, V.rhat, W.cols, ctl);
   k_stage_alpha<<<1, 1024, 0, st>>>(W.cols, ctl);
   // s = r - alpha v ; ||s||                                     (:1306-1308)
   k_update_s<R, VU><<<grid_of(Lud), BS, red_smem(Lud, 1), st>>>(Lud, V.r, V.v, V.s, W.cols, ctl);
   k_stage_check_s<<<1, 1024, 0, st>>>(W.cols, ctl);
   // Gs = G s ; z = G^T Gs ; t = A z ; (G t).Gs, (G t).(G t)     (:1315-1325)
-  k_spmm<R, VS, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, G, V.s, V.T1, nullptr, W.cols, ctl);
-  k_spmm<R, VS, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, GT, V.T1, V.z, nullptr, W.cols, ctl);
-  k_spmm<R, VS, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, A, V.z, V.t, nullptr, W.cols, ctl);
-  k_spmm<R, VD, 2><<<grid_of(Lsd), BS, red_smem(Lsd, 2), st>>>(Lsd, G, V.t, nullptr, V.T1, W.cols, ctl);
+  spmm_go<R, VS, 0>(S, Ls, 0, st, G, V.s, V.T1, nullptr, W.cols, ctl);
+  spmm_go<R, VS, 0>(S, Ls, 0, st, GT, V.T1, V.z, nullptr, W.cols, ctl);
+  spmm_go<R, VS, 0>(S, Ls, 0, st, A, V.z, V.t, nullptr, W.cols, ctl);
+  spmm_go<R, VD, 2>(S, Lsd, red_smem(Lsd, 2), st, G, V.t, nullptr, V.T1, W.cols, ctl);
   k_stage_omega<<<1, 1024, 0, st>>>(W.cols, ctl);
   // x += alpha h + om z ; r = s - om t ; p -= om v ; ||r|| ; r0^.r   (:1305, :1327-1337)
   k_update_xrp<R, VU><<<grid_of(Lud), BS, red_smem(Lud, 2), st>>>(Lud, V.x, V.h, V.z, V.r, V.s, V.t, V.p, V.v,
@@ -1734,8 +1822,8 @@ void enqueue_cocg_precond(const SolverPlan *S, const OpG &G, const OpG &GT, cons
   }
   if (!done) {
     const Layout Ls = spmm_layouts(S, VS, sizeof(R) == 4).L, Lsd = spmm_layouts(S, VD, sizeof(R) == 4).Ld;
-    k_spmm<R, VD, 3><<<grid_of(Lsd), BS, red_smem(Lsd, 1), st>>>(Lsd, G, V.r, V.T1, nullptr, W.cols, ctl);
-    k_spmm<R, VS, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, GT, V.T1, V.z, nullptr, W.cols, ctl);
+    spmm_go<R, VD, 3>(S, Lsd, red_smem(Lsd, 1), st, G, V.r, V.T1, nullptr, W.cols, ctl);
+    spmm_go<R, VS, 0>(S, Ls, 0, st, GT, V.T1, V.z, nullptr, W.cols, ctl);
   }
   k_cocg_rho<<<1, 1024, 0, st>>>(W.cols, ctl, first);
 }
@@ -1767,7 +1855,7 @@ void enqueue_cocg(const SolverPlan *S, const OpA &A, const OpG &G, const OpG &GT
   }
   if (!done) {
     const Layout Lsd = spmm_layouts(S, VD, sizeof(R) == 4).Ld;
-    k_spmm<R, VD, 1><<<grid_of(Lsd), BS, red_smem(Lsd, 1), st>>>(Lsd, A, V.p, V.v, V.p, W.cols, ctl);
+    spmm_go<R, VD, 1>(S, Lsd, red_smem(Lsd, 1), st, A, V.p, V.v, V.p, W.cols, ctl);
   }
   k_cocg_alpha<<<1, 1024, 0, st>>>(W.cols, ctl);
   k_update_r<R, VU><<<grid_of(Lud), BS, red_smem(Lud, 1), st>>>(Lud, V.r, V.v, W.cols, ctl);
@@ -2187,10 +2275,10 @@ void profile_launch(int which, const SolverPlan *S, const OpA32 &A, const OpG32 
   const Layout L = spmm_layouts(S, VEC, true).L, Ld = spmm_layouts(S, VEC, true).Ld;
   const Layout Lu = layouts_for(S, VU).L, Lud = layouts_for(S, VU).Ld;
   switch (which) {
-    case 0: k_spmm<float, VEC, 0><<<grid_of(L), BS, 0, st>>>(L, A, V.z, V.x, nullptr, W.cols, ctl); break;
-    case 1: k_spmm<float, VEC, 0><<<grid_of(L), BS, 0, st>>>(L, G, V.p, V.T1, nullptr, W.cols, ctl); break;
-    case 4: k_spmm<float, VEC, 1><<<grid_of(Ld), BS, red_smem(Ld, 1), st>>>(Ld, A, V.p, V.v, V.p, W.cols, ctl); break;
-    case 5: k_spmm<float, VEC, 3><<<grid_of(Ld), BS, red_smem(Ld, 1), st>>>(Ld, G, V.r, V.T1, nullptr, W.cols, ctl); break;
+    case 0: spmm_go<float, VEC, 0>(S, L, 0, st, A, V.z, V.x, nullptr, W.cols, ctl); break;
+    case 1: spmm_go<float, VEC, 0>(S, L, 0, st, G, V.p, V.T1, nullptr, W.cols, ctl); break;
+    case 4: spmm_go<float, VEC, 1>(S, Ld, red_smem(Ld, 1), st, A, V.p, V.v, V.p, W.cols, ctl); break;
+    case 5: spmm_go<float, VEC, 3>(S, Ld, red_smem(Ld, 1), st, G, V.r, V.T1, nullptr, W.cols, ctl); break;
     case 6: k_update_r<float, VU><<<grid_of(Lud), BS, red_smem(Lud, 1), st>>>(Lud, V.r, V.v, W.cols, ctl); break;
     case 7: k_update_px<float, VU><<<grid_of(Lu), BS, 0, st>>>(Lu, V.x, V.p, V.z, W.cols, ctl); break;
     case 2:
@@ -2276,13 +2364,13 @@ void spmm_set(const SolverPlan *S, const OpA32 &A, const OpG32 &G, const OpG32 &
   const Layouts LL = spmm_layouts(S, VEC, true);
   const Layout Ls = LL.L, Lsd = LL.Ld;
   // scratch vectors from the first NVEC_COCG slots only (x, r and r^ stand in for h, s and t)
-  k_spmm<float, VEC, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, G, V.p, V.T1, nullptr, W.cols, ctl);
-  k_spmm<float, VEC, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, GT, V.T1, V.x, nullptr, W.cols, ctl);
-  k_spmm<float, VEC, 1><<<grid_of(Lsd), BS, red_smem(Lsd, 1), st>>>(Lsd, A, V.x, V.v, V.rhat, W.cols, ctl);
-  k_spmm<float, VEC, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, G, V.r, V.T1, nullptr, W.cols, ctl);
-  k_spmm<float, VEC, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, GT, V.T1, V.z, nullptr, W.cols, ctl);
-  k_spmm<float, VEC, 0><<<grid_of(Ls), BS, 0, st>>>(Ls, A, V.z, V.rhat, nullptr, W.cols, ctl);
-  k_spmm<float, VEC, 2><<<grid_of(Lsd), BS, red_smem(Lsd, 2), st>>>(Lsd, G, V.rhat, nullptr, V.T1, W.cols, ctl);
+  spmm_go<float, VEC, 0>(S, Ls, 0, st, G, V.p, V.T1, nullptr, W.cols, ctl);
+  spmm_go<float, VEC, 0>(S, Ls, 0, st, GT, V.T1, V.x, nullptr, W.cols, ctl);
+  spmm_go<float, VEC, 1>(S, Lsd, red_smem(Lsd, 1), st, A, V.x, V.v, V.rhat, W.cols, ctl);
+  spmm_go<float, VEC, 0>(S, Ls, 0, st, G, V.r, V.T1, nullptr, W.cols, ctl);
+  spmm_go<float, VEC, 0>(S, Ls, 0, st, GT, V.T1, V.z, nullptr, W.cols, ctl);
+  spmm_go<float, VEC, 0>(S, Ls, 0, st, A, V.z, V.rhat, nullptr, W.cols, ctl);
+  spmm_go<float, VEC, 2>(S, Lsd, red_smem(Lsd, 2), st, G, V.rhat, nullptr, V.T1, W.cols, ctl);
 }
 }  // namespace
 
@@ -2352,18 +2440,20 @@ int solver_autotune(SolverPlan *S, int32_t *tiled_out, int32_t *vec_out, int32_t
   cudaEvent_t e0, e1;
   DGP_CUDA(cudaEventCreate(&e0));
   DGP_CUDA(cudaEventCreate(&e1));
-  const int32_t old_vec = S->tune_vec, old_rows = S->tune_rows, old_tiled = S->tiled;
+  const int32_t old_vec = S->tune_vec, old_rows = S->tune_rows, old_tiled = S->tiled, old_kind = S->tune_kind;
   S->tiled = 0;
   float best = 3.4e38f;
-  int32_t bv = 0, br = 0;
+  int32_t bv = 0, br = 0, bk = 0;
   int launches = 0;
   int rc = DGP_OK;
+  for (int kind = 0; kind < 4 && rc == DGP_OK; ++kind)
   for (int vec : {8, 4, 2}) {
     if (vec > S->nsp || S->nsp / vec > 32) continue;
     int last_ipb = -1;
     for (int rows : {32, 64, 128, 256}) {
       S->tune_vec = vec;
       S->tune_rows = rows;
+      S->tune_kind = kind;
       const int ipb = spmm_layouts(S, vec, true).L.ipb;
       if (ipb == last_ipb) continue;  // same launch shape as the previous candidate
       last_ipb = ipb;
@@ -2392,6 +2482,7 @@ int solver_autotune(SolverPlan *S, int32_t *tiled_out, int32_t *vec_out, int32_t
         best = t;
         bv = vec;
         br = rows;
+        bk = kind;
       }
     }
     if (rc != DGP_OK) break;
@@ -2426,11 +2517,13 @@ int solver_autotune(SolverPlan *S, int32_t *tiled_out, int32_t *vec_out, int32_t
     S->tune_vec = old_vec;
     S->tune_rows = old_rows;
     S->tiled = old_tiled;
+    S->tune_kind = old_kind;
     return rc != DGP_OK ? rc : fail(DGP_ERR_UNSUPPORTED, "autotune: no launch shape fits this plan");
   }
   DGP_CHECK_LAUNCH();
   S->tune_vec = bv;
   S->tune_rows = br;
+  S->tune_kind = bk;
   S->tiled = bt;
   for (auto &g : S->graph)
     if (g) {
@@ -2461,6 +2554,18 @@ int solver_set_spmm(SolverPlan *S, int32_t tiled, int32_t vec, int32_t rows) {
     S->tune_vec = vec;
     S->tune_rows = vec ? rows : 0;
   }
+  for (auto &g : S->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  for (int &gi : S->graph_iters) gi = 0;
+  return DGP_OK;
+}
+
+int solver_set_spmm_kind(SolverPlan *S, int32_t kind) {
+  DGP_REQUIRE(kind >= 0 && kind <= 3, "set_spmm_kind: kind must be 0, 1, 2 or 3");
+  S->tune_kind = kind;
   for (auto &g : S->graph)
     if (g) {
       cudaGraphExecDestroy(g);

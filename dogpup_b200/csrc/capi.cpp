@@ -331,6 +331,20 @@ int dgp_solver_set_spmm(dgp_solver_t s, int32_t tiled, int32_t vec, int32_t rows
   DGP_GUARD(solver_set_spmm(&s->plan, tiled, vec, rows));
 }
 
+int dgp_solver_set_spmm_kind(dgp_solver_t s, int32_t kind) {
+  if (!s) return fail(DGP_ERR_ARG, "solver_set_spmm_kind: null handle");
+  DGP_GUARD(solver_set_spmm_kind(&s->plan, kind));
+}
+
+int dgp_solver_spmm_shape(dgp_solver_t s, int32_t *tiled, int32_t *vec, int32_t *rows, int32_t *kind) {
+  if (!s) return fail(DGP_ERR_ARG, "solver_spmm_shape: null handle");
+  if (tiled) *tiled = s->plan.tiled;
+  if (vec) *vec = s->plan.tune_vec;
+  if (rows) *rows = s->plan.tune_rows;
+  if (kind) *kind = s->plan.tune_kind;
+  return DGP_OK;
+}
+
 int dgp_solver_set_dot_rows(dgp_solver_t s, int32_t mult) {
   if (!s) return fail(DGP_ERR_ARG, "solver_set_dot_rows: null handle");
   DGP_GUARD(solver_set_dot_rows(&s->plan, mult));

@@ -99,6 +99,7 @@ struct SolverPlan {
   int graph_iters[3] = {0, 0, 0};
   // SpMM launch shape of the complex-FP32 sweeps chosen by solver_autotune (0 = built-in default)
   int32_t tune_vec = 0, tune_rows = 0;
+  int32_t tune_kind = 0;  // gather SpMM inner loop: 0 one nonzero per step, 1 two, 2 four, 3 four + packed FMAs
   int32_t tune_dot = 0;  // rows per block of the FP32 dot-product sweeps, as a multiple of tune_rows (0: 4)
   // tiled SpMM (halo rows staged in shared memory) for A, G and G^T; tiled = 1 selects it
   TiledPlan tA, tG, tGT;
@@ -126,6 +127,7 @@ int solver_profile(SolverPlan *S, int which, int reps, float *ms, double *bytes,
 int solver_autotune(SolverPlan *S, int32_t *tiled, int32_t *vec, int32_t *rows, float *ms, cudaStream_t st);
 // sets the SpMM kind / shape explicitly (tiled 0: gather kernel with vec, rows; 1: tiled)
 int solver_set_spmm(SolverPlan *S, int32_t tiled, int32_t vec, int32_t rows);
+int solver_set_spmm_kind(SolverPlan *S, int32_t kind);
 int solver_set_dot_rows(SolverPlan *S, int32_t mult);
 // largest relative difference between the tiled and the gather SpMM on the plan's operators
 int solver_check_spmm(SolverPlan *S, double *max_rel, cudaStream_t st);

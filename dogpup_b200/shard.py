@@ -77,27 +77,27 @@ def sharded_tg_data(coef, harmonics, gate_fc, nt, fc2tg, group=None):
 
 def gather_spectra(data, nf, rank, world, group=None):
     """[NM x NF] detector data from every rank's [NM x len(own harmonics)] block (one
-    all-gather; blocks padded to ceil(NF / W) columns)."""
+    all-gather of real views; blocks padded to ceil(NF / W) columns)."""
     import torch
     import torch.distributed as dist
     nm = data.shape[0]
     width = -(-nf // world)
-    block = data.new_zeros((width, nm))
+    block = torch.zeros((width, nm, 2), dtype=torch.float64, device=data.device)
     own = harmonic_shard(nf, rank, world)
     if own:
-        block[:len(own)] = data.transpose(0, 1)
-    parts = [torch.empty_like(block) for _ in range(world)]
+        block[:len(own)] = torch.view_as_real(data.transpose(0, 1).contiguous())
     if block.is_cuda and dist.get_backend(group) == "gloo":
-        hp = [p.cpu() for p in parts]
+        hp = [torch.empty_like(block, device="cpu") for _ in range(world)]
         dist.all_gather(hp, block.cpu(), group=group)
         parts = [p.to(block.device) for p in hp]
     else:
+        parts = [torch.empty_like(block) for _ in range(world)]
         dist.all_gather(parts, block, group=group)
-    out = data.new_empty((nm, nf))
+    out = torch.empty((nm, nf), dtype=torch.complex128, device=data.device)
     for r in range(world):
         ks = harmonic_shard(nf, r, world)
         if ks:
-            out[:, ks] = parts[r][:len(ks)].transpose(0, 1)
+            out[:, ks] = torch.view_as_complex(parts[r][:len(ks)].contiguous()).transpose(0, 1)
     return out
 
 

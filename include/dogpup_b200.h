@@ -246,8 +246,9 @@ int dgp_solver_destroy(dgp_solver_t solver);
 int dgp_solver_memory(dgp_solver_t solver, int64_t *bytes);
 /* Autotuner of the complex-FP32 (DGP_PREC_MIXED) sweeps: times the seven
  * SpMM launches of one BiCGSTAB iteration for each candidate -- the gather
- * SpMM at each lane width (8, 4, 2 complex values per lane) x rows per block
- * (32 .. 256) that fits the plan, and the tiled SpMM (32-row blocks whose
+ * SpMM of each inner-loop kind (dgp_solver_set_spmm_kind) at each lane width
+ * (8, 4, 2 complex values per lane) x rows per block (32 .. 256) that fits
+ * the plan, and the tiled SpMM (32-row blocks whose
  * halo rows are staged in shared memory) when it fits -- on the plan's own
  * workspace (allocating it if needed), and keeps the fastest for later
  * solves.  Outputs (each may be NULL): 1 if the tiled SpMM won, the best
@@ -262,6 +263,15 @@ int dgp_solver_autotune(dgp_solver_t solver, int32_t *tiled, int32_t *vec,
  * block (32, 64, 128, 256; 0 = 64). */
 int dgp_solver_set_spmm(dgp_solver_t solver, int32_t tiled, int32_t vec,
                         int32_t rows);
+/* Inner loop of the complex-FP32 gather SpMM: kind 0 handles one nonzero
+ * per step; 1 and 2 issue the gathers of 2 or 4 nonzeros together (lanes
+ * past a row's end carry a zero coefficient on the row's own column); 3 is
+ * kind 2 with packed FP32 FMAs (two instead of four FMA instructions per
+ * complex product).  dgp_solver_autotune searches the kinds with the lane widths and
+ * block heights; dgp_solver_spmm_shape reports the plan's current choice. */
+int dgp_solver_set_spmm_kind(dgp_solver_t solver, int32_t kind);
+int dgp_solver_spmm_shape(dgp_solver_t solver, int32_t *tiled, int32_t *vec,
+                          int32_t *rows, int32_t *kind);
 /* Rows per block of the complex-FP32 SpMM sweeps that also reduce a dot
  * product (v = A h with v.r^, the COCG sweeps q = A p with p.q and T = G r
  * with T.T), as a multiple of the plain sweeps' rows per block: 1, 2, 4, 8

@@ -112,6 +112,30 @@ def test_sharded_tg_data_gloo(world, nf):
     assert max(errs.values()) <= 1e-12, errs
 
 
+def _gather_rank_main(rank, world, port, q, nf):
+    import torch
+    import torch.distributed as dist
+    from dogpup_b200.shard import gather_spectra
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        rng = np.random.default_rng(11)
+        full = torch.as_tensor(rng.standard_normal((5, nf)) + 1j * rng.standard_normal((5, nf)))
+        mine = harmonic_shard(nf, rank, world)
+        got = gather_spectra(full[:, mine], nf, rank, world)
+        q.put((rank, bool(torch.equal(got, full))))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,nf", [(2, 9), (3, 7), (3, 2)])
+def test_gather_spectra_gloo(world, nf):
+    """The all-gather of the ranks' harmonic columns rebuilds the full [NM x NF] spectra
+    bit for bit on every rank, empty shares included."""
+    res = _spawn(_gather_rank_main, world, nf)
+    assert all(res.values()), res
+
+
 @pytest.mark.gpu
 def test_sharded_forward_shares_sum_to_full_tg_data():
     """Both shards of a 2-way split run in one process (no process group: each
