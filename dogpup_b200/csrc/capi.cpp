@@ -84,6 +84,7 @@ int csr_spmv_run(const int32_t *rowptr, const int32_t *col, const double *val, i
 int mex_fsaip(double *out_re, double *out_im, const double *A_re, const double *A_im, const int *rPtrA,
               const int *cPtrA, const int *rPtrG, const int *cPtrG, int nfreqs, int nrows, cudaStream_t st,
               int es = 1);
+int set_jacobian_engine(int engine);
 int jacobian_run(int mode, const int32_t *prow, const int32_t *pcol, const double *pval, int64_t nv, const double *w,
                  const double *phi, int ns, const double *phiA, int nd, int64_t nn, int nf, const double *fpsf,
                  const int32_t *link, int nm, const double *gate, int ng, int nt, const double *rytov, void *out,
@@ -436,6 +437,8 @@ int dgp_fc2tg(const double *d_c, int64_t nr, int32_t nf, const double *d_gate_fc
 }
 
 // --------------------------------------------------------------- Jacobian
+int dgp_set_jacobian_engine(int32_t engine) { DGP_GUARD(set_jacobian_engine(engine)); }
+
 int dgp_jacobian_complex(const int32_t *d_P_rowptr, const int32_t *d_P_col, const double *d_P_val, int64_t nv,
                          const double *d_w, const double *d_phi, int32_t ns, const double *d_phiA, int32_t nd,
                          int64_t nn, int32_t nf, const double *d_fpsf, const int32_t *d_link, int32_t nm, double *d_J,

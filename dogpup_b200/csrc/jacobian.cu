@@ -29,6 +29,7 @@
 
 #include "dgp_common.cuh"
 #include "dgp_internal.h"
+#include "tc_common.cuh"
 
 namespace dgp {
 
@@ -173,6 +174,387 @@ __global__ void __launch_bounds__(JBS) k_jacobian_tg(JArgs a, const float2 *__re
   }
 }
 
+// ------------------------------------------------------------------------------------------
+// Time-gated Jacobian on the tensor cores (tcgen05, kind::tf32, 3xTF32 split).
+//
+// Per voxel v and tile of 128 links m, J_tg[v][g][m] = w_v * sum_K' A'[m][K'] B'[K'][g] with
+//   A'[m][K'] = Re / Im of a_k(m) = (P phi_s)_k (P phiA_d)_k  and  B'[K'][g] = Re / -Im of C[g,k],
+// K' = 2 NF (the real and imaginary parts of the DFT's complex products).  K' runs in chunks of
+// 16 harmonics = 32 values ([16 real | 16 imaginary], one 128-byte row of a 128B-swizzled
+// K-major tile).  FP32 values x are split x = hi + lo with hi = tf32(x), lo = tf32(x - hi), and
+// each chunk issues hi*hi + hi*lo + lo*hi into an FP32 accumulator in tensor memory (the lo*lo
+// term, ~2^-22 relative, is dropped).
+//
+// CTA = 256 threads, persistent over voxels (one CTA per SM).  All threads build the A' chunks
+// (two threads per link row, 8 harmonics each) from the voxel's fields staged in shared memory;
+// thread 0 issues the chunk's 12 MMAs (M = 128, N = 32 gate columns, K = 8) and commits them to
+// the chunk buffer's mbarrier.  Two chunk buffers: the next chunk is built while the tensor core
+// works on the previous one.  Two accumulators in tensor memory (2 x 32 columns): a tile's
+// epilogue (tcgen05.ld, w_v and Rytov scaling, coalesced FP32 stores) runs while the next tile's
+// MMAs are in flight.  Every mbarrier wait is bounded; a timeout raises err and ends the kernel
+// after waiting (bounded) for the MMAs it issued, and the tensor memory is always freed.
+constexpr int TC_THREADS = 256;
+constexpr int TC_CH = 16;                    // harmonics per K' chunk
+constexpr int TC_ROWS = 128;                 // links per tile (MMA M)
+constexpr int TC_N = 32;                     // gate columns (MMA N), NG <= 32
+constexpr int TC_ATILE = TC_ROWS * 128;      // one 128 x 32 fp32 operand tile: 16 KB
+constexpr int TC_BTILE = TC_N * 128;         // one 32 x 32 fp32 operand tile: 4 KB
+constexpr uint32_t TC_IDESC = tc::idesc(2, 2, TC_ROWS, TC_N);
+
+struct TcLayout {
+  uint32_t a_off, b_off, f_off, bytes;       // A' buffers, B' table, staged fields, total (from the 1 KB-aligned base)
+  int nch;
+};
+
+__host__ __device__ inline TcLayout tc_layout(int nf, int ns, int nd) {
+  TcLayout L;
+  L.nch = (nf + TC_CH - 1) / TC_CH;
+  L.a_off = 0;                                               // 2 buffers x (hi, lo)
+  L.b_off = 4 * TC_ATILE;                                    // nch x (hi) then nch x (lo)
+  L.f_off = L.b_off + 2 * L.nch * TC_BTILE;
+  L.bytes = L.f_off + (uint32_t)(sizeof(float2) * (size_t)nf * (ns + nd));
+  return L;
+}
+
+__device__ inline void st_split4(unsigned char *hi, unsigned char *lo, uint32_t off, const float (&x)[4]) {
+  float h[4], l[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    h[i] = tc::to_tf32(x[i]);
+    l[i] = tc::to_tf32(x[i] - h[i]);
+  }
+  *reinterpret_cast<float4 *>(hi + off) = make_float4(h[0], h[1], h[2], h[3]);
+  *reinterpret_cast<float4 *>(lo + off) = make_float4(l[0], l[1], l[2], l[3]);
+}
+
+__global__ void __launch_bounds__(TC_THREADS, 1) k_jacobian_tg_tc(JArgs a, const float2 *__restrict__ C /*[ng][nf]*/,
+                                                                 const double *__restrict__ rytov,
+                                                                 float *__restrict__ Jtg, int *err) {
+  extern __shared__ __align__(1024) unsigned char tc_raw[];
+  __shared__ __align__(8) uint64_t bar_buf[2], bar_d[2];
+  __shared__ uint32_t tmem_slot;
+  __shared__ int abort_flag;
+  unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(tc_raw) + 1023) & ~uintptr_t(1023));
+  const TcLayout L = tc_layout(a.nf, a.ns, a.nd);
+  unsigned char *Ab = sm + L.a_off;                   // buffer b: hi at b*2*ATILE, lo at +ATILE
+  unsigned char *Bhi = sm + L.b_off, *Blo = Bhi + L.nch * TC_BTILE;
+  float2 *Ps = reinterpret_cast<float2 *>(sm + L.f_off), *Pd = Ps + a.nf * a.ns;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  if (tid == 0) {
+    for (int b = 0; b < 2; ++b) {
+      tc::mbar_init(&bar_buf[b], 1);
+      tc::mbar_init(&bar_d[b], 1);
+    }
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) tc::tmem_alloc(&tmem_slot, 2 * TC_N);
+  // B' = the gate table, split: row g (MMA N), K' = chunk c's [Re C[g][16c..16c+15] | -Im C[g][..]]
+  for (int t = tid; t < L.nch * TC_N * 8; t += TC_THREADS) {
+    const int c = t / (TC_N * 8), g = (t / 8) % TC_N, q = t % 8;   // 16-byte chunk q of row g in chunk c
+    float x[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int j = 4 * q + i, k = c * TC_CH + (j & 15);
+      const float2 v = (g < a.ng && k < a.nf) ? C[g * a.nf + k] : make_float2(0.f, 0.f);
+      x[i] = j < 16 ? v.x : -v.y;
+    }
+    st_split4(Bhi + c * TC_BTILE, Blo + c * TC_BTILE, tc::sw128_chunk(g, q), x);
+  }
+  tc::fence_async_smem();
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = tmem_slot;
+
+  const int r = tid & (TC_ROWS - 1), half = tid >> 7;   // link row of the tile, harmonic half of a chunk
+  uint32_t q = 0, t = 0;                               // chunks and tiles issued by this CTA
+  bool have_prev = false, stop = false;
+  int64_t pv = 0;
+  int pm0 = 0;
+  uint32_t pt = 0;
+  float pw = 0.f;
+
+  // epilogue of tile tp (voxel vp, links m0p..): TMEM accumulator tp & 1 -> J
+  auto epilogue = [&](uint32_t tp, int64_t vp, int m0p, float wp) {
+    bool ok = tc::mbar_wait(&bar_d[tp & 1], (tp >> 1) & 1);
+    if (!ok) atomicOr(err, 1);
+    ok = __all_sync(0xffffffffu, ok);
+    tc::fence_after_sync();
+    if (ok) {
+      const int quad = warp & 3, cbase = (warp >> 2) * 16;
+      uint32_t v[16];
+      tc::tmem_ld16(tmem + ((uint32_t)(32 * quad) << 16) + (tp & 1) * TC_N + cbase, v);
+      const int m = m0p + 32 * quad + lane;
+      if (m < a.nm) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const int g = cbase + i;
+          if (g < a.ng) {
+            float val = wp * __uint_as_float(v[i]);
+            if (rytov) val = val / (float)rytov[(int64_t)m * a.ng + g];
+            Jtg[((int64_t)vp * a.ng + g) * a.nm + m] = val;
+          }
+        }
+      }
+    }
+    tc::fence_before_sync();
+    return ok;
+  };
+
+  for (int64_t v = blockIdx.x; v < a.nv && !stop; v += gridDim.x) {
+    __syncthreads();                                   // the previous voxel's chunks are built
+    stage_field(a, v, a.phi, a.ns, Ps);
+    stage_field(a, v, a.phiA, a.nd, Pd);
+    __syncthreads();
+    const float wv = (float)(a.w ? a.w[v] : 1.0);
+    for (int m0 = 0; m0 < a.nm && !stop; m0 += TC_ROWS) {
+      const int m = m0 + r;
+      const bool valid = m < a.nm;
+      const int s = valid ? a.link[2 * m] : 0, d = valid ? a.link[2 * m + 1] : 0;
+      for (int c = 0; c < L.nch; ++c) {
+        const uint32_t b = q & 1;
+        bool ok = true;
+        if (q >= 2) ok = tc::mbar_wait(&bar_buf[b], ((q >> 1) - 1) & 1);   // chunk q-2 has been consumed
+        if (!ok) {
+          atomicOr(err, 2);
+          abort_flag = 1;
+        }
+        unsigned char *hi = Ab + b * 2 * TC_ATILE, *lo = hi + TC_ATILE;
+        if (ok) {
+          // this thread's 8 harmonics of chunk c: K' = 8 half + i (real) and 16 + 8 half + i (imaginary)
+          float re[8], im[8];
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            const int k = c * TC_CH + 8 * half + i;
+            re[i] = im[i] = 0.f;
+            if (valid && k < a.nf) {
+              const float2 x = Ps[k * a.ns + s], y = Pd[k * a.nd + d];
+              re[i] = x.x * y.x - x.y * y.y;
+              im[i] = x.x * y.y + x.y * y.x;
+            }
+          }
+          const float r0[4] = {re[0], re[1], re[2], re[3]}, r1[4] = {re[4], re[5], re[6], re[7]};
+          const float i0[4] = {im[0], im[1], im[2], im[3]}, i1[4] = {im[4], im[5], im[6], im[7]};
+          st_split4(hi, lo, tc::sw128_chunk(r, 2 * half + 0), r0);
+          st_split4(hi, lo, tc::sw128_chunk(r, 2 * half + 1), r1);
+          st_split4(hi, lo, tc::sw128_chunk(r, 4 + 2 * half + 0), i0);
+          st_split4(hi, lo, tc::sw128_chunk(r, 4 + 2 * half + 1), i1);
+        }
+        tc::fence_async_smem();
+        tc::fence_before_sync();
+        if (__syncthreads_or(abort_flag)) {
+          stop = true;
+          break;
+        }
+        if (tid == 0) {
+          tc::fence_after_sync();
+          const uint32_t d_tm = tmem + (t & 1) * TC_N;
+          const uint32_t ah = tc::smem_u32(hi), al = tc::smem_u32(lo);
+          const uint32_t bh = tc::smem_u32(Bhi + c * TC_BTILE), bl = tc::smem_u32(Blo + c * TC_BTILE);
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk) {             // K = 8 tf32 = 32 bytes per MMA
+            const uint32_t o = 32u * kk;
+            tc::umma_tf32<TC_IDESC>(d_tm, tc::sdesc_k_sw128(ah + o), tc::sdesc_k_sw128(bh + o), (c | kk) ? 1u : 0u);
+            tc::umma_tf32<TC_IDESC>(d_tm, tc::sdesc_k_sw128(ah + o), tc::sdesc_k_sw128(bl + o), 1u);
+            tc::umma_tf32<TC_IDESC>(d_tm, tc::sdesc_k_sw128(al + o), tc::sdesc_k_sw128(bh + o), 1u);
+          }
+          tc::umma_commit(&bar_buf[b]);
+          if (c == L.nch - 1) tc::umma_commit(&bar_d[t & 1]);
+        }
+        ++q;
+        if (have_prev && c == (L.nch > 1 ? 1 : 0)) {   // the previous tile's MMAs are done by now
+          if (!epilogue(pt, pv, pm0, pw)) abort_flag = 1;
+          have_prev = false;
+        }
+      }
+      if (stop) break;
+      have_prev = true;
+      pt = t;
+      pv = v;
+      pm0 = m0;
+      pw = wv;
+      ++t;
+    }
+  }
+  if (!stop && have_prev) epilogue(pt, pv, pm0, pw);
+  // teardown: every MMA this CTA issued has completed (bounded) before the tensor memory is freed
+  if (q > 0 && tid == 0) {
+    const uint32_t last = q - 1;
+    tc::mbar_wait(&bar_buf[last & 1], (last >> 1) & 1);
+    if (q > 1) tc::mbar_wait(&bar_buf[(last - 1) & 1], ((last - 1) >> 1) & 1);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_free(tmem, 2 * TC_N);
+}
+
+// ------------------------------------------------------------------------------------------
+// Vector-Jacobian product on the tensor cores.
+//
+//   vjp[v] = w_v Re sum_k sum_s (P phi)_k[v][s] Y_k[v][s],   Y_k = (P phiA)_k Chat_k^T,
+//
+// with Chat_k[s][d] = sum over links m = (s, d) of Chat[m][k] (the upstream gradient folded into
+// the DFT, zero for source-detector pairs without a link).  Per harmonic this is a complex GEMM
+// over all voxels, [NV x ND] x [ND x NS], written as a real one with K' = 2 ND (re, im of each
+// detector, interleaved) and N' = 2 NS (re, im of each source, interleaved), on the tensor cores
+// (kind::tf32, 3xTF32 split, M = 128 voxels, N' = 64, K' = 64: NS, ND <= 32, padded with zeros).
+// The per-harmonic operand B'_k = the real embedding of Chat_k^T is built once per call in
+// global memory, already split and swizzled (k_vjp_btab), and copied into shared memory.
+//
+// CTA = 256 threads over a tile of 128 voxels, looping over the harmonics: the threads convert
+// this tile's (P phiA)_k rows to the split A' operand (coalesced FP64 loads), thread 0 issues the
+// 24 MMAs, and in the epilogue each warp reads its 32 voxel rows x 32 columns of Y_k from tensor
+// memory, dots them with (P phi)_k read from global memory and accumulates in FP64.  96 KB of
+// shared memory: two CTAs per SM overlap one's loads with the other's MMAs and epilogue.
+constexpr int VT_THREADS = 256;
+constexpr int VT_ROWS = 128;                       // voxels per tile (MMA M)
+constexpr int VT_NP = 64;                          // N' = 2 x 32 sources
+constexpr int VT_KP = 64;                          // K' = 2 x 32 detectors
+constexpr int VT_A = VT_ROWS * VT_KP * 4;          // 32 KB: 128 rows x 64 fp32 (two 128-byte atoms)
+constexpr int VT_B = VT_NP * VT_KP * 4;            // 16 KB
+constexpr int VT_SMEM = 2 * VT_A + 2 * VT_B + 1024;
+constexpr uint32_t VT_IDESC = tc::idesc(2, 2, VT_ROWS, VT_NP);
+
+// K-major split operand image: element (row, j) of a [rows][64] fp32 tile stored as two 128-byte
+// swizzled sub-tiles (j < 32, j >= 32) of rows x 128 B
+__host__ __device__ inline uint32_t kmaj64(uint32_t row, uint32_t j, uint32_t rows) {
+  return (j >> 5) * rows * 128u + tc::sw128_chunk(row, (j & 31u) >> 2) + (j & 3u) * 4u;
+}
+
+// Btab[k] = (hi, lo) images of B'_k [64 rows n'][64 K'] (16 KB each), from Chat [nm][nf]:
+//   B'[2s][2d] = Re C, B'[2s][2d+1] = -Im C, B'[2s+1][2d] = Im C, B'[2s+1][2d+1] = Re C,
+// C = Chat_k[s][d]; one thread per (k, s, d).
+__global__ void k_vjp_btab(const float2 *__restrict__ Chat, const int32_t *__restrict__ link, int nm, int nf,
+                           unsigned char *__restrict__ Btab) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= (int64_t)nf * 32 * 32) return;
+  const int k = (int)(t / 1024), s = (int)(t / 32 % 32), d = (int)(t % 32);
+  float2 c = make_float2(0.f, 0.f);
+  for (int m = 0; m < nm; ++m)  // link tables are small (nm <= 1024 here): a scan per entry
+    if (link[2 * m] == s && link[2 * m + 1] == d) {
+      const float2 x = Chat[(int64_t)m * nf + k];
+      c.x += x.x;
+      c.y += x.y;
+    }
+  unsigned char *hi = Btab + (size_t)k * 2 * VT_B, *lo = hi + VT_B;
+  const float v[2][2] = {{c.x, -c.y}, {c.y, c.x}};
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      const float x = v[a][b], h = tc::to_tf32(x), l = tc::to_tf32(x - h);
+      const uint32_t off = kmaj64(2 * s + a, 2 * d + b, VT_NP);
+      *reinterpret_cast<float *>(hi + off) = h;
+      *reinterpret_cast<float *>(lo + off) = l;
+    }
+}
+
+// (P f)_k[v][o] for o < cnt optodes of field f [nf][nn][cnt], FP64
+__device__ inline double2 basis_field(const JArgs &a, int64_t v, int k, int o, const double2 *__restrict__ f, int cnt) {
+  if (!a.prow) return f[((int64_t)k * a.nn + v) * cnt + o];
+  double2 acc = make_double2(0.0, 0.0);
+  const int b = a.prow[v], e = min(a.prow[v + 1], b + PMAX);
+  for (int q = b; q < e; ++q) {
+    const double2 x = f[((int64_t)k * a.nn + a.pcol[q]) * cnt + o];
+    acc.x += a.pval[q] * x.x;
+    acc.y += a.pval[q] * x.y;
+  }
+  return acc;
+}
+
+__global__ void __launch_bounds__(VT_THREADS, 2) k_jacobian_vjp_tc(JArgs a, const unsigned char *__restrict__ Btab,
+                                                                  double *__restrict__ vjp, int *err) {
+  extern __shared__ __align__(1024) unsigned char vt_raw[];
+  __shared__ __align__(8) uint64_t bar_mma;
+  __shared__ uint32_t tmem_slot;
+  __shared__ double part[VT_THREADS];
+  unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(vt_raw) + 1023) & ~uintptr_t(1023));
+  unsigned char *Ahi = sm, *Alo = sm + VT_A, *Bhi = sm + 2 * VT_A, *Blo = Bhi + VT_B;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) {
+    tc::mbar_init(&bar_mma, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) tc::tmem_alloc(&tmem_slot, VT_NP);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = tmem_slot;
+  const int quad = warp & 3, chalf = warp >> 2;    // TMEM lanes 32 quad.., columns 32 chalf.. (sources 16 chalf..)
+  uint32_t phase = 0;
+  bool ok = true;
+  for (int64_t v0 = (int64_t)blockIdx.x * VT_ROWS; v0 < a.nv && ok; v0 += (int64_t)gridDim.x * VT_ROWS) {
+    const int64_t vr = v0 + 32 * quad + lane;      // this thread's voxel row in the epilogue
+    double acc = 0.0;
+    for (int k = 0; k < a.nf && ok; ++k) {
+      // A' = split real embedding of (P phiA)_k for the tile's voxels: element (row, d) -> K' 2d, 2d+1
+      for (int e = tid; e < VT_ROWS * 32; e += VT_THREADS) {
+        const int row = e >> 5, d = e & 31;
+        const int64_t v = v0 + row;
+        double2 x = make_double2(0.0, 0.0);
+        if (v < a.nv && d < a.nd) x = basis_field(a, v, k, d, a.phiA, a.nd);
+        const float xr = (float)x.x, xi = (float)x.y;
+        const float hr = tc::to_tf32(xr), hi_ = tc::to_tf32(xi);
+        const uint32_t off = kmaj64(row, 2 * d, VT_ROWS);
+        *reinterpret_cast<float2 *>(Ahi + off) = make_float2(hr, hi_);
+        *reinterpret_cast<float2 *>(Alo + off) = make_float2(tc::to_tf32(xr - hr), tc::to_tf32(xi - hi_));
+      }
+      // B'_k: a straight copy of its (hi, lo) images
+      {
+        const uint4 *src = reinterpret_cast<const uint4 *>(Btab + (size_t)k * 2 * VT_B);
+        uint4 *dst = reinterpret_cast<uint4 *>(Bhi);
+        for (int e = tid; e < 2 * VT_B / 16; e += VT_THREADS) dst[e] = __ldg(src + e);
+      }
+      tc::fence_async_smem();
+      tc::fence_before_sync();
+      __syncthreads();
+      if (tid == 0) {
+        tc::fence_after_sync();
+        const uint32_t ah = tc::smem_u32(Ahi), al = tc::smem_u32(Alo), bh = tc::smem_u32(Bhi), bl = tc::smem_u32(Blo);
+#pragma unroll
+        for (int kk = 0; kk < VT_KP / 8; ++kk) {       // K = 8 tf32 per MMA; 4 per 128-byte atom
+          const uint32_t oa = (kk >> 2) * VT_ROWS * 128u + 32u * (kk & 3);
+          const uint32_t ob = (kk >> 2) * VT_NP * 128u + 32u * (kk & 3);
+          tc::umma_tf32<VT_IDESC>(tmem, tc::sdesc_k_sw128(ah + oa), tc::sdesc_k_sw128(bh + ob), kk ? 1u : 0u);
+          tc::umma_tf32<VT_IDESC>(tmem, tc::sdesc_k_sw128(ah + oa), tc::sdesc_k_sw128(bl + ob), 1u);
+          tc::umma_tf32<VT_IDESC>(tmem, tc::sdesc_k_sw128(al + oa), tc::sdesc_k_sw128(bh + ob), 1u);
+        }
+        tc::umma_commit(&bar_mma);
+      }
+      bool w = tc::mbar_wait(&bar_mma, phase);
+      phase ^= 1u;
+      if (!w) atomicOr(err, 1);
+      w = __all_sync(0xffffffffu, w);
+      tc::fence_after_sync();
+      if (w) {
+        uint32_t y[32];                                // Y_k[vr][s], s = 16 chalf + i: (re, im) pairs
+        tc::tmem_ld32(tmem + ((uint32_t)(32 * quad) << 16) + 32u * chalf, y);
+        if (vr < a.nv) {
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const int sidx = 16 * chalf + i;
+            if (sidx < a.ns) {
+              const double2 p = basis_field(a, vr, k, sidx, a.phi, a.ns);
+              acc += p.x * (double)__uint_as_float(y[2 * i]) - p.y * (double)__uint_as_float(y[2 * i + 1]);
+            }
+          }
+        }
+      }
+      tc::fence_before_sync();
+      ok = __syncthreads_and(w);                       // operands and accumulator are free again
+    }
+    part[tid] = acc;
+    __syncthreads();
+    if (chalf == 0 && vr < a.nv && ok) vjp[vr] = (a.w ? a.w[vr] : 1.0) * (part[tid] + part[tid + 128]);
+    __syncthreads();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_free(tmem, VT_NP);
+}
+
 // Vector-Jacobian product out[v] = w_v sum_m sum_k Re(Chat[m,k] a_k(m)) for VB voxels per block
 // pass: the fields of VB voxels are staged together, so each Chat[m,k] read from global memory
 // (L2) serves VB voxels.
@@ -275,6 +657,16 @@ int launch_common(JArgs &a, size_t &smem, int &grid) {
 
 }  // namespace
 
+// 0: the time-gated Jacobian on the tensor cores where its shapes fit (else CUDA cores);
+// 1: always the CUDA-core kernel
+static int g_jacobian_engine = 0;
+
+int set_jacobian_engine(int engine) {
+  DGP_REQUIRE(engine == 0 || engine == 1, "jacobian engine must be 0 (tensor cores where they fit) or 1 (CUDA cores)");
+  g_jacobian_engine = engine;
+  return DGP_OK;
+}
+
 int jacobian_run(int mode, const int32_t *prow, const int32_t *pcol, const double *pval, int64_t nv, const double *w,
                  const double *phi, int ns, const double *phiA, int nd, int64_t nn, int nf, const double *fpsf,
                  const int32_t *link, int nm, const double *gate, int ng, int nt, const double *rytov, void *out,
@@ -310,6 +702,23 @@ int jacobian_run(int mode, const int32_t *prow, const int32_t *pcol, const doubl
   DGP_CHECK_LAUNCH();
   if (smem > 48 * 1024)
     DGP_CUDA(cudaFuncSetAttribute(k_jacobian_complex, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const TcLayout tl = tc_layout(nf, ns, nd);
+  const size_t smem_tc = tl.bytes + 1024;
+  if (mode == 0 && g_jacobian_engine == 0 && smem_tc <= 227 * 1024) {
+    // tensor cores: one persistent CTA per SM
+    DevBuf flag;
+    DGP_TRY(flag.alloc(sizeof(int)));
+    DGP_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), st));
+    DGP_CUDA(cudaFuncSetAttribute(k_jacobian_tg_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tc));
+    const int gtc = (int)std::min<int64_t>(nv, (int64_t)sm_count());
+    k_jacobian_tg_tc<<<gtc, TC_THREADS, smem_tc, st>>>(a, ctab.as<float2>(), rytov, (float *)out, flag.as<int>());
+    DGP_CHECK_LAUNCH();
+    int h = 0;
+    DGP_CUDA(cudaMemcpyAsync(&h, flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    DGP_CUDA(cudaStreamSynchronize(st));
+    if (h) return fail(DGP_ERR_CUDA, "jacobian_tg: a tensor-core pipeline wait timed out");
+    return DGP_OK;
+  }
   if (mode == 0) {
     // register-blocked TG kernel: gates padded to 8/16/24/32, MT measurements per thread
     const int ngc = ng <= 8 ? 8 : ng <= 16 ? 16 : ng <= 24 ? 24 : 32;
@@ -348,6 +757,25 @@ int jacobian_run(int mode, const int32_t *prow, const int32_t *pcol, const doubl
     k_chat<<<(unsigned)ceil_div((int64_t)nm * nf, 256), 256, 0, st>>>(gin, ctab.as<float2>(), rytov, nm, ng, nf,
                                                                       chat.as<float2>());
     DGP_CHECK_LAUNCH();
+    if (g_jacobian_engine == 0 && ns <= 32 && nd <= 32 && nm <= 4096) {
+      // tensor cores: per-harmonic complex GEMM over voxel tiles
+      DevBuf btab, flag;
+      DGP_TRY(btab.alloc((size_t)nf * 2 * VT_B));
+      DGP_TRY(flag.alloc(sizeof(int)));
+      DGP_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), st));
+      k_vjp_btab<<<(unsigned)ceil_div((int64_t)nf * 1024, 256), 256, 0, st>>>(chat.as<float2>(), link, nm, nf,
+                                                                              btab.as<unsigned char>());
+      DGP_CHECK_LAUNCH();
+      DGP_CUDA(cudaFuncSetAttribute(k_jacobian_vjp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, VT_SMEM));
+      const int gv = (int)std::min<int64_t>(ceil_div(nv, VT_ROWS), (int64_t)sm_count() * 2);
+      k_jacobian_vjp_tc<<<gv, VT_THREADS, VT_SMEM, st>>>(a, btab.as<unsigned char>(), (double *)out, flag.as<int>());
+      DGP_CHECK_LAUNCH();
+      int h = 0;
+      DGP_CUDA(cudaMemcpyAsync(&h, flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+      DGP_CUDA(cudaStreamSynchronize(st));
+      if (h) return fail(DGP_ERR_CUDA, "jacobian_tg_vjp: a tensor-core pipeline wait timed out");
+      return DGP_OK;
+    }
     // voxels per block pass: as many as 200 KB of staged fields allow, up to 4
     const size_t per = sizeof(float2) * (size_t)nf * (ns + nd);
     const int vb = (int)std::min<size_t>(4, std::max<size_t>(1, (200 * 1024) / per));

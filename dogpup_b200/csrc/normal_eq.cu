@@ -47,6 +47,7 @@
 
 #include "dgp_common.cuh"
 #include "dgp_internal.h"
+#include "tc_common.cuh"
 
 namespace dgp {
 
@@ -56,35 +57,14 @@ constexpr int TM = 128, TN = 128, TK = 64, STAGES = 3;
 constexpr int TILE_BYTES = TM * TK * 2;       // 16 KB: 128 rows x 64 bf16
 constexpr int STAGE_BYTES = 4 * TILE_BYTES;   // A hi, A lo, B hi, B lo
 constexpr int SYRK_SMEM = STAGES * STAGE_BYTES + 1024;  // + alignment slack
-constexpr uint32_t kSpinLimit = 1u << 22;     // bounded mbarrier waits (~0.5 s)
 
-__device__ inline uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ inline void mbar_init(uint64_t *bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ inline void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-
-// bounded wait for the phase with the given parity; false on timeout
-__device__ inline bool mbar_wait(uint64_t *bar, uint32_t parity) {
-  const uint32_t addr = smem_u32(bar);
-  for (uint32_t it = 0; it < kSpinLimit; ++it) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(ok)
-        : "r"(addr), "r"(parity)
-        : "memory");
-    if (ok) return true;
-    if (it > 256) __nanosleep(100);
-  }
-  return false;
-}
+using tc::mbar_expect_tx;
+using tc::mbar_init;
+using tc::mbar_wait;
+using tc::sdesc_k_sw128;
+using tc::smem_u32;
+using tc::tmem_ld32;
+using tc::umma_commit;
 
 __device__ inline void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y) {
   asm volatile(
@@ -94,47 +74,11 @@ __device__ inline void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *
       : "memory");
 }
 
-// UMMA shared-memory descriptor: K-major operand, 128-byte swizzle, rows of
-// 128 B grouped by 8 (stride 1024 B), sm100 descriptor version 1.
-__device__ inline uint64_t sdesc_k_sw128(uint32_t saddr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t)1 << 16;             // leading byte offset (unused for swizzled K-major)
-  d |= (uint64_t)(1024 >> 4) << 32;   // stride byte offset
-  d |= (uint64_t)1 << 46;             // descriptor version
-  d |= (uint64_t)2 << 61;             // SWIZZLE_128B
-  return d;
-}
-
 // instruction descriptor, kind::f16: BF16 x BF16 -> F32, both K-major, M=128, N=128
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) |
-                            ((uint32_t)(TM >> 4) << 24);
+constexpr uint32_t kIdesc = tc::idesc(1, 1, TM, TN);
 
 __device__ inline void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accum) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
-      "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accum)
-      : "memory");
-}
-
-__device__ inline void umma_commit(uint64_t *bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-               : "memory");
-}
-
-__device__ inline void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+  tc::umma_bf16<kIdesc>(d_tmem, adesc, bdesc, accum);
 }
 
 __global__ void __launch_bounds__(128, 1) k_syrk_tc(const __grid_constant__ CUtensorMap map_hi,

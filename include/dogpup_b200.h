@@ -426,7 +426,14 @@ int dgp_jacobian_complex(const int32_t *d_P_rowptr, const int32_t *d_P_col,
 /* J_tg[v][g][m] float32 = Nt 2 Re sum_k conj(gate_fc[g][k]) J~[m][k][v]
  * (J~_0 = J_0/2), divided by d_data_tg[m][g] when that is not NULL (Rytov
  * normalisation).  1 <= ng <= 32.  Row v of the output is row v of J^T
- * with measurement index g*nm + m. */
+ * with measurement index g*nm + m.  The DFT over harmonics runs on the
+ * tensor cores (tcgen05, TF32 operands split in two so that three products
+ * keep FP32 accuracy) when nf * (ns + nd) * 8 bytes of staged fields and the
+ * gate table fit one block's shared memory, else on the CUDA cores
+ * (dgp_set_jacobian_engine). */
+/* Engine of dgp_jacobian_tg: 0 (default) the tensor cores where the shapes
+ * fit, 1 always the CUDA-core kernel (cross-checks, timing).  Process-wide. */
+int dgp_set_jacobian_engine(int32_t engine);
 int dgp_jacobian_tg(const int32_t *d_P_rowptr, const int32_t *d_P_col,
                     const double *d_P_val, int64_t nv, const double *d_w,
                     const double *d_phi, int32_t ns, const double *d_phiA,
