@@ -79,6 +79,7 @@ _SIGS = {
     "dgp_fc2tg": (C.c_int, [P, I64, I32, P, I32, I32, P, P]),
     "dgp_csr_spmv": (C.c_int, [P, P, P, I64, I64, P, P, P]),
     "dgp_set_jacobian_engine": (C.c_int, [I32]),
+    "dgp_times_jt": (C.c_int, [P, I64, I64, P, I64, P, P]),
     "dgp_tg_adjoint_rhs": (C.c_int, [P, P, I32, P, I32, P, I32, I32, P, I64, I32, I32, P, P]),
     "dgp_locate_points": (C.c_int, [P, P, I64, I64, P, I64, D, P, P, P]),
     "dgp_grid_to_mesh": (C.c_int, [P, I64, P, P, P, P, P, P, P]),

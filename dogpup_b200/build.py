@@ -67,7 +67,7 @@ def build_library(verbose: bool = False, jobs: int | None = None) -> Path:
         return LIB
     tmp = LIB.with_suffix(".so.tmp")
     cuda_lib = Path(nvcc()).resolve().parent.parent / "lib64"
-    cmd = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", *map(str, objs), f"-L{cuda_lib}", "-lcublas",
+    cmd = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", *map(str, objs), f"-L{cuda_lib}",
            "-Xlinker", "-rpath", "-Xlinker", str(cuda_lib), "-o", str(tmp)]
     if verbose:
         print(" ".join(cmd), flush=True)

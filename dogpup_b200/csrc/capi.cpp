@@ -92,6 +92,7 @@ int jacobian_run(int mode, const int32_t *prow, const int32_t *pcol, const doubl
 int normal_eq_run(const float *Jt, int64_t nv, int64_t nm, const double *W, const double *y, double lam, int mode,
                   double *H, int64_t ldh, double *rhs, cudaStream_t st);
 int cholesky_solve_run(double *H, int64_t n, int64_t ldh, double *x, cudaStream_t st);
+int times_jt_run(const double *A, int64_t na, int64_t nv, const float *Jt, int64_t nm, double *out, cudaStream_t st);
 int row_dots_run(const float *Jt, int64_t nv, int64_t nm, const double *W, const double *y, double *diag, double *rhs,
                  cudaStream_t st);
 int lm_update_run(const float *Jt, int64_t nv, int64_t nm, const double *W, const double *y, double lam, double *x,
@@ -494,6 +495,11 @@ int dgp_snap_to_surface(const double *d_node, int64_t nn, const int32_t *d_bnd, 
 int dgp_normal_eq(const float *d_Jt, int64_t nv, int64_t nmeas, const double *d_w, const double *d_y, double lambda,
                   int32_t damping, double *d_H, int64_t ldh, double *d_rhs, dgp_stream_t stream) {
   DGP_GUARD(normal_eq_run(d_Jt, nv, nmeas, d_w, d_y, lambda, damping, d_H, ldh, d_rhs, (cudaStream_t)stream));
+}
+
+int dgp_times_jt(const double *d_A, int64_t na, int64_t nv, const float *d_Jt, int64_t nmeas, double *d_out,
+                 dgp_stream_t stream) {
+  DGP_GUARD(times_jt_run(d_A, na, nv, d_Jt, nmeas, d_out, (cudaStream_t)stream));
 }
 
 int dgp_cholesky_solve(double *d_H, int64_t n, int64_t ldh, double *d_x, dgp_stream_t stream) {

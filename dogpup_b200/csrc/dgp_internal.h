@@ -159,4 +159,10 @@ int spmm_A_f64(const int32_t *rowptr, const int32_t *col, const double2 *KM, con
 int fsai_apply_f64(const int32_t *rowptr, const int32_t *col, const double2 *G, int64_t n, int64_t nnzG,
                    int32_t nf, int32_t ns, const double2 *X, double2 *Y, cudaStream_t st);
 
+// FP64 Cholesky H = L L^T (lower triangle of the row-major H, overwritten by L) and the solve of
+// L L^T x = b for one (cholesky_solve_run) or nrhs right-hand sides stored as the rows of x
+int cholesky_solve_run(double *H, int64_t n, int64_t ldh, double *x, cudaStream_t st);
+int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_t nrhs, int64_t ldx,
+                            cudaStream_t st);
+
 }  // namespace dgp

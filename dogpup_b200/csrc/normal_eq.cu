@@ -9,13 +9,7 @@
 //   H_ii += lam * max_j (J'WJ)_jj      (or lam * (J'WJ)_ii), FP64 exact diagonal
 //   r = J' W y                         FP64
 //   H = L L', solve L L' x = r         FP64 blocked Cholesky + triangular solves
-//
-// Cholesky: right-looking over 256-column block steps.  Inside the 256 x 256
-// diagonal block, 64-column steps: this file's one-warp factor of the 64 x 64
-// diagonal, then DTRSM / DSYRK for the rest of the block; below the block the
-// panel is a cuBLAS DTRSM and the trailing update a cuBLAS DSYRK (plain
-// BLAS-3, where n^3/3 of the flops are); the two triangular solves are cuBLAS
-// DTRSV.
+//                                      (cholesky.cu: FP64 tensor-core GEMMs, no BLAS)
 //
 // Input J is given transposed, Jt [nv][nmeas] float32 row-major -- the layout
 // the TG Jacobian kernel writes -- so both GEMM operands are K-major.
@@ -36,8 +30,6 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
-
-#include <cublas_v2.h>
 
 #include <algorithm>
 #include <cmath>
@@ -250,45 +242,6 @@ __global__ void k_damp(double *H, int64_t ldh, const double *__restrict__ diag, 
     H[i * ldh + i] = diag[i] + lam * (mode == 0 ? smax : mode == 1 ? diag[i] : 1.0);
 }
 
-// ------------------------------------------------------- FP64 Cholesky
-constexpr int NB = 64;
-// outer block width: the trailing DSYRK is rank-NBO (n = 22,971: 225.6 / 217.9 / 214.2 ms for
-// 256 / 512 / 1024)
-#ifndef DGP_CHOL_NBO
-#define DGP_CHOL_NBO 1024
-#endif
-
-// Factors the nb x nb (nb <= 64) diagonal block at k0 in place, one warp,
-// right-looking in shared memory: each column is scaled by 1/sqrt(pivot) and
-// every lane updates the rows it owns (rows j+1+lane, j+33+lane) -- only warp
-// barriers between columns.  A non-positive or non-finite pivot sets err bit 8.
-__global__ void __launch_bounds__(32) k_potrf_diag(double *H, int64_t ldh, int64_t k0, int nb, int *err) {
-  __shared__ double A[NB][NB + 1];
-  const int lane = threadIdx.x;
-  for (int i = 0; i < nb; ++i)
-    for (int j = lane; j <= i; j += 32) A[i][j] = H[(k0 + i) * ldh + k0 + j];
-  __syncwarp();
-  for (int j = 0; j < nb; ++j) {
-    double d = A[j][j];
-    if (!(d > 0.0) || !isfinite(d)) {
-      d = 1.0;
-      if (lane == 0) atomicOr(err, 8);
-    }
-    const double sd = sqrt(d), inv = 1.0 / sd;
-    __syncwarp();
-    if (lane == 0) A[j][j] = sd;
-    for (int i = j + 1 + lane; i < nb; i += 32) A[i][j] *= inv;
-    __syncwarp();
-    for (int i = j + 1 + lane; i < nb; i += 32) {
-      const double aij = A[i][j];
-      for (int l = j + 1; l <= i; ++l) A[i][l] -= aij * A[l][j];
-    }
-    __syncwarp();
-  }
-  for (int i = 0; i < nb; ++i)
-    for (int j = lane; j <= i; j += 32) H[(k0 + i) * ldh + k0 + j] = A[i][j];
-}
-
 PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   static std::once_flag once;
@@ -367,97 +320,6 @@ int normal_eq_run(const float *Jt, int64_t nv, int64_t nm, const double *W, cons
   return DGP_OK;
 }
 
-// one cuBLAS handle per device, created on first use and kept for the process
-cublasHandle_t blas_handle(std::unique_lock<std::mutex> &lk) {
-  static std::mutex mu;
-  static std::map<int, cublasHandle_t> handles;
-  lk = std::unique_lock<std::mutex>(mu);
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
-  auto it = handles.find(dev);
-  if (it != handles.end()) return it->second;
-  cublasHandle_t h = nullptr;
-  if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) return nullptr;
-  handles[dev] = h;
-  return h;
-}
-
-int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_t nrhs, int64_t ldx,
-                            cudaStream_t st);
-
-int cholesky_solve_run(double *H, int64_t n, int64_t ldh, double *x, cudaStream_t st) {
-  return cholesky_solve_many_run(H, n, ldh, x, 1, n, st);
-}
-
-int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_t nrhs, int64_t ldx,
-                            cudaStream_t st) {
-  DGP_REQUIRE(H && x && n > 0 && ldh >= n, "cholesky: bad arguments");
-  DGP_REQUIRE(nrhs >= 1 && ldx >= n, "cholesky: need nrhs >= 1 and ldx >= n");
-  DGP_REQUIRE(n <= INT32_MAX && ldh <= INT32_MAX && ldx <= INT32_MAX, "cholesky: n, ldh and ldx must fit int32 (cuBLAS)");
-  DevBuf errb;
-  DGP_TRY(errb.alloc(sizeof(int)));
-  DGP_CUDA(cudaMemsetAsync(errb.p, 0, sizeof(int), st));
-  constexpr int64_t NBO = DGP_CHOL_NBO;  // outer block step: DTRSM panel + DSYRK trailing update
-  std::unique_lock<std::mutex> lk;
-  cublasHandle_t hb = blas_handle(lk);
-  if (!hb) return fail(DGP_ERR_CUDA, "cholesky: cuBLAS handle creation failed");
-  if (cublasSetStream(hb, st) != CUBLAS_STATUS_SUCCESS) return fail(DGP_ERR_CUDA, "cholesky: cublasSetStream failed");
-  const double one = 1.0, minus_one = -1.0;
-  for (int64_t k0 = 0; k0 < n; k0 += NBO) {
-    const int64_t kend = std::min(n, k0 + NBO);
-    // factor the diagonal block [k0, kend) in 64-column steps: warp factor of the 64 x 64
-    // diagonal, then DTRSM / DSYRK for the rest of the block (same column-major view as below)
-    for (int64_t j0 = k0; j0 < kend; j0 += NB) {
-      const int64_t jb = std::min<int64_t>(NB, kend - j0), jend = j0 + jb, jr = kend - jend;
-      k_potrf_diag<<<1, 32, 0, st>>>(H, ldh, j0, (int)jb, errb.as<int>());
-      count_launches(1);
-      if (jr <= 0) continue;
-      if (cublasDtrsm(hb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, (int)jb,
-                      (int)jr, &one, H + j0 * ldh + j0, (int)ldh, H + jend * ldh + j0,
-                      (int)ldh) != CUBLAS_STATUS_SUCCESS ||
-          cublasDsyrk(hb, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, (int)jr, (int)jb, &minus_one, H + jend * ldh + j0,
-                      (int)ldh, &one, H + jend * ldh + jend, (int)ldh) != CUBLAS_STATUS_SUCCESS)
-        return fail(DGP_ERR_CUDA, "cholesky: cuBLAS call in the diagonal block failed");
-    }
-    DGP_CHECK_LAUNCH();
-    const int64_t rest = n - kend, nb = kend - k0;
-    if (rest <= 0) break;
-    // Column-major view of the row-major lower triangle: Hc = H^T (upper), leading dimension ldh.
-    // Panel rows [kend, n) x cols [k0, kend):  P <- P L^-T   <=>  Pc <- (Lc^T)^-1 Pc
-    if (cublasDtrsm(hb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, (int)nb,
-                    (int)rest, &one, H + k0 * ldh + k0, (int)ldh, H + kend * ldh + k0,
-                    (int)ldh) != CUBLAS_STATUS_SUCCESS)
-      return fail(DGP_ERR_CUDA, "cholesky: cublasDtrsm failed");
-    // Trailing lower triangle: H[i][l] -= sum_j P[i][j] P[l][j]  <=>  upper(Cc) -= Pc^T Pc
-    if (cublasDsyrk(hb, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, (int)rest, (int)nb, &minus_one, H + kend * ldh + k0,
-                    (int)ldh, &one, H + kend * ldh + kend, (int)ldh) != CUBLAS_STATUS_SUCCESS)
-      return fail(DGP_ERR_CUDA, "cholesky: cublasDsyrk failed");
-  }
-  DGP_CHECK_LAUNCH();
-  // L y = b, then L^T x = y on the column-major view Hc = L^T (upper): DTRSV for one right-hand
-  // side, DTRSM for several (right-hand side r is row r of x, i.e. column r of the n x nrhs
-  // column-major view with leading dimension ldx)
-  if (nrhs == 1) {
-    if (cublasDtrsv(hb, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, (int)n, H, (int)ldh, x, 1) !=
-            CUBLAS_STATUS_SUCCESS ||
-        cublasDtrsv(hb, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, (int)n, H, (int)ldh, x, 1) !=
-            CUBLAS_STATUS_SUCCESS)
-      return fail(DGP_ERR_CUDA, "cholesky: cublasDtrsv failed");
-  } else {
-    if (cublasDtrsm(hb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, (int)n, nrhs,
-                    &one, H, (int)ldh, x, (int)ldx) != CUBLAS_STATUS_SUCCESS ||
-        cublasDtrsm(hb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, (int)n, nrhs,
-                    &one, H, (int)ldh, x, (int)ldx) != CUBLAS_STATUS_SUCCESS)
-      return fail(DGP_ERR_CUDA, "cholesky: cublasDtrsm (solve) failed");
-  }
-  lk.unlock();
-  int herr = 0;
-  DGP_CUDA(cudaMemcpyAsync(&herr, errb.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-  DGP_CUDA(cudaStreamSynchronize(st));
-  if (herr) return fail(DGP_ERR_ARG, "cholesky: matrix is not positive definite");
-  return DGP_OK;
-}
-
 // ----------------------------------------------------- tik_inv update
 namespace {
 
@@ -484,6 +346,47 @@ __global__ void k_scale_sqrtw(const double *in, const double *__restrict__ W, in
 }
 
 }  // namespace
+
+namespace {
+// out[a][m] = sum_v A[a][v] Jt[v][m]: thread m of block (x, y) accumulates spots 8y .. 8y+7 in
+// FP64; the A columns of a 256-voxel chunk are staged in shared memory, Jt is read once per
+// 8 spots with consecutive threads on consecutive m (coalesced)
+__global__ void __launch_bounds__(256) k_times_jt(const double *__restrict__ A, int64_t na, int64_t nv,
+                                                  const float *__restrict__ Jt, int64_t nm, double *__restrict__ out) {
+  __shared__ double As[8][256];
+  const int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t a0 = (int64_t)blockIdx.y * 8;
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int64_t v0 = 0; v0 < nv; v0 += 256) {
+    __syncthreads();
+    for (int q = 0; q < 8; ++q) {
+      const int64_t v = v0 + threadIdx.x;
+      As[q][threadIdx.x] = (a0 + q < na && v < nv) ? A[(a0 + q) * nv + v] : 0.0;
+    }
+    __syncthreads();
+    if (m < nm) {
+      const int64_t vend = min(nv - v0, (int64_t)256);
+      for (int64_t j = 0; j < vend; ++j) {
+        const double x = (double)Jt[(v0 + j) * nm + m];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) acc[q] += As[q][j] * x;
+      }
+    }
+  }
+  if (m < nm)
+    for (int q = 0; q < 8; ++q)
+      if (a0 + q < na) out[(a0 + q) * nm + m] = acc[q];
+}
+}  // namespace
+
+int times_jt_run(const double *A, int64_t na, int64_t nv, const float *Jt, int64_t nm, double *out, cudaStream_t st) {
+  DGP_REQUIRE(A && Jt && out && na > 0 && nv > 0 && nm > 0, "times_jt: bad arguments");
+  DGP_REQUIRE(ceil_div(na, 8) <= 65535, "times_jt: too many rows in A");
+  dim3 grid((unsigned)ceil_div(nm, 256), (unsigned)ceil_div(na, 8));
+  k_times_jt<<<grid, 256, 0, st>>>(A, na, nv, Jt, nm, out);
+  DGP_CHECK_LAUNCH();
+  return DGP_OK;
+}
 
 int row_dots_run(const float *Jt, int64_t nv, int64_t nm, const double *W, const double *y, double *diag, double *rhs,
                  cudaStream_t st) {

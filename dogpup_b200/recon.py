@@ -18,8 +18,8 @@ Data weighting: with target spots (``pos_s``) the rows of J and y are
 mixed by reshape_J's dense w (wghtd_LM_recon.m:35-37, :72-76;
 reconstruction/reshape_J.m:13-15; dMesh.m:250-282), computed on the device:
 J J^T + lam2 max diag by the split-BF16 tensor-core kernel (dgp_normal_eq on
-J), Js J^T by cuBLAS SGEMM, and w by one FP64 Cholesky factorisation with
-one right-hand side per spot (dgp_cholesky_solve_many).  Without spots the
+J), Js J^T by dgp_times_jt (FP64 accumulation), and w by one FP64 Cholesky
+factorisation with one right-hand side per spot (dgp_cholesky_solve_many).  Without spots the
 rows are weighted by a diagonal W = 1/sigma^2 or by 1.
 """
 from __future__ import annotations
@@ -80,16 +80,20 @@ def reshape_J(Jt: torch.Tensor, Js: torch.Tensor, lam: float, normal_eq="split_b
     """w [NS][NM] = (Js J^T)(J J^T + lam max diag I)^-1 (reconstruction/reshape_J.m:13-15).
 
     Jt [NV][NM] is J transposed (the TG Jacobian's layout), Js [NS][NV] the spots on the
-    same voxels.  J J^T: split-BF16 tensor cores (or FP64 for normal_eq='fp64'); the
-    solve: FP64 Cholesky with one right-hand side per spot."""
+    same voxels.  J J^T: split-BF16 tensor cores (or FP64 for normal_eq='fp64', the all-FP64
+    cross-check mode, with torch matrix products); the solve: FP64 Cholesky with one
+    right-hand side per spot."""
     nv, nm = Jt.shape
     ns = Js.shape[0]
     A = torch.empty((nm, nm), dtype=torch.float64, device="cuda")
     v = lambda t: C.c_void_p(t.data_ptr())
     if normal_eq == "split_bf16":
-        J = Jt.to(torch.float32).t().contiguous()                        # [NM][NV]: rows of J
+        Jf = Jt.to(torch.float32).contiguous()
+        J = Jf.t().contiguous()                                           # [NM][NV]: rows of J
         check(lib.dgp_normal_eq(v(J), nm, nv, None, None, float(lam), 0, v(A), nm, None, api.stream_ptr()))
-        B = (Js.to(torch.float32) @ Jt.to(torch.float32)).to(torch.float64).contiguous()
+        Jsd = Js.to(torch.float64).contiguous()
+        B = torch.empty((ns, nm), dtype=torch.float64, device="cuda")
+        check(lib.dgp_times_jt(v(Jsd), ns, nv, v(Jf), nm, v(B), api.stream_ptr()))     # Js J^T
     else:
         Jd = Jt.to(torch.float64)
         A.copy_(Jd.T @ Jd)

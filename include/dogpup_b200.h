@@ -512,6 +512,13 @@ enum { DGP_DAMP_MAX_DIAG = 0, DGP_DAMP_DIAG = 1, DGP_DAMP_ADD = 2 };
 int dgp_normal_eq(const float *d_Jt, int64_t nv, int64_t nmeas, const double *d_w,
                   const double *d_y, double lambda, int32_t damping, double *d_H,
                   int64_t ldh, double *d_rhs, dgp_stream_t stream);
+/* out[a][m] = sum_v A[a][v] Jt[v][m] (FP64 accumulation): A [na][nv] f64,
+ * Jt [nv][nmeas] f32 (J transposed, the TG Jacobian's layout), out [na][nmeas]
+ * f64.  The spots-times-J^T product of reshape_J (reconstruction/reshape_J.m:
+ * 15, Js*J'). */
+int dgp_times_jt(const double *d_A, int64_t na, int64_t nv, const float *d_Jt,
+                 int64_t nmeas, double *d_out, dgp_stream_t stream);
+
 /* Solves H x = b in place (d_x: b in, x out) by an FP64 Cholesky
  * factorisation of the lower triangle of d_H (overwritten by L).
  * Returns DGP_ERR_ARG if H is not positive definite. */

@@ -48,9 +48,12 @@ def test_normal_equations_match_fp64(nv, nm):
     assert np.linalg.norm(rhs.cpu().numpy() - r0) / np.linalg.norm(r0) < 1e-12
 
 
-@pytest.mark.parametrize("n,pad", [(333, 0), (1100, 7)])
+@pytest.mark.parametrize("n,pad", [(333, 0), (1100, 7), (2501, 3), (128, 0), (129, 1)])
 def test_cholesky_solve_exact_matrix(n, pad):
-    """n > 256 crosses the 256-column block steps (DTRSM panel + DSYRK update); pad > 0 tests ldh > n."""
+    """n > 128 crosses the 128-column panels (diagonal factor + inverse, panel GEMM, trailing
+    lower-triangle GEMM on the FP64 tensor cores) with a partial last panel; pad > 0 tests
+    ldh > n (an odd ldh takes the 8-byte copy path of the GEMM); the strict upper triangle holds
+    NaN and must never be read.  Solution 1e-10 against NumPy, L L^T 1e-13."""
     import torch
     from dogpup_b200._lib import lib, check
     rng = np.random.default_rng(3)
@@ -161,3 +164,20 @@ def test_lm_update_rejects_bad_weights_in_both_forms():
         for form in (1, 2):
             x = torch.zeros(nv, dtype=torch.float64, device="cuda")
             assert lib.dgp_lm_update(_v(Jt), nv, nm, _v(Wd), _v(yd), 1e-2, _v(x), form, None, None) == 1, (bad, form)
+
+
+@pytest.mark.parametrize("na,nv,nm", [(1, 5, 3), (6, 1000, 777), (13, 2049, 300)])
+def test_times_jt_against_numpy(na, nv, nm):
+    """dgp_times_jt (the Js J^T product of reshape_J): FP64 accumulation of an FP64 left factor
+    and the FP32 Jacobian, against NumPy in FP64 on the same FP32 values, 1e-12; spot counts
+    that are not multiples of its 8-row groups and voxel counts across its 256-voxel chunks."""
+    import torch
+    from dogpup_b200._lib import lib, check
+    rng = np.random.default_rng(na + nv)
+    A = rng.standard_normal((na, nv))
+    Jt = rng.standard_normal((nv, nm)).astype(np.float32)
+    out = torch.empty((na, nm), dtype=torch.float64, device="cuda")
+    Ad, Jd = torch.as_tensor(A, device="cuda"), torch.as_tensor(Jt, device="cuda")
+    check(lib.dgp_times_jt(_v(Ad), na, nv, _v(Jd), nm, _v(out), None))
+    ref = A @ Jt.astype(np.float64)
+    assert np.abs(out.cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
