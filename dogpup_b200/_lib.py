@@ -63,6 +63,7 @@ _SIGS = {
     "dgp_solver_autotune": (C.c_int, [P, C.POINTER(I32), C.POINTER(I32), C.POINTER(I32), C.POINTER(C.c_float), P]),
     "dgp_solver_set_spmm": (C.c_int, [P, I32, I32, I32]),
     "dgp_solver_set_spmm_kind": (C.c_int, [P, I32]),
+    "dgp_solver_set_device_loop": (C.c_int, [P, I32]),
     "dgp_solver_spmm_shape": (C.c_int, [P, C.POINTER(I32), C.POINTER(I32), C.POINTER(I32), C.POINTER(I32)]),
     "dgp_solver_check_spmm": (C.c_int, [P, C.POINTER(D), P]),
     "dgp_solve": (C.c_int, [P, P, P, I32, C.POINTER(SolveOpts), C.POINTER(SolveReport), P]),

@@ -133,6 +133,10 @@ class Solver:
     def set_spmm(self, tiled: bool, vec: int = 0, rows: int = 0):
         check(lib.dgp_solver_set_spmm(self._h, int(tiled), int(vec), int(rows)))
 
+    def set_device_loop(self, on: bool):
+        """True (default): one graph launch per inner solve (device-driven WHILE loop); False: host polling."""
+        check(lib.dgp_solver_set_device_loop(self._h, int(bool(on))))
+
     def set_spmm_kind(self, kind: int):
         """Inner loop of the gather SpMM: 0 one nonzero per step, 1 two, 2 four, 3 four with packed FMAs."""
         check(lib.dgp_solver_set_spmm_kind(self._h, int(kind)))

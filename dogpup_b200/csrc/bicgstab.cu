@@ -66,6 +66,10 @@ struct Ctl {
   double max_err;
   int n_active;
   int reason;  // 0 tol reached, 1 maxit, 2 nothing to solve
+  // stall guard of the device-driven loop: best max_err seen and checks since it halved
+  double stall_ref;
+  int stall_since;
+  int loops;   // blocks of iterations the device-driven loop ran
 };
 
 struct Cols {
@@ -1248,6 +1252,9 @@ __global__ void __launch_bounds__(1024) k_stage_init(Cols c, Ctl *ctl, int nsp, 
   if (threadIdx.x == 0) {
     ctl->n_active = a;
     ctl->iters = 0;
+    ctl->stall_ref = 0.0;
+    ctl->stall_since = 0;
+    ctl->loops = 0;
     ctl->max_err = a ? 1.0 : 0.0;
     ctl->state = a ? ST_RUNNING : ST_DONE;
     ctl->reason = a ? 1 : 2;
@@ -1905,12 +1912,93 @@ int enqueue_vec(SolverPlan *S, const Vecs<R> &V, const Work &W, cudaStream_t st,
   }
 }
 
+// End of one block of iterations in the device-driven loop: keep looping while the control block
+// is not DONE, the iteration count is below maxit + one block (the iteration kernels stop at
+// maxit themselves; this bound ends the loop even if they did not), and -- with the stall guard
+// of the mixed path's inner solves -- the largest residual of the active columns halved within
+// the last `patience` blocks.
+__global__ void k_loop_cond(cudaGraphConditionalHandle h, Ctl *ctl, int stall_guard, int patience, int block) {
+  if (threadIdx.x != 0) return;
+  int cont = ctl->state != ST_DONE;
+  ctl->loops += 1;
+  if (cont && ctl->iters >= ctl->maxit + block) cont = 0;
+  if (cont && ctl->loops > ctl->maxit + 2) cont = 0;  // blocks run without counting iterations
+  if (cont && stall_guard) {
+    const double e = ctl->max_err;
+    if (ctl->stall_ref == 0.0 || e < 0.5 * ctl->stall_ref) {
+      ctl->stall_ref = e;
+      ctl->stall_since = 0;
+    } else if (++ctl->stall_since >= patience) {
+      cont = 0;
+    }
+  }
+  cudaGraphSetConditional(h, cont ? 1u : 0u);
+}
+
+// Device-driven form of run_iterations: ONE graph launch whose WHILE node replays blocks of
+// check_every iterations until k_loop_cond clears the condition; the host waits once for the
+// control block.
+template <class R>
+int run_iterations_device(SolverPlan *S, const Vecs<R> &V, const Work &W, int check_every, cudaStream_t st,
+                          int *iters_out, bool stall_guard, bool cocg) {
+  const int gi = 3 + (sizeof(R) == 4 ? (cocg ? 2 : 1) : 0);
+  const int per_iter = cocg ? KERNELS_PER_ITER_COCG : KERNELS_PER_ITER;
+  const int patience = std::max(3, 40 / check_every);
+  if (!S->graph[gi] || S->graph_iters[gi] != check_every) {
+    if (S->graph[gi]) {
+      cudaGraphExecDestroy(S->graph[gi]);
+      S->graph[gi] = nullptr;
+    }
+    cudaGraph_t g;
+    DGP_CUDA(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle h;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, nullptr, 0, &p);
+    if (e != cudaSuccess) {
+      cudaGraphDestroy(g);
+      return cuda_fail(e, "solver: conditional graph node", __FILE__, __LINE__);
+    }
+    cudaGraph_t body = p.conditional.phGraph_out[0];
+    cudaStream_t cs;
+    DGP_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    int rc = DGP_OK;
+    if (e == cudaSuccess) {
+      for (int q = 0; q < check_every && rc == DGP_OK; ++q)
+        rc = enqueue_vec<R>(S, V, W, cs, cocg ? ENQ_COCG : ENQ_BICGSTAB);
+      k_loop_cond<<<1, 32, 0, cs>>>(h, W.ctl, stall_guard ? 1 : 0, patience, check_every);
+      cudaGraph_t out = nullptr;
+      e = cudaStreamEndCapture(cs, &out);
+    }
+    cudaStreamDestroy(cs);
+    if (rc == DGP_OK && e == cudaSuccess) e = cudaGraphInstantiate(&S->graph[gi], g, 0);
+    cudaGraphDestroy(g);
+    if (rc != DGP_OK) return rc;
+    DGP_CUDA(e);
+    S->graph_iters[gi] = check_every;
+  }
+  Ctl *hb = (Ctl *)S->h_ctl;
+  DGP_CUDA(cudaGraphLaunch(S->graph[gi], st));
+  DGP_CUDA(cudaMemcpyAsync(hb, W.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+  DGP_CUDA(cudaStreamSynchronize(st));
+  count_launches((int64_t)hb->loops * (per_iter * check_every + 1));
+  *iters_out = hb->iters;
+  return DGP_OK;
+}
+
 template <class R>
 int run_iterations(SolverPlan *S, const Vecs<R> &V, const Work &W, int check_every, int maxit, cudaStream_t st,
                    int *iters_out, bool stall_guard = false, bool cocg = false) {
   const int gi = sizeof(R) == 4 ? (cocg ? 2 : 1) : 0;
   const int per_iter = cocg ? KERNELS_PER_ITER_COCG : KERNELS_PER_ITER;
   if (check_every < 1) check_every = 1;
+  if (S->device_loop) return run_iterations_device<R>(S, V, W, check_every, st, iters_out, stall_guard, cocg);
   if (!S->graph[gi] || S->graph_iters[gi] != check_every) {
     if (S->graph[gi]) {
       cudaGraphExecDestroy(S->graph[gi]);
@@ -2572,6 +2660,12 @@ int solver_set_spmm_kind(SolverPlan *S, int32_t kind) {
       g = nullptr;
     }
   for (int &gi : S->graph_iters) gi = 0;
+  return DGP_OK;
+}
+
+int solver_set_device_loop(SolverPlan *S, int32_t on) {
+  DGP_REQUIRE(on == 0 || on == 1, "set_device_loop: 0 (host polling) or 1 (device-driven loop)");
+  S->device_loop = on;
   return DGP_OK;
 }
 

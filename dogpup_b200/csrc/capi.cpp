@@ -338,6 +338,11 @@ int dgp_solver_set_spmm_kind(dgp_solver_t s, int32_t kind) {
   DGP_GUARD(solver_set_spmm_kind(&s->plan, kind));
 }
 
+int dgp_solver_set_device_loop(dgp_solver_t s, int32_t on) {
+  if (!s) return fail(DGP_ERR_ARG, "solver_set_device_loop: null handle");
+  DGP_GUARD(solver_set_device_loop(&s->plan, on));
+}
+
 int dgp_solver_spmm_shape(dgp_solver_t s, int32_t *tiled, int32_t *vec, int32_t *rows, int32_t *kind) {
   if (!s) return fail(DGP_ERR_ARG, "solver_spmm_shape: null handle");
   if (tiled) *tiled = s->plan.tiled;

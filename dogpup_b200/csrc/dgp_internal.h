@@ -95,8 +95,11 @@ struct SolverPlan {
   DevBuf status;                 // per-column status
   void *h_ctl = nullptr;         // pinned mirrors of the control block (two)
   cudaEvent_t poll_ev[2] = {nullptr, nullptr};  // the two mirrors' copy-done events
-  cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};  // FP64 BiCGSTAB, FP32 BiCGSTAB, FP32 COCG
-  int graph_iters[3] = {0, 0, 0};
+  // blocks of iterations captured as graphs -- [0..2]: FP64 BiCGSTAB, FP32 BiCGSTAB, FP32 COCG
+  // (replayed and polled by the host); [3..5]: the same inside a device-driven WHILE loop
+  cudaGraphExec_t graph[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  int graph_iters[6] = {0, 0, 0, 0, 0, 0};
+  int32_t device_loop = 1;       // 1: an inner solve is one graph launch (WHILE node), 0: host polling
   // SpMM launch shape of the complex-FP32 sweeps chosen by solver_autotune (0 = built-in default)
   int32_t tune_vec = 0, tune_rows = 0;
   int32_t tune_kind = 0;  // gather SpMM inner loop: 0 one nonzero per step, 1 two, 2 four, 3 four + packed FMAs
@@ -128,6 +131,7 @@ int solver_autotune(SolverPlan *S, int32_t *tiled, int32_t *vec, int32_t *rows, 
 // sets the SpMM kind / shape explicitly (tiled 0: gather kernel with vec, rows; 1: tiled)
 int solver_set_spmm(SolverPlan *S, int32_t tiled, int32_t vec, int32_t rows);
 int solver_set_spmm_kind(SolverPlan *S, int32_t kind);
+int solver_set_device_loop(SolverPlan *S, int32_t on);
 int solver_set_dot_rows(SolverPlan *S, int32_t mult);
 // largest relative difference between the tiled and the gather SpMM on the plan's operators
 int solver_check_spmm(SolverPlan *S, double *max_rel, cudaStream_t st);

@@ -270,6 +270,13 @@ int dgp_solver_set_spmm(dgp_solver_t solver, int32_t tiled, int32_t vec,
  * complex product).  dgp_solver_autotune searches the kinds with the lane widths and
  * block heights; dgp_solver_spmm_shape reports the plan's current choice. */
 int dgp_solver_set_spmm_kind(dgp_solver_t solver, int32_t kind);
+/* How a solve runs its iterations.  1 (default): each inner solve is ONE
+ * graph launch -- a CUDA-graph WHILE node replays blocks of check_every
+ * iterations and a device kernel ends the loop on convergence, at maxit, or
+ * (mixed precision's inner solves) when the largest residual has stopped
+ * halving; the host waits once per inner solve.  0: the host replays the
+ * block graph and polls the control block between blocks. */
+int dgp_solver_set_device_loop(dgp_solver_t solver, int32_t on);
 int dgp_solver_spmm_shape(dgp_solver_t solver, int32_t *tiled, int32_t *vec,
                           int32_t *rows, int32_t *kind);
 /* Rows per block of the complex-FP32 SpMM sweeps that also reduce a dot

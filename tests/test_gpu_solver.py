@@ -349,6 +349,44 @@ def test_solver_autotune_then_mixed_accuracy(small_case, gpu_case, torch):
     assert err.max() < 1e-6, err.max()
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "mixed_bicgstab"])
+def test_device_driven_loop_matches_host_polling(small_case, gpu_case, torch, precision):
+    """One graph launch per inner solve (WHILE node, the loop ended on the device) against the
+    host replaying blocks of iterations and polling the control block: the FP64 solve is the same
+    computation (same iteration count, bit-identical fields); the mixed solves may stop their
+    inner solves one block apart (the stall guard is checked at block ends on the device), so
+    both must meet the 1e-6 fluence bar against the sparse-direct solution."""
+    from dogpup_b200 import api
+    from oracle import solver as osv
+    K0, M0 = small_case["K"], small_case["M"]
+    nf, ns = 4, 6
+    dfc = 2 * np.pi / 10e-9 / (C_VAC / 1.4)
+    nodes, w = _point_sources(small_case, ns, 23)
+    fpsf = np.exp(-0.1j * np.arange(nf))
+    fem = gpu_case["fem"]
+    out = {}
+    for loop in (True, False):
+        S = api.Solver(fem.rowptr, fem.col, gpu_case["K"], gpu_case["M"], dfc, nf, ns)
+        S.set_device_loop(loop)
+        X, rep = S.solve_sources(torch.as_tensor(nodes, device="cuda"), torch.as_tensor(w, device="cuda"),
+                                 torch.as_tensor(fpsf, device="cuda"),
+                                 api.make_opts(tol=1e-10, precision=precision, check_every=4))
+        out[loop] = (X.cpu().numpy(), rep.iterations, rep.max_rel_residual)
+        del S
+    if precision == "fp64":
+        assert out[True][1] == out[False][1]
+        assert np.array_equal(out[True][0], out[False][0])
+    Q = np.zeros((K0.shape[0], ns, nf), complex)
+    for s_ in range(ns):
+        Q[nodes[s_], s_, :] = w[s_][:, None] * fpsf[None, :]
+    xd = osv.direct_solve(K0, M0, dfc, Q)
+    for loop in (True, False):
+        x = np.transpose(out[loop][0], (1, 2, 0))
+        err = np.linalg.norm(x - xd, axis=0) / np.linalg.norm(xd, axis=0)
+        assert err.max() < 1e-6, (loop, err.max())
+        assert out[loop][2] < 1e-10
+
+
 @pytest.mark.parametrize("kind", [1, 2, 3])
 @pytest.mark.parametrize("ns,vec", [(3, 2), (16, 4), (40, 8), (64, 4)])
 def test_gather_spmm_kinds_solve_to_the_bar(small_case, gpu_case, torch, kind, ns, vec):

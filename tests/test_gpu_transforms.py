@@ -127,10 +127,10 @@ def test_source_spectrum_of_the_optode_constructor():
     tpsf = gaussian_pulse(t)
     for nf, avg in ((32, 1e3), (7, 2.5)):
         o = DOptode(np.zeros((1, 3)), np.zeros((1, 3)), [[0, 0]], avg, tpsf, t, nf)
-        fAxis = np.arange(nf) * 2 * np.pi / t[-1]
-        assert np.array_equal(o.fAxis, fAxis) and o.df == fAxis[1] - fAxis[0]
+        fAxis = np.arange(nf) * (2 * np.pi / t[-1])                  # (0:Nf-1) .* w0, w0 = 2 pi / T
+        assert np.allclose(o.fAxis, fAxis, rtol=1e-15, atol=0) and abs(o.df - (fAxis[1] - fAxis[0])) <= 1e-15 * o.df
         scaled = tpsf * (avg / tpsf.mean())
         assert np.abs(o.s_tpsf - scaled).max() <= 1e-15 * np.abs(scaled).max()
-        ref = td2fc(scaled[None, :], fAxis, t)[0]
+        ref = td2fc(scaled[None, :], o.fAxis, t)[0]
         assert _rel(o.s_fpsf.cpu().numpy(), ref) < TOL
         assert abs(ref[0].real - avg * t[1] * len(t) / t[-1]) < 1e-9 * avg   # c_0 = dt/T sum = avgPow * Nt dt / T
