@@ -265,7 +265,7 @@ def plain_fp64_small_bench(tol=1e-10, truth_tol=1e-13):
     return out
 
 
-def tg_jacobian_bench(reps=3, tols=(1e-8, 1e-10, 1e-12), truth_tol=1e-13):
+def tg_jacobian_bench(reps=3, tols=(1e-10, 1e-12, 1e-13, 1e-14), truth_tol=1e-14):
     """Sensitivity configuration: ellipsoid at 100k nodes, 32 sources x 32 detectors, 64 harmonics,
     20 gates of 250 ps, nodal basis (J^T is [nodes][20 x 1024] FP32).
 
@@ -294,8 +294,8 @@ def tg_jacobian_bench(reps=3, tols=(1e-8, 1e-10, 1e-12), truth_tol=1e-13):
     ns, nd = len(w["src"]), len(w["det"])
 
     # FP64 truth for every source and detector
-    phi0, data0 = mesh.flu_solve(precision="fp64", tol=truth_tol)
-    phiA0 = mesh.adj_flu_solve(precision="fp64", tol=truth_tol)
+    phi0, data0, rep0 = mesh.flu_solve(precision="fp64", tol=truth_tol, maxit=3000, return_report=True)
+    phiA0, repA0 = mesh.adj_flu_solve(precision="fp64", tol=truth_tol, maxit=3000, return_report=True)
     tg0 = api.fc2tg(data0, gfc, nt)
     J0 = api.jacobian_tg(nb, phi0, phiA0, fpsf, link, gfc, nt)
     del phi0, phiA0
@@ -309,12 +309,21 @@ def tg_jacobian_bench(reps=3, tols=(1e-8, 1e-10, 1e-12), truth_tol=1e-13):
         return float(e_d), float(e_t), float(e_j)
 
     sweep, phi, phiA = {}, None, None
+    # the reference's own arithmetic and tolerance (FP64 BiCGSTAB, max-over-columns stop at 1e-12)
+    # against the same truth: the accuracy a link of the reference's output has
+    phi64, data64 = mesh.flu_solve(precision="fp64", tol=1e-12)
+    phiA64 = mesh.adj_flu_solve(precision="fp64", tol=1e-12)
+    J64 = api.jacobian_tg(nb, phi64, phiA64, fpsf, link, gfc, nt)
+    e_d, e_t, e_j = link_errors(data64, J64)
+    sweep["fp64 1e-12"] = {"detector_data_per_link_max": e_d, "tg_data_per_link_max": e_t,
+                           "tg_jacobian_per_link_max": e_j}
+    del phi64, phiA64, J64
     for tol in tols:
         mesh.flu_solve(precision="mixed", tol=tol)                # warm-up (graphs, workspace)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        phi, data = mesh.flu_solve(precision="mixed", tol=tol)
-        phiA = mesh.adj_flu_solve(precision="mixed", tol=tol)
+        phi, data, rf = mesh.flu_solve(precision="mixed", tol=tol, return_report=True)
+        phiA, ra = mesh.adj_flu_solve(precision="mixed", tol=tol, return_report=True)
         torch.cuda.synchronize()
         t_solve = time.perf_counter() - t0
         out = {}
@@ -325,10 +334,12 @@ def tg_jacobian_bench(reps=3, tols=(1e-8, 1e-10, 1e-12), truth_tol=1e-13):
                              "batched_s": round(t_solve + ms * 1e-3, 3),
                              "detector_data_per_link_max": e_d, "tg_data_per_link_max": e_t,
                              "tg_jacobian_per_link_max": e_j,
+                             "max_rel_residual": max(rf.max_rel_residual, ra.max_rel_residual),
+                             "iterations_refinements": [[rf.iterations, rf.refinements], [ra.iterations, ra.refinements]],
                              "meets_bar": bool(e_d <= 1e-6 and e_j <= 1e-5)}
         log(f"[rank 0] sensitivity at tol {tol:g}: {sweep[f'{tol:g}']}")
     del J0
-    ok = [k for k in sweep if sweep[k]["meets_bar"]]
+    ok = [k for k in sweep if sweep[k].get("meets_bar")]
     pick = min(ok, key=lambda k: sweep[k]["batched_s"]) if ok else f"{tols[-1]:g}"
 
     # kernel timings on the last (tightest) fields
@@ -337,6 +348,14 @@ def tg_jacobian_bench(reps=3, tols=(1e-8, 1e-10, 1e-12), truth_tol=1e-13):
     del out
     g = torch.as_tensor(np.random.default_rng(5).standard_normal((nm, 20)), device="cuda")
     ms_vjp = _event_ms(lambda: api.jacobian_tg_vjp(nb, phi, phiA, fpsf, link, gfc, nt, g), reps)
+    # the same two kernels with the CUDA-core engine (dgp_set_jacobian_engine(1))
+    from dogpup_b200._lib import lib as _dl
+    _dl.dgp_set_jacobian_engine(1)
+    out = {}
+    ms_cc = _event_ms(lambda: out.__setitem__("J", api.jacobian_tg(nb, phi, phiA, fpsf, link, gfc, nt)), reps)
+    del out
+    ms_vjp_cc = _event_ms(lambda: api.jacobian_tg_vjp(nb, phi, phiA, fpsf, link, gfc, nt, g), reps)
+    _dl.dgp_set_jacobian_engine(0)
     field_bytes = 16.0 * nf * nv * (ns + nd)
     j_bytes = 4.0 * nv * 20 * nm
     flops = 2.0 * nv * nm * nf * (2 + 2 * 20)
@@ -361,10 +380,12 @@ def tg_jacobian_bench(reps=3, tols=(1e-8, 1e-10, 1e-12), truth_tol=1e-13):
     mesh._solver = None
     return {"workload": f"ellipsoid 90x75x70 @1.38mm, {nv} nodes, 32x32 optodes, 64 harmonics, 20 gates",
             "J_shape": [20 * nm, nv], "ms": round(ms, 3), "vjp_ms": round(ms_vjp, 3),
+            "cuda_core_engine": {"ms": round(ms_cc, 3), "vjp_ms": round(ms_vjp_cc, 3)},
             "achieved_gbs": round((field_bytes + j_bytes) / (ms * 1e-3) / 1e9, 1),
             "achieved_tflops_fp32": round(flops / (ms * 1e-3) / 1e12, 2),
-            "mixed_vs_fp64": {"truth": f"FP64 fields to {truth_tol:g}, all {ns} sources and {nd} detectors, "
-                                       f"all {nm} links", "by_tol": sweep},
+            "mixed_vs_fp64": {"truth": f"FP64 fields to {truth_tol:g} (reached {max(rep0.max_rel_residual, repA0.max_rel_residual):.2e}), "
+                                       f"all {ns} sources and {nd} detectors, all {nm} links", "by_tol": sweep,
+                              "bar": "detector data 1e-6 and TG Jacobian 1e-5 per link"},
             "headline": {"tol": float(pick), "batched_mixed_forward_adjoint_tgJ_s": batched_s,
                          "plain_fp64_per_rhs_s": round(plain_s, 3),
                          "plain_fp64_per_rhs_solves_per_s": round(plain["value"], 2),
