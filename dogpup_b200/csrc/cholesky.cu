@@ -41,6 +41,8 @@ constexpr int LDK = GK + 4;      // padded shared-memory row (doubles)
 constexpr int GSTAGES = 4;
 constexpr int GTHREADS = 256;
 constexpr int GEMM_SMEM = GSTAGES * 2 * CB * LDK * (int)sizeof(double);   // 160 KB
+static_assert(GEMM_SMEM >= CB * (CB + 1) * (int)sizeof(double), "the epilogue tile must fit the stage ring");
+constexpr int GV = 256;          // k per CTA of the solves' off-diagonal partial sums
 
 __device__ inline uint32_t su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -152,21 +154,30 @@ __global__ void __launch_bounds__(GTHREADS, 1) k_dgemm_nt(Gemm g) {
     }
   }
   cp_wait<0>();
-  __syncthreads();   // every CTA's A rows are in registers / consumed before any C write (in-place panel)
-  // epilogue: C = beta C + alpha acc
+  __syncthreads();   // the stage ring is free: the epilogue goes through shared memory
+  // epilogue: the accumulators are written to shared memory (a 128 x 129-double tile), then the
+  // CTA reads and writes C row by row, coalesced, with every load of C in flight together
+  // (C = beta C + alpha acc; in diagonal tiles of the lower mode only entries c <= r)
+  double *T = gsm;
+  constexpr int TLD = CB + 1;
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j)
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const int64_t r = r0 + wm * 64 + i * 16 + gid + (q >> 1) * 8;
-        const int64_t c = c0 + wn * 32 + j * 8 + 2 * tig + (q & 1);
-        if (r < g.M && c < g.N && (!g.lower || ti != tj || c <= r)) {
-          double *p = g.C + r * g.ldc + c;
-          *p = (g.beta == 0.0 ? 0.0 : g.beta * *p) + g.alpha * acc[i][j][q];
-        }
+        const int r = wm * 64 + i * 16 + gid + (q >> 1) * 8, c = wn * 32 + j * 8 + 2 * tig + (q & 1);
+        T[r * TLD + c] = acc[i][j][q];
       }
+  __syncthreads();
+  const int64_t rows = min((int64_t)CB, g.M - r0), cols = min((int64_t)CB, g.N - c0);
+  for (int e = tid; e < CB * CB; e += GTHREADS) {
+    const int r = e / CB, c = e % CB;
+    if (r < rows && c < cols && (!g.lower || ti != tj || c <= r)) {
+      double *p = g.C + (r0 + r) * g.ldc + c0 + c;
+      *p = (g.beta == 0.0 ? 0.0 : g.beta * *p) + g.alpha * T[r * TLD + c];
+    }
+  }
 }
 
 // Factor the nb x nb diagonal block at (k0, k0) in place (lower) and write inv(L) (row-major,
@@ -240,28 +251,35 @@ __global__ void __launch_bounds__(128) k_potrf_tile(double *__restrict__ H, int6
     const int r = e / nb, c = e % nb;
     if (c <= r) H[(k0 + r) * ldh + k0 + c] = L[r * PLD + c];
   }
-  // inv(L): thread c solves L x = e_c (x_i = 0 for i < c), written to column c of Linv
+  // inv(L) in shared memory: thread c solves L x = e_c (x_i = 0 for i < c) and keeps x_i, i > c,
+  // in row c of the strict upper triangle (L itself is lower) and x_c in dinv[c]
+  __shared__ double dinv[PT];
   for (int c = tid; c < nb; c += blockDim.x) {
-    double *col = Linv + c;                          // column c, stride nb
-    for (int i = 0; i < c; ++i) col[(int64_t)i * nb] = 0.0;
-    for (int i = c; i < nb; ++i) {
-      double s = i == c ? 1.0 : 0.0;
-      for (int l = c; l < i; ++l) s -= L[i * PLD + l] * col[(int64_t)l * nb];
-      col[(int64_t)i * nb] = s / L[i * PLD + i];
+    const double xc = 1.0 / L[c * PLD + c];
+    dinv[c] = xc;
+    for (int i = c + 1; i < nb; ++i) {
+      double s = L[i * PLD + c] * xc;
+      for (int l = c + 1; l < i; ++l) s += L[i * PLD + l] * L[c * PLD + l];
+      L[c * PLD + i] = -s / L[i * PLD + i];
     }
+  }
+  __syncthreads();
+  for (int e = tid; e < nb * nb; e += blockDim.x) {
+    const int i = e / nb, c = e % nb;
+    Linv[e] = i < c ? 0.0 : (i == c ? dinv[c] : L[c * PLD + i]);
   }
 }
 
 // ---------------------------------------------------------------- solves
 // forward:  acc[r][i] += sum_{k in [kb, ke)} H[base + i][k] X[r][k]     (L_bc y_c)
 // backward: acc[r][i] += sum_{k in [kb, ke)} H[k][base + i] X[r][k]     (L_cb^T x_c)
-// blockIdx.y = right-hand side r, blockIdx.x = a chunk of 1024 k; partial sums reduced by warp
+// blockIdx.y = right-hand side r, blockIdx.x = a chunk of GV k; partial sums reduced by warp
 // shuffles (forward) or per thread (backward), then FP64 atomics.  X is row-major [nrhs][ldx].
 template <bool TRANS>
 __global__ void k_block_gemv(const double *__restrict__ H, int64_t ldh, int64_t base, int nbi, int64_t kb,
                              int64_t ke, const double *__restrict__ X, int64_t ldx, double *acc) {
   const int r = blockIdx.y;
-  const int64_t k_lo = kb + (int64_t)blockIdx.x * 1024, k_hi = min(ke, k_lo + 1024);
+  const int64_t k_lo = kb + (int64_t)blockIdx.x * GV, k_hi = min(ke, k_lo + GV);
   if (k_lo >= k_hi) return;
   const double *x = X + (int64_t)r * ldx;
   if (!TRANS) {
@@ -364,7 +382,7 @@ int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_
     const int64_t k0 = b * CB;
     const int nb = (int)std::min<int64_t>(CB, n - k0);
     if (k0 > 0) {
-      dim3 gr((unsigned)ceil_div(k0, 1024), (unsigned)nrhs);
+      dim3 gr((unsigned)ceil_div(k0, GV), (unsigned)nrhs);
       k_block_gemv<false><<<gr, 128, 0, st>>>(H, ldh, k0, nb, 0, k0, x, ldx, acc.as<double>());
       ++launches;
     }
@@ -376,7 +394,7 @@ int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_
     const int nb = (int)std::min<int64_t>(CB, n - k0);
     const int64_t kend = k0 + nb;
     if (kend < n) {
-      dim3 gr((unsigned)ceil_div(n - kend, 1024), (unsigned)nrhs);
+      dim3 gr((unsigned)ceil_div(n - kend, GV), (unsigned)nrhs);
       k_block_gemv<true><<<gr, 128, 0, st>>>(H, ldh, k0, nb, kend, n, x, ldx, acc.as<double>());
       ++launches;
     }
