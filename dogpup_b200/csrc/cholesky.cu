@@ -5,15 +5,18 @@
 // symmetric positive definite, i.e. a Cholesky factorisation and two triangular solves).
 //
 // H is row-major [n][ldh]; its lower triangle is read and overwritten by L (H = L L^T); the
-// strict upper triangle is not touched.  Right-looking, 128-column panels:
+// strict upper triangle is not touched.  Right-looking, 512-column outer panels of 128-column
+// steps:
 //
-//   for each panel k (columns [k0, k0 + 128)):
+//   for each step k (columns [k0, k0 + 128)) of the outer panel [o0, o0 + 512):
 //     k_potrf_tile   the 128 x 128 diagonal block: L_kk in place, and inv(L_kk) into a scratch
 //                    table (one CTA, block in shared memory: 32-column steps, a warp factors the
-//                    32 x 32 diagonal, all warps solve and update the rest)
+//                    32 x 32 diagonal, all warps solve and update the rest; the inverse by
+//                    32-blocks)
 //     k_dgemm_nt     panel: L_ik = A_ik inv(L_kk)^T for the rows below (in place: a CTA owns
 //                    whole 128-row strips of the panel)
-//     k_dgemm_nt     trailing update: A_il -= L_ik L_lk^T on the lower-triangle tiles
+//     k_dgemm_nt     update of the outer panel's remaining columns: A_il -= L_ik L_lk^T
+//   k_dgemm_nt       trailing update of the rest, depth 512: A_il -= sum over the outer panel
 //
 // k_dgemm_nt: C = beta C + alpha A B^T with A, B row-major (K contiguous); 128 x 128 CTA tiles,
 // 256 threads (8 warps of 64 x 32), K in stages of 16 doubles moved by cp.async through a
@@ -43,6 +46,7 @@ constexpr int GTHREADS = 256;
 constexpr int GEMM_SMEM = GSTAGES * 2 * CB * LDK * (int)sizeof(double);   // 160 KB
 static_assert(GEMM_SMEM >= CB * (CB + 1) * (int)sizeof(double), "the epilogue tile must fit the stage ring");
 constexpr int GV = 256;          // k per CTA of the solves' off-diagonal partial sums
+constexpr int64_t NBO = 512;     // outer panel width: depth of the trailing update GEMM
 
 __device__ inline uint32_t su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -171,11 +175,22 @@ __global__ void __launch_bounds__(GTHREADS, 1) k_dgemm_nt(Gemm g) {
       }
   __syncthreads();
   const int64_t rows = min((int64_t)CB, g.M - r0), cols = min((int64_t)CB, g.N - c0);
-  for (int e = tid; e < CB * CB; e += GTHREADS) {
-    const int r = e / CB, c = e % CB;
-    if (r < rows && c < cols && (!g.lower || ti != tj || c <= r)) {
-      double *p = g.C + (r0 + r) * g.ldc + c0 + c;
-      *p = (g.beta == 0.0 ? 0.0 : g.beta * *p) + g.alpha * T[r * TLD + c];
+  // batches of 16 entries per thread: all 16 loads of C are issued before any store (a store to
+  // C between loads would otherwise keep the compiler from overlapping their latencies)
+  constexpr int BATCH = 16;
+  for (int e0 = tid; e0 < CB * CB; e0 += GTHREADS * BATCH) {
+    double cv[BATCH];
+    bool in[BATCH];
+#pragma unroll
+    for (int u = 0; u < BATCH; ++u) {
+      const int e = e0 + u * GTHREADS, r = e / CB, c = e % CB;
+      in[u] = e < CB * CB && r < rows && c < cols && (!g.lower || ti != tj || c <= r);
+      cv[u] = (in[u] && g.beta != 0.0) ? g.C[(r0 + r) * g.ldc + c0 + c] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < BATCH; ++u) {
+      const int e = e0 + u * GTHREADS, r = e / CB, c = e % CB;
+      if (in[u]) g.C[(r0 + r) * g.ldc + c0 + c] = g.beta * cv[u] + g.alpha * T[r * TLD + c];
     }
   }
 }
@@ -187,9 +202,10 @@ __global__ void __launch_bounds__(GTHREADS, 1) k_dgemm_nt(Gemm g) {
 // panel below and the trailing lower triangle is updated.  err |= 1 on a non-positive or
 // non-finite pivot.
 constexpr int PT = 128, PLD = 129;
+constexpr size_t POT_SMEM = sizeof(double) * ((size_t)PT * PLD + 3 * 32 * 33);
 __global__ void __launch_bounds__(128) k_potrf_tile(double *__restrict__ H, int64_t ldh, int64_t k0, int nb,
                                                    double *__restrict__ Linv, int *err) {
-  extern __shared__ double L[];                      // [PT][PLD]
+  extern __shared__ double L[];                      // [PT][PLD], then the [3][32][33] level products
   __shared__ int bad;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) bad = 0;
@@ -251,56 +267,90 @@ __global__ void __launch_bounds__(128) k_potrf_tile(double *__restrict__ H, int6
     const int r = e / nb, c = e % nb;
     if (c <= r) H[(k0 + r) * ldh + k0 + c] = L[r * PLD + c];
   }
-  // inv(L) in shared memory: thread c solves L x = e_c (x_i = 0 for i < c) and keeps x_i, i > c,
-  // in row c of the strict upper triangle (L itself is lower) and x_c in dinv[c]
+  // inv(L) = X, blocked by 32 (entries X[i][c], i > c, kept in the strict upper triangle of the
+  // shared tile at [c][i]; X[c][c] = 1 / L[c][c] in dinv):
+  //   1. the diagonal 32-blocks: warp w, lane l solves column c = 32 w + l of inv(L_ww)
+  //   2. the off-diagonal blocks by distance d = I - J = 1, 2, 3 below the diagonal:
+  //      T = sum_{K = J .. I-1} L_IK X_KJ, then X_IJ = -X_II T
   __shared__ double dinv[PT];
-  for (int c = tid; c < nb; c += blockDim.x) {
-    const double xc = 1.0 / L[c * PLD + c];
-    dinv[c] = xc;
-    for (int i = c + 1; i < nb; ++i) {
-      double s = L[i * PLD + c] * xc;
-      for (int l = c + 1; l < i; ++l) s += L[i * PLD + l] * L[c * PLD + l];
-      L[c * PLD + i] = -s / L[i * PLD + i];
+  for (int c = tid; c < nb; c += blockDim.x) dinv[c] = 1.0 / L[c * PLD + c];
+  __syncthreads();
+  auto X = [&](int k, int c) -> double { return k < c ? 0.0 : (k == c ? dinv[c] : L[c * PLD + k]); };
+  {
+    const int c = 32 * warp + lane;
+    if (c < nb) {
+      const int iend = min(32 * (warp + 1), nb);
+      for (int i = c + 1; i < iend; ++i) {
+        double t = L[i * PLD + c] * dinv[c];
+        for (int l = c + 1; l < i; ++l) t += L[i * PLD + l] * L[c * PLD + l];
+        L[c * PLD + i] = -t * dinv[i];
+      }
     }
   }
   __syncthreads();
+  double *Tb = L + PT * PLD;                          // [3][32][33] products of one level
+  for (int d = 1; d < 4; ++d) {
+    const int nblk = 4 - d;
+    for (int e = tid; e < nblk * 1024; e += blockDim.x) {
+      const int J = e / 1024, I = J + d, i = 32 * I + (e % 1024) / 32, c = 32 * J + e % 32;
+      double t = 0.0;
+      if (i < nb && c < nb)
+        for (int k = 32 * J; k < 32 * I; ++k) t += L[i * PLD + k] * X(k, c);
+      Tb[(J * 32 + (e % 1024) / 32) * 33 + e % 32] = t;
+    }
+    __syncthreads();
+    for (int e = tid; e < nblk * 1024; e += blockDim.x) {
+      const int J = e / 1024, I = J + d, i = 32 * I + (e % 1024) / 32, c = 32 * J + e % 32;
+      if (i >= nb || c >= nb) continue;
+      double x = 0.0;
+      for (int m = 32 * I; m <= i; ++m) x += X(i, m) * Tb[(J * 32 + m - 32 * I) * 33 + e % 32];
+      L[c * PLD + i] = -x;
+    }
+    __syncthreads();
+  }
   for (int e = tid; e < nb * nb; e += blockDim.x) {
     const int i = e / nb, c = e % nb;
-    Linv[e] = i < c ? 0.0 : (i == c ? dinv[c] : L[c * PLD + i]);
+    Linv[e] = X(i, c);
   }
 }
 
 // ---------------------------------------------------------------- solves
 // forward:  acc[r][i] += sum_{k in [kb, ke)} H[base + i][k] X[r][k]     (L_bc y_c)
+//   block (x, y, z): k chunk x of GV, rows 8y .. 8y + 7 (one warp each), right-hand side z;
+//   lanes stride k, warp shuffle, one FP64 atomic per (row, chunk)
 // backward: acc[r][i] += sum_{k in [kb, ke)} H[k][base + i] X[r][k]     (L_cb^T x_c)
-// blockIdx.y = right-hand side r, blockIdx.x = a chunk of GV k; partial sums reduced by warp
-// shuffles (forward) or per thread (backward), then FP64 atomics.  X is row-major [nrhs][ldx].
+//   block (x, -, z): rows k of chunk x (GVB of them), thread i = column i (consecutive threads
+//   read consecutive columns of a row), one FP64 atomic per (column, chunk)
+// X is row-major [nrhs][ldx].
+constexpr int GVB = 32;
 template <bool TRANS>
 __global__ void k_block_gemv(const double *__restrict__ H, int64_t ldh, int64_t base, int nbi, int64_t kb,
                              int64_t ke, const double *__restrict__ X, int64_t ldx, double *acc) {
-  const int r = blockIdx.y;
-  const int64_t k_lo = kb + (int64_t)blockIdx.x * GV, k_hi = min(ke, k_lo + GV);
-  if (k_lo >= k_hi) return;
+  const int r = blockIdx.z;
   const double *x = X + (int64_t)r * ldx;
   if (!TRANS) {
-    for (int i = threadIdx.x >> 5; i < nbi; i += blockDim.x >> 5) {
-      const double *row = H + (base + i) * ldh;
-      double s = 0.0;
-      for (int64_t k = k_lo + (threadIdx.x & 31); k < k_hi; k += 32) s += row[k] * x[k];
-      for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-      if ((threadIdx.x & 31) == 0) atomicAdd(acc + (int64_t)r * CB + i, s);
-    }
+    const int64_t k_lo = kb + (int64_t)blockIdx.x * GV, k_hi = min(ke, k_lo + GV);
+    const int i = blockIdx.y * 8 + (threadIdx.x >> 5);
+    if (i >= nbi || k_lo >= k_hi) return;
+    const double *row = H + (base + i) * ldh;
+    double s = 0.0;
+    for (int64_t k = k_lo + (threadIdx.x & 31); k < k_hi; k += 32) s += row[k] * x[k];
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if ((threadIdx.x & 31) == 0) atomicAdd(acc + (int64_t)r * CB + i, s);
   } else {
-    for (int i = threadIdx.x; i < nbi; i += blockDim.x) {
-      double s = 0.0;
-      for (int64_t k = k_lo; k < k_hi; ++k) s += H[k * ldh + base + i] * x[k];
-      atomicAdd(acc + (int64_t)r * CB + i, s);
-    }
+    const int64_t k_lo = kb + (int64_t)blockIdx.x * GVB, k_hi = min(ke, k_lo + GVB);
+    const int i = threadIdx.x;
+    if (i >= nbi || k_lo >= k_hi) return;
+    double s = 0.0;
+#pragma unroll 8
+    for (int64_t k = k_lo; k < k_hi; ++k) s += H[k * ldh + base + i] * x[k];
+    atomicAdd(acc + (int64_t)r * CB + i, s);
   }
 }
 
 // X[r][base + i] = sum_j Linv'[i][j] (X[r][base + j] - acc[r][j]), Linv' = inv(L_bb) (forward) or
-// its transpose (backward); acc is cleared for the next block.
+// its transpose (backward); one warp per output entry (lanes stride j, coalesced along rows of
+// Linv for the forward product); acc is cleared for the next block.
 template <bool TRANS>
 __global__ void k_block_diag(const double *__restrict__ Linv, int nbi, int64_t base, double *X, int64_t ldx,
                              double *acc) {
@@ -309,15 +359,19 @@ __global__ void k_block_diag(const double *__restrict__ Linv, int nbi, int64_t b
   double *x = X + (int64_t)r * ldx + base;
   for (int j = threadIdx.x; j < nbi; j += blockDim.x) rhs[j] = x[j] - acc[(int64_t)r * CB + j];
   __syncthreads();
-  for (int i = threadIdx.x; i < nbi; i += blockDim.x) {
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int i = threadIdx.x >> 5; i < nbi; i += nw) {
     double s = 0.0;
     if (!TRANS) {
-      for (int j = 0; j <= i; ++j) s += Linv[(int64_t)i * nbi + j] * rhs[j];
+      for (int j = lane; j <= i; j += 32) s += Linv[(int64_t)i * nbi + j] * rhs[j];
     } else {
-      for (int j = i; j < nbi; ++j) s += Linv[(int64_t)j * nbi + i] * rhs[j];
+      for (int j = i + lane; j < nbi; j += 32) s += Linv[(int64_t)j * nbi + i] * rhs[j];
     }
-    x[i] = s;
-    acc[(int64_t)r * CB + i] = 0.0;
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (lane == 0) {
+      x[i] = s;
+      acc[(int64_t)r * CB + i] = 0.0;
+    }
   }
 }
 
@@ -348,6 +402,7 @@ int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_
   DGP_REQUIRE(H && x && n > 0 && ldh >= n, "cholesky: bad arguments");
   DGP_REQUIRE(nrhs >= 1 && ldx >= n, "cholesky: need nrhs >= 1 and ldx >= n");
   DGP_REQUIRE(nrhs <= 65535, "cholesky: at most 65535 right-hand sides");
+  DGP_REQUIRE(ceil_div(n, (int64_t)GVB) <= INT32_MAX, "cholesky: n too large for the solve grid");
   const int64_t nblk = ceil_div(n, CB);
   DevBuf linv, errb, acc;
   DGP_TRY(linv.alloc(sizeof(double) * (size_t)nblk * CB * CB));
@@ -355,38 +410,63 @@ int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_
   DGP_TRY(acc.alloc(sizeof(double) * (size_t)CB * nrhs));
   DGP_CUDA(cudaMemsetAsync(errb.p, 0, sizeof(int), st));
   DGP_CUDA(cudaMemsetAsync(acc.p, 0, sizeof(double) * (size_t)CB * nrhs, st));
-  const size_t pot_smem = sizeof(double) * PT * PLD;
+  const size_t pot_smem = POT_SMEM;
   DGP_CUDA(cudaFuncSetAttribute(k_potrf_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pot_smem));
   double *Li = linv.as<double>();
   int64_t launches = 0;
-  for (int64_t b = 0; b < nblk; ++b) {
-    const int64_t k0 = b * CB;
-    const int nb = (int)std::min<int64_t>(CB, n - k0);
-    double *Lb = Li + b * CB * CB;
-    k_potrf_tile<<<1, 128, pot_smem, st>>>(H, ldh, k0, nb, Lb, errb.as<int>());
-    DGP_CHECK_LAUNCH();
-    ++launches;
-    const int64_t kend = k0 + nb, rest = n - kend;
-    if (rest <= 0) break;
-    // panel: rows [kend, n) x cols [k0, kend) <- panel inv(L_kk)^T  (in place, one CTA per row strip)
-    Gemm p{H + kend * ldh + k0, ldh, Lb, nb, H + kend * ldh + k0, ldh, rest, nb, nb, 1.0, 0.0, 0, 0};
-    DGP_TRY(gemm_nt(p, st));
-    // trailing lower triangle: rows/cols [kend, n) -= panel panel^T
-    Gemm t{H + kend * ldh + k0, ldh, H + kend * ldh + k0, ldh, H + kend * ldh + kend, ldh, rest, rest, nb,
-           -1.0, 1.0, 1, 0};
+  // 512-column outer panels: inside one, 128-column steps update only the outer panel's own
+  // columns (the rows below included); the rest of the matrix takes the outer panel's update in
+  // one lower-triangle GEMM of depth 512
+  for (int64_t o0 = 0; o0 < n; o0 += NBO) {
+    const int64_t oend = std::min(n, o0 + NBO);
+    bool last = false;
+    for (int64_t k0 = o0; k0 < oend; k0 += CB) {
+      const int64_t b = k0 / CB;
+      const int nb = (int)std::min<int64_t>(CB, n - k0);
+      double *Lb = Li + b * CB * CB;
+      k_potrf_tile<<<1, 128, pot_smem, st>>>(H, ldh, k0, nb, Lb, errb.as<int>());
+      DGP_CHECK_LAUNCH();
+      ++launches;
+      const int64_t kend = k0 + nb, rest = n - kend;
+      if (rest <= 0) {
+        last = true;
+        break;
+      }
+      // L_ik = A_ik inv(L_kk)^T for every row below (in place, one CTA per 128-row strip)
+      const Gemm p{H + kend * ldh + k0, ldh, Lb, nb, H + kend * ldh + k0, ldh, rest, nb, nb, 1.0, 0.0, 0, 0};
+      DGP_TRY(gemm_nt(p, st));
+      ++launches;
+      const int64_t w = oend - kend;  // the outer panel's remaining columns
+      if (w > 0) {
+        const Gemm a{H + kend * ldh + k0, ldh, H + kend * ldh + k0, ldh, H + kend * ldh + kend, ldh, w, w, nb,
+                     -1.0, 1.0, 1, 0};
+        DGP_TRY(gemm_nt(a, st));
+        ++launches;
+        if (n > oend) {
+          const Gemm r{H + oend * ldh + k0, ldh, H + kend * ldh + k0, ldh, H + oend * ldh + kend, ldh, n - oend, w,
+                       nb, -1.0, 1.0, 0, 0};
+          DGP_TRY(gemm_nt(r, st));
+          ++launches;
+        }
+      }
+    }
+    if (last || n <= oend) break;
+    // trailing lower triangle: rows/cols [oend, n) -= Q Q^T, Q = rows [oend, n) x cols [o0, oend)
+    const Gemm t{H + oend * ldh + o0, ldh, H + oend * ldh + o0, ldh, H + oend * ldh + oend, ldh, n - oend, n - oend,
+                 oend - o0, -1.0, 1.0, 1, 0};
     DGP_TRY(gemm_nt(t, st));
-    launches += 2;
+    ++launches;
   }
   // L y = b, then L^T x = y, by 128-row blocks
   for (int64_t b = 0; b < nblk; ++b) {
     const int64_t k0 = b * CB;
     const int nb = (int)std::min<int64_t>(CB, n - k0);
     if (k0 > 0) {
-      dim3 gr((unsigned)ceil_div(k0, GV), (unsigned)nrhs);
-      k_block_gemv<false><<<gr, 128, 0, st>>>(H, ldh, k0, nb, 0, k0, x, ldx, acc.as<double>());
+      dim3 gr((unsigned)ceil_div(k0, GV), (unsigned)ceil_div(nb, 8), (unsigned)nrhs);
+      k_block_gemv<false><<<gr, 256, 0, st>>>(H, ldh, k0, nb, 0, k0, x, ldx, acc.as<double>());
       ++launches;
     }
-    k_block_diag<false><<<(unsigned)nrhs, 128, 0, st>>>(Li + b * CB * CB, nb, k0, x, ldx, acc.as<double>());
+    k_block_diag<false><<<(unsigned)nrhs, 256, 0, st>>>(Li + b * CB * CB, nb, k0, x, ldx, acc.as<double>());
     ++launches;
   }
   for (int64_t b = nblk - 1; b >= 0; --b) {
@@ -394,11 +474,11 @@ int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_
     const int nb = (int)std::min<int64_t>(CB, n - k0);
     const int64_t kend = k0 + nb;
     if (kend < n) {
-      dim3 gr((unsigned)ceil_div(n - kend, GV), (unsigned)nrhs);
+      dim3 gr((unsigned)ceil_div(n - kend, GVB), 1, (unsigned)nrhs);
       k_block_gemv<true><<<gr, 128, 0, st>>>(H, ldh, k0, nb, kend, n, x, ldx, acc.as<double>());
       ++launches;
     }
-    k_block_diag<true><<<(unsigned)nrhs, 128, 0, st>>>(Li + b * CB * CB, nb, k0, x, ldx, acc.as<double>());
+    k_block_diag<true><<<(unsigned)nrhs, 256, 0, st>>>(Li + b * CB * CB, nb, k0, x, ldx, acc.as<double>());
     ++launches;
   }
   DGP_CHECK_LAUNCH();
