@@ -348,13 +348,17 @@ def tg_jacobian_bench(reps=3, tols=(1e-10, 1e-12, 1e-13, 1e-14), truth_tol=1e-14
     del out
     g = torch.as_tensor(np.random.default_rng(5).standard_normal((nm, 20)), device="cuda")
     ms_vjp = _event_ms(lambda: api.jacobian_tg_vjp(nb, phi, phiA, fpsf, link, gfc, nt, g), reps)
-    # the same two kernels with the CUDA-core engine (dgp_set_jacobian_engine(1))
+    # the same two kernels on each engine (dgp_set_jacobian_engine: 1 CUDA cores, 2 tensor cores)
     from dogpup_b200._lib import lib as _dl
-    _dl.dgp_set_jacobian_engine(1)
-    out = {}
-    ms_cc = _event_ms(lambda: out.__setitem__("J", api.jacobian_tg(nb, phi, phiA, fpsf, link, gfc, nt)), reps)
-    del out
-    ms_vjp_cc = _event_ms(lambda: api.jacobian_tg_vjp(nb, phi, phiA, fpsf, link, gfc, nt, g), reps)
+    engines = {}
+    for eng, name in ((1, "cuda_cores"), (2, "tensor_cores")):
+        _dl.dgp_set_jacobian_engine(eng)
+        out = {}
+        ms_e = _event_ms(lambda: out.__setitem__("J", api.jacobian_tg(nb, phi, phiA, fpsf, link, gfc, nt)), reps)
+        del out
+        engines[name] = {"ms": round(ms_e, 3),
+                         "vjp_ms": round(_event_ms(lambda: api.jacobian_tg_vjp(nb, phi, phiA, fpsf, link, gfc, nt, g),
+                                                   reps), 3)}
     _dl.dgp_set_jacobian_engine(0)
     field_bytes = 16.0 * nf * nv * (ns + nd)
     j_bytes = 4.0 * nv * 20 * nm
@@ -380,7 +384,7 @@ def tg_jacobian_bench(reps=3, tols=(1e-10, 1e-12, 1e-13, 1e-14), truth_tol=1e-14
     mesh._solver = None
     return {"workload": f"ellipsoid 90x75x70 @1.38mm, {nv} nodes, 32x32 optodes, 64 harmonics, 20 gates",
             "J_shape": [20 * nm, nv], "ms": round(ms, 3), "vjp_ms": round(ms_vjp, 3),
-            "cuda_core_engine": {"ms": round(ms_cc, 3), "vjp_ms": round(ms_vjp_cc, 3)},
+            "engines": engines, "engine_used": "auto: TG Jacobian on CUDA cores, vjp on tensor cores",
             "achieved_gbs": round((field_bytes + j_bytes) / (ms * 1e-3) / 1e9, 1),
             "achieved_tflops_fp32": round(flops / (ms * 1e-3) / 1e12, 2),
             "mixed_vs_fp64": {"truth": f"FP64 fields to {truth_tol:g} (reached {max(rep0.max_rel_residual, repA0.max_rel_residual):.2e}), "

@@ -46,7 +46,10 @@ constexpr int GTHREADS = 256;
 constexpr int GEMM_SMEM = GSTAGES * 2 * CB * LDK * (int)sizeof(double);   // 160 KB
 static_assert(GEMM_SMEM >= CB * (CB + 1) * (int)sizeof(double), "the epilogue tile must fit the stage ring");
 constexpr int GV = 256;          // k per CTA of the solves' off-diagonal partial sums
-constexpr int64_t NBO = 512;     // outer panel width: depth of the trailing update GEMM
+#ifndef DGP_CHOL_NBO
+#define DGP_CHOL_NBO 512
+#endif
+constexpr int64_t NBO = DGP_CHOL_NBO;  // outer panel width: depth of the trailing update GEMM
 
 __device__ inline uint32_t su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 

@@ -657,12 +657,16 @@ int launch_common(JArgs &a, size_t &smem, int &grid) {
 
 }  // namespace
 
-// 0: the time-gated Jacobian on the tensor cores where its shapes fit (else CUDA cores);
-// 1: always the CUDA-core kernel
+// 0 (auto): for each kernel the engine measured faster at the sensitivity configuration's
+//   shapes (100k voxels, 32 x 32 optodes, 64 harmonics, 20 gates, one B200): the TG Jacobian on
+//   the CUDA cores (20.0 ms; its tensor-core form, latency-bound in every phase with one CTA per
+//   SM, 42.5 ms), the vjp on the tensor cores (5.2 ms against 16.4 ms);
+// 1: both on the CUDA cores;  2: both on the tensor cores where their shapes fit
 static int g_jacobian_engine = 0;
 
 int set_jacobian_engine(int engine) {
-  DGP_REQUIRE(engine == 0 || engine == 1, "jacobian engine must be 0 (tensor cores where they fit) or 1 (CUDA cores)");
+  DGP_REQUIRE(engine >= 0 && engine <= 2,
+              "jacobian engine must be 0 (auto), 1 (CUDA cores) or 2 (tensor cores where the shapes fit)");
   g_jacobian_engine = engine;
   return DGP_OK;
 }
@@ -704,7 +708,7 @@ int jacobian_run(int mode, const int32_t *prow, const int32_t *pcol, const doubl
     DGP_CUDA(cudaFuncSetAttribute(k_jacobian_complex, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const TcLayout tl = tc_layout(nf, ns, nd);
   const size_t smem_tc = tl.bytes + 1024;
-  if (mode == 0 && g_jacobian_engine == 0 && smem_tc <= 227 * 1024) {
+  if (mode == 0 && g_jacobian_engine == 2 && smem_tc <= 227 * 1024) {
     // tensor cores: one persistent CTA per SM
     DevBuf flag;
     DGP_TRY(flag.alloc(sizeof(int)));
@@ -757,7 +761,7 @@ int jacobian_run(int mode, const int32_t *prow, const int32_t *pcol, const doubl
     k_chat<<<(unsigned)ceil_div((int64_t)nm * nf, 256), 256, 0, st>>>(gin, ctab.as<float2>(), rytov, nm, ng, nf,
                                                                       chat.as<float2>());
     DGP_CHECK_LAUNCH();
-    if (g_jacobian_engine == 0 && ns <= 32 && nd <= 32 && nm <= 4096) {
+    if (g_jacobian_engine != 1 && ns <= 32 && nd <= 32 && nm <= 4096) {
       // tensor cores: per-harmonic complex GEMM over voxel tiles
       DevBuf btab, flag;
       DGP_TRY(btab.alloc((size_t)nf * 2 * VT_B));

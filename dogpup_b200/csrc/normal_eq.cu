@@ -407,10 +407,13 @@ int lm_update_run(const float *Jt, int64_t nv, int64_t nm, const double *W, cons
   const bool dual = form == 2 || (form == 0 && nm < nv);
   if (form_used) *form_used = dual ? 2 : 1;
   if (!dual) {
+    // an even leading dimension keeps every row 16-byte aligned: the Cholesky's GEMMs then move
+    // their operands with 16-byte copies
+    const int64_t ldh = nv + (nv & 1);
     DevBuf H;
-    DGP_TRY(H.alloc(sizeof(double) * (size_t)nv * nv));
-    DGP_TRY(normal_eq_run(Jt, nv, nm, W, y, lam, 0, H.as<double>(), nv, x, st));
-    return cholesky_solve_run(H.as<double>(), nv, nv, x, st);
+    DGP_TRY(H.alloc(sizeof(double) * (size_t)nv * ldh));
+    DGP_TRY(normal_eq_run(Jt, nv, nm, W, y, lam, 0, H.as<double>(), ldh, x, st));
+    return cholesky_solve_run(H.as<double>(), nv, ldh, x, st);
   }
   DevBuf diag, Jw, G, z, errb;
   if (W) {
@@ -420,7 +423,8 @@ int lm_update_run(const float *Jt, int64_t nv, int64_t nm, const double *W, cons
   }
   DGP_TRY(diag.alloc(sizeof(double) * nv));
   DGP_TRY(Jw.alloc(sizeof(float) * (size_t)nm * nv));
-  DGP_TRY(G.alloc(sizeof(double) * (size_t)nm * nm));
+  const int64_t ldg = nm + (nm & 1);
+  DGP_TRY(G.alloc(sizeof(double) * (size_t)nm * ldg));
   DGP_TRY(z.alloc(sizeof(double) * nm));
   DGP_TRY(row_dots_run(Jt, nv, nm, W, nullptr, diag.as<double>(), nullptr, st));
   std::vector<double> hd((size_t)nv);
@@ -434,10 +438,10 @@ int lm_update_run(const float *Jt, int64_t nv, int64_t nm, const double *W, cons
   k_scale_transpose<<<tg, tb, 0, st>>>(Jt, W, nv, nm, Jw.as<float>());
   DGP_CHECK_LAUNCH();
   // G = J_w J_w^T + mu I: the split-BF16 Gram kernel on J_w (rows = measurements)
-  DGP_TRY(normal_eq_run(Jw.as<float>(), nm, nv, nullptr, nullptr, mu, 2, G.as<double>(), nm, nullptr, st));
+  DGP_TRY(normal_eq_run(Jw.as<float>(), nm, nv, nullptr, nullptr, mu, 2, G.as<double>(), ldg, nullptr, st));
   k_scale_sqrtw<<<(unsigned)ceil_div(nm, 256), 256, 0, st>>>(y, W, nm, z.as<double>());
   DGP_CHECK_LAUNCH();
-  DGP_TRY(cholesky_solve_run(G.as<double>(), nm, nm, z.as<double>(), st));
+  DGP_TRY(cholesky_solve_run(G.as<double>(), nm, ldg, z.as<double>(), st));
   k_scale_sqrtw<<<(unsigned)ceil_div(nm, 256), 256, 0, st>>>(z.as<double>(), W, nm, z.as<double>());
   DGP_CHECK_LAUNCH();
   // x = J^T (W^1/2 z)

@@ -153,8 +153,8 @@ def test_jacobian_rejects_bad_link_and_basis(jac_case):
 
 @pytest.fixture
 def cuda_core_engine():
-    """Runs the test's body with dgp_jacobian_tg forced to its CUDA-core kernel, then restores
-    the default (tensor cores where the shapes fit)."""
+    """use(e) selects the Jacobian engines (1 CUDA cores, 2 tensor cores where the shapes fit);
+    the default (0, auto) is restored after the test."""
     from dogpup_b200._lib import lib, check
 
     def use(engine):
@@ -195,6 +195,7 @@ def test_tg_jacobian_tensor_cores_match_cuda_cores_and_oracle(ns, nd, nf, ng, sh
     nb = mesh.nodal_basis()
     link = mesh._link()
     nt = len(t)
+    cuda_core_engine(2)
     J_tc = api.jacobian_tg(nb, phi, phiA, mesh.optode.s_fpsf, link, gfc_d, nt)
     cuda_core_engine(1)
     J_cc = api.jacobian_tg(nb, phi, phiA, mesh.optode.s_fpsf, link, gfc_d, nt)
@@ -210,6 +211,7 @@ def test_tg_jacobian_tensor_cores_match_cuda_cores_and_oracle(ns, nd, nf, ng, sh
     assert per_link < 1e-5, per_link
     g = np.random.default_rng(nf).standard_normal((link.shape[0], ng))
     g_d = torch.as_tensor(g, device="cuda")
+    cuda_core_engine(2)
     v_tc = api.jacobian_tg_vjp(nb, phi, phiA, mesh.optode.s_fpsf, link, gfc_d, nt, g_d).cpu().numpy()
     cuda_core_engine(1)
     v_cc = api.jacobian_tg_vjp(nb, phi, phiA, mesh.optode.s_fpsf, link, gfc_d, nt, g_d).cpu().numpy()
@@ -220,5 +222,5 @@ def test_tg_jacobian_tensor_cores_match_cuda_cores_and_oracle(ns, nd, nf, ng, sh
 
 def test_tg_jacobian_engine_switch_rejects_unknown_engines():
     from dogpup_b200._lib import lib
-    assert lib.dgp_set_jacobian_engine(2) == 1 and lib.dgp_set_jacobian_engine(-1) == 1
-    assert lib.dgp_set_jacobian_engine(0) == 0
+    assert lib.dgp_set_jacobian_engine(3) == 1 and lib.dgp_set_jacobian_engine(-1) == 1
+    assert lib.dgp_set_jacobian_engine(2) == 0 and lib.dgp_set_jacobian_engine(0) == 0
