@@ -18,10 +18,11 @@
 //     k_dgemm_nt     update of the outer panel's remaining columns: A_il -= L_ik L_lk^T
 //   k_dgemm_nt       trailing update of the rest, depth 512: A_il -= sum over the outer panel
 //
-// k_dgemm_nt: C = beta C + alpha A B^T with A, B row-major (K contiguous); 128 x 128 CTA tiles,
-// 256 threads (8 warps of 64 x 32), K in stages of 16 doubles moved by cp.async through a
-// 4-deep shared-memory ring (rows padded to 20 doubles: the fragment loads hit 32 distinct banks
-// per half-warp), 16 mma.sync m16n8k4 .f64 per warp per 4 K.
+// k_dgemm_nt: C = beta C + alpha A B^T with A, B row-major (K contiguous); 128 x 64 CTA tiles,
+// two CTAs per SM (one's epilogue overlaps the other's main loop), 256 threads (8 warps of
+// 32 x 32), K in stages of 16 doubles moved by cp.async through a 3-deep shared-memory ring
+// (rows padded to 20 doubles: the fragment loads hit 32 distinct banks per half-warp), 8
+// mma.sync m16n8k4 .f64 per warp per 4 K.
 //
 // Solves: L y = b and L^T x = y by 128-row blocks with the stored diagonal inverses:
 //   y_b = inv(L_bb) (b_b - sum_{c<b} L_bc y_c),   x_b = inv(L_bb)^T (y_b - sum_{c>b} L_cb^T x_c),
@@ -39,12 +40,16 @@ namespace dgp {
 namespace {
 
 constexpr int CB = 128;          // panel width = CTA tile
+constexpr int GBM = 128;         // GEMM CTA tile rows; columns GBN = 64 (two CTAs per SM) or 128
 constexpr int GK = 16;           // K per pipeline stage (doubles)
 constexpr int LDK = GK + 4;      // padded shared-memory row (doubles)
-constexpr int GSTAGES = 4;
+constexpr int GSTAGES = 3;
 constexpr int GTHREADS = 256;
-constexpr int GEMM_SMEM = GSTAGES * 2 * CB * LDK * (int)sizeof(double);   // 160 KB
-static_assert(GEMM_SMEM >= CB * (CB + 1) * (int)sizeof(double), "the epilogue tile must fit the stage ring");
+// the stage ring, or the epilogue tile where that is larger: 90 KB (GBN = 64), 132 KB (GBN = 128)
+constexpr int gemm_smem(int gbn) {
+  return (int)sizeof(double) * (GSTAGES * (GBM + gbn) * LDK > GBM * (gbn + 1) ? GSTAGES * (GBM + gbn) * LDK
+                                                                               : GBM * (gbn + 1));
+}
 constexpr int GV = 256;          // k per CTA of the solves' off-diagonal partial sums
 #ifndef DGP_CHOL_NBO
 #define DGP_CHOL_NBO 512
@@ -82,54 +87,63 @@ struct Gemm {
   int64_t ldc;
   int64_t M, N, K;     // C is M x N, A is M x K, B is N x K
   double alpha, beta;
-  int lower;           // 1: tiles with tj <= ti only, and in diagonal tiles only entries c <= r
+  int lower;           // 1: only the tiles that meet the lower triangle, only entries c <= r
   int64_t tn;          // tiles along N (full mode)
 };
 
-// C = beta C + alpha A B^T on 128 x 128 tiles (see the file comment).  V: bytes per cp.async
-// (16 when every row start and the base addresses are 16-byte aligned, else 8).
-template <int V>
-__global__ void __launch_bounds__(GTHREADS, 1) k_dgemm_nt(Gemm g) {
+// C = beta C + alpha A B^T on 128 x GBN CTA tiles (see the file comment).  V: bytes per cp.async
+// (16 when every row start and the base addresses are 16-byte aligned, else 8).  GBN = 128 when C
+// is A itself (the in-place panel: a CTA must own whole rows of it).  Lower mode (GBN = 64): the
+// tiles that meet the lower triangle, row ti holding tiles tj = 0 .. 2 ti + 1 (the last two
+// straddle the diagonal; only entries c <= r are written).
+template <int V, int GBN>
+__global__ void __launch_bounds__(GTHREADS, GBN == 64 ? 2 : 1) k_dgemm_nt(Gemm g) {
+  constexpr int NJ = GBN / 16;                      // n8 fragments per warp (warp tile 32 x GBN / 2)
   extern __shared__ __align__(16) double gsm[];
   int64_t ti, tj;
   if (g.lower) {
-    const int64_t b = blockIdx.x;
-    ti = (int64_t)((sqrt(8.0 * (double)b + 1.0) - 1.0) * 0.5);
-    while (ti * (ti + 1) / 2 > b) --ti;
-    while ((ti + 1) * (ti + 2) / 2 <= b) ++ti;
-    tj = b - ti * (ti + 1) / 2;
+    const int64_t b = blockIdx.x;                   // row ti starts at tile ti (ti + 1)
+    ti = (int64_t)((sqrt(4.0 * (double)b + 1.0) - 1.0) * 0.5);
+    while (ti * (ti + 1) > b) --ti;
+    while ((ti + 1) * (ti + 2) <= b) ++ti;
+    tj = b - ti * (ti + 1);
   } else {
     ti = blockIdx.x / g.tn;
     tj = blockIdx.x % g.tn;
   }
-  const int64_t r0 = ti * CB, c0 = tj * CB;
+  const int64_t r0 = ti * GBM, c0 = tj * GBN;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int wm = warp & 1, wn = warp >> 1;          // warp tile: rows wm*64.., cols wn*32..
+  const int wm = warp & 3, wn = warp >> 2;          // warp tile: rows wm*32.., cols wn*GBN/2..
   const int gid = lane >> 2, tig = lane & 3;
-  double acc[4][4][4];
+  double acc[2][NJ][4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
+    for (int j = 0; j < NJ; ++j)
 #pragma unroll
       for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
 
   const int nk = (int)((g.K + GK - 1) / GK);
   constexpr int E = V / 8;                          // doubles per copy
   constexpr int PER_ROW = GK / E;                   // copies per row per stage
+  constexpr int COPIES = (GBM + GBN) * PER_ROW;
   auto load_stage = [&](int kb, int slot) {
-    double *As = gsm + (size_t)slot * 2 * CB * LDK, *Bs = As + CB * LDK;
+    double *As = gsm + (size_t)slot * (GBM + GBN) * LDK, *Bs = As + GBM * LDK;
     const int64_t kbase = (int64_t)kb * GK;
-    for (int e = tid; e < 2 * CB * PER_ROW; e += GTHREADS) {
-      const int which = e / (CB * PER_ROW), rem = e % (CB * PER_ROW), row = rem / PER_ROW, kc = (rem % PER_ROW) * E;
-      const int64_t grow = (which ? c0 : r0) + row, gk = kbase + kc;
-      const bool ok = grow < (which ? g.N : g.M) && gk + E <= g.K;
-      const double *base = which ? g.B : g.A;
-      const int64_t ld = which ? g.ldb : g.lda;
+#pragma unroll
+    for (int e0 = 0; e0 < COPIES; e0 += GTHREADS) {
+      const int e = e0 + tid;
+      const bool isb = e >= GBM * PER_ROW;
+      const int rem = isb ? e - GBM * PER_ROW : e, row = rem / PER_ROW, kc = (rem % PER_ROW) * E;
+      const int64_t grow = (isb ? c0 : r0) + row, gk = kbase + kc;
+      const bool ok = grow < (isb ? g.N : g.M) && gk + E <= g.K;
+      const double *base = isb ? g.B : g.A;
+      const int64_t ld = isb ? g.ldb : g.lda;
       const double *src = ok ? base + grow * ld + gk : base;
-      cp_async<V>((which ? Bs : As) + row * LDK + kc, src, ok);
+      cp_async<V>((isb ? Bs : As) + row * LDK + kc, src, ok);
     }
   };
+  static_assert(COPIES % GTHREADS == 0, "whole copy rounds per stage");
   // prologue: GSTAGES - 1 stages in flight
 #pragma unroll
   for (int s = 0; s < GSTAGES - 1; ++s) {
@@ -142,178 +156,274 @@ __global__ void __launch_bounds__(GTHREADS, 1) k_dgemm_nt(Gemm g) {
     const int nxt = kb + GSTAGES - 1;
     if (nxt < nk) load_stage(nxt, nxt % GSTAGES);
     cp_commit();
-    const double *As = gsm + (size_t)(kb % GSTAGES) * 2 * CB * LDK, *Bs = As + CB * LDK;
+    const double *As = gsm + (size_t)(kb % GSTAGES) * (GBM + GBN) * LDK, *Bs = As + GBM * LDK;
 #pragma unroll
     for (int k4 = 0; k4 < GK; k4 += 4) {
-      double a[4][2], b[4];
+      double a[2][2], b[NJ];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int row = wm * 64 + i * 16 + gid;
+      for (int i = 0; i < 2; ++i) {
+        const int row = wm * 32 + i * 16 + gid;
         a[i][0] = As[row * LDK + k4 + tig];
         a[i][1] = As[(row + 8) * LDK + k4 + tig];
       }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[(wn * 32 + j * 8 + gid) * LDK + k4 + tig];
+      for (int j = 0; j < NJ; ++j) b[j] = Bs[(wn * (GBN / 2) + j * 8 + gid) * LDK + k4 + tig];
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) mma_f64(acc[i][j], a[i][0], a[i][1], b[j]);
+        for (int j = 0; j < NJ; ++j) mma_f64(acc[i][j], a[i][0], a[i][1], b[j]);
     }
   }
   cp_wait<0>();
   __syncthreads();   // the stage ring is free: the epilogue goes through shared memory
-  // epilogue: the accumulators are written to shared memory (a 128 x 129-double tile), then the
+  // epilogue: the accumulators are written to shared memory (a 128 x (GBN + 1)-double tile), then the
   // CTA reads and writes C row by row, coalesced, with every load of C in flight together
-  // (C = beta C + alpha acc; in diagonal tiles of the lower mode only entries c <= r)
+  // (C = beta C + alpha acc; in the lower mode only entries c <= r)
   double *T = gsm;
-  constexpr int TLD = CB + 1;
+  constexpr int TLD = GBN + 1;
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
+    for (int j = 0; j < NJ; ++j)
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const int r = wm * 64 + i * 16 + gid + (q >> 1) * 8, c = wn * 32 + j * 8 + 2 * tig + (q & 1);
+        const int r = wm * 32 + i * 16 + gid + (q >> 1) * 8, c = wn * (GBN / 2) + j * 8 + 2 * tig + (q & 1);
         T[r * TLD + c] = acc[i][j][q];
       }
   __syncthreads();
-  const int64_t rows = min((int64_t)CB, g.M - r0), cols = min((int64_t)CB, g.N - c0);
+  const int64_t rows = min((int64_t)GBM, g.M - r0), cols = min((int64_t)GBN, g.N - c0);
   // batches of 16 entries per thread: all 16 loads of C are issued before any store (a store to
   // C between loads would otherwise keep the compiler from overlapping their latencies)
   constexpr int BATCH = 16;
-  for (int e0 = tid; e0 < CB * CB; e0 += GTHREADS * BATCH) {
+  static_assert(GBM * GBN % (GTHREADS * BATCH) == 0, "whole epilogue batches");
+#pragma unroll 1
+  for (int e0 = tid; e0 < GBM * GBN; e0 += GTHREADS * BATCH) {
     double cv[BATCH];
     bool in[BATCH];
 #pragma unroll
     for (int u = 0; u < BATCH; ++u) {
-      const int e = e0 + u * GTHREADS, r = e / CB, c = e % CB;
-      in[u] = e < CB * CB && r < rows && c < cols && (!g.lower || ti != tj || c <= r);
+      const int e = e0 + u * GTHREADS, r = e / GBN, c = e % GBN;
+      in[u] = r < rows && c < cols && (!g.lower || c0 + c <= r0 + r);
       cv[u] = (in[u] && g.beta != 0.0) ? g.C[(r0 + r) * g.ldc + c0 + c] : 0.0;
     }
 #pragma unroll
     for (int u = 0; u < BATCH; ++u) {
-      const int e = e0 + u * GTHREADS, r = e / CB, c = e % CB;
+      const int e = e0 + u * GTHREADS, r = e / GBN, c = e % GBN;
       if (in[u]) g.C[(r0 + r) * g.ldc + c0 + c] = g.beta * cv[u] + g.alpha * T[r * TLD + c];
     }
   }
 }
 
 // Factor the nb x nb diagonal block at (k0, k0) in place (lower) and write inv(L) (row-major,
-// nb x nb, zero above the diagonal) to Linv.  One CTA of 128 threads; the block sits in shared
-// memory with rows padded to 129 doubles.  32-column steps: warp 0 factors the 32 x 32 diagonal
-// (warp-synchronous, one column per step), then every thread solves its rows of the 32-column
-// panel below and the trailing lower triangle is updated.  err |= 1 on a non-positive or
-// non-finite pivot.
-constexpr int PT = 128, PLD = 129;
-constexpr size_t POT_SMEM = sizeof(double) * ((size_t)PT * PLD + 3 * 32 * 33);
-__global__ void __launch_bounds__(128) k_potrf_tile(double *__restrict__ H, int64_t ldh, int64_t k0, int nb,
-                                                   double *__restrict__ Linv, int *err) {
-  extern __shared__ double L[];                      // [PT][PLD], then the [3][32][33] level products
+// nb x nb, zero above the diagonal) to Linv.  One CTA of 256 threads; the block sits in shared
+// memory with rows padded to 129 doubles, rows and columns past nb set to the identity (which
+// the factorisation leaves alone).  The strict upper triangle of the shared tile collects
+// X = inv(L) transposed ([c][i] holds X[i][c]); dinv[c] = 1 / L[c][c].  Four 32-column steps:
+//   1. warp 0 factors the 32 x 32 diagonal block D, one row per lane in registers (a column per
+//      step: the pivot by shuffle, its reciprocal square root, the column scaled, the rank-1
+//      update of the lanes' rows), then forms X_D = inv(D), one column per lane
+//   2. the rows below: L_rD = A_rD X_D^T (a 32-term product per entry; lane = column)
+//   3. the trailing lower triangle: A -= L_rD L_cD^T in 4 x 4 register tiles
+// then the off-diagonal blocks of X by their distance d = I - J below the diagonal:
+//   T = sum_{K = J .. I-1} L_IK X_KJ,   X_IJ = -X_II T   (a column of T per group of lanes).
+// err |= 1 on a non-positive or non-finite pivot.
+constexpr int PT = 128, PLD = 129, PTHREADS = 256;
+constexpr size_t POT_SMEM = sizeof(double) * ((size_t)PT * PLD + PT);   // 130 KB: fits beside a GEMM CTA
+__global__ void __launch_bounds__(PTHREADS, 1) k_potrf_tile(double *__restrict__ H, int64_t ldh, int64_t k0, int nb,
+                                                           double *__restrict__ Linv, int *err) {
+  extern __shared__ double L[];                      // [PT][PLD], then dinv[PT]
+  double *dinv = L + PT * PLD;
   __shared__ int bad;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr unsigned FULL = 0xffffffffu;
   if (tid == 0) bad = 0;
-  for (int e = tid; e < nb * nb; e += blockDim.x) {
-    const int r = e / nb, c = e % nb;
-    L[r * PLD + c] = c <= r ? H[(k0 + r) * ldh + k0 + c] : 0.0;
+  // the lower triangle (16 loads in flight per thread); the identity past nb; zero above
+  constexpr int PER = PT * PT / PTHREADS;
+#pragma unroll 1
+  for (int u0 = 0; u0 < PER; u0 += 16) {
+    double v[16];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      const int e = tid + (u0 + u) * PTHREADS, r = e >> 7, c = e & (PT - 1);
+      v[u] = (c <= r && r < nb) ? H[(k0 + r) * ldh + k0 + c] : (r == c ? 1.0 : 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      const int e = tid + (u0 + u) * PTHREADS, r = e >> 7, c = e & (PT - 1);
+      L[r * PLD + c] = v[u];
+    }
   }
   __syncthreads();
-  for (int j0 = 0; j0 < nb; j0 += 32) {
-    const int jw = min(32, nb - j0);
-    // 1. warp 0: factor the jw x jw diagonal block, one column per step
+  for (int j0 = 0; j0 < PT; j0 += 32) {
+    // 1. D = L_D L_D^T with row lane of D in lane's registers (loops unrolled: every register
+    //    index is a constant), then X_D = inv(L_D) with column lane in registers
     if (warp == 0) {
-      for (int j = 0; j < jw; ++j) {
-        const int c = j0 + j;
-        double d = L[c * PLD + c];
-        if (!(d > 0.0) || !isfinite(d)) {
-          if (lane == 0) bad = 1;
+      double a[32];
+      double *row = L + (j0 + lane) * PLD + j0;            // row lane of D
+#pragma unroll
+      for (int q = 0; q < 32; ++q) a[q] = q <= lane ? row[q] : 0.0;
+      bool lbad = false;
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        double d = __shfl_sync(FULL, a[j], j);
+        if (!(d > 0.0) || !isfinite(d)) {                  // the same d in every lane
+          lbad = true;
           d = 1.0;
         }
-        d = sqrt(d);
-        __syncwarp();
-        const int r = j0 + lane;
-        if (lane > j && lane < jw) L[r * PLD + c] /= d;
-        if (lane == 0) L[c * PLD + c] = d;
-        __syncwarp();
-        // update the rest of the diagonal block's lower triangle: columns j+1 .. lane of row r
-        if (lane > j && lane < jw) {
-          const double lrc = L[r * PLD + c];
-          for (int q = j + 1; q <= lane; ++q) L[r * PLD + j0 + q] -= lrc * L[(j0 + q) * PLD + c];
+        const double inv = rsqrt(d), s = d * inv;
+        a[j] = lane == j ? s : (lane > j ? a[j] * inv : 0.0);
+        if (lane == 0) dinv[j0 + j] = inv;
+        const double aj = a[j];
+#pragma unroll
+        for (int q = 0; q < 32; ++q) {                     // (q <= j folds away: both are constants)
+          const double lq = __shfl_sync(FULL, aj, q);      // L[q][j]
+          if (q > j && lane >= q) a[q] -= aj * lq;
         }
-        __syncwarp();
+      }
+#pragma unroll
+      for (int q = 0; q < 32; ++q)
+        if (q <= lane) row[q] = a[q];                      // L[lane][q]
+      if (lbad && lane == 0) bad = 1;
+      __syncwarp();
+      // column c = lane of X_D: X[i][c] = (delta_ic - sum_{m<i} L[i][m] X[m][c]) / L[i][i]
+      // (X[m][c] = 0 for m < c; two partial sums halve the dependent chain), kept at [c][i]
+      double x[32];
+#pragma unroll
+      for (int i = 0; i < 32; ++i) {
+        const double *li = L + (j0 + i) * PLD + j0;
+        double t0 = i == lane ? 1.0 : 0.0, t1 = 0.0;
+#pragma unroll
+        for (int m = 0; m + 1 < i; m += 2) {
+          t0 -= li[m] * x[m];
+          t1 -= li[m + 1] * x[m + 1];
+        }
+        if (i & 1) t0 -= li[i - 1] * x[i - 1];
+        x[i] = i >= lane ? (t0 + t1) * dinv[j0 + i] : 0.0;
+      }
+#pragma unroll
+      for (int i = 0; i < 32; ++i)
+        if (i > lane) row[i] = x[i];
+    }
+    __syncthreads();
+    const int t0 = j0 + 32, nr = PT - t0;
+    if (nr == 0) break;
+    // 2. rows below: L[r][j0 + c] = sum_{k <= c} A[r][j0 + k] X[c][k]  (lane = c; column c of
+    //    X_D^T in registers, zero above its diagonal)
+    {
+      double xc[32];
+#pragma unroll
+      for (int k = 0; k < 32; ++k)
+        xc[k] = k < lane ? L[(j0 + k) * PLD + j0 + lane] : (k == lane ? dinv[j0 + lane] : 0.0);
+      double out[12];
+#pragma unroll
+      for (int u = 0; u < 12; ++u) out[u] = 0.0;
+#pragma unroll 2
+      for (int u = 0; u < 12; ++u) {
+        const int r = t0 + warp + 8 * u;
+        if (r < PT) {
+          const double *ar = L + r * PLD + j0;
+          double s = 0.0;
+#pragma unroll
+          for (int k = 0; k < 32; ++k) s += ar[k] * xc[k];
+#pragma unroll
+          for (int v = 0; v < 12; ++v) out[v] = v == u ? s : out[v];
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int u = 0; u < 12; ++u) {
+        const int r = t0 + warp + 8 * u;
+        if (r < PT) L[r * PLD + j0 + lane] = out[u];
       }
     }
     __syncthreads();
-    // 2. panel rows below: row r solves x L_dd^T = a  (forward substitution over the jw columns)
-    for (int r = j0 + jw + tid; r < nb; r += blockDim.x) {
-      for (int j = 0; j < jw; ++j) {
-        const int c = j0 + j;
-        double s = L[r * PLD + c];
-        for (int q = 0; q < j; ++q) s -= L[r * PLD + j0 + q] * L[c * PLD + j0 + q];
-        L[r * PLD + c] = s / L[c * PLD + c];
+    // 3. trailing lower triangle of rows/columns [t0, PT): 4 x 4 tiles (ti >= tj)
+    {
+      const int T = nr / 4, ntile = T * (T + 1) / 2;
+      for (int t = tid; t < ntile; t += PTHREADS) {
+        int ti = (int)((sqrtf(8.0f * (float)t + 1.0f) - 1.0f) * 0.5f);
+        while (ti * (ti + 1) / 2 > t) --ti;
+        while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
+        const int tj = t - ti * (ti + 1) / 2;
+        const int r0 = t0 + 4 * ti, c0 = t0 + 4 * tj;
+        double acc[4][4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int v = 0; v < 4; ++v) acc[u][v] = 0.0;
+#pragma unroll 8
+        for (int q = 0; q < 32; ++q) {
+          double lr[4], lc[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            lr[u] = L[(r0 + u) * PLD + j0 + q];
+            lc[u] = L[(c0 + u) * PLD + j0 + q];
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) acc[u][v] += lr[u] * lc[v];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int v = 0; v < 4; ++v)
+            if (c0 + v <= r0 + u) L[(r0 + u) * PLD + c0 + v] -= acc[u][v];
       }
-    }
-    __syncthreads();
-    // 3. trailing lower triangle: A[r][c] -= sum_q L[r][q] L[c][q] over the panel's columns
-    const int t0 = j0 + jw, nt = nb - t0;
-    for (int e = tid; e < nt * nt; e += blockDim.x) {
-      const int r = t0 + e / nt, c = t0 + e % nt;
-      if (c > r) continue;
-      double s = 0.0;
-      for (int q = j0; q < j0 + jw; ++q) s += L[r * PLD + q] * L[c * PLD + q];
-      L[r * PLD + c] -= s;
     }
     __syncthreads();
   }
   if (bad && tid == 0) atomicOr(err, 1);
-  // write L back
-  for (int e = tid; e < nb * nb; e += blockDim.x) {
-    const int r = e / nb, c = e % nb;
-    if (c <= r) H[(k0 + r) * ldh + k0 + c] = L[r * PLD + c];
-  }
-  // inv(L) = X, blocked by 32 (entries X[i][c], i > c, kept in the strict upper triangle of the
-  // shared tile at [c][i]; X[c][c] = 1 / L[c][c] in dinv):
-  //   1. the diagonal 32-blocks: warp w, lane l solves column c = 32 w + l of inv(L_ww)
-  //   2. the off-diagonal blocks by distance d = I - J = 1, 2, 3 below the diagonal:
-  //      T = sum_{K = J .. I-1} L_IK X_KJ, then X_IJ = -X_II T
-  __shared__ double dinv[PT];
-  for (int c = tid; c < nb; c += blockDim.x) dinv[c] = 1.0 / L[c * PLD + c];
-  __syncthreads();
-  auto X = [&](int k, int c) -> double { return k < c ? 0.0 : (k == c ? dinv[c] : L[c * PLD + k]); };
-  {
-    const int c = 32 * warp + lane;
-    if (c < nb) {
-      const int iend = min(32 * (warp + 1), nb);
-      for (int i = c + 1; i < iend; ++i) {
-        double t = L[i * PLD + c] * dinv[c];
-        for (int l = c + 1; l < i; ++l) t += L[i * PLD + l] * L[c * PLD + l];
-        L[c * PLD + i] = -t * dinv[i];
+  // the off-diagonal blocks of X, by distance d (level d reads only levels < d and the diagonal):
+  // g = 2, 4, 8 adjacent lanes per column c of the 4 - d block pairs (J = pair, I = J + d) sum
+  // their shares of the depth 32 d into T[:, c] = sum_{k in [32J, 32I)} L[I rows][k] X[k][c]
+  // (32 rows in registers), the shares meet by butterfly shuffles, then X_IJ[:, c] = -X_II T[:, c]
+  // with the rows split over the group.  No shared scratch: X_IJ goes to [c][i], which nothing
+  // at this level reads.
+  for (int d = 1; d < 4; ++d) {
+    const int g = 1 << d, share = 32 * d / g;          // 2, 4, 8 lanes; depth shares 16, 16, 12
+    const bool on = tid < (4 - d) * 32 * g;            // whole warps (192 or 256 threads)
+    const int col = tid / g, part = tid % g;
+    const int J = col >> 5, I = J + d, c = 32 * J + (col & 31);
+    double t[32];
+#pragma unroll
+    for (int r = 0; r < 32; ++r) t[r] = 0.0;
+    if (on) {
+      const int kb = 32 * J + part * share;
+      for (int kk = 0; kk < share; ++kk) {
+        const int k = kb + (kk + part) % share;         // parts start apart: no shared bank
+        const double up = L[c * PLD + k];
+        const double x = k > c ? up : (k == c ? dinv[c] : 0.0);
+        const double *lk = L + 32 * I * PLD + k;
+#pragma unroll
+        for (int r = 0; r < 32; ++r) t[r] += lk[r * PLD] * x;
       }
     }
-  }
-  __syncthreads();
-  double *Tb = L + PT * PLD;                          // [3][32][33] products of one level
-  for (int d = 1; d < 4; ++d) {
-    const int nblk = 4 - d;
-    for (int e = tid; e < nblk * 1024; e += blockDim.x) {
-      const int J = e / 1024, I = J + d, i = 32 * I + (e % 1024) / 32, c = 32 * J + e % 32;
-      double t = 0.0;
-      if (i < nb && c < nb)
-        for (int k = 32 * J; k < 32 * I; ++k) t += L[i * PLD + k] * X(k, c);
-      Tb[(J * 32 + (e % 1024) / 32) * 33 + e % 32] = t;
-    }
-    __syncthreads();
-    for (int e = tid; e < nblk * 1024; e += blockDim.x) {
-      const int J = e / 1024, I = J + d, i = 32 * I + (e % 1024) / 32, c = 32 * J + e % 32;
-      if (i >= nb || c >= nb) continue;
-      double x = 0.0;
-      for (int m = 32 * I; m <= i; ++m) x += X(i, m) * Tb[(J * 32 + m - 32 * I) * 33 + e % 32];
-      L[c * PLD + i] = -x;
+    for (int off = 1; off < g; off <<= 1)
+#pragma unroll
+      for (int r = 0; r < 32; ++r) t[r] += __shfl_xor_sync(FULL, t[r], off);
+    if (on) {
+#pragma unroll
+      for (int r = 0; r < 32; ++r) {
+        if (r % g != part) continue;
+        const int i = 32 * I + r;
+        double x = dinv[i] * t[r];
+#pragma unroll
+        for (int m = 0; m < r; ++m) x += L[(32 * I + m) * PLD + i] * t[m];   // X_II[i][m] at [m][i]
+        L[c * PLD + i] = -x;
+      }
     }
     __syncthreads();
   }
-  for (int e = tid; e < nb * nb; e += blockDim.x) {
+  // L back to H, inv(L) to Linv
+#pragma unroll 16
+  for (int u = 0; u < PER; ++u) {
+    const int e = tid + u * PTHREADS, r = e >> 7, c = e & (PT - 1);
+    if (r < nb && c <= r) H[(k0 + r) * ldh + k0 + c] = L[r * PLD + c];
+  }
+  for (int e = tid; e < nb * nb; e += PTHREADS) {
     const int i = e / nb, c = e % nb;
-    Linv[e] = X(i, c);
+    Linv[e] = c > i ? 0.0 : (c == i ? dinv[i] : L[c * PLD + i]);
   }
 }
 
@@ -352,51 +462,114 @@ __global__ void k_block_gemv(const double *__restrict__ H, int64_t ldh, int64_t 
 }
 
 // X[r][base + i] = sum_j Linv'[i][j] (X[r][base + j] - acc[r][j]), Linv' = inv(L_bb) (forward) or
-// its transpose (backward); one warp per output entry (lanes stride j, coalesced along rows of
-// Linv for the forward product); acc is cleared for the next block.
+// its transpose (backward), DRHS right-hand sides per CTA; acc is cleared for the next block.
+//   forward:  warp w takes rows 8w .. 8w + 7 of Linv (all 32 of a lane's loads in flight
+//             together, coalesced along the rows), then a warp sum per row
+//   backward: thread (g, i) reads column i of Linv over rows 32g .. 32g + 31 (coalesced along
+//             each row), and the four groups' partial sums meet in shared memory
+constexpr int DTHREADS = 512, DRHS = 8;
 template <bool TRANS>
-__global__ void k_block_diag(const double *__restrict__ Linv, int nbi, int64_t base, double *X, int64_t ldx,
-                             double *acc) {
+__global__ void __launch_bounds__(DTHREADS) k_block_diag(const double *__restrict__ Linv, int nbi, int64_t base,
+                                                        double *X, int64_t ldx, double *acc, int nrhs) {
   __shared__ double rhs[CB];
-  const int r = blockIdx.x;
-  double *x = X + (int64_t)r * ldx + base;
-  for (int j = threadIdx.x; j < nbi; j += blockDim.x) rhs[j] = x[j] - acc[(int64_t)r * CB + j];
-  __syncthreads();
-  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  for (int i = threadIdx.x >> 5; i < nbi; i += nw) {
-    double s = 0.0;
+  __shared__ double part[4][CB];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int r_end = min(nrhs, (int)(blockIdx.x + 1) * DRHS);
+  for (int r = blockIdx.x * DRHS; r < r_end; ++r) {
+    double *x = X + (int64_t)r * ldx + base;
+    __syncthreads();                                 // the previous right-hand side is done with rhs / part
+    if (tid < CB) rhs[tid] = tid < nbi ? x[tid] - acc[(int64_t)r * CB + tid] : 0.0;
+    __syncthreads();
     if (!TRANS) {
-      for (int j = lane; j <= i; j += 32) s += Linv[(int64_t)i * nbi + j] * rhs[j];
+      double s[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int i = warp * 8 + u;
+        double t = 0.0;
+#pragma unroll
+        for (int q = 0; q < CB / 32; ++q) {
+          const int j = lane + 32 * q;
+          if (i < nbi && j < nbi) t += Linv[(int64_t)i * nbi + j] * rhs[j];
+        }
+        s[u] = t;
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) s[u] += __shfl_xor_sync(0xffffffffu, s[u], off);
+      if (lane < 8) {
+        double v = s[0];
+#pragma unroll
+        for (int u = 1; u < 8; ++u) v = lane == u ? s[u] : v;
+        const int i = warp * 8 + lane;
+        if (i < nbi) x[i] = v;
+      }
     } else {
-      for (int j = i + lane; j < nbi; j += 32) s += Linv[(int64_t)j * nbi + i] * rhs[j];
+      const int i = tid & (CB - 1), g = tid / CB;
+      double t = 0.0;
+      if (i < nbi) {
+#pragma unroll 8
+        for (int jj = 0; jj < 32; ++jj) {
+          const int j = 32 * g + jj;
+          if (j < nbi) t += Linv[(int64_t)j * nbi + i] * rhs[j];
+        }
+      }
+      part[g][i] = t;
+      __syncthreads();
+      if (tid < nbi) x[tid] = part[0][tid] + part[1][tid] + part[2][tid] + part[3][tid];
     }
-    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-    if (lane == 0) {
-      x[i] = s;
-      acc[(int64_t)r * CB + i] = 0.0;
-    }
+    if (tid < nbi) acc[(int64_t)r * CB + tid] = 0.0;
   }
 }
 
-int gemm_nt(const Gemm &g0, cudaStream_t st) {
-  Gemm g = g0;
-  if (g.M <= 0 || g.N <= 0) return DGP_OK;
-  const bool a16 = ((uintptr_t)g.A % 16 == 0) && ((uintptr_t)g.B % 16 == 0) && g.lda % 2 == 0 && g.ldb % 2 == 0 &&
-                   g.K % 2 == 0;
-  const int64_t tm = ceil_div(g.M, CB), tn = ceil_div(g.N, CB);
+template <int V, int GBN>
+int gemm_launch(Gemm g, cudaStream_t st) {
+  constexpr int smem = gemm_smem(GBN);
+  const int64_t tm = ceil_div(g.M, (int64_t)GBM), tn = ceil_div(g.N, (int64_t)GBN);
   g.tn = tn;
-  const int64_t tiles = g.lower ? tm * (tm + 1) / 2 : tm * tn;
+  // lower mode (M == N, GBN = 64): row ti of tiles holds tj = 0 .. 2 ti + 1; a tile past N (the
+  // last one of a row when N is not a multiple of 128) writes nothing
+  const int64_t tiles = g.lower ? tm * (tm + 1) : tm * tn;
   DGP_REQUIRE(tiles <= INT32_MAX, "cholesky: too many tiles");
-  if (a16) {
-    DGP_CUDA(cudaFuncSetAttribute(k_dgemm_nt<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM));
-    k_dgemm_nt<16><<<(unsigned)tiles, GTHREADS, GEMM_SMEM, st>>>(g);
-  } else {
-    DGP_CUDA(cudaFuncSetAttribute(k_dgemm_nt<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM));
-    k_dgemm_nt<8><<<(unsigned)tiles, GTHREADS, GEMM_SMEM, st>>>(g);
-  }
+  DGP_CUDA(cudaFuncSetAttribute(k_dgemm_nt<V, GBN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  k_dgemm_nt<V, GBN><<<(unsigned)tiles, GTHREADS, smem, st>>>(g);
   DGP_CHECK_LAUNCH();
   return DGP_OK;
 }
+
+// C = beta C + alpha A B^T; 128-column tiles when C is A (in place), else 64-column tiles
+int gemm_nt(const Gemm &g, cudaStream_t st) {
+  if (g.M <= 0 || g.N <= 0) return DGP_OK;
+  const bool a16 = ((uintptr_t)g.A % 16 == 0) && ((uintptr_t)g.B % 16 == 0) && g.lda % 2 == 0 && g.ldb % 2 == 0 &&
+                   g.K % 2 == 0;
+  const bool inplace = g.C == g.A;
+  if (inplace) DGP_REQUIRE(!g.lower && g.N <= GBM, "cholesky: an in-place product must fit one 128-column tile");
+  if (inplace) return a16 ? gemm_launch<16, 128>(g, st) : gemm_launch<8, 128>(g, st);
+  return a16 ? gemm_launch<16, 64>(g, st) : gemm_launch<8, 64>(g, st);
+}
+
+// The two streams and four events of the lookahead; the destructor waits for both streams, so
+// that an early error return never frees buffers that queued kernels still use.
+struct LookaheadStreams {
+  cudaStream_t f = nullptr, r = nullptr;
+  cudaEvent_t fork = nullptr, panel = nullptr, rest = nullptr, join = nullptr;
+  int create() {
+    int lo = 0, hi = 0;
+    DGP_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    DGP_CUDA(cudaStreamCreateWithPriority(&f, cudaStreamNonBlocking, hi));
+    DGP_CUDA(cudaStreamCreateWithPriority(&r, cudaStreamNonBlocking, lo));
+    for (cudaEvent_t *e : {&fork, &panel, &rest, &join}) DGP_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    return DGP_OK;
+  }
+  ~LookaheadStreams() {
+    if (f) cudaStreamSynchronize(f);
+    if (r) cudaStreamSynchronize(r);
+    for (cudaEvent_t e : {fork, panel, rest, join})
+      if (e) cudaEventDestroy(e);
+    if (f) cudaStreamDestroy(f);
+    if (r) cudaStreamDestroy(r);
+  }
+};
 
 }  // namespace
 
@@ -417,9 +590,22 @@ int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_
   DGP_CUDA(cudaFuncSetAttribute(k_potrf_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pot_smem));
   double *Li = linv.as<double>();
   int64_t launches = 0;
-  // 512-column outer panels: inside one, 128-column steps update only the outer panel's own
-  // columns (the rows below included); the rest of the matrix takes the outer panel's update in
-  // one lower-triangle GEMM of depth 512
+  // Lookahead on two streams forked from st: sf (high priority) factors the outer panels and
+  // gives the next outer panel its update; sr (low priority) updates the rest of the matrix.
+  // Outer panel p = columns [o0, oend), next panel [oend, nend):
+  //   sf:  F_p   the 128-column steps of panel p (diagonal block, the rows below, the panel's own
+  //              remaining columns)
+  //        N_p   rows [oend, n) x columns [oend, nend) -= Q Q_next^T, Q = panel p's rows  (after
+  //              R_{p-1}, which updates the same entries)
+  //   sr:  R_p   the lower triangle of [nend, n)^2 -= Q Q^T  (after F_p)
+  // so F_{p+1} runs while R_p does, and the GEMMs of the whole factorisation keep their depth 512.
+  LookaheadStreams ls;
+  DGP_TRY(ls.create());
+  DGP_CUDA(cudaEventRecord(ls.fork, st));
+  DGP_CUDA(cudaStreamWaitEvent(ls.f, ls.fork, 0));
+  DGP_CUDA(cudaStreamWaitEvent(ls.r, ls.fork, 0));
+  cudaStream_t sf = ls.f, sr = ls.r;
+  bool r_recorded = false;
   for (int64_t o0 = 0; o0 < n; o0 += NBO) {
     const int64_t oend = std::min(n, o0 + NBO);
     bool last = false;
@@ -427,7 +613,7 @@ int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_
       const int64_t b = k0 / CB;
       const int nb = (int)std::min<int64_t>(CB, n - k0);
       double *Lb = Li + b * CB * CB;
-      k_potrf_tile<<<1, 128, pot_smem, st>>>(H, ldh, k0, nb, Lb, errb.as<int>());
+      k_potrf_tile<<<1, PTHREADS, pot_smem, sf>>>(H, ldh, k0, nb, Lb, errb.as<int>());
       DGP_CHECK_LAUNCH();
       ++launches;
       const int64_t kend = k0 + nb, rest = n - kend;
@@ -437,39 +623,58 @@ int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_
       }
       // L_ik = A_ik inv(L_kk)^T for every row below (in place, one CTA per 128-row strip)
       const Gemm p{H + kend * ldh + k0, ldh, Lb, nb, H + kend * ldh + k0, ldh, rest, nb, nb, 1.0, 0.0, 0, 0};
-      DGP_TRY(gemm_nt(p, st));
+      DGP_TRY(gemm_nt(p, sf));
       ++launches;
       const int64_t w = oend - kend;  // the outer panel's remaining columns
       if (w > 0) {
         const Gemm a{H + kend * ldh + k0, ldh, H + kend * ldh + k0, ldh, H + kend * ldh + kend, ldh, w, w, nb,
                      -1.0, 1.0, 1, 0};
-        DGP_TRY(gemm_nt(a, st));
+        DGP_TRY(gemm_nt(a, sf));
         ++launches;
         if (n > oend) {
           const Gemm r{H + oend * ldh + k0, ldh, H + kend * ldh + k0, ldh, H + oend * ldh + kend, ldh, n - oend, w,
                        nb, -1.0, 1.0, 0, 0};
-          DGP_TRY(gemm_nt(r, st));
+          DGP_TRY(gemm_nt(r, sf));
           ++launches;
         }
       }
     }
     if (last || n <= oend) break;
-    // trailing lower triangle: rows/cols [oend, n) -= Q Q^T, Q = rows [oend, n) x cols [o0, oend)
-    const Gemm t{H + oend * ldh + o0, ldh, H + oend * ldh + o0, ldh, H + oend * ldh + oend, ldh, n - oend, n - oend,
-                 oend - o0, -1.0, 1.0, 1, 0};
-    DGP_TRY(gemm_nt(t, st));
+    const int64_t nend = std::min(n, oend + NBO), depth = oend - o0;
+    DGP_CUDA(cudaEventRecord(ls.panel, sf));
+    // N_p: the next panel's lower square, then the rows below it
+    if (r_recorded) DGP_CUDA(cudaStreamWaitEvent(sf, ls.rest, 0));
+    const Gemm nq{H + oend * ldh + o0, ldh, H + oend * ldh + o0, ldh, H + oend * ldh + oend, ldh, nend - oend,
+                  nend - oend, depth, -1.0, 1.0, 1, 0};
+    DGP_TRY(gemm_nt(nq, sf));
     ++launches;
+    if (n > nend) {
+      const Gemm nr{H + nend * ldh + o0, ldh, H + oend * ldh + o0, ldh, H + nend * ldh + oend, ldh, n - nend,
+                    nend - oend, depth, -1.0, 1.0, 0, 0};
+      DGP_TRY(gemm_nt(nr, sf));
+      // R_p: the lower triangle past the next panel
+      DGP_CUDA(cudaStreamWaitEvent(sr, ls.panel, 0));
+      const Gemm t{H + nend * ldh + o0, ldh, H + nend * ldh + o0, ldh, H + nend * ldh + nend, ldh, n - nend,
+                   n - nend, depth, -1.0, 1.0, 1, 0};
+      DGP_TRY(gemm_nt(t, sr));
+      DGP_CUDA(cudaEventRecord(ls.rest, sr));
+      r_recorded = true;
+      launches += 2;
+    }
   }
+  if (r_recorded) DGP_CUDA(cudaStreamWaitEvent(sf, ls.rest, 0));
   // L y = b, then L^T x = y, by 128-row blocks
+  const unsigned dgrid = (unsigned)ceil_div((int64_t)nrhs, (int64_t)DRHS);
   for (int64_t b = 0; b < nblk; ++b) {
     const int64_t k0 = b * CB;
     const int nb = (int)std::min<int64_t>(CB, n - k0);
     if (k0 > 0) {
       dim3 gr((unsigned)ceil_div(k0, GV), (unsigned)ceil_div(nb, 8), (unsigned)nrhs);
-      k_block_gemv<false><<<gr, 256, 0, st>>>(H, ldh, k0, nb, 0, k0, x, ldx, acc.as<double>());
+      k_block_gemv<false><<<gr, 256, 0, sf>>>(H, ldh, k0, nb, 0, k0, x, ldx, acc.as<double>());
       ++launches;
     }
-    k_block_diag<false><<<(unsigned)nrhs, 256, 0, st>>>(Li + b * CB * CB, nb, k0, x, ldx, acc.as<double>());
+    k_block_diag<false><<<dgrid, DTHREADS, 0, sf>>>(Li + b * CB * CB, nb, k0, x, ldx, acc.as<double>(),
+                                                          nrhs);
     ++launches;
   }
   for (int64_t b = nblk - 1; b >= 0; --b) {
@@ -478,12 +683,15 @@ int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_
     const int64_t kend = k0 + nb;
     if (kend < n) {
       dim3 gr((unsigned)ceil_div(n - kend, GVB), 1, (unsigned)nrhs);
-      k_block_gemv<true><<<gr, 128, 0, st>>>(H, ldh, k0, nb, kend, n, x, ldx, acc.as<double>());
+      k_block_gemv<true><<<gr, 128, 0, sf>>>(H, ldh, k0, nb, kend, n, x, ldx, acc.as<double>());
       ++launches;
     }
-    k_block_diag<true><<<(unsigned)nrhs, 256, 0, st>>>(Li + b * CB * CB, nb, k0, x, ldx, acc.as<double>());
+    k_block_diag<true><<<dgrid, DTHREADS, 0, sf>>>(Li + b * CB * CB, nb, k0, x, ldx, acc.as<double>(),
+                                                         nrhs);
     ++launches;
   }
+  DGP_CUDA(cudaEventRecord(ls.join, sf));
+  DGP_CUDA(cudaStreamWaitEvent(st, ls.join, 0));
   DGP_CHECK_LAUNCH();
   count_launches(launches);
   int herr = 0;
