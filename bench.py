@@ -203,18 +203,23 @@ def _gates(t, n, width, start, spacing):
 
 
 def _event_ms(fn, reps):
+    """Median over `reps` calls of each call's CUDA-event time (after two untimed calls): a
+    single call slowed by the shared node (a driver allocation path that another process
+    holds) moves the median of 5 less than the mean of 3."""
     import torch
     st = torch.cuda.current_stream()
     fn()
     fn()  # twice: a call that allocates its output while the previous one lives needs two blocks
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(st)
-    for _ in range(reps):
+    times = []
+    for _ in range(max(reps, 5)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
         fn()
-    e1.record(st)
-    torch.cuda.synchronize()
-    return e0.elapsed_time(e1) / reps
+        e1.record(st)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return float(np.median(times))
 
 
 def plain_fp64_small_bench(tol=1e-10, truth_tol=1e-13):
@@ -665,12 +670,15 @@ def plain_fp64_per_rhs(mesh, nsample=4, tol=1e-8):
 
 # --------------------------------------------------------------- our arm
 def _guarded(name, fn):
-    """Runs one secondary measurement; an exception is reported in its key instead of ending the
-    run (the main line is still printed)."""
+    """Runs one secondary measurement with nvidia-smi sampling the clocks meanwhile; an exception
+    is reported in its key instead of ending the run (the main line is still printed)."""
     import gc
     import torch
     gc.collect()
     torch.cuda.empty_cache()
+    clk = Clocks(torch.cuda.current_device())
+    clk.wait_ready()
+    clk.mark()
     t0 = time.perf_counter()
     try:
         out = fn()
@@ -678,6 +686,10 @@ def _guarded(name, fn):
         import traceback
         traceback.print_exc()
         out = {"error": f"{type(e).__name__}: {e}"}
+    if isinstance(out, dict):
+        out["clocks"] = clk.stop()      # SM clock and throttle reasons while this measurement ran
+    else:
+        clk.stop()
     log(f"[rank 0] {name} ({time.perf_counter() - t0:.1f} s): {json.dumps(out)[:2000]}")
     gc.collect()
     torch.cuda.empty_cache()
