@@ -389,7 +389,7 @@ def tg_jacobian_bench(reps=3, tols=(1e-10, 1e-12, 1e-13, 1e-14), truth_tol=1e-14
     mesh._solver = None
     return {"workload": f"ellipsoid 90x75x70 @1.38mm, {nv} nodes, 32x32 optodes, 64 harmonics, 20 gates",
             "J_shape": [20 * nm, nv], "ms": round(ms, 3), "vjp_ms": round(ms_vjp, 3),
-            "engines": engines, "engine_used": "auto: TG Jacobian on CUDA cores, vjp on tensor cores",
+            "engines": engines, "engine_used": "default: TG Jacobian and vjp on the tensor cores",
             "achieved_gbs": round((field_bytes + j_bytes) / (ms * 1e-3) / 1e9, 1),
             "achieved_tflops_fp32": round(flops / (ms * 1e-3) / 1e12, 2),
             "mixed_vs_fp64": {"truth": f"FP64 fields to {truth_tol:g} (reached {max(rep0.max_rel_residual, repA0.max_rel_residual):.2e}), "

@@ -175,47 +175,81 @@ __global__ void __launch_bounds__(JBS) k_jacobian_tg(JArgs a, const float2 *__re
 }
 
 // ------------------------------------------------------------------------------------------
-// Time-gated Jacobian on the tensor cores (tcgen05, kind::tf32, 3xTF32 split).
+// Time-gated Jacobian on the tensor cores (tcgen05, kind::tf32, 3xTF32 split), nodal basis.
 //
-// Per voxel v and tile of 128 links m, J_tg[v][g][m] = w_v * sum_K' A'[m][K'] B'[K'][g] with
-//   A'[m][K'] = Re / Im of a_k(m) = (P phi_s)_k (P phiA_d)_k  and  B'[K'][g] = Re / -Im of C[g,k],
-// K' = 2 NF (the real and imaginary parts of the DFT's complex products).  K' runs in chunks of
-// 16 harmonics = 32 values ([16 real | 16 imaginary], one 128-byte row of a 128B-swizzled
-// K-major tile).  FP32 values x are split x = hi + lo with hi = tf32(x), lo = tf32(x - hi), and
-// each chunk issues hi*hi + hi*lo + lo*hi into an FP32 accumulator in tensor memory (the lo*lo
-// term, ~2^-22 relative, is dropped).
+// Per voxel v the DFT over harmonics is a real GEMM over the (gate, source) x detector block:
+//   J_tg[v][g][m(s,d)] = w_v Re sum_k Q[g,s,k] Pd[k][d],   Q[g,s,k] = C[g,k] Ps[k][s]
+//                      = w_v sum_K' A'[(g,s)][K'] B'[d][K']
+// with A' = [Re Q | -Im Q] and B' = [Re Pd | Im Pd] over K' = 2 NF, Ps / Pd the source and
+// detector fields at node v.  An MMA tile is M = 128 rows (4 gates x 32 sources) x N = 32
+// detectors, K' in chunks of 16 harmonics (one 128-byte row: [16 real | 16 imaginary]).  Of the
+// two ways to form the per-voxel operand this one builds NG x NS x NF products (the gate
+// coefficient times the source field) instead of NS x ND x NF (the field products per link),
+// and no MMA column is spent on padded gates.  FP32 values x enter as hi = tf32(x) and
+// lo = tf32(x - hi); each chunk issues hi*hi + hi*lo + lo*hi into an FP32 accumulator in tensor
+// memory (the lo*lo term, ~2^-22 relative, is dropped).
 //
-// CTA = 256 threads, persistent over voxels (one CTA per SM).  All threads build the A' chunks
-// (two threads per link row, 8 harmonics each) from the voxel's fields staged in shared memory;
-// thread 0 issues the chunk's 12 MMAs (M = 128, N = 32 gate columns, K = 8) and commits them to
-// the chunk buffer's mbarrier.  Two chunk buffers: the next chunk is built while the tensor core
-// works on the previous one.  Two accumulators in tensor memory (2 x 32 columns): a tile's
-// epilogue (tcgen05.ld, w_v and Rytov scaling, coalesced FP32 stores) runs while the next tile's
-// MMAs are in flight.  Every mbarrier wait is bounded; a timeout raises err and ends the kernel
-// after waiting (bounded) for the MMAs it issued, and the tensor memory is always freed.
-constexpr int TC_THREADS = 256;
-constexpr int TC_CH = 16;                    // harmonics per K' chunk
-constexpr int TC_ROWS = 128;                 // links per tile (MMA M)
-constexpr int TC_N = 32;                     // gate columns (MMA N), NG <= 32
-constexpr int TC_ATILE = TC_ROWS * 128;      // one 128 x 32 fp32 operand tile: 16 KB
-constexpr int TC_BTILE = TC_N * 128;         // one 32 x 32 fp32 operand tile: 4 KB
-constexpr uint32_t TC_IDESC = tc::idesc(2, 2, TC_ROWS, TC_N);
+// Persistent CTA (one per SM), warp-specialised, all hand-offs through mbarriers:
+//   warps 0-3   epilogue: tensor memory -> w_v (and Rytov) scaling -> J (warp q reads the
+//               accumulator lanes 32q..32q+31 = gate 4t+q of tile t, lane = source)
+//   warps 4-11  builders: B' of the voxel (one chunk x 8 harmonics per warp, lane = detector),
+//               then the A' stages (lane = source, warp = gate within the tile x harmonic half);
+//               each work item's 8 field loads are issued one item ahead (register prefetch)
+//   warp 12     one thread issues the 12 MMAs of each stage; tensor-memory allocation
+// Rings: 4 A' stages (32 KB each), 2 B' buffers (one per voxel in flight), 2 accumulator sets
+// in tensor memory (32 NTILE columns each), so building voxel i+1, its MMAs and the epilogue of
+// voxel i overlap.  Every mbarrier wait is bounded: a timeout sets err, raises the abort flag
+// that every role polls, and the MMA thread waits (bounded) for all of its MMAs before the
+// tensor memory is freed.
+constexpr int T2_EPI = 4, T2_BLD = 8;
+constexpr int T2_THREADS = 32 * (T2_EPI + T2_BLD + 1);
+constexpr int T2_NST = 4;                          // A' stages
+constexpr int T2_ASTAGE = 2 * 128 * 128;           // hi + lo of 128 rows x 128 B
+constexpr int T2_BCH = 2 * 32 * 128;               // one chunk of B': hi + lo of 32 rows x 128 B
+constexpr uint32_t T2_IDESC = tc::idesc(2, 2, 128, 32);
 
-struct TcLayout {
-  uint32_t a_off, b_off, f_off, bytes;       // A' buffers, B' table, staged fields, total (from the 1 KB-aligned base)
-  int nch;
+struct T2Layout {
+  uint32_t a_off, b_off, c_off, l_off, bytes;      // from the 1 KB-aligned base
+  int nch, ntile, nkp;
+  uint32_t tcols;
 };
 
-__host__ __device__ inline TcLayout tc_layout(int nf, int ns, int nd) {
-  TcLayout L;
-  L.nch = (nf + TC_CH - 1) / TC_CH;
-  L.a_off = 0;                                               // 2 buffers x (hi, lo)
-  L.b_off = 4 * TC_ATILE;                                    // nch x (hi) then nch x (lo)
-  L.f_off = L.b_off + 2 * L.nch * TC_BTILE;
-  L.bytes = L.f_off + (uint32_t)(sizeof(float2) * (size_t)nf * (ns + nd));
+__host__ __device__ inline T2Layout t2_layout(int nf, int ng) {
+  T2Layout L;
+  L.nch = (nf + 15) / 16;
+  L.ntile = (ng + 3) / 4;
+  L.nkp = 16 * L.nch;
+  L.a_off = 0;
+  L.b_off = T2_NST * T2_ASTAGE;
+  L.c_off = L.b_off + 2 * L.nch * T2_BCH;                        // gate table [4 NTILE][NKP] float2
+  L.l_off = L.c_off + (uint32_t)(8 * 4 * L.ntile * L.nkp);        // link lookup [32][32] int
+  L.bytes = L.l_off + 4 * 32 * 32;
+  uint32_t need = 2u * 32u * (uint32_t)L.ntile, cols = 32;
+  while (cols < need) cols <<= 1;
+  L.tcols = cols;
   return L;
 }
 
+// 8 harmonics k0 .. k0+7 of optode o of field f [nf][nn][cnt] at node v (zero past nf / cnt):
+// the loads, kept as FP64 until t2_cvt8 (so that they can be issued one work item ahead)
+__device__ inline void t2_load8(const JArgs &a, int64_t v, const double2 *__restrict__ f, int cnt, int o, int k0,
+                                double2 (&x)[8]) {
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int k = k0 + i;
+    x[i] = (o < cnt && k < a.nf) ? __ldg(f + ((int64_t)k * a.nn + v) * cnt + o) : make_double2(0.0, 0.0);
+  }
+}
+
+__device__ inline void t2_cvt8(const double2 (&x)[8], float (&re)[8], float (&im)[8]) {
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    re[i] = (float)x[i].x;
+    im[i] = (float)x[i].y;
+  }
+}
+
+// x -> (tf32(x), tf32(x - tf32(x))) for 4 values, stored as 16-byte chunks of the hi and lo images
 __device__ inline void st_split4(unsigned char *hi, unsigned char *lo, uint32_t off, const float (&x)[4]) {
   float h[4], l[4];
 #pragma unroll
@@ -227,167 +261,231 @@ __device__ inline void st_split4(unsigned char *hi, unsigned char *lo, uint32_t 
   *reinterpret_cast<float4 *>(lo + off) = make_float4(l[0], l[1], l[2], l[3]);
 }
 
-__global__ void __launch_bounds__(TC_THREADS, 1) k_jacobian_tg_tc(JArgs a, const float2 *__restrict__ C /*[ng][nf]*/,
-                                                                 const double *__restrict__ rytov,
+// rows of a K-major 128-byte-swizzled split operand: 8 real values into chunks (2h, 2h+1), 8
+// imaginary into (4+2h, 5+2h) of row r
+__device__ inline void t2_store_row(unsigned char *hi, unsigned char *lo, int r, int h, const float (&re)[8],
+                                    const float (&im)[8]) {
+  const float r0[4] = {re[0], re[1], re[2], re[3]}, r1[4] = {re[4], re[5], re[6], re[7]};
+  const float i0[4] = {im[0], im[1], im[2], im[3]}, i1[4] = {im[4], im[5], im[6], im[7]};
+  st_split4(hi, lo, tc::sw128_chunk(r, 2 * h + 0), r0);
+  st_split4(hi, lo, tc::sw128_chunk(r, 2 * h + 1), r1);
+  st_split4(hi, lo, tc::sw128_chunk(r, 4 + 2 * h + 0), i0);
+  st_split4(hi, lo, tc::sw128_chunk(r, 4 + 2 * h + 1), i1);
+}
+
+__global__ void __launch_bounds__(T2_THREADS, 1) k_jacobian_tg_tc(JArgs a, const float2 *__restrict__ C /*[ng][nf]*/,
+                                                                 const double *__restrict__ rytov, int dense,
                                                                  float *__restrict__ Jtg, int *err) {
-  extern __shared__ __align__(1024) unsigned char tc_raw[];
-  __shared__ __align__(8) uint64_t bar_buf[2], bar_d[2];
+  extern __shared__ __align__(1024) unsigned char t2_raw[];
+  __shared__ __align__(8) uint64_t full[T2_NST], empty[T2_NST], bfull[2], bempty[2], tfull[2], tempty[2], done;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
-  unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(tc_raw) + 1023) & ~uintptr_t(1023));
-  const TcLayout L = tc_layout(a.nf, a.ns, a.nd);
-  unsigned char *Ab = sm + L.a_off;                   // buffer b: hi at b*2*ATILE, lo at +ATILE
-  unsigned char *Bhi = sm + L.b_off, *Blo = Bhi + L.nch * TC_BTILE;
-  float2 *Ps = reinterpret_cast<float2 *>(sm + L.f_off), *Pd = Ps + a.nf * a.ns;
+  unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(t2_raw) + 1023) & ~uintptr_t(1023));
+  const T2Layout L = t2_layout(a.nf, a.ng);
+  float2 *Ct = reinterpret_cast<float2 *>(sm + L.c_off);
+  int *lk = reinterpret_cast<int *>(sm + L.l_off);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  constexpr unsigned FULL = 0xffffffffu;
+  volatile int *abort_v = &abort_flag;
 
   if (tid == 0) {
-    for (int b = 0; b < 2; ++b) {
-      tc::mbar_init(&bar_buf[b], 1);
-      tc::mbar_init(&bar_d[b], 1);
+    for (int i = 0; i < T2_NST; ++i) {
+      tc::mbar_init(&full[i], T2_BLD);                 // one arrival per builder warp
+      tc::mbar_init(&empty[i], 1);
     }
+    for (int b = 0; b < 2; ++b) {
+      tc::mbar_init(&bfull[b], T2_BLD);
+      tc::mbar_init(&bempty[b], 1);
+      tc::mbar_init(&tfull[b], 1);
+      tc::mbar_init(&tempty[b], T2_EPI);
+    }
+    tc::mbar_init(&done, 1);
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 0) tc::tmem_alloc(&tmem_slot, 2 * TC_N);
-  // B' = the gate table, split: row g (MMA N), K' = chunk c's [Re C[g][16c..16c+15] | -Im C[g][..]]
-  for (int t = tid; t < L.nch * TC_N * 8; t += TC_THREADS) {
-    const int c = t / (TC_N * 8), g = (t / 8) % TC_N, q = t % 8;   // 16-byte chunk q of row g in chunk c
-    float x[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int j = 4 * q + i, k = c * TC_CH + (j & 15);
-      const float2 v = (g < a.ng && k < a.nf) ? C[g * a.nf + k] : make_float2(0.f, 0.f);
-      x[i] = j < 16 ? v.x : -v.y;
-    }
-    st_split4(Bhi + c * TC_BTILE, Blo + c * TC_BTILE, tc::sw128_chunk(g, q), x);
+  if (warp == T2_EPI + T2_BLD) tc::tmem_alloc(&tmem_slot, L.tcols);
+  for (int t = tid; t < 4 * L.ntile * L.nkp; t += T2_THREADS) {
+    const int g = t / L.nkp, k = t % L.nkp;
+    Ct[t] = (g < a.ng && k < a.nf) ? C[g * a.nf + k] : make_float2(0.f, 0.f);
   }
-  tc::fence_async_smem();
+  for (int t = tid; t < 32 * 32; t += T2_THREADS) lk[t] = -1;
+  __syncthreads();
+  if (!dense)
+    for (int m = tid; m < a.nm; m += T2_THREADS) lk[a.link[2 * m] * 32 + a.link[2 * m + 1]] = m;  // unique links
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tmem = tmem_slot;
 
-  const int r = tid & (TC_ROWS - 1), half = tid >> 7;   // link row of the tile, harmonic half of a chunk
-  uint32_t q = 0, t = 0;                               // chunks and tiles issued by this CTA
-  bool have_prev = false, stop = false;
-  int64_t pv = 0;
-  int pm0 = 0;
-  uint32_t pt = 0;
-  float pw = 0.f;
-
-  // epilogue of tile tp (voxel vp, links m0p..): TMEM accumulator tp & 1 -> J
-  auto epilogue = [&](uint32_t tp, int64_t vp, int m0p, float wp) {
-    bool ok = tc::mbar_wait(&bar_d[tp & 1], (tp >> 1) & 1);
-    if (!ok) atomicOr(err, 1);
-    ok = __all_sync(0xffffffffu, ok);
-    tc::fence_after_sync();
-    if (ok) {
-      const int quad = warp & 3, cbase = (warp >> 2) * 16;
-      uint32_t v[16];
-      tc::tmem_ld16(tmem + ((uint32_t)(32 * quad) << 16) + (tp & 1) * TC_N + cbase, v);
-      const int m = m0p + 32 * quad + lane;
-      if (m < a.nm) {
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          const int g = cbase + i;
-          if (g < a.ng) {
-            float val = wp * __uint_as_float(v[i]);
-            if (rytov) val = val / (float)rytov[(int64_t)m * a.ng + g];
-            Jtg[((int64_t)vp * a.ng + g) * a.nm + m] = val;
-          }
-        }
-      }
-    }
-    tc::fence_before_sync();
-    return ok;
-  };
-
-  for (int64_t v = blockIdx.x; v < a.nv && !stop; v += gridDim.x) {
-    __syncthreads();                                   // the previous voxel's chunks are built
-    stage_field(a, v, a.phi, a.ns, Ps);
-    stage_field(a, v, a.phiA, a.nd, Pd);
-    __syncthreads();
-    const float wv = (float)(a.w ? a.w[v] : 1.0);
-    for (int m0 = 0; m0 < a.nm && !stop; m0 += TC_ROWS) {
-      const int m = m0 + r;
-      const bool valid = m < a.nm;
-      const int s = valid ? a.link[2 * m] : 0, d = valid ? a.link[2 * m + 1] : 0;
-      for (int c = 0; c < L.nch; ++c) {
-        const uint32_t b = q & 1;
-        bool ok = true;
-        if (q >= 2) ok = tc::mbar_wait(&bar_buf[b], ((q >> 1) - 1) & 1);   // chunk q-2 has been consumed
-        if (!ok) {
-          atomicOr(err, 2);
-          abort_flag = 1;
-        }
-        unsigned char *hi = Ab + b * 2 * TC_ATILE, *lo = hi + TC_ATILE;
-        if (ok) {
-          // this thread's 8 harmonics of chunk c: K' = 8 half + i (real) and 16 + 8 half + i (imaginary)
-          float re[8], im[8];
-#pragma unroll
-          for (int i = 0; i < 8; ++i) {
-            const int k = c * TC_CH + 8 * half + i;
-            re[i] = im[i] = 0.f;
-            if (valid && k < a.nf) {
-              const float2 x = Ps[k * a.ns + s], y = Pd[k * a.nd + d];
-              re[i] = x.x * y.x - x.y * y.y;
-              im[i] = x.x * y.y + x.y * y.x;
+  if (warp == T2_EPI + T2_BLD) {
+    // ---------------------------------------------------------------- MMA issue (one thread)
+    if (lane == 0) {
+      uint32_t st_idx = 0;
+      int i = 0;
+      for (int64_t v = blockIdx.x; v < a.nv; v += gridDim.x, ++i) {
+        if (*abort_v) break;
+        const int buf = i & 1;
+        bool ok = tc::mbar_wait(&bfull[buf], (i >> 1) & 1);
+        if (ok && i >= 2) ok = tc::mbar_wait(&tempty[buf], ((i >> 1) - 1) & 1);
+        tc::fence_after_sync();
+        const uint32_t dbase = tmem + (uint32_t)(buf * 32 * L.ntile);
+        const unsigned char *bb = sm + L.b_off + buf * L.nch * T2_BCH;
+        for (int c = 0; c < L.nch && ok; ++c) {
+          const uint32_t bh = tc::smem_u32(bb + c * T2_BCH), bl = bh + 4096;
+          for (int t = 0; t < L.ntile; ++t, ++st_idx) {
+            const uint32_t s = st_idx % T2_NST;
+            if (!tc::mbar_wait(&full[s], (st_idx / T2_NST) & 1)) {
+              ok = false;
+              break;
             }
+            tc::fence_after_sync();
+            const uint32_t ah = tc::smem_u32(sm + L.a_off + s * T2_ASTAGE), al = ah + 16384;
+            const uint32_t d_tm = dbase + 32u * t;
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) {           // K = 8 tf32 = 32 bytes per MMA
+              const uint32_t o = 32u * kk;
+              tc::umma_tf32<T2_IDESC>(d_tm, tc::sdesc_k_sw128(ah + o), tc::sdesc_k_sw128(bh + o), (c | kk) ? 1u : 0u);
+              tc::umma_tf32<T2_IDESC>(d_tm, tc::sdesc_k_sw128(ah + o), tc::sdesc_k_sw128(bl + o), 1u);
+              tc::umma_tf32<T2_IDESC>(d_tm, tc::sdesc_k_sw128(al + o), tc::sdesc_k_sw128(bh + o), 1u);
+            }
+            tc::umma_commit(&empty[s]);
           }
-          const float r0[4] = {re[0], re[1], re[2], re[3]}, r1[4] = {re[4], re[5], re[6], re[7]};
-          const float i0[4] = {im[0], im[1], im[2], im[3]}, i1[4] = {im[4], im[5], im[6], im[7]};
-          st_split4(hi, lo, tc::sw128_chunk(r, 2 * half + 0), r0);
-          st_split4(hi, lo, tc::sw128_chunk(r, 2 * half + 1), r1);
-          st_split4(hi, lo, tc::sw128_chunk(r, 4 + 2 * half + 0), i0);
-          st_split4(hi, lo, tc::sw128_chunk(r, 4 + 2 * half + 1), i1);
         }
-        tc::fence_async_smem();
-        tc::fence_before_sync();
-        if (__syncthreads_or(abort_flag)) {
-          stop = true;
+        if (!ok) {
+          atomicOr(err, 4);
+          *abort_v = 1;
           break;
         }
-        if (tid == 0) {
-          tc::fence_after_sync();
-          const uint32_t d_tm = tmem + (t & 1) * TC_N;
-          const uint32_t ah = tc::smem_u32(hi), al = tc::smem_u32(lo);
-          const uint32_t bh = tc::smem_u32(Bhi + c * TC_BTILE), bl = tc::smem_u32(Blo + c * TC_BTILE);
-#pragma unroll
-          for (int kk = 0; kk < 4; ++kk) {             // K = 8 tf32 = 32 bytes per MMA
-            const uint32_t o = 32u * kk;
-            tc::umma_tf32<TC_IDESC>(d_tm, tc::sdesc_k_sw128(ah + o), tc::sdesc_k_sw128(bh + o), (c | kk) ? 1u : 0u);
-            tc::umma_tf32<TC_IDESC>(d_tm, tc::sdesc_k_sw128(ah + o), tc::sdesc_k_sw128(bl + o), 1u);
-            tc::umma_tf32<TC_IDESC>(d_tm, tc::sdesc_k_sw128(al + o), tc::sdesc_k_sw128(bh + o), 1u);
+        tc::umma_commit(&tfull[buf]);
+        tc::umma_commit(&bempty[buf]);
+      }
+      tc::umma_commit(&done);                            // arrives once every MMA issued has completed
+      if (!tc::mbar_wait(&done, 0)) atomicOr(err, 4);
+    }
+    __syncwarp();
+  } else if (warp >= T2_EPI) {
+    // ---------------------------------------------------------------- builders
+    // Work items of a voxel: item 0 = this warp's share of B' (chunk/half pairs bw, bw + 8, ...),
+    // then the source chunks c = 0 .. nch - 1 of A'.  Each item's 8 field loads are issued one
+    // item ahead into registers (x).  Waits are made warp-uniform, so a warp's lanes always take
+    // the same path.
+    const int b = tid - 32 * T2_EPI, s = lane, gl = (b >> 5) & 3, half = b >> 7;
+    const int bw = b >> 5;                               // builder warp 0..7
+    uint32_t st_idx = 0;
+    int i = 0;
+    double2 x[8];
+    int64_t v = blockIdx.x;
+    if (v < a.nv && bw < 2 * L.nch) t2_load8(a, v, a.phiA, a.nd, lane, 16 * (bw >> 1) + 8 * (bw & 1), x);
+    bool fail = false;
+    for (; v < a.nv && !fail; v += gridDim.x, ++i) {
+      if (__any_sync(FULL, *abort_v != 0)) break;
+      const int buf = i & 1;
+      unsigned char *bb = sm + L.b_off + buf * L.nch * T2_BCH;
+      if (i >= 2 && !__all_sync(FULL, tc::mbar_wait(&bempty[buf], ((i >> 1) - 1) & 1))) {
+        fail = true;
+        break;
+      }
+      // B': row d = lane, chunk c = p / 2, harmonic half p % 2, for p = bw, bw + 8, ...
+      for (int p = bw; p < 2 * L.nch; p += T2_BLD) {
+        float re[8], im[8];
+        t2_cvt8(x, re, im);
+        const int pn = p + T2_BLD;
+        if (pn < 2 * L.nch) t2_load8(a, v, a.phiA, a.nd, lane, 16 * (pn >> 1) + 8 * (pn & 1), x);
+        else t2_load8(a, v, a.phi, a.ns, s, 8 * half, x);           // the first A' chunk
+        unsigned char *bh = bb + (p >> 1) * T2_BCH;
+        t2_store_row(bh, bh + 4096, lane, p & 1, re, im);
+      }
+      if (bw >= 2 * L.nch) t2_load8(a, v, a.phi, a.ns, s, 8 * half, x);
+      tc::fence_async_smem();                            // each lane's writes -> async proxy, then
+      __syncwarp();                                      // one arrival per warp
+      if (lane == 0) tc::mbar_arrive(&bfull[buf]);
+      // A' stages: chunk c, tile t -> row gl * 32 + s, harmonics 16 c + 8 half + 0..7
+      for (int c = 0; c < L.nch && !fail; ++c) {
+        float pr[8], pi[8];
+        t2_cvt8(x, pr, pi);
+        const int64_t vn = v + gridDim.x;
+        if (c + 1 < L.nch) t2_load8(a, v, a.phi, a.ns, s, 16 * (c + 1) + 8 * half, x);
+        else if (vn < a.nv && bw < 2 * L.nch) t2_load8(a, vn, a.phiA, a.nd, lane, 16 * (bw >> 1) + 8 * (bw & 1), x);
+        else if (vn < a.nv) t2_load8(a, vn, a.phi, a.ns, s, 8 * half, x);
+        for (int t = 0; t < L.ntile; ++t, ++st_idx) {
+          const uint32_t si = st_idx % T2_NST;
+          if (st_idx >= T2_NST && !__all_sync(FULL, tc::mbar_wait(&empty[si], ((st_idx / T2_NST) - 1) & 1))) {
+            fail = true;
+            break;
           }
-          tc::umma_commit(&bar_buf[b]);
-          if (c == L.nch - 1) tc::umma_commit(&bar_d[t & 1]);
-        }
-        ++q;
-        if (have_prev && c == (L.nch > 1 ? 1 : 0)) {   // the previous tile's MMAs are done by now
-          if (!epilogue(pt, pv, pm0, pw)) abort_flag = 1;
-          have_prev = false;
+          const float2 *cg = Ct + (4 * t + gl) * L.nkp + 16 * c + 8 * half;
+          float qr[8], qi[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const float2 cc = cg[j];
+            qr[j] = cc.x * pr[j] - cc.y * pi[j];
+            qi[j] = -(cc.x * pi[j] + cc.y * pr[j]);
+          }
+          unsigned char *hi = sm + L.a_off + si * T2_ASTAGE;
+          t2_store_row(hi, hi + 16384, gl * 32 + s, half, qr, qi);
+          tc::fence_async_smem();
+          __syncwarp();
+          if (lane == 0) tc::mbar_arrive(&full[si]);
         }
       }
-      if (stop) break;
-      have_prev = true;
-      pt = t;
-      pv = v;
-      pm0 = m0;
-      pw = wv;
-      ++t;
     }
-  }
-  if (!stop && have_prev) epilogue(pt, pv, pm0, pw);
-  // teardown: every MMA this CTA issued has completed (bounded) before the tensor memory is freed
-  if (q > 0 && tid == 0) {
-    const uint32_t last = q - 1;
-    tc::mbar_wait(&bar_buf[last & 1], (last >> 1) & 1);
-    if (q > 1) tc::mbar_wait(&bar_buf[(last - 1) & 1], ((last - 1) >> 1) & 1);
+    if (fail && lane == 0) {
+      atomicOr(err, 8);
+      *abort_v = 1;
+    }
+  } else {
+    // ---------------------------------------------------------------- epilogue
+    const int gl = warp, s = lane;
+    int i = 0;
+    for (int64_t v = blockIdx.x; v < a.nv; v += gridDim.x, ++i) {
+      if (__any_sync(FULL, *abort_v != 0)) break;
+      const int buf = i & 1;
+      bool ok = tc::mbar_wait(&tfull[buf], (i >> 1) & 1);
+      ok = __all_sync(FULL, ok);
+      if (!ok) {
+        if (lane == 0) {
+          atomicOr(err, 16);
+          *abort_v = 1;
+        }
+        break;
+      }
+      tc::fence_after_sync();
+      const float wv = (float)(a.w ? a.w[v] : 1.0);
+      for (int t = 0; t < L.ntile; ++t) {
+        uint32_t r[32];
+        tc::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(buf * 32 * L.ntile + 32 * t), r);
+        if (t == L.ntile - 1) {                          // the accumulators are read: release them
+          tc::fence_before_sync();
+          __syncwarp();
+          if (lane == 0) tc::mbar_arrive(&tempty[buf]);
+        }
+        const int g = 4 * t + gl;
+        if (g >= a.ng || s >= a.ns) continue;
+        float *row = Jtg + ((int64_t)v * a.ng + g) * a.nm;
+        if (dense == 2) {                                // m = s nd + d, nd and nm multiples of 4
+          float4 *dst = reinterpret_cast<float4 *>(row + s * a.nd);
+#pragma unroll
+          for (int d4 = 0; d4 < 8; ++d4)
+            if (4 * d4 < a.nd)
+              dst[d4] = make_float4(wv * __uint_as_float(r[4 * d4]), wv * __uint_as_float(r[4 * d4 + 1]),
+                                    wv * __uint_as_float(r[4 * d4 + 2]), wv * __uint_as_float(r[4 * d4 + 3]));
+        } else {
+#pragma unroll
+          for (int d = 0; d < 32; ++d) {
+            if (d >= a.nd) break;
+            const int m = dense ? s * a.nd + d : lk[s * 32 + d];
+            if (m < 0) continue;
+            float val = wv * __uint_as_float(r[d]);
+            if (rytov) val = val / (float)rytov[(int64_t)m * a.ng + g];
+            row[m] = val;
+          }
+        }
+      }
+    }
   }
   tc::fence_before_sync();
   __syncthreads();
-  if (warp == 0) tc::tmem_free(tmem, 2 * TC_N);
+  if (warp == T2_EPI + T2_BLD) tc::tmem_free(tmem, L.tcols);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -657,16 +755,17 @@ int launch_common(JArgs &a, size_t &smem, int &grid) {
 
 }  // namespace
 
-// 0 (auto): for each kernel the engine measured faster at the sensitivity configuration's
-//   shapes (100k voxels, 32 x 32 optodes, 64 harmonics, 20 gates, one B200): the TG Jacobian on
-//   the CUDA cores (20.0 ms; its tensor-core form, latency-bound in every phase with one CTA per
-//   SM, 42.5 ms), the vjp on the tensor cores (5.2 ms against 16.4 ms);
-// 1: both on the CUDA cores;  2: both on the tensor cores where their shapes fit
+// 0 (default) and 2: the tensor cores where the shapes fit (TG Jacobian: nodal basis, unique
+//   links, up to 32 sources and detectors, shared memory for the operand rings; vjp: up to 32
+//   sources and detectors), else the CUDA cores.  Measured at the sensitivity configuration
+//   (100k voxels, 32 x 32 optodes, 64 harmonics, 20 gates, one B200): TG Jacobian 11.9 ms
+//   against 20.0 ms, vjp 5.2 ms against 16.4 ms.
+// 1: both on the CUDA cores (cross-checks, timing)
 static int g_jacobian_engine = 0;
 
 int set_jacobian_engine(int engine) {
   DGP_REQUIRE(engine >= 0 && engine <= 2,
-              "jacobian engine must be 0 (auto), 1 (CUDA cores) or 2 (tensor cores where the shapes fit)");
+              "jacobian engine must be 0 (default), 1 (CUDA cores) or 2 (tensor cores where the shapes fit)");
   g_jacobian_engine = engine;
   return DGP_OK;
 }
@@ -685,13 +784,23 @@ int jacobian_run(int mode, const int32_t *prow, const int32_t *pcol, const doubl
   DGP_TRY(launch_common(a, smem, grid));
   // the link table addresses the staged fields in shared memory and P's columns address the
   // fields in HBM: both are checked before the first kernel uses them
+  // links_unique: every (s, d) pair at most once (the tensor-core epilogue writes each pair's
+  // entries from one accumulator row); links_dense: link m is (m / nd, m % nd) for all NS x ND
+  bool links_unique = ns <= 32 && nd <= 32, links_dense = nm == ns * nd;
   {
     std::vector<int32_t> hl(2 * (size_t)nm);
     DGP_CUDA(cudaMemcpyAsync(hl.data(), link, sizeof(int32_t) * 2 * nm, cudaMemcpyDeviceToHost, st));
     DGP_CUDA(cudaStreamSynchronize(st));
-    for (int m = 0; m < nm; ++m)
-      if (hl[2 * m] < 0 || hl[2 * m] >= ns || hl[2 * m + 1] < 0 || hl[2 * m + 1] >= nd)
-        return fail(DGP_ERR_ARG, "jacobian: link index out of range");
+    std::vector<char> seen(links_unique ? 32 * 32 : 0, 0);
+    for (int m = 0; m < nm; ++m) {
+      const int32_t s_ = hl[2 * m], d_ = hl[2 * m + 1];
+      if (s_ < 0 || s_ >= ns || d_ < 0 || d_ >= nd) return fail(DGP_ERR_ARG, "jacobian: link index out of range");
+      if (links_unique) {
+        if (seen[s_ * 32 + d_]) links_unique = false;
+        else seen[s_ * 32 + d_] = 1;
+      }
+      if (s_ != m / nd || d_ != m % nd) links_dense = false;
+    }
   }
   if (prow) {
     DGP_REQUIRE(pcol && pval, "jacobian: null basis column or value array");
@@ -706,16 +815,20 @@ int jacobian_run(int mode, const int32_t *prow, const int32_t *pcol, const doubl
   DGP_CHECK_LAUNCH();
   if (smem > 48 * 1024)
     DGP_CUDA(cudaFuncSetAttribute(k_jacobian_complex, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const TcLayout tl = tc_layout(nf, ns, nd);
+  const T2Layout tl = t2_layout(nf, std::max(1, ng));
   const size_t smem_tc = tl.bytes + 1024;
-  if (mode == 0 && g_jacobian_engine == 2 && smem_tc <= 227 * 1024) {
-    // tensor cores: one persistent CTA per SM
+  // (+ 1 KB of the kernel's own static shared memory)
+  const bool tc_fits = mode == 0 && !prow && links_unique && smem_tc + 1024 <= 227 * 1024;
+  if (tc_fits && g_jacobian_engine != 1) {
+    // tensor cores: one persistent warp-specialised CTA per SM
+    const int dense = !links_dense ? 0 : (!rytov && nd % 4 == 0 && nm % 4 == 0) ? 2 : 1;
     DevBuf flag;
     DGP_TRY(flag.alloc(sizeof(int)));
     DGP_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), st));
     DGP_CUDA(cudaFuncSetAttribute(k_jacobian_tg_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tc));
     const int gtc = (int)std::min<int64_t>(nv, (int64_t)sm_count());
-    k_jacobian_tg_tc<<<gtc, TC_THREADS, smem_tc, st>>>(a, ctab.as<float2>(), rytov, (float *)out, flag.as<int>());
+    k_jacobian_tg_tc<<<gtc, T2_THREADS, smem_tc, st>>>(a, ctab.as<float2>(), rytov, dense, (float *)out,
+                                                       flag.as<int>());
     DGP_CHECK_LAUNCH();
     int h = 0;
     DGP_CUDA(cudaMemcpyAsync(&h, flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -433,16 +433,16 @@ int dgp_jacobian_complex(const int32_t *d_P_rowptr, const int32_t *d_P_col,
 /* J_tg[v][g][m] float32 = Nt 2 Re sum_k conj(gate_fc[g][k]) J~[m][k][v]
  * (J~_0 = J_0/2), divided by d_data_tg[m][g] when that is not NULL (Rytov
  * normalisation).  1 <= ng <= 32.  Row v of the output is row v of J^T
- * with measurement index g*nm + m.  The DFT over harmonics runs on the CUDA
- * cores or, with dgp_set_jacobian_engine(2), on the tensor cores (tcgen05,
- * TF32 operands split in two so that three products keep FP32 accuracy)
- * when nf * (ns + nd) * 8 bytes of staged fields and the gate table fit one
- * block's shared memory. */
-/* Engines of dgp_jacobian_tg and dgp_jacobian_tg_vjp, process-wide: 0 (default,
- * auto) the TG Jacobian on the CUDA cores and the vjp on the tensor cores (the
- * faster of each pair, measured at 100k voxels x 1024 links x 64 harmonics x
- * 20 gates); 1 both on the CUDA cores; 2 both on the tensor cores where their
- * shapes fit (cross-checks, timing). */
+ * with measurement index g*nm + m.  The DFT over harmonics runs on the tensor
+ * cores (tcgen05: per voxel a GEMM over (gate, source) x detector with TF32
+ * operands split in two, so that three products keep FP32 accuracy) where the
+ * shapes fit (dgp_set_jacobian_engine), else on the CUDA cores. */
+/* Engines of dgp_jacobian_tg and dgp_jacobian_tg_vjp, process-wide: 0 (default)
+ * and 2 the tensor cores where the shapes fit, else the CUDA cores; 1 both on
+ * the CUDA cores (cross-checks, timing).  The tensor-core TG Jacobian takes the
+ * nodal basis (P = NULL), at most 32 sources and 32 detectors, each (source,
+ * detector) pair at most once in the link table, and NF, NG small enough for its
+ * operand rings in shared memory (NF = 64 with NG <= 24, for example). */
 int dgp_set_jacobian_engine(int32_t engine);
 int dgp_jacobian_tg(const int32_t *d_P_rowptr, const int32_t *d_P_col,
                     const double *d_P_val, int64_t nv, const double *d_w,

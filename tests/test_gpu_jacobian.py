@@ -154,7 +154,7 @@ def test_jacobian_rejects_bad_link_and_basis(jac_case):
 @pytest.fixture
 def cuda_core_engine():
     """use(e) selects the Jacobian engines (1 CUDA cores, 2 tensor cores where the shapes fit);
-    the default (0, auto) is restored after the test."""
+    the default (0) is restored after the test."""
     from dogpup_b200._lib import lib, check
 
     def use(engine):
@@ -164,13 +164,15 @@ def cuda_core_engine():
 
 
 @pytest.mark.parametrize("ns,nd,nf,ng,shuffle", [(32, 32, 64, 20, False), (7, 5, 33, 29, True),
-                                                 (13, 11, 17, 3, False), (9, 16, 80, 32, True)])
+                                                 (13, 11, 17, 3, False), (9, 16, 80, 32, True),
+                                                 (9, 16, 80, 12, True), (32, 32, 48, 24, True)])
 def test_tg_jacobian_tensor_cores_match_cuda_cores_and_oracle(ns, nd, nf, ng, shuffle, cuda_core_engine):
     """The tcgen05 TG Jacobian (3xTF32 split, FP32 accumulate in tensor memory) and the CUDA-core
     FP32 kernel, each against the FP64 oracle: link counts that are not multiples of the 128-link
-    tile (1024, 28, 143, 115), harmonic counts that are not multiples of the 16-harmonic chunk,
-    gate counts below and at the 32-column limit, and a shuffled, partial link table (not all
-    source-detector pairs, in no particular order).  Bar: 1e-5 norm-wise against the oracle (the
+    tile (1024, 28, 143, 115, 819), harmonic counts that are not multiples of the 16-harmonic
+    chunk, gate counts from 3 to 32, and shuffled, partial link tables (not all source-detector
+    pairs, in no particular order).  NF = 80 with 32 gates does not fit the tensor-core kernel's
+    shared memory, so engine 2 runs the CUDA-core kernel there too.  Bar: 1e-5 norm-wise against the oracle (the
     TG Jacobian's tolerance); between the engines 1e-5 per link, relative to the link's largest
     entry.  The vjp of both engines (the tensor-core one runs for up to 32 sources and detectors)
     against the oracle's J^T g, 1e-5.  (Without the Rytov division: early gates carry TG data
