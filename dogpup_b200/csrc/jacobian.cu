@@ -175,43 +175,57 @@ __global__ void __launch_bounds__(JBS) k_jacobian_tg(JArgs a, const float2 *__re
 }
 
 // ------------------------------------------------------------------------------------------
-// Time-gated Jacobian on the tensor cores (tcgen05, kind::tf32, 3xTF32 split), nodal basis.
+// Time-gated Jacobian on the tensor cores (tcgen05, kind::tf32, split operands), nodal basis.
 //
 // Per voxel v the DFT over harmonics is a real GEMM over the (gate, source) x detector block:
 //   J_tg[v][g][m(s,d)] = w_v Re sum_k Q[g,s,k] Pd[k][d],   Q[g,s,k] = C[g,k] Ps[k][s]
 //                      = w_v sum_K' A'[(g,s)][K'] B'[d][K']
 // with A' = [Re Q | -Im Q] and B' = [Re Pd | Im Pd] over K' = 2 NF, Ps / Pd the source and
-// detector fields at node v.  An MMA tile is M = 128 rows (4 gates x 32 sources) x N = 32
-// detectors, K' in chunks of 16 harmonics (one 128-byte row: [16 real | 16 imaginary]).  Of the
-// two ways to form the per-voxel operand this one builds NG x NS x NF products (the gate
-// coefficient times the source field) instead of NS x ND x NF (the field products per link),
-// and no MMA column is spent on padded gates.  FP32 values x enter as hi = tf32(x) and
-// lo = tf32(x - hi); each chunk issues hi*hi + hi*lo + lo*hi into an FP32 accumulator in tensor
-// memory (the lo*lo term, ~2^-22 relative, is dropped).
+// detector fields at node v.  An MMA tile is M = 128 rows (4 gates x 32 sources), K' in chunks
+// of 16 harmonics ([16 real | 16 imaginary]).  Of the two ways to form the per-voxel operand
+// this one builds NG x NS x NF products (the gate coefficient times the source field) instead
+// of NS x ND x NF (the field products per link), and no MMA column is spent on padded gates.
+//
+// Split operands: FP32 values x enter as hi = tf32(x) and lo = tf32(x - hi).  The B operand of
+// each MMA is the 64 rows [B'_hi ; B'_lo] (N = 64), so two MMAs per K step, A'_hi [B'_hi ; B'_lo]
+// and A'_lo [B'_hi ; B'_lo], leave (A'_hi + A'_lo) B'_hi in accumulator columns 0-31 and
+// (A'_hi + A'_lo) B'_lo in columns 32-63, which the epilogue adds.  A tf32 MMA of M = 128, K = 8
+// takes about the same time at N = 64 as at N = 32 on B200 (48 vs 46 cycles measured), so this
+// forms the three products of a 3xTF32 scheme (and lo x lo) in 2/3 of the MMAs.
+//
+// Data paths.  Shared-memory bandwidth bounded earlier forms of this kernel (the A' operand
+// written to shared memory and read back by every MMA: ~100 KB per stage), so here:
+//   - the A' stages go from the builders' registers straight into tensor memory (tcgen05.st;
+//     warp 4+q writes lanes 32q.. = the rows of gate 4t+q) and the MMAs read A' from there;
+//   - the fields of the next voxel are copied into shared memory by cp.async while the current
+//     one is built (completion counted on an mbarrier), and each builder keeps its source
+//     fields in registers for the whole voxel.
 //
 // Persistent CTA (one per SM), warp-specialised, all hand-offs through mbarriers:
-//   warps 0-3   epilogue: tensor memory -> w_v (and Rytov) scaling -> J (warp q reads the
-//               accumulator lanes 32q..32q+31 = gate 4t+q of tile t, lane = source)
-//   warps 4-11  builders: B' of the voxel (one chunk x 8 harmonics per warp, lane = detector),
-//               then the A' stages (lane = source, warp = gate within the tile x harmonic half);
-//               each work item's 8 field loads are issued one item ahead (register prefetch)
-//   warp 12     one thread issues the 12 MMAs of each stage; tensor-memory allocation
-// Rings: 4 A' stages (32 KB each), 2 B' buffers (one per voxel in flight), 2 accumulator sets
-// in tensor memory (32 NTILE columns each), so building voxel i+1, its MMAs and the epilogue of
-// voxel i overlap.  Every mbarrier wait is bounded: a timeout sets err, raises the abort flag
-// that every role polls, and the MMA thread waits (bounded) for all of its MMAs before the
-// tensor memory is freed.
+//   warps 0-3   epilogue: per tile, tensor memory -> hi + lo halves, w_v (and Rytov) -> J
+//               (warp q reads accumulator lanes 32q.. = gate 4t+q of tile t, lane = source)
+//   warps 4-11  builders: field copies, B'' rows (warp bw: harmonics 8 bw .. 8 bw + 7,
+//               lane = detector), A' stages tile by tile (lane = source, warp = gate within
+//               the tile x harmonic half)
+//   warp 12     one thread issues the MMAs (tile by tile: every chunk of a tile, after which
+//               its accumulator is complete); tensor-memory allocation
+// Tensor memory: 5 accumulator slots of 64 columns (a tile's slot is released as soon as the
+// epilogue has read it), then 3 A' stages of 64 columns (hi 0-31, lo 32-63).  Every mbarrier
+// wait is bounded: a timeout sets err, raises the abort flag that every role polls, and the
+// MMA thread waits (bounded) for all of its MMAs before the tensor memory is freed.
 constexpr int T2_EPI = 4, T2_BLD = 8;
 constexpr int T2_THREADS = 32 * (T2_EPI + T2_BLD + 1);
-constexpr int T2_NST = 4;                          // A' stages
-constexpr int T2_ASTAGE = 2 * 128 * 128;           // hi + lo of 128 rows x 128 B
-constexpr int T2_BCH = 2 * 32 * 128;               // one chunk of B': hi + lo of 32 rows x 128 B
-constexpr uint32_t T2_IDESC = tc::idesc(2, 2, 128, 32);
+constexpr int T2_BT = 32 * T2_BLD;                 // builder threads
+constexpr int T2_NSLOT = 5;                        // accumulator slots (64 columns each)
+constexpr int T2_NST = 3;                          // A' stages in tensor memory (64 columns each)
+constexpr uint32_t T2_ACOL = 64u * T2_NSLOT;       // first A' column
+constexpr int T2_BCH = 2 * 32 * 128;               // one chunk of B'': 32 hi rows, then 32 lo rows
+constexpr uint32_t T2_IDESC = tc::idesc(2, 2, 128, 64);
 
 struct T2Layout {
-  uint32_t a_off, b_off, c_off, l_off, bytes;      // from the 1 KB-aligned base
+  uint32_t b_off, f_off, c_off, l_off, bytes;      // shared memory, from the 1 KB-aligned base
+  uint32_t fbuf;                                   // bytes of one voxel's staged fields
   int nch, ntile, nkp;
-  uint32_t tcols;
 };
 
 __host__ __device__ inline T2Layout t2_layout(int nf, int ng) {
@@ -219,33 +233,25 @@ __host__ __device__ inline T2Layout t2_layout(int nf, int ng) {
   L.nch = (nf + 15) / 16;
   L.ntile = (ng + 3) / 4;
   L.nkp = 16 * L.nch;
-  L.a_off = 0;
-  L.b_off = T2_NST * T2_ASTAGE;
-  L.c_off = L.b_off + 2 * L.nch * T2_BCH;                        // gate table [4 NTILE][NKP] float2
+  L.fbuf = (uint32_t)(2 * 32 * 16 * L.nkp);                      // [2 fields][NKP][32] complex FP64
+  L.b_off = 0;
+  L.f_off = L.b_off + 2 * L.nch * T2_BCH;                        // two voxels' staged fields
+  L.c_off = L.f_off + 2 * L.fbuf;                                // gate table [4 NTILE][NKP] float2
   L.l_off = L.c_off + (uint32_t)(8 * 4 * L.ntile * L.nkp);        // link lookup [32][32] int
   L.bytes = L.l_off + 4 * 32 * 32;
-  uint32_t need = 2u * 32u * (uint32_t)L.ntile, cols = 32;
-  while (cols < need) cols <<= 1;
-  L.tcols = cols;
   return L;
 }
 
-// 8 harmonics k0 .. k0+7 of optode o of field f [nf][nn][cnt] at node v (zero past nf / cnt):
-// the loads, kept as FP64 until t2_cvt8 (so that they can be issued one work item ahead)
-__device__ inline void t2_load8(const JArgs &a, int64_t v, const double2 *__restrict__ f, int cnt, int o, int k0,
-                                double2 (&x)[8]) {
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int k = k0 + i;
-    x[i] = (o < cnt && k < a.nf) ? __ldg(f + ((int64_t)k * a.nn + v) * cnt + o) : make_double2(0.0, 0.0);
-  }
-}
-
-__device__ inline void t2_cvt8(const double2 (&x)[8], float (&re)[8], float (&im)[8]) {
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    re[i] = (float)x[i].x;
-    im[i] = (float)x[i].y;
+// cp.async copies of voxel v's fields into a staging buffer [2][NKP][32] (source, then detector;
+// zero past NF and past the optode counts): builder thread bt copies elements bt + 256 q
+__device__ inline void t2_stage_fields(const JArgs &a, int64_t v, int nkp, unsigned char *dst, int bt) {
+  const int per = nkp * 32;
+  for (int e = bt; e < 2 * per; e += T2_BT) {
+    const bool det = e >= per;
+    const int r = det ? e - per : e, k = r >> 5, o = r & 31, cnt = det ? a.nd : a.ns;
+    const double2 *f = det ? a.phiA : a.phi;
+    const bool ok = o < cnt && k < a.nf;
+    tc::cp_async16(dst + 16 * (size_t)e, ok ? f + ((int64_t)k * a.nn + v) * cnt + o : f, ok);
   }
 }
 
@@ -261,23 +267,12 @@ __device__ inline void st_split4(unsigned char *hi, unsigned char *lo, uint32_t 
   *reinterpret_cast<float4 *>(lo + off) = make_float4(l[0], l[1], l[2], l[3]);
 }
 
-// rows of a K-major 128-byte-swizzled split operand: 8 real values into chunks (2h, 2h+1), 8
-// imaginary into (4+2h, 5+2h) of row r
-__device__ inline void t2_store_row(unsigned char *hi, unsigned char *lo, int r, int h, const float (&re)[8],
-                                    const float (&im)[8]) {
-  const float r0[4] = {re[0], re[1], re[2], re[3]}, r1[4] = {re[4], re[5], re[6], re[7]};
-  const float i0[4] = {im[0], im[1], im[2], im[3]}, i1[4] = {im[4], im[5], im[6], im[7]};
-  st_split4(hi, lo, tc::sw128_chunk(r, 2 * h + 0), r0);
-  st_split4(hi, lo, tc::sw128_chunk(r, 2 * h + 1), r1);
-  st_split4(hi, lo, tc::sw128_chunk(r, 4 + 2 * h + 0), i0);
-  st_split4(hi, lo, tc::sw128_chunk(r, 4 + 2 * h + 1), i1);
-}
-
 __global__ void __launch_bounds__(T2_THREADS, 1) k_jacobian_tg_tc(JArgs a, const float2 *__restrict__ C /*[ng][nf]*/,
                                                                  const double *__restrict__ rytov, int dense,
                                                                  float *__restrict__ Jtg, int *err) {
   extern __shared__ __align__(1024) unsigned char t2_raw[];
-  __shared__ __align__(8) uint64_t full[T2_NST], empty[T2_NST], bfull[2], bempty[2], tfull[2], tempty[2], done;
+  __shared__ __align__(8) uint64_t full[T2_NST], empty[T2_NST], bfull[2], bempty[2], fready[2], fdone[2];
+  __shared__ __align__(8) uint64_t tfull[T2_NSLOT], tempty[T2_NSLOT], done;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
   unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(t2_raw) + 1023) & ~uintptr_t(1023));
@@ -296,14 +291,18 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_jacobian_tg_tc(JArgs a, const
     for (int b = 0; b < 2; ++b) {
       tc::mbar_init(&bfull[b], T2_BLD);
       tc::mbar_init(&bempty[b], 1);
-      tc::mbar_init(&tfull[b], 1);
-      tc::mbar_init(&tempty[b], T2_EPI);
+      tc::mbar_init(&fready[b], T2_BT);                // one cp.async arrival per builder thread
+      tc::mbar_init(&fdone[b], T2_BLD);
+    }
+    for (int q = 0; q < T2_NSLOT; ++q) {
+      tc::mbar_init(&tfull[q], 1);
+      tc::mbar_init(&tempty[q], T2_EPI);
     }
     tc::mbar_init(&done, 1);
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == T2_EPI + T2_BLD) tc::tmem_alloc(&tmem_slot, L.tcols);
+  if (warp == T2_EPI + T2_BLD) tc::tmem_alloc(&tmem_slot, 512);
   for (int t = tid; t < 4 * L.ntile * L.nkp; t += T2_THREADS) {
     const int g = t / L.nkp, k = t % L.nkp;
     Ct[t] = (g < a.ng && k < a.nf) ? C[g * a.nf + k] : make_float2(0.f, 0.f);
@@ -320,44 +319,45 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_jacobian_tg_tc(JArgs a, const
   if (warp == T2_EPI + T2_BLD) {
     // ---------------------------------------------------------------- MMA issue (one thread)
     if (lane == 0) {
-      uint32_t st_idx = 0;
+      uint32_t st_idx = 0, tl_idx = 0;
       int i = 0;
-      for (int64_t v = blockIdx.x; v < a.nv; v += gridDim.x, ++i) {
+      bool ok = true;
+      for (int64_t v = blockIdx.x; v < a.nv && ok; v += gridDim.x, ++i) {
         if (*abort_v) break;
         const int buf = i & 1;
-        bool ok = tc::mbar_wait(&bfull[buf], (i >> 1) & 1);
-        if (ok && i >= 2) ok = tc::mbar_wait(&tempty[buf], ((i >> 1) - 1) & 1);
+        ok = tc::mbar_wait(&bfull[buf], (i >> 1) & 1);
         tc::fence_after_sync();
-        const uint32_t dbase = tmem + (uint32_t)(buf * 32 * L.ntile);
-        const unsigned char *bb = sm + L.b_off + buf * L.nch * T2_BCH;
-        for (int c = 0; c < L.nch && ok; ++c) {
-          const uint32_t bh = tc::smem_u32(bb + c * T2_BCH), bl = bh + 4096;
-          for (int t = 0; t < L.ntile; ++t, ++st_idx) {
+        // B'' descriptors: one per chunk, K steps of 32 bytes = +2 in the descriptor's address field
+        const uint64_t bdesc0 = tc::sdesc_k_sw128(tc::smem_u32(sm + L.b_off + buf * L.nch * T2_BCH));
+        for (int t = 0; t < L.ntile && ok; ++t, ++tl_idx) {
+          const uint32_t slot = tl_idx % T2_NSLOT, use = tl_idx / T2_NSLOT;
+          if (use >= 1) ok = tc::mbar_wait(&tempty[slot], (use - 1) & 1);   // the epilogue has read it
+          tc::fence_after_sync();
+          const uint32_t d_tm = tmem + 64u * slot;
+          for (int c = 0; c < L.nch && ok; ++c) {
             const uint32_t s = st_idx % T2_NST;
-            if (!tc::mbar_wait(&full[s], (st_idx / T2_NST) & 1)) {
-              ok = false;
-              break;
-            }
+            ok = tc::mbar_wait(&full[s], (st_idx / T2_NST) & 1);
+            if (!ok) break;
             tc::fence_after_sync();
-            const uint32_t ah = tc::smem_u32(sm + L.a_off + s * T2_ASTAGE), al = ah + 16384;
-            const uint32_t d_tm = dbase + 32u * t;
+            const uint32_t ah = tmem + T2_ACOL + 64u * s, al = ah + 32u;    // A' in tensor memory
+            const uint64_t bd = bdesc0 + (uint64_t)((c * T2_BCH) >> 4);    // B'' = [hi ; lo] rows
+            tc::umma_tf32_ts<T2_IDESC>(d_tm, ah, bd, c ? 1u : 0u);
+            tc::umma_tf32_ts<T2_IDESC>(d_tm, al, bd, 1u);
 #pragma unroll
-            for (int kk = 0; kk < 4; ++kk) {           // K = 8 tf32 = 32 bytes per MMA
-              const uint32_t o = 32u * kk;
-              tc::umma_tf32<T2_IDESC>(d_tm, tc::sdesc_k_sw128(ah + o), tc::sdesc_k_sw128(bh + o), (c | kk) ? 1u : 0u);
-              tc::umma_tf32<T2_IDESC>(d_tm, tc::sdesc_k_sw128(ah + o), tc::sdesc_k_sw128(bl + o), 1u);
-              tc::umma_tf32<T2_IDESC>(d_tm, tc::sdesc_k_sw128(al + o), tc::sdesc_k_sw128(bh + o), 1u);
+            for (int kk = 1; kk < 4; ++kk) {           // K = 8 tf32: 8 columns of A', 32 bytes of B''
+              tc::umma_tf32_ts<T2_IDESC>(d_tm, ah + 8u * kk, bd + 2u * kk, 1u);
+              tc::umma_tf32_ts<T2_IDESC>(d_tm, al + 8u * kk, bd + 2u * kk, 1u);
             }
             tc::umma_commit(&empty[s]);
+            ++st_idx;
           }
+          if (ok) tc::umma_commit(&tfull[slot]);
         }
-        if (!ok) {
-          atomicOr(err, 4);
-          *abort_v = 1;
-          break;
-        }
-        tc::umma_commit(&tfull[buf]);
-        tc::umma_commit(&bempty[buf]);
+        if (ok) tc::umma_commit(&bempty[buf]);
+      }
+      if (!ok) {
+        atomicOr(err, 4);
+        *abort_v = 1;
       }
       tc::umma_commit(&done);                            // arrives once every MMA issued has completed
       if (!tc::mbar_wait(&done, 0)) atomicOr(err, 4);
@@ -365,70 +365,106 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_jacobian_tg_tc(JArgs a, const
     __syncwarp();
   } else if (warp >= T2_EPI) {
     // ---------------------------------------------------------------- builders
-    // Work items of a voxel: item 0 = this warp's share of B' (chunk/half pairs bw, bw + 8, ...),
-    // then the source chunks c = 0 .. nch - 1 of A'.  Each item's 8 field loads are issued one
-    // item ahead into registers (x).  Waits are made warp-uniform, so a warp's lanes always take
-    // the same path.
-    const int b = tid - 32 * T2_EPI, s = lane, gl = (b >> 5) & 3, half = b >> 7;
-    const int bw = b >> 5;                               // builder warp 0..7
+    // Per voxel i (staging buffer i % 2): copy voxel i+1's fields into the other buffer once
+    // every builder has read voxel i-1's (fdone), wait for voxel i's copies (fready), then
+    // B'' rows from the detector fields of this warp's block (k = 8 bw .. 8 bw + 7, d = lane)
+    // and this thread's source fields into registers (harmonics 16 c + 8 half + j), then the A'
+    // stages tile by tile into tensor memory.  Waits are warp-uniform.
+    const int bt = tid - 32 * T2_EPI, bw = bt >> 5, gl = bw & 3, half = bw >> 2, s = lane;
+    unsigned char *fst = sm + L.f_off;
+    int64_t v = blockIdx.x;
+    if (v < a.nv) t2_stage_fields(a, v, L.nkp, fst, bt);
+    tc::cp_async_arrive(&fready[0]);
     uint32_t st_idx = 0;
     int i = 0;
-    double2 x[8];
-    int64_t v = blockIdx.x;
-    if (v < a.nv && bw < 2 * L.nch) t2_load8(a, v, a.phiA, a.nd, lane, 16 * (bw >> 1) + 8 * (bw & 1), x);
     bool fail = false;
     for (; v < a.nv && !fail; v += gridDim.x, ++i) {
       if (__any_sync(FULL, *abort_v != 0)) break;
       const int buf = i & 1;
-      unsigned char *bb = sm + L.b_off + buf * L.nch * T2_BCH;
-      if (i >= 2 && !__all_sync(FULL, tc::mbar_wait(&bempty[buf], ((i >> 1) - 1) & 1))) {
+      const int64_t vn = v + gridDim.x;
+      if (vn < a.nv) {
+        if (i >= 1 && !__all_sync(FULL, tc::mbar_wait(&fdone[buf ^ 1], ((i - 1) >> 1) & 1))) {
+          fail = true;
+          break;
+        }
+        t2_stage_fields(a, vn, L.nkp, fst + (buf ^ 1) * L.fbuf, bt);
+        tc::cp_async_arrive(&fready[buf ^ 1]);
+      }
+      if (!__all_sync(FULL, tc::mbar_wait(&fready[buf], (i >> 1) & 1)) ||
+          (i >= 2 && !__all_sync(FULL, tc::mbar_wait(&bempty[buf], ((i >> 1) - 1) & 1)))) {
         fail = true;
         break;
       }
-      // B': row d = lane, chunk c = p / 2, harmonic half p % 2, for p = bw, bw + 8, ...
-      for (int p = bw; p < 2 * L.nch; p += T2_BLD) {
+      const double2 *fs = reinterpret_cast<const double2 *>(fst + buf * L.fbuf), *fd = fs + L.nkp * 32;
+      unsigned char *bb = sm + L.b_off + buf * L.nch * T2_BCH;
+      if (bw < 2 * L.nch) {
         float re[8], im[8];
-        t2_cvt8(x, re, im);
-        const int pn = p + T2_BLD;
-        if (pn < 2 * L.nch) t2_load8(a, v, a.phiA, a.nd, lane, 16 * (pn >> 1) + 8 * (pn & 1), x);
-        else t2_load8(a, v, a.phi, a.ns, s, 8 * half, x);           // the first A' chunk
-        unsigned char *bh = bb + (p >> 1) * T2_BCH;
-        t2_store_row(bh, bh + 4096, lane, p & 1, re, im);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const double2 y = fd[(8 * bw + j) * 32 + lane];
+          re[j] = (float)y.x;
+          im[j] = (float)y.y;
+        }
+        unsigned char *bh = bb + (bw >> 1) * T2_BCH;
+        const float r0[4] = {re[0], re[1], re[2], re[3]}, r1[4] = {re[4], re[5], re[6], re[7]};
+        const float i0[4] = {im[0], im[1], im[2], im[3]}, i1[4] = {im[4], im[5], im[6], im[7]};
+        const int h = bw & 1;                            // hi rows 0-31, lo rows 32-63
+        st_split4(bh, bh + 4096, tc::sw128_chunk(lane, 2 * h + 0), r0);
+        st_split4(bh, bh + 4096, tc::sw128_chunk(lane, 2 * h + 1), r1);
+        st_split4(bh, bh + 4096, tc::sw128_chunk(lane, 4 + 2 * h + 0), i0);
+        st_split4(bh, bh + 4096, tc::sw128_chunk(lane, 4 + 2 * h + 1), i1);
       }
-      if (bw >= 2 * L.nch) t2_load8(a, v, a.phi, a.ns, s, 8 * half, x);
-      tc::fence_async_smem();                            // each lane's writes -> async proxy, then
-      __syncwarp();                                      // one arrival per warp
-      if (lane == 0) tc::mbar_arrive(&bfull[buf]);
-      // A' stages: chunk c, tile t -> row gl * 32 + s, harmonics 16 c + 8 half + 0..7
-      for (int c = 0; c < L.nch && !fail; ++c) {
-        float pr[8], pi[8];
-        t2_cvt8(x, pr, pi);
-        const int64_t vn = v + gridDim.x;
-        if (c + 1 < L.nch) t2_load8(a, v, a.phi, a.ns, s, 16 * (c + 1) + 8 * half, x);
-        else if (vn < a.nv && bw < 2 * L.nch) t2_load8(a, vn, a.phiA, a.nd, lane, 16 * (bw >> 1) + 8 * (bw & 1), x);
-        else if (vn < a.nv) t2_load8(a, vn, a.phi, a.ns, s, 8 * half, x);
-        for (int t = 0; t < L.ntile; ++t, ++st_idx) {
+      float pr[4][8], pi[4][8];
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const double2 y = c < L.nch ? fs[(16 * c + 8 * half + j) * 32 + s] : make_double2(0.0, 0.0);
+          pr[c][j] = (float)y.x;
+          pi[c][j] = (float)y.y;
+        }
+      tc::fence_async_smem();                            // B'' -> async proxy
+      __syncwarp();
+      if (lane == 0) {
+        tc::mbar_arrive(&bfull[buf]);
+        tc::mbar_arrive(&fdone[buf]);
+      }
+      for (int t = 0; t < L.ntile && !fail; ++t) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          if (c >= L.nch || fail) break;
           const uint32_t si = st_idx % T2_NST;
           if (st_idx >= T2_NST && !__all_sync(FULL, tc::mbar_wait(&empty[si], ((st_idx / T2_NST) - 1) & 1))) {
             fail = true;
             break;
           }
+          tc::fence_after_sync();                        // after the MMAs that read this stage
           const float2 *cg = Ct + (4 * t + gl) * L.nkp + 16 * c + 8 * half;
-          float qr[8], qi[8];
+          float hr[8], lr[8], hm[8], lm[8];
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
             const float2 cc = cg[j];
-            qr[j] = cc.x * pr[j] - cc.y * pi[j];
-            qi[j] = -(cc.x * pi[j] + cc.y * pr[j]);
+            const float qr = cc.x * pr[c][j] - cc.y * pi[c][j], qi = -(cc.x * pi[c][j] + cc.y * pr[c][j]);
+            hr[j] = tc::to_tf32(qr);
+            lr[j] = tc::to_tf32(qr - hr[j]);
+            hm[j] = tc::to_tf32(qi);
+            lm[j] = tc::to_tf32(qi - hm[j]);
           }
-          unsigned char *hi = sm + L.a_off + si * T2_ASTAGE;
-          t2_store_row(hi, hi + 16384, gl * 32 + s, half, qr, qi);
-          tc::fence_async_smem();
+          // row gl * 32 + s = lane s of this warp's quadrant; K' = 8 half + j (real), 16 + 8 half + j
+          const uint32_t tq = tmem + ((uint32_t)(32 * gl) << 16) + T2_ACOL + 64u * si + 8u * half;
+          tc::tmem_st8(tq, hr);
+          tc::tmem_st8(tq + 16u, hm);
+          tc::tmem_st8(tq + 32u, lr);
+          tc::tmem_st8(tq + 48u, lm);
+          tc::tmem_wait_st();                            // the stores have landed, then
+          tc::fence_before_sync();                       // ordered before the arrival
           __syncwarp();
           if (lane == 0) tc::mbar_arrive(&full[si]);
+          ++st_idx;
         }
       }
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");    // no copy outlives the kernel
     if (fail && lane == 0) {
       atomicOr(err, 8);
       *abort_v = 1;
@@ -436,29 +472,29 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_jacobian_tg_tc(JArgs a, const
   } else {
     // ---------------------------------------------------------------- epilogue
     const int gl = warp, s = lane;
-    int i = 0;
-    for (int64_t v = blockIdx.x; v < a.nv; v += gridDim.x, ++i) {
+    uint32_t tl_idx = 0;
+    bool ok = true;
+    for (int64_t v = blockIdx.x; v < a.nv && ok; v += gridDim.x) {
       if (__any_sync(FULL, *abort_v != 0)) break;
-      const int buf = i & 1;
-      bool ok = tc::mbar_wait(&tfull[buf], (i >> 1) & 1);
-      ok = __all_sync(FULL, ok);
-      if (!ok) {
-        if (lane == 0) {
-          atomicOr(err, 16);
-          *abort_v = 1;
-        }
-        break;
-      }
-      tc::fence_after_sync();
       const float wv = (float)(a.w ? a.w[v] : 1.0);
-      for (int t = 0; t < L.ntile; ++t) {
-        uint32_t r[32];
-        tc::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(buf * 32 * L.ntile + 32 * t), r);
-        if (t == L.ntile - 1) {                          // the accumulators are read: release them
-          tc::fence_before_sync();
-          __syncwarp();
-          if (lane == 0) tc::mbar_arrive(&tempty[buf]);
+      for (int t = 0; t < L.ntile; ++t, ++tl_idx) {
+        const uint32_t slot = tl_idx % T2_NSLOT, use = tl_idx / T2_NSLOT;
+        ok = __all_sync(FULL, tc::mbar_wait(&tfull[slot], use & 1));
+        if (!ok) {
+          if (lane == 0) {
+            atomicOr(err, 16);
+            *abort_v = 1;
+          }
+          break;
         }
+        tc::fence_after_sync();
+        uint32_t r[32], q[32];
+        const uint32_t ta = tmem + ((uint32_t)(32 * warp) << 16) + 64u * slot;
+        tc::tmem_ld32(ta, r);                            // (A_hi + A_lo) B_hi
+        tc::tmem_ld32(ta + 32u, q);                      // (A_hi + A_lo) B_lo
+        tc::fence_before_sync();
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&tempty[slot]);
         const int g = 4 * t + gl;
         if (g >= a.ng || s >= a.ns) continue;
         float *row = Jtg + ((int64_t)v * a.ng + g) * a.nm;
@@ -466,16 +502,20 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_jacobian_tg_tc(JArgs a, const
           float4 *dst = reinterpret_cast<float4 *>(row + s * a.nd);
 #pragma unroll
           for (int d4 = 0; d4 < 8; ++d4)
-            if (4 * d4 < a.nd)
-              dst[d4] = make_float4(wv * __uint_as_float(r[4 * d4]), wv * __uint_as_float(r[4 * d4 + 1]),
-                                    wv * __uint_as_float(r[4 * d4 + 2]), wv * __uint_as_float(r[4 * d4 + 3]));
+            if (4 * d4 < a.nd) {
+              const int d = 4 * d4;
+              dst[d4] = make_float4(wv * (__uint_as_float(r[d]) + __uint_as_float(q[d])),
+                                    wv * (__uint_as_float(r[d + 1]) + __uint_as_float(q[d + 1])),
+                                    wv * (__uint_as_float(r[d + 2]) + __uint_as_float(q[d + 2])),
+                                    wv * (__uint_as_float(r[d + 3]) + __uint_as_float(q[d + 3])));
+            }
         } else {
 #pragma unroll
           for (int d = 0; d < 32; ++d) {
             if (d >= a.nd) break;
             const int m = dense ? s * a.nd + d : lk[s * 32 + d];
             if (m < 0) continue;
-            float val = wv * __uint_as_float(r[d]);
+            float val = wv * (__uint_as_float(r[d]) + __uint_as_float(q[d]));
             if (rytov) val = val / (float)rytov[(int64_t)m * a.ng + g];
             row[m] = val;
           }
@@ -485,7 +525,7 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_jacobian_tg_tc(JArgs a, const
   }
   tc::fence_before_sync();
   __syncthreads();
-  if (warp == T2_EPI + T2_BLD) tc::tmem_free(tmem, L.tcols);
+  if (warp == T2_EPI + T2_BLD) tc::tmem_free(tmem, 512);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -818,7 +858,7 @@ int jacobian_run(int mode, const int32_t *prow, const int32_t *pcol, const doubl
   const T2Layout tl = t2_layout(nf, std::max(1, ng));
   const size_t smem_tc = tl.bytes + 1024;
   // (+ 1 KB of the kernel's own static shared memory)
-  const bool tc_fits = mode == 0 && !prow && links_unique && smem_tc + 1024 <= 227 * 1024;
+  const bool tc_fits = mode == 0 && !prow && links_unique && nf <= 64 && smem_tc + 1024 <= 227 * 1024;
   if (tc_fits && g_jacobian_engine != 1) {
     // tensor cores: one persistent warp-specialised CTA per SM
     const int dense = !links_dense ? 0 : (!rytov && nd % 4 == 0 && nm % 4 == 0) ? 2 : 1;

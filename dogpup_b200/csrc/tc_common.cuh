@@ -91,6 +91,17 @@ __device__ inline void umma_tf32(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc
       : "memory");
 }
 
+// D (tensor memory) += A (tensor memory: M rows = lanes, K along columns) x B (shared memory)
+template <uint32_t IDESC>
+__device__ inline void umma_tf32_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc, uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "r"(a_tmem), "l"(bdesc), "r"(IDESC), "r"(accum)
+      : "memory");
+}
+
 // arrive on `bar` once every tcgen05.mma issued so far by this thread has completed
 __device__ inline void umma_commit(uint64_t *bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
@@ -136,6 +147,27 @@ __device__ inline void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
         "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// warp-collective: each lane writes 8 consecutive 32-bit columns of its own lane at taddr
+// (lanes 32 (warp % 4) ..); tmem_wait_st() before the values are handed to the tensor core
+__device__ inline void tmem_st8(uint32_t taddr, const float (&v)[8]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr),
+               "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+               "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+               "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7]))
+               : "memory");
+}
+__device__ inline void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// 16-byte global -> shared copy (zero-filled when !pred; src must still be a valid address)
+__device__ inline void cp_async16(void *dst, const void *src, bool pred) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(pred ? 16 : 0)
+               : "memory");
+}
+// arrive on `bar` (without raising its expected count) once this thread's earlier cp.async copies land
+__device__ inline void cp_async_arrive(uint64_t *bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 // round to TF32 (10 explicit mantissa bits, to nearest, ties away), kept in an FP32 register
