@@ -209,15 +209,17 @@ __global__ void __launch_bounds__(JBS) k_jacobian_tg(JArgs a, const float2 *__re
 //               the tile x harmonic half)
 //   warp 12     one thread issues the MMAs (tile by tile: every chunk of a tile, after which
 //               its accumulator is complete); tensor-memory allocation
-// Tensor memory: 5 accumulator slots of 64 columns (a tile's slot is released as soon as the
-// epilogue has read it), then 3 A' stages of 64 columns (hi 0-31, lo 32-63).  Every mbarrier
+// Tensor memory: 4 accumulator slots of 64 columns (a tile's slot is released as soon as the
+// epilogue has read it), then 2 A' stages of two chunks each (128 columns: hi 0-63, lo 64-127),
+// so the MMA thread waits once per 16 MMAs (an mbarrier wait right after a burst of MMAs costs
+// a few hundred cycles on B200).  Every mbarrier
 // wait is bounded: a timeout sets err, raises the abort flag that every role polls, and the
 // MMA thread waits (bounded) for all of its MMAs before the tensor memory is freed.
 constexpr int T2_EPI = 4, T2_BLD = 8;
 constexpr int T2_THREADS = 32 * (T2_EPI + T2_BLD + 1);
 constexpr int T2_BT = 32 * T2_BLD;                 // builder threads
-constexpr int T2_NSLOT = 5;                        // accumulator slots (64 columns each)
-constexpr int T2_NST = 3;                          // A' stages in tensor memory (64 columns each)
+constexpr int T2_NSLOT = 4;                        // accumulator slots (64 columns each)
+constexpr int T2_NST = 2;                          // A' stages in tensor memory (2 chunks, 128 columns each)
 constexpr uint32_t T2_ACOL = 64u * T2_NSLOT;       // first A' column
 constexpr int T2_BCH = 2 * 32 * 128;               // one chunk of B'': 32 hi rows, then 32 lo rows
 constexpr uint32_t T2_IDESC = tc::idesc(2, 2, 128, 64);
@@ -334,19 +336,22 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_jacobian_tg_tc(JArgs a, const
           if (use >= 1) ok = tc::mbar_wait(&tempty[slot], (use - 1) & 1);   // the epilogue has read it
           tc::fence_after_sync();
           const uint32_t d_tm = tmem + 64u * slot;
-          for (int c = 0; c < L.nch && ok; ++c) {
+          for (int c0 = 0; c0 < L.nch && ok; c0 += 2) {   // a stage = chunks c0, c0 + 1
             const uint32_t s = st_idx % T2_NST;
             ok = tc::mbar_wait(&full[s], (st_idx / T2_NST) & 1);
             if (!ok) break;
             tc::fence_after_sync();
-            const uint32_t ah = tmem + T2_ACOL + 64u * s, al = ah + 32u;    // A' in tensor memory
-            const uint64_t bd = bdesc0 + (uint64_t)((c * T2_BCH) >> 4);    // B'' = [hi ; lo] rows
-            tc::umma_tf32_ts<T2_IDESC>(d_tm, ah, bd, c ? 1u : 0u);
-            tc::umma_tf32_ts<T2_IDESC>(d_tm, al, bd, 1u);
+            for (int cc = 0; cc < 2 && c0 + cc < L.nch; ++cc) {
+              const int c = c0 + cc;
+              const uint32_t ah = tmem + T2_ACOL + 128u * s + 32u * cc, al = ah + 64u;   // A' in tensor memory
+              const uint64_t bd = bdesc0 + (uint64_t)((c * T2_BCH) >> 4);             // B'' = [hi ; lo] rows
+              tc::umma_tf32_ts<T2_IDESC>(d_tm, ah, bd, c ? 1u : 0u);
+              tc::umma_tf32_ts<T2_IDESC>(d_tm, al, bd, 1u);
 #pragma unroll
-            for (int kk = 1; kk < 4; ++kk) {           // K = 8 tf32: 8 columns of A', 32 bytes of B''
-              tc::umma_tf32_ts<T2_IDESC>(d_tm, ah + 8u * kk, bd + 2u * kk, 1u);
-              tc::umma_tf32_ts<T2_IDESC>(d_tm, al + 8u * kk, bd + 2u * kk, 1u);
+              for (int kk = 1; kk < 4; ++kk) {         // K = 8 tf32: 8 columns of A', 32 bytes of B''
+                tc::umma_tf32_ts<T2_IDESC>(d_tm, ah + 8u * kk, bd + 2u * kk, 1u);
+                tc::umma_tf32_ts<T2_IDESC>(d_tm, al + 8u * kk, bd + 2u * kk, 1u);
+              }
             }
             tc::umma_commit(&empty[s]);
             ++st_idx;
@@ -431,31 +436,37 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_jacobian_tg_tc(JArgs a, const
       }
       for (int t = 0; t < L.ntile && !fail; ++t) {
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          if (c >= L.nch || fail) break;
+        for (int c0 = 0; c0 < 4; c0 += 2) {             // a stage = chunks c0, c0 + 1
+          if (c0 >= L.nch || fail) break;
           const uint32_t si = st_idx % T2_NST;
           if (st_idx >= T2_NST && !__all_sync(FULL, tc::mbar_wait(&empty[si], ((st_idx / T2_NST) - 1) & 1))) {
             fail = true;
             break;
           }
           tc::fence_after_sync();                        // after the MMAs that read this stage
-          const float2 *cg = Ct + (4 * t + gl) * L.nkp + 16 * c + 8 * half;
-          float hr[8], lr[8], hm[8], lm[8];
 #pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            const float2 cc = cg[j];
-            const float qr = cc.x * pr[c][j] - cc.y * pi[c][j], qi = -(cc.x * pi[c][j] + cc.y * pr[c][j]);
-            hr[j] = tc::to_tf32(qr);
-            lr[j] = tc::to_tf32(qr - hr[j]);
-            hm[j] = tc::to_tf32(qi);
-            lm[j] = tc::to_tf32(qi - hm[j]);
+          for (int cc = 0; cc < 2; ++cc) {
+            const int c = c0 + cc;
+            if (c >= L.nch) break;
+            const float2 *cg = Ct + (4 * t + gl) * L.nkp + 16 * c + 8 * half;
+            float hr[8], lr[8], hm[8], lm[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              const float2 q = cg[j];
+              const float qr = q.x * pr[c][j] - q.y * pi[c][j], qi = -(q.x * pi[c][j] + q.y * pr[c][j]);
+              hr[j] = tc::to_tf32(qr);
+              lr[j] = tc::to_tf32(qr - hr[j]);
+              hm[j] = tc::to_tf32(qi);
+              lm[j] = tc::to_tf32(qi - hm[j]);
+            }
+            // row gl * 32 + s = lane s of this warp's quadrant; chunk cc of the stage: K' = 8 half + j
+            // (real), 16 + 8 half + j (imaginary); lo 64 columns after hi
+            const uint32_t tq = tmem + ((uint32_t)(32 * gl) << 16) + T2_ACOL + 128u * si + 32u * cc + 8u * half;
+            tc::tmem_st8(tq, hr);
+            tc::tmem_st8(tq + 16u, hm);
+            tc::tmem_st8(tq + 64u, lr);
+            tc::tmem_st8(tq + 80u, lm);
           }
-          // row gl * 32 + s = lane s of this warp's quadrant; K' = 8 half + j (real), 16 + 8 half + j
-          const uint32_t tq = tmem + ((uint32_t)(32 * gl) << 16) + T2_ACOL + 64u * si + 8u * half;
-          tc::tmem_st8(tq, hr);
-          tc::tmem_st8(tq + 16u, hm);
-          tc::tmem_st8(tq + 32u, lr);
-          tc::tmem_st8(tq + 48u, lm);
           tc::tmem_wait_st();                            // the stores have landed, then
           tc::fence_before_sync();                       // ordered before the arrival
           __syncwarp();
