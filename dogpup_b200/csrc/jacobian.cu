@@ -203,24 +203,24 @@ __global__ void __launch_bounds__(JBS) k_jacobian_tg(JArgs a, const float2 *__re
 //
 // Persistent CTA (one per SM), warp-specialised, all hand-offs through mbarriers:
 //   warps 0-3   epilogue: per tile, tensor memory -> hi + lo halves, w_v (and Rytov) -> J
-//               (warp q reads accumulator lanes 32q.. = gate 4t+q of tile t, lane = source);
-//               and B'' of the next voxel (lane = detector), so that the MMAs of a new voxel
-//               do not wait for it
+//               (warp q reads accumulator lanes 32q.. = gate 4t+q of tile t, lane = source)
 //   warps 4-11  builders: field copies, A' stages tile by tile (lane = source, warp = gate
 //               within the tile x harmonic half)
 //   warp 12     one thread issues the MMAs (tile by tile: every chunk of a tile, after which
 //               its accumulator is complete); tensor-memory allocation
-// Tensor memory: 4 accumulator slots of 64 columns (a tile's slot is released as soon as the
-// epilogue has read it), then 2 A' stages of two chunks each (128 columns: hi 0-63, lo 64-127),
+//   warps 13-14 B'' of each voxel as soon as its fields are staged (lane = detector), ahead of
+//               the MMAs that need it
+// Tensor memory: 2 accumulator slots of 64 columns (a tile's slot is released as soon as the
+// epilogue has read it), then 3 A' stages of two chunks each (128 columns: hi 0-63, lo 64-127),
 // so the MMA thread waits once per 16 MMAs (an mbarrier wait right after a burst of MMAs costs
 // a few hundred cycles on B200).  Every mbarrier
 // wait is bounded: a timeout sets err, raises the abort flag that every role polls, and the
 // MMA thread waits (bounded) for all of its MMAs before the tensor memory is freed.
-constexpr int T2_EPI = 4, T2_BLD = 8;
-constexpr int T2_THREADS = 32 * (T2_EPI + T2_BLD + 1);
+constexpr int T2_EPI = 4, T2_BLD = 8, T2_BB = 2;    // epilogue, A' builder, B'' builder warps
+constexpr int T2_THREADS = 32 * (T2_EPI + T2_BLD + 1 + T2_BB);
 constexpr int T2_BT = 32 * T2_BLD;                 // builder threads
-constexpr int T2_NSLOT = 4;                        // accumulator slots (64 columns each)
-constexpr int T2_NST = 2;                          // A' stages in tensor memory (2 chunks, 128 columns each)
+constexpr int T2_NSLOT = 2;                        // accumulator slots (64 columns each)
+constexpr int T2_NST = 3;                          // A' stages in tensor memory (2 chunks, 128 columns each)
 constexpr uint32_t T2_ACOL = 64u * T2_NSLOT;       // first A' column
 constexpr int T2_BCH = 2 * 32 * 128;               // one chunk of B'': 32 hi rows, then 32 lo rows
 constexpr uint32_t T2_IDESC = tc::idesc(2, 2, 128, 64);
@@ -292,10 +292,10 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_jacobian_tg_tc(JArgs a, const
       tc::mbar_init(&empty[i], 1);
     }
     for (int b = 0; b < 2; ++b) {
-      tc::mbar_init(&bfull[b], T2_EPI);                // B'' is built by the epilogue warps
+      tc::mbar_init(&bfull[b], T2_BB);
       tc::mbar_init(&bempty[b], 1);
       tc::mbar_init(&fready[b], T2_BT);                // one cp.async arrival per builder thread
-      tc::mbar_init(&fdone[b], T2_BLD + T2_EPI);       // readers of a staged voxel's fields
+      tc::mbar_init(&fdone[b], T2_BLD + T2_BB);        // readers of a staged voxel's fields
     }
     for (int q = 0; q < T2_NSLOT; ++q) {
       tc::mbar_init(&tfull[q], 1);
@@ -369,6 +369,53 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_jacobian_tg_tc(JArgs a, const
       if (!tc::mbar_wait(&done, 0)) atomicOr(err, 4);
     }
     __syncwarp();
+  } else if (warp > T2_EPI + T2_BLD) {
+    // ---------------------------------------------------------------- B'' builders
+    // Voxel i's detector operand into buffer i % 2 as soon as its fields are staged (fready) and
+    // the MMAs of voxel i - 2 are done with the buffer (bempty): warp w takes the 8-harmonic
+    // blocks p = w, w + 2, .. (chunk p / 2, half p % 2), lane = detector.
+    const int w = warp - (T2_EPI + T2_BLD + 1);
+    unsigned char *fst = sm + L.f_off;
+    int i = 0;
+    bool fail = false;
+    for (int64_t v = blockIdx.x; v < a.nv; v += gridDim.x, ++i) {
+      if (__any_sync(FULL, *abort_v != 0)) break;
+      const int bj = i & 1;
+      if (!__all_sync(FULL, tc::mbar_wait(&fready[bj], (i >> 1) & 1)) ||
+          (i >= 2 && !__all_sync(FULL, tc::mbar_wait(&bempty[bj], ((i >> 1) - 1) & 1)))) {
+        fail = true;
+        break;
+      }
+      const double2 *fd = reinterpret_cast<const double2 *>(fst + bj * L.fbuf) + L.nkp * 32;
+      unsigned char *bb = sm + L.b_off + bj * L.nch * T2_BCH;
+      for (int p = w; p < 2 * L.nch; p += T2_BB) {
+        float re[8], im[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const double2 y = fd[(8 * p + q) * 32 + lane];
+          re[q] = (float)y.x;
+          im[q] = (float)y.y;
+        }
+        unsigned char *bh = bb + (p >> 1) * T2_BCH;
+        const float r0[4] = {re[0], re[1], re[2], re[3]}, r1[4] = {re[4], re[5], re[6], re[7]};
+        const float i0[4] = {im[0], im[1], im[2], im[3]}, i1[4] = {im[4], im[5], im[6], im[7]};
+        const int h = p & 1;                             // hi rows 0-31, lo rows 32-63
+        st_split4(bh, bh + 4096, tc::sw128_chunk(lane, 2 * h + 0), r0);
+        st_split4(bh, bh + 4096, tc::sw128_chunk(lane, 2 * h + 1), r1);
+        st_split4(bh, bh + 4096, tc::sw128_chunk(lane, 4 + 2 * h + 0), i0);
+        st_split4(bh, bh + 4096, tc::sw128_chunk(lane, 4 + 2 * h + 1), i1);
+      }
+      tc::fence_async_smem();                            // B'' -> async proxy
+      __syncwarp();
+      if (lane == 0) {
+        tc::mbar_arrive(&bfull[bj]);
+        tc::mbar_arrive(&fdone[bj]);
+      }
+    }
+    if (fail && lane == 0) {
+      atomicOr(err, 32);
+      *abort_v = 1;
+    }
   } else if (warp >= T2_EPI) {
     // ---------------------------------------------------------------- builders
     // Per voxel i (staging buffer i % 2): copy voxel i+1's fields into the other buffer once
@@ -459,60 +506,11 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_jacobian_tg_tc(JArgs a, const
     }
   } else {
     // ---------------------------------------------------------------- epilogue
-    // Besides the accumulators, the epilogue warps build B'' one voxel ahead (voxel i+1's at the
-    // start of voxel i), from the staged detector fields: warp w takes the 8-harmonic blocks
-    // p = w, w + 4, .. (chunk p / 2, half p % 2), lane = detector.
     const int gl = warp, s = lane;
-    unsigned char *fst = sm + L.f_off;
-    auto build_b = [&](int j) -> bool {                 // B'' of voxel index j (buffer j % 2)
-      const int bj = j & 1;
-      bool okb = __all_sync(FULL, tc::mbar_wait(&fready[bj], (j >> 1) & 1));
-      if (okb && j >= 2) okb = __all_sync(FULL, tc::mbar_wait(&bempty[bj], ((j >> 1) - 1) & 1));
-      if (!okb) return false;
-      const double2 *fd = reinterpret_cast<const double2 *>(fst + bj * L.fbuf) + L.nkp * 32;
-      unsigned char *bb = sm + L.b_off + bj * L.nch * T2_BCH;
-      for (int p = warp; p < 2 * L.nch; p += T2_EPI) {
-        float re[8], im[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const double2 y = fd[(8 * p + q) * 32 + lane];
-          re[q] = (float)y.x;
-          im[q] = (float)y.y;
-        }
-        unsigned char *bh = bb + (p >> 1) * T2_BCH;
-        const float r0[4] = {re[0], re[1], re[2], re[3]}, r1[4] = {re[4], re[5], re[6], re[7]};
-        const float i0[4] = {im[0], im[1], im[2], im[3]}, i1[4] = {im[4], im[5], im[6], im[7]};
-        const int h = p & 1;                             // hi rows 0-31, lo rows 32-63
-        st_split4(bh, bh + 4096, tc::sw128_chunk(lane, 2 * h + 0), r0);
-        st_split4(bh, bh + 4096, tc::sw128_chunk(lane, 2 * h + 1), r1);
-        st_split4(bh, bh + 4096, tc::sw128_chunk(lane, 4 + 2 * h + 0), i0);
-        st_split4(bh, bh + 4096, tc::sw128_chunk(lane, 4 + 2 * h + 1), i1);
-      }
-      tc::fence_async_smem();                            // B'' -> async proxy
-      __syncwarp();
-      if (lane == 0) {
-        tc::mbar_arrive(&bfull[bj]);
-        tc::mbar_arrive(&fdone[bj]);
-      }
-      return true;
-    };
     uint32_t tl_idx = 0;
-    bool ok = blockIdx.x >= a.nv || build_b(0);
-    if (!ok && lane == 0) {
-      atomicOr(err, 16);
-      *abort_v = 1;
-    }
-    int i = 0;
-    for (int64_t v = blockIdx.x; v < a.nv && ok; v += gridDim.x, ++i) {
+    bool ok = true;
+    for (int64_t v = blockIdx.x; v < a.nv && ok; v += gridDim.x) {
       if (__any_sync(FULL, *abort_v != 0)) break;
-      if (v + gridDim.x < a.nv && !build_b(i + 1)) {
-        ok = false;
-        if (lane == 0) {
-          atomicOr(err, 16);
-          *abort_v = 1;
-        }
-        break;
-      }
       const float wv = (float)(a.w ? a.w[v] : 1.0);
       for (int t = 0; t < L.ntile; ++t, ++tl_idx) {
         const uint32_t slot = tl_idx % T2_NSLOT, use = tl_idx / T2_NSLOT;
