@@ -186,7 +186,8 @@ __global__ void __launch_bounds__(JBS) k_jacobian_tg(JArgs a, const float2 *__re
 // this one builds NG x NS x NF products (the gate coefficient times the source field) instead
 // of NS x ND x NF (the field products per link), and no MMA column is spent on padded gates.
 //
-// Split operands: FP32 values x enter as hi = tf32(x) and lo = tf32(x - hi).  The B operand of
+// Split operands: FP32 values x enter as hi and lo = x - hi, hi = tf32(x) rounded (B'') or x
+// with its 13 low mantissa bits cleared (A', one logic operation).  The B operand of
 // each MMA is the 64 rows [B'_hi ; B'_lo] (N = 64), so two MMAs per K step, A'_hi [B'_hi ; B'_lo]
 // and A'_lo [B'_hi ; B'_lo], leave (A'_hi + A'_lo) B'_hi in accumulator columns 0-31 and
 // (A'_hi + A'_lo) B'_lo in columns 32-63, which the epilogue adds.  A tf32 MMA of M = 128, K = 8
@@ -478,10 +479,12 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_jacobian_tg_tc(JArgs a, const
             for (int j = 0; j < 8; ++j) {
               const float2 q = cg[j];
               const float qr = q.x * pr[c][j] - q.y * pi[c][j], qi = -(q.x * pi[c][j] + q.y * pr[c][j]);
-              hr[j] = tc::to_tf32(qr);
-              lr[j] = tc::to_tf32(qr - hr[j]);
-              hm[j] = tc::to_tf32(qi);
-              lm[j] = tc::to_tf32(qi - hm[j]);
+              // hi = x with the 13 low mantissa bits cleared (a TF32 value), lo = x - hi (exact);
+              // the MMA reads lo as TF32 too, which drops ~2^-22 of x
+              hr[j] = __uint_as_float(__float_as_uint(qr) & 0xffffe000u);
+              lr[j] = qr - hr[j];
+              hm[j] = __uint_as_float(__float_as_uint(qi) & 0xffffe000u);
+              lm[j] = qi - hm[j];
             }
             // row gl * 32 + s = lane s of this warp's quadrant; chunk cc of the stage: K' = 8 half + j
             // (real), 16 + 8 half + j (imaginary); lo 64 columns after hi
