@@ -54,9 +54,11 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-secondary", action="store_true", help="skip the TG Jacobian / LM / plain-FP64 timings")
-    ap.add_argument("--only", choices=["tg", "small", "lm", "recon", "uneven", "grad500k"], default=None,
+    ap.add_argument("--only", choices=["tg", "small", "lm", "recon", "uneven", "grad500k", "tgk", "chol"], default=None,
                     help="run one secondary timing alone and print its JSON (profiling cases)")
     ap.add_argument("--lm-grid-mm", type=float, default=2.0, help="voxel pitch of the LM step's Jacobian basis")
+    ap.add_argument("--tgk-h", type=float, default=1.38, help="--only tgk: mesh pitch (mm) of the ellipsoid")
+    ap.add_argument("--chol-n", type=int, default=22971, help="--only chol: order of the matrix")
     ap.add_argument("--order", choices=["morton", "lattice"], default="morton", help="mesh node numbering")
     ap.add_argument("--no-autotune", action="store_true", help="keep the built-in SpMM launch shape")
     ap.add_argument("--clock-ms", type=int, default=200, help="nvidia-smi sampling interval in the timed region")
@@ -590,6 +592,57 @@ def uneven_bench(count=24, seed=11, streams=4):
             "vjp_finite": bool(all(torch.isfinite(r.vjp).all() for r in res))}
 
 
+def tg_kernels_bench(h=1.38, reps=5):
+    """The TG Jacobian and its vjp alone on both engines (kernel timing and profiling case):
+    ellipsoid 90 x 75 x 70 mm at pitch h (h = 1.38 mm: 101,880 nodes; 2.4 mm: 20,497), 32 x 32
+    optodes, 64 harmonics, 20 gates of 250 ps, nodal basis, fields from mixed solves to 1e-6.
+    The default engine runs first (the tensor cores where the shapes fit)."""
+    import torch
+    from dogpup_b200 import api, workloads
+    from dogpup_b200._lib import lib as _dl
+    w = workloads.ellipsoid_fwd(seed=3, h=h, ns=32, nd=32, nf=64)
+    mesh = workloads.build_dmesh(w)
+    gfc = api.td2fc(torch.as_tensor(_gates(w["t"], 20, 250e-12, 0.5e-9, 250e-12), device="cuda"),
+                    torch.as_tensor(mesh.optode.fAxis), torch.as_tensor(w["t"]))
+    nb, link, nt, fpsf = mesh.nodal_basis(), mesh._link(), len(w["t"]), mesh.optode.s_fpsf
+    phi, _ = mesh.flu_solve(precision="mixed", tol=1e-6)
+    phiA = mesh.adj_flu_solve(precision="mixed", tol=1e-6)
+    g = torch.as_tensor(np.random.default_rng(5).standard_normal((int(link.shape[0]), 20)), device="cuda")
+    res = {"workload": f"ellipsoid 90x75x70 @{h}mm, {mesh.nn} nodes, 32x32 optodes, 64 harmonics, 20 gates"}
+    for eng, name in ((0, "default"), (1, "cuda_cores")):
+        _dl.dgp_set_jacobian_engine(eng)
+        out = {}
+        ms = _event_ms(lambda: out.__setitem__("J", api.jacobian_tg(nb, phi, phiA, fpsf, link, gfc, nt)), reps)
+        del out
+        res[name] = {"tg_jacobian_ms": round(ms, 3),
+                     "vjp_ms": round(_event_ms(lambda: api.jacobian_tg_vjp(nb, phi, phiA, fpsf, link, gfc, nt, g),
+                                               reps), 3)}
+    _dl.dgp_set_jacobian_engine(0)
+    return res
+
+
+def cholesky_bench(n=22971, reps=3):
+    """The library's FP64 Cholesky solve alone (kernel timing and profiling case): a random
+    diagonally dominant symmetric positive definite matrix of order n, even leading dimension."""
+    import ctypes as C
+    import torch
+    from dogpup_b200._lib import lib, check
+    ld = n + (n & 1)
+    gen = torch.Generator(device="cuda").manual_seed(3)
+    H0 = torch.rand((n, ld), generator=gen, device="cuda", dtype=torch.float64) - 0.5
+    H0.diagonal()[:n] += float(n)
+    x0 = torch.rand(n, generator=gen, device="cuda", dtype=torch.float64)
+    H, x = H0.clone(), x0.clone()
+
+    def run():
+        H.copy_(H0)
+        x.copy_(x0)
+        check(lib.dgp_cholesky_solve(C.c_void_p(H.data_ptr()), n, ld, C.c_void_p(x.data_ptr()), None))
+    ms = _event_ms(run, reps)
+    return {"n": n, "ld": ld, "cholesky_solve_ms": round(ms, 3),
+            "tflops_fp64": round(n ** 3 / 3 / (ms * 1e-3) / 1e12, 2)}
+
+
 def grad_big_bench(target_nodes=500_000, ns=32, nd=32, nf=32):
     """End-to-end gradient of a TG least-squares loss w.r.t. nodal mua on a ~500k-node ellipsoid,
     fields recomputed in backward instead of stored; mixed precision vs plain FP64 solves, both to
@@ -900,7 +953,8 @@ def main():
         out = {"tg": tg_jacobian_bench, "small": plain_fp64_small_bench,
                "lm": lambda: lm_step_bench(grid_mm=a.lm_grid_mm),
                "recon": lambda: lm_recon_bench(grid_mm=a.lm_grid_mm), "uneven": uneven_bench,
-               "grad500k": grad_big_bench}[a.only]()
+               "grad500k": grad_big_bench, "tgk": lambda: tg_kernels_bench(h=a.tgk_h),
+               "chol": lambda: cholesky_bench(n=a.chol_n)}[a.only]()
         print(json.dumps(out))
         return
     if world > 1:
