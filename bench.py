@@ -872,9 +872,12 @@ def run_ours(a, rank, world, local_rank):
     per_iter = {0: 2, 1: 5, 2: 1, 3: 1} if a.inner == "bicgstab" else {4: 1, 5: 1, 1: 1, 6: 1, 7: 1}
     shp = solver.spmm_shape()
     sv, sk = shp["vec"] or 4, shp["kind"]
-    names = {0: f"k_spmm<float,{sv},0,OpA32,{sk}> (K + i w M SpMM)", 1: f"k_spmm<float,{sv},0,OpG32,{sk}> (FSAI apply)",
+    gk = 0 if sk == 4 else sk                       # kind 4 pairs the harmonics of A only
+    a0 = f"k_spmm_pair<{sv},0> (K + i w M SpMM, harmonic pairs)" if sk == 4 else f"k_spmm<float,{sv},0,OpA32,{sk}> (K + i w M SpMM)"
+    a1 = f"k_spmm_pair<{sv},1> (q = A p, p.q, harmonic pairs)" if sk == 4 else f"k_spmm<float,{sv},1,OpA32,{sk}> (q = A p, p.q)"
+    names = {0: a0, 1: f"k_spmm<float,{sv},0,OpG32,{gk}> (FSAI apply)",
              2: "k_update_xrp<float>", 3: "k_update_s<float>",
-             4: f"k_spmm<float,{sv},1,OpA32,{sk}> (q = A p, p.q)", 5: f"k_spmm<float,{sv},3,OpG32,{sk}> (T = G r, T.T)",
+             4: a1, 5: f"k_spmm<float,{sv},3,OpG32,{gk}> (T = G r, T.T)",
              6: "k_update_r<float>", 7: "k_update_px<float>"}
     prof = {q: solver.profile_kernel(q, 5) for q in per_iter}
     dom = max(prof, key=lambda q: prof[q][0] * per_iter[q])

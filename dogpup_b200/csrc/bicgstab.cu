@@ -40,6 +40,7 @@
 #include <initializer_list>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "dgp_common.cuh"
@@ -542,6 +543,138 @@ __global__ void __launch_bounds__(BS) k_spmm(Layout L, Op op, const typename CT<
     } else {
       const int slot[2] = {ACC_D2, ACC_D3};
       block_reduce<VEC, 2, E>(L, ln, pd, cols.acc, cols.C, slot, smem);
+    }
+  }
+}
+
+// Harmonic pairs (SpMM kind 4, the A operator only: its record (column, K, M) is the same for
+// every harmonic, only w_k differs).  A block computes harmonics 2 y and 2 y + 1 of its rows
+// together: each nonzero's record is loaded and handed out by shuffles once for both harmonics,
+// a_k = K + i w_k M is formed per harmonic, and the two harmonics' x gathers are in flight
+// together.  With an odd harmonic count the last block's second harmonic is a copy of its
+// first, computed and not written.
+template <int VEC>
+__device__ inline void row_spmv_shfl_pair(int nsp, int cs, const int32_t *__restrict__ rowptr, int64_t i,
+                                          const Rec32 *__restrict__ rec, float om0, float om1,
+                                          const float2 *__restrict__ X0, const float2 *__restrict__ X1,
+                                          float2 (&y0)[VEC], float2 (&y1)[VEC], int lpr, int sub, unsigned mask) {
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) {
+    y0[v] = make_float2(0.f, 0.f);
+    y1[v] = make_float2(0.f, 0.f);
+  }
+  const int b = __ldg(rowptr + i), e = __ldg(rowptr + i + 1);
+  const int cmax = __reduce_max_sync(mask, e - b);
+  for (int base = 0; base < cmax; base += lpr) {
+    int j0 = 0;
+    float k0 = 0.f, m0 = 0.f;
+    if (b + base + sub < e) {
+      const int4 r = __ldg(reinterpret_cast<const int4 *>(rec + b + base + sub));
+      j0 = r.x;
+      k0 = __int_as_float(r.y);
+      m0 = __int_as_float(r.z);
+    }
+    const int cnt = min(lpr, cmax - base);
+    for (int u = 0; u < cnt; ++u) {
+      const int j = __shfl_sync(mask, j0, u, lpr);
+      const float kk = __shfl_sync(mask, k0, u, lpr), mm = __shfl_sync(mask, m0, u, lpr);
+      if (b + base + u < e) {
+        float2 x0[VEC], x1[VEC];
+        ldgv<VEC>(X0 + j * nsp, cs, x0);
+        ldgv<VEC>(X1 + j * nsp, cs, x1);
+        const float2 a0 = make_float2(kk, om0 * mm), a1 = make_float2(kk, om1 * mm);
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) {
+          y0[v] = cfmaf(a0, x0[v], y0[v]);
+          y1[v] = cfmaf(a1, x1[v], y1[v]);
+        }
+      }
+    }
+  }
+}
+
+// Y = A_k X for the harmonic pair of blockIdx.y; MODE as k_spmm.
+template <int VEC, int MODE>
+__global__ void __launch_bounds__(BS) k_spmm_pair(Layout L, OpA32 op, const float2 *__restrict__ X,
+                                                  float2 *__restrict__ Y, const float2 *__restrict__ W, Cols cols,
+                                                  const Ctl *ctl) {
+  if (ctl && halted(ctl, ST_RUNNING)) return;
+  const int k0 = 2 * (int)blockIdx.y, k1 = k0 + 1;
+  const bool has1 = k1 < L.nf;
+  const bool live0 = !harmonic_done(cols, k0), live1 = has1 && !harmonic_done(cols, k1);
+  if (!live0 && !live1) return;
+  extern __shared__ double2 smem[];
+  Lane ln(L);
+  constexpr int E = 2;
+  const int c0 = ln.template col0<E>(), cs = ln.template cs<E>(L);
+  const int64_t plane = L.n * (int64_t)L.nsp;
+  const float2 *X0 = X + (int64_t)k0 * plane + c0;
+  const float2 *X1 = has1 ? X0 + plane : X0;
+  const float om0 = op.omega[k0], om1 = has1 ? op.omega[k1] : om0;
+  constexpr int NQ = MODE == 2 ? 2 : 1;
+  float2 p0[VEC][NQ], p1[VEC][NQ];
+#pragma unroll
+  for (int v = 0; v < VEC; ++v)
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) p0[v][q] = p1[v][q] = make_float2(0.f, 0.f);
+  for (int it = 0; it < L.ipb; ++it) {
+    const int64_t i = ln.row(L, it);
+    const bool valid = i < L.n;
+    const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+    if (vmask == 0u) break;
+    if (!valid) continue;
+    float2 y0[VEC], y1[VEC];
+    row_spmv_shfl_pair<VEC>(L.nsp, cs, op.rowptr, i, op.rec, om0, om1, X0, X1, y0, y1, L.lpr, ln.sub, vmask);
+    const int64_t o0 = vidx(L, k0, i, c0), o1 = o0 + plane;
+    if (MODE != 2) {
+      if (live0) stv<VEC>(Y + o0, cs, y0);
+      if (live1) stv<VEC>(Y + o1, cs, y1);
+    }
+    if constexpr (MODE == 3) {
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) {
+        acc_bil(p0[v][0], y0[v], y0[v]);
+        acc_bil(p1[v][0], y1[v], y1[v]);
+      }
+    } else if (MODE != 0) {
+      float2 w0[VEC], w1[VEC];
+      ldv<VEC>(W + o0, cs, w0);
+      ldv<VEC>(W + (has1 ? o1 : o0), cs, w1);
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) {
+        acc_bil(p0[v][0], y0[v], w0[v]);
+        acc_bil(p1[v][0], y1[v], w1[v]);
+        if (MODE == 2) {
+          acc_bil(p0[v][NQ - 1], y0[v], y0[v]);
+          acc_bil(p1[v][NQ - 1], y1[v], y1[v]);
+        }
+      }
+    }
+  }
+  if constexpr (MODE != 0) {
+    double2 d0[VEC][NQ], d1[VEC][NQ];
+#pragma unroll
+    for (int v = 0; v < VEC; ++v)
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        d0[v][q] = d2(p0[v][q]);
+        d1[v][q] = d2(p1[v][q]);
+      }
+    constexpr int S0 = MODE == 2 ? ACC_D2 : ACC_D1;
+    const int slot[NQ] = {S0};
+    int slot2[2] = {ACC_D2, ACC_D3};
+    Lane l0 = ln, l1 = ln;
+    l0.k = k0;
+    l1.k = k1;
+    // (block-uniform conditions: block_reduce synchronises the block)
+    if constexpr (MODE == 2) {
+      if (live0) block_reduce<VEC, 2, E>(L, l0, d0, cols.acc, cols.C, slot2, smem);
+      __syncthreads();
+      if (live1) block_reduce<VEC, 2, E>(L, l1, d1, cols.acc, cols.C, slot2, smem);
+    } else {
+      if (live0) block_reduce<VEC, 1, E>(L, l0, d0, cols.acc, cols.C, slot, smem);
+      __syncthreads();
+      if (live1) block_reduce<VEC, 1, E>(L, l1, d1, cols.acc, cols.C, slot, smem);
     }
   }
 }
@@ -1743,6 +1876,13 @@ void spmm_go(const SolverPlan *S, const Layout &L, size_t smem, cudaStream_t st,
       case 1: k_spmm<R, VEC, MODE, Op, 1><<<grid_of(L), BS, smem, st>>>(L, op, X, Y, W, cols, ctl); return;
       case 2: k_spmm<R, VEC, MODE, Op, 2><<<grid_of(L), BS, smem, st>>>(L, op, X, Y, W, cols, ctl); return;
       case 3: k_spmm<R, VEC, MODE, Op, 3><<<grid_of(L), BS, smem, st>>>(L, op, X, Y, W, cols, ctl); return;
+      case 4:                                           // harmonic pairs for A; kind 0 for G, G^T
+        if constexpr (std::is_same<Op, OpA32>::value) {
+          const dim3 g((unsigned)ceil_div(L.n, L.rows_per_block()), (unsigned)ceil_div(L.nf, 2));
+          k_spmm_pair<VEC, MODE><<<g, BS, smem, st>>>(L, op, X, Y, W, cols, ctl);
+          return;
+        }
+        break;
       default: break;
     }
   }
@@ -2534,7 +2674,7 @@ int solver_autotune(SolverPlan *S, int32_t *tiled_out, int32_t *vec_out, int32_t
   int32_t bv = 0, br = 0, bk = 0;
   int launches = 0;
   int rc = DGP_OK;
-  for (int kind = 0; kind < 4 && rc == DGP_OK; ++kind)
+  for (int kind = 0; kind < 5 && rc == DGP_OK; ++kind)
   for (int vec : {8, 4, 2}) {
     if (vec > S->nsp || S->nsp / vec > 32) continue;
     int last_ipb = -1;
@@ -2652,7 +2792,7 @@ int solver_set_spmm(SolverPlan *S, int32_t tiled, int32_t vec, int32_t rows) {
 }
 
 int solver_set_spmm_kind(SolverPlan *S, int32_t kind) {
-  DGP_REQUIRE(kind >= 0 && kind <= 3, "set_spmm_kind: kind must be 0, 1, 2 or 3");
+  DGP_REQUIRE(kind >= 0 && kind <= 4, "set_spmm_kind: kind must be 0, 1, 2, 3 or 4");
   S->tune_kind = kind;
   for (auto &g : S->graph)
     if (g) {

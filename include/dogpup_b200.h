@@ -267,7 +267,9 @@ int dgp_solver_set_spmm(dgp_solver_t solver, int32_t tiled, int32_t vec,
  * per step; 1 and 2 issue the gathers of 2 or 4 nonzeros together (lanes
  * past a row's end carry a zero coefficient on the row's own column); 3 is
  * kind 2 with packed FP32 FMAs (two instead of four FMA instructions per
- * complex product).  dgp_solver_autotune searches the kinds with the lane widths and
+ * complex product); 4 computes two harmonics of A per block, so that each
+ * nonzero's record (column, K, M) is loaded and handed out once for both (the
+ * G sweeps run kind 0).  dgp_solver_autotune searches the kinds with the lane widths and
  * block heights; dgp_solver_spmm_shape reports the plan's current choice. */
 int dgp_solver_set_spmm_kind(dgp_solver_t solver, int32_t kind);
 /* How a solve runs its iterations.  1 (default): each inner solve is ONE
