@@ -338,11 +338,18 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_jacobian_tg_tc(JArgs a, const
           if (use >= 1) ok = tc::mbar_wait(&tempty[slot], (use - 1) & 1);   // the epilogue has read it
           tc::fence_after_sync();
           const uint32_t d_tm = tmem + 64u * slot;
+          // one wait per tile: on its last stage.  Every builder warp fills a tile's stages in
+          // order and its arrival on a stage's barrier releases all of its earlier writes, so the
+          // last stage's completion covers the tile's earlier stages too (an mbarrier wait right
+          // after a burst of MMAs costs a few hundred cycles).
+          {
+            const int nst_tile = (L.nch + 1) / 2;
+            const uint32_t sl = st_idx + (uint32_t)nst_tile - 1u;
+            ok = tc::mbar_wait(&full[sl % T2_NST], (sl / T2_NST) & 1);
+            tc::fence_after_sync();
+          }
           for (int c0 = 0; c0 < L.nch && ok; c0 += 2) {   // a stage = chunks c0, c0 + 1
             const uint32_t s = st_idx % T2_NST;
-            ok = tc::mbar_wait(&full[s], (st_idx / T2_NST) & 1);
-            if (!ok) break;
-            tc::fence_after_sync();
             for (int cc = 0; cc < 2 && c0 + cc < L.nch; ++cc) {
               const int c = c0 + cc;
               const uint32_t ah = tmem + T2_ACOL + 128u * s + 32u * cc, al = ah + 64u;   // A' in tensor memory
