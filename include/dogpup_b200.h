@@ -443,8 +443,9 @@ int dgp_jacobian_complex(const int32_t *d_P_rowptr, const int32_t *d_P_col,
  * and 2 the tensor cores where the shapes fit, else the CUDA cores; 1 both on
  * the CUDA cores (cross-checks, timing).  The tensor-core TG Jacobian takes the
  * nodal basis (P = NULL), at most 32 sources and 32 detectors, each (source,
- * detector) pair at most once in the link table, and NF, NG small enough for its
- * operand rings in shared memory (NF = 64 with NG <= 24, for example). */
+ * detector) pair at most once in the link table, and at most 64 harmonics; the
+ * tensor-core vjp the nodal basis or a basis P, at most 32 sources and 32
+ * detectors and 4096 links. */
 int dgp_set_jacobian_engine(int32_t engine);
 int dgp_jacobian_tg(const int32_t *d_P_rowptr, const int32_t *d_P_col,
                     const double *d_P_val, int64_t nv, const double *d_w,
