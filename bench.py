@@ -64,6 +64,7 @@ def parse():
     ap.add_argument("--clock-ms", type=int, default=200, help="nvidia-smi sampling interval in the timed region")
     ap.add_argument("--spmm-vec", type=int, default=0, help="with --no-autotune: gather SpMM complex values per lane")
     ap.add_argument("--spmm-rows", type=int, default=0, help="with --no-autotune: gather SpMM rows per block")
+    ap.add_argument("--spmm-kind", type=int, default=0, help="with --no-autotune: gather SpMM inner-loop kind (0-4)")
     return ap.parse_args()
 
 
@@ -787,6 +788,7 @@ def run_ours(a, rank, world, local_rank):
     tuned = None
     if a.no_autotune and a.spmm_vec:
         solver.set_spmm(False, a.spmm_vec, a.spmm_rows)
+        solver.set_spmm_kind(a.spmm_kind)
         tuned = dict(solver.spmm_shape(), set_by="command line")
     if not a.no_autotune:
         t0 = time.perf_counter()
