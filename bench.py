@@ -65,6 +65,9 @@ def parse():
     ap.add_argument("--spmm-vec", type=int, default=0, help="with --no-autotune: gather SpMM complex values per lane")
     ap.add_argument("--spmm-rows", type=int, default=0, help="with --no-autotune: gather SpMM rows per block")
     ap.add_argument("--spmm-kind", type=int, default=0, help="with --no-autotune: gather SpMM inner-loop kind (0-4)")
+    ap.add_argument("--host-loop", action="store_true",
+                    help="host-polled iteration loop instead of the graph's device-driven WHILE node "
+                         "(for launch lists: ncu does not list kernels inside a conditional node)")
     return ap.parse_args()
 
 
@@ -785,6 +788,8 @@ def run_ours(a, rank, world, local_rank):
 
     log(f"[rank {rank}] setup done: {mesh.nn} nodes, nnz {mesh.fem.nnz}, harmonics "
         f"{'all' if fw is None else len(fw.harm)}, solver {solver.memory() / 1e9:.1f} GB")
+    if a.host_loop:
+        solver.set_device_loop(False)
     tuned = None
     if a.no_autotune and a.spmm_vec:
         solver.set_spmm(False, a.spmm_vec, a.spmm_rows)
@@ -986,7 +991,8 @@ def main():
                        "max_rel_residual": rep.max_rel_residual, "l2": "inputs larger than L2 (vectors ~GB)",
                        "parallelism": f"harmonics split over {world} GPUs (k = r mod {world}), detector data "
                                       f"all-gathered every step" if world > 1 else "single GPU",
-                       "node_order": a.order, "autotuned": r["tuned"]},
+                       "node_order": a.order, "autotuned": r["tuned"],
+                       "iteration_loop": "host-polled" if a.host_loop else "device-driven (graph WHILE node)"},
             "e2e": r["e2e"], "roofline": r["roof"], "cpu_baseline": cpu, "clocks": r["clocks"],
             "gpu_launches": r["launches"],
             "plain_fp64_per_rhs": r.get("plain"), "plain_fp64_small": r.get("small"), "tg_jacobian": r.get("tg"),
