@@ -19,10 +19,11 @@
 //   k_dgemm_nt       trailing update of the rest, depth 512: A_il -= sum over the outer panel
 //
 // k_dgemm_nt: C = beta C + alpha A B^T with A, B row-major (K contiguous); 128 x 64 CTA tiles,
-// two CTAs per SM (one's epilogue overlaps the other's main loop), 256 threads (8 warps of
-// 32 x 32), K in stages of 16 doubles moved by cp.async through a 3-deep shared-memory ring
-// (rows padded to 20 doubles: the fragment loads hit 32 distinct banks per half-warp), 8
-// mma.sync m16n8k4 .f64 per warp per 4 K.
+// two CTAs per SM, 256 threads (8 warps of 32 x 32), K in stages of 16 doubles moved by cp.async
+// through a 3-deep shared-memory ring (rows padded to 20 doubles: the fragment loads hit 32
+// distinct banks per half-warp), 8 mma.sync m16n8k4 .f64 per warp per 4 K.  The updates of the
+// factorisation (beta = 1, alpha = -1) start their accumulators from C in the fragments and
+// store them back from registers.
 //
 // Solves: L y = b and L^T x = y by 128-row blocks with the stored diagonal inverses:
 //   y_b = inv(L_bb) (b_b - sum_{c<b} L_bc y_c),   x_b = inv(L_bb)^T (y_b - sum_{c>b} L_cb^T x_c),
@@ -89,14 +90,18 @@ struct Gemm {
   double alpha, beta;
   int lower;           // 1: only the tiles that meet the lower triangle, only entries c <= r
   int64_t tn;          // tiles along N (full mode)
+  int cvec;            // C and ldc allow 16-byte accesses to column pairs (set by gemm_launch)
 };
 
 // C = beta C + alpha A B^T on 128 x GBN CTA tiles (see the file comment).  V: bytes per cp.async
 // (16 when every row start and the base addresses are 16-byte aligned, else 8).  GBN = 128 when C
 // is A itself (the in-place panel: a CTA must own whole rows of it).  Lower mode (GBN = 64): the
 // tiles that meet the lower triangle, row ti holding tiles tj = 0 .. 2 ti + 1 (the last two
-// straddle the diagonal; only entries c <= r are written).
-template <int V, int GBN>
+// straddle the diagonal; only entries c <= r are written).  REG (beta = 1, alpha = +-1): the
+// accumulators start from C / alpha (exact) in the mma fragments, loaded before the main loop so
+// that their latency hides behind the first stages, and C = alpha acc goes back from registers;
+// otherwise the accumulators start at zero and C = beta C + alpha acc goes through shared memory.
+template <int V, int GBN, bool REG>
 __global__ void __launch_bounds__(GTHREADS, GBN == 64 ? 2 : 1) k_dgemm_nt(Gemm g) {
   constexpr int NJ = GBN / 16;                      // n8 fragments per warp (warp tile 32 x GBN / 2)
   extern __shared__ __align__(16) double gsm[];
@@ -116,12 +121,38 @@ __global__ void __launch_bounds__(GTHREADS, GBN == 64 ? 2 : 1) k_dgemm_nt(Gemm g
   const int wm = warp & 3, wn = warp >> 2;          // warp tile: rows wm*32.., cols wn*GBN/2..
   const int gid = lane >> 2, tig = lane & 3;
   double acc[2][NJ][4];
+  // fragment entry (i, j, q) is C row wm*32 + i*16 + gid + 8*(q/2), column wn*GBN/2 + j*8 + 2*tig + q%2
+  const int64_t rows = min((int64_t)GBM, g.M - r0), cols = min((int64_t)GBN, g.N - c0);
+  // whole tile inside C and (lower mode) on or below the diagonal: column pairs as 16-byte accesses
+  const bool whole = rows == GBM && cols == GBN && (!g.lower || c0 + GBN - 1 <= r0) && g.cvec;
+  auto frag_in = [&](int r, int c) { return r < rows && c < cols && (!g.lower || c0 + c <= r0 + r); };
+  if constexpr (REG) {
+    const double sgn = g.alpha;                     // +-1: C / alpha = sgn C
 #pragma unroll
-  for (int i = 0; i < 2; ++i)
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int j = 0; j < NJ; ++j)
+      for (int j = 0; j < NJ; ++j)
 #pragma unroll
-      for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
+        for (int h = 0; h < 2; ++h) {
+          const int r = wm * 32 + i * 16 + gid + 8 * h, c = wn * (GBN / 2) + j * 8 + 2 * tig;
+          const double *cp = g.C + (r0 + r) * g.ldc + c0 + c;
+          if (whole) {
+            const double2 v = *reinterpret_cast<const double2 *>(cp);
+            acc[i][j][2 * h] = sgn * v.x;
+            acc[i][j][2 * h + 1] = sgn * v.y;
+          } else {
+            acc[i][j][2 * h] = frag_in(r, c) ? sgn * cp[0] : 0.0;
+            acc[i][j][2 * h + 1] = frag_in(r, c + 1) ? sgn * cp[1] : 0.0;
+          }
+        }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < NJ; ++j)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
+  }
 
   const int nk = (int)((g.K + GK - 1) / GK);
   constexpr int E = V / 8;                          // doubles per copy
@@ -175,6 +206,25 @@ __global__ void __launch_bounds__(GTHREADS, GBN == 64 ? 2 : 1) k_dgemm_nt(Gemm g
     }
   }
   cp_wait<0>();
+  if constexpr (REG) {
+    const double sgn = g.alpha;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < NJ; ++j)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int r = wm * 32 + i * 16 + gid + 8 * h, c = wn * (GBN / 2) + j * 8 + 2 * tig;
+          double *cp = g.C + (r0 + r) * g.ldc + c0 + c;
+          if (whole) {
+            *reinterpret_cast<double2 *>(cp) = make_double2(sgn * acc[i][j][2 * h], sgn * acc[i][j][2 * h + 1]);
+          } else {
+            if (frag_in(r, c)) cp[0] = sgn * acc[i][j][2 * h];
+            if (frag_in(r, c + 1)) cp[1] = sgn * acc[i][j][2 * h + 1];
+          }
+        }
+    return;
+  }
   __syncthreads();   // the stage ring is free: the epilogue goes through shared memory
   // epilogue: the accumulators are written to shared memory (a 128 x (GBN + 1)-double tile), then the
   // CTA reads and writes C row by row, coalesced, with every load of C in flight together
@@ -191,7 +241,6 @@ __global__ void __launch_bounds__(GTHREADS, GBN == 64 ? 2 : 1) k_dgemm_nt(Gemm g
         T[r * TLD + c] = acc[i][j][q];
       }
   __syncthreads();
-  const int64_t rows = min((int64_t)GBM, g.M - r0), cols = min((int64_t)GBN, g.N - c0);
   // batches of 16 entries per thread: all 16 loads of C are issued before any store (a store to
   // C between loads would otherwise keep the compiler from overlapping their latencies)
   constexpr int BATCH = 16;
@@ -522,30 +571,34 @@ __global__ void __launch_bounds__(DTHREADS) k_block_diag(const double *__restric
   }
 }
 
-template <int V, int GBN>
+template <int V, int GBN, bool REG>
 int gemm_launch(Gemm g, cudaStream_t st) {
   constexpr int smem = gemm_smem(GBN);
   const int64_t tm = ceil_div(g.M, (int64_t)GBM), tn = ceil_div(g.N, (int64_t)GBN);
   g.tn = tn;
+  g.cvec = ((uintptr_t)g.C % 16 == 0) && g.ldc % 2 == 0;
   // lower mode (M == N, GBN = 64): row ti of tiles holds tj = 0 .. 2 ti + 1; a tile past N (the
   // last one of a row when N is not a multiple of 128) writes nothing
   const int64_t tiles = g.lower ? tm * (tm + 1) : tm * tn;
   DGP_REQUIRE(tiles <= INT32_MAX, "cholesky: too many tiles");
-  DGP_CUDA(cudaFuncSetAttribute(k_dgemm_nt<V, GBN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  k_dgemm_nt<V, GBN><<<(unsigned)tiles, GTHREADS, smem, st>>>(g);
+  DGP_CUDA(cudaFuncSetAttribute(k_dgemm_nt<V, GBN, REG>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  k_dgemm_nt<V, GBN, REG><<<(unsigned)tiles, GTHREADS, smem, st>>>(g);
   DGP_CHECK_LAUNCH();
   return DGP_OK;
 }
 
-// C = beta C + alpha A B^T; 128-column tiles when C is A (in place), else 64-column tiles
+// C = beta C + alpha A B^T; 128-column tiles when C is A (in place), else 64-column tiles, with
+// the accumulators started from C when beta = 1 and alpha = +-1 (every update of the factorisation)
 int gemm_nt(const Gemm &g, cudaStream_t st) {
   if (g.M <= 0 || g.N <= 0) return DGP_OK;
   const bool a16 = ((uintptr_t)g.A % 16 == 0) && ((uintptr_t)g.B % 16 == 0) && g.lda % 2 == 0 && g.ldb % 2 == 0 &&
                    g.K % 2 == 0;
   const bool inplace = g.C == g.A;
   if (inplace) DGP_REQUIRE(!g.lower && g.N <= GBM, "cholesky: an in-place product must fit one 128-column tile");
-  if (inplace) return a16 ? gemm_launch<16, 128>(g, st) : gemm_launch<8, 128>(g, st);
-  return a16 ? gemm_launch<16, 64>(g, st) : gemm_launch<8, 64>(g, st);
+  if (inplace) return a16 ? gemm_launch<16, 128, false>(g, st) : gemm_launch<8, 128, false>(g, st);
+  const bool reg = g.beta == 1.0 && (g.alpha == 1.0 || g.alpha == -1.0);
+  if (reg) return a16 ? gemm_launch<16, 64, true>(g, st) : gemm_launch<8, 64, true>(g, st);
+  return a16 ? gemm_launch<16, 64, false>(g, st) : gemm_launch<8, 64, false>(g, st);
 }
 
 // The two streams and four events of the lookahead; the destructor waits for both streams, so
