@@ -26,9 +26,12 @@
 // store them back from registers.
 //
 // Solves: L y = b and L^T x = y by 128-row blocks with the stored diagonal inverses:
-//   y_b = inv(L_bb) (b_b - sum_{c<b} L_bc y_c),   x_b = inv(L_bb)^T (y_b - sum_{c>b} L_cb^T x_c),
-// each block one partial-sum kernel over the off-diagonal blocks (FP64, atomics into a 128 x nrhs
-// accumulator) and one small kernel for the diagonal product.
+//   y_b = inv(L_bb) (b_b - sum_{c<b} L_bc y_c),   x_b = inv(L_bb)^T (y_b - sum_{c>b} L_cb^T x_c).
+// One right-hand side: one cooperative launch per direction, a CTA per block, each block
+// published by a flag that the later blocks wait for (k_trsv_chain).  Several right-hand sides
+// (or more blocks than fit on the GPU at once): per block, one partial-sum kernel over the
+// off-diagonal blocks (FP64, atomics into a 128 x nrhs accumulator) and one small kernel for the
+// diagonal product.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -571,6 +574,221 @@ __global__ void __launch_bounds__(DTHREADS) k_block_diag(const double *__restric
   }
 }
 
+// ---------------------------------------------------------------- chained solves (one right-hand side)
+// One cooperative launch per direction (every CTA resident at once): CTA b owns the 128-row
+// block b of the solution and publishes it through flags[b] (release) once it is final; a CTA
+// that needs block c waits for flags[c] (acquire; bounded: a wait that gives up sets err bit 2
+// and goes on, so every CTA ends).
+//   forward  (L y = b):   CTA b = blockIdx adds L_bc y_c for c = 0 .. b-1 as the flags come, then
+//                         y_b = inv(L_bb) (b_b - sum)
+//   backward (L^T x = y): CTA b = nblk-1-blockIdx adds L_cb^T x_c for c = nblk-1 .. b+1, then
+//                         x_b = inv(L_bb)^T (y_b - sum)
+// A 128 x 128 block M is read by rows: warp w takes rows 16w .. 16w + 15, lane l columns
+// 4l .. 4l + 3 (each row one coalesced 1 KB read).  Forward sums over the lanes (a transpose
+// through shared memory), backward over the warps.
+constexpr int TS_THREADS = 256, TS_RLD = 33;
+constexpr uint32_t TS_SPIN = 1u << 18;   // polls (~0.3 s) per wait; the whole chain takes about a millisecond
+
+__device__ inline uint32_t ld_acquire_gpu(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ inline void st_release_gpu(uint32_t *p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// bounded wait for a published block; false when it gave up
+__device__ inline bool wait_block(const uint32_t *f) {
+  for (uint32_t it = 0; it < TS_SPIN; ++it) {
+    if (ld_acquire_gpu(f)) return true;
+    if (it > 64) __nanosleep(64);
+  }
+  return false;
+}
+
+// m <- entries col .. col + 3 of a row (p points at col), zero from ncol on; 16-byte loads when vec
+// (p 16-byte aligned) and the four are inside
+__device__ inline void ts_load4(const double *p, int col, int ncol, bool vec, double (&m)[4]) {
+  if (vec && col + 3 < ncol) {
+    const double2 a = __ldg(reinterpret_cast<const double2 *>(p)), b = __ldg(reinterpret_cast<const double2 *>(p + 2));
+    m[0] = a.x;
+    m[1] = a.y;
+    m[2] = b.x;
+    m[3] = b.y;
+  } else {
+#pragma unroll
+    for (int e = 0; e < 4; ++e) m[e] = col + e < ncol ? __ldg(p + e) : 0.0;
+  }
+}
+
+// Rows 16w .. 16w + 15 (below nrow) of M (row stride ld, ncol columns) times the lane's four
+// entries of v:  forward  part[r] += sum_e M[16w + r][4l + e] v[4l + e]   (v4 = those four)
+//                backward part[e] += sum_r M[16w + r][4l + e] v[16w + r]  (v16 = those sixteen)
+template <bool TRANS>
+__device__ inline void ts_block(const double *M, int64_t ld, int nrow, int ncol, bool vec, const double (&v4)[4],
+                                const double (&v16)[16], double (&part)[16]) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const double *p0 = M + (int64_t)(16 * warp) * ld + 4 * lane;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    double m[8][4];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      if (16 * warp + 8 * h + r < nrow) {
+        ts_load4(p0 + (int64_t)(8 * h + r) * ld, 4 * lane, ncol, vec, m[r]);
+      } else {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) m[r][e] = 0.0;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        if (TRANS)
+          part[e] += m[r][e] * v16[8 * h + r];
+        else
+          part[8 * h + r] += m[r][e] * v4[e];
+      }
+  }
+}
+
+// out[i] for i < 128 of the CTA's block: the per-thread partials summed over lanes (forward) or
+// warps (backward); red is the shared scratch, valid for threads < 128 after the call
+template <bool TRANS>
+__device__ inline double ts_reduce(double *red, const double (&part)[16]) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  __syncthreads();                                   // red is free
+  if (TRANS) {
+#pragma unroll
+    for (int e = 0; e < 4; ++e) red[warp * CB + 4 * lane + e] = part[e];
+  } else {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) red[(16 * warp + r) * TS_RLD + lane] = part[r];
+  }
+  __syncthreads();
+  double s = 0.0;
+  if (tid < CB) {
+    if (TRANS) {
+#pragma unroll
+      for (int w = 0; w < TS_THREADS / 32; ++w) s += red[w * CB + tid];
+    } else {
+#pragma unroll 8
+      for (int k = 0; k < 32; ++k) s += red[tid * TS_RLD + k];
+    }
+  }
+  return s;
+}
+
+template <bool TRANS>
+__global__ void __launch_bounds__(TS_THREADS, 2) k_trsv_chain(const double *__restrict__ H, int64_t ldh, int64_t n,
+                                                             int nblk, const double *__restrict__ Linv, double *x,
+                                                             uint32_t *flags, int *err, int vech) {
+  __shared__ double red[CB * TS_RLD];
+  __shared__ double rhs[CB];
+  __shared__ int s_ready[2];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int b = TRANS ? nblk - 1 - (int)blockIdx.x : (int)blockIdx.x;
+  const int64_t base = (int64_t)b * CB;
+  const int nbi = (int)min((int64_t)CB, n - base);
+  // forward: blocks [0, ready) are known final; backward: blocks [ready, nblk).  Every thread holds
+  // the same value: thread 0 polls, writes slot (k & 1) before the k-th barrier, and each thread
+  // reads that slot right after it; the slot is written again only after barrier k + 1, which
+  // every thread reaches after its read.
+  int ready = TRANS ? nblk : 0, nsync = 0;
+  bool gave_up = false;
+  double part[16];
+#pragma unroll
+  for (int r = 0; r < 16; ++r) part[r] = 0.0;
+  const int steps = TRANS ? nblk - 1 - b : b;
+  for (int st = 0; st < steps; ++st) {
+    const int c = TRANS ? nblk - 1 - st : st;
+    if (TRANS ? c < ready : c >= ready) {
+      if (tid == 0) {
+        if (!wait_block(flags + c)) gave_up = true;
+        int r = c;                                   // and every later block already published
+        if (TRANS) {
+          while (r - 1 > b && ld_acquire_gpu(flags + r - 1)) --r;
+        } else {
+          ++r;
+          while (r < b && ld_acquire_gpu(flags + r)) ++r;
+        }
+        s_ready[nsync & 1] = r;
+      }
+      __syncthreads();
+      ready = s_ready[nsync & 1];
+      ++nsync;
+    }
+    const int64_t cb = (int64_t)c * CB;
+    double v4[4], v16[16];
+    if (TRANS) {
+      const int nbc = (int)min((int64_t)CB, n - cb);
+#pragma unroll
+      for (int r = 0; r < 16; ++r) v16[r] = 16 * warp + r < nbc ? __ldcg(x + cb + 16 * warp + r) : 0.0;
+      ts_block<true>(H + cb * ldh + base, ldh, nbc, CB, vech, v4, v16, part);
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) v4[e] = __ldcg(x + cb + 4 * lane + e);
+      ts_block<false>(H + base * ldh + cb, ldh, nbi, CB, vech, v4, v16, part);
+    }
+  }
+  // the block's right-hand side, then the product with inv(L_bb) (forward) or its transpose
+  const double s = ts_reduce<TRANS>(red, part);
+  if (tid < CB) rhs[tid] = tid < nbi ? x[base + tid] - s : 0.0;
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < 16; ++r) part[r] = 0.0;
+  {
+    const double *Lb = Linv + base * CB;             // nbi x nbi, row-major
+    const bool vl = nbi % 2 == 0;
+    double v4[4], v16[16];
+    if (TRANS) {
+#pragma unroll
+      for (int r = 0; r < 16; ++r) v16[r] = rhs[16 * warp + r];
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) v4[e] = rhs[4 * lane + e];
+    }
+    ts_block<TRANS>(Lb, nbi, nbi, nbi, vl, v4, v16, part);
+  }
+  const double y = ts_reduce<TRANS>(red, part);
+  if (tid < nbi) {
+    x[base + tid] = y;
+    __threadfence();
+  }
+  __syncthreads();
+  if (tid == 0) {
+    st_release_gpu(flags + b, 1u);
+    if (gave_up) atomicOr(err, 2);
+  }
+}
+
+// Both solves as two cooperative launches when every CTA fits on the GPU at once; false (nothing
+// launched) when they do not, and the caller takes the per-block launches
+bool trsv_chain(const double *H, int64_t ldh, int64_t n, const double *Linv, double *x, uint32_t *flags, int *err,
+                cudaStream_t st, int *rc) {
+  *rc = DGP_OK;
+  const int nblk = (int)ceil_div(n, (int64_t)CB);
+  int dev = 0, coop = 0, per_sm_f = 0, per_sm_b = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop) return false;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, k_trsv_chain<false>, TS_THREADS, 0) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_b, k_trsv_chain<true>, TS_THREADS, 0) != cudaSuccess)
+    return false;
+  if ((int64_t)std::min(per_sm_f, per_sm_b) * sm_count() < nblk) return false;
+  int vech = ((uintptr_t)H % 16 == 0) && ldh % 2 == 0;
+  uint32_t *ff = flags, *fb = flags + nblk;
+  void *af[] = {(void *)&H, (void *)&ldh, (void *)&n, (void *)&nblk, (void *)&Linv, (void *)&x, (void *)&ff,
+                (void *)&err, (void *)&vech};
+  void *ab[] = {(void *)&H, (void *)&ldh, (void *)&n, (void *)&nblk, (void *)&Linv, (void *)&x, (void *)&fb,
+                (void *)&err, (void *)&vech};
+  cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_trsv_chain<false>, dim3(nblk), dim3(TS_THREADS), af, 0, st);
+  if (e == cudaSuccess)
+    e = cudaLaunchCooperativeKernel((const void *)k_trsv_chain<true>, dim3(nblk), dim3(TS_THREADS), ab, 0, st);
+  if (e != cudaSuccess) *rc = fail(DGP_ERR_CUDA, std::string("cholesky: chained solve launch: ") + cudaGetErrorString(e));
+  return true;
+}
+
 template <int V, int GBN, bool REG>
 int gemm_launch(Gemm g, cudaStream_t st) {
   constexpr int smem = gemm_smem(GBN);
@@ -633,11 +851,13 @@ int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_
   DGP_REQUIRE(nrhs <= 65535, "cholesky: at most 65535 right-hand sides");
   DGP_REQUIRE(ceil_div(n, (int64_t)GVB) <= INT32_MAX, "cholesky: n too large for the solve grid");
   const int64_t nblk = ceil_div(n, CB);
-  DevBuf linv, errb, acc;
+  DevBuf linv, errb, acc, flags;
   DGP_TRY(linv.alloc(sizeof(double) * (size_t)nblk * CB * CB));
   DGP_TRY(errb.alloc(sizeof(int)));
   DGP_TRY(acc.alloc(sizeof(double) * (size_t)CB * nrhs));
+  DGP_TRY(flags.alloc(sizeof(uint32_t) * 2 * (size_t)nblk));
   DGP_CUDA(cudaMemsetAsync(errb.p, 0, sizeof(int), st));
+  DGP_CUDA(cudaMemsetAsync(flags.p, 0, sizeof(uint32_t) * 2 * (size_t)nblk, st));
   DGP_CUDA(cudaMemsetAsync(acc.p, 0, sizeof(double) * (size_t)CB * nrhs, st));
   const size_t pot_smem = POT_SMEM;
   DGP_CUDA(cudaFuncSetAttribute(k_potrf_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pot_smem));
@@ -716,9 +936,14 @@ int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_
     }
   }
   if (r_recorded) DGP_CUDA(cudaStreamWaitEvent(sf, ls.rest, 0));
-  // L y = b, then L^T x = y, by 128-row blocks
+  // L y = b, then L^T x = y: one right-hand side as two chained launches where every CTA fits on
+  // the GPU at once, else (and for several right-hand sides) by 128-row blocks
+  int crc = DGP_OK;
+  const bool chained = nrhs == 1 && trsv_chain(H, ldh, n, Li, x, flags.as<uint32_t>(), errb.as<int>(), sf, &crc);
+  if (crc) return crc;
+  if (chained) launches += 2;
   const unsigned dgrid = (unsigned)ceil_div((int64_t)nrhs, (int64_t)DRHS);
-  for (int64_t b = 0; b < nblk; ++b) {
+  for (int64_t b = 0; b < nblk && !chained; ++b) {
     const int64_t k0 = b * CB;
     const int nb = (int)std::min<int64_t>(CB, n - k0);
     if (k0 > 0) {
@@ -730,7 +955,7 @@ int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_
                                                           nrhs);
     ++launches;
   }
-  for (int64_t b = nblk - 1; b >= 0; --b) {
+  for (int64_t b = nblk - 1; b >= 0 && !chained; --b) {
     const int64_t k0 = b * CB;
     const int nb = (int)std::min<int64_t>(CB, n - k0);
     const int64_t kend = k0 + nb;
@@ -750,7 +975,8 @@ int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_
   int herr = 0;
   DGP_CUDA(cudaMemcpyAsync(&herr, errb.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   DGP_CUDA(cudaStreamSynchronize(st));
-  if (herr) return fail(DGP_ERR_ARG, "cholesky: matrix is not positive definite");
+  if (herr & 1) return fail(DGP_ERR_ARG, "cholesky: matrix is not positive definite");
+  if (herr & 2) return fail(DGP_ERR_CUDA, "cholesky: a wait of the chained solve gave up");
   return DGP_OK;
 }
 
