@@ -272,19 +272,82 @@ __global__ void __launch_bounds__(GTHREADS, GBN == 64 ? 2 : 1) k_dgemm_nt(Gemm g
 // the factorisation leaves alone).  The strict upper triangle of the shared tile collects
 // X = inv(L) transposed ([c][i] holds X[i][c]); dinv[c] = 1 / L[c][c].  Four 32-column steps:
 //   1. warp 0 factors the 32 x 32 diagonal block D, one row per lane in registers (a column per
-//      step: the pivot by shuffle, its reciprocal square root, the column scaled, the rank-1
-//      update of the lanes' rows), then forms X_D = inv(D), one column per lane
-//   2. the rows below: L_rD = A_rD X_D^T (a 32-term product per entry; lane = column)
+//      step: the pivot by shuffle, its reciprocal square root, the column scaled and passed
+//      through shared memory, the rank-1 update of the lanes' rows)
+//   2. the rows below by forward substitution, one row per thread: L_rD = A_rD L_D^-T
 //   3. the trailing lower triangle: A -= L_rD L_cD^T in 4 x 4 register tiles
-// then the off-diagonal blocks of X by their distance d = I - J below the diagonal:
+// then the four diagonal inverses X_II (a warp each, one column per lane) and the off-diagonal
+// blocks of X by their distance d = I - J below the diagonal:
 //   T = sum_{K = J .. I-1} L_IK X_KJ,   X_IJ = -X_II T   (a column of T per group of lanes).
 // err |= 1 on a non-positive or non-finite pivot.
 constexpr int PT = 128, PLD = 129, PTHREADS = 256;
+// One level of the off-diagonal blocks of X = inv(L) in the shared tile of k_potrf_tile (X[i][c]
+// kept at [c][i]), the 4 - D block pairs (J, I = J + D):
+//   A. T = sum_{K=J}^{I-1} L_IK X_KJ, a TR x TC register tile per thread (rows i of block I,
+//      columns c of block J), written where X_IJ goes ([c][32I + i], which nothing at this level
+//      reads); X[k][c] is L[c][k] above c, dinv[c] on it, zero below
+//   B. X_IJ = -X_II T, one column c per thread, T's column in registers and X_II[i][m] (at
+//      [32I + m][32I + i]) read as a broadcast
+template <int D, int TR, int TC>
+__device__ inline void inv_level(double *L, const double *dinv) {
+  constexpr int TPP = (32 / TR) * (32 / TC), NP = 4 - D;      // tiles per pair, pairs
+  static_assert(NP * TPP <= PTHREADS, "one tile per thread");
+  const int tid = threadIdx.x;
+  if (tid < NP * TPP) {
+    const int J = tid / TPP, rem = tid % TPP, I = J + D;
+    const int i0 = 32 * I + (rem / (32 / TC)) * TR, c0 = 32 * J + (rem % (32 / TC)) * TC;
+    double acc[TR][TC];
+#pragma unroll
+    for (int u = 0; u < TR; ++u)
+#pragma unroll
+      for (int v = 0; v < TC; ++v) acc[u][v] = 0.0;
+#pragma unroll 4
+    for (int k = 32 * J; k < 32 * I; ++k) {
+      double lr[TR], xc[TC];
+#pragma unroll
+      for (int u = 0; u < TR; ++u) lr[u] = L[(i0 + u) * PLD + k];
+#pragma unroll
+      for (int v = 0; v < TC; ++v) {
+        const int c = c0 + v;
+        const double up = L[c * PLD + k];
+        xc[v] = k > c ? up : (k == c ? dinv[c] : 0.0);
+      }
+#pragma unroll
+      for (int u = 0; u < TR; ++u)
+#pragma unroll
+        for (int v = 0; v < TC; ++v) acc[u][v] += lr[u] * xc[v];
+    }
+#pragma unroll
+    for (int u = 0; u < TR; ++u)
+#pragma unroll
+      for (int v = 0; v < TC; ++v) L[(c0 + v) * PLD + i0 + u] = acc[u][v];
+  }
+  __syncthreads();
+  if (tid < NP * 32) {
+    const int J = tid >> 5, I = J + D, c = 32 * J + (tid & 31), b = 32 * I;
+    double t[32];
+#pragma unroll
+    for (int m = 0; m < 32; ++m) t[m] = L[c * PLD + b + m];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+      double x0 = dinv[b + i] * t[i], x1 = 0.0;
+#pragma unroll
+      for (int m = 0; m + 1 < i; m += 2) {
+        x0 += L[(b + m) * PLD + b + i] * t[m];
+        x1 += L[(b + m + 1) * PLD + b + i] * t[m + 1];
+      }
+      if (i & 1) x0 += L[(b + i - 1) * PLD + b + i] * t[i - 1];
+      L[c * PLD + b + i] = -(x0 + x1);
+    }
+  }
+  __syncthreads();
+}
 constexpr size_t POT_SMEM = sizeof(double) * ((size_t)PT * PLD + PT);   // 130 KB: fits beside a GEMM CTA
 __global__ void __launch_bounds__(PTHREADS, 1) k_potrf_tile(double *__restrict__ H, int64_t ldh, int64_t k0, int nb,
                                                            double *__restrict__ Linv, int *err) {
   extern __shared__ double L[];                      // [PT][PLD], then dinv[PT]
   double *dinv = L + PT * PLD;
+  __shared__ __align__(16) double colj[32];
   __shared__ int bad;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr unsigned FULL = 0xffffffffu;
@@ -308,7 +371,7 @@ __global__ void __launch_bounds__(PTHREADS, 1) k_potrf_tile(double *__restrict__
   __syncthreads();
   for (int j0 = 0; j0 < PT; j0 += 32) {
     // 1. D = L_D L_D^T with row lane of D in lane's registers (loops unrolled: every register
-    //    index is a constant), then X_D = inv(L_D) with column lane in registers
+    //    index is a constant)
     if (warp == 0) {
       double a[32];
       double *row = L + (j0 + lane) * PLD + j0;            // row lane of D
@@ -326,67 +389,38 @@ __global__ void __launch_bounds__(PTHREADS, 1) k_potrf_tile(double *__restrict__
         a[j] = lane == j ? s : (lane > j ? a[j] * inv : 0.0);
         if (lane == 0) dinv[j0 + j] = inv;
         const double aj = a[j];
+        colj[lane] = aj;                                   // column j of L_D, read back as a broadcast
+        __syncwarp();
 #pragma unroll
-        for (int q = 0; q < 32; ++q) {                     // (q <= j folds away: both are constants)
-          const double lq = __shfl_sync(FULL, aj, q);      // L[q][j]
-          if (q > j && lane >= q) a[q] -= aj * lq;
-        }
+        for (int q = j + 1; q < 32; ++q)
+          if (lane >= q) a[q] -= aj * colj[q];             // colj[q] = L[q][j]
+        __syncwarp();                                      // colj is rewritten at the next step
       }
 #pragma unroll
       for (int q = 0; q < 32; ++q)
         if (q <= lane) row[q] = a[q];                      // L[lane][q]
       if (lbad && lane == 0) bad = 1;
       __syncwarp();
-      // column c = lane of X_D: X[i][c] = (delta_ic - sum_{m<i} L[i][m] X[m][c]) / L[i][i]
-      // (X[m][c] = 0 for m < c; two partial sums halve the dependent chain), kept at [c][i]
-      double x[32];
-#pragma unroll
-      for (int i = 0; i < 32; ++i) {
-        const double *li = L + (j0 + i) * PLD + j0;
-        double t0 = i == lane ? 1.0 : 0.0, t1 = 0.0;
-#pragma unroll
-        for (int m = 0; m + 1 < i; m += 2) {
-          t0 -= li[m] * x[m];
-          t1 -= li[m + 1] * x[m + 1];
-        }
-        if (i & 1) t0 -= li[i - 1] * x[i - 1];
-        x[i] = i >= lane ? (t0 + t1) * dinv[j0 + i] : 0.0;
-      }
-#pragma unroll
-      for (int i = 0; i < 32; ++i)
-        if (i > lane) row[i] = x[i];
     }
     __syncthreads();
     const int t0 = j0 + 32, nr = PT - t0;
     if (nr == 0) break;
-    // 2. rows below: L[r][j0 + c] = sum_{k <= c} A[r][j0 + k] X[c][k]  (lane = c; column c of
-    //    X_D^T in registers, zero above its diagonal)
-    {
-      double xc[32];
+    // 2. rows below by substitution, one row per thread:
+    //    L[r][j0 + c] = (A[r][j0 + c] - sum_{k<c} L[r][j0 + k] L[j0 + c][j0 + k]) / L[j0 + c][j0 + c]
+    if (tid < nr) {
+      const int r = t0 + tid;
+      double a[32];
 #pragma unroll
-      for (int k = 0; k < 32; ++k)
-        xc[k] = k < lane ? L[(j0 + k) * PLD + j0 + lane] : (k == lane ? dinv[j0 + lane] : 0.0);
-      double out[12];
+      for (int k = 0; k < 32; ++k) a[k] = L[r * PLD + j0 + k];
 #pragma unroll
-      for (int u = 0; u < 12; ++u) out[u] = 0.0;
-#pragma unroll 2
-      for (int u = 0; u < 12; ++u) {
-        const int r = t0 + warp + 8 * u;
-        if (r < PT) {
-          const double *ar = L + r * PLD + j0;
-          double s = 0.0;
+      for (int c = 0; c < 32; ++c) {
+        const double l = a[c] * dinv[j0 + c];
+        a[c] = l;
 #pragma unroll
-          for (int k = 0; k < 32; ++k) s += ar[k] * xc[k];
-#pragma unroll
-          for (int v = 0; v < 12; ++v) out[v] = v == u ? s : out[v];
-        }
+        for (int q = c + 1; q < 32; ++q) a[q] -= l * L[(j0 + q) * PLD + j0 + c];
       }
-      __syncthreads();
 #pragma unroll
-      for (int u = 0; u < 12; ++u) {
-        const int r = t0 + warp + 8 * u;
-        if (r < PT) L[r * PLD + j0 + lane] = out[u];
-      }
+      for (int k = 0; k < 32; ++k) L[r * PLD + j0 + k] = a[k];
     }
     __syncthreads();
     // 3. trailing lower triangle of rows/columns [t0, PT): 4 x 4 tiles (ti >= tj)
@@ -425,57 +459,53 @@ __global__ void __launch_bounds__(PTHREADS, 1) k_potrf_tile(double *__restrict__
     }
     __syncthreads();
   }
-  if (bad && tid == 0) atomicOr(err, 1);
-  // the off-diagonal blocks of X, by distance d (level d reads only levels < d and the diagonal):
-  // g = 2, 4, 8 adjacent lanes per column c of the 4 - d block pairs (J = pair, I = J + d) sum
-  // their shares of the depth 32 d into T[:, c] = sum_{k in [32J, 32I)} L[I rows][k] X[k][c]
-  // (32 rows in registers), the shares meet by butterfly shuffles, then X_IJ[:, c] = -X_II T[:, c]
-  // with the rows split over the group.  No shared scratch: X_IJ goes to [c][i], which nothing
-  // at this level reads.
-  for (int d = 1; d < 4; ++d) {
-    const int g = 1 << d, share = 32 * d / g;          // 2, 4, 8 lanes; depth shares 16, 16, 12
-    const bool on = tid < (4 - d) * 32 * g;            // whole warps (192 or 256 threads)
-    const int col = tid / g, part = tid % g;
-    const int J = col >> 5, I = J + d, c = 32 * J + (col & 31);
-    double t[32];
+  // the four 32 x 32 diagonal inverses X_II, warp I each
+  if (warp < 4) {
+    const int j0 = 32 * warp;
+    double *row = L + (j0 + lane) * PLD + j0;
+    // column c = lane of X_D: X[i][c] = (delta_ic - sum_{m<i} L[i][m] X[m][c]) / L[i][i]
+    // (X[m][c] = 0 for m < c; two partial sums halve the dependent chain), kept at [c][i]
+    double x[32];
 #pragma unroll
-    for (int r = 0; r < 32; ++r) t[r] = 0.0;
-    if (on) {
-      const int kb = 32 * J + part * share;
-      for (int kk = 0; kk < share; ++kk) {
-        const int k = kb + (kk + part) % share;         // parts start apart: no shared bank
-        const double up = L[c * PLD + k];
-        const double x = k > c ? up : (k == c ? dinv[c] : 0.0);
-        const double *lk = L + 32 * I * PLD + k;
+    for (int i = 0; i < 32; ++i) {
+      const double *li = L + (j0 + i) * PLD + j0;
+      double t0 = i == lane ? 1.0 : 0.0, t1 = 0.0;
 #pragma unroll
-        for (int r = 0; r < 32; ++r) t[r] += lk[r * PLD] * x;
+      for (int m = 0; m + 1 < i; m += 2) {
+        t0 -= li[m] * x[m];
+        t1 -= li[m + 1] * x[m + 1];
       }
+      if (i & 1) t0 -= li[i - 1] * x[i - 1];
+      x[i] = i >= lane ? (t0 + t1) * dinv[j0 + i] : 0.0;
     }
-    for (int off = 1; off < g; off <<= 1)
 #pragma unroll
-      for (int r = 0; r < 32; ++r) t[r] += __shfl_xor_sync(FULL, t[r], off);
-    if (on) {
-#pragma unroll
-      for (int r = 0; r < 32; ++r) {
-        if (r % g != part) continue;
-        const int i = 32 * I + r;
-        double x = dinv[i] * t[r];
-#pragma unroll
-        for (int m = 0; m < r; ++m) x += L[(32 * I + m) * PLD + i] * t[m];   // X_II[i][m] at [m][i]
-        L[c * PLD + i] = -x;
-      }
-    }
-    __syncthreads();
+    for (int i = 0; i < 32; ++i)
+      if (i > lane) row[i] = x[i];
   }
+  __syncthreads();
+  if (bad && tid == 0) atomicOr(err, 1);
+  // the off-diagonal blocks of X by distance D = I - J (level D reads only the diagonal inverses
+  // and the levels below it)
+  inv_level<1, 4, 4>(L, dinv);
+  inv_level<2, 4, 2>(L, dinv);
+  inv_level<3, 2, 2>(L, dinv);
   // L back to H, inv(L) to Linv
 #pragma unroll 16
   for (int u = 0; u < PER; ++u) {
     const int e = tid + u * PTHREADS, r = e >> 7, c = e & (PT - 1);
     if (r < nb && c <= r) H[(k0 + r) * ldh + k0 + c] = L[r * PLD + c];
   }
-  for (int e = tid; e < nb * nb; e += PTHREADS) {
-    const int i = e / nb, c = e % nb;
-    Linv[e] = c > i ? 0.0 : (c == i ? dinv[i] : L[c * PLD + i]);
+  if (nb == PT) {
+#pragma unroll 16
+    for (int u = 0; u < PER; ++u) {
+      const int e = tid + u * PTHREADS, i = e >> 7, c = e & (PT - 1);
+      Linv[e] = c > i ? 0.0 : (c == i ? dinv[i] : L[c * PLD + i]);
+    }
+  } else {
+    for (int e = tid; e < nb * nb; e += PTHREADS) {
+      const int i = e / nb, c = e % nb;
+      Linv[e] = c > i ? 0.0 : (c == i ? dinv[i] : L[c * PLD + i]);
+    }
   }
 }
 
