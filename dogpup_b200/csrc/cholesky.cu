@@ -5,10 +5,10 @@
 // symmetric positive definite, i.e. a Cholesky factorisation and two triangular solves).
 //
 // H is row-major [n][ldh]; its lower triangle is read and overwritten by L (H = L L^T); the
-// strict upper triangle is not touched.  Right-looking, 512-column outer panels of 128-column
+// strict upper triangle is not touched.  Right-looking, 1024-column outer panels of 128-column
 // steps:
 //
-//   for each step k (columns [k0, k0 + 128)) of the outer panel [o0, o0 + 512):
+//   for each step k (columns [k0, k0 + 128)) of the outer panel [o0, o0 + 1024):
 //     k_potrf_tile   the 128 x 128 diagonal block: L_kk in place, and inv(L_kk) into a scratch
 //                    table (one CTA, block in shared memory: 32-column steps, a warp factors the
 //                    32 x 32 diagonal, all warps solve and update the rest; the inverse by
@@ -16,7 +16,7 @@
 //     k_dgemm_nt     panel: L_ik = A_ik inv(L_kk)^T for the rows below (in place: a CTA owns
 //                    whole 128-row strips of the panel)
 //     k_dgemm_nt     update of the outer panel's remaining columns: A_il -= L_ik L_lk^T
-//   k_dgemm_nt       trailing update of the rest, depth 512: A_il -= sum over the outer panel
+//   k_dgemm_nt       trailing update of the rest, depth 1024: A_il -= sum over the outer panel
 //
 // k_dgemm_nt: C = beta C + alpha A B^T with A, B row-major (K contiguous); 128 x 64 CTA tiles,
 // two CTAs per SM, 256 threads (8 warps of 32 x 32), K in stages of 16 doubles moved by cp.async
@@ -56,7 +56,7 @@ constexpr int gemm_smem(int gbn) {
 }
 constexpr int GV = 256;          // k per CTA of the solves' off-diagonal partial sums
 #ifndef DGP_CHOL_NBO
-#define DGP_CHOL_NBO 512
+#define DGP_CHOL_NBO 1024
 #endif
 constexpr int64_t NBO = DGP_CHOL_NBO;  // outer panel width: depth of the trailing update GEMM
 
@@ -852,23 +852,25 @@ int gemm_nt(const Gemm &g, cudaStream_t st) {
 // The two streams and four events of the lookahead; the destructor waits for both streams, so
 // that an early error return never frees buffers that queued kernels still use.
 struct LookaheadStreams {
-  cudaStream_t f = nullptr, r = nullptr;
-  cudaEvent_t fork = nullptr, panel = nullptr, rest = nullptr, join = nullptr;
+  cudaStream_t f = nullptr, s = nullptr, r = nullptr;
+  cudaEvent_t fork = nullptr, panel = nullptr, rest = nullptr, join = nullptr, step = nullptr, side = nullptr;
   int create() {
     int lo = 0, hi = 0;
     DGP_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
     DGP_CUDA(cudaStreamCreateWithPriority(&f, cudaStreamNonBlocking, hi));
+    DGP_CUDA(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, hi));
     DGP_CUDA(cudaStreamCreateWithPriority(&r, cudaStreamNonBlocking, lo));
-    for (cudaEvent_t *e : {&fork, &panel, &rest, &join}) DGP_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    for (cudaEvent_t *e : {&fork, &panel, &rest, &join, &step, &side})
+      DGP_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     return DGP_OK;
   }
   ~LookaheadStreams() {
-    if (f) cudaStreamSynchronize(f);
-    if (r) cudaStreamSynchronize(r);
-    for (cudaEvent_t e : {fork, panel, rest, join})
+    for (cudaStream_t q : {f, s, r})
+      if (q) cudaStreamSynchronize(q);
+    for (cudaEvent_t e : {fork, panel, rest, join, step, side})
       if (e) cudaEventDestroy(e);
-    if (f) cudaStreamDestroy(f);
-    if (r) cudaStreamDestroy(r);
+    for (cudaStream_t q : {f, s, r})
+      if (q) cudaStreamDestroy(q);
   }
 };
 
@@ -893,22 +895,27 @@ int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_
   DGP_CUDA(cudaFuncSetAttribute(k_potrf_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pot_smem));
   double *Li = linv.as<double>();
   int64_t launches = 0;
-  // Lookahead on two streams forked from st: sf (high priority) factors the outer panels and
-  // gives the next outer panel its update; sr (low priority) updates the rest of the matrix.
+  // Lookahead on three streams forked from st: sf (high priority) factors the outer panels and
+  // gives the next outer panel its update; ss (high priority) takes the off-chain part of each
+  // step's update; sr (low priority) updates the rest of the matrix.
   // Outer panel p = columns [o0, oend), next panel [oend, nend):
-  //   sf:  F_p   the 128-column steps of panel p (diagonal block, the rows below, the panel's own
-  //              remaining columns)
-  //        N_p   rows [oend, n) x columns [oend, nend) -= Q Q_next^T, Q = panel p's rows  (after
+  //   sf:  F_p   the 128-column steps of panel p: the diagonal block, the rows below, then the
+  //              next step's diagonal block (its update and its factorisation)
+  //   ss:        beside that, the step's update of the panel's other remaining columns (the
+  //              panel's rows, and the rows below it), which sf waits for before the next rows below
+  //   sf:  N_p   rows [oend, n) x columns [oend, nend) -= Q Q_next^T, Q = panel p's rows  (after
   //              R_{p-1}, which updates the same entries)
   //   sr:  R_p   the lower triangle of [nend, n)^2 -= Q Q^T  (after F_p)
-  // so F_{p+1} runs while R_p does, and the GEMMs of the whole factorisation keep their depth 512.
+  // so F_{p+1} runs while R_p does, and the trailing GEMMs keep the outer panel width as depth.
   LookaheadStreams ls;
   DGP_TRY(ls.create());
   DGP_CUDA(cudaEventRecord(ls.fork, st));
   DGP_CUDA(cudaStreamWaitEvent(ls.f, ls.fork, 0));
+  DGP_CUDA(cudaStreamWaitEvent(ls.s, ls.fork, 0));
   DGP_CUDA(cudaStreamWaitEvent(ls.r, ls.fork, 0));
-  cudaStream_t sf = ls.f, sr = ls.r;
+  cudaStream_t sf = ls.f, ss = ls.s, sr = ls.r;
   bool r_recorded = false;
+  bool side_pending = false;   // a step's off-chain updates queued on ss that sf has not waited for
   for (int64_t o0 = 0; o0 < n; o0 += NBO) {
     const int64_t oend = std::min(n, o0 + NBO);
     bool last = false;
@@ -916,13 +923,19 @@ int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_
       const int64_t b = k0 / CB;
       const int nb = (int)std::min<int64_t>(CB, n - k0);
       double *Lb = Li + b * CB * CB;
-      k_potrf_tile<<<1, PTHREADS, pot_smem, sf>>>(H, ldh, k0, nb, Lb, errb.as<int>());
-      DGP_CHECK_LAUNCH();
-      ++launches;
+      if (k0 == o0) {  // a later step's diagonal block was started by the step before it
+        k_potrf_tile<<<1, PTHREADS, pot_smem, sf>>>(H, ldh, k0, nb, Lb, errb.as<int>());
+        DGP_CHECK_LAUNCH();
+        ++launches;
+      }
       const int64_t kend = k0 + nb, rest = n - kend;
       if (rest <= 0) {
         last = true;
         break;
+      }
+      if (side_pending) {  // the rows below carry the previous step's off-chain updates
+        DGP_CUDA(cudaStreamWaitEvent(sf, ls.side, 0));
+        side_pending = false;
       }
       // L_ik = A_ik inv(L_kk)^T for every row below (in place, one CTA per 128-row strip)
       const Gemm p{H + kend * ldh + k0, ldh, Lb, nb, H + kend * ldh + k0, ldh, rest, nb, nb, 1.0, 0.0, 0, 0};
@@ -930,16 +943,36 @@ int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_
       ++launches;
       const int64_t w = oend - kend;  // the outer panel's remaining columns
       if (w > 0) {
-        const Gemm a{H + kend * ldh + k0, ldh, H + kend * ldh + k0, ldh, H + kend * ldh + kend, ldh, w, w, nb,
-                     -1.0, 1.0, 1, 0};
-        DGP_TRY(gemm_nt(a, sf));
-        ++launches;
+        // the next diagonal block's update, then its factorisation at once on sf; the rest of the
+        // step's update (the outer panel's remaining rows, and the rows below the outer panel in
+        // its remaining columns) on ss beside it
+        const int nb2 = (int)std::min<int64_t>(CB, w);
+        const int64_t k2 = kend + nb2, w2 = oend - k2;
+        DGP_CUDA(cudaEventRecord(ls.step, sf));
+        const Gemm a1{H + kend * ldh + k0, ldh, H + kend * ldh + k0, ldh, H + kend * ldh + kend, ldh, nb2, nb2, nb,
+                      -1.0, 1.0, 1, 0};
+        DGP_TRY(gemm_nt(a1, sf));
+        k_potrf_tile<<<1, PTHREADS, pot_smem, sf>>>(H, ldh, kend, nb2, Li + (b + 1) * CB * CB, errb.as<int>());
+        DGP_CHECK_LAUNCH();
+        launches += 2;
+        DGP_CUDA(cudaStreamWaitEvent(ss, ls.step, 0));
+        if (w2 > 0) {
+          const Gemm a2{H + k2 * ldh + k0, ldh, H + kend * ldh + k0, ldh, H + k2 * ldh + kend, ldh, w2, nb2, nb,
+                        -1.0, 1.0, 0, 0};
+          const Gemm a3{H + k2 * ldh + k0, ldh, H + k2 * ldh + k0, ldh, H + k2 * ldh + k2, ldh, w2, w2, nb,
+                        -1.0, 1.0, 1, 0};
+          DGP_TRY(gemm_nt(a2, ss));
+          DGP_TRY(gemm_nt(a3, ss));
+          launches += 2;
+        }
         if (n > oend) {
           const Gemm r{H + oend * ldh + k0, ldh, H + kend * ldh + k0, ldh, H + oend * ldh + kend, ldh, n - oend, w,
                        nb, -1.0, 1.0, 0, 0};
-          DGP_TRY(gemm_nt(r, sf));
+          DGP_TRY(gemm_nt(r, ss));
           ++launches;
         }
+        DGP_CUDA(cudaEventRecord(ls.side, ss));
+        side_pending = true;
       }
     }
     if (last || n <= oend) break;
@@ -966,6 +999,7 @@ int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_
     }
   }
   if (r_recorded) DGP_CUDA(cudaStreamWaitEvent(sf, ls.rest, 0));
+  if (side_pending) DGP_CUDA(cudaStreamWaitEvent(sf, ls.side, 0));
   // L y = b, then L^T x = y: one right-hand side as two chained launches where every CTA fits on
   // the GPU at once, else (and for several right-hand sides) by 128-row blocks
   int crc = DGP_OK;
