@@ -5,10 +5,10 @@
 // symmetric positive definite, i.e. a Cholesky factorisation and two triangular solves).
 //
 // H is row-major [n][ldh]; its lower triangle is read and overwritten by L (H = L L^T); the
-// strict upper triangle is not touched.  Right-looking, 1024-column outer panels of 128-column
+// strict upper triangle is not touched.  Right-looking, 1536-column outer panels of 128-column
 // steps:
 //
-//   for each step k (columns [k0, k0 + 128)) of the outer panel [o0, o0 + 1024):
+//   for each step k (columns [k0, k0 + 128)) of the outer panel [o0, o0 + 1536):
 //     k_potrf_tile   the 128 x 128 diagonal block: L_kk in place, and inv(L_kk) into a scratch
 //                    table (one CTA, block in shared memory: 32-column steps, a warp factors the
 //                    32 x 32 diagonal, all warps solve and update the rest; the inverse by
@@ -16,7 +16,7 @@
 //     k_dgemm_nt     panel: L_ik = A_ik inv(L_kk)^T for the rows below (in place: a CTA owns
 //                    whole 128-row strips of the panel)
 //     k_dgemm_nt     update of the outer panel's remaining columns: A_il -= L_ik L_lk^T
-//   k_dgemm_nt       trailing update of the rest, depth 1024: A_il -= sum over the outer panel
+//   k_dgemm_nt       trailing update of the rest, depth 1536: A_il -= sum over the outer panel
 //
 // k_dgemm_nt: C = beta C + alpha A B^T with A, B row-major (K contiguous); 128 x 64 CTA tiles,
 // two CTAs per SM, 256 threads (8 warps of 32 x 32), K in stages of 16 doubles moved by cp.async
@@ -56,7 +56,7 @@ constexpr int gemm_smem(int gbn) {
 }
 constexpr int GV = 256;          // k per CTA of the solves' off-diagonal partial sums
 #ifndef DGP_CHOL_NBO
-#define DGP_CHOL_NBO 1024
+#define DGP_CHOL_NBO 1536
 #endif
 constexpr int64_t NBO = DGP_CHOL_NBO;  // outer panel width: depth of the trailing update GEMM
 
@@ -852,24 +852,26 @@ int gemm_nt(const Gemm &g, cudaStream_t st) {
 // The two streams and four events of the lookahead; the destructor waits for both streams, so
 // that an early error return never frees buffers that queued kernels still use.
 struct LookaheadStreams {
-  cudaStream_t f = nullptr, s = nullptr, r = nullptr;
-  cudaEvent_t fork = nullptr, panel = nullptr, rest = nullptr, join = nullptr, step = nullptr, side = nullptr;
+  cudaStream_t f = nullptr, s = nullptr, b = nullptr, r = nullptr;
+  cudaEvent_t fork = nullptr, panel = nullptr, rest = nullptr, join = nullptr, step = nullptr, side = nullptr,
+              diag = nullptr, below = nullptr;
   int create() {
     int lo = 0, hi = 0;
     DGP_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
     DGP_CUDA(cudaStreamCreateWithPriority(&f, cudaStreamNonBlocking, hi));
     DGP_CUDA(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, hi));
+    DGP_CUDA(cudaStreamCreateWithPriority(&b, cudaStreamNonBlocking, hi));
     DGP_CUDA(cudaStreamCreateWithPriority(&r, cudaStreamNonBlocking, lo));
-    for (cudaEvent_t *e : {&fork, &panel, &rest, &join, &step, &side})
+    for (cudaEvent_t *e : {&fork, &panel, &rest, &join, &step, &side, &diag, &below})
       DGP_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     return DGP_OK;
   }
   ~LookaheadStreams() {
-    for (cudaStream_t q : {f, s, r})
+    for (cudaStream_t q : {f, s, b, r})
       if (q) cudaStreamSynchronize(q);
-    for (cudaEvent_t e : {fork, panel, rest, join, step, side})
+    for (cudaEvent_t e : {fork, panel, rest, join, step, side, diag, below})
       if (e) cudaEventDestroy(e);
-    for (cudaStream_t q : {f, s, r})
+    for (cudaStream_t q : {f, s, b, r})
       if (q) cudaStreamDestroy(q);
   }
 };
@@ -895,14 +897,17 @@ int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_
   DGP_CUDA(cudaFuncSetAttribute(k_potrf_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pot_smem));
   double *Li = linv.as<double>();
   int64_t launches = 0;
-  // Lookahead on three streams forked from st: sf (high priority) factors the outer panels and
-  // gives the next outer panel its update; ss (high priority) takes the off-chain part of each
-  // step's update; sr (low priority) updates the rest of the matrix.
+  // Lookahead on four streams forked from st: sf (high priority) factors the outer panels and
+  // gives the next outer panel its update; ss and sb (high priority) take the off-chain parts of
+  // each panel's work; sr (low priority) updates the rest of the matrix.
   // Outer panel p = columns [o0, oend), next panel [oend, nend):
-  //   sf:  F_p   the 128-column steps of panel p: the diagonal block, the rows below, then the
-  //              next step's diagonal block (its update and its factorisation)
-  //   ss:        beside that, the step's update of the panel's other remaining columns (the
-  //              panel's rows, and the rows below it), which sf waits for before the next rows below
+  //   sf:  F_p   the 128-column steps of panel p on the panel's own rows: the diagonal block,
+  //              the rows below it, then the next step's diagonal block (update, factorisation)
+  //   ss:        beside that, the step's update of the panel's other remaining columns, which sf
+  //              waits for before the next step's rows
+  //   sb:        the rows under the panel, left-looking per 128-column block (the update by the
+  //              panel's earlier columns, then the product with the block's inverse), off the step
+  //              chain; sf waits for them at the end of the panel
   //   sf:  N_p   rows [oend, n) x columns [oend, nend) -= Q Q_next^T, Q = panel p's rows  (after
   //              R_{p-1}, which updates the same entries)
   //   sr:  R_p   the lower triangle of [nend, n)^2 -= Q Q^T  (after F_p)
@@ -912,12 +917,14 @@ int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_
   DGP_CUDA(cudaEventRecord(ls.fork, st));
   DGP_CUDA(cudaStreamWaitEvent(ls.f, ls.fork, 0));
   DGP_CUDA(cudaStreamWaitEvent(ls.s, ls.fork, 0));
+  DGP_CUDA(cudaStreamWaitEvent(ls.b, ls.fork, 0));
   DGP_CUDA(cudaStreamWaitEvent(ls.r, ls.fork, 0));
-  cudaStream_t sf = ls.f, ss = ls.s, sr = ls.r;
+  cudaStream_t sf = ls.f, ss = ls.s, sb = ls.b, sr = ls.r;
   bool r_recorded = false;
   bool side_pending = false;   // a step's off-chain updates queued on ss that sf has not waited for
   for (int64_t o0 = 0; o0 < n; o0 += NBO) {
     const int64_t oend = std::min(n, o0 + NBO);
+    const bool below = n > oend;  // rows under the outer panel: left-looking on sb, off the step chain
     bool last = false;
     for (int64_t k0 = o0; k0 < oend; k0 += CB) {
       const int64_t b = k0 / CB;
@@ -928,52 +935,65 @@ int cholesky_solve_many_run(double *H, int64_t n, int64_t ldh, double *x, int32_
         DGP_CHECK_LAUNCH();
         ++launches;
       }
+      if (below) {
+        // rows [oend, n) of column block k: minus the panel's earlier columns (depth k0 - o0), then
+        // L = A inv(L_kk)^T in place; after this step's diagonal block and the rows of block k in
+        // the earlier columns (both on sf before this point)
+        DGP_CUDA(cudaEventRecord(ls.diag, sf));
+        DGP_CUDA(cudaStreamWaitEvent(sb, ls.diag, 0));
+        if (k0 > o0) {
+          const Gemm u{H + oend * ldh + o0, ldh, H + k0 * ldh + o0, ldh, H + oend * ldh + k0, ldh, n - oend, nb,
+                       k0 - o0, -1.0, 1.0, 0, 0};
+          DGP_TRY(gemm_nt(u, sb));
+          ++launches;
+        }
+        const Gemm pb{H + oend * ldh + k0, ldh, Lb, nb, H + oend * ldh + k0, ldh, n - oend, nb, nb, 1.0, 0.0, 0, 0};
+        DGP_TRY(gemm_nt(pb, sb));
+        ++launches;
+      }
       const int64_t kend = k0 + nb, rest = n - kend;
       if (rest <= 0) {
         last = true;
         break;
       }
-      if (side_pending) {  // the rows below carry the previous step's off-chain updates
+      const int64_t w = oend - kend;  // the outer panel's remaining columns (and rows)
+      if (w == 0) continue;
+      if (side_pending) {  // those rows carry the previous step's off-chain updates
         DGP_CUDA(cudaStreamWaitEvent(sf, ls.side, 0));
         side_pending = false;
       }
-      // L_ik = A_ik inv(L_kk)^T for every row below (in place, one CTA per 128-row strip)
-      const Gemm p{H + kend * ldh + k0, ldh, Lb, nb, H + kend * ldh + k0, ldh, rest, nb, nb, 1.0, 0.0, 0, 0};
+      // L_ik = A_ik inv(L_kk)^T for the outer panel's rows below the block (in place, one CTA per
+      // 128-row strip)
+      const Gemm p{H + kend * ldh + k0, ldh, Lb, nb, H + kend * ldh + k0, ldh, w, nb, nb, 1.0, 0.0, 0, 0};
       DGP_TRY(gemm_nt(p, sf));
       ++launches;
-      const int64_t w = oend - kend;  // the outer panel's remaining columns
-      if (w > 0) {
-        // the next diagonal block's update, then its factorisation at once on sf; the rest of the
-        // step's update (the outer panel's remaining rows, and the rows below the outer panel in
-        // its remaining columns) on ss beside it
-        const int nb2 = (int)std::min<int64_t>(CB, w);
-        const int64_t k2 = kend + nb2, w2 = oend - k2;
-        DGP_CUDA(cudaEventRecord(ls.step, sf));
-        const Gemm a1{H + kend * ldh + k0, ldh, H + kend * ldh + k0, ldh, H + kend * ldh + kend, ldh, nb2, nb2, nb,
-                      -1.0, 1.0, 1, 0};
-        DGP_TRY(gemm_nt(a1, sf));
-        k_potrf_tile<<<1, PTHREADS, pot_smem, sf>>>(H, ldh, kend, nb2, Li + (b + 1) * CB * CB, errb.as<int>());
-        DGP_CHECK_LAUNCH();
-        launches += 2;
+      // the next diagonal block's update, then its factorisation at once on sf; the rest of the
+      // step's update of the outer panel's remaining columns on ss beside it
+      const int nb2 = (int)std::min<int64_t>(CB, w);
+      const int64_t k2 = kend + nb2, w2 = oend - k2;
+      DGP_CUDA(cudaEventRecord(ls.step, sf));
+      const Gemm a1{H + kend * ldh + k0, ldh, H + kend * ldh + k0, ldh, H + kend * ldh + kend, ldh, nb2, nb2, nb,
+                    -1.0, 1.0, 1, 0};
+      DGP_TRY(gemm_nt(a1, sf));
+      k_potrf_tile<<<1, PTHREADS, pot_smem, sf>>>(H, ldh, kend, nb2, Li + (b + 1) * CB * CB, errb.as<int>());
+      DGP_CHECK_LAUNCH();
+      launches += 2;
+      if (w2 > 0) {
         DGP_CUDA(cudaStreamWaitEvent(ss, ls.step, 0));
-        if (w2 > 0) {
-          const Gemm a2{H + k2 * ldh + k0, ldh, H + kend * ldh + k0, ldh, H + k2 * ldh + kend, ldh, w2, nb2, nb,
-                        -1.0, 1.0, 0, 0};
-          const Gemm a3{H + k2 * ldh + k0, ldh, H + k2 * ldh + k0, ldh, H + k2 * ldh + k2, ldh, w2, w2, nb,
-                        -1.0, 1.0, 1, 0};
-          DGP_TRY(gemm_nt(a2, ss));
-          DGP_TRY(gemm_nt(a3, ss));
-          launches += 2;
-        }
-        if (n > oend) {
-          const Gemm r{H + oend * ldh + k0, ldh, H + kend * ldh + k0, ldh, H + oend * ldh + kend, ldh, n - oend, w,
-                       nb, -1.0, 1.0, 0, 0};
-          DGP_TRY(gemm_nt(r, ss));
-          ++launches;
-        }
+        const Gemm a2{H + k2 * ldh + k0, ldh, H + kend * ldh + k0, ldh, H + k2 * ldh + kend, ldh, w2, nb2, nb,
+                      -1.0, 1.0, 0, 0};
+        const Gemm a3{H + k2 * ldh + k0, ldh, H + k2 * ldh + k0, ldh, H + k2 * ldh + k2, ldh, w2, w2, nb,
+                      -1.0, 1.0, 1, 0};
+        DGP_TRY(gemm_nt(a2, ss));
+        DGP_TRY(gemm_nt(a3, ss));
+        launches += 2;
         DGP_CUDA(cudaEventRecord(ls.side, ss));
         side_pending = true;
       }
+    }
+    if (below) {  // the outer panel's rows below it are final before its updates of the rest
+      DGP_CUDA(cudaEventRecord(ls.below, sb));
+      DGP_CUDA(cudaStreamWaitEvent(sf, ls.below, 0));
     }
     if (last || n <= oend) break;
     const int64_t nend = std::min(n, oend + NBO), depth = oend - o0;

@@ -48,12 +48,13 @@ def test_normal_equations_match_fp64(nv, nm):
     assert np.linalg.norm(rhs.cpu().numpy() - r0) / np.linalg.norm(r0) < 1e-12
 
 
-@pytest.mark.parametrize("n,pad", [(333, 0), (1100, 7), (2501, 3), (128, 0), (129, 1)])
+@pytest.mark.parametrize("n,pad", [(333, 0), (1100, 7), (2501, 3), (3333, 0), (128, 0), (129, 1)])
 def test_cholesky_solve_exact_matrix(n, pad):
     """n > 128 crosses the 128-column panels (diagonal factor + inverse, panel GEMM, trailing
-    lower-triangle GEMM on the FP64 tensor cores) with a partial last panel; pad > 0 tests
-    ldh > n (an odd ldh takes the 8-byte copy path of the GEMM); the strict upper triangle holds
-    NaN and must never be read.  Solution 1e-10 against NumPy, L L^T 1e-13."""
+    lower-triangle GEMM on the FP64 tensor cores) with a partial last panel; n > 1536 crosses the
+    outer panels (the rows under each one, their update of the rest); pad > 0 tests ldh > n, and
+    an odd ldh (n = 333, 1100, 3333) takes the 8-byte copy path of the GEMM; the strict upper
+    triangle holds NaN and must never be read.  Solution 1e-10 against NumPy, L L^T 1e-13."""
     import torch
     from dogpup_b200._lib import lib, check
     rng = np.random.default_rng(3)
