@@ -456,10 +456,11 @@ def lm_step_bench(reps=2, grid_mm=2.0):
     rng = np.random.default_rng(9)
     W = torch.as_tensor(1.0 / (0.01 * (1 + rng.random(nmeas))) ** 2, device="cuda")
     y = torch.as_tensor(rng.standard_normal(nmeas) * 0.01, device="cuda")
-    H = torch.empty((nv, nv), dtype=torch.float64, device="cuda")
+    ld = nv + (nv & 1)                                  # even: 16-byte aligned rows, as dgp_lm_update uses
+    H = torch.empty((nv, ld), dtype=torch.float64, device="cuda")
     x = torch.empty(nv, dtype=torch.float64, device="cuda")
     v = lambda t: C.c_void_p(t.data_ptr())
-    ms_ne = _event_ms(lambda: check(lib.dgp_normal_eq(v(Jt), nv, nmeas, v(W), v(y), 1e-2, 0, v(H), nv, v(x),
+    ms_ne = _event_ms(lambda: check(lib.dgp_normal_eq(v(Jt), nv, nmeas, v(W), v(y), 1e-2, 0, v(H), ld, v(x),
                                                       api.stream_ptr())), reps)
     Hc = H.clone()
     xc = x.clone()
@@ -467,7 +468,7 @@ def lm_step_bench(reps=2, grid_mm=2.0):
     def restore():                                      # the factorisation overwrites Hc
         Hc.copy_(H)
         xc.copy_(x)
-    ms_chol = _event_ms_restored(restore, lambda: check(lib.dgp_cholesky_solve(v(Hc), nv, nv, v(xc),
+    ms_chol = _event_ms_restored(restore, lambda: check(lib.dgp_cholesky_solve(v(Hc), nv, ld, v(xc),
                                                                               api.stream_ptr())), reps)
     syrk_flops = 3 * 2.0 * nmeas * nv * (nv + 128) / 2
     # the same LM update from all-FP64 normal equations (cuBLAS DGEMM) and the FP64 Cholesky

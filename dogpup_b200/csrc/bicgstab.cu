@@ -1691,15 +1691,15 @@ void tspmm_launch(const SolverPlan *S, const TiledPlan &T, const int32_t *rowptr
   k_tspmm<MODE, SW, Op><<<grid, BS, tile_smem(T, SW, MODE), st>>>(L, op, X, Y, Wv, cols, ctl, T.hmax);
 }
 
-// dynamic shared-memory limits of the three modes, large enough for every plan in Ts
+// dynamic shared-memory sizes of the three modes for every plan in Ts, checked against the device
 template <int SW, class Op>
 int tspmm_attrs(std::initializer_list<const TiledPlan *> Ts) {
   size_t b[3] = {0, 0, 0};
   for (const TiledPlan *T : Ts)
     for (int m = 0; m < 3; ++m) b[m] = std::max(b[m], tile_smem(*T, SW, m));
-  DGP_CUDA(cudaFuncSetAttribute(k_tspmm<0, SW, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b[0]));
-  DGP_CUDA(cudaFuncSetAttribute(k_tspmm<1, SW, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b[1]));
-  DGP_CUDA(cudaFuncSetAttribute(k_tspmm<2, SW, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b[2]));
+  DGP_TRY(allow_dyn_smem(k_tspmm<0, SW, Op>, b[0]));
+  DGP_TRY(allow_dyn_smem(k_tspmm<1, SW, Op>, b[1]));
+  DGP_TRY(allow_dyn_smem(k_tspmm<2, SW, Op>, b[2]));
   return DGP_OK;
 }
 

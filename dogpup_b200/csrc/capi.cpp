@@ -69,6 +69,20 @@ int sm_count() {
   return n;
 }
 
+int allow_dyn_smem_impl(const void *kernel, size_t bytes) {
+  int dev = 0, optin = 0;
+  DGP_CUDA(cudaGetDevice(&dev));
+  DGP_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa;
+  DGP_CUDA(cudaFuncGetAttributes(&fa, kernel));
+  const int64_t cap = (int64_t)optin - (int64_t)fa.sharedSizeBytes;
+  if ((int64_t)bytes > cap)
+    return fail(DGP_ERR_ARG, "shared memory per block (" + std::to_string(bytes) + " bytes) above the device's " +
+                                 std::to_string(cap) + " for this kernel");
+  DGP_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap));
+  return DGP_OK;
+}
+
 int mex_spmv(int mode, double *out_re, double *out_im, const double *x_re, const double *x_im, const double *fAxis,
              const double *v_re, const double *v_im, const int *rPtr, const int *cPtr, int64_t nnz, int nrows,
              int ncols, int nfreqs, cudaStream_t st, int es = 1);

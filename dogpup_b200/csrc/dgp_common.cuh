@@ -46,6 +46,16 @@ int64_t launch_count();
 // Number of SMs of the current device (cached per device).
 int sm_count();
 
+// Allow `kernel` a dynamic shared-memory size of `bytes` (DGP_ERR_ARG when above what the device
+// gives one block beside the kernel's static shared memory).  The kernel's limit is always set to
+// that device maximum, never to the size of this call: the attribute is process-wide per kernel,
+// and a per-call size set by one host thread could lower the limit under another thread's larger
+// launch of the same kernel.
+int allow_dyn_smem_impl(const void *kernel, size_t bytes);
+template <class K> inline int allow_dyn_smem(K *kernel, size_t bytes) {
+  return allow_dyn_smem_impl(reinterpret_cast<const void *>(kernel), bytes);
+}
+
 // Device buffer owned by a plan; freed in the destructor.
 struct DevBuf {
   void *p = nullptr;

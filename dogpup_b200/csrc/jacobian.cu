@@ -898,8 +898,7 @@ int jacobian_run(int mode, const int32_t *prow, const int32_t *pcol, const doubl
   k_ctab<<<(unsigned)ceil_div(nt_, 256), 256, 0, st>>>((const double2 *)gate, (const double2 *)fpsf, mode == 1 ? 0 : ng,
                                                         nf, nt, ctab.as<float2>(), finv.as<double2>());
   DGP_CHECK_LAUNCH();
-  if (smem > 48 * 1024)
-    DGP_CUDA(cudaFuncSetAttribute(k_jacobian_complex, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (mode == 1) DGP_TRY(allow_dyn_smem(k_jacobian_complex, smem));
   const T2Layout tl = t2_layout(nf, std::max(1, ng));
   const size_t smem_tc = tl.bytes + 1024;
   // (+ 1 KB of the kernel's own static shared memory)
@@ -910,7 +909,7 @@ int jacobian_run(int mode, const int32_t *prow, const int32_t *pcol, const doubl
     DevBuf flag;
     DGP_TRY(flag.alloc(sizeof(int)));
     DGP_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), st));
-    DGP_CUDA(cudaFuncSetAttribute(k_jacobian_tg_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tc));
+    DGP_TRY(allow_dyn_smem(k_jacobian_tg_tc, smem_tc));
     const int gtc = (int)std::min<int64_t>(nv, (int64_t)sm_count());
     k_jacobian_tg_tc<<<gtc, T2_THREADS, smem_tc, st>>>(a, ctab.as<float2>(), rytov, dense, (float *)out,
                                                        flag.as<int>());
@@ -933,10 +932,11 @@ int jacobian_run(int mode, const int32_t *prow, const int32_t *pcol, const doubl
     DGP_CHECK_LAUNCH();
     const size_t smem_tg = sizeof(float2) * ((size_t)nf * (ns + nd) + 1 + (size_t)nf * ngc);
     DGP_REQUIRE(smem_tg <= 200 * 1024, "jacobian: NF*(NS+ND+NG) too large for one block's shared memory");
+    int arc = DGP_OK;
     auto go = [&](auto mtc, auto ngcc) {
       constexpr int MT_ = decltype(mtc)::value, NGC_ = decltype(ngcc)::value;
-      cudaFuncSetAttribute(k_jacobian_tg<MT_, NGC_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tg);
-      k_jacobian_tg<MT_, NGC_><<<grid, JBS, smem_tg, st>>>(a, ckg.as<float2>(), rytov, (float *)out);
+      arc = allow_dyn_smem(k_jacobian_tg<MT_, NGC_>, smem_tg);
+      if (arc == DGP_OK) k_jacobian_tg<MT_, NGC_><<<grid, JBS, smem_tg, st>>>(a, ckg.as<float2>(), rytov, (float *)out);
     };
     auto by_ngc = [&](auto mtc) {
       switch (ngc) {
@@ -949,6 +949,7 @@ int jacobian_run(int mode, const int32_t *prow, const int32_t *pcol, const doubl
     if (mt == 4) by_ngc(std::integral_constant<int, 4>());
     else if (mt == 2) by_ngc(std::integral_constant<int, 2>());
     else by_ngc(std::integral_constant<int, 1>());
+    DGP_TRY(arc);
     DGP_CHECK_LAUNCH();
     DGP_CUDA(cudaStreamSynchronize(st));  // ckg is released on return
   } else if (mode == 1) {
@@ -982,16 +983,18 @@ int jacobian_run(int mode, const int32_t *prow, const int32_t *pcol, const doubl
     const size_t per = sizeof(float2) * (size_t)nf * (ns + nd);
     const int vb = (int)std::min<size_t>(4, std::max<size_t>(1, (200 * 1024) / per));
     const size_t smem_v = per * vb;
+    int arc = DGP_OK;
     auto go = [&](auto vbc) {
       constexpr int VB_ = decltype(vbc)::value;
-      cudaFuncSetAttribute(k_jacobian_vjp<VB_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_v);
+      arc = allow_dyn_smem(k_jacobian_vjp<VB_>, smem_v);
       const int gv = (int)std::min<int64_t>(ceil_div(nv, VB_), (int64_t)sm_count() * 8);
-      k_jacobian_vjp<VB_><<<gv, JBS, smem_v, st>>>(a, chat.as<float2>(), (double *)out);
+      if (arc == DGP_OK) k_jacobian_vjp<VB_><<<gv, JBS, smem_v, st>>>(a, chat.as<float2>(), (double *)out);
     };
     if (vb >= 4) go(std::integral_constant<int, 4>());
     else if (vb == 3) go(std::integral_constant<int, 3>());
     else if (vb == 2) go(std::integral_constant<int, 2>());
     else go(std::integral_constant<int, 1>());
+    DGP_TRY(arc);
   }
   DGP_CHECK_LAUNCH();
   DGP_CUDA(cudaStreamSynchronize(st));  // scratch tables are released on return

@@ -226,3 +226,48 @@ def test_tg_jacobian_engine_switch_rejects_unknown_engines():
     from dogpup_b200._lib import lib
     assert lib.dgp_set_jacobian_engine(3) == 1 and lib.dgp_set_jacobian_engine(-1) == 1
     assert lib.dgp_set_jacobian_engine(2) == 0 and lib.dgp_set_jacobian_engine(0) == 0
+
+
+def test_vjp_from_several_host_threads(jac_case):
+    """Four host threads, each on its own stream, run the CUDA-core vjp on different harmonic
+    counts (different dynamic shared-memory sizes of the same kernel) at once, 25 times each:
+    every call succeeds and matches the same call made alone (1e-12).  The kernel's shared-memory limit
+    is process-wide, so one thread's launch must not depend on the size another thread set."""
+    import threading
+    import torch
+    from dogpup_b200 import api
+    from dogpup_b200._lib import lib, check
+    mesh = jac_case["mesh"]
+    nb = mesh.nodal_basis()
+    nt = len(mesh.optode.tAxis)
+    link = mesh._link()
+    g = torch.as_tensor(np.random.default_rng(4).standard_normal((link.shape[0], 20)))
+    fpsf = mesh.optode.s_fpsf
+    args = {k: (jac_case["phi"][:k].contiguous(), jac_case["phiA"][:k].contiguous(), fpsf[:k].contiguous(),
+                jac_case["gfc_d"][:, :k].contiguous()) for k in (16, 11, 6, 3)}
+    check(lib.dgp_set_jacobian_engine(1))
+    try:
+        alone = {k: api.jacobian_tg_vjp(nb, p, pa, f, link, gf, nt, g).cpu() for k, (p, pa, f, gf) in args.items()}
+        errors, results = [], {}
+
+        def work(k):
+            try:
+                s = torch.cuda.Stream()
+                with torch.cuda.stream(s):
+                    p, pa, f, gf = args[k]
+                    for _ in range(25):
+                        v = api.jacobian_tg_vjp(nb, p, pa, f, link, gf, nt, g)
+                    s.synchronize()
+                    results[k] = v.cpu()
+            except Exception as e:          # collected: the assertion below reports it
+                errors.append(repr(e))
+        threads = [threading.Thread(target=work, args=(k,)) for k in args]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+    finally:
+        check(lib.dgp_set_jacobian_engine(0))
+    assert not errors, errors
+    for k in args:
+        assert rel(results[k].numpy(), alone[k].numpy()) < 1e-12, k
