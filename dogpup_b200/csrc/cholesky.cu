@@ -849,7 +849,7 @@ int gemm_nt(const Gemm &g, cudaStream_t st) {
   return a16 ? gemm_launch<16, 64, false>(g, st) : gemm_launch<8, 64, false>(g, st);
 }
 
-// The two streams and four events of the lookahead; the destructor waits for both streams, so
+// The four streams and eight events of the lookahead; the destructor waits for every stream, so
 // that an early error return never frees buffers that queued kernels still use.
 struct LookaheadStreams {
   cudaStream_t f = nullptr, s = nullptr, b = nullptr, r = nullptr;
