@@ -800,11 +800,16 @@ bool trsv_chain(const double *H, int64_t ldh, int64_t n, const double *Linv, dou
   *rc = DGP_OK;
   const int nblk = (int)ceil_div(n, (int64_t)CB);
   int dev = 0, coop = 0, per_sm_f = 0, per_sm_b = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return false;
-  if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop) return false;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, k_trsv_chain<false>, TS_THREADS, 0) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_b, k_trsv_chain<true>, TS_THREADS, 0) != cudaSuccess)
+  // a query that fails leaves the per-block path; its error is cleared so that the next launch
+  // check does not report it
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, k_trsv_chain<false>, TS_THREADS, 0) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_b, k_trsv_chain<true>, TS_THREADS, 0) != cudaSuccess) {
+    (void)cudaGetLastError();
     return false;
+  }
+  if (!coop) return false;
   if ((int64_t)std::min(per_sm_f, per_sm_b) * sm_count() < nblk) return false;
   int vech = ((uintptr_t)H % 16 == 0) && ldh % 2 == 0;
   uint32_t *ff = flags, *fb = flags + nblk;
